@@ -1,0 +1,399 @@
+"""Benchmark: Born forward + adjoint (the FWI gradient kernel pair) of the
+elastic engine on the 600x1800 grid, nts=4000, 10 shots, one B200 per rank.
+
+One step = Born forward of every shot followed by the Born adjoint of every
+shot (image accumulated over shots) = 4 propagations per shot.
+Metric: cell-updates per second over the whole job (Gcell-updates/s).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value : device-resident inputs (single-shot *_reg_dev C entry points)
+e2e   : the reference-facing operator API (BornElasticShotsGpu.forward /
+        adjoint) with host buffers, host<->device copies inside the region
+reference arm (--impl reference): the reference's own CUDA drivers
+        (oracle/_ref, compiled from the reference tree for sm_100a), one shot
+        of the same workload per step.
+Shots are independent, so N > 1 ranks each take their own shots (weak
+scaling) and the image is summed with one all-reduce per step, the exchange
+the reference does on the host (BornElasticShotsGpu.cpp:313-323).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+BYTES_PER_CELL = 80.0    # read 5 current + 5 old + 5 medium, write 5 new (FP32)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--shots", type=int, default=10)
+    ap.add_argument("--nts", type=int, default=4000)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- helpers
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            cmd = ["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits", "-lms", "200"]
+            if self.gpu_id:
+                cmd += ["-i", self.gpu_id]
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per k_step launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "k_step_traffic.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch_full_size:"):
+                return float(line.split(":", 1)[1])
+    except Exception:
+        pass
+    return None
+
+
+def dist_init(args):
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, v):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------------------- our arm
+def run_ours(args, ws, rank, local):
+    import ctypes
+    import torch
+    from elastic_isotropic_operators_b200 import _lib, prop, synthetic
+
+    w = synthetic.born_600x1800(nts=args.nts, nshots=args.shots, seed=2024 + rank)
+    src, rec = w.geometry()
+    sig = [w.source_signal()]
+    dev = torch.device("cuda", local)
+    w.par.set("iGpu", str(local))
+    born = prop.BornElasticShotsGpu(w.elastic, w.par, sig, *src, *rec)
+    L = _lib.lib()
+    ctx = born.ctx
+    nsh = w.nExp
+    fine_steps, cells = ctypes.c_longlong(), ctypes.c_longlong()
+    _lib.check(L.eio_ctx_counts(ctx, ctypes.byref(fine_steps), ctypes.byref(cells)))
+    fine_steps, cells = fine_steps.value, cells.value
+    updates_per_step = 4.0 * nsh * fine_steps * cells     # fwd: 2 propagations, adj: 2
+
+    # ---- device-resident inputs
+    dm5 = [torch.from_numpy(a).to(dev) for a in born.prepareModel(w.extra["dmodel"])]
+    grad5 = [torch.zeros_like(a) for a in dm5]
+    shots = []
+    for e in range(nsh):
+        fine, sp, rp = born.prepareShot(e)
+        f_dev = [torch.from_numpy(a).to(dev) for a in fine]
+        d_dev = [torch.zeros((len(rp[prop._FIELD_GRID[f]]), w.nts), dtype=torch.float32, device=dev)
+                 for f in range(5)]
+        sp_a = [np.ascontiguousarray(p, np.int32) for p in sp]
+        rp_a = [np.ascontiguousarray(p, np.int32) for p in rp]
+        shots.append(dict(
+            fine=f_dev, data=d_dev, sp=sp_a, rp=rp_a,
+            fine_pp=_lib.ptr_array([t.data_ptr() for t in f_dev]),
+            data_pp=_lib.ptr_array([t.data_ptr() for t in d_dev]),
+            sp_pp=_lib.ptr_array([a.ctypes.data for a in sp_a]), sn=(ctypes.c_int * 4)(*[len(a) for a in sp_a]),
+            rp_pp=_lib.ptr_array([a.ctypes.data for a in rp_a]), rn=(ctypes.c_int * 4)(*[len(a) for a in rp_a])))
+    dm_pp = _lib.ptr_array([t.data_ptr() for t in dm5])
+    grad_pp = _lib.ptr_array([t.data_ptr() for t in grad5])
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
+    torch.cuda.synchronize()
+
+    def step():
+        for s in shots:
+            _lib.check(L.eio_born_fwd_reg_dev(ctx, s["fine_pp"], dm_pp, s["data_pp"], s["sp_pp"], s["sn"],
+                                              s["rp_pp"], s["rn"]))
+        for s in shots:
+            _lib.check(L.eio_born_adj_reg_dev(ctx, s["fine_pp"], grad_pp, s["data_pp"], s["sp_pp"], s["sn"],
+                                              s["rp_pp"], s["rn"]))
+        if ws > 1:
+            import torch.distributed as dist
+            for g in grad5:
+                dist.all_reduce(g)
+
+    for _ in range(args.warmup):
+        step()
+        flush.zero_()
+    torch.cuda.synchronize()
+
+    # ---- timed region (device-resident)
+    gpu_uuid = None
+    try:
+        gpu_uuid = str(torch.cuda.get_device_properties(dev).uuid)
+        if not gpu_uuid.startswith("GPU-"):
+            gpu_uuid = "GPU-" + gpu_uuid
+    except Exception:
+        pass
+    clocks = ClockSampler(gpu_uuid)
+    L.eio_ctx_stats(ctx, 1, 1, None, None, None)
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks.start()
+    t_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record()
+        step()
+        ev1.record()
+        torch.cuda.synchronize()
+        t_ms += ev0.elapsed_time(ev1)
+    barrier(ws)
+    clk = clocks.stop()
+    launches, step_launches, step_ms = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_double()
+    L.eio_ctx_stats(ctx, 0, 1, ctypes.byref(launches), ctypes.byref(step_launches), ctypes.byref(step_ms))
+    t_ms = max_over_ranks(ws, t_ms)
+    value = ws * updates_per_step * args.steps / (t_ms * 1e-3) / 1e9
+
+    # roofline of the dominant kernel (fused step)
+    avg_launch_ms = step_ms.value / max(step_launches.value, 1)
+    achieved = BYTES_PER_CELL * cells / (avg_launch_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": profile_traffic(),
+            "peak_source": peak_kind, "kernel": "k_step (fused 5-field update)",
+            "avg_launch_us": round(avg_launch_ms * 1e3, 3),
+            "algorithmic_bytes_per_launch": BYTES_PER_CELL * cells}
+
+    # ---- e2e through the reference-facing operator API (host buffers)
+    e2e = None
+    if not args.no_e2e:
+        model = born.modelSpace()
+        model.getNdArray()[...] = w.extra["dmodel"]
+        data = born.dataSpace()
+        gvec = born.modelSpace()
+        born.forward(False, model, data)   # warm the host path
+        torch.cuda.synchronize()
+        barrier(ws)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            born.forward(False, model, data)
+            born.adjoint(False, gvec, data)
+            if ws > 1:
+                import torch.distributed as dist
+                g = torch.from_numpy(gvec.getNdArray()).to(dev)
+                dist.all_reduce(g)
+                gvec.getNdArray()[...] = g.cpu().numpy()
+        torch.cuda.synchronize()
+        t_e2e = max_over_ranks(ws, time.perf_counter() - t0)
+        n = w.nz * w.nx
+        src_bytes = sum(4 * s["fine"][f].numel() for s in shots for f in range(5))
+        rec_bytes = sum(4 * s["data"][f].numel() for s in shots for f in range(5))
+        h2d = src_bytes * 2 + 4 * 5 * n * nsh * 2 + rec_bytes
+        d2h = rec_bytes + 4 * 5 * n * nsh
+        e2e = {"value": round(ws * updates_per_step * args.steps / t_e2e / 1e9, 3), "unit": "Gcell-updates/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "ms_per_step": round(1e3 * t_e2e / args.steps, 1)}
+
+    # ---- CPU baseline: the oracle port (OpenMP, FP32) on a bounded sample
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_baseline(w, born)
+
+    out = {
+        "metric": "Gcells/s", "value": round(value, 3), "unit": "Gcell-updates/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_ms / args.steps, 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "born_600x1800: Born forward + adjoint, %d shots per GPU, nts=%d (%d fine steps), "
+                               "600x1800 grid, 900 receivers" % (nsh, w.nts, fine_steps),
+                   "nz": w.nz, "nx": w.nx, "nts": w.nts, "shots_per_gpu": nsh, "propagations_per_step": 4 * nsh,
+                   "cell_updates_per_step": updates_per_step * ws,
+                   "l2": "inputs larger than L2 (34.6 GB FP32 source-wavefield history per shot) and a 256 MB "
+                         "L2 flush between timed steps"},
+        "shot_gradients_per_s": round(ws * nsh * args.steps / (t_ms * 1e-3), 4),
+        "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+        "gpu_launches": int(launches.value),
+    }
+    return out
+
+
+def cpu_baseline(w, born):
+    """Oracle (FP32 OpenMP port) Born forward of one shot of the same grid on a
+    bounded number of time samples."""
+    from oracle import oracle as O
+    nts_s = 150
+    c = O.Case.from_workload(w)
+    c.par["nts"] = nts_s
+    orc = O.Oracle("f")
+    g = c.grid()
+    med = orc.medium(c.ep, g["dts"], g["S"])
+    src = O._grids(orc, c, *c.src[0])
+    rec = O._grids(orc, c, *c.rec)
+    sig = w.source_signal()[:, :, :nts_s]
+    fine = O.born_sources(orc, c, g, med, src, sig)
+    dm = O.born_model_slice(orc, g, med, w.extra["dmodel"])
+    data = [np.zeros((len(rec[O.FIELD_GRID[f]]["uniq"]), nts_s), np.float32) for f in range(5)]
+    t0 = time.perf_counter()
+    orc.born_prop(0, g, med, fine, dm, data, O._reg_pos(src), O._reg_pos(rec))
+    dt = time.perf_counter() - t0
+    upd = 2.0 * (nts_s - 1) * g["S"] * (g["nz"] - 8) * (g["nx"] - 8)
+    return {"value": round(upd / dt / 1e9, 4), "unit": "Gcell-updates/s", "cores": O.num_threads(),
+            "kind": "port",
+            "sample": "oracle FP32 Born forward (source + scattered propagation), 1 shot, 600x1800 grid, "
+                      "nts=%d (%d fine steps), %.1f s" % (nts_s, (nts_s - 1) * g["S"], dt)}
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args, ws, rank, local):
+    """The reference's own CUDA drivers (oracle/_ref) on one shot of the same workload
+    per step: Born forward then Born adjoint, each a full init/alloc/propagate/free
+    like BornElasticGpu::forward/adjoint."""
+    from oracle import oracle as O
+    from elastic_isotropic_operators_b200 import synthetic
+    if not O.RefGpu.available("f"):
+        return {"impl": "reference", "unavailable": "oracle/_ref not built (reference tree absent at build time)"}
+    w = synthetic.born_600x1800(nts=args.nts, nshots=1, seed=2024)
+    orc = O.Oracle("f")
+    c = O.Case.from_workload(w)
+    g = c.grid()
+    med = orc.medium(c.ep, g["dts"], g["S"])
+    src = O._grids(orc, c, *c.src[0])
+    rec = O._grids(orc, c, *c.rec)
+    fine = O.born_sources(orc, c, g, med, src, w.source_signal())
+    dm = O.born_model_slice(orc, g, med, w.extra["dmodel"])
+    ref = O.RefGpu("f")
+    data = [np.zeros((len(rec[O.FIELD_GRID[f]]["uniq"]), g["nts"]), np.float32) for f in range(5)]
+    grad = [np.zeros_like(a) for a in dm]
+
+    def step():
+        ref.born_prop(0, g, med, fine, [a.copy() for a in dm], data, O._reg_pos(src), O._reg_pos(rec))
+        ref.born_prop(1, g, med, fine, grad, data, O._reg_pos(src), O._reg_pos(rec))
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    cells = (g["nz"] - 8) * (g["nx"] - 8)
+    upd = 4.0 * (g["nts"] - 1) * g["S"] * cells * args.steps
+    v = upd / dt / 1e9
+    return {"impl": "reference", "metric": "Gcells/s", "value": round(v, 3), "unit": "Gcell-updates/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * dt / args.steps, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "born_600x1800: Born forward + adjoint, 1 shot per step (bounded sample of the "
+                                   "10-shot workload), nts=%d" % g["nts"], "nz": g["nz"], "nx": g["nx"]},
+            "cpu_baseline": {"value": round(v, 3), "unit": "Gcell-updates/s", "cores": 1, "kind": "reference",
+                             "sample": "reference CUDA drivers (elastic_iso_float, built for sm_100a) on the B200; "
+                                       "the reference has no CPU implementation of this path"},
+            "e2e": {"value": round(v, 3), "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        # rank 0 alone times the reference; the other ranks exit without work
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0
+        print(json.dumps(run_reference(args, 1, 0, int(os.environ.get("LOCAL_RANK", "0")))))
+        return 0
+    ws, rank, local = dist_init(args)
+    out = run_ours(args, ws, rank, local)
+    if rank == 0:
+        print(json.dumps(out))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

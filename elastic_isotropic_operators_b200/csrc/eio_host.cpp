@@ -1,0 +1,891 @@
+// Host side of the engine: finite-difference parameters and QC, medium
+// preparation, staggering, spatial and temporal interpolation of the
+// acquisition, the multi-shot operators, and the extern "C" boundary.
+//
+// Restates (paths relative to the reference project, F = elastic_iso_lib/elastic_iso_float/prop):
+//   fdParamElastic            F/src/fdParamElastic.cpp:12-332
+//   staggerX / staggerZ       F/src/stagger.cpp:18-114
+//   spaceInterpGpu            F/src/spaceInterpGpu.cpp:11-362
+//   interpTimeLinTbb          F/src/interpTimeLinTbb.cpp:9-102
+//   nonlinearPropElasticGpu   F/src/nonlinearPropElasticGpu.cpp:43-473 (per-shot host prep)
+//   seismicElasticOperator2D  F/include/seismicElasticOperator2D.cpp:27-117 (Born source prep)
+//   nonlinearPropElasticShotsGpu::forward/adjoint  F/src/nonlinearPropElasticShotsGpu.cpp:80-422
+//   BornElasticShotsGpu::forward/adjoint           F/src/BornElasticShotsGpu.cpp:85-378
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "eio_internal.h"
+
+#define EIO_API extern "C" __attribute__((visibility("default")))
+
+namespace eio {
+
+static thread_local std::string g_last_error;
+
+// ------------------------------------------------------------------ fdParam
+void stagger_x(int adj, int add, int nz, int nx, float* model, float* data) {
+    const long long n = (long long)nz * nx;
+    if (!adj) {
+        if (!add) std::fill(data, data + n, 0.f);
+        for (int ix = 0; ix < nx - 1; ix++)
+            for (int iz = 0; iz < nz; iz++) {
+                const long long i = (long long)ix * nz + iz;
+                data[i] = (float)(data[i] + 0.5 * (model[i] + model[i + nz]));
+            }
+        for (int iz = 0; iz < nz; iz++) data[(long long)(nx - 1) * nz + iz] += model[(long long)(nx - 1) * nz + iz];
+    } else {
+        if (!add) std::fill(model, model + n, 0.f);
+        for (int ix = 1; ix < nx - 1; ix++)
+            for (int iz = 0; iz < nz; iz++) {
+                const long long i = (long long)ix * nz + iz;
+                model[i] = (float)(model[i] + 0.5 * (data[i] + data[i - nz]));
+            }
+        for (int iz = 0; iz < nz; iz++) {
+            model[iz] = (float)(model[iz] + 0.5 * data[iz]);
+            const long long l = (long long)(nx - 1) * nz + iz;
+            model[l] = (float)(model[l] + (data[l] + 0.5 * data[l - nz]));
+        }
+    }
+}
+
+void stagger_z(int adj, int add, int nz, int nx, float* model, float* data) {
+    const long long n = (long long)nz * nx;
+    if (!adj) {
+        if (!add) std::fill(data, data + n, 0.f);
+        for (int ix = 0; ix < nx; ix++) {
+            float* d = data + (long long)ix * nz;
+            const float* m = model + (long long)ix * nz;
+            for (int iz = 0; iz < nz - 1; iz++) d[iz] = (float)(d[iz] + 0.5 * (m[iz] + m[iz + 1]));
+            d[nz - 1] += m[nz - 1];
+        }
+    } else {
+        if (!add) std::fill(model, model + n, 0.f);
+        for (int ix = 0; ix < nx; ix++) {
+            float* m = model + (long long)ix * nz;
+            const float* d = data + (long long)ix * nz;
+            for (int iz = 1; iz < nz - 1; iz++) m[iz] = (float)(m[iz] + 0.5 * (d[iz] + d[iz - 1]));
+            m[0] = (float)(m[0] + 0.5 * d[0]);
+            m[nz - 1] = (float)(m[nz - 1] + (d[nz - 1] + 0.5 * d[nz - 2]));
+        }
+    }
+}
+
+static std::string fmt(double v) {
+    std::ostringstream s;
+    s << v;
+    return s.str();
+}
+
+void build_fdparam(const eio_fd_params& pin, const float* ep, FdParam& o) {
+    eio_fd_params p = pin;
+    if (p.nts < 2) throw Error(EIO_ERR_ARG, "nts must be >= 2");
+    if (p.nz <= 0 || p.nx <= 0) throw Error(EIO_ERR_ARG, "nz and nx must be positive");
+    if (p.surfaceCondition != 0)
+        throw Error(EIO_ERR_UNSUPPORTED, "surfaceCondition=1 (free surface) is not available in this build");
+    o.S = 2 * p.sub;
+    if (o.S > SUB_MAX || o.S >= SUB_MAX)
+        throw Error(EIO_ERR_QC, "**** ERROR: 2*_sub is greater than the allowed SUB_MAX value. " +
+                                    std::to_string(o.S) + " > " + std::to_string(SUB_MAX) + " ****");
+    if (p.sub < 1) throw Error(EIO_ERR_ARG, "sub must be >= 1");
+    o.ntw = (p.nts - 1) * o.S + 1;
+    o.dtw = p.dts / float(o.S);
+    if (p.mod_par == 2) { p.dz *= 1000.f; p.dx *= 1000.f; p.oz *= 1000.f; p.ox *= 1000.f; }
+    const int zPad = std::min(p.zPadMinus, p.zPadPlus);
+    const int xPad = std::min(p.xPadMinus, p.xPadPlus);
+    o.minPad = std::min(zPad, xPad);
+    if (o.minPad >= PAD_MAX) throw Error(EIO_ERR_QC, "**** ERROR: Padding value is too high ****");
+    if (o.minPad < 0) throw Error(EIO_ERR_ARG, "negative padding");
+    if (p.blockSize != 16)
+        throw Error(EIO_ERR_QC, "**** ERROR: Block size for time stepper is not consistent with parfile ****");
+    if (p.fat != 4) throw Error(EIO_ERR_UNSUPPORTED, "fat must be 4 (8th-order stencil)");
+    o.p = p;
+    const int nz = p.nz, nx = p.nx, fat = p.fat;
+    const long long n = (long long)nz * nx;
+    // velocity range, fdParamElastic.cpp:80-97 (note the reference's 2*fat upper bound)
+    float vmin = 10000.f, vmax = -1.f;
+    for (int ix = fat; ix < nx - 2 * fat; ix++)
+        for (int iz = fat; iz < nz - 2 * fat; iz++) {
+            const long long i = (long long)ix * nz + iz;
+            const float rho = ep[i], lam = ep[n + i], mu = ep[2 * n + i];
+            const float vp = std::sqrt((lam + 2 * mu) / rho), vs = std::sqrt(mu / rho);
+            if (vp < vmin) vmin = vp;
+            if (vp > vmax) vmax = vp;
+            if (vs < vmin && vs != 0) vmin = vs;
+            if (vs > vmax) vmax = vs;
+        }
+    o.minVpVs = vmin;
+    o.maxVpVs = vmax;
+    // checkFdStability / checkFdDispersion / checkModelSize, fdParamElastic.cpp:256-297
+    const float courant = vmax * o.dtw * 2.0f / std::min(p.dz, p.dx);
+    if (courant > 0.45f)
+        throw Error(EIO_ERR_QC, "**** ERROR: Courant is too big: " + fmt(courant) + " ****\nMax velocity value: " +
+                                    fmt(vmax) + " [m/s]\nDtw: " + fmt(o.dtw) + " [s]\nMin (dz, dx): " +
+                                    fmt(std::min(p.dz, p.dx)) + " [m]");
+    const float disp = vmin / (p.fMax * std::max(p.dz, p.dx));
+    if (disp < 3.0f)
+        throw Error(EIO_ERR_QC, "**** ERROR: Dispersion is too small: " + fmt(disp) + " > 3 ****\nMin velocity value = " +
+                                    fmt(vmin) + " [m/s]\nMax (dz, dx) = " + fmt(std::max(p.dz, p.dx)) +
+                                    " [m]\nMax frequency = " + fmt(p.fMax) + " [Hz]");
+    if ((nz - 2 * fat) % p.blockSize != 0)
+        throw Error(EIO_ERR_QC, "**** ERROR: nz-2*_fat not a multiple of block size ****");
+    if ((nx - 2 * fat) % p.blockSize != 0)
+        throw Error(EIO_ERR_QC, "**** ERROR: nx-2*_fat not a multiple of block size ****");
+
+    // scaled staggered medium, fdParamElastic.cpp:116-148
+    for (int f = 0; f < 5; f++) o.par[f].assign(n, 0.f);
+    std::vector<float> rho(ep, ep + n), mu(ep + 2 * n, ep + 3 * n), tmp(n);
+    stagger_x(1, 0, nz, nx, o.par[0].data(), rho.data());
+    stagger_z(1, 0, nz, nx, o.par[1].data(), rho.data());
+    stagger_x(1, 0, nz, nx, tmp.data(), mu.data());
+    stagger_z(1, 0, nz, nx, o.par[4].data(), tmp.data());
+    const float dtw = o.dtw;
+    for (long long i = 0; i < n; i++) {
+        const float lam = ep[n + i], m = ep[2 * n + i];
+        o.par[0][i] = (float)(2.0 * dtw / o.par[0][i]);
+        o.par[1][i] = (float)(2.0 * dtw / o.par[1][i]);
+        o.par[2][i] = (float)(2.0 * dtw * (lam + 2 * m));
+        o.par[3][i] = (float)(2.0 * dtw * lam);
+        o.par[4][i] = (float)(2.0 * dtw * o.par[4][i]);
+    }
+    // FD coefficients, time filter and taper, nonlinearPropElasticGpuFunctions.cu:155-202
+    static const double C[4] = {1.196289062541883, -0.079752604188901, 0.009570312506634, -6.975446437140719e-04};
+    for (int k = 0; k < 4; k++) { o.zc[k] = (float)(C[k] / p.dz); o.xc[k] = (float)(C[k] / p.dx); }
+    const int h = o.S + 1;
+    o.filt.assign(2 * h, 0.f);
+    const float sc = std::sqrt(float(o.ntw) / float(p.nts));
+    for (int i = 0; i < h; i++) {
+        const float a = (float)(1.0 - 1.0 * i / o.S);
+        const float b = (float)(1.0 - a);
+        o.filt[i] = (float)(a * (1.0 / sc));
+        o.filt[i + h] = (float)(b * (1.0 / sc));
+    }
+    o.damp.assign(std::max(o.minPad, 1), 1.f);
+    for (int i = 0; i < o.minPad; i++) {
+        float arg = (float)(M_PI / (1.0 * o.minPad) * 1.0 * (o.minPad - i));
+        arg = (float)(p.alphaCos + (1.0 - p.alphaCos) * std::cos(arg));
+        o.damp[i] = arg;
+    }
+    o.dts_inv = (float)(1.0 / (2.0 * p.dts));
+}
+
+// ------------------------------------------------------------------ time interp
+void time_interp(int adj, int add, int nts, float dts, float ots, int S, int nDev, float* coarse, float* fine) {
+    const int ntw = (nts - 1) * S + 1;
+    const float dtw = dts / S, otw = ots;
+    float scale = float(ntw) / float(nts);
+    scale = (float)(1.0 / std::sqrt(scale));
+    if (!adj) {
+        if (!add) std::fill(fine, fine + (long long)nDev * ntw, 0.f);
+        for (int d = 0; d < nDev; d++) {
+            const float* m = coarse + (long long)d * nts;
+            float* f = fine + (long long)d * ntw;
+            for (int itw = 0; itw < ntw - 1; itw++) {
+                const float tw = otw + itw * dtw;
+                float w = (tw - ots) / dts;
+                const int i0 = (int)w;
+                w = w - i0;
+                f[itw] = (float)(f[itw] + (m[i0] * (1.0 - w) + m[i0 + 1] * w) * scale);
+            }
+            f[ntw - 1] += scale * m[nts - 1];
+        }
+    } else {
+        if (!add) std::fill(coarse, coarse + (long long)nDev * nts, 0.f);
+        for (int d = 0; d < nDev; d++) {
+            float* m = coarse + (long long)d * nts;
+            const float* f = fine + (long long)d * ntw;
+            for (int itw = 0; itw < ntw - 1; itw++) {
+                const float tw = otw + itw * dtw;
+                float w = (tw - ots) / dts;
+                const int i0 = (int)w;
+                w = w - i0;
+                m[i0] = (float)(m[i0] + scale * f[itw] * (1.0 - w));
+                m[i0 + 1] += scale * f[itw] * w;
+            }
+            m[nts - 1] += scale * f[ntw - 1];
+        }
+    }
+}
+
+// ------------------------------------------------------------------ spatial interp
+static double sinc_pi(double x) {
+    // published Boost.Math sinc_pi algorithm: Taylor expansion near zero
+    const double eps = 2.220446049250313e-16, t2 = std::sqrt(eps), tn = std::sqrt(t2);
+    const double ax = std::fabs(x);
+    if (ax >= tn) return std::sin(x) / x;
+    double r = 1.0;
+    if (ax >= eps) {
+        const double x2 = x * x;
+        r -= x2 / 6.0;
+        if (ax >= t2) r += (x2 * x2) / 120.0;
+    }
+    return r;
+}
+static double normal_pdf(double mean, double sd, double x) {
+    const double z = (x - mean) / sd;
+    return std::exp(-0.5 * z * z) / (sd * std::sqrt(2.0 * M_PI));
+}
+
+void build_sinterp(const float* zc, const float* xc, int nDev, int nz, float oz, float dz, int nx, float ox,
+                   float dx, int nt, const std::string& method, int nFilt, int dipole, float zDip, float xDip,
+                   SInterp& s) {
+    int m;
+    if (method == "linear") { m = 0; nFilt = 1; }
+    else if (method == "sinc") m = 1;
+    else if (method == "gauss") m = 2;
+    else throw Error(EIO_ERR_ARG, "**** ERROR: Space interp method not defined ****");
+    if (nFilt < 1) throw Error(EIO_ERR_ARG, "nFilt must be >= 1");
+    if (m != 0 && dipole == 1)
+        throw Error(EIO_ERR_ARG, m == 1 ? "**** ERROR: Spatial sinc interpolation and dipole acquisition not implemented ****"
+                                         : "**** ERROR: Gaussian spatial interpolation and dipole acquisition not implemented ****");
+    if (nDev < 0 || nt < 1) throw Error(EIO_ERR_ARG, "invalid device count or nt");
+    const int n2 = 2 * nFilt;
+    const int nft = (m == 0) ? (dipole == 1 ? 8 : 4) : n2 * n2;
+    // checkOutOfBounds, spaceInterpGpu.cpp:364-388
+    const float zMax = oz + (nz - 1) * dz, xMax = ox + (nx - 1) * dx;
+    const float zBuf = dz * nFilt, xBuf = dx * nFilt;
+    for (int i = 0; i < nDev; i++) {
+        if (zc[i] >= zMax - zBuf || zc[i] <= oz + zBuf)
+            throw Error(EIO_ERR_BOUNDS, "**** ERROR: One of the device is out of bounds in the z direction ****");
+        if (xc[i] >= xMax - xBuf || xc[i] <= ox + xBuf)
+            throw Error(EIO_ERR_BOUNDS, "**** ERROR: One of the device is out of bounds in the x direction ****");
+    }
+    s.nIrreg = nDev; s.nft = nft; s.nt = nt; s.nz = nz; s.nx = nx;
+    s.gpi.assign((size_t)nDev * nft, 0);
+    s.w.assign((size_t)nDev * nft, 0.f);
+    const float zDS = zDip * dz, xDS = xDip * dx;
+    for (int d = 0; d < nDev; d++) {
+        int* g = s.gpi.data() + (size_t)d * nft;
+        float* w = s.w.data() + (size_t)d * nft;
+        if (m == 0) {
+            float wz = (zc[d] - oz) / dz, wx = (xc[d] - ox) / dx;
+            const int zr = (int)wz; wz = wz - zr; wz = (float)(1.0 - wz);
+            const int xr = (int)wx; wx = wx - xr; wx = (float)(1.0 - wx);
+            g[0] = xr * nz + zr;      w[0] = wz * wx;
+            g[1] = g[0] + 1;          w[1] = (float)((1.0 - wz) * wx);
+            g[2] = g[0] + nz;         w[2] = (float)(wz * (1.0 - wx));
+            g[3] = g[0] + nz + 1;     w[3] = (float)((1.0 - wz) * (1.0 - wx));
+            if (dipole == 1) {
+                float a = (zc[d] + zDS - oz) / dz, b = (xc[d] + xDS - ox) / dx;
+                const int za = (int)a; a = a - za; a = (float)(1.0 - a);
+                const int xb = (int)b; b = b - xb; b = (float)(1.0 - b);
+                g[4] = xb * nz + za;      w[4] = (float)((-1.0) * a * b);
+                g[5] = g[4] + 1;          w[5] = (float)((-1.0) * (1.0 - a) * b);
+                g[6] = g[4] + nz;         w[6] = (float)((-1.0) * a * (1.0 - b));
+                g[7] = g[4] + nz + 1;     w[7] = (float)((-1.0) * (1.0 - a) * (1.0 - b));
+            }
+        } else {
+            const float zi = zc[d], xi = xc[d];
+            const int zr = (int)((zi - oz) / dz), xr = (int)((xi - ox) / dx);
+            float sum = 0.f;
+            for (int ix = 0; ix < n2; ix++)
+                for (int iz = 0; iz < n2; iz++) {
+                    const float xcur = (xr + ix - nFilt + 1) * dx + ox;
+                    const float zcur = (zr + iz - nFilt + 1) * dz + oz;
+                    const float xin = (xi - xcur) / dx, zin = (zi - zcur) / dz;
+                    const float v = (m == 1) ? (float)(sinc_pi(M_PI * zin) * sinc_pi(M_PI * xin))
+                                             : (float)(normal_pdf(xi, 2 * dx, xcur) * normal_pdf(zi, 2 * dz, zcur));
+                    w[n2 * ix + iz] = v;
+                    g[n2 * ix + iz] = nz * (xr + ix - nFilt + 1) + (zr + iz - nFilt + 1);
+                    sum += v;
+                }
+            for (int i = 0; i < nft; i++) w[i] = w[i] / sum;
+        }
+    }
+    // convertIrregToReg: unique grid points in first-seen order, spaceInterpGpu.cpp:288-311
+    std::unordered_map<int, int> idx;
+    s.slot.assign(s.gpi.size(), 0);
+    s.uniq.clear();
+    for (size_t i = 0; i < s.gpi.size(); i++) {
+        auto it = idx.find(s.gpi[i]);
+        if (it == idx.end()) {
+            idx.emplace(s.gpi[i], (int)s.uniq.size());
+            s.slot[i] = (int)s.uniq.size();
+            s.uniq.push_back(s.gpi[i]);
+        } else {
+            s.slot[i] = it->second;
+        }
+    }
+    s.nReg = (int)s.uniq.size();
+}
+
+void sinterp_forward(const SInterp& s, bool add, const float* reg, float* irreg) {
+    const int nt = s.nt;
+    if (!add) std::fill(irreg, irreg + (size_t)s.nIrreg * nt, 0.f);
+    for (int d = 0; d < s.nIrreg; d++)
+        for (int f = 0; f < s.nft; f++) {
+            const size_t i1 = (size_t)d * s.nft + f;
+            const float w = s.w[i1];
+            const float* m = reg + (size_t)s.slot[i1] * nt;
+            float* o = irreg + (size_t)d * nt;
+            for (int t = 0; t < nt; t++) o[t] += w * m[t];
+        }
+}
+
+void sinterp_adjoint(const SInterp& s, bool add, float* reg, const float* irreg) {
+    const int nt = s.nt;
+    if (!add) std::fill(reg, reg + (size_t)s.nReg * nt, 0.f);
+    for (int d = 0; d < s.nIrreg; d++)
+        for (int f = 0; f < s.nft; f++) {
+            const size_t i1 = (size_t)d * s.nft + f;
+            const float w = s.w[i1];
+            float* m = reg + (size_t)s.slot[i1] * nt;
+            const float* o = irreg + (size_t)d * nt;
+            for (int t = 0; t < nt; t++) m[t] += w * o[t];
+        }
+}
+
+}  // namespace eio
+
+// ====================================================================== C ABI
+using namespace eio;
+
+struct eio_sinterp {
+    SInterp s;
+};
+
+struct eio_ctx {
+    FdParam fd;
+    Engine* eng = nullptr;
+    int device = 0;
+};
+
+template <class F>
+static int guarded(F&& f) {
+    try {
+        f();
+        return EIO_OK;
+    } catch (const Error& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return EIO_ERR_NOMEM;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return EIO_ERR_ARG;
+    }
+}
+
+static const int kFG[5] = {1, 2, 0, 0, 3};   // field -> grid (x, z, center, center, xz)
+
+EIO_API void eio_fd_params_default(eio_fd_params* p) {
+    std::memset(p, 0, sizeof(*p));
+    p->fMax = 1000.f;
+    p->blockSize = 16;
+    p->fat = 4;
+    p->alphaCos = 0.99f;
+    p->surfaceCondition = 0;
+    p->mod_par = 1;
+    p->errorTolerance = 1e-6f;
+}
+
+EIO_API const char* eio_last_error(void) { return g_last_error.c_str(); }
+EIO_API int eio_version(void) { return 1; }
+
+EIO_API int eio_sinterp_create(const float* zCoord, const float* xCoord, int nDevice, int nz, float oz, float dz,
+                               int nx, float ox, float dx, int nt, const char* method, int nFilt, int dipole,
+                               float zDipoleShift, float xDipoleShift, eio_sinterp** out) {
+    return guarded([&] {
+        if (!out || !method || (nDevice > 0 && (!zCoord || !xCoord))) throw Error(EIO_ERR_ARG, "null argument");
+        auto s = std::make_unique<eio_sinterp>();
+        build_sinterp(zCoord, xCoord, nDevice, nz, oz, dz, nx, ox, dx, nt, method, nFilt, dipole, zDipoleShift,
+                      xDipoleShift, s->s);
+        *out = s.release();
+    });
+}
+EIO_API void eio_sinterp_destroy(eio_sinterp* s) { delete s; }
+EIO_API int eio_sinterp_sizes(const eio_sinterp* s, int* nIrreg, int* nReg, int* nFiltTotal) {
+    return guarded([&] {
+        if (!s) throw Error(EIO_ERR_ARG, "null interpolator");
+        if (nIrreg) *nIrreg = s->s.nIrreg;
+        if (nReg) *nReg = s->s.nReg;
+        if (nFiltTotal) *nFiltTotal = s->s.nft;
+    });
+}
+EIO_API int eio_sinterp_positions(const eio_sinterp* s, int* regPos) {
+    return guarded([&] {
+        if (!s || !regPos) throw Error(EIO_ERR_ARG, "null argument");
+        std::copy(s->s.uniq.begin(), s->s.uniq.end(), regPos);
+    });
+}
+EIO_API int eio_sinterp_weights(const eio_sinterp* s, int* gpi, float* w) {
+    return guarded([&] {
+        if (!s) throw Error(EIO_ERR_ARG, "null interpolator");
+        if (gpi) std::copy(s->s.gpi.begin(), s->s.gpi.end(), gpi);
+        if (w) std::copy(s->s.w.begin(), s->s.w.end(), w);
+    });
+}
+EIO_API int eio_sinterp_forward(const eio_sinterp* s, int add, const float* reg, float* irreg) {
+    return guarded([&] {
+        if (!s || !reg || !irreg) throw Error(EIO_ERR_ARG, "null argument");
+        sinterp_forward(s->s, add != 0, reg, irreg);
+    });
+}
+EIO_API int eio_sinterp_adjoint(const eio_sinterp* s, int add, float* reg, const float* irreg) {
+    return guarded([&] {
+        if (!s || !reg || !irreg) throw Error(EIO_ERR_ARG, "null argument");
+        sinterp_adjoint(s->s, add != 0, reg, irreg);
+    });
+}
+
+EIO_API int eio_medium_prepare(const eio_fd_params* p, const float* ep, float* rx, float* rz, float* l2m, float* lam,
+                               float* mu) {
+    return guarded([&] {
+        if (!p || !ep) throw Error(EIO_ERR_ARG, "null argument");
+        FdParam fd;
+        build_fdparam(*p, ep, fd);
+        float* o[5] = {rx, rz, l2m, lam, mu};
+        for (int f = 0; f < 5; f++)
+            if (o[f]) std::copy(fd.par[f].begin(), fd.par[f].end(), o[f]);
+    });
+}
+
+EIO_API int eio_stagger(int axis, int adj, int add, int nz, int nx, float* model, float* data) {
+    return guarded([&] {
+        if (!model || !data || nz < 2 || nx < 2) throw Error(EIO_ERR_ARG, "invalid stagger arguments");
+        if (axis == 0) stagger_x(adj, add, nz, nx, model, data);
+        else stagger_z(adj, add, nz, nx, model, data);
+    });
+}
+
+EIO_API int eio_time_interp(int adj, int add, int nts, float dts, float ots, int S, int nDev, float* coarse,
+                            float* fine) {
+    return guarded([&] {
+        if (!coarse || !fine || nts < 2 || S < 1) throw Error(EIO_ERR_ARG, "invalid time-interp arguments");
+        time_interp(adj, add, nts, dts, ots, S, nDev, coarse, fine);
+    });
+}
+
+EIO_API int eio_ctx_create(const eio_fd_params* p, const float* ep, int device, eio_ctx** out) {
+    return guarded([&] {
+        if (!p || !ep || !out) throw Error(EIO_ERR_ARG, "null argument");
+        auto c = std::make_unique<eio_ctx>();
+        build_fdparam(*p, ep, c->fd);
+        c->device = device;
+        c->eng = engine_create(device, c->fd);
+        *out = c.release();
+    });
+}
+EIO_API int eio_ctx_set_background(eio_ctx* c, const float* ep) {
+    return guarded([&] {
+        if (!c || !ep) throw Error(EIO_ERR_ARG, "null argument");
+        FdParam fd;
+        build_fdparam(c->fd.p, ep, fd);   // QC may throw; the context keeps its old medium then
+        engine_set_medium(c->eng, fd);
+        c->fd = std::move(fd);
+    });
+}
+EIO_API void eio_ctx_destroy(eio_ctx* c) {
+    if (!c) return;
+    engine_destroy(c->eng);
+    delete c;
+}
+EIO_API int eio_ctx_set_checkpoint_precision(eio_ctx* c, int mode) {
+    return guarded([&] {
+        if (!c) throw Error(EIO_ERR_ARG, "null context");
+        engine_set_checkpoint(c->eng, mode);
+    });
+}
+EIO_API int eio_ctx_get_medium(const eio_ctx* c, float* rx, float* rz, float* l2m, float* lam, float* mu) {
+    return guarded([&] {
+        if (!c) throw Error(EIO_ERR_ARG, "null context");
+        float* o[5] = {rx, rz, l2m, lam, mu};
+        for (int f = 0; f < 5; f++)
+            if (o[f]) std::copy(c->fd.par[f].begin(), c->fd.par[f].end(), o[f]);
+    });
+}
+EIO_API int eio_ctx_counts(const eio_ctx* c, long long* fineSteps, long long* cells) {
+    return guarded([&] {
+        if (!c) throw Error(EIO_ERR_ARG, "null context");
+        if (fineSteps) *fineSteps = (long long)(c->fd.p.nts - 1) * c->fd.S;
+        if (cells) *cells = (long long)(c->fd.p.nz - 8) * (c->fd.p.nx - 8);
+    });
+}
+EIO_API void* eio_ctx_stream(eio_ctx* c) { return c ? engine_stream(c->eng) : nullptr; }
+EIO_API int eio_ctx_stats(eio_ctx* c, int enable, int reset, long long* launches, long long* stepLaunches,
+                          double* stepMs) {
+    return guarded([&] {
+        if (!c) throw Error(EIO_ERR_ARG, "null context");
+        engine_stats(c->eng, enable, reset, launches, stepLaunches, stepMs);
+    });
+}
+
+static ShotGeom make_geom(const int* const srcPos[4], const int nSrc[4], const int* const recPos[4],
+                          const int nRec[4]) {
+    ShotGeom g;
+    for (int k = 0; k < 4; k++) {
+        g.srcPos[k] = srcPos[k]; g.nSrc[k] = nSrc[k];
+        g.recPos[k] = recPos[k]; g.nRec[k] = nRec[k];
+        if (nSrc[k] < 0 || nRec[k] < 0) throw Error(EIO_ERR_ARG, "negative point count");
+    }
+    return g;
+}
+
+EIO_API int eio_nl_fwd_reg(eio_ctx* c, float* const model[5], float* const data[5], const int* const srcPos[4],
+                           const int nSrc[4], const int* const recPos[4], const int nRec[4]) {
+    return guarded([&] { engine_nl_host(c->eng, 0, model, data, make_geom(srcPos, nSrc, recPos, nRec)); });
+}
+EIO_API int eio_nl_adj_reg(eio_ctx* c, float* const model[5], float* const data[5], const int* const srcPos[4],
+                           const int nSrc[4], const int* const recPos[4], const int nRec[4]) {
+    return guarded([&] { engine_nl_host(c->eng, 1, model, data, make_geom(srcPos, nSrc, recPos, nRec)); });
+}
+EIO_API int eio_born_fwd_reg(eio_ctx* c, float* const srcDtw[5], float* const dm[5], float* const data[5],
+                             const int* const srcPos[4], const int nSrc[4], const int* const recPos[4],
+                             const int nRec[4]) {
+    return guarded([&] { engine_born_host(c->eng, 0, srcDtw, dm, data, make_geom(srcPos, nSrc, recPos, nRec)); });
+}
+EIO_API int eio_born_adj_reg(eio_ctx* c, float* const srcDtw[5], float* const dm[5], float* const data[5],
+                             const int* const srcPos[4], const int nSrc[4], const int* const recPos[4],
+                             const int nRec[4]) {
+    return guarded([&] { engine_born_host(c->eng, 1, srcDtw, dm, data, make_geom(srcPos, nSrc, recPos, nRec)); });
+}
+EIO_API int eio_nl_fwd_reg_dev(eio_ctx* c, float* const model[5], float* const data[5], const int* const srcPos[4],
+                               const int nSrc[4], const int* const recPos[4], const int nRec[4]) {
+    return guarded([&] { engine_nl(c->eng, 0, model, data, make_geom(srcPos, nSrc, recPos, nRec)); });
+}
+EIO_API int eio_nl_adj_reg_dev(eio_ctx* c, float* const model[5], float* const data[5], const int* const srcPos[4],
+                               const int nSrc[4], const int* const recPos[4], const int nRec[4]) {
+    return guarded([&] { engine_nl(c->eng, 1, model, data, make_geom(srcPos, nSrc, recPos, nRec)); });
+}
+EIO_API int eio_born_fwd_reg_dev(eio_ctx* c, float* const srcDtw[5], float* const dm[5], float* const data[5],
+                                 const int* const srcPos[4], const int nSrc[4], const int* const recPos[4],
+                                 const int nRec[4]) {
+    return guarded([&] { engine_born(c->eng, 0, srcDtw, dm, data, make_geom(srcPos, nSrc, recPos, nRec)); });
+}
+EIO_API int eio_born_adj_reg_dev(eio_ctx* c, float* const srcDtw[5], float* const dm[5], float* const data[5],
+                                 const int* const srcPos[4], const int nSrc[4], const int* const recPos[4],
+                                 const int nRec[4]) {
+    return guarded([&] { engine_born(c->eng, 1, srcDtw, dm, data, make_geom(srcPos, nSrc, recPos, nRec)); });
+}
+
+// ------------------------------------------------------------ multi-shot operators
+namespace {
+
+struct ShotGrids {
+    const SInterp* s[4];
+    const SInterp* r[4];
+};
+
+ShotGrids shot_grids(eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom, int iExp) {
+    ShotGrids g;
+    const int ir = (nRecGeom == 1) ? 0 : iExp;
+    for (int k = 0; k < 4; k++) {
+        if (!src[4 * iExp + k] || !rec[4 * ir + k]) throw Error(EIO_ERR_ARG, "null interpolator in geometry list");
+        g.s[k] = &src[4 * iExp + k]->s;
+        g.r[k] = &rec[4 * ir + k]->s;
+    }
+    return g;
+}
+
+// per-shot source signals on the regular grid, scaled like
+// nonlinearPropElasticGpu.cpp:119-144 (scale by 2*dtw or the staggered
+// buoyancy at the injection point, then by 1/(dx*dz))
+void scale_sources(const FdParam& fd, const ShotGrids& g, std::vector<float>* reg, int nt) {
+    const float tdtw = 2.0f * fd.dtw;   // exact: power-of-two scaling of a float
+    const float area = (float)(1.0 / (fd.p.dx * fd.p.dz));
+    for (int f = 0; f < 5; f++) {
+        const SInterp& s = *g.s[kFG[f]];
+        for (int k = 0; k < s.nReg; k++) {
+            float* v = reg[f].data() + (size_t)k * nt;
+            const float sc = (f == 0) ? fd.par[0][s.uniq[k]] : (f == 1) ? fd.par[1][s.uniq[k]] : tdtw;
+            for (int t = 0; t < nt; t++) v[t] = v[t] * sc;
+        }
+    }
+    for (int f = 0; f < 5; f++)
+        for (auto& v : reg[f]) v = v * area;
+}
+
+// adjoint order, nonlinearPropElasticGpu.cpp:425-452: area first, then 2*dtw / buoyancy
+void scale_sources_adj(const FdParam& fd, const ShotGrids& g, std::vector<float>* reg, int nt) {
+    const float tdtw = 2.0f * fd.dtw;
+    const float area = (float)(1.0 / (fd.p.dx * fd.p.dz));
+    for (int f = 0; f < 5; f++)
+        for (auto& v : reg[f]) v = v * area;
+    for (int f = 0; f < 5; f++) {
+        const SInterp& s = *g.s[kFG[f]];
+        for (int k = 0; k < s.nReg; k++) {
+            float* v = reg[f].data() + (size_t)k * nt;
+            const float sc = (f == 0) ? fd.par[0][s.uniq[k]] : (f == 1) ? fd.par[1][s.uniq[k]] : tdtw;
+            for (int t = 0; t < nt; t++) v[t] = v[t] * sc;
+        }
+    }
+}
+
+ShotGeom reg_geom(const ShotGrids& g) {
+    ShotGeom sg;
+    for (int k = 0; k < 4; k++) {
+        sg.srcPos[k] = g.s[k]->uniq.data(); sg.nSrc[k] = g.s[k]->nReg;
+        sg.recPos[k] = g.r[k]->uniq.data(); sg.nRec[k] = g.r[k]->nReg;
+    }
+    return sg;
+}
+
+void check_nt(const ShotGrids& g, int nts) {
+    for (int k = 0; k < 4; k++)
+        if (g.s[k]->nt != nts || g.r[k]->nt != nts)
+            throw Error(EIO_ERR_ARG, "**** ERROR: nts not consistent with parfile ****");
+    for (int k = 1; k < 4; k++)
+        if (g.s[k]->nIrreg != g.s[0]->nIrreg || g.r[k]->nIrreg != g.r[0]->nIrreg)
+            throw Error(EIO_ERR_ARG, "the four staggered grids of a shot must hold the same devices");
+}
+
+// nonlinearPropElasticGpu::forward with add = false: irregular source -> data slice
+void nl_shot_forward(eio_ctx* c, const ShotGrids& g, const float* model, float* data) {
+    const int nts = c->fd.p.nts;
+    const int nsi = g.s[0]->nIrreg, nri = g.r[0]->nIrreg;
+    std::vector<float> reg[5], dreg[5];
+    float* mp[5]; float* dp[5];
+    for (int f = 0; f < 5; f++) {
+        const SInterp& s = *g.s[kFG[f]];
+        reg[f].assign((size_t)s.nReg * nts, 0.f);
+        sinterp_adjoint(s, false, reg[f].data(), model + (size_t)f * nsi * nts);
+    }
+    scale_sources(c->fd, g, reg, nts);
+    for (int f = 0; f < 5; f++) {
+        dreg[f].assign((size_t)g.r[kFG[f]]->nReg * nts, 0.f);
+        mp[f] = reg[f].data(); dp[f] = dreg[f].data();
+    }
+    engine_nl_host(c->eng, 0, mp, dp, reg_geom(g));
+    std::fill(data, data + (size_t)5 * nri * nts, 0.f);
+    for (int f = 0; f < 5; f++) sinterp_forward(*g.r[kFG[f]], true, dreg[f].data(), data + (size_t)f * nri * nts);
+}
+
+// nonlinearPropElasticGpu::adjoint with add = true into model
+void nl_shot_adjoint(eio_ctx* c, const ShotGrids& g, float* model, const float* data) {
+    const int nts = c->fd.p.nts;
+    const int nsi = g.s[0]->nIrreg, nri = g.r[0]->nIrreg;
+    std::vector<float> reg[5], dreg[5];
+    float* mp[5]; float* dp[5];
+    for (int f = 0; f < 5; f++) {
+        const SInterp& r = *g.r[kFG[f]];
+        dreg[f].assign((size_t)r.nReg * nts, 0.f);
+        sinterp_adjoint(r, false, dreg[f].data(), data + (size_t)f * nri * nts);
+        reg[f].assign((size_t)g.s[kFG[f]]->nReg * nts, 0.f);
+        mp[f] = reg[f].data(); dp[f] = dreg[f].data();
+    }
+    engine_nl_host(c->eng, 1, mp, dp, reg_geom(g));
+    scale_sources_adj(c->fd, g, reg, nts);
+    for (int f = 0; f < 5; f++) sinterp_forward(*g.s[kFG[f]], true, reg[f].data(), model + (size_t)f * nsi * nts);
+}
+
+// Born setSources: irregular signal -> scaled regular fine-time source (seismicElasticOperator2D.cpp:27-117)
+void born_sources(eio_ctx* c, const ShotGrids& g, const float* sig, std::vector<float>* fine) {
+    const int nts = c->fd.p.nts, ntw = c->fd.ntw;
+    const int nsi = g.s[0]->nIrreg;
+    std::vector<float> reg[5];
+    for (int f = 0; f < 5; f++) {
+        const SInterp& s = *g.s[kFG[f]];
+        reg[f].assign((size_t)s.nReg * nts, 0.f);
+        sinterp_adjoint(s, false, reg[f].data(), sig + (size_t)f * nsi * nts);
+    }
+    scale_sources(c->fd, g, reg, nts);
+    for (int f = 0; f < 5; f++) {
+        const int nr = g.s[kFG[f]]->nReg;
+        fine[f].assign((size_t)nr * ntw, 0.f);
+        time_interp(0, 0, nts, c->fd.p.dts, c->fd.p.ots, c->fd.S, nr, reg[f].data(), fine[f].data());
+    }
+}
+
+// (drho, dlambda, dmu) -> 5 staggered, scaled components (BornElasticShotsGpu.cpp:107-150)
+void born_model_slice(const FdParam& fd, const float* model, std::vector<float>* sl) {
+    const int nz = fd.p.nz, nx = fd.p.nx;
+    const size_t n = (size_t)nz * nx;
+    std::vector<float> tmp(model, model + n), tmp1(n);
+    for (int f = 0; f < 5; f++) sl[f].assign(n, 0.f);
+    stagger_x(1, 0, nz, nx, sl[0].data(), tmp.data());
+    stagger_z(1, 0, nz, nx, sl[1].data(), tmp.data());
+    std::copy(model + n, model + 2 * n, sl[2].begin());
+    std::copy(model + 2 * n, model + 3 * n, sl[3].begin());
+    std::copy(model + 2 * n, model + 3 * n, tmp.begin());
+    stagger_x(1, 0, nz, nx, tmp1.data(), tmp.data());
+    stagger_z(1, 0, nz, nx, sl[4].data(), tmp1.data());
+    const double tdtw = 2.0 * fd.dtw;
+    for (size_t i = 0; i < n; i++) {
+        sl[0][i] *= fd.par[0][i];
+        sl[1][i] *= fd.par[1][i];
+        sl[2][i] = (float)(sl[2][i] * tdtw);
+        sl[3][i] = (float)(sl[3][i] * tdtw);
+        sl[4][i] = (float)(sl[4][i] * tdtw);
+    }
+}
+
+}  // namespace
+
+EIO_API int eio_born_prepare_sources(eio_ctx* c, const float* signal, eio_sinterp* const src[4], float* const out[5]) {
+    return guarded([&] {
+        if (!c || !signal || !src || !out) throw Error(EIO_ERR_ARG, "null argument");
+        ShotGrids g;
+        for (int k = 0; k < 4; k++) {
+            if (!src[k]) throw Error(EIO_ERR_ARG, "null interpolator");
+            g.s[k] = &src[k]->s;
+            g.r[k] = &src[k]->s;
+        }
+        check_nt(g, c->fd.p.nts);
+        std::vector<float> fine[5];
+        born_sources(c, g, signal, fine);
+        for (int f = 0; f < 5; f++) std::copy(fine[f].begin(), fine[f].end(), out[f]);
+    });
+}
+
+EIO_API int eio_born_prepare_model(eio_ctx* c, const float* model, float* const out[5]) {
+    return guarded([&] {
+        if (!c || !model || !out) throw Error(EIO_ERR_ARG, "null argument");
+        std::vector<float> sl[5];
+        born_model_slice(c->fd, model, sl);
+        for (int f = 0; f < 5; f++) std::copy(sl[f].begin(), sl[f].end(), out[f]);
+    });
+}
+
+EIO_API int eio_nl_forward(eio_ctx* c, int add, int nExp, int nModelExp, const float* model, float* data,
+                           eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom) {
+    return guarded([&] {
+        if (!c || !model || !data || !src || !rec || nExp < 1) throw Error(EIO_ERR_ARG, "null argument");
+        if (nModelExp != 1 && nModelExp != nExp) throw Error(EIO_ERR_ARG, "model shot axis must be 1 or nExp");
+        if (nRecGeom != 1 && nRecGeom != nExp) throw Error(EIO_ERR_ARG, "receiver geometry count must be 1 or nExp");
+        const int nts = c->fd.p.nts;
+        ShotGrids g0 = shot_grids(src, rec, nRecGeom, 0);
+        const size_t dslice = (size_t)5 * g0.r[0]->nIrreg * nts;
+        const size_t mslice = (size_t)5 * g0.s[0]->nIrreg * nts;
+        if (!add) std::fill(data, data + dslice * nExp, 0.f);
+        std::vector<float> tmp(dslice);
+        for (int e = 0; e < nExp; e++) {
+            ShotGrids g = shot_grids(src, rec, nRecGeom, e);
+            check_nt(g, nts);
+            if ((size_t)5 * g.s[0]->nIrreg * nts != mslice || (size_t)5 * g.r[0]->nIrreg * nts != dslice)
+                throw Error(EIO_ERR_ARG, "device counts differ between shots");
+            nl_shot_forward(c, g, model + (nModelExp == 1 ? 0 : (size_t)e * mslice), tmp.data());
+            float* d = data + (size_t)e * dslice;
+            for (size_t i = 0; i < dslice; i++) d[i] += tmp[i];
+        }
+    });
+}
+
+EIO_API int eio_nl_adjoint(eio_ctx* c, int add, int nExp, int nModelExp, float* model, const float* data,
+                           eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom) {
+    return guarded([&] {
+        if (!c || !model || !data || !src || !rec || nExp < 1) throw Error(EIO_ERR_ARG, "null argument");
+        if (nModelExp != 1 && nModelExp != nExp) throw Error(EIO_ERR_ARG, "model shot axis must be 1 or nExp");
+        if (nRecGeom != 1 && nRecGeom != nExp) throw Error(EIO_ERR_ARG, "receiver geometry count must be 1 or nExp");
+        const int nts = c->fd.p.nts;
+        ShotGrids g0 = shot_grids(src, rec, nRecGeom, 0);
+        const size_t dslice = (size_t)5 * g0.r[0]->nIrreg * nts;
+        const size_t mslice = (size_t)5 * g0.s[0]->nIrreg * nts;
+        if (!add) std::fill(model, model + mslice * nModelExp, 0.f);
+        std::vector<float> slice(mslice, 0.f);
+        for (int e = 0; e < nExp; e++) {
+            ShotGrids g = shot_grids(src, rec, nRecGeom, e);
+            check_nt(g, nts);
+            if ((size_t)5 * g.s[0]->nIrreg * nts != mslice || (size_t)5 * g.r[0]->nIrreg * nts != dslice)
+                throw Error(EIO_ERR_ARG, "device counts differ between shots");
+            if (nModelExp == 1) {
+                // constant source signal: stack every shot (nonlinearPropElasticShotsGpu.cpp:384-417)
+                nl_shot_adjoint(c, g, slice.data(), data + (size_t)e * dslice);
+            } else {
+                std::fill(slice.begin(), slice.end(), 0.f);
+                nl_shot_adjoint(c, g, slice.data(), data + (size_t)e * dslice);
+                float* m = model + (size_t)e * mslice;
+                for (size_t i = 0; i < mslice; i++) m[i] += slice[i];
+            }
+        }
+        if (nModelExp == 1)
+            for (size_t i = 0; i < mslice; i++) model[i] += slice[i];
+    });
+}
+
+EIO_API int eio_born_forward(eio_ctx* c, int add, int nExp, const float* model, float* data,
+                             const float* const* sigs, int nSignals, eio_sinterp* const* src, eio_sinterp* const* rec,
+                             int nRecGeom) {
+    return guarded([&] {
+        if (!c || !model || !data || !src || !rec || !sigs || nExp < 1) throw Error(EIO_ERR_ARG, "null argument");
+        if (nSignals != 1 && nSignals != nExp) throw Error(EIO_ERR_ARG, "source signal count must be 1 or nExp");
+        if (nRecGeom != 1 && nRecGeom != nExp) throw Error(EIO_ERR_ARG, "receiver geometry count must be 1 or nExp");
+        const int nts = c->fd.p.nts;
+        ShotGrids g0 = shot_grids(src, rec, nRecGeom, 0);
+        const size_t dslice = (size_t)5 * g0.r[0]->nIrreg * nts;
+        if (!add) std::fill(data, data + dslice * nExp, 0.f);
+        std::vector<float> sl[5];
+        born_model_slice(c->fd, model, sl);
+        float* dm[5];
+        for (int f = 0; f < 5; f++) dm[f] = sl[f].data();
+        for (int e = 0; e < nExp; e++) {
+            ShotGrids g = shot_grids(src, rec, nRecGeom, e);
+            check_nt(g, nts);
+            if ((size_t)5 * g.r[0]->nIrreg * nts != dslice) throw Error(EIO_ERR_ARG, "receiver counts differ");
+            std::vector<float> fine[5], dreg[5];
+            born_sources(c, g, sigs[nSignals == 1 ? 0 : e], fine);
+            float* sp[5]; float* dp[5];
+            for (int f = 0; f < 5; f++) {
+                dreg[f].assign((size_t)g.r[kFG[f]]->nReg * nts, 0.f);
+                sp[f] = fine[f].data(); dp[f] = dreg[f].data();
+            }
+            engine_born_host(c->eng, 0, sp, dm, dp, reg_geom(g));
+            float* d = data + (size_t)e * dslice;
+            const int nri = g.r[0]->nIrreg;
+            std::vector<float> tmp(dslice, 0.f);
+            for (int f = 0; f < 5; f++) sinterp_forward(*g.r[kFG[f]], true, dreg[f].data(), tmp.data() + (size_t)f * nri * nts);
+            for (size_t i = 0; i < dslice; i++) d[i] += tmp[i];
+        }
+    });
+}
+
+EIO_API int eio_born_adjoint(eio_ctx* c, int add, int nExp, float* model, const float* data,
+                             const float* const* sigs, int nSignals, eio_sinterp* const* src, eio_sinterp* const* rec,
+                             int nRecGeom) {
+    return guarded([&] {
+        if (!c || !model || !data || !src || !rec || !sigs || nExp < 1) throw Error(EIO_ERR_ARG, "null argument");
+        if (nSignals != 1 && nSignals != nExp) throw Error(EIO_ERR_ARG, "source signal count must be 1 or nExp");
+        if (nRecGeom != 1 && nRecGeom != nExp) throw Error(EIO_ERR_ARG, "receiver geometry count must be 1 or nExp");
+        const FdParam& fd = c->fd;
+        const int nts = fd.p.nts, nz = fd.p.nz, nx = fd.p.nx;
+        const size_t n = (size_t)nz * nx;
+        if (!add) std::fill(model, model + 3 * n, 0.f);
+        ShotGrids g0 = shot_grids(src, rec, nRecGeom, 0);
+        const size_t dslice = (size_t)5 * g0.r[0]->nIrreg * nts;
+        std::vector<float> sl[5];
+        float* dm[5];
+        for (int f = 0; f < 5; f++) { sl[f].assign(n, 0.f); dm[f] = sl[f].data(); }
+        for (int e = 0; e < nExp; e++) {
+            ShotGrids g = shot_grids(src, rec, nRecGeom, e);
+            check_nt(g, nts);
+            if ((size_t)5 * g.r[0]->nIrreg * nts != dslice) throw Error(EIO_ERR_ARG, "receiver counts differ");
+            std::vector<float> fine[5], dreg[5];
+            born_sources(c, g, sigs[nSignals == 1 ? 0 : e], fine);
+            float* sp[5]; float* dp[5];
+            const int nri = g.r[0]->nIrreg;
+            for (int f = 0; f < 5; f++) {
+                const SInterp& r = *g.r[kFG[f]];
+                dreg[f].assign((size_t)r.nReg * nts, 0.f);
+                sinterp_adjoint(r, false, dreg[f].data(), data + (size_t)e * dslice + (size_t)f * nri * nts);
+                sp[f] = fine[f].data(); dp[f] = dreg[f].data();
+            }
+            engine_born_host(c->eng, 1, sp, dm, dp, reg_geom(g));
+        }
+        // scaling and un-staggering, BornElasticShotsGpu.cpp:325-371
+        const double tdtw = 2.0 * fd.dtw;
+        for (size_t i = 0; i < n; i++) {
+            sl[0][i] *= fd.par[0][i];
+            sl[1][i] *= fd.par[1][i];
+            sl[2][i] = (float)(sl[2][i] * tdtw);
+            sl[3][i] = (float)(sl[3][i] * tdtw);
+            sl[4][i] = (float)(sl[4][i] * tdtw);
+        }
+        std::vector<float> t1(model, model + n);
+        stagger_x(0, 1, nz, nx, sl[0].data(), t1.data());
+        stagger_z(0, 1, nz, nx, sl[1].data(), t1.data());
+        std::copy(t1.begin(), t1.end(), model);
+        std::vector<float> t2(n);
+        stagger_z(0, 0, nz, nx, sl[4].data(), t2.data());
+        std::vector<float> t3(n);
+        stagger_x(0, 0, nz, nx, t2.data(), t3.data());
+        for (size_t i = 0; i < n; i++) {
+            model[n + i] += sl[2][i];
+            model[2 * n + i] += sl[3][i] + t3[i];
+        }
+    });
+}

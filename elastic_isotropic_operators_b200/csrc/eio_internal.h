@@ -1,0 +1,79 @@
+// Internal declarations shared by the host-preparation code (eio_host.cpp) and
+// the device engine (eio_engine.cu).
+#pragma once
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "eio_b200.h"
+
+namespace eio {
+
+constexpr int SUB_MAX = 100;   // varDeclare.h:11 (2*sub must stay below it)
+constexpr int PAD_MAX = 500;   // varDeclare.h:10
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+// ---------------------------------------------------------------- host prep
+struct FdParam {
+    eio_fd_params p;
+    int S = 0;            // internal sub-steps per coarse sample (2*sub)
+    int ntw = 0;
+    float dtw = 0.f;
+    int minPad = 0;
+    float zc[4], xc[4];   // FD coefficients
+    std::vector<float> filt;   // 2*(S+1) time-interpolation filter
+    std::vector<float> damp;   // [minPad] cosine taper
+    float dts_inv = 0.f;       // Born: 1/(2 dts)
+    float minVpVs = 0.f, maxVpVs = 0.f;
+    std::vector<float> par[5]; // rhoxDtw, rhozDtw, lamb2MuDtw, lambDtw, muxzDtw
+};
+
+// Builds the FD parameters, checks the QC of fdParamElastic and prepares the
+// scaled staggered medium.  Throws Error(EIO_ERR_QC, ...) on QC failure.
+void build_fdparam(const eio_fd_params& p, const float* elasticParam, FdParam& out);
+void stagger_x(int adj, int add, int nz, int nx, float* model, float* data);
+void stagger_z(int adj, int add, int nz, int nx, float* model, float* data);
+void time_interp(int adj, int add, int nts, float dts, float ots, int S, int nDev, float* coarse, float* fine);
+
+struct SInterp {
+    int nIrreg = 0, nReg = 0, nft = 0, nt = 0;
+    std::vector<int> gpi;      // [nIrreg*nft]
+    std::vector<float> w;      // [nIrreg*nft]
+    std::vector<int> slot;     // unique slot of every (device, filter) entry
+    std::vector<int> uniq;     // [nReg] unique regular positions, first-seen order
+    int nz = 0, nx = 0;
+};
+void build_sinterp(const float* zc, const float* xc, int nDev, int nz, float oz, float dz, int nx, float ox,
+                   float dx, int nt, const std::string& method, int nFilt, int dipole, float zDip, float xDip,
+                   SInterp& out);
+void sinterp_forward(const SInterp& s, bool add, const float* reg, float* irreg);
+void sinterp_adjoint(const SInterp& s, bool add, float* reg, const float* irreg);
+
+// ---------------------------------------------------------------- device engine
+struct Engine;   // opaque, defined in eio_engine.cu
+Engine* engine_create(int device, const FdParam& fd);
+void engine_destroy(Engine* e);
+void engine_set_medium(Engine* e, const FdParam& fd);
+void engine_set_checkpoint(Engine* e, int mode);
+void* engine_stream(Engine* e);
+// launch statistics: enable = 1/0 (-1 leaves it), reset = 1 zeroes the counters after reading
+void engine_stats(Engine* e, int enable, int reset, long long* launches, long long* step_launches, double* step_ms);
+
+struct ShotGeom {
+    const int* srcPos[4]; int nSrc[4];
+    const int* recPos[4]; int nRec[4];
+};
+// all float arrays are device pointers
+void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], const ShotGeom& g);
+void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5], float* const data[5],
+                 const ShotGeom& g);
+// host-pointer convenience wrappers (copy in/out through the engine's staging buffers)
+void engine_nl_host(Engine* e, int adj, float* const model[5], float* const data[5], const ShotGeom& g);
+void engine_born_host(Engine* e, int adj, float* const srcDtw[5], float* const dm[5], float* const data[5],
+                      const ShotGeom& g);
+}  // namespace eio

@@ -1,0 +1,472 @@
+// sm_100a kernels for the 2-D isotropic elastic velocity-stress staggered-grid
+// engine: one fused kernel per fine time step (leapfrog update of all five
+// fields + cosine taper + sparse source/receiver injection/extraction +
+// Born dense epilogues), plus the Born secondary-source / imaging kernels.
+//
+// Reference semantics restated here (paths relative to the reference project,
+// F/ = elastic_iso_lib/elastic_iso_float/prop, K = F/src/kernelsGpuElastic.cu):
+//   ker_step_fwd K:234-377, ker_step_adj K:380-529, dampCosineEdge K:1192-1221,
+//   ker_inject_interp_source_* K:172-189, ker_inject_source_* K:121-168,
+//   ker_interp_inject_data_* K:191-229, ker_record_interp_* K:7-60,100-116,
+//   interpWavefieldSingleComp K:1337-1346, injectSecondarySource K:1363-1367,
+//   extractInterpAdjointWavefield K:1369-1376, imagingElaFwdGpu K:1381-1459,
+//   imagingElaAdjGpu K:1538-1613.
+//
+// Fusion of the taper.  The reference runs  n = o + D(c); n += src;
+// damp(n); damp(c); swap  with o and n aliased.  The copy of c damped at step
+// k is only consumed as "o" at step k+1, so the second damping of each array
+// is deferred to its next use:  n = d * (d * o + D(c) + src).  Every array is
+// therefore multiplied by the same taper coefficients in the same order as in
+// the reference, without a separate full-grid launch.
+//
+// Layout: every field is [nx][nz] with z fastest (i = ix*nz + iz), exactly
+// the reference layout.  The interior (FAT..n-FAT) is updated; the 4-cell FAT
+// frame is never written and stays zero.  nz % 4 == 0 always holds because the
+// reference requires (nz - 2*FAT) % 16 == 0, so every column is 16-byte
+// aligned and the z axis is processed with float4 vectors.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace eio {
+
+constexpr int FAT = 4;
+constexpr int TZ = 64;             // tile cells along z
+constexpr int TX = 16;             // tile cells along x
+constexpr int NTZ = TZ / 4;        // threads along z (one float4 each)
+constexpr int NTX = TX / 2;        // threads along x (two columns each)
+constexpr int NT = NTZ * NTX;      // 128 threads per CTA
+constexpr int SZ = TZ + 2 * FAT;   // shared tile extent along z (72)
+constexpr int SX = TX + 2 * FAT;   // shared tile extent along x (24)
+constexpr int SMEM_FIELD = SX * SZ;
+
+// sparse point entry: packed local cell + field, and the column of the
+// time-major signal matrix of that field
+struct PointEntry {
+    int key;   // field << 16 | lx << 8 | lz   (lx < TX, lz < TZ)
+    int col;
+};
+
+struct SparseOp {
+    const int* tile_start;    // [ntiles+1] CSR over tiles, or nullptr
+    const PointEntry* ent;
+    float* sig[5];            // time-major [nt][ld[f]] per field
+    int ld[5];
+    int t0;                   // coarse (or fine) time row
+    float w0, w1;             // time-interpolation weights for rows t0, t0+1
+};
+
+struct StepArgs {
+    float* o[5];              // old level, overwritten with the new level
+    const float* c[5];        // current level
+    const float* par[5];      // rhoxDtw, rhozDtw, lamb2MuDtw, lambDtw, muxzDtw
+    const float* dampz;       // [nz] taper along z (1 outside the pad band)
+    const float* dampx;       // [nx]
+    int nz, nx;
+    int ntz;                  // number of tiles along z
+    float cz[4], cx[4];
+    SparseOp inj;             // added before the final taper (sources / data)
+    SparseOp ext;             // read after the final taper (receivers / sources)
+    // Born dense epilogues
+    float* W0; float* W1;     // source history vx / vz, [nts][nx*nz]
+    long long wstride;        // nx*nz
+    int wt;                   // coarse row
+    float ww0, ww1;
+    const float* ssL[5]; const float* ssR[5];   // scattered-field injection
+    float* eL[5]; float* eR[5];                 // adjoint extraction
+    float sw0, sw1;
+};
+
+enum { EPI_NONE = 0, EPI_SAVE_W = 1, EPI_INJ_SS = 2, EPI_EXT_SS = 3 };
+
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+__device__ __forceinline__ float& at(float4& v, int j) { return reinterpret_cast<float*>(&v)[j]; }
+__device__ __forceinline__ float at(const float4& v, int j) { return reinterpret_cast<const float*>(&v)[j]; }
+
+// z-derivatives of 4 consecutive cells from a 12-value window v[-4..7]
+// (w = v shifted by +4).  Dminus: sum c_k (f[z+k] - f[z-1-k]); Dplus: sum c_k (f[z+1+k] - f[z-k]).
+__device__ __forceinline__ float4 dmz(const float* w, const float* c)
+{
+    float4 r;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const float* v = w + 4 + j;
+        at(r, j) = c[0] * (v[0] - v[-1]) + c[1] * (v[1] - v[-2]) + c[2] * (v[2] - v[-3]) + c[3] * (v[3] - v[-4]);
+    }
+    return r;
+}
+__device__ __forceinline__ float4 dpz(const float* w, const float* c)
+{
+    float4 r;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const float* v = w + 4 + j;
+        at(r, j) = c[0] * (v[1] - v[0]) + c[1] * (v[2] - v[-1]) + c[2] * (v[3] - v[-2]) + c[3] * (v[4] - v[-3]);
+    }
+    return r;
+}
+// x-derivatives at column index m of a window of float4 columns q[] (q[m] = column x)
+__device__ __forceinline__ float4 dmx(const float4* q, int m, const float* c)
+{
+    float4 r;
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        at(r, j) = c[0] * (at(q[m], j) - at(q[m - 1], j)) + c[1] * (at(q[m + 1], j) - at(q[m - 2], j)) +
+                   c[2] * (at(q[m + 2], j) - at(q[m - 3], j)) + c[3] * (at(q[m + 3], j) - at(q[m - 4], j));
+    return r;
+}
+__device__ __forceinline__ float4 dpx(const float4* q, int m, const float* c)
+{
+    float4 r;
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        at(r, j) = c[0] * (at(q[m + 1], j) - at(q[m], j)) + c[1] * (at(q[m + 2], j) - at(q[m - 1], j)) +
+                   c[2] * (at(q[m + 3], j) - at(q[m - 2], j)) + c[3] * (at(q[m + 4], j) - at(q[m - 3], j));
+    return r;
+}
+
+// Load the 12-value z window for local column lx starting at local z lz (multiple of 4)
+__device__ __forceinline__ void zwin(const float* s, int lx, int lz, float* w)
+{
+    const float* p = s + lx * SZ + lz - FAT;
+    float4 a = ld4(p), b = ld4(p + 4), c = ld4(p + 8);
+    w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
+    w[4] = b.x; w[5] = b.y; w[6] = b.z; w[7] = b.w;
+    w[8] = c.x; w[9] = c.y; w[10] = c.z; w[11] = c.w;
+}
+// Load the 10 float4 columns lx0-4 .. lx0+5 at local z lz
+__device__ __forceinline__ void xwin(const float* s, int lx0, int lz, float4* q)
+{
+#pragma unroll
+    for (int m = 0; m < 10; m++) q[m] = ld4(s + (lx0 - FAT + m) * SZ + lz);
+}
+
+// One fused fine time step.  DIR 0 = forward (ker_step_fwd), 1 = adjoint (ker_step_adj).
+template <int DIR, int EPI>
+__global__ void __launch_bounds__(NT) k_step(StepArgs a)
+{
+    __shared__ __align__(16) float sm[5 * SMEM_FIELD];
+
+    const int tid = threadIdx.x;
+    const int tile = blockIdx.x;
+    const int bz = tile % a.ntz, bx = tile / a.ntz;
+    const int z0 = FAT + bz * TZ, x0 = FAT + bx * TX;
+    const int nz = a.nz;
+
+    // ---- stage the current level (forward) or its scaled combinations (adjoint)
+    {
+        const int nq = SZ / 4;                    // float4 per shared column
+        for (int q = tid; q < nq * SX; q += NT) {
+            const int lx = q / nq, lz4 = (q % nq) * 4;
+            const int gz = z0 - FAT + lz4, gx = x0 - FAT + lx;
+            float4 v[5];
+            if (gz < nz) {
+                const long long gi = (long long)gx * nz + gz;
+                if (DIR == 0) {
+#pragma unroll
+                    for (int f = 0; f < 5; f++) v[f] = ldg4(a.c[f] + gi);
+                } else {
+                    float4 vx = ldg4(a.c[0] + gi), vz = ldg4(a.c[1] + gi), sxx = ldg4(a.c[2] + gi),
+                           szz = ldg4(a.c[3] + gi), sxz = ldg4(a.c[4] + gi);
+                    float4 rx = ldg4(a.par[0] + gi), rz = ldg4(a.par[1] + gi), l2m = ldg4(a.par[2] + gi),
+                           lam = ldg4(a.par[3] + gi), mu = ldg4(a.par[4] + gi);
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        at(v[0], j) = at(l2m, j) * at(sxx, j) + at(lam, j) * at(szz, j);  // -> d/dx-  (vx)
+                        at(v[1], j) = at(lam, j) * at(sxx, j) + at(l2m, j) * at(szz, j);  // -> d/dz-  (vz)
+                        at(v[2], j) = at(mu, j) * at(sxz, j);                             // -> vx, vz
+                        at(v[3], j) = at(rx, j) * at(vx, j);                              // -> sxx, sxz
+                        at(v[4], j) = at(rz, j) * at(vz, j);                              // -> szz, sxz
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int f = 0; f < 5; f++) v[f] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int f = 0; f < 5; f++) st4(sm + f * SMEM_FIELD + lx * SZ + lz4, v[f]);
+        }
+    }
+    __syncthreads();
+
+    const int tzi = tid % NTZ, txi = tid / NTZ;
+    const int lz = FAT + 4 * tzi;              // local z of my float4
+    const int lxa = FAT + 2 * txi;             // my two local columns: lxa, lxa+1
+    const int gz = z0 + 4 * tzi;
+    const bool valid = gz < nz - FAT;
+    float4 t[5][2];                            // new values before the final taper
+
+    {
+        const float* cz = a.cz;
+        const float* cx = a.cx;
+        const float* s0 = sm;
+        const float* s1 = sm + SMEM_FIELD;
+        const float* s2 = sm + 2 * SMEM_FIELD;
+        const float* s3 = sm + 3 * SMEM_FIELD;
+        const float* s4 = sm + 4 * SMEM_FIELD;
+        float4 q[10];
+        float w[12];
+        if (DIR == 0) {
+            // s0 vx, s1 vz, s2 sxx, s3 szz, s4 sxz
+            float4 dxsxx[2], dxsxz[2], dxvx[2], dxvz[2];
+            xwin(s2, lxa, lz, q); dxsxx[0] = dmx(q, 4, cx); dxsxx[1] = dmx(q, 5, cx);
+            xwin(s4, lxa, lz, q); dxsxz[0] = dpx(q, 4, cx); dxsxz[1] = dpx(q, 5, cx);
+            xwin(s0, lxa, lz, q); dxvx[0] = dpx(q, 4, cx); dxvx[1] = dpx(q, 5, cx);
+            xwin(s1, lxa, lz, q); dxvz[0] = dmx(q, 4, cx); dxvz[1] = dmx(q, 5, cx);
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const int lx = lxa + k;
+                float4 dzsxz, dzszz, dzvx, dzvz;
+                zwin(s4, lx, lz, w); dzsxz = dpz(w, cz);
+                zwin(s3, lx, lz, w); dzszz = dmz(w, cz);
+                zwin(s0, lx, lz, w); dzvx = dmz(w, cz);
+                zwin(s1, lx, lz, w); dzvz = dpz(w, cz);
+                const long long gi = (long long)(x0 + 2 * txi + k) * nz + gz;
+                if (valid) {
+                    const float4 rx = ldg4(a.par[0] + gi), rz = ldg4(a.par[1] + gi), l2m = ldg4(a.par[2] + gi),
+                                 lam = ldg4(a.par[3] + gi), mu = ldg4(a.par[4] + gi);
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        at(t[0][k], j) = at(rx, j) * (at(dxsxx[k], j) + at(dzsxz, j));
+                        at(t[1][k], j) = at(rz, j) * (at(dzszz, j) + at(dxsxz[k], j));
+                        at(t[2][k], j) = at(l2m, j) * at(dxvx[k], j) + at(lam, j) * at(dzvz, j);
+                        at(t[3][k], j) = at(lam, j) * at(dxvx[k], j) + at(l2m, j) * at(dzvz, j);
+                        at(t[4][k], j) = at(mu, j) * (at(dzvx, j) + at(dxvz[k], j));
+                    }
+                }
+            }
+        } else {
+            // s0 A=l2m*sxx+lam*szz, s1 B=lam*sxx+l2m*szz, s2 M=mu*sxz, s3 P=rhox*vx, s4 Q=rhoz*vz
+            float4 dxA[2], dxM[2], dxP[2], dxQ[2];
+            xwin(s0, lxa, lz, q); dxA[0] = dmx(q, 4, cx); dxA[1] = dmx(q, 5, cx);
+            xwin(s2, lxa, lz, q); dxM[0] = dpx(q, 4, cx); dxM[1] = dpx(q, 5, cx);
+            xwin(s3, lxa, lz, q); dxP[0] = dpx(q, 4, cx); dxP[1] = dpx(q, 5, cx);
+            xwin(s4, lxa, lz, q); dxQ[0] = dmx(q, 4, cx); dxQ[1] = dmx(q, 5, cx);
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const int lx = lxa + k;
+                float4 dzM, dzB, dzP, dzQ;
+                zwin(s2, lx, lz, w); dzM = dpz(w, cz);
+                zwin(s1, lx, lz, w); dzB = dmz(w, cz);
+                zwin(s3, lx, lz, w); dzP = dmz(w, cz);
+                zwin(s4, lx, lz, w); dzQ = dpz(w, cz);
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    at(t[0][k], j) = -(at(dxA[k], j) + at(dzM, j));
+                    at(t[1][k], j) = -(at(dzB, j) + at(dxM[k], j));
+                    at(t[2][k], j) = -at(dxP[k], j);
+                    at(t[3][k], j) = -at(dzQ, j);
+                    at(t[4][k], j) = -(at(dzP, j) + at(dxQ[k], j));
+                }
+            }
+        }
+    }
+
+    // ---- deferred taper of the old level, leapfrog sum
+    float dz4[4], dxk[2];
+#pragma unroll
+    for (int j = 0; j < 4; j++) dz4[j] = valid ? __ldg(a.dampz + gz + j) : 1.f;
+#pragma unroll
+    for (int k = 0; k < 2; k++) dxk[k] = __ldg(a.dampx + x0 + 2 * txi + k);
+    if (valid) {
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const long long gi = (long long)(x0 + 2 * txi + k) * nz + gz;
+#pragma unroll
+            for (int f = 0; f < 5; f++) {
+                const float4 o = ld4(a.o[f] + gi);
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const float d = fminf(dz4[j], dxk[k]);
+                    at(t[f][k], j) = d * at(o, j) + at(t[f][k], j);
+                }
+            }
+            if (EPI == EPI_INJ_SS) {
+#pragma unroll
+                for (int f = 0; f < 5; f++) {
+                    const float4 l = ldg4(a.ssL[f] + gi), r = ldg4(a.ssR[f] + gi);
+#pragma unroll
+                    for (int j = 0; j < 4; j++) at(t[f][k], j) += at(l, j) * a.sw0 + at(r, j) * a.sw1;
+                }
+            }
+        }
+    }
+
+    // ---- sparse injection (sources / adjoint data), before the final taper
+    const int tz_total = a.ntz;
+    (void)tz_total;
+    if (a.inj.tile_start) {
+        const int e0 = a.inj.tile_start[tile], e1 = a.inj.tile_start[tile + 1];
+        if (e1 > e0) {   // CTA-uniform
+            float* acc = sm;                      // reuse: [5][TX][TZ]
+            __syncthreads();
+            for (int i = tid; i < 5 * TX * TZ; i += NT) acc[i] = 0.f;
+            __syncthreads();
+            for (int e = e0 + tid; e < e1; e += NT) {
+                const PointEntry pe = a.inj.ent[e];
+                const int f = pe.key >> 16, lx = (pe.key >> 8) & 0xff, lzz = pe.key & 0xff;
+                const float* sg = a.inj.sig[f];
+                const int ld = a.inj.ld[f];
+                const float v = sg[(long long)a.inj.t0 * ld + pe.col] * a.inj.w0 +
+                                sg[(long long)(a.inj.t0 + 1) * ld + pe.col] * a.inj.w1;
+                atomicAdd(acc + (f * TX + lx) * TZ + lzz, v);
+            }
+            __syncthreads();
+            if (valid) {
+#pragma unroll
+                for (int k = 0; k < 2; k++)
+#pragma unroll
+                    for (int f = 0; f < 5; f++) {
+                        const float4 v = ld4(acc + (f * TX + 2 * txi + k) * TZ + 4 * tzi);
+#pragma unroll
+                        for (int j = 0; j < 4; j++) at(t[f][k], j) += at(v, j);
+                    }
+            }
+        }
+    }
+
+    // ---- final taper, store, dense epilogues
+    if (valid) {
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const long long gi = (long long)(x0 + 2 * txi + k) * nz + gz;
+#pragma unroll
+            for (int f = 0; f < 5; f++) {
+#pragma unroll
+                for (int j = 0; j < 4; j++) at(t[f][k], j) *= fminf(dz4[j], dxk[k]);
+                st4(a.o[f] + gi, t[f][k]);
+            }
+            if (EPI == EPI_SAVE_W) {
+                float* w0p = a.W0 + (long long)a.wt * a.wstride + gi;
+                float* w1p = a.W1 + (long long)a.wt * a.wstride + gi;
+                float4 u0 = ld4(w0p), u1 = ld4(w0p + a.wstride), v0 = ld4(w1p), v1 = ld4(w1p + a.wstride);
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    at(u0, j) += at(t[0][k], j) * a.ww0; at(u1, j) += at(t[0][k], j) * a.ww1;
+                    at(v0, j) += at(t[1][k], j) * a.ww0; at(v1, j) += at(t[1][k], j) * a.ww1;
+                }
+                st4(w0p, u0); st4(w0p + a.wstride, u1); st4(w1p, v0); st4(w1p + a.wstride, v1);
+            }
+            if (EPI == EPI_EXT_SS) {
+#pragma unroll
+                for (int f = 0; f < 5; f++) {
+                    float4 l = ld4(a.eL[f] + gi), r = ld4(a.eR[f] + gi);
+#pragma unroll
+                    for (int j = 0; j < 4; j++) { at(l, j) += at(t[f][k], j) * a.sw0; at(r, j) += at(t[f][k], j) * a.sw1; }
+                    st4(a.eL[f] + gi, l); st4(a.eR[f] + gi, r);
+                }
+            }
+        }
+    }
+
+    // ---- sparse extraction (receivers / adjoint sources), after the final taper
+    if (a.ext.tile_start) {
+        const int e0 = a.ext.tile_start[tile], e1 = a.ext.tile_start[tile + 1];
+        if (e1 > e0) {
+            float* stg = sm;                      // [5][TX][TZ]
+            __syncthreads();
+            if (valid) {
+#pragma unroll
+                for (int k = 0; k < 2; k++)
+#pragma unroll
+                    for (int f = 0; f < 5; f++) st4(stg + (f * TX + 2 * txi + k) * TZ + 4 * tzi, t[f][k]);
+            }
+            __syncthreads();
+            for (int e = e0 + tid; e < e1; e += NT) {
+                const PointEntry pe = a.ext.ent[e];
+                const int f = pe.key >> 16, lx = (pe.key >> 8) & 0xff, lzz = pe.key & 0xff;
+                const float v = stg[(f * TX + lx) * TZ + lzz];
+                float* sg = a.ext.sig[f];
+                const int ld = a.ext.ld[f];
+                sg[(long long)a.ext.t0 * ld + pe.col] += v * a.ext.w0;
+                sg[(long long)(a.ext.t0 + 1) * ld + pe.col] += v * a.ext.w1;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Born secondary source (imagingElaFwdGpu) and imaging condition (imagingElaAdjGpu)
+// One thread per interior cell; W holds coarse Vx/Vz snapshots [nts][nx*nz].
+// ---------------------------------------------------------------------------
+struct ImagingArgs {
+    const float* Wvx; const float* Wvz;
+    long long wstride;
+    int nz, nx, nts, its;
+    float cz[4], cx[4];
+    float dts_inv;
+    float* dm[5];   // fwd: read; adj: accumulated
+    float* ss[5];   // fwd: written; adj: read
+};
+
+__device__ __forceinline__ float dminus(const float* f, long long i, long long s, const float* c)
+{
+    return c[0] * (f[i] - f[i - s]) + c[1] * (f[i + s] - f[i - 2 * s]) + c[2] * (f[i + 2 * s] - f[i - 3 * s]) +
+           c[3] * (f[i + 3 * s] - f[i - 4 * s]);
+}
+__device__ __forceinline__ float dplus(const float* f, long long i, long long s, const float* c)
+{
+    return c[0] * (f[i + s] - f[i]) + c[1] * (f[i + 2 * s] - f[i - s]) + c[2] * (f[i + 3 * s] - f[i - 2 * s]) +
+           c[3] * (f[i + 4 * s] - f[i - 3 * s]);
+}
+
+template <int ADJ>
+__global__ void __launch_bounds__(256) k_imaging(ImagingArgs a)
+{
+    const int iz = FAT + blockIdx.x * blockDim.x + threadIdx.x;
+    const int ix = FAT + blockIdx.y;
+    if (iz >= a.nz - FAT) return;
+    const long long nz = a.nz;
+    const long long i = (long long)ix * nz + iz;
+    const float* vx = a.Wvx + (long long)a.its * a.wstride;
+    const float* vz = a.Wvz + (long long)a.its * a.wstride;
+    const float dvx_dx = dplus(vx, i, nz, a.cx);
+    const float dvz_dz = dplus(vz, i, 1, a.cz);
+    const float dmix = dminus(vx, i, 1, a.cz) + dminus(vz, i, nz, a.cx);
+    float tx, tz;
+    if (a.its == 0) {
+        tx = -a.Wvx[a.wstride + i];
+        tz = -a.Wvz[a.wstride + i];
+    } else if (a.its == a.nts - 1) {
+        tx = a.Wvx[(long long)(a.its - 1) * a.wstride + i];
+        tz = a.Wvz[(long long)(a.its - 1) * a.wstride + i];
+    } else {
+        tx = a.Wvx[(long long)(a.its - 1) * a.wstride + i] - a.Wvx[(long long)(a.its + 1) * a.wstride + i];
+        tz = a.Wvz[(long long)(a.its - 1) * a.wstride + i] - a.Wvz[(long long)(a.its + 1) * a.wstride + i];
+    }
+    if (!ADJ) {
+        a.ss[0][i] = a.dm[0][i] * tx * a.dts_inv;
+        a.ss[1][i] = a.dm[1][i] * tz * a.dts_inv;
+        const float dl = a.dm[2][i], dmu = a.dm[3][i];
+        a.ss[2][i] = dl * (dvx_dx + dvz_dz) + 2.0f * dmu * dvx_dx;
+        a.ss[3][i] = dl * (dvx_dx + dvz_dz) + 2.0f * dmu * dvz_dz;
+        a.ss[4][i] = a.dm[4][i] * dmix;
+    } else {
+        const float s0 = a.ss[0][i], s1 = a.ss[1][i], s2 = a.ss[2][i], s3 = a.ss[3][i], s4 = a.ss[4][i];
+        a.dm[0][i] += s0 * tx * a.dts_inv;
+        a.dm[1][i] += s1 * tz * a.dts_inv;
+        a.dm[2][i] += (s2 + s3) * (dvx_dx + dvz_dz);
+        a.dm[3][i] += 2.0f * (dvx_dx * s2 + dvz_dz * s3);
+        a.dm[4][i] += s4 * dmix;
+    }
+}
+
+// time-major <-> trace-major transposes for the sparse signal matrices
+__global__ void k_transpose(const float* __restrict__ in, float* __restrict__ out, int rows, int cols)
+{
+    __shared__ float tileb[32][33];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int r = by + k, c = bx + threadIdx.x;
+        if (r < rows && c < cols) tileb[k][threadIdx.x] = in[(long long)r * cols + c];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int r = bx + k, c = by + threadIdx.x;   // out is [cols][rows]
+        if (r < cols && c < rows) out[(long long)r * rows + c] = tileb[threadIdx.x][k];
+    }
+}
+
+}  // namespace eio

@@ -1,0 +1,513 @@
+"""Operator classes of the elastic propagation path, drop-in for the reference's
+pybind11 modules ``pyElastic_iso_float_nl`` / ``pyElastic_iso_float_born`` and
+the Python wrappers of ``Elastic_iso_float_prop.py``.
+
+Same class names, constructor arguments, method names, argument meaning and
+``add`` semantics as the reference:
+
+* ``spaceInterpGpu(zCoord, xCoord, gridHyper, nt, method, nFilt, dipole,
+  zDipoleShift, xDipoleShift)``            (PF/pyElastic_iso_float_nl.cpp:19-30)
+* ``nonlinearPropElasticShotsGpu(elasticParam, par, 8 geometry lists)`` with
+  ``forward``, ``adjoint``, ``setBackground``, ``dotTest``
+                                            (PF/pyElastic_iso_float_nl.cpp:32-54)
+* ``BornElasticShotsGpu(elasticParam, par, sourcesSignalsVector, 8 geometry
+  lists)`` with ``forward``, ``adjoint``, ``setBackground``, ``dotTest``
+                                            (PF/pyElastic_iso_float_born.cpp:19-36)
+* ``buildSourceGeometry`` / ``buildReceiversGeometry``
+                                            (PF/Elastic_iso_float_prop.py:205-364, 525-661)
+
+(PF = elastic_iso_lib/python/python_float of the reference project.)
+Every numerical call goes through the CUDA library; errors from the C ABI
+(QC failures, bounds, CUDA) surface as ``EioError``.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import EioError, check, fptr, iptr
+from .sepvec import axis, hypercube, floatVector, getSepVector, paramObj
+
+__all__ = [
+    "EioError", "spaceInterpGpu", "nonlinearPropElasticShotsGpu", "BornElasticShotsGpu",
+    "buildSourceGeometry", "buildReceiversGeometry", "fd_params_from_par",
+]
+
+_FIELD_GRID = (1, 2, 0, 0, 3)   # vx -> x grid, vz -> z grid, sxx/szz -> center, sxz -> xz
+
+
+def _arr(v, dtype=np.float32):
+    a = v.getNdArray() if hasattr(v, "getNdArray") else np.asarray(v)
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def _hyper_of(v):
+    return v.getHyper() if hasattr(v, "getHyper") else None
+
+
+class spaceInterpGpu:
+    """Irregular acquisition devices <-> unique regular grid points
+    (spaceInterpGpu, F/src/spaceInterpGpu.cpp:11-362)."""
+
+    def __init__(self, zCoord, xCoord, gridHyper, nt, method="linear", nFilt=1, dipole=0,
+                 zDipoleShift=0.0, xDipoleShift=0.0):
+        z = _arr(zCoord).ravel()
+        x = _arr(xCoord).ravel()
+        if z.size != x.size:
+            raise ValueError("zCoord and xCoord must have the same length")
+        az, ax = gridHyper.getAxis(1), gridHyper.getAxis(2)
+        L = _lib.lib()
+        h = ctypes.c_void_p()
+        check(L.eio_sinterp_create(fptr(z), fptr(x), int(z.size), az.n, az.o, az.d, ax.n, ax.o, ax.d, int(nt),
+                                   method.encode(), int(nFilt), int(dipole), float(zDipoleShift),
+                                   float(xDipoleShift), ctypes.byref(h)))
+        self._h = h
+        self._L = L
+        self.nt = int(nt)
+        self.gridHyper = gridHyper
+        ni, nr, nf = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(L.eio_sinterp_sizes(h, ctypes.byref(ni), ctypes.byref(nr), ctypes.byref(nf)))
+        self.nDeviceIrreg, self.nDeviceReg, self.nFiltTotal = ni.value, nr.value, nf.value
+        pos = np.zeros(max(self.nDeviceReg, 1), dtype=np.int32)
+        check(L.eio_sinterp_positions(h, iptr(pos)))
+        self.regPosUnique = pos[: self.nDeviceReg].copy()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._L.eio_sinterp_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def getNDeviceReg(self):
+        return self.nDeviceReg
+
+    def getNDeviceIrreg(self):
+        return self.nDeviceIrreg
+
+    def getRegPosUnique(self):
+        return self.regPosUnique
+
+    def getWeights(self):
+        n = self.nDeviceIrreg * self.nFiltTotal
+        gpi = np.zeros(max(n, 1), dtype=np.int32)
+        w = np.zeros(max(n, 1), dtype=np.float32)
+        check(self._L.eio_sinterp_weights(self._h, iptr(gpi), fptr(w)))
+        return gpi[:n], w[:n]
+
+    def getInfo(self):
+        gpi, w = self.getWeights()
+        lines = ["---------- Space Interp Info ----------",
+                 "_nDeviceIrreg= %d" % self.nDeviceIrreg, "_nDeviceRreg= %d" % self.nDeviceReg]
+        for i in range(self.nDeviceIrreg):
+            lines.append("Irreg Device %d weights %s" % (i, w[i * self.nFiltTotal:(i + 1) * self.nFiltTotal]))
+        return "\n".join(lines)
+
+    def forward(self, add, signalReg, signalIrreg):
+        """regular [nReg][nt] -> irregular [nIrreg][nt]"""
+        reg = _arr(signalReg)
+        out = signalIrreg.getNdArray() if hasattr(signalIrreg, "getNdArray") else signalIrreg
+        res = np.ascontiguousarray(out, dtype=np.float32)
+        check(self._L.eio_sinterp_forward(self._h, int(bool(add)), fptr(reg), fptr(res)))
+        if res is not out:
+            out[...] = res
+        return out
+
+    def adjoint(self, add, signalReg, signalIrreg):
+        irr = _arr(signalIrreg)
+        out = signalReg.getNdArray() if hasattr(signalReg, "getNdArray") else signalReg
+        res = np.ascontiguousarray(out, dtype=np.float32)
+        check(self._L.eio_sinterp_adjoint(self._h, int(bool(add)), fptr(res), fptr(irr)))
+        if res is not out:
+            out[...] = res
+        return out
+
+
+def fd_params_from_par(par, elasticParam):
+    """eio_fd_params from a paramObj (keys of fdParamElastic.cpp:18-77) and the
+    elastic-parameter vector (whose first two axes give oz, ox)."""
+    if isinstance(par, dict):
+        par = paramObj(par)
+    p = _lib.FdParams()
+    _lib.lib().eio_fd_params_default(ctypes.byref(p))
+    hyp = _hyper_of(elasticParam)
+    p.nts = par.getInt("nts")
+    p.dts = par.getFloat("dts", 0.0)
+    p.ots = par.getFloat("ots", 0.0)
+    p.sub = par.getInt("sub")
+    p.nz = par.getInt("nz")
+    p.nx = par.getInt("nx")
+    p.dz = par.getFloat("dz", -1.0)
+    p.dx = par.getFloat("dx", -1.0)
+    p.oz = hyp.getAxis(1).o if hyp is not None else par.getFloat("oz", 0.0)
+    p.ox = hyp.getAxis(2).o if hyp is not None else par.getFloat("ox", 0.0)
+    p.zPadMinus = par.getInt("zPadMinus")
+    p.zPadPlus = par.getInt("zPadPlus")
+    p.xPadMinus = par.getInt("xPadMinus")
+    p.xPadPlus = par.getInt("xPadPlus")
+    p.fMax = par.getFloat("fMax", 1000.0)
+    p.blockSize = par.getInt("blockSize", 16)
+    p.fat = par.getInt("fat", 4)
+    p.alphaCos = par.getFloat("alphaCos", 0.99)
+    p.surfaceCondition = par.getInt("surfaceCondition", 0)
+    p.mod_par = par.getInt("mod_par", 1)
+    p.errorTolerance = par.getFloat("errorTolerance", 0.000001)
+    if hyp is not None:
+        # checkParfileConsistencySpace, F/src/fdParamElastic.cpp:308-326
+        scale = 1000.0 if p.mod_par == 2 else 1.0
+        tol = p.errorTolerance
+        az, ax = hyp.getAxis(1), hyp.getAxis(2)
+        dz = p.dz * (1000.0 if p.mod_par == 2 else 1.0)
+        dx = p.dx * (1000.0 if p.mod_par == 2 else 1.0)
+        if p.nz != az.n or abs(dz - az.d * scale) > tol:
+            raise EioError(-2, "**** ERROR: nz/dz not consistent with parfile ****")
+        if p.nx != ax.n or abs(dx - ax.d * scale) > tol:
+            raise EioError(-2, "**** ERROR: nx/dx not consistent with parfile ****")
+    return p
+
+
+def _device_from_par(par):
+    ids = par.getInts("iGpu", [-1])
+    if ids and ids[0] >= 0:
+        return int(ids[0])
+    return 0
+
+
+class _ElasticOp:
+    """Shared state of the two multi-shot operators: one device context
+    (fdParamElastic + device allocation) on the first GPU of the list."""
+
+    def __init__(self, elasticParam, par, src, rec):
+        if isinstance(par, dict):
+            par = paramObj(par)
+        self.par = par
+        self.nExp = par.getInt("nExp")
+        self.fd = fd_params_from_par(par, elasticParam)
+        self.device = _device_from_par(par)
+        ep = _arr(elasticParam)
+        if ep.size != 3 * self.fd.nz * self.fd.nx:
+            raise EioError(-1, "elastic parameter size does not match nz*nx*3")
+        self._L = _lib.lib()
+        h = ctypes.c_void_p()
+        check(self._L.eio_ctx_create(ctypes.byref(self.fd), fptr(ep), self.device, ctypes.byref(h)))
+        self._ctx = h
+        self.src = [list(g) for g in src]
+        self.rec = [list(g) for g in rec]
+        if any(len(g) != self.nExp for g in self.src):
+            raise EioError(-1, "each source geometry list must hold nExp interpolators")
+        nrg = {len(g) for g in self.rec}
+        if len(nrg) != 1 or list(nrg)[0] not in (1, self.nExp):
+            raise EioError(-1, "receiver geometry lists must hold 1 or nExp interpolators")
+        self.nRecGeom = len(self.rec[0])
+        self._src_arr = _lib.ptr_array([g[i].handle.value for i in range(self.nExp) for g in self.src])
+        self._rec_arr = _lib.ptr_array([g[i].handle.value for i in range(self.nRecGeom) for g in self.rec])
+        self.nSrcIrreg = self.src[0][0].nDeviceIrreg
+        self.nRecIrreg = self.rec[0][0].nDeviceIrreg
+
+    def __del__(self):
+        h = getattr(self, "_ctx", None)
+        if h is not None and h.value:
+            self._L.eio_ctx_destroy(h)
+            self._ctx = None
+
+    @property
+    def ctx(self):
+        return self._ctx
+
+    def setBackground(self, elasticParam):
+        """Rebuild the medium (fdParamElastic QC runs again and may raise)."""
+        ep = _arr(elasticParam)
+        check(self._L.eio_ctx_set_background(self._ctx, fptr(ep)))
+
+    def setCheckpointPrecision(self, mode):
+        """Born source-wavefield snapshots: 0 FP32, 1 BF16, 2 FP16."""
+        check(self._L.eio_ctx_set_checkpoint_precision(self._ctx, int(mode)))
+
+    def getMedium(self):
+        n = self.fd.nz * self.fd.nx
+        out = [np.zeros((self.fd.nx, self.fd.nz), np.float32) for _ in range(5)]
+        check(self._L.eio_ctx_get_medium(self._ctx, *[fptr(o) for o in out]))
+        return out
+
+    def _check_time(self, vec):
+        hyp = _hyper_of(vec)
+        if hyp is None:
+            return
+        t = hyp.getAxis(1)
+        tol = self.fd.errorTolerance
+        if t.n != self.fd.nts or abs(t.d - self.fd.dts) > tol or abs(t.o - self.fd.ots) > tol:
+            raise EioError(-2, "**** ERROR: nts/dts/ots not consistent with parfile ****")
+
+    def _dot_test(self, model_space, data_space, verbose, maxError):
+        """operator.h:50-89 dot-product test, with FP64 dot products."""
+        d1 = model_space.clone().rand(1234)
+        r1 = data_space.clone().rand(4321)
+        d2 = model_space.clone()
+        r2 = data_space.clone()
+        self.forward(False, d1, r2)
+        self.adjoint(False, d2, r1)
+        dot1, dot2 = r1.dot(r2), d1.dot(d2)
+        err_no_add = abs((dot1 - dot2) / dot2)
+        self.forward(True, d1, r2)
+        self.adjoint(True, d2, r1)
+        dot3, dot4 = r1.dot(r2), d1.dot(d2)
+        err_add = abs((dot3 - dot4) / dot4)
+        if verbose:
+            print("WITHOUT ADD:\ndot1: %.16g\ndot2: %.16g\nerror WITHOUT ADD: %.16g" % (dot1, dot2, err_no_add))
+            print("WITH ADD:\ndot3: %.16g\ndot4: %.16g\nerror with ADD: %.16g" % (dot3, dot4, err_add))
+        self.lastDotTest = (err_no_add, err_add)
+        return err_no_add <= maxError and err_add <= maxError
+
+
+class nonlinearPropElasticShotsGpu(_ElasticOp):
+    """Nonlinear elastic propagation over many shots
+    (nonlinearPropElasticShotsGpu, F/src/nonlinearPropElasticShotsGpu.cpp).
+
+    model: [nts, nSrc, 5, nModelExp] (numpy (nModelExp, 5, nSrc, nts));
+    data:  [nts, nRec, 5, nExp]      (numpy (nExp, 5, nRec, nts)).
+    """
+
+    def __init__(self, elasticParam, par, sourcesVectorCenterGrid, sourcesVectorXGrid, sourcesVectorZGrid,
+                 sourcesVectorXZGrid, receiversVectorCenterGrid, receiversVectorXGrid, receiversVectorZGrid,
+                 receiversVectorXZGrid):
+        super().__init__(elasticParam, par,
+                         [sourcesVectorCenterGrid, sourcesVectorXGrid, sourcesVectorZGrid, sourcesVectorXZGrid],
+                         [receiversVectorCenterGrid, receiversVectorXGrid, receiversVectorZGrid,
+                          receiversVectorXZGrid])
+
+    def _shapes(self, model, data):
+        m = model.getNdArray() if hasattr(model, "getNdArray") else model
+        d = data.getNdArray() if hasattr(data, "getNdArray") else data
+        if m.ndim == 3:
+            m = m.reshape((1,) + m.shape)
+        if m.shape[1] != 5:
+            raise EioError(-1, "model must have five wavefield components")
+        nme = m.shape[0]
+        if m.shape[2:] != (self.nSrcIrreg, self.fd.nts) or d.shape != (self.nExp, 5, self.nRecIrreg, self.fd.nts):
+            raise EioError(-1, "model/data shapes do not match the acquisition geometry")
+        return m, d, nme
+
+    def forward(self, add, model, data):
+        self._check_time(model)
+        self._check_time(data)
+        m, d, nme = self._shapes(model, data)
+        mm = np.ascontiguousarray(m, dtype=np.float32)
+        dd = np.ascontiguousarray(d, dtype=np.float32)
+        check(self._L.eio_nl_forward(self._ctx, int(bool(add)), self.nExp, nme, fptr(mm), fptr(dd),
+                                     self._src_arr, self._rec_arr, self.nRecGeom))
+        if dd is not d:
+            d[...] = dd
+
+    def adjoint(self, add, model, data):
+        self._check_time(model)
+        self._check_time(data)
+        m, d, nme = self._shapes(model, data)
+        mm = np.ascontiguousarray(m, dtype=np.float32)
+        dd = np.ascontiguousarray(d, dtype=np.float32)
+        check(self._L.eio_nl_adjoint(self._ctx, int(bool(add)), self.nExp, nme, fptr(mm), fptr(dd),
+                                     self._src_arr, self._rec_arr, self.nRecGeom))
+        if mm is not m:
+            m[...] = mm
+
+    def modelSpace(self, nModelExp=1):
+        t = axis(self.fd.nts, self.fd.ots, self.fd.dts)
+        return floatVector(hypercube(axes=[t, axis(self.nSrcIrreg), axis(5), axis(nModelExp)]))
+
+    def dataSpace(self):
+        t = axis(self.fd.nts, self.fd.ots, self.fd.dts)
+        return floatVector(hypercube(axes=[t, axis(self.nRecIrreg), axis(5), axis(self.nExp)]))
+
+    def dotTest(self, verbose=False, maxError=0.00001):
+        return self._dot_test(self.modelSpace(), self.dataSpace(), verbose, maxError)
+
+
+class BornElasticShotsGpu(_ElasticOp):
+    """Born (linearised) elastic operator over (drho, dlambda, dmu)
+    (BornElasticShotsGpu, F/src/BornElasticShotsGpu.cpp).
+
+    model: [nz, nx, 3] (numpy (3, nx, nz)); data: [nts, nRec, 5, nExp];
+    sourcesSignalsVector: list (1 or nExp) of [nts, nSrc, 5] vectors.
+    """
+
+    def __init__(self, elasticParam, par, sourcesSignalsVector, sourcesVectorCenterGrid, sourcesVectorXGrid,
+                 sourcesVectorZGrid, sourcesVectorXZGrid, receiversVectorCenterGrid, receiversVectorXGrid,
+                 receiversVectorZGrid, receiversVectorXZGrid):
+        super().__init__(elasticParam, par,
+                         [sourcesVectorCenterGrid, sourcesVectorXGrid, sourcesVectorZGrid, sourcesVectorXZGrid],
+                         [receiversVectorCenterGrid, receiversVectorXGrid, receiversVectorZGrid,
+                          receiversVectorXZGrid])
+        self.elasticHyper = _hyper_of(elasticParam)
+        self._sigs = []
+        for s in sourcesSignalsVector:
+            self._check_time(s)
+            a = _arr(s).reshape(5, self.nSrcIrreg, self.fd.nts)
+            self._sigs.append(np.ascontiguousarray(a))
+        if len(self._sigs) not in (1, self.nExp):
+            raise EioError(-1, "sourcesSignalsVector must hold 1 or nExp signals")
+        self._sig_arr = _lib.ptr_array([a.ctypes.data for a in self._sigs])
+
+    def _shapes(self, model, data):
+        m = model.getNdArray() if hasattr(model, "getNdArray") else model
+        d = data.getNdArray() if hasattr(data, "getNdArray") else data
+        if m.shape != (3, self.fd.nx, self.fd.nz) or d.shape != (self.nExp, 5, self.nRecIrreg, self.fd.nts):
+            raise EioError(-1, "model/data shapes do not match the grid or acquisition")
+        return m, d
+
+    def forward(self, add, model, data):
+        self._check_time(data)
+        m, d = self._shapes(model, data)
+        mm = np.ascontiguousarray(m, dtype=np.float32)
+        dd = np.ascontiguousarray(d, dtype=np.float32)
+        check(self._L.eio_born_forward(self._ctx, int(bool(add)), self.nExp, fptr(mm), fptr(dd), self._sig_arr,
+                                       len(self._sigs), self._src_arr, self._rec_arr, self.nRecGeom))
+        if dd is not d:
+            d[...] = dd
+
+    def adjoint(self, add, model, data):
+        self._check_time(data)
+        m, d = self._shapes(model, data)
+        mm = np.ascontiguousarray(m, dtype=np.float32)
+        dd = np.ascontiguousarray(d, dtype=np.float32)
+        check(self._L.eio_born_adjoint(self._ctx, int(bool(add)), self.nExp, fptr(mm), fptr(dd), self._sig_arr,
+                                       len(self._sigs), self._src_arr, self._rec_arr, self.nRecGeom))
+        if mm is not m:
+            m[...] = mm
+
+    def prepareShot(self, iExp):
+        """Regular-grid inputs of shot iExp for the single-shot *_reg_dev entry
+        points: 5 scaled fine-time source traces and the source / receiver
+        position lists (grid order center, x, z, xz)."""
+        src = [g[iExp] for g in self.src]
+        rec = [g[0 if self.nRecGeom == 1 else iExp] for g in self.rec]
+        ntw = (self.fd.nts - 1) * 2 * self.fd.sub + 1
+        fine = [np.zeros((src[_FIELD_GRID[f]].nDeviceReg, ntw), np.float32) for f in range(5)]
+        sig = self._sigs[0 if len(self._sigs) == 1 else iExp]
+        check(self._L.eio_born_prepare_sources(self._ctx, fptr(sig), _lib.ptr_array([g.handle.value for g in src]),
+                                               _lib.ptr_array([a.ctypes.data for a in fine])))
+        return fine, [g.getRegPosUnique() for g in src], [g.getRegPosUnique() for g in rec]
+
+    def prepareModel(self, model):
+        """(drho, dlambda, dmu) [3][nx][nz] -> the 5 staggered, scaled perturbation grids."""
+        m = _arr(model).reshape(3, self.fd.nx, self.fd.nz)
+        out = [np.zeros((self.fd.nx, self.fd.nz), np.float32) for _ in range(5)]
+        check(self._L.eio_born_prepare_model(self._ctx, fptr(m), _lib.ptr_array([a.ctypes.data for a in out])))
+        return out
+
+    def modelSpace(self):
+        if self.elasticHyper is not None:
+            return floatVector(self.elasticHyper.clone())
+        return floatVector(hypercube(ns=[self.fd.nz, self.fd.nx, 3]))
+
+    def dataSpace(self):
+        t = axis(self.fd.nts, self.fd.ots, self.fd.dts)
+        return floatVector(hypercube(axes=[t, axis(self.nRecIrreg), axis(5), axis(self.nExp)]))
+
+    def dotTest(self, verbose=False, maxError=0.00001):
+        return self._dot_test(self.modelSpace(), self.dataSpace(), verbose, maxError)
+
+
+# ---------------------------------------------------------------------------
+# Acquisition geometry builders, PF/Elastic_iso_float_prop.py:205-364, 525-661
+# ---------------------------------------------------------------------------
+def _staggered_hypers(elasticParam):
+    h = elasticParam.getHyper()
+    az, ax = h.getAxis(1), h.getAxis(2)
+    pax = h.getAxis(3) if h.getNdim() >= 3 else axis(3)
+    z = axis(az.n, az.o, az.d)
+    zs = axis(az.n, az.o - 0.5 * az.d, az.d)
+    x = axis(ax.n, ax.o, ax.d)
+    xs = axis(ax.n, ax.o - 0.5 * ax.d, ax.d)
+    return (hypercube(axes=[z, x, pax]), hypercube(axes=[z, xs, pax]),
+            hypercube(axes=[zs, x, pax]), hypercube(axes=[zs, xs, pax]))
+
+
+def _four_grids(zc, xc, hypers, nts, method, nfilt, dipole, zds, xds):
+    return [spaceInterpGpu(zc, xc, h, nts, method, nfilt, dipole, zds, xds) for h in hypers]
+
+
+def buildSourceGeometry(parObject, elasticParam):
+    """Sources on the four staggered grids, one set per shot.
+    Returns (center, x, z, xz) lists and the shot axis."""
+    if isinstance(parObject, dict):
+        parObject = paramObj(parObject)
+    dipole = parObject.getInt("dipole", 0)
+    zds = parObject.getFloat("zDipoleShift", 0.0)
+    xds = parObject.getFloat("xDipoleShift", 0.0)
+    nts = parObject.getInt("nts")
+    nExp = parObject.getInt("nExp")
+    h = elasticParam.getHyper()
+    dz, oz = h.getAxis(1).d, h.getAxis(1).o
+    dx, ox = h.getAxis(2).d, h.getAxis(2).o
+    hypers = _staggered_hypers(elasticParam)
+    method = parObject.getString("sourceInterpMethod", "linear")
+    nfilt = parObject.getInt("sourceInterpNumFilters", 4)
+    lists = ([], [], [], [])
+    geom = parObject.getString("sourceGeomFile", "None")
+    if geom != "None":
+        # numpy array [3][nSimSou][nExp] (x, y, z coordinates), as read from the geometry file
+        g = np.load(geom) if isinstance(geom, str) else np.asarray(geom)
+        if g.shape[2] != nExp:
+            raise ValueError("ERROR! nExp (%d) not consistent with number of shots provided within "
+                             "sourceGeomFile (%d)" % (nExp, g.shape[2]))
+        sourceAxis = axis(nExp, 1.0, 1.0)
+        for iExp in range(nExp):
+            zc = np.ascontiguousarray(g[2, :, iExp], dtype=np.float32)
+            xc = np.ascontiguousarray(g[0, :, iExp], dtype=np.float32)
+            for lst, grid in zip(lists, _four_grids(zc, xc, hypers, nts, method, nfilt, dipole, zds, xds)):
+                lst.append(grid)
+    else:
+        ozs = parObject.getInt("zSource") - 1 + parObject.getInt("zPadMinus") + parObject.getInt("fat", 4)
+        oxs = parObject.getInt("xSource") - 1 + parObject.getInt("xPadMinus") + parObject.getInt("fat", 4)
+        spacing = parObject.getInt("spacingShots")
+        sourceAxis = axis(nExp, ox + oxs * dx, spacing * dx)
+        for iExp in range(nExp):
+            zc = np.array([oz + ozs * dz], dtype=np.float32)
+            xc = np.array([ox + oxs * dx], dtype=np.float32)
+            for lst, grid in zip(lists, _four_grids(zc, xc, hypers, nts, method, nfilt, dipole, zds, xds)):
+                lst.append(grid)
+            oxs = oxs + spacing
+    return lists[0], lists[1], lists[2], lists[3], sourceAxis
+
+
+def buildReceiversGeometry(parObject, elasticParam):
+    """Receivers on the four staggered grids (constant geometry for all shots).
+    Returns (center, x, z, xz) lists and the receiver axis."""
+    if isinstance(parObject, dict):
+        parObject = paramObj(parObject)
+    dipole = parObject.getInt("dipole", 0)
+    zds = parObject.getFloat("zDipoleShift", 0.0)
+    xds = parObject.getFloat("xDipoleShift", 0.0)
+    nts = parObject.getInt("nts")
+    h = elasticParam.getHyper()
+    dz, oz = h.getAxis(1).d, h.getAxis(1).o
+    dx, ox = h.getAxis(2).d, h.getAxis(2).o
+    hypers = _staggered_hypers(elasticParam)
+    method = parObject.getString("recInterpMethod", "linear")
+    nfilt = parObject.getInt("recInterpNumFilters", 4)
+    geom = parObject.getString("recGeomFile", "none")
+    if geom != "none":
+        g = np.load(geom) if isinstance(geom, str) else np.asarray(geom)
+        xc = np.ascontiguousarray(g[0, :, 0], dtype=np.float32)
+        zc = np.ascontiguousarray(g[2, :, 0], dtype=np.float32)
+        nRec = parObject.getInt("nReceiver")
+        if nRec != len(xc):
+            raise ValueError("ERROR [buildReceiversGeometry]: Number of receiver coordinates (%s) not consistent "
+                             "with parameter file (nReceiver=%d)" % (len(xc), nRec))
+        receiverAxis = axis(nRec, 1.0, 1.0)
+    else:
+        ozr = parObject.getInt("depthReceiver") - 1 + parObject.getInt("zPadMinus") + parObject.getInt("fat", 4)
+        nxr = parObject.getInt("nReceiver")
+        oxr = parObject.getInt("oReceiver") - 1 + parObject.getInt("xPadMinus") + parObject.getInt("fat", 4)
+        dxr = parObject.getInt("dReceiver")
+        receiverAxis = axis(nxr, ox + oxr * dx, dxr * dx)
+        irec = np.arange(nxr, dtype=np.float64)
+        zc = np.empty(nxr, dtype=np.float32)
+        xc = np.empty(nxr, dtype=np.float32)
+        # float32 element-wise assignment like the SepVector ndarray writes
+        zc[:] = oz + ozr * dz + 0 * dz * irec
+        xc[:] = ox + oxr * dx + dxr * dx * irec
+    grids = _four_grids(zc, xc, hypers, nts, method, nfilt, dipole, zds, xds)
+    return [grids[0]], [grids[1]], [grids[2]], [grids[3]], receiverAxis

@@ -1,0 +1,213 @@
+/*
+ * eio_b200.h -- C ABI of the B200 (sm_100a) 2-D isotropic elastic
+ * velocity-stress staggered-grid finite-difference engine.
+ *
+ * This is the drop-in boundary for the reference's elastic propagation path
+ * (biondiettore/elastic_isotropic_operators).  Paths in the citations are
+ * relative to that project:
+ *   F  = elastic_iso_lib/elastic_iso_float/prop
+ *   PF = elastic_iso_lib/python/python_float
+ *
+ * Conventions
+ *   - Every function returns an int status: EIO_OK (0) or a negative error
+ *     code; eio_last_error() returns the message of the last failure on the
+ *     calling thread.  Nothing here calls exit() (the reference's cudaErrors.cu
+ *     does); QC failures that the reference reports with std::runtime_error
+ *     ("" + stderr message) come back as EIO_ERR_QC with the same message.
+ *   - Arrays use the reference layouts, z fastest:
+ *       elastic parameters  [3][nx][nz]   (rho, lambda, mu)
+ *       wavefield fields    [nx][nz]      (vx, vz, sigmaxx, sigmazz, sigmaxz)
+ *       regular-grid traces [nPoints][nt] (time fastest)
+ *     Field order is always vx, vz, sigmaxx, sigmazz, sigmaxz.  Position
+ *     lists come in grid order center (sigmaxx, sigmazz), x-shifted (vx),
+ *     z-shifted (vz), xz-shifted (sigmaxz).
+ *   - Host-pointer entry points copy in and out themselves; *_dev entry points
+ *     take device pointers (plus host position lists) and run on the
+ *     context's stream; every entry point synchronizes that stream before
+ *     it returns.
+ *   - A context is bound to one GPU and is not re-entrant (like the
+ *     reference operator objects); different contexts may be used from
+ *     different host threads.
+ */
+#ifndef EIO_B200_H
+#define EIO_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EIO_OK 0
+#define EIO_ERR_ARG -1     /* invalid argument / inconsistent sizes */
+#define EIO_ERR_QC -2      /* finite-difference QC failed (stability, dispersion, size) */
+#define EIO_ERR_CUDA -3    /* CUDA runtime error (message has the CUDA error string) */
+#define EIO_ERR_BOUNDS -4  /* acquisition device outside the usable grid */
+#define EIO_ERR_UNSUPPORTED -5
+#define EIO_ERR_NOMEM -6
+
+typedef struct eio_sinterp eio_sinterp;
+typedef struct eio_ctx eio_ctx;
+
+/* Finite-difference parameters: the par-file keys read by
+ * fdParamElastic::fdParamElastic (F/src/fdParamElastic.cpp:12-77). */
+typedef struct eio_fd_params {
+    int nts;            /* coarse (data) time samples */
+    float dts;          /* coarse sampling [s] */
+    float ots;
+    int sub;            /* par-file sub; doubled internally (fdParamElastic.cpp:28) */
+    int nz, nx;         /* total grid incl. padding and FAT */
+    float oz, ox;       /* origin of the padded grid */
+    float dz, dx;
+    int zPadMinus, zPadPlus, xPadMinus, xPadPlus;
+    float fMax;         /* default 1000 */
+    int blockSize;      /* must be 16 (reference constraint) */
+    int fat;            /* must be 4 */
+    float alphaCos;     /* default 0.99 */
+    int surfaceCondition; /* 0 only */
+    int mod_par;        /* 1: metres (default), 2: km in the par file */
+    float errorTolerance; /* default 1e-6 */
+} eio_fd_params;
+
+/* Fills p with the reference defaults (fMax 1000, blockSize 16, fat 4,
+ * alphaCos 0.99, surfaceCondition 0, mod_par 1, errorTolerance 1e-6). */
+void eio_fd_params_default(eio_fd_params *p);
+
+const char *eio_last_error(void);
+int eio_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Spatial interpolation of acquisition devices (spaceInterpGpu)
+ * replaces spaceInterpGpu::spaceInterpGpu / forward / adjoint / getRegPosUnique
+ * (F/src/spaceInterpGpu.cpp:11-362; pybind PF/pyElastic_iso_float_nl.cpp:19-30)
+ * method: "linear" (bilinear 2x2; nFilt forced to 1), "sinc" (normalised
+ * (2 nFilt)^2 sinc stencil; equals the reference exactly for nFilt = 1),
+ * "gauss".  dipole = 1 is supported for "linear" only, as in the reference.
+ * ------------------------------------------------------------------------ */
+int eio_sinterp_create(const float *zCoord, const float *xCoord, int nDevice,
+                       int nz, float oz, float dz, int nx, float ox, float dx,
+                       int nt, const char *method, int nFilt, int dipole,
+                       float zDipoleShift, float xDipoleShift, eio_sinterp **out);
+void eio_sinterp_destroy(eio_sinterp *s);
+/* nIrreg devices, nReg unique regular grid points, nFiltTotal points per device */
+int eio_sinterp_sizes(const eio_sinterp *s, int *nIrreg, int *nReg, int *nFiltTotal);
+int eio_sinterp_positions(const eio_sinterp *s, int *regPos /* [nReg] */);
+int eio_sinterp_weights(const eio_sinterp *s, int *gridPointIndex, float *weight /* [nIrreg*nFiltTotal] */);
+/* forward: regular [nReg][nt] -> irregular [nIrreg][nt]; adjoint: the transpose */
+int eio_sinterp_forward(const eio_sinterp *s, int add, const float *signalReg, float *signalIrreg);
+int eio_sinterp_adjoint(const eio_sinterp *s, int add, float *signalReg, const float *signalIrreg);
+
+/* ---------------------------------------------------------------------------
+ * Medium preparation + QC (fdParamElastic), host only
+ * replaces fdParamElastic::fdParamElastic (F/src/fdParamElastic.cpp:12-157)
+ * outputs the five scaled staggered coefficient grids [nx][nz]:
+ * rhoxDtw, rhozDtw, lamb2MuDtw, lambDtw, muxzDtw
+ * ------------------------------------------------------------------------ */
+int eio_medium_prepare(const eio_fd_params *p, const float *elasticParam,
+                       float *rhoxDtw, float *rhozDtw, float *lamb2MuDtw, float *lambDtw, float *muxzDtw);
+
+/* Staggering operators (staggerX / staggerZ, F/src/stagger.cpp:18-114), [nx][nz] */
+int eio_stagger(int axis /*0 = x, 1 = z*/, int adj, int add, int nz, int nx, float *model, float *data);
+
+/* Linear coarse<->fine time interpolation (interpTimeLinTbb, F/src/interpTimeLinTbb.cpp:26-102)
+ * sub_internal = 2*sub.  fwd: coarse [nDev][nts] -> fine [nDev][ntw] */
+int eio_time_interp(int adj, int add, int nts, float dts, float ots, int sub_internal, int nDev,
+                    float *coarse, float *fine);
+
+/* ---------------------------------------------------------------------------
+ * Device context = fdParamElastic + init/allocate on one GPU
+ * replaces initNonlinearElasticGpu + allocateNonlinearElasticGpu and
+ * initBornGpu + allocateBornElasticGpu
+ * (F/src/nonlinearPropElasticGpuFunctions.cu:85-264,
+ *  F/src/BornElasticGpuFunctions.cu:88-338), plus the QC of fdParamElastic.
+ * ------------------------------------------------------------------------ */
+int eio_ctx_create(const eio_fd_params *p, const float *elasticParam, int device, eio_ctx **out);
+/* setBackground: rebuild the medium (QC may fail) (PF/pyElastic_iso_float_nl.cpp:48) */
+int eio_ctx_set_background(eio_ctx *c, const float *elasticParam);
+void eio_ctx_destroy(eio_ctx *c);
+/* Source-wavefield snapshot storage for the Born operators:
+ * 0 = FP32 (bit-faithful to the reference), 1 = BF16, 2 = FP16 (both scaled per snapshot). */
+int eio_ctx_set_checkpoint_precision(eio_ctx *c, int mode);
+/* Scaled coefficient grids of the context (for inspection / tests). */
+int eio_ctx_get_medium(const eio_ctx *c, float *rhoxDtw, float *rhozDtw, float *lamb2MuDtw,
+                       float *lambDtw, float *muxzDtw);
+/* Fine time steps and updated cells of one propagation (for throughput accounting). */
+int eio_ctx_counts(const eio_ctx *c, long long *fineSteps, long long *cellsPerStep);
+/* CUDA stream of the context (cudaStream_t as void*). */
+void *eio_ctx_stream(eio_ctx *c);
+/* Instrumentation (no reference counterpart): kernel launch counters and,
+ * when enabled, CUDA-event timing of every fused step-kernel launch.
+ * enable: 1 on, 0 off, -1 unchanged; reset: zero the counters after reading. */
+int eio_ctx_stats(eio_ctx *c, int enable, int reset, long long *launches, long long *stepLaunches,
+                  double *stepMs);
+
+/* ---------------------------------------------------------------------------
+ * Single-shot propagation on the regular grid
+ * replaces propShotsElasticFwdGpu / propShotsElasticAdjGpu
+ * (F/src/nonlinearPropElasticGpuFunctions.cu:561-648, 932-1027) and
+ * BornShotsFwdGpu / BornShotsAdjGpu (F/src/BornElasticGpuFunctions.cu:719-1454).
+ * model: 5 source traces [nSrcReg(grid)][nts]; data: 5 receiver traces [nRecReg(grid)][nts]
+ * srcPos / recPos: 4 position lists (center, x, z, xz) with counts.
+ *   nl_fwd overwrites data; nl_adj overwrites model.
+ *   born_fwd: srcDtw = 5 fine-time source traces [nSrcReg][ntw] (already scaled),
+ *             dm = 5 staggered+scaled perturbations [nx][nz]; overwrites data.
+ *   born_adj: ACCUMULATES into dm (the reference copies dm in and back).
+ * ------------------------------------------------------------------------ */
+int eio_nl_fwd_reg(eio_ctx *c, float *const model[5], float *const data[5],
+                   const int *const srcPos[4], const int nSrc[4], const int *const recPos[4], const int nRec[4]);
+int eio_nl_adj_reg(eio_ctx *c, float *const model[5], float *const data[5],
+                   const int *const srcPos[4], const int nSrc[4], const int *const recPos[4], const int nRec[4]);
+int eio_born_fwd_reg(eio_ctx *c, float *const srcDtw[5], float *const dm[5], float *const data[5],
+                     const int *const srcPos[4], const int nSrc[4], const int *const recPos[4], const int nRec[4]);
+int eio_born_adj_reg(eio_ctx *c, float *const srcDtw[5], float *const dm[5], float *const data[5],
+                     const int *const srcPos[4], const int nSrc[4], const int *const recPos[4], const int nRec[4]);
+/* Same, with every float array a DEVICE pointer on the context's GPU
+ * (positions stay host arrays). */
+int eio_nl_fwd_reg_dev(eio_ctx *c, float *const model[5], float *const data[5],
+                       const int *const srcPos[4], const int nSrc[4], const int *const recPos[4], const int nRec[4]);
+int eio_nl_adj_reg_dev(eio_ctx *c, float *const model[5], float *const data[5],
+                       const int *const srcPos[4], const int nSrc[4], const int *const recPos[4], const int nRec[4]);
+int eio_born_fwd_reg_dev(eio_ctx *c, float *const srcDtw[5], float *const dm[5], float *const data[5],
+                         const int *const srcPos[4], const int nSrc[4], const int *const recPos[4], const int nRec[4]);
+int eio_born_adj_reg_dev(eio_ctx *c, float *const srcDtw[5], float *const dm[5], float *const data[5],
+                         const int *const srcPos[4], const int nSrc[4], const int *const recPos[4], const int nRec[4]);
+
+/* ---------------------------------------------------------------------------
+ * Multi-shot operators (the pybind11 targets)
+ * replace nonlinearPropElasticShotsGpu::forward/adjoint
+ * (F/src/nonlinearPropElasticShotsGpu.cpp:80-183, 304-422; pybind
+ * PF/pyElastic_iso_float_nl.cpp:32-54) and BornElasticShotsGpu::forward/adjoint
+ * (F/src/BornElasticShotsGpu.cpp:85-378; pybind PF/pyElastic_iso_float_born.cpp:19-36).
+ *
+ * Geometry: src[4*nExp] = the four spaceInterp objects of each shot in grid
+ * order (center, x, z, xz); rec[4*nRecGeom] likewise with nRecGeom = 1
+ * (constant receivers) or nExp.
+ * NL model  [nModelExp][5][nSrcIrreg][nts] (nModelExp = 1: same signal for all shots)
+ * NL data   [nExp][5][nRecIrreg][nts]
+ * Born model [3][nx][nz] (drho, dlambda, dmu); Born data like NL data;
+ * Born source signals: nSignals (1 or nExp) arrays [5][nSrcIrreg][nts].
+ * add = 0 zeroes the output first, add = 1 accumulates (reference semantics).
+ * ------------------------------------------------------------------------ */
+int eio_nl_forward(eio_ctx *c, int add, int nExp, int nModelExp, const float *model, float *data,
+                   eio_sinterp *const *src, eio_sinterp *const *rec, int nRecGeom);
+int eio_nl_adjoint(eio_ctx *c, int add, int nExp, int nModelExp, float *model, const float *data,
+                   eio_sinterp *const *src, eio_sinterp *const *rec, int nRecGeom);
+int eio_born_forward(eio_ctx *c, int add, int nExp, const float *model, float *data,
+                     const float *const *srcSignals, int nSignals,
+                     eio_sinterp *const *src, eio_sinterp *const *rec, int nRecGeom);
+int eio_born_adjoint(eio_ctx *c, int add, int nExp, float *model, const float *data,
+                     const float *const *srcSignals, int nSignals,
+                     eio_sinterp *const *src, eio_sinterp *const *rec, int nRecGeom);
+
+/* Born host preparation of one shot, exposed so that callers can keep the
+ * single-shot *_dev entry points fed from device memory:
+ * - sources: seismicElasticOperator2D::setSources, Born branch
+ *   (F/include/seismicElasticOperator2D.cpp:27-117): irregular signal
+ *   [5][nSrcIrreg][nts] -> 5 scaled regular fine-time traces [nSrcReg(grid)][ntw];
+ * - model: staggering and scaling of (drho, dlambda, dmu) [3][nx][nz] into the
+ *   5 perturbation grids [nx][nz] (F/src/BornElasticShotsGpu.cpp:107-150). */
+int eio_born_prepare_sources(eio_ctx *c, const float *signal, eio_sinterp *const src[4], float *const out[5]);
+int eio_born_prepare_model(eio_ctx *c, const float *model, float *const out[5]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EIO_B200_H */

@@ -1,0 +1,227 @@
+"""Parity of the sm_100a engine (through the C ABI) with the CPU oracle and with
+the reference's own CUDA drivers (oracle/_ref), plus adjointness.
+
+Tolerances (relative L2 over the whole output):
+  FP32 engine vs FP32 oracle / reference float build   <= 1e-5
+  FP32 engine vs FP64 oracle (elastic_iso_double)       <= 1e-4 (nonlinear), 1e-4 (Born)
+  dot-product tests (FP64 reductions)                    <= 1e-5
+  reference float build vs FP32 oracle                   <= 1e-5
+  reference double build vs FP64 oracle                  <= 1e-10
+"""
+import numpy as np
+import pytest
+
+from elastic_isotropic_operators_b200 import prop, synthetic
+from oracle import oracle as O
+
+from helpers import Ctx, reg_inputs, rel
+
+pytestmark = pytest.mark.gpu
+
+TOL32 = 1e-5
+TOL64 = 1e-4
+
+
+@pytest.fixture(scope="module")
+def w():
+    return synthetic.small()
+
+
+@pytest.fixture(scope="module")
+def ctx(w):
+    c = Ctx(w)
+    yield c
+    c.close()
+
+
+def _copy(xs):
+    return [x.copy() for x in xs]
+
+
+@pytest.mark.parametrize("adj", [0, 1])
+def test_nl_reg_vs_oracle(w, ctx, adj):
+    for prec, tol in (("f", TOL32), ("d", TOL64)):
+        r = reg_inputs(w, prec)
+        orc = r["orc"]
+        m, d = _copy(r["model"]), _copy(r["data"])
+        orc.nl_prop(adj, r["g"], r["med"], m, d, r["sp"], r["rp"])
+        pm, pd = ctx.nl(adj, r["model"], r["data"], r["sp"], r["rp"])
+        got, want = (pm, m) if adj else (pd, d)
+        assert rel(got, want) < tol, (prec, rel(got, want))
+
+
+@pytest.mark.parametrize("adj", [0, 1])
+def test_born_reg_vs_oracle(w, ctx, adj):
+    for prec, tol in (("f", TOL32), ("d", TOL64)):
+        r = reg_inputs(w, prec)
+        orc = r["orc"]
+        dm, d = _copy(r["dm"]), _copy(r["data"])
+        orc.born_prop(adj, r["g"], r["med"], r["fine"], dm, d, r["sp"], r["rp"])
+        pdm, pd = ctx.born(adj, r["fine"], r["dm"], r["data"], r["sp"], r["rp"])
+        got, want = (pdm, dm) if adj else (pd, d)
+        assert rel(got, want) < tol, (prec, rel(got, want))
+
+
+def _ops(w, nModelExp=1, per_shot_rec=False, method="linear", nfilt=1):
+    src, rec = w.geometry(method, nfilt)
+    if per_shot_rec:
+        rec = [g * w.nExp for g in rec]
+    nl = prop.nonlinearPropElasticShotsGpu(w.elastic, w.par, *src, *rec)
+    return nl, src, rec
+
+
+def test_nl_operator_vs_oracle(w):
+    nl, src, rec = _ops(w)
+    c = O.Case.from_workload(w)
+    model = nl.modelSpace()
+    model.getNdArray()[...] = w.source_signal()[None]
+    data = nl.dataSpace()
+    nl.forward(False, model, data)
+    want = O.nl_forward(O.Oracle("f"), c, model.getNdArray())
+    assert O.rel_l2(data.getNdArray(), want) < TOL32
+    want64 = O.nl_forward(O.Oracle("d"), c, model.getNdArray())
+    assert O.rel_l2(data.getNdArray(), want64) < TOL64
+    # add = True accumulates
+    d0 = data.getNdArray().copy()
+    nl.forward(True, model, data)
+    assert O.rel_l2(data.getNdArray(), 2 * d0) < 1e-6
+    # adjoint, constant source signal: shots are stacked
+    rng = np.random.default_rng(8)
+    dd = nl.dataSpace()
+    dd.getNdArray()[...] = rng.standard_normal(dd.getNdArray().shape)
+    m2 = nl.modelSpace()
+    nl.adjoint(False, m2, dd)
+    want = O.nl_adjoint(O.Oracle("f"), c, dd.getNdArray(), 1)
+    assert O.rel_l2(m2.getNdArray(), want) < TOL32
+
+
+def test_nl_operator_per_shot_signals_and_receivers(w):
+    nl, src, rec = _ops(w, per_shot_rec=True)
+    c = O.Case.from_workload(w)
+    rng = np.random.default_rng(9)
+    model = nl.modelSpace(nModelExp=w.nExp)
+    model.getNdArray()[...] = rng.standard_normal(model.getNdArray().shape)
+    data = nl.dataSpace()
+    nl.forward(False, model, data)
+    want = O.nl_forward(O.Oracle("f"), c, model.getNdArray())
+    assert O.rel_l2(data.getNdArray(), want) < TOL32
+    m2 = nl.modelSpace(nModelExp=w.nExp)
+    nl.adjoint(False, m2, data)
+    want = O.nl_adjoint(O.Oracle("f"), c, data.getNdArray(), w.nExp)
+    assert O.rel_l2(m2.getNdArray(), want) < TOL32
+
+
+def test_nl_operator_sinc_geometry(w):
+    nl, src, rec = _ops(w, method="sinc", nfilt=1)
+    c = O.Case.from_workload(w, "sinc", 1)
+    model = nl.modelSpace()
+    model.getNdArray()[...] = w.source_signal()[None]
+    data = nl.dataSpace()
+    nl.forward(False, model, data)
+    assert O.rel_l2(data.getNdArray(), O.nl_forward(O.Oracle("f"), c, model.getNdArray())) < TOL32
+
+
+def test_born_operator_vs_oracle(w):
+    src, rec = w.geometry()
+    sig = [w.source_signal()]
+    born = prop.BornElasticShotsGpu(w.elastic, w.par, sig, *src, *rec)
+    c = O.Case.from_workload(w)
+    dm = born.modelSpace()
+    dm.getNdArray()[...] = w.extra["dmodel"]
+    data = born.dataSpace()
+    born.forward(False, dm, data)
+    assert O.rel_l2(data.getNdArray(), O.born_forward(O.Oracle("f"), c, dm.getNdArray(), sig)) < TOL32
+    assert O.rel_l2(data.getNdArray(), O.born_forward(O.Oracle("d"), c, dm.getNdArray(), sig)) < TOL64
+    g = born.modelSpace()
+    born.adjoint(False, g, data)
+    want = O.born_adjoint(O.Oracle("f"), c, data.getNdArray(), sig)
+    assert O.rel_l2(g.getNdArray(), want) < TOL32
+    want64 = O.born_adjoint(O.Oracle("d"), c, data.getNdArray(), sig)
+    assert O.rel_l2(g.getNdArray(), want64) < TOL64
+
+
+def test_dot_products(w):
+    nl, src, rec = _ops(w)
+    assert nl.dotTest(False, 1e-5), nl.lastDotTest
+    born = prop.BornElasticShotsGpu(w.elastic, w.par, [w.source_signal()], *src, *rec)
+    assert born.dotTest(False, 1e-5), born.lastDotTest
+
+
+def test_set_background(w):
+    nl, src, rec = _ops(w)
+    ep2 = w.elastic.clone()
+    ep2.getNdArray()[0] *= 1.1
+    nl.setBackground(ep2)
+    model = nl.modelSpace()
+    model.getNdArray()[...] = w.source_signal()[None]
+    data = nl.dataSpace()
+    nl.forward(False, model, data)
+    c = O.Case(ep2.getNdArray(), w.par.as_dict(), w.oz, w.ox, O.Case.from_workload(w).src, (w.rec_z, w.rec_x))
+    assert O.rel_l2(data.getNdArray(), O.nl_forward(O.Oracle("f"), c, model.getNdArray())) < TOL32
+    bad = w.elastic.clone()
+    bad.getNdArray()[1] *= 100.0     # Courant violation
+    with pytest.raises(prop.EioError):
+        nl.setBackground(bad)
+
+
+def test_out_of_interior_point_rejected(w, ctx):
+    r = reg_inputs(w, "f")
+    sp = [p.copy() for p in r["sp"]]
+    sp[0][0] = 1     # inside the FAT frame
+    with pytest.raises(prop.EioError):
+        ctx.nl(0, r["model"], r["data"], sp, r["rp"])
+
+
+# ------------------------------------------------------------------ reference's own CUDA build
+ref_available = O.RefGpu.available("f") and O.RefGpu.available("d")
+
+
+@pytest.mark.skipif(not ref_available, reason="oracle/_ref not built")
+@pytest.mark.parametrize("kind", ["nl_fwd", "nl_adj", "born_fwd", "born_adj"])
+def test_reference_gpu_pins_oracle_and_engine(w, ctx, kind):
+    adj = int(kind.endswith("adj"))
+    for prec, tol in (("f", TOL32), ("d", 1e-10)):
+        r = reg_inputs(w, prec)
+        orc, refg = r["orc"], O.RefGpu(prec)
+        if kind.startswith("nl"):
+            mo, do = _copy(r["model"]), _copy(r["data"])
+            orc.nl_prop(adj, r["g"], r["med"], mo, do, r["sp"], r["rp"])
+            mr, dr = _copy(r["model"]), _copy(r["data"])
+            refg.nl_prop(adj, r["g"], r["med"], mr, dr, r["sp"], r["rp"])
+            want, got_ref = (mo, mr) if adj else (do, dr)
+            if prec == "f":
+                pm, pd = ctx.nl(adj, r["model"], r["data"], r["sp"], r["rp"])
+                assert rel(pm if adj else pd, got_ref) < TOL32
+        else:
+            dmo, do = _copy(r["dm"]), _copy(r["data"])
+            orc.born_prop(adj, r["g"], r["med"], r["fine"], dmo, do, r["sp"], r["rp"])
+            dmr, dr = _copy(r["dm"]), _copy(r["data"])
+            refg.born_prop(adj, r["g"], r["med"], r["fine"], dmr, dr, r["sp"], r["rp"])
+            want, got_ref = (dmo, dmr) if adj else (do, dr)
+            if prec == "f":
+                pdm, pd = ctx.born(adj, r["fine"], r["dm"], r["data"], r["sp"], r["rp"])
+                assert rel(pdm if adj else pd, got_ref) < TOL32
+        assert rel(got_ref, want) < tol, (prec, kind, rel(got_ref, want))
+
+
+# ------------------------------------------------------------------ full-size properties
+def test_full_size_nl_312x520_vs_oracle():
+    """The nonlinear benchmark case at full size (312x520, 3998 fine steps)."""
+    w = synthetic.nl_312x520()
+    src, rec = w.geometry()
+    nl = prop.nonlinearPropElasticShotsGpu(w.elastic, w.par, *src, *rec)
+    model = nl.modelSpace()
+    model.getNdArray()[...] = w.source_signal()[None]
+    data = nl.dataSpace()
+    nl.forward(False, model, data)
+    want = O.nl_forward(O.Oracle("f"), O.Case.from_workload(w), model.getNdArray())
+    assert O.rel_l2(data.getNdArray(), want) < TOL32
+    assert np.abs(data.getNdArray()).max() > 0
+
+
+def test_full_size_born_600x1800_dot_product():
+    """Born adjointness on the 600x1800, nts=4000 benchmark grid (one shot)."""
+    w = synthetic.born_600x1800(nshots=1)
+    src, rec = w.geometry()
+    born = prop.BornElasticShotsGpu(w.elastic, w.par, [w.source_signal()], *src, *rec)
+    assert born.dotTest(False, 1e-5), born.lastDotTest
