@@ -73,6 +73,9 @@ _SIGS = {
     "eio_ctx_get_medium": (I, [P, FP, FP, FP, FP, FP]),
     "eio_ctx_counts": (I, [P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     "eio_ctx_stream": (P, [P]),
+    "eio_ctx_set_kernel": (I, [P, I, I, I, I]),
+    "eio_ctx_get_kernel": (I, [P, IP, IP, IP, IP]),
+    "eio_ctx_autotune": (I, [P, IP, IP, IP, IP]),
     "eio_ctx_stats": (I, [P, I, I, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
                           ctypes.POINTER(ctypes.c_double)]),
     "eio_nl_fwd_reg": (I, [P, P, P, P, IP, P, IP]),

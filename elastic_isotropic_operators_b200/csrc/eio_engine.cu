@@ -13,8 +13,11 @@
 #include <string>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "eio_internal.h"
 #include "eio_kernels.cuh"
+#include "eio_sweep.cuh"
 
 namespace eio {
 
@@ -75,6 +78,15 @@ struct Engine {
     DBuf sig_in[5], sig_out[5];
     DBuf stage_a[5], stage_b[5], stage_c[5];
     DBuf W, ss[10];
+    // step-kernel choice: kind 0 = shared-memory tile kernel (k_step),
+    // kind 1 = TMA x-sweep (k_sweep) with strip height tz, chunk width cw and
+    // cpr chunks per CTA
+    int kind = 1, tz = 64, cw = 8, cpr = 8;
+    bool tuned = false;
+    // tensor maps of the sweep kernel (valid for mtz/mcw)
+    int mtz = -1, mcw = -1;
+    CUtensorMap mwf_halo[10], mwf_int[10], mpar_halo[5], mpar_int[5];
+    DBuf err;
     // launch statistics (bench instrumentation)
     long long launches = 0, step_launches = 0;
     double step_ms = 0.0;
@@ -175,7 +187,7 @@ void engine_destroy(Engine* e) {
     if (!e) return;
     cudaSetDevice(e->device);
     if (e->st) cudaStreamSynchronize(e->st);
-    DBuf* all[] = {&e->dampz, &e->dampx, &e->inj_ts, &e->inj_ent, &e->ext_ts, &e->ext_ent, &e->W};
+    DBuf* all[] = {&e->dampz, &e->dampx, &e->inj_ts, &e->inj_ent, &e->ext_ts, &e->ext_ent, &e->W, &e->err};
     for (DBuf* b : all) b->release();
     for (int f = 0; f < 5; f++) {
         e->par[f].release(); e->sig_in[f].release(); e->sig_out[f].release();
@@ -203,8 +215,20 @@ void engine_stats(Engine* e, int enable, int reset, long long* launches, long lo
     if (enable >= 0) e->stats = enable != 0;
 }
 
+// tile geometry the sparse point lists are bucketed with
+struct TileGeom {
+    int tz, tx, ntz;
+};
+static TileGeom tile_geom(const Engine* e) {
+    if (e->kind == 0) return {TZ, TX, e->ntz};
+    return {e->tz, e->cw, (e->nz - 2 * FAT + e->tz - 1) / e->tz};
+}
+
 // Sort the points of the four position lists into per-tile buckets.
 static void build_points(const Engine* e, const int* const pos[4], const int npos[4], PointList& pl) {
+    const TileGeom tg = tile_geom(e);
+    const int nchunks = (e->nx - 2 * FAT) / tg.tx;
+    const int ntiles = tg.ntz * nchunks;
     std::vector<std::pair<int, PointEntry>> tmp;
     for (int f = 0; f < 5; f++) {
         const int g = kFieldGrid[f];
@@ -215,17 +239,18 @@ static void build_points(const Engine* e, const int* const pos[4], const int npo
             if (cell < 0 || ix < FAT || ix >= e->nx - FAT || iz < FAT || iz >= e->nz - FAT)
                 throw Error(EIO_ERR_BOUNDS, "acquisition point " + std::to_string(cell) +
                                                 " lies outside the updated interior of the grid");
-            const int bz = (iz - FAT) / TZ, bx = (ix - FAT) / TX;
+            const int bz = (iz - FAT) / tg.tz, bx = (ix - FAT) / tg.tx;
             PointEntry pe;
-            pe.key = (f << 16) | (((ix - FAT) % TX) << 8) | ((iz - FAT) % TZ);
+            pe.key = (f << 16) | (((ix - FAT) % tg.tx) << 8) | ((iz - FAT) % tg.tz);
             pe.col = k;
-            tmp.push_back({bx * e->ntz + bz, pe});
+            // k_step numbers tiles z-fastest, k_sweep strip-major
+            tmp.push_back({e->kind == 0 ? bx * tg.ntz + bz : bz * nchunks + bx, pe});
         }
     }
     pl.any = !tmp.empty();
-    pl.tile_start.assign(e->ntiles + 1, 0);
+    pl.tile_start.assign(ntiles + 1, 0);
     for (auto& t : tmp) pl.tile_start[t.first + 1]++;
-    for (int i = 0; i < e->ntiles; i++) pl.tile_start[i + 1] += pl.tile_start[i];
+    for (int i = 0; i < ntiles; i++) pl.tile_start[i + 1] += pl.tile_start[i];
     pl.ent.resize(tmp.size());
     std::vector<int> cur(pl.tile_start.begin(), pl.tile_start.end() - 1);
     for (auto& t : tmp) pl.ent[cur[t.first]++] = t.second;
@@ -267,13 +292,187 @@ static StepArgs base_args(Engine* e) {
     return a;
 }
 
+// ---------------------------------------------------------------- step launch
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        EIO_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (!p || q != cudaDriverEntryPointSuccess) throw Error(EIO_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 2-D map of one [nx][nz] float field (z innermost) with a box of bz rows x bx columns
+static CUtensorMap make_map(const float* base, int nz, int nx, int bz, int bx) {
+    CUtensorMap m;
+    cuuint64_t dims[2] = {(cuuint64_t)nz, (cuuint64_t)nx};
+    cuuint64_t strides[1] = {(cuuint64_t)nz * sizeof(float)};
+    cuuint32_t box[2] = {(cuuint32_t)bz, (cuuint32_t)bx};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, es,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(EIO_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return m;
+}
+
+static void ensure_maps(Engine* e) {
+    if (e->mtz == e->tz && e->mcw == e->cw) return;
+    for (int b = 0; b < 10; b++) {
+        e->mwf_halo[b] = make_map(e->wf[b].f(), e->nz, e->nx, e->tz + 2 * FAT, e->cw);
+        e->mwf_int[b] = make_map(e->wf[b].f(), e->nz, e->nx, e->tz, e->cw);
+    }
+    for (int f = 0; f < 5; f++) {
+        e->mpar_halo[f] = make_map(e->par[f].f(), e->nz, e->nx, e->tz + 2 * FAT, e->cw);
+        e->mpar_int[f] = make_map(e->par[f].f(), e->nz, e->nx, e->tz, e->cw);
+    }
+    e->mtz = e->tz;
+    e->mcw = e->cw;
+}
+
+template <int DIR, int EPI, int TZ, int CW>
+static void launch_sweep_t(Engine* e, const SweepArgs& s, int nblocks) {
+    using Ly = SweepLayout<TZ, CW, DIR>;
+    static bool attr = false;
+    if (!attr) {
+        EIO_CUDA(cudaFuncSetAttribute(k_sweep<DIR, EPI, TZ, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)Ly::BYTES));
+        attr = true;
+    }
+    k_sweep<DIR, EPI, TZ, CW><<<nblocks, Ly::NT, Ly::BYTES, e->st>>>(s);
+}
+
 template <int DIR, int EPI>
-static void launch_step(Engine* e, StepArgs& a) {
+static void launch_sweep(Engine* e, const StepArgs& a, int cur) {
+    ensure_maps(e);
+    SweepArgs s;
+    memset(&s, 0, sizeof(s));
+    const int oc = cur * 5, cc = (1 - cur) * 5;   // buffer of the old / current level
+    for (int f = 0; f < 5; f++) {
+        s.tc[f] = e->mwf_halo[cc + f];
+        s.to[f] = e->mwf_int[oc + f];
+        s.tp[f] = DIR == 0 ? e->mpar_int[f] : e->mpar_halo[f];
+        s.o[f] = a.o[f];
+        s.ssL[f] = a.ssL[f]; s.ssR[f] = a.ssR[f]; s.eL[f] = a.eL[f]; s.eR[f] = a.eR[f];
+    }
+    s.dampz = a.dampz; s.dampx = a.dampx;
+    s.nz = e->nz; s.nx = e->nx;
+    s.nstrips = (e->nz - 2 * FAT + e->tz - 1) / e->tz;
+    s.nchunks = (e->nx - 2 * FAT) / e->cw;
+    s.cpr = std::max(1, std::min(e->cpr, s.nchunks));
+    s.nranges = (s.nchunks + s.cpr - 1) / s.cpr;
+    for (int i = 0; i < 4; i++) { s.cz[i] = a.cz[i]; s.cx[i] = a.cx[i]; }
+    s.inj = a.inj; s.ext = a.ext;
+    // the sweep kernel buckets points per (strip, chunk): rebuilt by the caller
+    s.W0 = a.W0; s.W1 = a.W1; s.wstride = a.wstride; s.wt = a.wt; s.ww0 = a.ww0; s.ww1 = a.ww1;
+    s.sw0 = a.sw0; s.sw1 = a.sw1;
+    s.err = static_cast<int*>(e->err.p);
+    const int nb = s.nstrips * s.nranges;
+    if (e->tz == 64 && e->cw == 8) launch_sweep_t<DIR, EPI, 64, 8>(e, s, nb);
+    else if (e->tz == 64 && e->cw == 16) launch_sweep_t<DIR, EPI, 64, 16>(e, s, nb);
+    else if (e->tz == 128 && e->cw == 8) launch_sweep_t<DIR, EPI, 128, 8>(e, s, nb);
+    else throw Error(EIO_ERR_ARG, "unsupported sweep configuration");
+}
+
+template <int DIR, int EPI>
+static void launch_step(Engine* e, StepArgs& a, int cur) {
     stats_mark(e);
-    k_step<DIR, EPI><<<e->ntiles, NT, 0, e->st>>>(a);
+    if (e->kind == 0) k_step<DIR, EPI><<<e->ntiles, NT, 0, e->st>>>(a);
+    else launch_sweep<DIR, EPI>(e, a, cur);
     stats_mark(e);
     e->launches++;
     e->step_launches++;
+}
+
+// ---------------------------------------------------------------- autotuner
+struct KernelCfg {
+    int kind, tz, cw, cpr;
+};
+static const KernelCfg kCandidates[] = {
+    {0, TZ, TX, 0},
+    {1, 64, 8, 4}, {1, 64, 8, 8}, {1, 64, 8, 16}, {1, 64, 8, 32},
+    {1, 64, 16, 2}, {1, 64, 16, 4}, {1, 64, 16, 8},
+    {1, 128, 8, 4}, {1, 128, 8, 8}, {1, 128, 8, 16},
+};
+
+static bool cfg_valid(const Engine* e, const KernelCfg& c) {
+    if (c.kind == 0) return true;
+    return (e->nx - 2 * FAT) % c.cw == 0;
+}
+
+void engine_set_kernel(Engine* e, int kind, int tz, int cw, int cpr) {
+    KernelCfg c{kind, tz, cw, cpr};
+    bool known = false;
+    for (const KernelCfg& k : kCandidates)
+        if (k.kind == c.kind && (c.kind == 0 || (k.tz == c.tz && k.cw == c.cw))) known = true;
+    if (!known || !cfg_valid(e, c) || (kind == 1 && cpr < 1)) throw Error(EIO_ERR_ARG, "unsupported kernel configuration");
+    e->kind = kind;
+    if (kind == 1) { e->tz = tz; e->cw = cw; e->cpr = cpr; }
+    e->tuned = true;
+}
+
+void engine_get_kernel(const Engine* e, int* kind, int* tz, int* cw, int* cpr) {
+    if (kind) *kind = e->kind;
+    if (tz) *tz = e->kind ? e->tz : TZ;
+    if (cw) *cw = e->kind ? e->cw : TX;
+    if (cpr) *cpr = e->kind ? e->cpr : 0;
+}
+
+static void zero_wavefields(Engine* e);
+
+// Times every candidate on a few forward and adjoint fine steps of this grid
+// (no sparse points; the step cost does not depend on the field values) and
+// keeps the fastest.
+void engine_autotune(Engine* e) {
+    EIO_CUDA(cudaSetDevice(e->device));
+    const bool stats = e->stats;
+    e->stats = false;
+    zero_wavefields(e);
+    e->err.ensure(16);
+    EIO_CUDA(cudaMemsetAsync(e->err.p, 0, sizeof(int), e->st));
+    StepArgs a = base_args(e);
+    cudaEvent_t t0, t1;
+    EIO_CUDA(cudaEventCreate(&t0));
+    EIO_CUDA(cudaEventCreate(&t1));
+    float best = 1e30f;
+    KernelCfg bestc = kCandidates[0];
+    for (const KernelCfg& c : kCandidates) {
+        if (!cfg_valid(e, c)) continue;
+        e->kind = c.kind;
+        if (c.kind) { e->tz = c.tz; e->cw = c.cw; e->cpr = c.cpr; }
+        float tot = 0.f;
+        for (int dir = 0; dir < 2; dir++) {
+            int cur = 0;
+            const int reps = 12;
+            for (int r = 0; r < reps + 3; r++) {
+                if (r == 3) EIO_CUDA(cudaEventRecord(t0, e->st));
+                for (int f = 0; f < 5; f++) { a.o[f] = e->wf[cur * 5 + f].f(); a.c[f] = e->wf[(1 - cur) * 5 + f].f(); }
+                if (dir == 0) launch_step<0, EPI_NONE>(e, a, cur);
+                else launch_step<1, EPI_NONE>(e, a, cur);
+                cur ^= 1;
+            }
+            EIO_CUDA(cudaEventRecord(t1, e->st));
+            EIO_CUDA(cudaEventSynchronize(t1));
+            float ms = 0.f;
+            EIO_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+            tot += ms / reps;
+        }
+        if (tot < best) { best = tot; bestc = c; }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    e->launches = 0;
+    e->step_launches = 0;
+    e->kind = bestc.kind;
+    if (bestc.kind) { e->tz = bestc.tz; e->cw = bestc.cw; e->cpr = bestc.cpr; }
+    e->tuned = true;
+    e->stats = stats;
+    int flag = 0;
+    EIO_CUDA(cudaMemcpy(&flag, e->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) throw Error(EIO_ERR_CUDA, "a TMA pipeline wait timed out while tuning");
 }
 
 static void zero_wavefields(Engine* e) {
@@ -303,8 +502,20 @@ static void stage_out(Engine* e, const int ld[5], int nt, DBuf* src, float* cons
     for (int f = 0; f < 5; f++) transpose(e, src[f].f(), tr[f], nt, ld[f]);
 }
 
+static void err_reset(Engine* e) {
+    e->err.ensure(16);
+    EIO_CUDA(cudaMemsetAsync(e->err.p, 0, sizeof(int), e->st));
+}
+static void err_check(Engine* e) {
+    int flag = 0;
+    EIO_CUDA(cudaMemcpy(&flag, e->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) throw Error(EIO_ERR_CUDA, "a TMA pipeline wait timed out in the step kernel");
+}
+
 void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], const ShotGeom& g) {
     EIO_CUDA(cudaSetDevice(e->device));
+    if (!e->tuned) engine_autotune(e);
+    err_reset(e);
     PointList src, rec;
     build_points(e, g.srcPos, g.nSrc, src);
     build_points(e, g.recPos, g.nRec, rec);
@@ -312,6 +523,7 @@ void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], 
     zero_wavefields(e);
     float* p0[5]; float* p1[5];
     for (int f = 0; f < 5; f++) { p0[f] = e->wf[f].f(); p1[f] = e->wf[5 + f].f(); }
+    int cur = 0;   // buffer holding the old level (p0)
     const float* F = e->filt.data();
     const int h = e->h;
     if (!adj) {
@@ -324,8 +536,9 @@ void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], 
                 for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; }
                 a.inj.t0 = its; a.inj.w0 = F[it2 - 1]; a.inj.w1 = F[h + it2 - 1];
                 a.ext.t0 = its; a.ext.w0 = F[it2]; a.ext.w1 = F[h + it2];
-                launch_step<0, EPI_NONE>(e, a);
+                launch_step<0, EPI_NONE>(e, a, cur);
                 std::swap(p0, p1);
+                cur ^= 1;
             }
         check_launch();
         stage_out(e, rec.ld, e->nts, e->sig_out, data);
@@ -339,14 +552,16 @@ void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], 
                 for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; }
                 a.inj.t0 = its; a.inj.w0 = F[it2 + 1]; a.inj.w1 = F[h + it2 + 1];
                 a.ext.t0 = its; a.ext.w0 = F[it2]; a.ext.w1 = F[h + it2];
-                launch_step<1, EPI_NONE>(e, a);
+                launch_step<1, EPI_NONE>(e, a, cur);
                 std::swap(p0, p1);
+                cur ^= 1;
             }
         check_launch();
         stage_out(e, src.ld, e->nts, e->sig_out, model);
     }
     EIO_CUDA(cudaStreamSynchronize(e->st));
     stats_flush(e);
+    err_check(e);
 }
 
 static void launch_imaging(Engine* e, int adj, int its, float* const dm[5], float* const ss[5]) {
@@ -373,6 +588,7 @@ static void born_source(Engine* e, const PointList& src, StepArgs a) {
     zero_wavefields(e);
     float* p0[5]; float* p1[5];
     for (int f = 0; f < 5; f++) { p0[f] = e->wf[f].f(); p1[f] = e->wf[5 + f].f(); }
+    int cur = 0;
     a.inj = upload_points(e, src, e->inj_ts, e->inj_ent, e->sig_in);
     memset(&a.ext, 0, sizeof(a.ext));
     a.W0 = e->W.f();
@@ -384,8 +600,9 @@ static void born_source(Engine* e, const PointList& src, StepArgs a) {
             for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; }
             a.inj.t0 = itw - 1; a.inj.w0 = 1.f; a.inj.w1 = 0.f;
             a.wt = its; a.ww0 = F[it2]; a.ww1 = F[e->h + it2];
-            launch_step<0, EPI_SAVE_W>(e, a);
+            launch_step<0, EPI_SAVE_W>(e, a, cur);
             std::swap(p0, p1);
+            cur ^= 1;
         }
     check_launch();
 }
@@ -393,6 +610,8 @@ static void born_source(Engine* e, const PointList& src, StepArgs a) {
 void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5], float* const data[5],
                  const ShotGeom& g) {
     EIO_CUDA(cudaSetDevice(e->device));
+    if (!e->tuned) engine_autotune(e);
+    err_reset(e);
     if (e->ckpt != 0) throw Error(EIO_ERR_UNSUPPORTED, "checkpoint mode");
     PointList src, rec;
     build_points(e, g.srcPos, g.nSrc, src);
@@ -414,6 +633,7 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
         p0[f] = e->wf[f].f(); p1[f] = e->wf[5 + f].f();
         sL[f] = e->ss[f].f(); sR[f] = e->ss[5 + f].f();
     }
+    int cur = 0;
     StepArgs a = base;
     if (!adj) {
         zero_out(e, rec.ld, e->nts, e->sig_out);
@@ -425,8 +645,9 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
                 for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; a.ssL[f] = sL[f]; a.ssR[f] = sR[f]; }
                 a.sw0 = F[it2 - 1]; a.sw1 = F[h + it2 - 1];
                 a.ext.t0 = its; a.ext.w0 = F[it2]; a.ext.w1 = F[h + it2];
-                launch_step<0, EPI_INJ_SS>(e, a);
+                launch_step<0, EPI_INJ_SS>(e, a, cur);
                 std::swap(p0, p1);
+                cur ^= 1;
             }
             // the imaging kernel rewrites every interior cell of the right slice,
             // so the reference's memset of it (BornElasticGpuFunctions.cu:806-810) is not needed
@@ -442,8 +663,9 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
                 for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; a.eL[f] = sL[f]; a.eR[f] = sR[f]; }
                 a.inj.t0 = its; a.inj.w0 = F[it2 + 1]; a.inj.w1 = F[h + it2 + 1];
                 a.sw0 = F[it2]; a.sw1 = F[h + it2];
-                launch_step<1, EPI_EXT_SS>(e, a);
+                launch_step<1, EPI_EXT_SS>(e, a, cur);
                 std::swap(p0, p1);
+                cur ^= 1;
             }
             launch_imaging(e, 1, its + 1, dm, sR);
             std::swap(sL, sR);
@@ -454,6 +676,7 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
     }
     EIO_CUDA(cudaStreamSynchronize(e->st));
     stats_flush(e);
+    err_check(e);
 }
 
 // ---------------------------------------------------------------- host wrappers

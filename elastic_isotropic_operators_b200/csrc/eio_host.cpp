@@ -508,6 +508,25 @@ EIO_API int eio_ctx_counts(const eio_ctx* c, long long* fineSteps, long long* ce
     });
 }
 EIO_API void* eio_ctx_stream(eio_ctx* c) { return c ? engine_stream(c->eng) : nullptr; }
+EIO_API int eio_ctx_set_kernel(eio_ctx* c, int kind, int tz, int cw, int cpr) {
+    return guarded([&] {
+        if (!c) throw Error(EIO_ERR_ARG, "null context");
+        engine_set_kernel(c->eng, kind, tz, cw, cpr);
+    });
+}
+EIO_API int eio_ctx_autotune(eio_ctx* c, int* kind, int* tz, int* cw, int* cpr) {
+    return guarded([&] {
+        if (!c) throw Error(EIO_ERR_ARG, "null context");
+        engine_autotune(c->eng);
+        engine_get_kernel(c->eng, kind, tz, cw, cpr);
+    });
+}
+EIO_API int eio_ctx_get_kernel(const eio_ctx* c, int* kind, int* tz, int* cw, int* cpr) {
+    return guarded([&] {
+        if (!c) throw Error(EIO_ERR_ARG, "null context");
+        engine_get_kernel(c->eng, kind, tz, cw, cpr);
+    });
+}
 EIO_API int eio_ctx_stats(eio_ctx* c, int enable, int reset, long long* launches, long long* stepLaunches,
                           double* stepMs) {
     return guarded([&] {

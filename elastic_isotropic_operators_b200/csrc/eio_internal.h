@@ -60,6 +60,10 @@ Engine* engine_create(int device, const FdParam& fd);
 void engine_destroy(Engine* e);
 void engine_set_medium(Engine* e, const FdParam& fd);
 void engine_set_checkpoint(Engine* e, int mode);
+// step-kernel selection: kind 0 tile kernel, 1 TMA sweep (tz, cw, cpr); autotune times the candidates
+void engine_set_kernel(Engine* e, int kind, int tz, int cw, int cpr);
+void engine_get_kernel(const Engine* e, int* kind, int* tz, int* cw, int* cpr);
+void engine_autotune(Engine* e);
 void* engine_stream(Engine* e);
 // launch statistics: enable = 1/0 (-1 leaves it), reset = 1 zeroes the counters after reading
 void engine_stats(Engine* e, int enable, int reset, long long* launches, long long* step_launches, double* step_ms);

@@ -133,6 +133,14 @@ int eio_ctx_get_medium(const eio_ctx *c, float *rhoxDtw, float *rhozDtw, float *
 int eio_ctx_counts(const eio_ctx *c, long long *fineSteps, long long *cellsPerStep);
 /* CUDA stream of the context (cudaStream_t as void*). */
 void *eio_ctx_stream(eio_ctx *c);
+/* Step-kernel selection (no reference counterpart; the reference has one
+ * 16x16-tile kernel).  kind 0: shared-memory tile kernel; kind 1: TMA-pipelined
+ * x-sweep with strip height tz (64 or 128), chunk width cw (8 or 16) and cpr
+ * chunks per CTA.  By default the first propagation of a context times every
+ * candidate on its grid (eio_ctx_autotune) and keeps the fastest. */
+int eio_ctx_set_kernel(eio_ctx *c, int kind, int tz, int cw, int cpr);
+int eio_ctx_get_kernel(const eio_ctx *c, int *kind, int *tz, int *cw, int *cpr);
+int eio_ctx_autotune(eio_ctx *c, int *kind, int *tz, int *cw, int *cpr);
 /* Instrumentation (no reference counterpart): kernel launch counters and,
  * when enabled, CUDA-event timing of every fused step-kernel launch.
  * enable: 1 on, 0 off, -1 unchanged; reset: zero the counters after reading. */

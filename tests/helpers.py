@@ -41,6 +41,19 @@ class Ctx:
         _lib.check(self.L.eio_ctx_create(ctypes.byref(self.fd), _lib.fptr(ep), 0, ctypes.byref(h)))
         self.h = h
 
+    def set_kernel(self, kind, tz=64, cw=8, cpr=8):
+        _lib.check(self.L.eio_ctx_set_kernel(self.h, kind, tz, cw, cpr))
+
+    def get_kernel(self):
+        v = [ctypes.c_int() for _ in range(4)]
+        _lib.check(self.L.eio_ctx_get_kernel(self.h, *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    def autotune(self):
+        v = [ctypes.c_int() for _ in range(4)]
+        _lib.check(self.L.eio_ctx_autotune(self.h, *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
     def close(self):
         if self.h is not None:
             self.L.eio_ctx_destroy(self.h)

@@ -172,6 +172,44 @@ def test_out_of_interior_point_rejected(w, ctx):
         ctx.nl(0, r["model"], r["data"], sp, r["rp"])
 
 
+# ------------------------------------------------------------------ every step-kernel variant
+KERNELS = [(0, 64, 16, 0), (1, 64, 8, 4), (1, 64, 16, 2), (1, 128, 8, 3)]
+
+
+@pytest.mark.parametrize("cfg", KERNELS, ids=lambda c: "k%d_tz%d_cw%d_cpr%d" % c)
+def test_kernel_variants_vs_oracle(w, cfg):
+    c = Ctx(w)
+    try:
+        c.set_kernel(*cfg)
+        r = reg_inputs(w, "f", seed=5)
+        orc = r["orc"]
+        for adj in (0, 1):
+            m, d = _copy(r["model"]), _copy(r["data"])
+            orc.nl_prop(adj, r["g"], r["med"], m, d, r["sp"], r["rp"])
+            pm, pd = c.nl(adj, r["model"], r["data"], r["sp"], r["rp"])
+            assert rel(pm if adj else pd, m if adj else d) < TOL32, ("nl", adj)
+            dm, d = _copy(r["dm"]), _copy(r["data"])
+            orc.born_prop(adj, r["g"], r["med"], r["fine"], dm, d, r["sp"], r["rp"])
+            pdm, pd = c.born(adj, r["fine"], r["dm"], r["data"], r["sp"], r["rp"])
+            assert rel(pdm if adj else pd, dm if adj else d) < TOL32, ("born", adj)
+        assert c.get_kernel()[0] == cfg[0]
+    finally:
+        c.close()
+
+
+def test_autotune_picks_a_valid_kernel(w):
+    c = Ctx(w)
+    try:
+        kind, tz, cw, cpr = c.autotune()
+        assert kind in (0, 1)
+        if kind == 1:
+            assert tz in (64, 128) and cw in (8, 16) and cpr >= 1
+        with pytest.raises(prop.EioError):
+            c.set_kernel(1, 96, 8, 4)
+    finally:
+        c.close()
+
+
 # ------------------------------------------------------------------ reference's own CUDA build
 ref_available = O.RefGpu.available("f") and O.RefGpu.available("d")
 
