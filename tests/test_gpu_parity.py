@@ -173,7 +173,7 @@ def test_out_of_interior_point_rejected(w, ctx):
 
 
 # ------------------------------------------------------------------ every step-kernel variant
-KERNELS = [(0, 64, 16, 0), (1, 64, 8, 4), (1, 64, 16, 2), (1, 128, 8, 3)]
+KERNELS = [(0, 64, 16, 0), (1, 64, 8, 4), (1, 64, 8, 5), (1, 64, 16, 2), (1, 64, 16, 1), (1, 128, 8, 3)]
 
 
 @pytest.mark.parametrize("cfg", KERNELS, ids=lambda c: "k%d_tz%d_cw%d_cpr%d" % c)
