@@ -362,7 +362,7 @@ static void launch_sweep(Engine* e, const StepArgs& a, int cur) {
     s.nz = e->nz; s.nx = e->nx;
     s.nstrips = (e->nz - 2 * FAT + e->tz - 1) / e->tz;
     s.nchunks = (e->nx - 2 * FAT) / e->cw;
-    s.cpr = std::max(1, std::min(e->cpr, s.nchunks));
+    s.cpr = std::max(1, std::min(std::min(e->cpr, s.nchunks), SWEEP_MAXK));
     s.nranges = (s.nchunks + s.cpr - 1) / s.cpr;
     for (int i = 0; i < 4; i++) { s.cz[i] = a.cz[i]; s.cx[i] = a.cx[i]; }
     s.inj = a.inj; s.ext = a.ext;
@@ -408,7 +408,7 @@ void engine_set_kernel(Engine* e, int kind, int tz, int cw, int cpr) {
     bool known = false;
     for (const KernelCfg& k : kCandidates)
         if (k.kind == c.kind && (c.kind == 0 || (k.tz == c.tz && k.cw == c.cw))) known = true;
-    if (!known || !cfg_valid(e, c) || (kind == 1 && cpr < 1)) throw Error(EIO_ERR_ARG, "unsupported kernel configuration");
+    if (!known || !cfg_valid(e, c) || (kind == 1 && (cpr < 1 || cpr > SWEEP_MAXK))) throw Error(EIO_ERR_ARG, "unsupported kernel configuration");
     e->kind = kind;
     if (kind == 1) { e->tz = tz; e->cw = cw; e->cpr = cpr; }
     e->tuned = true;

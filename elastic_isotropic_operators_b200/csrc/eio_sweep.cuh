@@ -20,6 +20,7 @@
 namespace eio {
 
 constexpr long long WAIT_LIMIT = 1LL << 20;   // try_wait polls before an mbarrier wait gives up
+constexpr int SWEEP_MAXK = 64;                // chunks per CTA range (upper bound)
 
 struct SweepArgs {
     CUtensorMap tc[5];    // current level, box (TZ+8) x CW
@@ -93,7 +94,9 @@ struct SweepLayout {
     static constexpr int PROD = RAW + NRAWBUF * NRAWF * UNIT;            // adjoint product ring
     static constexpr int STAGE = PROD + (DIR == 0 ? 0 : RU * 5 * UNIT);
     static constexpr int SPARSE = STAGE + 2 * NSTGF * STG;
-    static constexpr int BAR = SPARSE + 5 * STG;                          // mbarriers (8 B each)
+    static constexpr int META = SPARSE + 5 * STG;                         // per-CTA metadata
+    static constexpr int META_F = 2 * (SWEEP_MAXK + 1) + SWEEP_MAXK * CW;  // 2 bucket offset lists + taper
+    static constexpr int BAR = META + ((META_F + 3) / 4) * 4;            // mbarriers (8 B each)
     static constexpr int NBAR = NRAWBUF + 2;
     static constexpr size_t BYTES = (size_t)BAR * 4 + NBAR * 8;
     static constexpr unsigned UNIT_TX = NRAWF * UNIT * 4;
@@ -110,6 +113,9 @@ __global__ void __launch_bounds__(SweepLayout<TZ, CW, DIR>::NT) k_sweep(const __
     float* prod = (DIR == 0) ? raw : sm + Ly::PROD;   // ring the stencils read
     float* stage = sm + Ly::STAGE;
     float* sparse = sm + Ly::SPARSE;
+    int* m_inj = reinterpret_cast<int*>(sm + Ly::META);          // [K+1] bucket offsets of my chunks
+    int* m_ext = m_inj + (SWEEP_MAXK + 1);
+    float* m_dx = sm + Ly::META + 2 * (SWEEP_MAXK + 1);          // [K*CW] taper along x
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(sm + Ly::BAR);
     unsigned long long* rbar = bar;                       // [NRAWBUF]
     unsigned long long* sbar = bar + Ly::NRAWBUF;         // [2]
@@ -129,6 +135,15 @@ __global__ void __launch_bounds__(SweepLayout<TZ, CW, DIR>::NT) k_sweep(const __
         for (int i = 0; i < Ly::NBAR; i++) mbar_init(bar + i, 1);
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // per-CTA metadata, read once instead of once per chunk on the critical path
+    {
+        const int tile0 = strip * a.nchunks + ck0;
+        for (int i = tid; i <= K; i += NT) {
+            m_inj[i] = a.inj.tile_start ? __ldg(a.inj.tile_start + tile0 + i) : 0;
+            m_ext[i] = a.ext.tile_start ? __ldg(a.ext.tile_start + tile0 + i) : 0;
+        }
+        for (int i = tid; i < K * CW; i += NT) m_dx[i] = __ldg(a.dampx + xb + i);
     }
     __syncthreads();
 
@@ -240,6 +255,15 @@ __global__ void __launch_bounds__(SweepLayout<TZ, CW, DIR>::NT) k_sweep(const __
 #pragma unroll
             for (int f = 0; f < 5; f++) { pre[f] = ldg4(a.ssL[f] + gi); pre[5 + f] = ldg4(a.ssR[f] + gi); }
         }
+        if (EPI == EPI_EXT_SS && valid) {
+#pragma unroll
+            for (int f = 0; f < 5; f++) { pre[f] = ld4(a.eL[f] + gi); pre[5 + f] = ld4(a.eR[f] + gi); }
+        }
+        if (EPI == EPI_SAVE_W && valid) {
+            const float* w0p = a.W0 + (long long)a.wt * a.wstride + gi;
+            const float* w1p = a.W1 + (long long)a.wt * a.wstride + gi;
+            pre[0] = ld4(w0p); pre[1] = ld4(w0p + a.wstride); pre[2] = ld4(w1p); pre[3] = ld4(w1p + a.wstride);
+        }
         if (DIR == 0) {
             if (!mbar_wait(rbar + ((k + 1) % RU), ((k + 1) / RU) & 1)) fail();
         }
@@ -312,7 +336,7 @@ __global__ void __launch_bounds__(SweepLayout<TZ, CW, DIR>::NT) k_sweep(const __
             }
         }
         // deferred taper of the old level + leapfrog sum (+ scattered-field source)
-        const float dxc = __ldg(a.dampx + gx);
+        const float dxc = m_dx[k * CW + jc];
         float dd[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) dd[j] = fminf(dz4[j], dxc);
@@ -328,10 +352,9 @@ __global__ void __launch_bounds__(SweepLayout<TZ, CW, DIR>::NT) k_sweep(const __
 #pragma unroll
                 for (int j = 0; j < 4; j++) at(t[f], j) += at(pre[f], j) * a.sw0 + at(pre[5 + f], j) * a.sw1;
         }
-        const int tile = strip * a.nchunks + ck0 + k;
         // sparse injection before the final taper
-        if (a.inj.tile_start) {
-            const int e0 = a.inj.tile_start[tile], e1 = a.inj.tile_start[tile + 1];
+        {
+            const int e0 = m_inj[k], e1 = m_inj[k + 1];
             if (e1 > e0) {
                 for (int i = tid; i < 5 * STG; i += NT) sparse[i] = 0.f;
                 __syncthreads();
@@ -364,7 +387,7 @@ __global__ void __launch_bounds__(SweepLayout<TZ, CW, DIR>::NT) k_sweep(const __
             if (EPI == EPI_SAVE_W) {
                 float* w0p = a.W0 + (long long)a.wt * a.wstride + gi;
                 float* w1p = a.W1 + (long long)a.wt * a.wstride + gi;
-                float4 p0 = ld4(w0p), p1 = ld4(w0p + a.wstride), q0 = ld4(w1p), q1 = ld4(w1p + a.wstride);
+                float4 p0 = pre[0], p1 = pre[1], q0 = pre[2], q1 = pre[3];
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     at(p0, j) += at(t[0], j) * a.ww0; at(p1, j) += at(t[0], j) * a.ww1;
@@ -375,7 +398,7 @@ __global__ void __launch_bounds__(SweepLayout<TZ, CW, DIR>::NT) k_sweep(const __
             if (EPI == EPI_EXT_SS) {
 #pragma unroll
                 for (int f = 0; f < 5; f++) {
-                    float4 l = ld4(a.eL[f] + gi), r = ld4(a.eR[f] + gi);
+                    float4 l = pre[f], r = pre[5 + f];
 #pragma unroll
                     for (int j = 0; j < 4; j++) { at(l, j) += at(t[f], j) * a.sw0; at(r, j) += at(t[f], j) * a.sw1; }
                     st4(a.eL[f] + gi, l); st4(a.eR[f] + gi, r);
@@ -383,8 +406,8 @@ __global__ void __launch_bounds__(SweepLayout<TZ, CW, DIR>::NT) k_sweep(const __
             }
         }
         // sparse extraction after the final taper
-        if (a.ext.tile_start) {
-            const int e0 = a.ext.tile_start[tile], e1 = a.ext.tile_start[tile + 1];
+        {
+            const int e0 = m_ext[k], e1 = m_ext[k + 1];
             if (e1 > e0) {
                 __syncthreads();
 #pragma unroll
