@@ -34,8 +34,8 @@ constexpr int FAT = 4;
 constexpr int TZ = 64;             // tile cells along z
 constexpr int TX = 16;             // tile cells along x
 constexpr int NTZ = TZ / 4;        // threads along z (one float4 each)
-constexpr int NTX = TX / 2;        // threads along x (two columns each)
-constexpr int NT = NTZ * NTX;      // 128 threads per CTA
+constexpr int NTX = TX;            // threads along x (one column each)
+constexpr int NT = NTZ * NTX;      // 256 threads per CTA
 constexpr int SZ = TZ + 2 * FAT;   // shared tile extent along z (72)
 constexpr int SX = TX + 2 * FAT;   // shared tile extent along x (24)
 constexpr int SMEM_FIELD = SX * SZ;
@@ -145,7 +145,7 @@ __device__ __forceinline__ void xwin(const float* s, int lx0, int lz, float4* q)
 
 // One fused fine time step.  DIR 0 = forward (ker_step_fwd), 1 = adjoint (ker_step_adj).
 template <int DIR, int EPI>
-__global__ void __launch_bounds__(NT) k_step(StepArgs a)
+__global__ void __launch_bounds__(NT, 3) k_step(StepArgs a)
 {
     __shared__ __align__(16) float sm[5 * SMEM_FIELD];
 
@@ -193,10 +193,12 @@ __global__ void __launch_bounds__(NT) k_step(StepArgs a)
 
     const int tzi = tid % NTZ, txi = tid / NTZ;
     const int lz = FAT + 4 * tzi;              // local z of my float4
-    const int lxa = FAT + 2 * txi;             // my two local columns: lxa, lxa+1
+    const int lx = FAT + txi;                  // my local column
     const int gz = z0 + 4 * tzi;
+    const int gx = x0 + txi;
     const bool valid = gz < nz - FAT;
-    float4 t[5][2];                            // new values before the final taper
+    const long long gi = (long long)gx * nz + gz;
+    float4 t[5];                               // new values before the final taper
 
     {
         const float* cz = a.cz;
@@ -206,97 +208,93 @@ __global__ void __launch_bounds__(NT) k_step(StepArgs a)
         const float* s2 = sm + 2 * SMEM_FIELD;
         const float* s3 = sm + 3 * SMEM_FIELD;
         const float* s4 = sm + 4 * SMEM_FIELD;
-        float4 q[10];
+        float4 q[9];
         float w[12];
+        auto xw = [&](const float* sf) {
+#pragma unroll
+            for (int m = 0; m < 9; m++) q[m] = ld4(sf + (lx - FAT + m) * SZ + lz);
+        };
         if (DIR == 0) {
-            // s0 vx, s1 vz, s2 sxx, s3 szz, s4 sxz
-            float4 dxsxx[2], dxsxz[2], dxvx[2], dxvz[2];
-            xwin(s2, lxa, lz, q); dxsxx[0] = dmx(q, 4, cx); dxsxx[1] = dmx(q, 5, cx);
-            xwin(s4, lxa, lz, q); dxsxz[0] = dpx(q, 4, cx); dxsxz[1] = dpx(q, 5, cx);
-            xwin(s0, lxa, lz, q); dxvx[0] = dpx(q, 4, cx); dxvx[1] = dpx(q, 5, cx);
-            xwin(s1, lxa, lz, q); dxvz[0] = dmx(q, 4, cx); dxvz[1] = dmx(q, 5, cx);
+            // s0 vx, s1 vz, s2 sxx, s3 szz, s4 sxz; one output field at a time keeps few registers live
+            xw(s2); float4 dx = dmx(q, 4, cx);
+            zwin(s4, lx, lz, w); float4 dz = dpz(w, cz);
+            if (valid) {
+                const float4 rx = ldg4(a.par[0] + gi);
 #pragma unroll
-            for (int k = 0; k < 2; k++) {
-                const int lx = lxa + k;
-                float4 dzsxz, dzszz, dzvx, dzvz;
-                zwin(s4, lx, lz, w); dzsxz = dpz(w, cz);
-                zwin(s3, lx, lz, w); dzszz = dmz(w, cz);
-                zwin(s0, lx, lz, w); dzvx = dmz(w, cz);
-                zwin(s1, lx, lz, w); dzvz = dpz(w, cz);
-                const long long gi = (long long)(x0 + 2 * txi + k) * nz + gz;
-                if (valid) {
-                    const float4 rx = ldg4(a.par[0] + gi), rz = ldg4(a.par[1] + gi), l2m = ldg4(a.par[2] + gi),
-                                 lam = ldg4(a.par[3] + gi), mu = ldg4(a.par[4] + gi);
+                for (int j = 0; j < 4; j++) at(t[0], j) = at(rx, j) * (at(dx, j) + at(dz, j));
+            }
+            zwin(s3, lx, lz, w); dz = dmz(w, cz);
+            xw(s4); dx = dpx(q, 4, cx);
+            if (valid) {
+                const float4 rz = ldg4(a.par[1] + gi);
 #pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        at(t[0][k], j) = at(rx, j) * (at(dxsxx[k], j) + at(dzsxz, j));
-                        at(t[1][k], j) = at(rz, j) * (at(dzszz, j) + at(dxsxz[k], j));
-                        at(t[2][k], j) = at(l2m, j) * at(dxvx[k], j) + at(lam, j) * at(dzvz, j);
-                        at(t[3][k], j) = at(lam, j) * at(dxvx[k], j) + at(l2m, j) * at(dzvz, j);
-                        at(t[4][k], j) = at(mu, j) * (at(dzvx, j) + at(dxvz[k], j));
-                    }
+                for (int j = 0; j < 4; j++) at(t[1], j) = at(rz, j) * (at(dz, j) + at(dx, j));
+            }
+            xw(s0); dx = dpx(q, 4, cx);
+            zwin(s1, lx, lz, w); dz = dpz(w, cz);
+            if (valid) {
+                const float4 l2m = ldg4(a.par[2] + gi), lam = ldg4(a.par[3] + gi);
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    at(t[2], j) = at(l2m, j) * at(dx, j) + at(lam, j) * at(dz, j);
+                    at(t[3], j) = at(lam, j) * at(dx, j) + at(l2m, j) * at(dz, j);
                 }
+            }
+            zwin(s0, lx, lz, w); dz = dmz(w, cz);
+            xw(s1); dx = dmx(q, 4, cx);
+            if (valid) {
+                const float4 mu = ldg4(a.par[4] + gi);
+#pragma unroll
+                for (int j = 0; j < 4; j++) at(t[4], j) = at(mu, j) * (at(dz, j) + at(dx, j));
             }
         } else {
             // s0 A=l2m*sxx+lam*szz, s1 B=lam*sxx+l2m*szz, s2 M=mu*sxz, s3 P=rhox*vx, s4 Q=rhoz*vz
-            float4 dxA[2], dxM[2], dxP[2], dxQ[2];
-            xwin(s0, lxa, lz, q); dxA[0] = dmx(q, 4, cx); dxA[1] = dmx(q, 5, cx);
-            xwin(s2, lxa, lz, q); dxM[0] = dpx(q, 4, cx); dxM[1] = dpx(q, 5, cx);
-            xwin(s3, lxa, lz, q); dxP[0] = dpx(q, 4, cx); dxP[1] = dpx(q, 5, cx);
-            xwin(s4, lxa, lz, q); dxQ[0] = dmx(q, 4, cx); dxQ[1] = dmx(q, 5, cx);
+            xw(s0); float4 dx = dmx(q, 4, cx);
+            zwin(s2, lx, lz, w); float4 dz = dpz(w, cz);
 #pragma unroll
-            for (int k = 0; k < 2; k++) {
-                const int lx = lxa + k;
-                float4 dzM, dzB, dzP, dzQ;
-                zwin(s2, lx, lz, w); dzM = dpz(w, cz);
-                zwin(s1, lx, lz, w); dzB = dmz(w, cz);
-                zwin(s3, lx, lz, w); dzP = dmz(w, cz);
-                zwin(s4, lx, lz, w); dzQ = dpz(w, cz);
+            for (int j = 0; j < 4; j++) at(t[0], j) = -(at(dx, j) + at(dz, j));
+            zwin(s1, lx, lz, w); dz = dmz(w, cz);
+            xw(s2); dx = dpx(q, 4, cx);
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    at(t[0][k], j) = -(at(dxA[k], j) + at(dzM, j));
-                    at(t[1][k], j) = -(at(dzB, j) + at(dxM[k], j));
-                    at(t[2][k], j) = -at(dxP[k], j);
-                    at(t[3][k], j) = -at(dzQ, j);
-                    at(t[4][k], j) = -(at(dzP, j) + at(dxQ[k], j));
-                }
-            }
+            for (int j = 0; j < 4; j++) at(t[1], j) = -(at(dz, j) + at(dx, j));
+            xw(s3); dx = dpx(q, 4, cx);
+#pragma unroll
+            for (int j = 0; j < 4; j++) at(t[2], j) = -at(dx, j);
+            zwin(s4, lx, lz, w); dz = dpz(w, cz);
+#pragma unroll
+            for (int j = 0; j < 4; j++) at(t[3], j) = -at(dz, j);
+            zwin(s3, lx, lz, w); dz = dmz(w, cz);
+            xw(s4); dx = dmx(q, 4, cx);
+#pragma unroll
+            for (int j = 0; j < 4; j++) at(t[4], j) = -(at(dz, j) + at(dx, j));
         }
     }
 
     // ---- deferred taper of the old level, leapfrog sum
-    float dz4[4], dxk[2];
+    float dd[4];
+    {
+        const float dxc = __ldg(a.dampx + gx);
 #pragma unroll
-    for (int j = 0; j < 4; j++) dz4[j] = valid ? __ldg(a.dampz + gz + j) : 1.f;
-#pragma unroll
-    for (int k = 0; k < 2; k++) dxk[k] = __ldg(a.dampx + x0 + 2 * txi + k);
+        for (int j = 0; j < 4; j++) dd[j] = valid ? fminf(__ldg(a.dampz + gz + j), dxc) : 1.f;
+    }
     if (valid) {
 #pragma unroll
-        for (int k = 0; k < 2; k++) {
-            const long long gi = (long long)(x0 + 2 * txi + k) * nz + gz;
+        for (int f = 0; f < 5; f++) {
+            const float4 o = ld4(a.o[f] + gi);
+#pragma unroll
+            for (int j = 0; j < 4; j++) at(t[f], j) = dd[j] * at(o, j) + at(t[f], j);
+        }
+        if (EPI == EPI_INJ_SS) {
 #pragma unroll
             for (int f = 0; f < 5; f++) {
-                const float4 o = ld4(a.o[f] + gi);
+                const float4 l = ldg4(a.ssL[f] + gi), r = ldg4(a.ssR[f] + gi);
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const float d = fminf(dz4[j], dxk[k]);
-                    at(t[f][k], j) = d * at(o, j) + at(t[f][k], j);
-                }
-            }
-            if (EPI == EPI_INJ_SS) {
-#pragma unroll
-                for (int f = 0; f < 5; f++) {
-                    const float4 l = ldg4(a.ssL[f] + gi), r = ldg4(a.ssR[f] + gi);
-#pragma unroll
-                    for (int j = 0; j < 4; j++) at(t[f][k], j) += at(l, j) * a.sw0 + at(r, j) * a.sw1;
-                }
+                for (int j = 0; j < 4; j++) at(t[f], j) += at(l, j) * a.sw0 + at(r, j) * a.sw1;
             }
         }
     }
 
     // ---- sparse injection (sources / adjoint data), before the final taper
-    const int tz_total = a.ntz;
-    (void)tz_total;
     if (a.inj.tile_start) {
         const int e0 = a.inj.tile_start[tile], e1 = a.inj.tile_start[tile + 1];
         if (e1 > e0) {   // CTA-uniform
@@ -316,13 +314,11 @@ __global__ void __launch_bounds__(NT) k_step(StepArgs a)
             __syncthreads();
             if (valid) {
 #pragma unroll
-                for (int k = 0; k < 2; k++)
+                for (int f = 0; f < 5; f++) {
+                    const float4 v = ld4(acc + (f * TX + txi) * TZ + 4 * tzi);
 #pragma unroll
-                    for (int f = 0; f < 5; f++) {
-                        const float4 v = ld4(acc + (f * TX + 2 * txi + k) * TZ + 4 * tzi);
-#pragma unroll
-                        for (int j = 0; j < 4; j++) at(t[f][k], j) += at(v, j);
-                    }
+                    for (int j = 0; j < 4; j++) at(t[f], j) += at(v, j);
+                }
             }
         }
     }
@@ -330,33 +326,29 @@ __global__ void __launch_bounds__(NT) k_step(StepArgs a)
     // ---- final taper, store, dense epilogues
     if (valid) {
 #pragma unroll
-        for (int k = 0; k < 2; k++) {
-            const long long gi = (long long)(x0 + 2 * txi + k) * nz + gz;
+        for (int f = 0; f < 5; f++) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) at(t[f], j) *= dd[j];
+            st4(a.o[f] + gi, t[f]);
+        }
+        if (EPI == EPI_SAVE_W) {
+            float* w0p = a.W0 + (long long)a.wt * a.wstride + gi;
+            float* w1p = a.W1 + (long long)a.wt * a.wstride + gi;
+            float4 u0 = ld4(w0p), u1 = ld4(w0p + a.wstride), v0 = ld4(w1p), v1 = ld4(w1p + a.wstride);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                at(u0, j) += at(t[0], j) * a.ww0; at(u1, j) += at(t[0], j) * a.ww1;
+                at(v0, j) += at(t[1], j) * a.ww0; at(v1, j) += at(t[1], j) * a.ww1;
+            }
+            st4(w0p, u0); st4(w0p + a.wstride, u1); st4(w1p, v0); st4(w1p + a.wstride, v1);
+        }
+        if (EPI == EPI_EXT_SS) {
 #pragma unroll
             for (int f = 0; f < 5; f++) {
+                float4 l = ld4(a.eL[f] + gi), r = ld4(a.eR[f] + gi);
 #pragma unroll
-                for (int j = 0; j < 4; j++) at(t[f][k], j) *= fminf(dz4[j], dxk[k]);
-                st4(a.o[f] + gi, t[f][k]);
-            }
-            if (EPI == EPI_SAVE_W) {
-                float* w0p = a.W0 + (long long)a.wt * a.wstride + gi;
-                float* w1p = a.W1 + (long long)a.wt * a.wstride + gi;
-                float4 u0 = ld4(w0p), u1 = ld4(w0p + a.wstride), v0 = ld4(w1p), v1 = ld4(w1p + a.wstride);
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    at(u0, j) += at(t[0][k], j) * a.ww0; at(u1, j) += at(t[0][k], j) * a.ww1;
-                    at(v0, j) += at(t[1][k], j) * a.ww0; at(v1, j) += at(t[1][k], j) * a.ww1;
-                }
-                st4(w0p, u0); st4(w0p + a.wstride, u1); st4(w1p, v0); st4(w1p + a.wstride, v1);
-            }
-            if (EPI == EPI_EXT_SS) {
-#pragma unroll
-                for (int f = 0; f < 5; f++) {
-                    float4 l = ld4(a.eL[f] + gi), r = ld4(a.eR[f] + gi);
-#pragma unroll
-                    for (int j = 0; j < 4; j++) { at(l, j) += at(t[f][k], j) * a.sw0; at(r, j) += at(t[f][k], j) * a.sw1; }
-                    st4(a.eL[f] + gi, l); st4(a.eR[f] + gi, r);
-                }
+                for (int j = 0; j < 4; j++) { at(l, j) += at(t[f], j) * a.sw0; at(r, j) += at(t[f], j) * a.sw1; }
+                st4(a.eL[f] + gi, l); st4(a.eR[f] + gi, r);
             }
         }
     }
@@ -369,9 +361,7 @@ __global__ void __launch_bounds__(NT) k_step(StepArgs a)
             __syncthreads();
             if (valid) {
 #pragma unroll
-                for (int k = 0; k < 2; k++)
-#pragma unroll
-                    for (int f = 0; f < 5; f++) st4(stg + (f * TX + 2 * txi + k) * TZ + 4 * tzi, t[f][k]);
+                for (int f = 0; f < 5; f++) st4(stg + (f * TX + txi) * TZ + 4 * tzi, t[f]);
             }
             __syncthreads();
             for (int e = e0 + tid; e < e1; e += NT) {
