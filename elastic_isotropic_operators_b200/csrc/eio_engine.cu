@@ -9,7 +9,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -731,3 +733,242 @@ void engine_born_host(Engine* e, int adj, float* const srcDtw[5], float* const d
 }
 
 }  // namespace eio
+
+// ============================================================================
+// Allocation-free nonlinear forward propagation (eio_nl_fwd_noalloc).
+//
+// Some callers cannot call cudaMalloc: code whose device memory is owned by
+// another allocator (a framework's caching allocator that must see every
+// byte), processes that forbid allocation after start-up (real-time or
+// latency-critical services), or plug-ins that must not grow the device
+// footprint of their host process.  For them this entry point runs the same
+// nonlinear forward propagation as eio_nl_fwd_reg_dev with the same kernels,
+// but every scratch buffer (both wavefield time levels, the taper tables, the
+// sparse point lists and the time-major trace copies) lives in ONE
+// file-scope device array of fixed size.  The array is reserved when the
+// library's device code is loaded on a GPU and stays reserved on every GPU
+// that loads it until the process exits.  The caller passes the inputs
+// (medium, source traces) and the output (receiver traces) in its own device
+// memory.  Calls share the array: two calls that overlap on the GPU (other
+// host threads, other streams) race on it and must be serialised by the
+// caller.
+// ============================================================================
+namespace eio {
+namespace noalloc {
+
+constexpr long long MAX_CELLS = 262144;        // nz * nx (e.g. 312 x 520 fits)
+constexpr int MAX_AXIS = 16384;                // nz, nx each
+constexpr long long MAX_SIGNAL = 4LL << 20;    // floats of time-major trace copies (sources + receivers)
+constexpr int MAX_TILES = 8192;                // tile buckets per point list
+constexpr int MAX_POINTS = 65536;              // entries per point list
+
+constexpr long long OFF_WF = 0;
+constexpr long long OFF_TAPER = OFF_WF + 10 * MAX_CELLS;
+constexpr long long OFF_SIG = OFF_TAPER + 2LL * MAX_AXIS;
+constexpr long long OFF_TS = OFF_SIG + MAX_SIGNAL;                   // 2 x (MAX_TILES + 1) ints
+constexpr long long OFF_ENT = OFF_TS + 2LL * (MAX_TILES + 4);        // 2 x MAX_POINTS PointEntry
+constexpr long long TOTAL = OFF_ENT + 2LL * MAX_POINTS * 2;          // in 4-byte words
+
+static __device__ __align__(256) float g_noalloc_scratch[TOTAL];
+
+static std::mutex g_mu;
+static float* g_dev_addr[256];
+
+// Device address of the scratch array on the current device.  The first call on
+// a device looks it up (cudaGetSymbolAddress); later calls reuse it.
+static float* scratch_on_current_device() {
+    int dev = 0;
+    EIO_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) throw Error(EIO_ERR_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_dev_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (err != cudaSuccess || !p)
+            throw Error(EIO_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(err));
+        g_dev_addr[dev] = static_cast<float*>(p);
+    }
+    return g_dev_addr[dev];
+}
+
+// Per-tile buckets of the tile kernel (TZ x TX tiles numbered z-fastest).
+static int bucket(int nz, int nx, const int* const pos[4], const int npos[4], std::vector<int>& ts,
+                  std::vector<PointEntry>& ent, int ld[5]) {
+    const int ntz = (nz - 2 * FAT + TZ - 1) / TZ, ntx = (nx - 2 * FAT) / TX, ntiles = ntz * ntx;
+    std::vector<std::pair<int, PointEntry>> tmp;
+    for (int f = 0; f < 5; f++) {
+        const int g = kFieldGrid[f];
+        ld[f] = npos[g];
+        for (int k = 0; k < npos[g]; k++) {
+            const int cell = pos[g][k];
+            const int ix = cell / nz, iz = cell % nz;
+            if (cell < 0 || ix < FAT || ix >= nx - FAT || iz < FAT || iz >= nz - FAT)
+                throw Error(EIO_ERR_BOUNDS, "acquisition point " + std::to_string(cell) +
+                                                " lies outside the updated interior of the grid");
+            PointEntry pe;
+            pe.key = (f << 16) | (((ix - FAT) % TX) << 8) | ((iz - FAT) % TZ);
+            pe.col = k;
+            tmp.push_back({((ix - FAT) / TX) * ntz + (iz - FAT) / TZ, pe});
+        }
+    }
+    ts.assign(ntiles + 1, 0);
+    for (auto& t : tmp) ts[t.first + 1]++;
+    for (int i = 0; i < ntiles; i++) ts[i + 1] += ts[i];
+    ent.resize(tmp.size());
+    std::vector<int> cur(ts.begin(), ts.end() - 1);
+    for (auto& t : tmp) ent[cur[t.first]++] = t.second;
+    return ntiles;
+}
+
+static void nl_fwd(const eio_fd_params& p, float* const med[5], float* const model[5], float* const data[5],
+                   const int* const srcPos[4], const int nSrc[4], const int* const recPos[4], const int nRec[4],
+                   cudaStream_t st) {
+    const int nz = p.nz, nx = p.nx, nts = p.nts;
+    if (nz < 2 * FAT + 16 || nx < 2 * FAT + 16 || (nz - 2 * FAT) % 16 || (nx - 2 * FAT) % 16)
+        throw Error(EIO_ERR_QC, "nz-2*fat and nx-2*fat must be positive multiples of 16");
+    if ((long long)nz * nx > MAX_CELLS || nz > MAX_AXIS || nx > MAX_AXIS)
+        throw Error(EIO_ERR_ARG, "grid " + std::to_string(nz) + "x" + std::to_string(nx) +
+                                     " exceeds the allocation-free limit of " + std::to_string(MAX_CELLS) +
+                                     " cells (and " + std::to_string(MAX_AXIS) + " per axis)");
+    if (p.sub < 1 || 2 * p.sub >= SUB_MAX || nts < 2) throw Error(EIO_ERR_ARG, "invalid nts / sub");
+    if (p.fat != 4 || p.blockSize != 16 || p.surfaceCondition != 0)
+        throw Error(EIO_ERR_UNSUPPORTED, "fat 4, blockSize 16 and surfaceCondition 0 only");
+    for (int k = 0; k < 4; k++)
+        if (nSrc[k] < 0 || nRec[k] < 0) throw Error(EIO_ERR_ARG, "negative point count");
+    // constants, same formulas as build_fdparam (nonlinearPropElasticGpuFunctions.cu:155-202)
+    const int S = 2 * p.sub, h = S + 1;
+    const int ntw = (nts - 1) * S + 1;
+    float dz = p.dz, dx = p.dx;
+    if (p.mod_par == 2) { dz *= 1000.f; dx *= 1000.f; }
+    static const double C[4] = {1.196289062541883, -0.079752604188901, 0.009570312506634, -6.975446437140719e-04};
+    std::vector<float> filt(2 * h);
+    const float sc = std::sqrt(float(ntw) / float(nts));
+    for (int i = 0; i < h; i++) {
+        const float a0 = (float)(1.0 - 1.0 * i / S), b0 = (float)(1.0 - a0);
+        filt[i] = (float)(a0 * (1.0 / sc));
+        filt[i + h] = (float)(b0 * (1.0 / sc));
+    }
+    const int minPad = std::min(std::min(p.zPadMinus, p.zPadPlus), std::min(p.xPadMinus, p.xPadPlus));
+    if (minPad < 0 || minPad >= PAD_MAX) throw Error(EIO_ERR_QC, "**** ERROR: Padding value is too high ****");
+    std::vector<float> damp(std::max(minPad, 1), 1.f), tz(nz, 1.f), tx(nx, 1.f);
+    for (int i = 0; i < minPad; i++) {
+        float arg = (float)(M_PI / (1.0 * minPad) * 1.0 * (minPad - i));
+        damp[i] = (float)(p.alphaCos + (1.0 - p.alphaCos) * std::cos(arg));
+    }
+    for (int iz = FAT; iz < nz - FAT; iz++) {
+        const int d = std::min(iz - FAT, nz - iz - 1 - FAT);
+        if (d < minPad) tz[iz] = damp[d];
+    }
+    for (int ix = FAT; ix < nx - FAT; ix++) {
+        const int d = std::min(ix - FAT, nx - ix - 1 - FAT);
+        if (d < minPad) tx[ix] = damp[d];
+    }
+    // sparse point lists
+    std::vector<int> ts_i, ts_e;
+    std::vector<PointEntry> en_i, en_e;
+    int ld_i[5], ld_e[5];
+    const int ntiles = bucket(nz, nx, srcPos, nSrc, ts_i, en_i, ld_i);
+    bucket(nz, nx, recPos, nRec, ts_e, en_e, ld_e);
+    if (ntiles > MAX_TILES) throw Error(EIO_ERR_ARG, "too many tiles for the allocation-free scratch");
+    if ((long long)en_i.size() > MAX_POINTS || (long long)en_e.size() > MAX_POINTS)
+        throw Error(EIO_ERR_ARG, "more than " + std::to_string(MAX_POINTS) + " sparse points in one list");
+    long long sig_total = 0;
+    for (int f = 0; f < 5; f++) sig_total += (long long)(ld_i[f] + ld_e[f]) * nts;
+    if (sig_total > MAX_SIGNAL)
+        throw Error(EIO_ERR_ARG, "source + receiver traces (" + std::to_string(sig_total) +
+                                     " floats) exceed the allocation-free limit of " + std::to_string(MAX_SIGNAL));
+
+    // carve the scratch array
+    float* base = scratch_on_current_device();
+    const long long n = (long long)nz * nx;
+    float* wf = base + OFF_WF;
+    float* dampz = base + OFF_TAPER;
+    float* dampx = dampz + nz;
+    float* sig = base + OFF_SIG;
+    int* ts_dev_i = reinterpret_cast<int*>(base + OFF_TS);
+    int* ts_dev_e = ts_dev_i + (MAX_TILES + 2);
+    PointEntry* ent_dev_i = reinterpret_cast<PointEntry*>(base + OFF_ENT);
+    PointEntry* ent_dev_e = ent_dev_i + MAX_POINTS;
+    float* sin_f[5];
+    float* sout_f[5];
+    {
+        float* q = sig;
+        for (int f = 0; f < 5; f++) { sin_f[f] = q; q += (long long)ld_i[f] * nts; }
+        for (int f = 0; f < 5; f++) { sout_f[f] = q; q += (long long)ld_e[f] * nts; }
+    }
+    // set-up copies and clears (no allocation anywhere below)
+    EIO_CUDA(cudaMemcpyAsync(dampz, tz.data(), sizeof(float) * nz, cudaMemcpyHostToDevice, st));
+    EIO_CUDA(cudaMemcpyAsync(dampx, tx.data(), sizeof(float) * nx, cudaMemcpyHostToDevice, st));
+    EIO_CUDA(cudaMemcpyAsync(ts_dev_i, ts_i.data(), sizeof(int) * ts_i.size(), cudaMemcpyHostToDevice, st));
+    EIO_CUDA(cudaMemcpyAsync(ts_dev_e, ts_e.data(), sizeof(int) * ts_e.size(), cudaMemcpyHostToDevice, st));
+    if (!en_i.empty())
+        EIO_CUDA(cudaMemcpyAsync(ent_dev_i, en_i.data(), sizeof(PointEntry) * en_i.size(), cudaMemcpyHostToDevice, st));
+    if (!en_e.empty())
+        EIO_CUDA(cudaMemcpyAsync(ent_dev_e, en_e.data(), sizeof(PointEntry) * en_e.size(), cudaMemcpyHostToDevice, st));
+    EIO_CUDA(cudaMemsetAsync(wf, 0, sizeof(float) * 10 * n, st));   // both time levels start at zero
+    for (int f = 0; f < 5; f++) {
+        if (ld_e[f]) EIO_CUDA(cudaMemsetAsync(sout_f[f], 0, sizeof(float) * ld_e[f] * nts, st));
+        if (ld_i[f]) {
+            dim3 b(32, 8), g((nts + 31) / 32, (ld_i[f] + 31) / 32);
+            k_transpose<<<g, b, 0, st>>>(model[f], sin_f[f], ld_i[f], nts);
+        }
+    }
+    StepArgs a;
+    memset(&a, 0, sizeof(a));
+    for (int f = 0; f < 5; f++) a.par[f] = med[f];
+    a.dampz = dampz;
+    a.dampx = dampx;
+    a.nz = nz;
+    a.nx = nx;
+    a.ntz = (nz - 2 * FAT + TZ - 1) / TZ;
+    for (int k = 0; k < 4; k++) { a.cz[k] = (float)(C[k] / dz); a.cx[k] = (float)(C[k] / dx); }
+    if (!en_i.empty()) {
+        a.inj.tile_start = ts_dev_i;
+        a.inj.ent = ent_dev_i;
+        for (int f = 0; f < 5; f++) { a.inj.sig[f] = sin_f[f]; a.inj.ld[f] = ld_i[f]; }
+    }
+    if (!en_e.empty()) {
+        a.ext.tile_start = ts_dev_e;
+        a.ext.ent = ent_dev_e;
+        for (int f = 0; f < 5; f++) { a.ext.sig[f] = sout_f[f]; a.ext.ld[f] = ld_e[f]; }
+    }
+    float* p0[5];
+    float* p1[5];
+    for (int f = 0; f < 5; f++) { p0[f] = wf + f * n; p1[f] = wf + (5 + f) * n; }
+    for (int its = 0; its < nts - 1; its++)
+        for (int it2 = 1; it2 < S + 1; it2++) {
+            for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; }
+            a.inj.t0 = its; a.inj.w0 = filt[it2 - 1]; a.inj.w1 = filt[h + it2 - 1];
+            a.ext.t0 = its; a.ext.w0 = filt[it2]; a.ext.w1 = filt[h + it2];
+            k_step<0, EPI_NONE><<<ntiles, NT, 0, st>>>(a);
+            std::swap(p0, p1);
+        }
+    for (int f = 0; f < 5; f++) {
+        if (!ld_e[f]) continue;
+        dim3 b(32, 8), g((ld_e[f] + 31) / 32, (nts + 31) / 32);
+        k_transpose<<<g, b, 0, st>>>(sout_f[f], data[f], nts, ld_e[f]);
+    }
+    cudaError_t lerr = cudaGetLastError();
+    if (lerr != cudaSuccess) throw Error(EIO_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(lerr));
+    EIO_CUDA(cudaStreamSynchronize(st));
+}
+
+}  // namespace noalloc
+}  // namespace eio
+
+extern "C" __attribute__((visibility("default"))) int eio_nl_fwd_noalloc(
+    const eio_fd_params* p, float* const medium[5], float* const model[5], float* const data[5],
+    const int* const srcPos[4], const int nSrc[4], const int* const recPos[4], const int nRec[4], void* stream) {
+    try {
+        if (!p || !medium || !model || !data || !srcPos || !nSrc || !recPos || !nRec)
+            throw eio::Error(EIO_ERR_ARG, "null argument");
+        eio::noalloc::nl_fwd(*p, medium, model, data, srcPos, nSrc, recPos, nRec, static_cast<cudaStream_t>(stream));
+        return EIO_OK;
+    } catch (const eio::Error& e) {
+        eio::set_last_error(e.what());
+        return e.code;
+    } catch (const std::exception& e) {
+        eio::set_last_error(e.what());
+        return EIO_ERR_ARG;
+    }
+}

@@ -28,6 +28,8 @@ namespace eio {
 
 static thread_local std::string g_last_error;
 
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
 // ------------------------------------------------------------------ fdParam
 void stagger_x(int adj, int add, int nz, int nx, float* model, float* data) {
     const long long n = (long long)nz * nx;

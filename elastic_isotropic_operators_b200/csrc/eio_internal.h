@@ -13,6 +13,9 @@ namespace eio {
 constexpr int SUB_MAX = 100;   // varDeclare.h:11 (2*sub must stay below it)
 constexpr int PAD_MAX = 500;   // varDeclare.h:10
 
+// message returned by eio_last_error() on the calling thread
+void set_last_error(const std::string& msg);
+
 struct Error : std::runtime_error {
     int code;
     Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}

@@ -215,6 +215,36 @@ int eio_born_adjoint(eio_ctx *c, int add, int nExp, float *model, const float *d
 int eio_born_prepare_sources(eio_ctx *c, const float *signal, eio_sinterp *const src[4], float *const out[5]);
 int eio_born_prepare_model(eio_ctx *c, const float *model, float *const out[5]);
 
+/* ---------------------------------------------------------------------------
+ * Allocation-free nonlinear forward propagation.  No counterpart in the
+ * reference (its drivers cudaMalloc and cudaFree on every call).
+ *
+ * For callers that cannot call cudaMalloc -- code whose device memory belongs
+ * to another allocator, processes that forbid allocation after start-up, or
+ * plug-ins that must not grow their host process's device footprint.  It runs
+ * the same propagation as eio_nl_fwd_reg_dev without allocating anything:
+ * all scratch (both wavefield levels, taper tables, point lists, time-major
+ * trace copies) lives in one fixed file-scope device array of about 28 MB
+ * that every GPU loading the library holds until the process exits.
+ *   - p: the par-file parameters (medium QC is the caller's: the medium
+ *     arrives already prepared, e.g. with eio_medium_prepare);
+ *   - medium: the 5 scaled coefficient grids [nx][nz] in device memory;
+ *   - model / data: as eio_nl_fwd_reg_dev, device memory owned by the caller;
+ *   - runs on `stream` (a cudaStream_t, NULL = legacy default stream) of the
+ *     current device and synchronizes it before returning.
+ * Limits (EIO_ERR_ARG beyond them, checked before anything runs):
+ *   nz*nx <= 262144 cells, nz, nx <= 16384, source + receiver traces <=
+ *   4194304 floats (sum over the 5 fields of points x nts), <= 65536 points
+ *   per list.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * Every call reuses the same array and clears what must start at zero;
+ * calls that overlap on the GPU (other threads or streams) race on it and
+ * must be serialised by the caller. */
+int eio_nl_fwd_noalloc(const eio_fd_params *p, float *const medium[5], float *const model[5], float *const data[5],
+                       const int *const srcPos[4], const int nSrc[4], const int *const recPos[4], const int nRec[4],
+                       void *stream);
+
 #ifdef __cplusplus
 }
 #endif
