@@ -40,6 +40,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="born_600x1800", choices=["born_600x1800", "nl_312x520"])
     ap.add_argument("--shots", type=int, default=10)
     ap.add_argument("--nts", type=int, default=4000)
     ap.add_argument("--no-e2e", action="store_true")
@@ -339,7 +340,15 @@ def run_reference(args, ws, rank, local):
     from elastic_isotropic_operators_b200 import synthetic
     if not O.RefGpu.available("f"):
         return {"impl": "reference", "unavailable": "oracle/_ref not built (reference tree absent at build time)"}
+    if args.workload == "nl_312x520":
+        return run_reference_nl(args)
     w = synthetic.born_600x1800(nts=args.nts, nshots=1, seed=2024)
+    if not O.RefGpu.born_supported(O.Case.from_workload(w).grid()):
+        return {"impl": "reference",
+                "unavailable": "the reference Born drivers index their Vx/Vz history with the 32-bit product "
+                               "its*nz*nx (kernelsGpuElastic.cu:1342), which overflows for nts*nz*nx >= 2^31 "
+                               "(here 4000*600*1800); on this grid they faulted with an illegal memory access at "
+                               "BornElasticGpuFunctions.cu:763, so they are not run again"}
     orc = O.Oracle("f")
     c = O.Case.from_workload(w)
     g = c.grid()
@@ -377,6 +386,150 @@ def run_reference(args, ws, rank, local):
                     "d2h_bytes_per_step": 0}}
 
 
+def run_reference_nl(args):
+    """Reference CUDA drivers, nonlinear forward of the 312x520 shot (full nts)."""
+    from oracle import oracle as O
+    from elastic_isotropic_operators_b200 import synthetic
+    w = synthetic.nl_312x520()
+    orc = O.Oracle("f")
+    c = O.Case.from_workload(w)
+    g = c.grid()
+    med = orc.medium(c.ep, g["dts"], g["S"])
+    src = O._grids(orc, c, *c.src[0])
+    rec = O._grids(orc, c, *c.rec)
+    reg = []
+    sig = w.source_signal()
+    for f in range(5):
+        G = src[O.FIELD_GRID[f]]
+        r = np.zeros((len(G["uniq"]), g["nts"]), np.float32)
+        orc.sinterp_apply(G, 1, 0, r, np.ascontiguousarray(sig[f]))
+        reg.append(r)
+    O._scale_sources(orc, g, med, src, reg)
+    data = [np.zeros((len(rec[O.FIELD_GRID[f]]["uniq"]), g["nts"]), np.float32) for f in range(5)]
+    ref = O.RefGpu("f")
+
+    def step():
+        ref.nl_prop(0, g, med, reg, data, O._reg_pos(src), O._reg_pos(rec))
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    upd = (g["nts"] - 1) * g["S"] * (g["nz"] - 8) * (g["nx"] - 8) * args.steps
+    v = upd / dt / 1e9
+    return {"impl": "reference", "metric": "Gcells/s", "value": round(v, 3), "unit": "Gcell-updates/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * dt / args.steps, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "nl_312x520: nonlinear forward, 1 shot, nts=2000 (3998 fine steps)"},
+            "cpu_baseline": {"value": round(v, 3), "unit": "Gcell-updates/s", "cores": 1, "kind": "reference",
+                             "sample": "reference CUDA drivers (elastic_iso_float, built for sm_100a) on the B200; "
+                                       "the reference has no CPU implementation of this path"},
+            "e2e": {"value": round(v, 3), "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def run_ours_nl(args, ws, rank, local):
+    """Nonlinear forward of the 312x520 shot (one shot per rank)."""
+    import ctypes
+    import torch
+    from elastic_isotropic_operators_b200 import _lib, prop, synthetic
+    from oracle import oracle as O
+    w = synthetic.nl_312x520()
+    dev = torch.device("cuda", local)
+    w.par.set("iGpu", str(local))
+    src, rec = w.geometry()
+    nl = prop.nonlinearPropElasticShotsGpu(w.elastic, w.par, *src, *rec)
+    L = _lib.lib()
+    ctx = nl.ctx
+    fine_steps, cells = ctypes.c_longlong(), ctypes.c_longlong()
+    _lib.check(L.eio_ctx_counts(ctx, ctypes.byref(fine_steps), ctypes.byref(cells)))
+    fine_steps, cells = fine_steps.value, cells.value
+    upd = float(fine_steps * cells)
+    # regular-grid sources exactly as the operator prepares them
+    orc = O.Oracle("f")
+    c = O.Case.from_workload(w)
+    g = c.grid()
+    med = orc.medium(c.ep, g["dts"], g["S"])
+    sg = O._grids(orc, c, *c.src[0])
+    rg = O._grids(orc, c, *c.rec)
+    reg = []
+    sig = w.source_signal()
+    for f in range(5):
+        G = sg[O.FIELD_GRID[f]]
+        r = np.zeros((len(G["uniq"]), g["nts"]), np.float32)
+        orc.sinterp_apply(G, 1, 0, r, np.ascontiguousarray(sig[f]))
+        reg.append(r)
+    O._scale_sources(orc, g, med, sg, reg)
+    m_dev = [torch.from_numpy(a).to(dev) for a in reg]
+    d_dev = [torch.zeros((len(rg[O.FIELD_GRID[f]]["uniq"]), g["nts"]), device=dev) for f in range(5)]
+    sp = [np.ascontiguousarray(G["uniq"], np.int32) for G in sg]
+    rp = [np.ascontiguousarray(G["uniq"], np.int32) for G in rg]
+    args_c = (_lib.ptr_array([t.data_ptr() for t in m_dev]), _lib.ptr_array([t.data_ptr() for t in d_dev]),
+              _lib.ptr_array([a.ctypes.data for a in sp]), (ctypes.c_int * 4)(*[len(a) for a in sp]),
+              _lib.ptr_array([a.ctypes.data for a in rp]), (ctypes.c_int * 4)(*[len(a) for a in rp]))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        _lib.check(L.eio_nl_fwd_reg_dev(ctx, *args_c))
+
+    for _ in range(args.warmup):
+        step()
+        flush.zero_()
+    L.eio_ctx_stats(ctx, 1, 1, None, None, None)
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(None)
+    clocks.start()
+    t_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record()
+        step()
+        ev1.record()
+        torch.cuda.synchronize()
+        t_ms += ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    launches, sl, sms = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_double()
+    L.eio_ctx_stats(ctx, 0, 1, ctypes.byref(launches), ctypes.byref(sl), ctypes.byref(sms))
+    t_ms = max_over_ranks(ws, t_ms)
+    avg = sms.value / max(sl.value, 1)
+    peak, pk = measured_peak()
+    ach = BYTES_PER_CELL * cells / (avg * 1e-3) / 1e9
+    model = nl.modelSpace()
+    model.getNdArray()[...] = w.source_signal()[None]
+    data = nl.dataSpace()
+    nl.forward(False, model, data)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        nl.forward(False, model, data)
+    t_e2e = max_over_ranks(ws, time.perf_counter() - t0)
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        t0 = time.perf_counter()
+        O.nl_forward(orc, c, model.getNdArray())
+        dt = time.perf_counter() - t0
+        cpu = {"value": round(upd / dt / 1e9, 4), "unit": "Gcell-updates/s", "cores": O.num_threads(), "kind": "port",
+               "sample": "oracle FP32 nonlinear forward of the whole workload (1 shot, 3998 fine steps), %.1f s" % dt}
+    return {"metric": "Gcells/s", "value": round(ws * upd * args.steps / (t_ms * 1e-3) / 1e9, 3),
+            "unit": "Gcell-updates/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(t_ms / args.steps, 2), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "nl_312x520: nonlinear forward, 1 shot per GPU, 312x520 grid, nts=2000 "
+                                   "(3998 fine steps), 400 receivers",
+                       "l2": "working set (13 MB) is L2-resident by construction; 256 MB L2 flush between steps"},
+            "e2e": {"value": round(ws * upd * args.steps / t_e2e / 1e9, 3), "unit": "Gcell-updates/s",
+                    "h2d_bytes_per_step": int(sum(4 * a.size for a in reg)),
+                    "d2h_bytes_per_step": int(sum(4 * t.numel() for t in d_dev))},
+            "roofline": {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(ach / peak, 4), "traffic": None, "peak_source": pk,
+                         "avg_launch_us": round(avg * 1e3, 3)},
+            "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches.value)}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -386,7 +539,10 @@ def main():
         print(json.dumps(run_reference(args, 1, 0, int(os.environ.get("LOCAL_RANK", "0")))))
         return 0
     ws, rank, local = dist_init(args)
-    out = run_ours(args, ws, rank, local)
+    if args.workload == "nl_312x520":
+        out = run_ours_nl(args, ws, rank, local)
+    else:
+        out = run_ours(args, ws, rank, local)
     if rank == 0:
         print(json.dumps(out))
     if ws > 1:

@@ -80,6 +80,7 @@ struct Engine {
     DBuf sig_in[5], sig_out[5];
     DBuf stage_a[5], stage_b[5], stage_c[5];
     DBuf W, ss[10];
+    bool w_clean = false;   // history zeroed and only written by single stores since
     // step-kernel choice: kind 0 = shared-memory tile kernel (k_step),
     // kind 1 = TMA x-sweep (k_sweep) with strip height tz, chunk width cw and
     // cpr chunks per CTA
@@ -371,6 +372,8 @@ static void launch_sweep(Engine* e, const StepArgs& a, int cur) {
     // the sweep kernel buckets points per (strip, chunk): rebuilt by the caller
     s.W0 = a.W0; s.W1 = a.W1; s.wstride = a.wstride; s.wt = a.wt; s.ww0 = a.ww0; s.ww1 = a.ww1;
     s.sw0 = a.sw0; s.sw1 = a.sw1;
+    s.tmode = a.tmode; s.tw_o = a.tw_o; s.tw_c = a.tw_c; s.tw_n = a.tw_n;
+    for (int f = 0; f < 5; f++) s.c[f] = a.c[f];
     s.err = static_cast<int*>(e->err.p);
     const int nb = s.nstrips * s.nranges;
     if (e->tz == 64 && e->cw == 8) launch_sweep_t<DIR, EPI, 64, 8>(e, s, nb);
@@ -582,11 +585,22 @@ static void launch_imaging(Engine* e, int adj, int its, float* const dm[5], floa
     e->launches++;
 }
 
-// Source wavefield + coarse Vx/Vz history (BornElasticGpuFunctions.cu:746-768)
+// Source wavefield + coarse Vx/Vz history (BornElasticGpuFunctions.cu:746-768).
+// The reference accumulates every fine step into rows its and its+1 of the
+// history (interpWavefieldSingleComp, K:1337-1346).  With two fine steps per
+// coarse sample (sub = 1) row its only ever receives the three fine samples
+// that the step (its, it2 = 1) holds as its old, current and new level, so
+// that step writes the row once (EPI_TRI, same operation order) and the other
+// steps touch no history at all; other sub values keep the running sums.
 static void born_source(Engine* e, const PointList& src, StepArgs a) {
     const size_t wbytes = sizeof(float) * 2 * (size_t)e->nts * e->n;
+    const bool fresh = e->W.cap < wbytes;
     e->W.ensure(wbytes);
-    EIO_CUDA(cudaMemsetAsync(e->W.p, 0, wbytes, e->st));
+    const bool tri = (e->S == 2);
+    // running sums need a zeroed history; single writes only need the never
+    // written FAT frame to be zero, which holds from the first clear on
+    if (!tri || fresh || !e->w_clean) EIO_CUDA(cudaMemsetAsync(e->W.p, 0, wbytes, e->st));
+    e->w_clean = tri;
     zero_wavefields(e);
     float* p0[5]; float* p1[5];
     for (int f = 0; f < 5; f++) { p0[f] = e->wf[f].f(); p1[f] = e->wf[5 + f].f(); }
@@ -596,13 +610,27 @@ static void born_source(Engine* e, const PointList& src, StepArgs a) {
     a.W0 = e->W.f();
     a.W1 = e->W.f() + (long long)e->nts * e->n;
     const float* F = e->filt.data();
+    const int h = e->h;
     for (int its = 0; its < e->nts - 1; its++)
         for (int it2 = 1; it2 < e->S + 1; it2++) {
             const int itw = its * e->S + it2;
             for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; }
             a.inj.t0 = itw - 1; a.inj.w0 = 1.f; a.inj.w1 = 0.f;
-            a.wt = its; a.ww0 = F[it2]; a.ww1 = F[e->h + it2];
-            launch_step<0, EPI_SAVE_W>(e, a, cur);
+            if (tri) {
+                const bool last = (its == e->nts - 2 && it2 == 2);
+                if (it2 == 1) {          // row its = o*f[h+1] + c*f[h+2] + n*f[1]
+                    a.tmode = 1; a.wt = its; a.tw_o = F[h + 1]; a.tw_c = F[h + 2]; a.tw_n = F[1];
+                    launch_step<0, EPI_TRI>(e, a, cur);
+                } else if (last) {       // row nts-1 = c*f[h+1] + n*f[h+2]
+                    a.tmode = 2; a.wt = its + 1; a.tw_o = 0.f; a.tw_c = F[h + 1]; a.tw_n = F[h + 2];
+                    launch_step<0, EPI_TRI>(e, a, cur);
+                } else {
+                    launch_step<0, EPI_NONE>(e, a, cur);
+                }
+            } else {
+                a.wt = its; a.ww0 = F[it2]; a.ww1 = F[h + it2];
+                launch_step<0, EPI_SAVE_W>(e, a, cur);
+            }
             std::swap(p0, p1);
             cur ^= 1;
         }
@@ -657,6 +685,35 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
         }
         check_launch();
         stage_out(e, rec.ld, e->nts, e->sig_out, data);
+    } else if (e->S == 2) {
+        // Adjoint extraction with two fine steps per coarse sample: the coarse
+        // sample T of the reference's running sums ssL/ssR (extractInterpAdjointWavefield,
+        // K:1369-1376) is ((p(2T+1) f[1] + p(2T) f[0]) + p(2T-1) f[h+1]) (+ p(2T-2) * f[h] = 0),
+        // i.e. the old, current and new level of the step (T-1, it2 = 1): that step
+        // writes it once (EPI_TRI) and the imaging condition of T runs right after.
+        stage_in(e, data, rec.ld, e->nts, e->sig_in);
+        a.inj = upload_points(e, rec, e->inj_ts, e->inj_ent, e->sig_in);
+        for (int f = 0; f < 5; f++) a.eL[f] = sL[f];
+        for (int its = e->nts - 2; its > -1; its--) {
+            for (int it2 = e->S - 1; it2 > -1; it2--) {
+                for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; }
+                a.inj.t0 = its; a.inj.w0 = F[it2 + 1]; a.inj.w1 = F[h + it2 + 1];
+                if (it2 == 1) {
+                    a.tmode = 1; a.tw_o = F[1]; a.tw_c = F[0]; a.tw_n = F[h + 1];
+                    launch_step<1, EPI_TRI>(e, a, cur);
+                } else if (its == 0) {   // sample 0 = p(1) f[1] + p(0) f[0]
+                    a.tmode = 2; a.tw_o = 0.f; a.tw_c = F[1]; a.tw_n = F[0];
+                    launch_step<1, EPI_TRI>(e, a, cur);
+                } else {
+                    launch_step<1, EPI_NONE>(e, a, cur);
+                }
+                std::swap(p0, p1);
+                cur ^= 1;
+                if (it2 == 1) launch_imaging(e, 1, its + 1, dm, sL);
+            }
+        }
+        launch_imaging(e, 1, 0, dm, sL);
+        check_launch();
     } else {
         stage_in(e, data, rec.ld, e->nts, e->sig_in);
         a.inj = upload_points(e, rec, e->inj_ts, e->inj_ent, e->sig_in);

@@ -75,15 +75,34 @@ struct StepArgs {
     const float* ssL[5]; const float* ssR[5];   // scattered-field injection
     float* eL[5]; float* eR[5];                 // adjoint extraction
     float sw0, sw1;
+    // EPI_TRI (two fine steps per coarse sample): one coarse sample written at
+    // once from the old (o), current (c) and new (n) levels of this step,
+    //   tmode 1: fma(n, tw_n, fma(c, tw_c, o * tw_o));  tmode 2: fma(n, tw_n, c * tw_c)
+    // forward: vx, vz into row wt of W0 / W1;  adjoint: all five fields into eL[f]
+    int tmode;
+    float tw_o, tw_c, tw_n;
 };
 
-enum { EPI_NONE = 0, EPI_SAVE_W = 1, EPI_INJ_SS = 2, EPI_EXT_SS = 3 };
+enum { EPI_NONE = 0, EPI_SAVE_W = 1, EPI_INJ_SS = 2, EPI_EXT_SS = 3, EPI_TRI = 4 };
 
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 __device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
 __device__ __forceinline__ float& at(float4& v, int j) { return reinterpret_cast<float*>(&v)[j]; }
 __device__ __forceinline__ float at(const float4& v, int j) { return reinterpret_cast<const float*>(&v)[j]; }
+
+// coarse sample of EPI_TRI, same operation order as the reference's running sums
+__device__ __forceinline__ float4 tri_sample(int mode, float4 o, float4 c, float4 n, float wo, float wc, float wn)
+{
+    float4 r;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const float a = (mode == 1) ? fmaf(at(c, j), wc, at(o, j) * wo) : at(c, j) * wc;
+        at(r, j) = fmaf(at(n, j), wn, a);
+    }
+    return r;
+}
+
 
 // z-derivatives of 4 consecutive cells from a 12-value window v[-4..7]
 // (w = v shifted by +4).  Dminus: sum c_k (f[z+k] - f[z-1-k]); Dplus: sum c_k (f[z+1+k] - f[z-k]).
@@ -271,6 +290,12 @@ __global__ void __launch_bounds__(NT, 3) k_step(StepArgs a)
     }
 
     // ---- deferred taper of the old level, leapfrog sum
+    float4 osave[5];      // old level (EPI_TRI)
+    float4 csave[2];      // current vx, vz (forward EPI_TRI; shared memory is reused below)
+    if (EPI == EPI_TRI && DIR == 0) {
+        csave[0] = ld4(sm + lx * SZ + lz);
+        csave[1] = ld4(sm + SMEM_FIELD + lx * SZ + lz);
+    }
     float dd[4];
     {
         const float dxc = __ldg(a.dampx + gx);
@@ -281,13 +306,18 @@ __global__ void __launch_bounds__(NT, 3) k_step(StepArgs a)
 #pragma unroll
         for (int f = 0; f < 5; f++) {
             const float4 o = ld4(a.o[f] + gi);
+            if (EPI == EPI_TRI) osave[f] = o;
 #pragma unroll
             for (int j = 0; j < 4; j++) at(t[f], j) = dd[j] * at(o, j) + at(t[f], j);
         }
         if (EPI == EPI_INJ_SS) {
+            // with two fine steps per coarse sample every other step has sw1 == 0:
+            // the right slice is then not read (ssR * 0 adds nothing)
+            const bool right = a.sw1 != 0.f;
 #pragma unroll
             for (int f = 0; f < 5; f++) {
-                const float4 l = ldg4(a.ssL[f] + gi), r = ldg4(a.ssR[f] + gi);
+                const float4 l = ldg4(a.ssL[f] + gi);
+                const float4 r = right ? ldg4(a.ssR[f] + gi) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
                 for (int j = 0; j < 4; j++) at(t[f], j) += at(l, j) * a.sw0 + at(r, j) * a.sw1;
             }
@@ -349,6 +379,18 @@ __global__ void __launch_bounds__(NT, 3) k_step(StepArgs a)
 #pragma unroll
                 for (int j = 0; j < 4; j++) { at(l, j) += at(t[f], j) * a.sw0; at(r, j) += at(t[f], j) * a.sw1; }
                 st4(a.eL[f] + gi, l); st4(a.eR[f] + gi, r);
+            }
+        }
+        if (EPI == EPI_TRI && a.tmode) {
+            if (DIR == 0) {
+                st4(a.W0 + (long long)a.wt * a.wstride + gi,
+                    tri_sample(a.tmode, osave[0], csave[0], t[0], a.tw_o, a.tw_c, a.tw_n));
+                st4(a.W1 + (long long)a.wt * a.wstride + gi,
+                    tri_sample(a.tmode, osave[1], csave[1], t[1], a.tw_o, a.tw_c, a.tw_n));
+            } else {
+#pragma unroll
+                for (int f = 0; f < 5; f++)
+                    st4(a.eL[f] + gi, tri_sample(a.tmode, osave[f], ldg4(a.c[f] + gi), t[f], a.tw_o, a.tw_c, a.tw_n));
             }
         }
     }

@@ -40,6 +40,8 @@ struct SweepArgs {
     const float* ssL[5]; const float* ssR[5];
     float* eL[5]; float* eR[5];
     float sw0, sw1;
+    int tmode; float tw_o, tw_c, tw_n;   // EPI_TRI, see StepArgs
+    const float* c[5];                  // current level (adjoint EPI_TRI reads it directly)
     int* err;
 };
 
@@ -252,8 +254,12 @@ __global__ void __launch_bounds__(SweepLayout<TZ, CW, DIR>::NT) k_sweep(const __
         // Born dense inputs: issue the loads before waiting on the pipeline
         float4 pre[10];
         if (EPI == EPI_INJ_SS && valid) {
+            const bool right = a.sw1 != 0.f;
 #pragma unroll
-            for (int f = 0; f < 5; f++) { pre[f] = ldg4(a.ssL[f] + gi); pre[5 + f] = ldg4(a.ssR[f] + gi); }
+            for (int f = 0; f < 5; f++) {
+                pre[f] = ldg4(a.ssL[f] + gi);
+                pre[5 + f] = right ? ldg4(a.ssR[f] + gi) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
         }
         if (EPI == EPI_EXT_SS && valid) {
 #pragma unroll
@@ -340,9 +346,16 @@ __global__ void __launch_bounds__(SweepLayout<TZ, CW, DIR>::NT) k_sweep(const __
         float dd[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) dd[j] = fminf(dz4[j], dxc);
+        float4 osave[5];
+        float4 csave[2];
+        if (EPI == EPI_TRI && DIR == 0) {
+            csave[0] = ld4(colp(0, 4) + zrow);
+            csave[1] = ld4(colp(1, 4) + zrow);
+        }
 #pragma unroll
         for (int f = 0; f < 5; f++) {
             const float4 o = ld4(stg + f * STG);
+            if (EPI == EPI_TRI) osave[f] = o;
 #pragma unroll
             for (int j = 0; j < 4; j++) at(t[f], j) = dd[j] * at(o, j) + at(t[f], j);
         }
@@ -402,6 +415,19 @@ __global__ void __launch_bounds__(SweepLayout<TZ, CW, DIR>::NT) k_sweep(const __
 #pragma unroll
                     for (int j = 0; j < 4; j++) { at(l, j) += at(t[f], j) * a.sw0; at(r, j) += at(t[f], j) * a.sw1; }
                     st4(a.eL[f] + gi, l); st4(a.eR[f] + gi, r);
+                }
+            }
+            if (EPI == EPI_TRI && a.tmode) {
+                if (DIR == 0) {
+                    st4(a.W0 + (long long)a.wt * a.wstride + gi,
+                        tri_sample(a.tmode, osave[0], csave[0], t[0], a.tw_o, a.tw_c, a.tw_n));
+                    st4(a.W1 + (long long)a.wt * a.wstride + gi,
+                        tri_sample(a.tmode, osave[1], csave[1], t[1], a.tw_o, a.tw_c, a.tw_n));
+                } else {
+#pragma unroll
+                    for (int f = 0; f < 5; f++)
+                        st4(a.eL[f] + gi,
+                            tri_sample(a.tmode, osave[f], ldg4(a.c[f] + gi), t[f], a.tw_o, a.tw_c, a.tw_n));
                 }
             }
         }

@@ -193,7 +193,16 @@ class RefGpu:
                                 _pp(sp, None), ns, _pp(rp, None), nr)
         assert r == 0
 
+    @staticmethod
+    def born_supported(g):
+        """The reference's Born drivers index the coarse history with the 32-bit
+        product its*nz*nx (kernelsGpuElastic.cu:1342) and fault once
+        nts*nz*nx >= 2^31; those sizes are never run."""
+        return int(g["nts"]) * int(g["nz"]) * int(g["nx"]) < 2 ** 31
+
     def born_prop(self, adj, g, medium5, srcDtw5, dm5, data5, srcPos, recPos):
+        if not self.born_supported(g):
+            raise ValueError("reference Born drivers overflow their 32-bit history index at this size")
         ns = (ctypes.c_int * 4)(*[len(p) for p in srcPos])
         nr = (ctypes.c_int * 4)(*[len(p) for p in recPos])
         sp = [np.ascontiguousarray(p, np.int32) for p in srcPos]

@@ -54,6 +54,11 @@ EXPORT int ref_born_prop(int adj, int nz, int nx, real dz, real dx, int nts, rea
                          int minPad, real alphaCos, real **medium, real **srcDtw, real **dm, real **data,
                          int **srcPos, const int *nSrc, int **recPos, const int *nRec)
 {
+    /* The reference indexes its coarse Vx/Vz history with the 32-bit product
+     * its * nz * nx (interpWavefieldSingleComp, kernelsGpuElastic.cu:1342), which
+     * overflows once nts * nz * nx reaches 2^31 and then faults with an illegal
+     * address.  Refuse those sizes instead of running them. */
+    if ((long long)nts * nz * nx >= (1LL << 31)) return -2;
     initBornGpu(dz, dx, nz, nx, nts, dts, sub_int, minPad, 16, alphaCos, 1, 0, 0);
     allocateBornElasticGpu(medium[0], medium[1], medium[2], medium[3], medium[4], 0, 0, 0);
     if (!adj)

@@ -263,3 +263,24 @@ def test_full_size_born_600x1800_dot_product():
     src, rec = w.geometry()
     born = prop.BornElasticShotsGpu(w.elastic, w.par, [w.source_signal()], *src, *rec)
     assert born.dotTest(False, 1e-5), born.lastDotTest
+
+
+def test_sub2_running_sum_path_vs_oracle():
+    """sub = 2 (four fine steps per coarse sample) keeps the running-sum history
+    and adjoint accumulation; sub = 1 (every other test) takes the single-write path."""
+    w2 = synthetic.small(nts=60, sub=2)
+    c = Ctx(w2)
+    try:
+        r = reg_inputs(w2, "f", seed=13)
+        orc = r["orc"]
+        for adj in (0, 1):
+            dm, d = _copy(r["dm"]), _copy(r["data"])
+            orc.born_prop(adj, r["g"], r["med"], r["fine"], dm, d, r["sp"], r["rp"])
+            pdm, pd = c.born(adj, r["fine"], r["dm"], r["data"], r["sp"], r["rp"])
+            assert rel(pdm if adj else pd, dm if adj else d) < TOL32, ("born", adj)
+            m, d = _copy(r["model"]), _copy(r["data"])
+            orc.nl_prop(adj, r["g"], r["med"], m, d, r["sp"], r["rp"])
+            pm, pd = c.nl(adj, r["model"], r["data"], r["sp"], r["rp"])
+            assert rel(pm if adj else pd, m if adj else d) < TOL32, ("nl", adj)
+    finally:
+        c.close()
