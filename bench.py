@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--nts", type=int, default=4000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--kernel", type=int, default=-1, choices=[-1, 0, 1],
+                    help="-1: autotune (default); 0: tile kernel k_step; 1: TMA sweep kernel k_sweep")
     return ap.parse_args()
 
 
@@ -124,6 +126,24 @@ def profile_traffic():
     return None
 
 
+def pin_kernel(L, ctx, args):
+    """--kernel 0/1 fixes the step kernel (profiling runs); -1 keeps the autotuner."""
+    from elastic_isotropic_operators_b200 import _lib
+    if args.kernel >= 0:
+        _lib.check(L.eio_ctx_set_kernel(ctx, args.kernel, 64, 8, 8))
+
+
+def kernel_name(L, ctx):
+    """Step kernel the context runs (autotuned or pinned)."""
+    import ctypes
+    v = [ctypes.c_int() for _ in range(4)]
+    L.eio_ctx_get_kernel(ctx, *[ctypes.byref(x) for x in v])
+    kind, tz, cw, cpr = (x.value for x in v)
+    if kind == 0:
+        return "k_step (fused 5-field update, 64x16 tiles)"
+    return "k_sweep (fused 5-field update, TMA x-sweep, tz=%d cw=%d cpr=%d)" % (tz, cw, cpr)
+
+
 def dist_init(args):
     import torch
     ws = int(os.environ.get("WORLD_SIZE", "1"))
@@ -167,6 +187,8 @@ def run_ours(args, ws, rank, local):
     born = prop.BornElasticShotsGpu(w.elastic, w.par, sig, *src, *rec)
     L = _lib.lib()
     ctx = born.ctx
+    pin_kernel(L, ctx, args)
+    est = torch.cuda.ExternalStream(L.eio_ctx_stream(ctx), device=dev)   # the engine's launch stream
     nsh = w.nExp
     fine_steps, cells = ctypes.c_longlong(), ctypes.c_longlong()
     _lib.check(L.eio_ctx_counts(ctx, ctypes.byref(fine_steps), ctypes.byref(cells)))
@@ -231,9 +253,9 @@ def run_ours(args, ws, rank, local):
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
-        ev0.record()
+        ev0.record(est)
         step()
-        ev1.record()
+        ev1.record(est)
         torch.cuda.synchronize()
         t_ms += ev0.elapsed_time(ev1)
     barrier(ws)
@@ -249,7 +271,7 @@ def run_ours(args, ws, rank, local):
     peak, peak_kind = measured_peak()
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": profile_traffic(),
-            "peak_source": peak_kind, "kernel": "k_step (fused 5-field update)",
+            "peak_source": peak_kind, "kernel": kernel_name(L, ctx),
             "avg_launch_us": round(avg_launch_ms * 1e3, 3),
             "algorithmic_bytes_per_launch": BYTES_PER_CELL * cells}
 
@@ -338,17 +360,19 @@ def run_reference(args, ws, rank, local):
     like BornElasticGpu::forward/adjoint."""
     from oracle import oracle as O
     from elastic_isotropic_operators_b200 import synthetic
-    if not O.RefGpu.available("f"):
-        return {"impl": "reference", "unavailable": "oracle/_ref not built (reference tree absent at build time)"}
     if args.workload == "nl_312x520":
+        if not O.RefGpu.available("f"):
+            return {"impl": "reference", "unavailable": "oracle/_ref not built (reference tree absent at build time)"}
         return run_reference_nl(args)
     w = synthetic.born_600x1800(nts=args.nts, nshots=1, seed=2024)
+    if not O.RefGpu.available("f"):
+        return run_reference_port(args, w, "oracle/_ref not built (reference tree absent at build time)")
     if not O.RefGpu.born_supported(O.Case.from_workload(w).grid()):
-        return {"impl": "reference",
-                "unavailable": "the reference Born drivers index their Vx/Vz history with the 32-bit product "
-                               "its*nz*nx (kernelsGpuElastic.cu:1342), which overflows for nts*nz*nx >= 2^31 "
-                               "(here 4000*600*1800); on this grid they faulted with an illegal memory access at "
-                               "BornElasticGpuFunctions.cu:763, so they are not run again"}
+        return run_reference_port(
+            args, w, "the reference Born drivers index their Vx/Vz history with the 32-bit product its*nz*nx "
+                     "(kernelsGpuElastic.cu:1342), which overflows for nts*nz*nx >= 2^31 (here 4000*600*1800); "
+                     "on this grid they faulted with an illegal memory access at BornElasticGpuFunctions.cu:763, "
+                     "so they are not run again")
     orc = O.Oracle("f")
     c = O.Case.from_workload(w)
     g = c.grid()
@@ -383,6 +407,51 @@ def run_reference(args, ws, rank, local):
                              "sample": "reference CUDA drivers (elastic_iso_float, built for sm_100a) on the B200; "
                                        "the reference has no CPU implementation of this path"},
             "e2e": {"value": round(v, 3), "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def run_reference_port(args, w, why_not_gpu):
+    """CPU arm: the oracle (FP32 OpenMP restatement of the reference's algorithm) on
+    the box's host cores, all threads.  Each step is a bounded sample of the
+    workload: Born forward + Born adjoint of one shot of the 600x1800 grid with
+    nts=60 coarse samples."""
+    from oracle import oracle as O
+    nts_s = 60
+    c = O.Case.from_workload(w)
+    c.par["nts"] = nts_s
+    orc = O.Oracle("f")
+    g = c.grid()
+    med = orc.medium(c.ep, g["dts"], g["S"])
+    src = O._grids(orc, c, *c.src[0])
+    rec = O._grids(orc, c, *c.rec)
+    fine = O.born_sources(orc, c, g, med, src, w.source_signal()[:, :, :nts_s])
+    dm = O.born_model_slice(orc, g, med, w.extra["dmodel"])
+    data = [np.zeros((len(rec[O.FIELD_GRID[f]]["uniq"]), nts_s), np.float32) for f in range(5)]
+    grad = [np.zeros_like(a) for a in dm]
+
+    def step():
+        orc.born_prop(0, g, med, fine, dm, data, O._reg_pos(src), O._reg_pos(rec))
+        orc.born_prop(1, g, med, fine, grad, data, O._reg_pos(src), O._reg_pos(rec))
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    upd = 4.0 * (nts_s - 1) * g["S"] * (g["nz"] - 8) * (g["nx"] - 8) * args.steps
+    v = upd / dt / 1e9
+    sample = ("oracle FP32 Born forward + adjoint (2 propagations each), 1 shot, 600x1800 grid, nts=%d "
+              "(%d fine steps) per step, %d threads" % (nts_s, (nts_s - 1) * g["S"], O.num_threads()))
+    return {"impl": "reference", "metric": "Gcells/s", "value": round(v, 4), "unit": "Gcell-updates/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * dt / args.steps, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "born_600x1800: Born forward + adjoint, bounded sample (1 shot, nts=%d) of the "
+                                   "10-shot nts=%d workload" % (nts_s, w.nts), "nz": w.nz, "nx": w.nx},
+            "cpu_baseline": {"value": round(v, 4), "unit": "Gcell-updates/s", "cores": O.num_threads(),
+                             "kind": "port", "sample": sample},
+            "reference_gpu": {"unavailable": why_not_gpu},
+            "e2e": {"value": round(v, 4), "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 
 
@@ -435,7 +504,6 @@ def run_ours_nl(args, ws, rank, local):
     import ctypes
     import torch
     from elastic_isotropic_operators_b200 import _lib, prop, synthetic
-    from oracle import oracle as O
     w = synthetic.nl_312x520()
     dev = torch.device("cuda", local)
     w.par.set("iGpu", str(local))
@@ -443,29 +511,18 @@ def run_ours_nl(args, ws, rank, local):
     nl = prop.nonlinearPropElasticShotsGpu(w.elastic, w.par, *src, *rec)
     L = _lib.lib()
     ctx = nl.ctx
+    pin_kernel(L, ctx, args)
+    est = torch.cuda.ExternalStream(L.eio_ctx_stream(ctx), device=dev)   # the engine's launch stream
     fine_steps, cells = ctypes.c_longlong(), ctypes.c_longlong()
     _lib.check(L.eio_ctx_counts(ctx, ctypes.byref(fine_steps), ctypes.byref(cells)))
     fine_steps, cells = fine_steps.value, cells.value
     upd = float(fine_steps * cells)
-    # regular-grid sources exactly as the operator prepares them
-    orc = O.Oracle("f")
-    c = O.Case.from_workload(w)
-    g = c.grid()
-    med = orc.medium(c.ep, g["dts"], g["S"])
-    sg = O._grids(orc, c, *c.src[0])
-    rg = O._grids(orc, c, *c.rec)
-    reg = []
-    sig = w.source_signal()
-    for f in range(5):
-        G = sg[O.FIELD_GRID[f]]
-        r = np.zeros((len(G["uniq"]), g["nts"]), np.float32)
-        orc.sinterp_apply(G, 1, 0, r, np.ascontiguousarray(sig[f]))
-        reg.append(r)
-    O._scale_sources(orc, g, med, sg, reg)
+    # regular-grid sources prepared by the library's own host code
+    reg, sp, rp = nl.prepareShot(0, w.source_signal())
     m_dev = [torch.from_numpy(a).to(dev) for a in reg]
-    d_dev = [torch.zeros((len(rg[O.FIELD_GRID[f]]["uniq"]), g["nts"]), device=dev) for f in range(5)]
-    sp = [np.ascontiguousarray(G["uniq"], np.int32) for G in sg]
-    rp = [np.ascontiguousarray(G["uniq"], np.int32) for G in rg]
+    d_dev = [torch.zeros((len(rp[prop._FIELD_GRID[f]]), w.nts), device=dev) for f in range(5)]
+    sp = [np.ascontiguousarray(a, np.int32) for a in sp]
+    rp = [np.ascontiguousarray(a, np.int32) for a in rp]
     args_c = (_lib.ptr_array([t.data_ptr() for t in m_dev]), _lib.ptr_array([t.data_ptr() for t in d_dev]),
               _lib.ptr_array([a.ctypes.data for a in sp]), (ctypes.c_int * 4)(*[len(a) for a in sp]),
               _lib.ptr_array([a.ctypes.data for a in rp]), (ctypes.c_int * 4)(*[len(a) for a in rp]))
@@ -487,9 +544,9 @@ def run_ours_nl(args, ws, rank, local):
         flush.zero_()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
-        ev0.record()
+        ev0.record(est)
         step()
-        ev1.record()
+        ev1.record(est)
         torch.cuda.synchronize()
         t_ms += ev0.elapsed_time(ev1)
     clk = clocks.stop()
@@ -509,6 +566,8 @@ def run_ours_nl(args, ws, rank, local):
     t_e2e = max_over_ranks(ws, time.perf_counter() - t0)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
+        from oracle import oracle as O
+        orc, c = O.Oracle("f"), O.Case.from_workload(w)
         t0 = time.perf_counter()
         O.nl_forward(orc, c, model.getNdArray())
         dt = time.perf_counter() - t0
@@ -526,7 +585,7 @@ def run_ours_nl(args, ws, rank, local):
                     "d2h_bytes_per_step": int(sum(4 * t.numel() for t in d_dev))},
             "roofline": {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(ach / peak, 4), "traffic": None, "peak_source": pk,
-                         "avg_launch_us": round(avg * 1e3, 3)},
+                         "kernel": kernel_name(L, ctx), "avg_launch_us": round(avg * 1e3, 3)},
             "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches.value)}
 
 

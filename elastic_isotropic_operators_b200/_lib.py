@@ -88,6 +88,7 @@ _SIGS = {
     "eio_born_adj_reg_dev": (I, [P, P, P, P, P, IP, P, IP]),
     "eio_born_prepare_sources": (I, [P, FP, P, P]),
     "eio_born_prepare_model": (I, [P, FP, P]),
+    "eio_nl_prepare_sources": (I, [P, FP, P, P]),
     "eio_nl_fwd_noalloc": (I, [ctypes.POINTER(FdParams), P, P, P, P, IP, P, IP, P]),
     "eio_nl_forward": (I, [P, I, I, I, FP, FP, P, P, I]),
     "eio_nl_adjoint": (I, [P, I, I, I, FP, FP, P, P, I]),

@@ -91,14 +91,16 @@ struct Engine {
     CUtensorMap mwf_halo[10], mwf_int[10], mpar_halo[5], mpar_int[5];
     DBuf err;
     // launch statistics (bench instrumentation)
-    long long launches = 0, step_launches = 0;
+    long long launches = 0, step_launches = 0, sampled = 0;
     double step_ms = 0.0;
     bool stats = false;
     std::vector<cudaEvent_t> ev;
     size_t ev_used = 0;
 };
 
-// Per-launch CUDA-event timing of the fused step kernel (only when enabled).
+// CUDA-event timing of every STATS_PERIOD-th launch of the fused step kernel
+// (only when enabled); sampling keeps the event records out of most gaps.
+constexpr long long STATS_PERIOD = 16;
 static void stats_flush(Engine* e) {
     if (!e->stats || e->ev_used == 0) return;
     EIO_CUDA(cudaStreamSynchronize(e->st));
@@ -213,8 +215,8 @@ void engine_stats(Engine* e, int enable, int reset, long long* launches, long lo
     stats_flush(e);
     if (launches) *launches = e->launches;
     if (step_launches) *step_launches = e->step_launches;
-    if (step_ms) *step_ms = e->step_ms;
-    if (reset) { e->launches = 0; e->step_launches = 0; e->step_ms = 0.0; }
+    if (step_ms) *step_ms = e->sampled ? e->step_ms * (double)e->step_launches / (double)e->sampled : 0.0;
+    if (reset) { e->launches = 0; e->step_launches = 0; e->sampled = 0; e->step_ms = 0.0; }
     if (enable >= 0) e->stats = enable != 0;
 }
 
@@ -384,10 +386,14 @@ static void launch_sweep(Engine* e, const StepArgs& a, int cur) {
 
 template <int DIR, int EPI>
 static void launch_step(Engine* e, StepArgs& a, int cur) {
-    stats_mark(e);
+    const bool timed = e->stats && e->step_launches % STATS_PERIOD == 0;
+    if (timed) stats_mark(e);
     if (e->kind == 0) k_step<DIR, EPI><<<e->ntiles, NT, 0, e->st>>>(a);
     else launch_sweep<DIR, EPI>(e, a, cur);
-    stats_mark(e);
+    if (timed) {
+        stats_mark(e);
+        e->sampled++;
+    }
     e->launches++;
     e->step_launches++;
 }
@@ -579,9 +585,9 @@ static void launch_imaging(Engine* e, int adj, int its, float* const dm[5], floa
     for (int i = 0; i < 4; i++) { ia.cz[i] = e->zc[i]; ia.cx[i] = e->xc[i]; }
     ia.dts_inv = e->dts_inv;
     for (int f = 0; f < 5; f++) { ia.dm[f] = dm[f]; ia.ss[f] = ss[f]; }
-    dim3 b(256), g((e->nz - 2 * FAT + 255) / 256, e->nx - 2 * FAT);
-    if (adj) k_imaging<1><<<g, b, 0, e->st>>>(ia);
-    else k_imaging<0><<<g, b, 0, e->st>>>(ia);
+    const int ntiles = ((e->nz - 2 * FAT + TZ - 1) / TZ) * ((e->nx - 2 * FAT) / TX);
+    if (adj) k_imaging<1><<<ntiles, NT, 0, e->st>>>(ia);
+    else k_imaging<0><<<ntiles, NT, 0, e->st>>>(ia);
     e->launches++;
 }
 

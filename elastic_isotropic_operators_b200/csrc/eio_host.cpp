@@ -754,6 +754,29 @@ EIO_API int eio_born_prepare_sources(eio_ctx* c, const float* signal, eio_sinter
     });
 }
 
+EIO_API int eio_nl_prepare_sources(eio_ctx* c, const float* model, eio_sinterp* const src[4], float* const out[5]) {
+    return guarded([&] {
+        if (!c || !model || !src || !out) throw Error(EIO_ERR_ARG, "null argument");
+        ShotGrids g;
+        for (int k = 0; k < 4; k++) {
+            if (!src[k]) throw Error(EIO_ERR_ARG, "null interpolator");
+            g.s[k] = &src[k]->s;
+            g.r[k] = &src[k]->s;
+        }
+        const int nts = c->fd.p.nts;
+        check_nt(g, nts);
+        const int nsi = g.s[0]->nIrreg;
+        std::vector<float> reg[5];
+        for (int f = 0; f < 5; f++) {
+            const SInterp& s = *g.s[kFG[f]];
+            reg[f].assign((size_t)s.nReg * nts, 0.f);
+            sinterp_adjoint(s, false, reg[f].data(), model + (size_t)f * nsi * nts);
+        }
+        scale_sources(c->fd, g, reg, nts);
+        for (int f = 0; f < 5; f++) std::copy(reg[f].begin(), reg[f].end(), out[f]);
+    });
+}
+
 EIO_API int eio_born_prepare_model(eio_ctx* c, const float* model, float* const out[5]) {
     return guarded([&] {
         if (!c || !model || !out) throw Error(EIO_ERR_ARG, "null argument");

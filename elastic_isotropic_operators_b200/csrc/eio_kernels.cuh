@@ -433,55 +433,102 @@ struct ImagingArgs {
     float* ss[5];   // fwd: written; adj: read
 };
 
-__device__ __forceinline__ float dminus(const float* f, long long i, long long s, const float* c)
-{
-    return c[0] * (f[i] - f[i - s]) + c[1] * (f[i + s] - f[i - 2 * s]) + c[2] * (f[i + 2 * s] - f[i - 3 * s]) +
-           c[3] * (f[i + 3 * s] - f[i - 4 * s]);
-}
-__device__ __forceinline__ float dplus(const float* f, long long i, long long s, const float* c)
-{
-    return c[0] * (f[i + s] - f[i]) + c[1] * (f[i + 2 * s] - f[i - s]) + c[2] * (f[i + 3 * s] - f[i - 2 * s]) +
-           c[3] * (f[i + 4 * s] - f[i - 3 * s]);
-}
-
+// Born secondary sources (ADJ=0, imagingElaFwdGpu, prop/src/kernelsGpuElastic.cu:1381)
+// and imaging condition (ADJ=1, imagingElaAdjGpu, kernelsGpuElastic.cu:1538) at
+// coarse sample its.  64x16-cell tiles, 256 threads (one float4 of z x one column
+// each); the snapshot at its is staged with its 4-cell halo in shared memory for
+// the staggered derivatives, the neighbouring snapshots give the time difference.
 template <int ADJ>
-__global__ void __launch_bounds__(256) k_imaging(ImagingArgs a)
+__global__ void __launch_bounds__(NT) k_imaging(ImagingArgs a)
 {
-    const int iz = FAT + blockIdx.x * blockDim.x + threadIdx.x;
-    const int ix = FAT + blockIdx.y;
-    if (iz >= a.nz - FAT) return;
+    __shared__ __align__(16) float sm[2 * SMEM_FIELD];
+    const int tid = threadIdx.x;
+    const int ntz = (a.nz - 2 * FAT + TZ - 1) / TZ;
+    const int bz = blockIdx.x % ntz, bx = blockIdx.x / ntz;
+    const int z0 = FAT + bz * TZ, x0 = FAT + bx * TX;
     const long long nz = a.nz;
-    const long long i = (long long)ix * nz + iz;
-    const float* vx = a.Wvx + (long long)a.its * a.wstride;
-    const float* vz = a.Wvz + (long long)a.its * a.wstride;
-    const float dvx_dx = dplus(vx, i, nz, a.cx);
-    const float dvz_dz = dplus(vz, i, 1, a.cz);
-    const float dmix = dminus(vx, i, 1, a.cz) + dminus(vz, i, nz, a.cx);
-    float tx, tz;
-    if (a.its == 0) {
-        tx = -a.Wvx[a.wstride + i];
-        tz = -a.Wvz[a.wstride + i];
-    } else if (a.its == a.nts - 1) {
-        tx = a.Wvx[(long long)(a.its - 1) * a.wstride + i];
-        tz = a.Wvz[(long long)(a.its - 1) * a.wstride + i];
-    } else {
-        tx = a.Wvx[(long long)(a.its - 1) * a.wstride + i] - a.Wvx[(long long)(a.its + 1) * a.wstride + i];
-        tz = a.Wvz[(long long)(a.its - 1) * a.wstride + i] - a.Wvz[(long long)(a.its + 1) * a.wstride + i];
+    const float* vxc = a.Wvx + (long long)a.its * a.wstride;
+    const float* vzc = a.Wvz + (long long)a.its * a.wstride;
+    {
+        const int nq = SZ / 4;
+        for (int q = tid; q < nq * SX; q += NT) {
+            const int lx = q / nq, lz4 = (q % nq) * 4;
+            const int gz = z0 - FAT + lz4, gx = x0 - FAT + lx;
+            float4 u = make_float4(0.f, 0.f, 0.f, 0.f), v = u;
+            if (gz < a.nz) {
+                const long long gi = (long long)gx * nz + gz;
+                u = ldg4(vxc + gi);
+                v = ldg4(vzc + gi);
+            }
+            st4(sm + lx * SZ + lz4, u);
+            st4(sm + SMEM_FIELD + lx * SZ + lz4, v);
+        }
+    }
+    __syncthreads();
+    const int tzi = tid % NTZ, txi = tid / NTZ;
+    const int lz = FAT + 4 * tzi, lx = FAT + txi;
+    const int gz = z0 + 4 * tzi;
+    if (gz >= a.nz - FAT) return;
+    const long long gi = (long long)(x0 + txi) * nz + gz;
+    const float* svx = sm;
+    const float* svz = sm + SMEM_FIELD;
+    float4 q[9];
+    float w[12];
+#pragma unroll
+    for (int m = 0; m < 9; m++) q[m] = ld4(svx + (lx - FAT + m) * SZ + lz);
+    const float4 dvx_dx = dpx(q, 4, a.cx);
+    zwin(svx, lx, lz, w);
+    const float4 dvx_dz = dmz(w, a.cz);
+#pragma unroll
+    for (int m = 0; m < 9; m++) q[m] = ld4(svz + (lx - FAT + m) * SZ + lz);
+    const float4 dvz_dx = dmx(q, 4, a.cx);
+    zwin(svz, lx, lz, w);
+    const float4 dvz_dz = dpz(w, a.cz);
+    float4 tx, tz;
+    {
+        const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 xo = a.its > 0 ? ldg4(a.Wvx + (long long)(a.its - 1) * a.wstride + gi) : zero;
+        const float4 zo = a.its > 0 ? ldg4(a.Wvz + (long long)(a.its - 1) * a.wstride + gi) : zero;
+        const float4 xn = a.its < a.nts - 1 ? ldg4(a.Wvx + (long long)(a.its + 1) * a.wstride + gi) : zero;
+        const float4 zn = a.its < a.nts - 1 ? ldg4(a.Wvz + (long long)(a.its + 1) * a.wstride + gi) : zero;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            // one-sided at the ends like the reference: -W[its+1] at its = 0, W[its-1] at nts-1
+            at(tx, j) = (a.its == 0) ? -at(xn, j) : (a.its == a.nts - 1) ? at(xo, j) : at(xo, j) - at(xn, j);
+            at(tz, j) = (a.its == 0) ? -at(zn, j) : (a.its == a.nts - 1) ? at(zo, j) : at(zo, j) - at(zn, j);
+        }
     }
     if (!ADJ) {
-        a.ss[0][i] = a.dm[0][i] * tx * a.dts_inv;
-        a.ss[1][i] = a.dm[1][i] * tz * a.dts_inv;
-        const float dl = a.dm[2][i], dmu = a.dm[3][i];
-        a.ss[2][i] = dl * (dvx_dx + dvz_dz) + 2.0f * dmu * dvx_dx;
-        a.ss[3][i] = dl * (dvx_dx + dvz_dz) + 2.0f * dmu * dvz_dz;
-        a.ss[4][i] = a.dm[4][i] * dmix;
+        const float4 d0 = ldg4(a.dm[0] + gi), d1 = ldg4(a.dm[1] + gi), dl = ldg4(a.dm[2] + gi),
+                     du = ldg4(a.dm[3] + gi), d4 = ldg4(a.dm[4] + gi);
+        float4 s0, s1, s2, s3, s4;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            at(s0, j) = at(d0, j) * at(tx, j) * a.dts_inv;
+            at(s1, j) = at(d1, j) * at(tz, j) * a.dts_inv;
+            const float dvx = at(dvx_dx, j), dvz = at(dvz_dz, j);
+            at(s2, j) = at(dl, j) * (dvx + dvz) + 2.0f * at(du, j) * dvx;
+            at(s3, j) = at(dl, j) * (dvx + dvz) + 2.0f * at(du, j) * dvz;
+            at(s4, j) = at(d4, j) * (at(dvx_dz, j) + at(dvz_dx, j));
+        }
+        st4(a.ss[0] + gi, s0); st4(a.ss[1] + gi, s1); st4(a.ss[2] + gi, s2);
+        st4(a.ss[3] + gi, s3); st4(a.ss[4] + gi, s4);
     } else {
-        const float s0 = a.ss[0][i], s1 = a.ss[1][i], s2 = a.ss[2][i], s3 = a.ss[3][i], s4 = a.ss[4][i];
-        a.dm[0][i] += s0 * tx * a.dts_inv;
-        a.dm[1][i] += s1 * tz * a.dts_inv;
-        a.dm[2][i] += (s2 + s3) * (dvx_dx + dvz_dz);
-        a.dm[3][i] += 2.0f * (dvx_dx * s2 + dvz_dz * s3);
-        a.dm[4][i] += s4 * dmix;
+        const float4 s0 = ldg4(a.ss[0] + gi), s1 = ldg4(a.ss[1] + gi), s2 = ldg4(a.ss[2] + gi),
+                     s3 = ldg4(a.ss[3] + gi), s4 = ldg4(a.ss[4] + gi);
+        float4 d0 = ld4(a.dm[0] + gi), d1 = ld4(a.dm[1] + gi), d2 = ld4(a.dm[2] + gi), d3 = ld4(a.dm[3] + gi),
+               d4 = ld4(a.dm[4] + gi);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const float dvx = at(dvx_dx, j), dvz = at(dvz_dz, j);
+            at(d0, j) += at(s0, j) * at(tx, j) * a.dts_inv;
+            at(d1, j) += at(s1, j) * at(tz, j) * a.dts_inv;
+            at(d2, j) += (at(s2, j) + at(s3, j)) * (dvx + dvz);
+            at(d3, j) += 2.0f * (dvx * at(s2, j) + dvz * at(s3, j));
+            at(d4, j) += at(s4, j) * (at(dvx_dz, j) + at(dvz_dx, j));
+        }
+        st4(a.dm[0] + gi, d0); st4(a.dm[1] + gi, d1); st4(a.dm[2] + gi, d2);
+        st4(a.dm[3] + gi, d3); st4(a.dm[4] + gi, d4);
     }
 }
 

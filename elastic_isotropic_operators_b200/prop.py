@@ -312,6 +312,19 @@ class nonlinearPropElasticShotsGpu(_ElasticOp):
         if mm is not m:
             m[...] = mm
 
+    def prepareShot(self, iExp, model):
+        """Regular-grid inputs of shot iExp for the single-shot eio_nl_fwd_reg_dev
+        entry point: the irregular source traces ``model`` [5][nSrc][nts] spread and
+        scaled onto the regular grid (5 arrays [nSrcReg(grid)][nts]) and the source /
+        receiver position lists (grid order center, x, z, xz)."""
+        src = [g[iExp] for g in self.src]
+        rec = [g[0 if self.nRecGeom == 1 else iExp] for g in self.rec]
+        m = np.ascontiguousarray(_arr(model).reshape(5, self.nSrcIrreg, self.fd.nts))
+        reg = [np.zeros((src[_FIELD_GRID[f]].nDeviceReg, self.fd.nts), np.float32) for f in range(5)]
+        check(self._L.eio_nl_prepare_sources(self._ctx, fptr(m), _lib.ptr_array([g.handle.value for g in src]),
+                                             _lib.ptr_array([a.ctypes.data for a in reg])))
+        return reg, [g.getRegPosUnique() for g in src], [g.getRegPosUnique() for g in rec]
+
     def modelSpace(self, nModelExp=1):
         t = axis(self.fd.nts, self.fd.ots, self.fd.dts)
         return floatVector(hypercube(axes=[t, axis(self.nSrcIrreg), axis(5), axis(nModelExp)]))

@@ -1,0 +1,124 @@
+"""Shot-parallel execution: one process per GPU under torch.distributed.
+
+The reference spreads the shots of one operator call over the GPUs of a single
+process with an OpenMP loop, one thread per GPU and ``schedule(dynamic,1)``
+(F/src/BornElasticShotsGpu.cpp:178-207 forward, :275-306 adjoint;
+F/src/nonlinearPropElasticShotsGpu.cpp the same), writes each shot's data
+slice straight into the shared data vector, and stacks the per-GPU model
+slices of the adjoint on the host (BornElasticShotsGpu.cpp:312-323).
+
+Here every rank owns a fixed contiguous block of shots (``shot_partition``),
+runs them through its own single-GPU operator, and the stacking becomes one
+all-reduce of the model vector over the process group (NCCL between GPUs,
+gloo on CPU).  Shots are independent, so the forward needs no exchange at all;
+``gather_data`` assembles the full data vector only when a caller asks for it.
+"""
+import numpy as np
+
+__all__ = ["shot_partition", "local_vectors", "stack_model", "gather_data", "ShotParallel"]
+
+
+def shot_partition(nExp, world, rank):
+    """Contiguous block of shot indices owned by ``rank``: the first
+    ``nExp % world`` ranks take one shot more than the others."""
+    if nExp < 0 or world < 1 or not 0 <= rank < world:
+        raise ValueError("bad shot partition request (nExp=%d, world=%d, rank=%d)" % (nExp, world, rank))
+    base, extra = divmod(nExp, world)
+    start = rank * base + min(rank, extra)
+    return range(start, start + base + (1 if rank < extra else 0))
+
+
+def local_vectors(vectors, shots):
+    """Per-shot list (length nExp) -> the entries of ``shots``; a list of length
+    one (a geometry or signal shared by every shot) is kept as it is."""
+    vectors = list(vectors)
+    if len(vectors) == 1:
+        return vectors
+    return [vectors[e] for e in shots]
+
+
+def _group_device(group):
+    import torch
+    import torch.distributed as dist
+    if dist.get_backend(group) == "nccl":
+        return torch.device("cuda", torch.cuda.current_device())
+    return torch.device("cpu")
+
+
+def stack_model(model, group=None):
+    """Sum a model-space array (numpy, float32) over the ranks of ``group`` in
+    place: the host stacking of the reference's per-GPU model slices."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_initialized() or dist.get_world_size(group) == 1:
+        return model
+    dev = _group_device(group)
+    t = torch.from_numpy(np.ascontiguousarray(model, np.float32)).to(dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    model[...] = t.cpu().numpy().reshape(model.shape)
+    return model
+
+
+def gather_data(local, nExp, group=None):
+    """Assemble the full data vector [nExp][...] from each rank's block of
+    shots [len(shot_partition)][...]; every rank receives the whole vector."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_initialized() or dist.get_world_size(group) == 1:
+        return np.array(local, np.float32, copy=True)
+    world = dist.get_world_size(group)
+    mine = dist.get_rank(group)
+    dev = _group_device(group)
+    cap = len(shot_partition(nExp, world, 0))        # the largest block
+    shape = tuple(local.shape[1:])
+    buf = torch.zeros((cap,) + shape, dtype=torch.float32, device=dev)
+    n = len(shot_partition(nExp, world, mine))
+    if n:
+        buf[:n] = torch.from_numpy(np.ascontiguousarray(local, np.float32)).to(dev)
+    parts = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(parts, buf, group=group)
+    out = np.zeros((nExp,) + shape, np.float32)
+    for r in range(world):
+        sh = shot_partition(nExp, world, r)
+        if len(sh):
+            out[sh.start:sh.stop] = parts[r][:len(sh)].cpu().numpy()
+    return out
+
+
+class ShotParallel:
+    """An operator over nExp shots split across the ranks of a process group.
+
+    ``make_local(shots)`` builds this rank's operator over the shot indices
+    ``shots`` (for instance ``BornElasticShotsGpu`` constructed with
+    ``local_vectors`` of the geometry and signal lists); it is not called when
+    the rank owns no shot.  ``forward``/``adjoint`` take this rank's data
+    block [len(shots)][5][nRec][nts].  When ``stacked`` (Born model, or a
+    nonlinear source signal shared by every shot) the adjoint's model is summed
+    over the ranks; otherwise each rank keeps its own model block.
+    """
+
+    def __init__(self, make_local, nExp, group=None, stacked=True):
+        import torch.distributed as dist
+        self.group = group
+        self.world = dist.get_world_size(group) if dist.is_initialized() else 1
+        self.rank = dist.get_rank(group) if dist.is_initialized() else 0
+        self.nExp = nExp
+        self.shots = shot_partition(nExp, self.world, self.rank)
+        self.stacked = stacked
+        self.local = make_local(self.shots) if len(self.shots) else None
+
+    def forward(self, add, model, data):
+        if self.local is not None:
+            self.local.forward(add, model, data)
+
+    def adjoint(self, add, model, data):
+        m = model.getNdArray() if hasattr(model, "getNdArray") else model
+        part = np.zeros_like(m)
+        if self.local is not None:
+            self.local.adjoint(False, part, data)
+        if self.stacked:
+            stack_model(part, self.group)
+        if add:
+            m += part
+        else:
+            m[...] = part

@@ -142,7 +142,8 @@ int eio_ctx_set_kernel(eio_ctx *c, int kind, int tz, int cw, int cpr);
 int eio_ctx_get_kernel(const eio_ctx *c, int *kind, int *tz, int *cw, int *cpr);
 int eio_ctx_autotune(eio_ctx *c, int *kind, int *tz, int *cw, int *cpr);
 /* Instrumentation (no reference counterpart): kernel launch counters and,
- * when enabled, CUDA-event timing of every fused step-kernel launch.
+ * when enabled, CUDA-event timing of every 16th fused step-kernel launch;
+ * stepMs is the sampled mean duration times stepLaunches.
  * enable: 1 on, 0 off, -1 unchanged; reset: zero the counters after reading. */
 int eio_ctx_stats(eio_ctx *c, int enable, int reset, long long *launches, long long *stepLaunches,
                   double *stepMs);
@@ -214,6 +215,12 @@ int eio_born_adjoint(eio_ctx *c, int add, int nExp, float *model, const float *d
  *   5 perturbation grids [nx][nz] (F/src/BornElasticShotsGpu.cpp:107-150). */
 int eio_born_prepare_sources(eio_ctx *c, const float *signal, eio_sinterp *const src[4], float *const out[5]);
 int eio_born_prepare_model(eio_ctx *c, const float *model, float *const out[5]);
+/* Nonlinear host preparation of one shot for eio_nl_fwd_reg_dev: irregular
+ * source traces [5][nSrcIrreg][nts] -> 5 regular traces [nSrcReg(grid)][nts],
+ * spread by the adjoint of the source interpolators and scaled by 2*dtw (or
+ * the staggered buoyancy for vx, vz) and 1/(dx*dz), as
+ * nonlinearPropElasticGpu::forward does (F/src/nonlinearPropElasticGpu.cpp:116-144). */
+int eio_nl_prepare_sources(eio_ctx *c, const float *model, eio_sinterp *const src[4], float *const out[5]);
 
 /* ---------------------------------------------------------------------------
  * Allocation-free nonlinear forward propagation.  No counterpart in the

@@ -1,0 +1,25 @@
+"""The bench's reference arm on CPU: the JSON line it prints for the Born
+workload, where the reference's own CUDA Born drivers cannot run (their 32-bit
+history index overflows at that size) and the oracle port stands in on the
+host cores."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_reference_arm_prints_cpu_port_line():
+    env = dict(os.environ, OMP_NUM_THREADS=str(min(os.cpu_count() or 1, 8)))
+    p = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0"],
+                       cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    line = [x for x in p.stdout.splitlines() if x.startswith("{")][-1]
+    d = json.loads(line)
+    assert d["impl"] == "reference"
+    assert d["metric"] == "Gcells/s" and d["unit"] == "Gcell-updates/s" and d["higher_is_better"] is True
+    assert d["value"] > 0
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    assert "2^31" in d["reference_gpu"]["unavailable"]

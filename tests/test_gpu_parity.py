@@ -140,6 +140,37 @@ def test_born_operator_vs_oracle(w):
     assert O.rel_l2(g.getNdArray(), want64) < TOL64
 
 
+def test_prepare_shot_matches_oracle_host_prep(w):
+    """Host preparation the single-shot device entry points are fed with:
+    nonlinear spread + scaling of the source traces, Born fine-time sources and
+    the staggered model perturbation; the oracle restates the same steps."""
+    src, rec = w.geometry()
+    sig = w.source_signal()
+    orc = O.Oracle("f")
+    c = O.Case.from_workload(w)
+    g = c.grid()
+    med = orc.medium(c.ep, g["dts"], g["S"])
+    sg = O._grids(orc, c, *c.src[1])
+    nl = prop.nonlinearPropElasticShotsGpu(w.elastic, w.par, *src, *rec)
+    reg, sp, rp = nl.prepareShot(1, sig)
+    want = []
+    for f in range(5):
+        G = sg[O.FIELD_GRID[f]]
+        r = np.zeros((len(G["uniq"]), g["nts"]), np.float32)
+        orc.sinterp_apply(G, 1, 0, r, np.ascontiguousarray(sig[f]))
+        want.append(r)
+    O._scale_sources(orc, g, med, sg, want)
+    assert rel(reg, want) < 1e-6
+    for k in range(4):
+        assert np.array_equal(sp[k], sg[k]["uniq"])
+    born = prop.BornElasticShotsGpu(w.elastic, w.par, [sig], *src, *rec)
+    fine, sp2, _ = born.prepareShot(1)
+    want_fine = O.born_sources(orc, c, g, med, sg, sig.reshape(5, 1, g["nts"]))
+    assert rel(fine, want_fine) < 1e-6
+    dm = born.prepareModel(w.extra["dmodel"])
+    assert rel(dm, O.born_model_slice(orc, g, med, w.extra["dmodel"])) < 1e-6
+
+
 def test_dot_products(w):
     nl, src, rec = _ops(w)
     assert nl.dotTest(False, 1e-5), nl.lastDotTest
