@@ -45,8 +45,9 @@ def parse():
     ap.add_argument("--nts", type=int, default=4000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--kernel", type=int, default=-1, choices=[-1, 0, 1],
-                    help="-1: autotune (default); 0: tile kernel k_step; 1: TMA sweep kernel k_sweep")
+    ap.add_argument("--kernel", type=int, default=-1, choices=[-1, 0, 1, 2, 3, 4],
+                    help="-1: autotune (default); 0: tile kernel k_step; 1: TMA sweep kernel k_sweep; "
+                         "2: persistent TMA tile kernel k_tile; 3: k_step at 4 CTAs/SM; 4: split-field k_split")
     return ap.parse_args()
 
 
@@ -141,6 +142,12 @@ def kernel_name(L, ctx):
     kind, tz, cw, cpr = (x.value for x in v)
     if kind == 0:
         return "k_step (fused 5-field update, 64x16 tiles)"
+    if kind == 2:
+        return "k_tile (fused 5-field update, persistent, 64x16 tiles staged by TMA)"
+    if kind == 3:
+        return "k_step (fused 5-field update, 64x16 tiles, 4 CTAs/SM)"
+    if kind == 4:
+        return "k_split (fused 5-field update, 64x16 tiles, two threads per float4)"
     return "k_sweep (fused 5-field update, TMA x-sweep, tz=%d cw=%d cpr=%d)" % (tz, cw, cpr)
 
 

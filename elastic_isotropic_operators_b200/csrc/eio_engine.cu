@@ -20,6 +20,7 @@
 #include "eio_internal.h"
 #include "eio_kernels.cuh"
 #include "eio_sweep.cuh"
+#include "eio_tile.cuh"
 
 namespace eio {
 
@@ -66,6 +67,7 @@ struct PointList {
 
 struct Engine {
     int device = 0;
+    int nsm = 148;          // SM count of the device
     cudaStream_t st = nullptr;
     int nz = 0, nx = 0;
     long long n = 0;
@@ -83,12 +85,17 @@ struct Engine {
     bool w_clean = false;   // history zeroed and only written by single stores since
     // step-kernel choice: kind 0 = shared-memory tile kernel (k_step),
     // kind 1 = TMA x-sweep (k_sweep) with strip height tz, chunk width cw and
-    // cpr chunks per CTA
+    // cpr chunks per CTA, kind 2 = persistent TMA-pipelined tile kernel (k_tile),
+    // kind 3 = k_step at 4 CTAs per SM, kind 4 = two threads per float4 (k_split)
     int kind = 1, tz = 64, cw = 8, cpr = 8;
     bool tuned = false;
     // tensor maps of the sweep kernel (valid for mtz/mcw)
     int mtz = -1, mcw = -1;
     CUtensorMap mwf_halo[10], mwf_int[10], mpar_halo[5], mpar_int[5];
+    // tensor maps of the TMA tile kernel (kind 2), valid for the buffers in tbase
+    CUtensorMap twf_halo[10], twf_int[10], tpar_halo[5], tpar_int[5];
+    const void* tbase[15] = {};
+    int tile_ctas[2] = {0, 0};    // persistent k_tile grid per direction (0 = not yet queried)
     DBuf err;
     // launch statistics (bench instrumentation)
     long long launches = 0, step_launches = 0, sampled = 0;
@@ -170,6 +177,7 @@ Engine* engine_create(int device, const FdParam& fd) {
     Engine* e = new Engine();
     try {
         e->device = device;
+        EIO_CUDA(cudaDeviceGetAttribute(&e->nsm, cudaDevAttrMultiProcessorCount, device));
         e->nz = fd.p.nz;
         e->nx = fd.p.nx;
         e->n = (long long)e->nz * e->nx;
@@ -220,12 +228,15 @@ void engine_stats(Engine* e, int enable, int reset, long long* launches, long lo
     if (enable >= 0) e->stats = enable != 0;
 }
 
+// every kind but the sweep (1) uses the 64x16 tiles of k_step and their numbering
+static bool tiled(int kind) { return kind != 1; }
+
 // tile geometry the sparse point lists are bucketed with
 struct TileGeom {
     int tz, tx, ntz;
 };
 static TileGeom tile_geom(const Engine* e) {
-    if (e->kind == 0) return {TZ, TX, e->ntz};
+    if (tiled(e->kind)) return {TZ, TX, e->ntz};
     return {e->tz, e->cw, (e->nz - 2 * FAT + e->tz - 1) / e->tz};
 }
 
@@ -248,8 +259,8 @@ static void build_points(const Engine* e, const int* const pos[4], const int npo
             PointEntry pe;
             pe.key = (f << 16) | (((ix - FAT) % tg.tx) << 8) | ((iz - FAT) % tg.tz);
             pe.col = k;
-            // k_step numbers tiles z-fastest, k_sweep strip-major
-            tmp.push_back({e->kind == 0 ? bx * tg.ntz + bz : bz * nchunks + bx, pe});
+            // k_step / k_tile number tiles z-fastest, k_sweep strip-major
+            tmp.push_back({tiled(e->kind) ? bx * tg.ntz + bz : bz * nchunks + bx, pe});
         }
     }
     pl.any = !tmp.empty();
@@ -384,11 +395,64 @@ static void launch_sweep(Engine* e, const StepArgs& a, int cur) {
     else throw Error(EIO_ERR_ARG, "unsupported sweep configuration");
 }
 
+static void ensure_tile_maps(Engine* e) {
+    bool same = true;
+    for (int b = 0; b < 10; b++) same = same && e->tbase[b] == e->wf[b].p;
+    for (int f = 0; f < 5; f++) same = same && e->tbase[10 + f] == e->par[f].p;
+    if (same) return;
+    for (int b = 0; b < 10; b++) {
+        e->twf_halo[b] = make_map(e->wf[b].f(), e->nz, e->nx, SZ, SX);
+        e->twf_int[b] = make_map(e->wf[b].f(), e->nz, e->nx, TZ, TX);
+        e->tbase[b] = e->wf[b].p;
+    }
+    for (int f = 0; f < 5; f++) {
+        e->tpar_halo[f] = make_map(e->par[f].f(), e->nz, e->nx, SZ, SX);
+        e->tpar_int[f] = make_map(e->par[f].f(), e->nz, e->nx, TZ, TX);
+        e->tbase[10 + f] = e->par[f].p;
+    }
+}
+
+template <int DIR, int EPI>
+static void launch_tile(Engine* e, const StepArgs& a, int cur) {
+    ensure_tile_maps(e);
+    static unsigned attr_done = 0;          // one bit per device
+    const unsigned bit = 1u << (e->device & 31);
+    if (!(attr_done & bit)) {
+        EIO_CUDA(cudaFuncSetAttribute(k_tile<DIR, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)TileLayout<DIR>::BYTES));
+        EIO_CUDA(cudaFuncSetAttribute(k_tile<DIR, EPI>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        attr_done |= bit;
+    }
+    if (!e->tile_ctas[DIR]) {
+        int per_sm = 0;
+        EIO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile<DIR, EPI>, NT,
+                                                               TileLayout<DIR>::BYTES));
+        if (per_sm < 1) throw Error(EIO_ERR_CUDA, "the TMA tile kernel does not fit on an SM");
+        e->tile_ctas[DIR] = per_sm * e->nsm;
+    }
+    TileArgs t;
+    memset(&t, 0, sizeof(t));
+    const int oc = cur * 5, cc = (1 - cur) * 5;   // buffer of the old / current level
+    for (int f = 0; f < 5; f++) {
+        t.tc[f] = e->twf_halo[cc + f];
+        t.to[f] = e->twf_int[oc + f];
+        t.tp[f] = DIR == 0 ? e->tpar_int[f] : e->tpar_halo[f];
+    }
+    t.s = a;
+    t.ntiles = e->ntiles;
+    t.err = static_cast<int*>(e->err.p);
+    const int grid = std::min(e->ntiles, e->tile_ctas[DIR]);
+    k_tile<DIR, EPI><<<grid, NT, TileLayout<DIR>::BYTES, e->st>>>(t);
+}
+
 template <int DIR, int EPI>
 static void launch_step(Engine* e, StepArgs& a, int cur) {
     const bool timed = e->stats && e->step_launches % STATS_PERIOD == 0;
     if (timed) stats_mark(e);
     if (e->kind == 0) k_step<DIR, EPI><<<e->ntiles, NT, 0, e->st>>>(a);
+    else if (e->kind == 2) launch_tile<DIR, EPI>(e, a, cur);
+    else if (e->kind == 3) k_step<DIR, EPI, 4><<<e->ntiles, NT, 0, e->st>>>(a);
+    else if (e->kind == 4) k_split<DIR, EPI><<<e->ntiles, NT2, 0, e->st>>>(a);
     else launch_sweep<DIR, EPI>(e, a, cur);
     if (timed) {
         stats_mark(e);
@@ -404,13 +468,16 @@ struct KernelCfg {
 };
 static const KernelCfg kCandidates[] = {
     {0, TZ, TX, 0},
+    {2, TZ, TX, 0},
+    {3, TZ, TX, 0},
+    {4, TZ, TX, 0},
     {1, 64, 8, 4}, {1, 64, 8, 8}, {1, 64, 8, 16}, {1, 64, 8, 32},
     {1, 64, 16, 2}, {1, 64, 16, 4}, {1, 64, 16, 8},
     {1, 128, 8, 4}, {1, 128, 8, 8}, {1, 128, 8, 16},
 };
 
 static bool cfg_valid(const Engine* e, const KernelCfg& c) {
-    if (c.kind == 0) return true;
+    if (tiled(c.kind)) return true;
     return (e->nx - 2 * FAT) % c.cw == 0;
 }
 
@@ -418,7 +485,7 @@ void engine_set_kernel(Engine* e, int kind, int tz, int cw, int cpr) {
     KernelCfg c{kind, tz, cw, cpr};
     bool known = false;
     for (const KernelCfg& k : kCandidates)
-        if (k.kind == c.kind && (c.kind == 0 || (k.tz == c.tz && k.cw == c.cw))) known = true;
+        if (k.kind == c.kind && (tiled(c.kind) || (k.tz == c.tz && k.cw == c.cw))) known = true;
     if (!known || !cfg_valid(e, c) || (kind == 1 && (cpr < 1 || cpr > SWEEP_MAXK))) throw Error(EIO_ERR_ARG, "unsupported kernel configuration");
     e->kind = kind;
     if (kind == 1) { e->tz = tz; e->cw = cw; e->cpr = cpr; }
@@ -427,9 +494,9 @@ void engine_set_kernel(Engine* e, int kind, int tz, int cw, int cpr) {
 
 void engine_get_kernel(const Engine* e, int* kind, int* tz, int* cw, int* cpr) {
     if (kind) *kind = e->kind;
-    if (tz) *tz = e->kind ? e->tz : TZ;
-    if (cw) *cw = e->kind ? e->cw : TX;
-    if (cpr) *cpr = e->kind ? e->cpr : 0;
+    if (tz) *tz = tiled(e->kind) ? TZ : e->tz;
+    if (cw) *cw = tiled(e->kind) ? TX : e->cw;
+    if (cpr) *cpr = tiled(e->kind) ? 0 : e->cpr;
 }
 
 static void zero_wavefields(Engine* e);
@@ -453,7 +520,7 @@ void engine_autotune(Engine* e) {
     for (const KernelCfg& c : kCandidates) {
         if (!cfg_valid(e, c)) continue;
         e->kind = c.kind;
-        if (c.kind) { e->tz = c.tz; e->cw = c.cw; e->cpr = c.cpr; }
+        if (c.kind == 1) { e->tz = c.tz; e->cw = c.cw; e->cpr = c.cpr; }
         float tot = 0.f;
         for (int dir = 0; dir < 2; dir++) {
             int cur = 0;
@@ -478,7 +545,7 @@ void engine_autotune(Engine* e) {
     e->launches = 0;
     e->step_launches = 0;
     e->kind = bestc.kind;
-    if (bestc.kind) { e->tz = bestc.tz; e->cw = bestc.cw; e->cpr = bestc.cpr; }
+    if (bestc.kind == 1) { e->tz = bestc.tz; e->cw = bestc.cw; e->cpr = bestc.cpr; }
     e->tuned = true;
     e->stats = stats;
     int flag = 0;

@@ -162,97 +162,51 @@ __device__ __forceinline__ void xwin(const float* s, int lx0, int lz, float4* q)
     for (int m = 0; m < 10; m++) q[m] = ld4(s + (lx0 - FAT + m) * SZ + lz);
 }
 
-// One fused fine time step.  DIR 0 = forward (ker_step_fwd), 1 = adjoint (ker_step_adj).
-template <int DIR, int EPI>
-__global__ void __launch_bounds__(NT, 3) k_step(StepArgs a)
+// Stencil part of one fused fine step for the float4 at local (lx, lz) of a
+// staged tile (5 fields [SX][SZ] at stride SMEM_FIELD): forward, the current
+// level and the medium at the cell from par(k); adjoint, the staged scaled
+// combinations.  t[f] receives the update of fields F0 <= f < F1 before the
+// old level is added; the field groups {vx, vz} and {sxx, szz, sxz} need four
+// derivatives each.
+template <int DIR, int F0, int F1, class Par>
+__device__ __forceinline__ void stencil_fields(const float* sm, int lx, int lz, const float* cz, const float* cx,
+                                               bool valid, Par par, float4 (&t)[5])
 {
-    __shared__ __align__(16) float sm[5 * SMEM_FIELD];
-
-    const int tid = threadIdx.x;
-    const int tile = blockIdx.x;
-    const int bz = tile % a.ntz, bx = tile / a.ntz;
-    const int z0 = FAT + bz * TZ, x0 = FAT + bx * TX;
-    const int nz = a.nz;
-
-    // ---- stage the current level (forward) or its scaled combinations (adjoint)
-    {
-        const int nq = SZ / 4;                    // float4 per shared column
-        for (int q = tid; q < nq * SX; q += NT) {
-            const int lx = q / nq, lz4 = (q % nq) * 4;
-            const int gz = z0 - FAT + lz4, gx = x0 - FAT + lx;
-            float4 v[5];
-            if (gz < nz) {
-                const long long gi = (long long)gx * nz + gz;
-                if (DIR == 0) {
+    static_assert((F0 == 0 && F1 == 5) || (F0 == 0 && F1 == 2) || (F0 == 2 && F1 == 5), "field group");
+    const float* s0 = sm;
+    const float* s1 = sm + SMEM_FIELD;
+    const float* s2 = sm + 2 * SMEM_FIELD;
+    const float* s3 = sm + 3 * SMEM_FIELD;
+    const float* s4 = sm + 4 * SMEM_FIELD;
+    float4 q[9];
+    float w[12];
+    auto xw = [&](const float* sf) {
 #pragma unroll
-                    for (int f = 0; f < 5; f++) v[f] = ldg4(a.c[f] + gi);
-                } else {
-                    float4 vx = ldg4(a.c[0] + gi), vz = ldg4(a.c[1] + gi), sxx = ldg4(a.c[2] + gi),
-                           szz = ldg4(a.c[3] + gi), sxz = ldg4(a.c[4] + gi);
-                    float4 rx = ldg4(a.par[0] + gi), rz = ldg4(a.par[1] + gi), l2m = ldg4(a.par[2] + gi),
-                           lam = ldg4(a.par[3] + gi), mu = ldg4(a.par[4] + gi);
-#pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        at(v[0], j) = at(l2m, j) * at(sxx, j) + at(lam, j) * at(szz, j);  // -> d/dx-  (vx)
-                        at(v[1], j) = at(lam, j) * at(sxx, j) + at(l2m, j) * at(szz, j);  // -> d/dz-  (vz)
-                        at(v[2], j) = at(mu, j) * at(sxz, j);                             // -> vx, vz
-                        at(v[3], j) = at(rx, j) * at(vx, j);                              // -> sxx, sxz
-                        at(v[4], j) = at(rz, j) * at(vz, j);                              // -> szz, sxz
-                    }
-                }
-            } else {
-#pragma unroll
-                for (int f = 0; f < 5; f++) v[f] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-#pragma unroll
-            for (int f = 0; f < 5; f++) st4(sm + f * SMEM_FIELD + lx * SZ + lz4, v[f]);
-        }
-    }
-    __syncthreads();
-
-    const int tzi = tid % NTZ, txi = tid / NTZ;
-    const int lz = FAT + 4 * tzi;              // local z of my float4
-    const int lx = FAT + txi;                  // my local column
-    const int gz = z0 + 4 * tzi;
-    const int gx = x0 + txi;
-    const bool valid = gz < nz - FAT;
-    const long long gi = (long long)gx * nz + gz;
-    float4 t[5];                               // new values before the final taper
-
-    {
-        const float* cz = a.cz;
-        const float* cx = a.cx;
-        const float* s0 = sm;
-        const float* s1 = sm + SMEM_FIELD;
-        const float* s2 = sm + 2 * SMEM_FIELD;
-        const float* s3 = sm + 3 * SMEM_FIELD;
-        const float* s4 = sm + 4 * SMEM_FIELD;
-        float4 q[9];
-        float w[12];
-        auto xw = [&](const float* sf) {
-#pragma unroll
-            for (int m = 0; m < 9; m++) q[m] = ld4(sf + (lx - FAT + m) * SZ + lz);
-        };
-        if (DIR == 0) {
-            // s0 vx, s1 vz, s2 sxx, s3 szz, s4 sxz; one output field at a time keeps few registers live
+        for (int m = 0; m < 9; m++) q[m] = ld4(sf + (lx - FAT + m) * SZ + lz);
+    };
+    if (DIR == 0) {
+        // s0 vx, s1 vz, s2 sxx, s3 szz, s4 sxz; one output field at a time keeps few registers live
+        if (F0 == 0) {
             xw(s2); float4 dx = dmx(q, 4, cx);
             zwin(s4, lx, lz, w); float4 dz = dpz(w, cz);
             if (valid) {
-                const float4 rx = ldg4(a.par[0] + gi);
+                const float4 rx = par(0);
 #pragma unroll
                 for (int j = 0; j < 4; j++) at(t[0], j) = at(rx, j) * (at(dx, j) + at(dz, j));
             }
             zwin(s3, lx, lz, w); dz = dmz(w, cz);
             xw(s4); dx = dpx(q, 4, cx);
             if (valid) {
-                const float4 rz = ldg4(a.par[1] + gi);
+                const float4 rz = par(1);
 #pragma unroll
                 for (int j = 0; j < 4; j++) at(t[1], j) = at(rz, j) * (at(dz, j) + at(dx, j));
             }
-            xw(s0); dx = dpx(q, 4, cx);
-            zwin(s1, lx, lz, w); dz = dpz(w, cz);
+        }
+        if (F1 == 5) {
+            xw(s0); float4 dx = dpx(q, 4, cx);
+            zwin(s1, lx, lz, w); float4 dz = dpz(w, cz);
             if (valid) {
-                const float4 l2m = ldg4(a.par[2] + gi), lam = ldg4(a.par[3] + gi);
+                const float4 l2m = par(2), lam = par(3);
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     at(t[2], j) = at(l2m, j) * at(dx, j) + at(lam, j) * at(dz, j);
@@ -262,12 +216,14 @@ __global__ void __launch_bounds__(NT, 3) k_step(StepArgs a)
             zwin(s0, lx, lz, w); dz = dmz(w, cz);
             xw(s1); dx = dmx(q, 4, cx);
             if (valid) {
-                const float4 mu = ldg4(a.par[4] + gi);
+                const float4 mu = par(4);
 #pragma unroll
                 for (int j = 0; j < 4; j++) at(t[4], j) = at(mu, j) * (at(dz, j) + at(dx, j));
             }
-        } else {
-            // s0 A=l2m*sxx+lam*szz, s1 B=lam*sxx+l2m*szz, s2 M=mu*sxz, s3 P=rhox*vx, s4 Q=rhoz*vz
+        }
+    } else {
+        // s0 A=l2m*sxx+lam*szz, s1 B=lam*sxx+l2m*szz, s2 M=mu*sxz, s3 P=rhox*vx, s4 Q=rhoz*vz
+        if (F0 == 0) {
             xw(s0); float4 dx = dmx(q, 4, cx);
             zwin(s2, lx, lz, w); float4 dz = dpz(w, cz);
 #pragma unroll
@@ -276,10 +232,12 @@ __global__ void __launch_bounds__(NT, 3) k_step(StepArgs a)
             xw(s2); dx = dpx(q, 4, cx);
 #pragma unroll
             for (int j = 0; j < 4; j++) at(t[1], j) = -(at(dz, j) + at(dx, j));
-            xw(s3); dx = dpx(q, 4, cx);
+        }
+        if (F1 == 5) {
+            xw(s3); float4 dx = dpx(q, 4, cx);
 #pragma unroll
             for (int j = 0; j < 4; j++) at(t[2], j) = -at(dx, j);
-            zwin(s4, lx, lz, w); dz = dpz(w, cz);
+            zwin(s4, lx, lz, w); float4 dz = dpz(w, cz);
 #pragma unroll
             for (int j = 0; j < 4; j++) at(t[3], j) = -at(dz, j);
             zwin(s3, lx, lz, w); dz = dmz(w, cz);
@@ -288,14 +246,42 @@ __global__ void __launch_bounds__(NT, 3) k_step(StepArgs a)
             for (int j = 0; j < 4; j++) at(t[4], j) = -(at(dz, j) + at(dx, j));
         }
     }
+}
 
-    // ---- deferred taper of the old level, leapfrog sum
-    float4 osave[5];      // old level (EPI_TRI)
-    float4 csave[2];      // current vx, vz (forward EPI_TRI; shared memory is reused below)
-    if (EPI == EPI_TRI && DIR == 0) {
-        csave[0] = ld4(sm + lx * SZ + lz);
-        csave[1] = ld4(sm + SMEM_FIELD + lx * SZ + lz);
+template <int DIR, class Par>
+__device__ __forceinline__ void stencil_core(const float* sm, int lx, int lz, const float* cz, const float* cx,
+                                             bool valid, Par par, float4 (&t)[5])
+{
+    stencil_fields<DIR, 0, 5>(sm, lx, lz, cz, cx, valid, par, t);
+}
+
+// adjoint staging: the scaled combinations the transposed stencils act on
+__device__ __forceinline__ void adj_products(float4 vx, float4 vz, float4 sxx, float4 szz, float4 sxz, float4 rx,
+                                             float4 rz, float4 l2m, float4 lam, float4 mu, float4 (&v)[5])
+{
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        at(v[0], j) = at(l2m, j) * at(sxx, j) + at(lam, j) * at(szz, j);  // -> d/dx-  (vx)
+        at(v[1], j) = at(lam, j) * at(sxx, j) + at(l2m, j) * at(szz, j);  // -> d/dz-  (vz)
+        at(v[2], j) = at(mu, j) * at(sxz, j);                             // -> vx, vz
+        at(v[3], j) = at(rx, j) * at(vx, j);                              // -> sxx, sxz
+        at(v[4], j) = at(rz, j) * at(vz, j);                              // -> szz, sxz
     }
+}
+
+// Everything of one fused fine step after the stencils, for the float4 of
+// thread (tzi, txi) of tile `tile` and the fields F0 <= f < F1: deferred taper
+// of the old level (o(f) returns it), leapfrog sum, scattered-field source,
+// sparse injection, final taper, store of the new level, dense Born
+// epilogues, sparse extraction.  NTHR threads of the CTA take part (every one
+// reaches the same barriers); scratch: >= 5*TX*TZ floats of shared memory that
+// the stencils no longer need.
+template <int DIR, int EPI, int F0, int F1, int NTHR, class Old>
+__device__ __forceinline__ void step_tail(const StepArgs& a, float* scratch, int tile, int tid, int tzi, int txi,
+                                          int gz, int gx, bool valid, long long gi, float4 (&t)[5], Old oload,
+                                          const float4 (&csave)[2])
+{
+    float4 osave[5];      // old level (EPI_TRI)
     float dd[4];
     {
         const float dxc = __ldg(a.dampx + gx);
@@ -304,8 +290,8 @@ __global__ void __launch_bounds__(NT, 3) k_step(StepArgs a)
     }
     if (valid) {
 #pragma unroll
-        for (int f = 0; f < 5; f++) {
-            const float4 o = ld4(a.o[f] + gi);
+        for (int f = F0; f < F1; f++) {
+            const float4 o = oload(f);
             if (EPI == EPI_TRI) osave[f] = o;
 #pragma unroll
             for (int j = 0; j < 4; j++) at(t[f], j) = dd[j] * at(o, j) + at(t[f], j);
@@ -315,7 +301,7 @@ __global__ void __launch_bounds__(NT, 3) k_step(StepArgs a)
             // the right slice is then not read (ssR * 0 adds nothing)
             const bool right = a.sw1 != 0.f;
 #pragma unroll
-            for (int f = 0; f < 5; f++) {
+            for (int f = F0; f < F1; f++) {
                 const float4 l = ldg4(a.ssL[f] + gi);
                 const float4 r = right ? ldg4(a.ssR[f] + gi) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
@@ -328,11 +314,11 @@ __global__ void __launch_bounds__(NT, 3) k_step(StepArgs a)
     if (a.inj.tile_start) {
         const int e0 = a.inj.tile_start[tile], e1 = a.inj.tile_start[tile + 1];
         if (e1 > e0) {   // CTA-uniform
-            float* acc = sm;                      // reuse: [5][TX][TZ]
+            float* acc = scratch;                 // [5][TX][TZ]
             __syncthreads();
-            for (int i = tid; i < 5 * TX * TZ; i += NT) acc[i] = 0.f;
+            for (int i = tid; i < 5 * TX * TZ; i += NTHR) acc[i] = 0.f;
             __syncthreads();
-            for (int e = e0 + tid; e < e1; e += NT) {
+            for (int e = e0 + tid; e < e1; e += NTHR) {
                 const PointEntry pe = a.inj.ent[e];
                 const int f = pe.key >> 16, lx = (pe.key >> 8) & 0xff, lzz = pe.key & 0xff;
                 const float* sg = a.inj.sig[f];
@@ -344,7 +330,7 @@ __global__ void __launch_bounds__(NT, 3) k_step(StepArgs a)
             __syncthreads();
             if (valid) {
 #pragma unroll
-                for (int f = 0; f < 5; f++) {
+                for (int f = F0; f < F1; f++) {
                     const float4 v = ld4(acc + (f * TX + txi) * TZ + 4 * tzi);
 #pragma unroll
                     for (int j = 0; j < 4; j++) at(t[f], j) += at(v, j);
@@ -356,12 +342,12 @@ __global__ void __launch_bounds__(NT, 3) k_step(StepArgs a)
     // ---- final taper, store, dense epilogues
     if (valid) {
 #pragma unroll
-        for (int f = 0; f < 5; f++) {
+        for (int f = F0; f < F1; f++) {
 #pragma unroll
             for (int j = 0; j < 4; j++) at(t[f], j) *= dd[j];
             st4(a.o[f] + gi, t[f]);
         }
-        if (EPI == EPI_SAVE_W) {
+        if (EPI == EPI_SAVE_W && F0 == 0) {
             float* w0p = a.W0 + (long long)a.wt * a.wstride + gi;
             float* w1p = a.W1 + (long long)a.wt * a.wstride + gi;
             float4 u0 = ld4(w0p), u1 = ld4(w0p + a.wstride), v0 = ld4(w1p), v1 = ld4(w1p + a.wstride);
@@ -374,7 +360,7 @@ __global__ void __launch_bounds__(NT, 3) k_step(StepArgs a)
         }
         if (EPI == EPI_EXT_SS) {
 #pragma unroll
-            for (int f = 0; f < 5; f++) {
+            for (int f = F0; f < F1; f++) {
                 float4 l = ld4(a.eL[f] + gi), r = ld4(a.eR[f] + gi);
 #pragma unroll
                 for (int j = 0; j < 4; j++) { at(l, j) += at(t[f], j) * a.sw0; at(r, j) += at(t[f], j) * a.sw1; }
@@ -383,13 +369,15 @@ __global__ void __launch_bounds__(NT, 3) k_step(StepArgs a)
         }
         if (EPI == EPI_TRI && a.tmode) {
             if (DIR == 0) {
-                st4(a.W0 + (long long)a.wt * a.wstride + gi,
-                    tri_sample(a.tmode, osave[0], csave[0], t[0], a.tw_o, a.tw_c, a.tw_n));
-                st4(a.W1 + (long long)a.wt * a.wstride + gi,
-                    tri_sample(a.tmode, osave[1], csave[1], t[1], a.tw_o, a.tw_c, a.tw_n));
+                if (F0 == 0) {
+                    st4(a.W0 + (long long)a.wt * a.wstride + gi,
+                        tri_sample(a.tmode, osave[0], csave[0], t[0], a.tw_o, a.tw_c, a.tw_n));
+                    st4(a.W1 + (long long)a.wt * a.wstride + gi,
+                        tri_sample(a.tmode, osave[1], csave[1], t[1], a.tw_o, a.tw_c, a.tw_n));
+                }
             } else {
 #pragma unroll
-                for (int f = 0; f < 5; f++)
+                for (int f = F0; f < F1; f++)
                     st4(a.eL[f] + gi, tri_sample(a.tmode, osave[f], ldg4(a.c[f] + gi), t[f], a.tw_o, a.tw_c, a.tw_n));
             }
         }
@@ -399,14 +387,14 @@ __global__ void __launch_bounds__(NT, 3) k_step(StepArgs a)
     if (a.ext.tile_start) {
         const int e0 = a.ext.tile_start[tile], e1 = a.ext.tile_start[tile + 1];
         if (e1 > e0) {
-            float* stg = sm;                      // [5][TX][TZ]
+            float* stg = scratch;                 // [5][TX][TZ]
             __syncthreads();
             if (valid) {
 #pragma unroll
-                for (int f = 0; f < 5; f++) st4(stg + (f * TX + txi) * TZ + 4 * tzi, t[f]);
+                for (int f = F0; f < F1; f++) st4(stg + (f * TX + txi) * TZ + 4 * tzi, t[f]);
             }
             __syncthreads();
-            for (int e = e0 + tid; e < e1; e += NT) {
+            for (int e = e0 + tid; e < e1; e += NTHR) {
                 const PointEntry pe = a.ext.ent[e];
                 const int f = pe.key >> 16, lx = (pe.key >> 8) & 0xff, lzz = pe.key & 0xff;
                 const float v = stg[(f * TX + lx) * TZ + lzz];
@@ -416,6 +404,118 @@ __global__ void __launch_bounds__(NT, 3) k_step(StepArgs a)
                 sg[(long long)(a.ext.t0 + 1) * ld + pe.col] += v * a.ext.w1;
             }
         }
+    }
+}
+
+// Stage the current level (forward) or its scaled combinations (adjoint) of
+// tile (z0, x0) with its 4-cell halo into sm [5][SX][SZ]; NTHR threads.
+template <int DIR, int NTHR>
+__device__ __forceinline__ void stage_tile(const StepArgs& a, float* sm, int z0, int x0, int tid)
+{
+    const int nz = a.nz;
+    const int nq = SZ / 4;                        // float4 per shared column
+    for (int q = tid; q < nq * SX; q += NTHR) {
+        const int lx = q / nq, lz4 = (q % nq) * 4;
+        const int gz = z0 - FAT + lz4, gx = x0 - FAT + lx;
+        float4 v[5];
+        if (gz < nz) {
+            const long long gi = (long long)gx * nz + gz;
+            if (DIR == 0) {
+#pragma unroll
+                for (int f = 0; f < 5; f++) v[f] = ldg4(a.c[f] + gi);
+            } else {
+                adj_products(ldg4(a.c[0] + gi), ldg4(a.c[1] + gi), ldg4(a.c[2] + gi), ldg4(a.c[3] + gi),
+                             ldg4(a.c[4] + gi), ldg4(a.par[0] + gi), ldg4(a.par[1] + gi), ldg4(a.par[2] + gi),
+                             ldg4(a.par[3] + gi), ldg4(a.par[4] + gi), v);
+            }
+        } else {
+#pragma unroll
+            for (int f = 0; f < 5; f++) v[f] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int f = 0; f < 5; f++) st4(sm + f * SMEM_FIELD + lx * SZ + lz4, v[f]);
+    }
+}
+
+// One fused fine step.  DIR 0 = forward (ker_step_fwd), 1 = adjoint (ker_step_adj).
+// The current level (forward) or its scaled combinations (adjoint) are staged
+// with plain loads; the old level and the medium are read from global memory.
+// MINB CTAs per SM (3: <= 80 registers, 4: <= 64).
+template <int DIR, int EPI, int MINB = 3>
+__global__ void __launch_bounds__(NT, MINB) k_step(StepArgs a)
+{
+    __shared__ __align__(16) float sm[5 * SMEM_FIELD];
+
+    const int tid = threadIdx.x;
+    const int tile = blockIdx.x;
+    const int bz = tile % a.ntz, bx = tile / a.ntz;
+    const int z0 = FAT + bz * TZ, x0 = FAT + bx * TX;
+    const int nz = a.nz;
+
+    stage_tile<DIR, NT>(a, sm, z0, x0, tid);
+    __syncthreads();
+
+    const int tzi = tid % NTZ, txi = tid / NTZ;
+    const int lz = FAT + 4 * tzi;              // local z of my float4
+    const int lx = FAT + txi;                  // my local column
+    const int gz = z0 + 4 * tzi;
+    const int gx = x0 + txi;
+    const bool valid = gz < nz - FAT;
+    const long long gi = (long long)gx * nz + gz;
+    float4 t[5];                               // new values before the final taper
+
+    stencil_core<DIR>(sm, lx, lz, a.cz, a.cx, valid, [&](int k) { return ldg4(a.par[k] + gi); }, t);
+
+    float4 csave[2];      // current vx, vz (forward EPI_TRI; shared memory is reused below)
+    if (EPI == EPI_TRI && DIR == 0) {
+        csave[0] = ld4(sm + lx * SZ + lz);
+        csave[1] = ld4(sm + SMEM_FIELD + lx * SZ + lz);
+    }
+    step_tail<DIR, EPI, 0, 5, NT>(a, sm, tile, tid, tzi, txi, gz, gx, valid, gi, t,
+                                  [&](int f) { return ld4(a.o[f] + gi); }, csave);
+}
+
+// Same step with two threads per float4: warps 0-7 update vx and vz, warps
+// 8-15 sxx, szz and sxz (four derivatives per thread either way), which halves
+// the dependent work on a thread's critical path.  2 CTAs per SM, <= 64 registers.
+constexpr int NT2 = 2 * NT;
+
+template <int DIR, int EPI>
+__global__ void __launch_bounds__(NT2, 2) k_split(StepArgs a)
+{
+    __shared__ __align__(16) float sm[5 * SMEM_FIELD];
+
+    const int tid = threadIdx.x;
+    const int tile = blockIdx.x;
+    const int bz = tile % a.ntz, bx = tile / a.ntz;
+    const int z0 = FAT + bz * TZ, x0 = FAT + bx * TX;
+    const int nz = a.nz;
+
+    stage_tile<DIR, NT2>(a, sm, z0, x0, tid);
+    __syncthreads();
+
+    const int lt = tid & (NT - 1);
+    const int tzi = lt % NTZ, txi = lt / NTZ;
+    const int lz = FAT + 4 * tzi;
+    const int lx = FAT + txi;
+    const int gz = z0 + 4 * tzi;
+    const int gx = x0 + txi;
+    const bool valid = gz < nz - FAT;
+    const long long gi = (long long)gx * nz + gz;
+    float4 t[5];
+    float4 csave[2];
+    auto par = [&](int k) { return ldg4(a.par[k] + gi); };
+    auto old = [&](int f) { return ld4(a.o[f] + gi); };
+    if (tid < NT) {                            // warp-uniform
+        stencil_fields<DIR, 0, 2>(sm, lx, lz, a.cz, a.cx, valid, par, t);
+        if (EPI == EPI_TRI && DIR == 0) {
+            csave[0] = ld4(sm + lx * SZ + lz);
+            csave[1] = ld4(sm + SMEM_FIELD + lx * SZ + lz);
+        }
+        step_tail<DIR, EPI, 0, 2, NT2>(a, sm, tile, tid, tzi, txi, gz, gx, valid, gi, t, old, csave);
+    } else {
+        stencil_fields<DIR, 2, 5>(sm, lx, lz, a.cz, a.cx, valid, par, t);
+        step_tail<DIR, EPI, 2, 5, NT2>(a, sm, tile, tid, tzi, txi, gz, gx, valid, gi, t, old, csave);
     }
 }
 

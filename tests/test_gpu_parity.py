@@ -204,7 +204,7 @@ def test_out_of_interior_point_rejected(w, ctx):
 
 
 # ------------------------------------------------------------------ every step-kernel variant
-KERNELS = [(0, 64, 16, 0), (1, 64, 8, 4), (1, 64, 8, 5), (1, 64, 16, 2), (1, 64, 16, 1), (1, 128, 8, 3)]
+KERNELS = [(0, 64, 16, 0), (2, 64, 16, 0), (3, 64, 16, 0), (4, 64, 16, 0), (1, 64, 8, 4), (1, 64, 8, 5), (1, 64, 16, 2), (1, 64, 16, 1), (1, 128, 8, 3)]
 
 
 @pytest.mark.parametrize("cfg", KERNELS, ids=lambda c: "k%d_tz%d_cw%d_cpr%d" % c)
@@ -296,22 +296,42 @@ def test_full_size_born_600x1800_dot_product():
     assert born.dotTest(False, 1e-5), born.lastDotTest
 
 
-def test_sub2_running_sum_path_vs_oracle():
+def _nl_born_vs_oracle(c, w, seed):
+    r = reg_inputs(w, "f", seed=seed)
+    orc = r["orc"]
+    for adj in (0, 1):
+        dm, d = _copy(r["dm"]), _copy(r["data"])
+        orc.born_prop(adj, r["g"], r["med"], r["fine"], dm, d, r["sp"], r["rp"])
+        pdm, pd = c.born(adj, r["fine"], r["dm"], r["data"], r["sp"], r["rp"])
+        assert rel(pdm if adj else pd, dm if adj else d) < TOL32, ("born", adj)
+        m, d = _copy(r["model"]), _copy(r["data"])
+        orc.nl_prop(adj, r["g"], r["med"], m, d, r["sp"], r["rp"])
+        pm, pd = c.nl(adj, r["model"], r["data"], r["sp"], r["rp"])
+        assert rel(pm if adj else pd, m if adj else d) < TOL32, ("nl", adj)
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2, 3, 4])
+def test_ragged_tiles_vs_oracle(kind):
+    """A grid whose interior (96 x 112) leaves a half-height last tile row, so the
+    TMA boxes reach past the grid edge and read the zero fill."""
+    w = synthetic.small(nz=104, nx=120, nts=80)
+    c = Ctx(w)
+    try:
+        c.set_kernel(kind, 64, 16, 2)
+        _nl_born_vs_oracle(c, w, 17)
+    finally:
+        c.close()
+
+
+@pytest.mark.parametrize("kind", [None, 0, 2, 3, 4])
+def test_sub2_running_sum_path_vs_oracle(kind):
     """sub = 2 (four fine steps per coarse sample) keeps the running-sum history
     and adjoint accumulation; sub = 1 (every other test) takes the single-write path."""
     w2 = synthetic.small(nts=60, sub=2)
     c = Ctx(w2)
     try:
-        r = reg_inputs(w2, "f", seed=13)
-        orc = r["orc"]
-        for adj in (0, 1):
-            dm, d = _copy(r["dm"]), _copy(r["data"])
-            orc.born_prop(adj, r["g"], r["med"], r["fine"], dm, d, r["sp"], r["rp"])
-            pdm, pd = c.born(adj, r["fine"], r["dm"], r["data"], r["sp"], r["rp"])
-            assert rel(pdm if adj else pd, dm if adj else d) < TOL32, ("born", adj)
-            m, d = _copy(r["model"]), _copy(r["data"])
-            orc.nl_prop(adj, r["g"], r["med"], m, d, r["sp"], r["rp"])
-            pm, pd = c.nl(adj, r["model"], r["data"], r["sp"], r["rp"])
-            assert rel(pm if adj else pd, m if adj else d) < TOL32, ("nl", adj)
+        if kind is not None:
+            c.set_kernel(kind, 64, 16, 0)
+        _nl_born_vs_oracle(c, w2, 13)
     finally:
         c.close()
