@@ -69,6 +69,10 @@ struct Engine {
     int device = 0;
     int nsm = 148;          // SM count of the device
     cudaStream_t st = nullptr;
+    // Born imaging runs on a second, lower-priority stream, decoupled from the
+    // step kernels by a ring of secondary-source slots and two events per slot
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev_ready[4] = {}, ev_free[4] = {}, ev_sync = nullptr;
     int nz = 0, nx = 0;
     long long n = 0;
     int nts = 0, S = 0, ntw = 0, h = 0;
@@ -81,7 +85,7 @@ struct Engine {
     DBuf inj_ts, inj_ent, ext_ts, ext_ent;
     DBuf sig_in[5], sig_out[5];
     DBuf stage_a[5], stage_b[5], stage_c[5];
-    DBuf W, ss[10];
+    DBuf W, ss[20];         // secondary-source ring: 4 slots x 5 fields
     bool w_clean = false;   // history zeroed and only written by single stores since
     // step-kernel choice: kind 0 = shared-memory tile kernel (k_step),
     // kind 1 = TMA x-sweep (k_sweep) with strip height tz, chunk width cw and
@@ -186,7 +190,15 @@ Engine* engine_create(int device, const FdParam& fd) {
         e->ntz = (e->nz - 2 * FAT + TZ - 1) / TZ;
         e->ntx = (e->nx - 2 * FAT) / TX;
         e->ntiles = e->ntz * e->ntx;
-        EIO_CUDA(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
+        int lo = 0, hi = 0;
+        EIO_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        EIO_CUDA(cudaStreamCreateWithPriority(&e->st, cudaStreamNonBlocking, hi));
+        EIO_CUDA(cudaStreamCreateWithPriority(&e->st2, cudaStreamNonBlocking, lo));
+        for (int k = 0; k < 4; k++) {
+            EIO_CUDA(cudaEventCreateWithFlags(&e->ev_ready[k], cudaEventDisableTiming));
+            EIO_CUDA(cudaEventCreateWithFlags(&e->ev_free[k], cudaEventDisableTiming));
+        }
+        EIO_CUDA(cudaEventCreateWithFlags(&e->ev_sync, cudaEventDisableTiming));
         for (int f = 0; f < 10; f++) e->wf[f].ensure(sizeof(float) * e->n);
         engine_set_medium(e, fd);
     } catch (...) {
@@ -200,14 +212,22 @@ void engine_destroy(Engine* e) {
     if (!e) return;
     cudaSetDevice(e->device);
     if (e->st) cudaStreamSynchronize(e->st);
+    if (e->st2) cudaStreamSynchronize(e->st2);
     DBuf* all[] = {&e->dampz, &e->dampx, &e->inj_ts, &e->inj_ent, &e->ext_ts, &e->ext_ent, &e->W, &e->err};
     for (DBuf* b : all) b->release();
     for (int f = 0; f < 5; f++) {
         e->par[f].release(); e->sig_in[f].release(); e->sig_out[f].release();
         e->stage_a[f].release(); e->stage_b[f].release(); e->stage_c[f].release();
     }
-    for (int f = 0; f < 10; f++) { e->wf[f].release(); e->ss[f].release(); }
+    for (int f = 0; f < 10; f++) e->wf[f].release();
+    for (int f = 0; f < 20; f++) e->ss[f].release();
     for (cudaEvent_t x : e->ev) cudaEventDestroy(x);
+    for (int k = 0; k < 4; k++) {
+        if (e->ev_ready[k]) cudaEventDestroy(e->ev_ready[k]);
+        if (e->ev_free[k]) cudaEventDestroy(e->ev_free[k]);
+    }
+    if (e->ev_sync) cudaEventDestroy(e->ev_sync);
+    if (e->st2) cudaStreamDestroy(e->st2);
     if (e->st) cudaStreamDestroy(e->st);
     delete e;
 }
@@ -642,7 +662,8 @@ void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], 
     err_check(e);
 }
 
-static void launch_imaging(Engine* e, int adj, int its, float* const dm[5], float* const ss[5]) {
+static void launch_imaging(Engine* e, int adj, int its, float* const dm[5], float* const ss[5],
+                           cudaStream_t st) {
     ImagingArgs ia;
     memset(&ia, 0, sizeof(ia));
     ia.Wvx = e->W.f();
@@ -653,8 +674,8 @@ static void launch_imaging(Engine* e, int adj, int its, float* const dm[5], floa
     ia.dts_inv = e->dts_inv;
     for (int f = 0; f < 5; f++) { ia.dm[f] = dm[f]; ia.ss[f] = ss[f]; }
     const int ntiles = ((e->nz - 2 * FAT + TZ - 1) / TZ) * ((e->nx - 2 * FAT) / TX);
-    if (adj) k_imaging<1><<<ntiles, NT, 0, e->st>>>(ia);
-    else k_imaging<0><<<ntiles, NT, 0, e->st>>>(ia);
+    if (adj) k_imaging<1><<<ntiles, NT, 0, st>>>(ia);
+    else k_imaging<0><<<ntiles, NT, 0, st>>>(ia);
     e->launches++;
 }
 
@@ -726,11 +747,22 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
     stage_in(e, srcDtw, src.ld, e->ntw, e->sig_in);
     born_source(e, src, base);
     // phase 2
-    for (int f = 0; f < 10; f++) {
-        e->ss[f].ensure(sizeof(float) * e->n);
-        EIO_CUDA(cudaMemsetAsync(e->ss[f].p, 0, sizeof(float) * e->n, e->st));
-    }
+    constexpr int R = 4;                 // secondary-source ring slots
+    float* ring[R][5];
+    for (int k = 0; k < R; k++)
+        for (int f = 0; f < 5; f++) {
+            e->ss[k * 5 + f].ensure(sizeof(float) * e->n);
+            ring[k][f] = e->ss[k * 5 + f].f();
+        }
+    for (int f = 0; f < 10; f++) EIO_CUDA(cudaMemsetAsync(e->ss[f].p, 0, sizeof(float) * e->n, e->st));
     zero_wavefields(e);
+    // the imaging stream starts after everything queued so far (history, model, clears)
+    EIO_CUDA(cudaEventRecord(e->ev_sync, e->st));
+    EIO_CUDA(cudaStreamWaitEvent(e->st2, e->ev_sync, 0));
+    for (int k = 0; k < R; k++) {       // no slot is in use at the start
+        EIO_CUDA(cudaEventRecord(e->ev_free[k], e->st2));
+        EIO_CUDA(cudaEventRecord(e->ev_ready[k], e->st2));
+    }
     float* p0[5]; float* p1[5]; float* sL[5]; float* sR[5];
     for (int f = 0; f < 5; f++) {
         p0[f] = e->wf[f].f(); p1[f] = e->wf[5 + f].f();
@@ -741,21 +773,35 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
     if (!adj) {
         zero_out(e, rec.ld, e->nts, e->sig_out);
         a.ext = upload_points(e, rec, e->ext_ts, e->ext_ent, e->sig_out);
-        launch_imaging(e, 0, 0, dm, sL);
+        // secondary sources of coarse sample k go to slot k % R on the imaging
+        // stream, up to R-1 samples ahead of the step kernels that inject them;
+        // slot k is free once coarse interval k - R (its last reader) is done
+        auto image = [&](int k) {
+            const int sl = k % R;
+            EIO_CUDA(cudaStreamWaitEvent(e->st2, e->ev_free[sl], 0));
+            launch_imaging(e, 0, k, dm, ring[sl], e->st2);
+            EIO_CUDA(cudaEventRecord(e->ev_ready[sl], e->st2));
+        };
+        for (int k = 0; k < R - 1 && k < e->nts; k++) image(k);
         for (int its = 0; its < e->nts - 1; its++) {
-            launch_imaging(e, 0, its + 1, dm, sR);
+            if (its + R - 1 < e->nts) image(its + R - 1);
+            const int l = its % R, r = (its + 1) % R;
+            EIO_CUDA(cudaStreamWaitEvent(e->st, e->ev_ready[l], 0));
+            EIO_CUDA(cudaStreamWaitEvent(e->st, e->ev_ready[r], 0));
             for (int it2 = 1; it2 < e->S + 1; it2++) {
-                for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; a.ssL[f] = sL[f]; a.ssR[f] = sR[f]; }
+                for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; a.ssL[f] = ring[l][f]; a.ssR[f] = ring[r][f]; }
                 a.sw0 = F[it2 - 1]; a.sw1 = F[h + it2 - 1];
                 a.ext.t0 = its; a.ext.w0 = F[it2]; a.ext.w1 = F[h + it2];
                 launch_step<0, EPI_INJ_SS>(e, a, cur);
                 std::swap(p0, p1);
                 cur ^= 1;
             }
-            // the imaging kernel rewrites every interior cell of the right slice,
-            // so the reference's memset of it (BornElasticGpuFunctions.cu:806-810) is not needed
-            std::swap(sL, sR);
+            // the imaging kernel rewrites every interior cell of a slot, so the
+            // reference's memset of the right slice (BornElasticGpuFunctions.cu:806-810) is not needed
+            EIO_CUDA(cudaEventRecord(e->ev_free[l], e->st));
         }
+        EIO_CUDA(cudaEventRecord(e->ev_sync, e->st2));
+        EIO_CUDA(cudaStreamWaitEvent(e->st, e->ev_sync, 0));
         check_launch();
         stage_out(e, rec.ld, e->nts, e->sig_out, data);
     } else if (e->S == 2) {
@@ -763,29 +809,35 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
         // sample T of the reference's running sums ssL/ssR (extractInterpAdjointWavefield,
         // K:1369-1376) is ((p(2T+1) f[1] + p(2T) f[0]) + p(2T-1) f[h+1]) (+ p(2T-2) * f[h] = 0),
         // i.e. the old, current and new level of the step (T-1, it2 = 1): that step
-        // writes it once (EPI_TRI) and the imaging condition of T runs right after.
+        // writes it once (EPI_TRI) and the imaging condition of T follows on the imaging stream.
         stage_in(e, data, rec.ld, e->nts, e->sig_in);
         a.inj = upload_points(e, rec, e->inj_ts, e->inj_ent, e->sig_in);
-        for (int f = 0; f < 5; f++) a.eL[f] = sL[f];
+        // sample T goes to slot T % R; its imaging runs on the imaging stream
+        // while the adjoint keeps stepping; the slot is rewritten R samples later
+        auto extract = [&](int T, int mode, float wo, float wc, float wn) {
+            const int sl = T % R;
+            EIO_CUDA(cudaStreamWaitEvent(e->st, e->ev_free[sl], 0));
+            for (int f = 0; f < 5; f++) a.eL[f] = ring[sl][f];
+            a.tmode = mode; a.tw_o = wo; a.tw_c = wc; a.tw_n = wn;
+            launch_step<1, EPI_TRI>(e, a, cur);
+            EIO_CUDA(cudaEventRecord(e->ev_ready[sl], e->st));
+            EIO_CUDA(cudaStreamWaitEvent(e->st2, e->ev_ready[sl], 0));
+            launch_imaging(e, 1, T, dm, ring[sl], e->st2);
+            EIO_CUDA(cudaEventRecord(e->ev_free[sl], e->st2));
+        };
         for (int its = e->nts - 2; its > -1; its--) {
             for (int it2 = e->S - 1; it2 > -1; it2--) {
                 for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; }
                 a.inj.t0 = its; a.inj.w0 = F[it2 + 1]; a.inj.w1 = F[h + it2 + 1];
-                if (it2 == 1) {
-                    a.tmode = 1; a.tw_o = F[1]; a.tw_c = F[0]; a.tw_n = F[h + 1];
-                    launch_step<1, EPI_TRI>(e, a, cur);
-                } else if (its == 0) {   // sample 0 = p(1) f[1] + p(0) f[0]
-                    a.tmode = 2; a.tw_o = 0.f; a.tw_c = F[1]; a.tw_n = F[0];
-                    launch_step<1, EPI_TRI>(e, a, cur);
-                } else {
-                    launch_step<1, EPI_NONE>(e, a, cur);
-                }
+                if (it2 == 1) extract(its + 1, 1, F[1], F[0], F[h + 1]);
+                else if (its == 0) extract(0, 2, 0.f, F[1], F[0]);   // sample 0 = p(1) f[1] + p(0) f[0]
+                else launch_step<1, EPI_NONE>(e, a, cur);
                 std::swap(p0, p1);
                 cur ^= 1;
-                if (it2 == 1) launch_imaging(e, 1, its + 1, dm, sL);
             }
         }
-        launch_imaging(e, 1, 0, dm, sL);
+        EIO_CUDA(cudaEventRecord(e->ev_sync, e->st2));
+        EIO_CUDA(cudaStreamWaitEvent(e->st, e->ev_sync, 0));
         check_launch();
     } else {
         stage_in(e, data, rec.ld, e->nts, e->sig_in);
@@ -799,11 +851,11 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
                 std::swap(p0, p1);
                 cur ^= 1;
             }
-            launch_imaging(e, 1, its + 1, dm, sR);
+            launch_imaging(e, 1, its + 1, dm, sR, e->st);
             std::swap(sL, sR);
             for (int f = 0; f < 5; f++) EIO_CUDA(cudaMemsetAsync(sL[f], 0, sizeof(float) * e->n, e->st));
         }
-        launch_imaging(e, 1, 0, dm, sR);
+        launch_imaging(e, 1, 0, dm, sR, e->st);
         check_launch();
     }
     EIO_CUDA(cudaStreamSynchronize(e->st));
