@@ -91,6 +91,8 @@ _SIGS = {
     "eio_nl_prepare_sources": (I, [P, FP, P, P]),
     "eio_nl_fwd_noalloc": (I, [ctypes.POINTER(FdParams), P, P, P, P, IP, P, IP, P]),
     "eio_nl_forward": (I, [P, I, I, I, FP, FP, P, P, I]),
+    "eio_nl_forward_wavefield": (I, [P, I, I, I, FP, FP, P, P, I, I, FP]),
+    "eio_nl_adjoint_wavefield": (I, [P, I, I, I, FP, FP, P, P, I, I, FP]),
     "eio_nl_adjoint": (I, [P, I, I, I, FP, FP, P, P, I]),
     "eio_born_forward": (I, [P, I, I, FP, FP, P, I, P, P, I]),
     "eio_born_adjoint": (I, [P, I, I, FP, FP, P, I, P, P, I]),

@@ -86,6 +86,7 @@ struct Engine {
     DBuf sig_in[5], sig_out[5];
     DBuf stage_a[5], stage_b[5], stage_c[5];
     DBuf W, ss[20];         // secondary-source ring: 4 slots x 5 fields
+    DBuf wsave;             // saved wavefield of the *Wavefield operators
     bool w_clean = false;   // history zeroed and only written by single stores since
     // step-kernel choice: kind 0 = shared-memory tile kernel (k_step),
     // kind 1 = TMA x-sweep (k_sweep) with strip height tz, chunk width cw and
@@ -213,7 +214,7 @@ void engine_destroy(Engine* e) {
     cudaSetDevice(e->device);
     if (e->st) cudaStreamSynchronize(e->st);
     if (e->st2) cudaStreamSynchronize(e->st2);
-    DBuf* all[] = {&e->dampz, &e->dampx, &e->inj_ts, &e->inj_ent, &e->ext_ts, &e->ext_ent, &e->W, &e->err};
+    DBuf* all[] = {&e->dampz, &e->dampx, &e->inj_ts, &e->inj_ent, &e->ext_ts, &e->ext_ent, &e->W, &e->err, &e->wsave};
     for (DBuf* b : all) b->release();
     for (int f = 0; f < 5; f++) {
         e->par[f].release(); e->sig_in[f].release(); e->sig_out[f].release();
@@ -610,7 +611,18 @@ static void err_check(Engine* e) {
     if (flag) throw Error(EIO_ERR_CUDA, "a TMA pipeline wait timed out in the step kernel");
 }
 
-void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], const ShotGeom& g) {
+// new level (in p) into coarse rows its, its+1 of the saved wavefield
+static void save_wavefield(Engine* e, float* W, float* const p[5], int its, float w0, float w1) {
+    SaveArgs s;
+    for (int f = 0; f < 5; f++) s.p[f] = p[f];
+    s.W = W; s.n = e->n; s.nz = e->nz; s.nx = e->nx; s.its = its; s.w0 = w0; s.w1 = w1;
+    const int nq = (e->nz - 2 * FAT) / 4;
+    dim3 g((nq + 127) / 128, e->nx - 2 * FAT);
+    k_save_wavefield<<<g, 128, 0, e->st>>>(s);
+    e->launches++;
+}
+
+void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], const ShotGeom& g, float* wfld) {
     EIO_CUDA(cudaSetDevice(e->device));
     if (!e->tuned) engine_autotune(e);
     err_reset(e);
@@ -635,6 +647,7 @@ void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], 
                 a.inj.t0 = its; a.inj.w0 = F[it2 - 1]; a.inj.w1 = F[h + it2 - 1];
                 a.ext.t0 = its; a.ext.w0 = F[it2]; a.ext.w1 = F[h + it2];
                 launch_step<0, EPI_NONE>(e, a, cur);
+                if (wfld) save_wavefield(e, wfld, p0, its, F[it2], F[h + it2]);
                 std::swap(p0, p1);
                 cur ^= 1;
             }
@@ -651,6 +664,7 @@ void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], 
                 a.inj.t0 = its; a.inj.w0 = F[it2 + 1]; a.inj.w1 = F[h + it2 + 1];
                 a.ext.t0 = its; a.ext.w0 = F[it2]; a.ext.w1 = F[h + it2];
                 launch_step<1, EPI_NONE>(e, a, cur);
+                if (wfld) save_wavefield(e, wfld, p0, its, F[it2], F[h + it2]);
                 std::swap(p0, p1);
                 cur ^= 1;
             }
@@ -872,7 +886,7 @@ static void d2h(Engine* e, float* h, const DBuf& b, size_t count) {
     if (count) EIO_CUDA(cudaMemcpyAsync(h, b.p, sizeof(float) * count, cudaMemcpyDeviceToHost, e->st));
 }
 
-void engine_nl_host(Engine* e, int adj, float* const model[5], float* const data[5], const ShotGeom& g) {
+void engine_nl_host(Engine* e, int adj, float* const model[5], float* const data[5], const ShotGeom& g, float* wfld) {
     EIO_CUDA(cudaSetDevice(e->device));
     float* dmod[5]; float* ddat[5];
     size_t nm[5], nd[5];
@@ -884,7 +898,15 @@ void engine_nl_host(Engine* e, int adj, float* const model[5], float* const data
         dmod[f] = e->stage_a[f].f();
         ddat[f] = e->stage_b[f].f();
     }
-    engine_nl(e, adj, dmod, ddat, g);
+    float* wdev = nullptr;
+    const size_t wcount = (size_t)5 * e->nts * e->n;
+    if (wfld) {
+        e->wsave.ensure(sizeof(float) * wcount);
+        EIO_CUDA(cudaMemsetAsync(e->wsave.p, 0, sizeof(float) * wcount, e->st));
+        wdev = e->wsave.f();
+    }
+    engine_nl(e, adj, dmod, ddat, g, wdev);
+    if (wfld) d2h(e, wfld, e->wsave, wcount);
     for (int f = 0; f < 5; f++) {
         if (!adj) d2h(e, data[f], e->stage_b[f], nd[f]);
         else d2h(e, model[f], e->stage_a[f], nm[f]);

@@ -656,8 +656,9 @@ void check_nt(const ShotGrids& g, int nts) {
             throw Error(EIO_ERR_ARG, "the four staggered grids of a shot must hold the same devices");
 }
 
-// nonlinearPropElasticGpu::forward with add = false: irregular source -> data slice
-void nl_shot_forward(eio_ctx* c, const ShotGrids& g, const float* model, float* data) {
+// nonlinearPropElasticGpu::forward with add = false: irregular source -> data slice;
+// wfld (host [nts][5][nx][nz]) receives the saved wavefield when not null
+void nl_shot_forward(eio_ctx* c, const ShotGrids& g, const float* model, float* data, float* wfld = nullptr) {
     const int nts = c->fd.p.nts;
     const int nsi = g.s[0]->nIrreg, nri = g.r[0]->nIrreg;
     std::vector<float> reg[5], dreg[5];
@@ -672,13 +673,30 @@ void nl_shot_forward(eio_ctx* c, const ShotGrids& g, const float* model, float* 
         dreg[f].assign((size_t)g.r[kFG[f]]->nReg * nts, 0.f);
         mp[f] = reg[f].data(); dp[f] = dreg[f].data();
     }
-    engine_nl_host(c->eng, 0, mp, dp, reg_geom(g));
+    engine_nl_host(c->eng, 0, mp, dp, reg_geom(g), wfld);
     std::fill(data, data + (size_t)5 * nri * nts, 0.f);
     for (int f = 0; f < 5; f++) sinterp_forward(*g.r[kFG[f]], true, dreg[f].data(), data + (size_t)f * nri * nts);
 }
 
-// nonlinearPropElasticGpu::adjoint with add = true into model
-void nl_shot_adjoint(eio_ctx* c, const ShotGrids& g, float* model, const float* data) {
+// The adjoint wavefield is scaled like the adjoint sources
+// (nonlinearPropElasticGpu.cpp:432-446): vx by rhoxDtw, vz by rhozDtw, the
+// stresses by 2*dtw (in double, as the reference), all by 1/(dx*dz).
+static void scale_adjoint_wavefield(const FdParam& fd, float* w) {
+    const float area = (float)(1.0 / (fd.p.dx * fd.p.dz));
+    const size_t n = (size_t)fd.p.nz * fd.p.nx;
+    const double tdtw = 2.0 * (double)fd.dtw * (double)area;
+    for (int it = 0; it < fd.p.nts; it++) {
+        float* slice = w + (size_t)it * 5 * n;
+        for (size_t i = 0; i < n; i++) {
+            slice[i] *= fd.par[0][i] * area;
+            slice[n + i] *= fd.par[1][i] * area;
+        }
+        for (size_t i = 2 * n; i < 5 * n; i++) slice[i] = (float)((double)slice[i] * tdtw);
+    }
+}
+
+// nonlinearPropElasticGpu::adjoint with add = true into model; wfld as for nl_shot_forward
+void nl_shot_adjoint(eio_ctx* c, const ShotGrids& g, float* model, const float* data, float* wfld = nullptr) {
     const int nts = c->fd.p.nts;
     const int nsi = g.s[0]->nIrreg, nri = g.r[0]->nIrreg;
     std::vector<float> reg[5], dreg[5];
@@ -690,7 +708,8 @@ void nl_shot_adjoint(eio_ctx* c, const ShotGrids& g, float* model, const float* 
         reg[f].assign((size_t)g.s[kFG[f]]->nReg * nts, 0.f);
         mp[f] = reg[f].data(); dp[f] = dreg[f].data();
     }
-    engine_nl_host(c->eng, 1, mp, dp, reg_geom(g));
+    engine_nl_host(c->eng, 1, mp, dp, reg_geom(g), wfld);
+    if (wfld) scale_adjoint_wavefield(c->fd, wfld);
     scale_sources_adj(c->fd, g, reg, nts);
     for (int f = 0; f < 5; f++) sinterp_forward(*g.s[kFG[f]], true, reg[f].data(), model + (size_t)f * nsi * nts);
 }
@@ -786,8 +805,8 @@ EIO_API int eio_born_prepare_model(eio_ctx* c, const float* model, float* const 
     });
 }
 
-EIO_API int eio_nl_forward(eio_ctx* c, int add, int nExp, int nModelExp, const float* model, float* data,
-                           eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom) {
+static int nl_forward_impl(eio_ctx* c, int add, int nExp, int nModelExp, const float* model, float* data,
+                           eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom, int wShot, float* wfld) {
     return guarded([&] {
         if (!c || !model || !data || !src || !rec || nExp < 1) throw Error(EIO_ERR_ARG, "null argument");
         if (nModelExp != 1 && nModelExp != nExp) throw Error(EIO_ERR_ARG, "model shot axis must be 1 or nExp");
@@ -803,15 +822,16 @@ EIO_API int eio_nl_forward(eio_ctx* c, int add, int nExp, int nModelExp, const f
             check_nt(g, nts);
             if ((size_t)5 * g.s[0]->nIrreg * nts != mslice || (size_t)5 * g.r[0]->nIrreg * nts != dslice)
                 throw Error(EIO_ERR_ARG, "device counts differ between shots");
-            nl_shot_forward(c, g, model + (nModelExp == 1 ? 0 : (size_t)e * mslice), tmp.data());
+            nl_shot_forward(c, g, model + (nModelExp == 1 ? 0 : (size_t)e * mslice), tmp.data(),
+                            e == wShot ? wfld : nullptr);
             float* d = data + (size_t)e * dslice;
             for (size_t i = 0; i < dslice; i++) d[i] += tmp[i];
         }
     });
 }
 
-EIO_API int eio_nl_adjoint(eio_ctx* c, int add, int nExp, int nModelExp, float* model, const float* data,
-                           eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom) {
+static int nl_adjoint_impl(eio_ctx* c, int add, int nExp, int nModelExp, float* model, const float* data,
+                           eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom, int wShot, float* wfld) {
     return guarded([&] {
         if (!c || !model || !data || !src || !rec || nExp < 1) throw Error(EIO_ERR_ARG, "null argument");
         if (nModelExp != 1 && nModelExp != nExp) throw Error(EIO_ERR_ARG, "model shot axis must be 1 or nExp");
@@ -829,10 +849,10 @@ EIO_API int eio_nl_adjoint(eio_ctx* c, int add, int nExp, int nModelExp, float* 
                 throw Error(EIO_ERR_ARG, "device counts differ between shots");
             if (nModelExp == 1) {
                 // constant source signal: stack every shot (nonlinearPropElasticShotsGpu.cpp:384-417)
-                nl_shot_adjoint(c, g, slice.data(), data + (size_t)e * dslice);
+                nl_shot_adjoint(c, g, slice.data(), data + (size_t)e * dslice, e == wShot ? wfld : nullptr);
             } else {
                 std::fill(slice.begin(), slice.end(), 0.f);
-                nl_shot_adjoint(c, g, slice.data(), data + (size_t)e * dslice);
+                nl_shot_adjoint(c, g, slice.data(), data + (size_t)e * dslice, e == wShot ? wfld : nullptr);
                 float* m = model + (size_t)e * mslice;
                 for (size_t i = 0; i < mslice; i++) m[i] += slice[i];
             }
@@ -840,6 +860,37 @@ EIO_API int eio_nl_adjoint(eio_ctx* c, int add, int nExp, int nModelExp, float* 
         if (nModelExp == 1)
             for (size_t i = 0; i < mslice; i++) model[i] += slice[i];
     });
+}
+
+EIO_API int eio_nl_forward(eio_ctx* c, int add, int nExp, int nModelExp, const float* model, float* data,
+                           eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom) {
+    return nl_forward_impl(c, add, nExp, nModelExp, model, data, src, rec, nRecGeom, -1, nullptr);
+}
+
+EIO_API int eio_nl_adjoint(eio_ctx* c, int add, int nExp, int nModelExp, float* model, const float* data,
+                           eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom) {
+    return nl_adjoint_impl(c, add, nExp, nModelExp, model, data, src, rec, nRecGeom, -1, nullptr);
+}
+
+static void check_wavefield_shot(int nExp, int wShot, const float* wfld) {
+    if (wShot >= nExp) throw Error(EIO_ERR_ARG, "wavefield shot number beyond the number of shots");
+    if (wShot >= 0 && !wfld) throw Error(EIO_ERR_ARG, "null wavefield buffer");
+}
+
+EIO_API int eio_nl_forward_wavefield(eio_ctx* c, int add, int nExp, int nModelExp, const float* model, float* data,
+                                     eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom, int wShot,
+                                     float* wfld) {
+    const int st = guarded([&] { check_wavefield_shot(nExp, wShot, wfld); });
+    if (st) return st;
+    return nl_forward_impl(c, add, nExp, nModelExp, model, data, src, rec, nRecGeom, wShot, wfld);
+}
+
+EIO_API int eio_nl_adjoint_wavefield(eio_ctx* c, int add, int nExp, int nModelExp, float* model, const float* data,
+                                     eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom, int wShot,
+                                     float* wfld) {
+    const int st = guarded([&] { check_wavefield_shot(nExp, wShot, wfld); });
+    if (st) return st;
+    return nl_adjoint_impl(c, add, nExp, nModelExp, model, data, src, rec, nRecGeom, wShot, wfld);
 }
 
 EIO_API int eio_born_forward(eio_ctx* c, int add, int nExp, const float* model, float* data,

@@ -76,11 +76,16 @@ struct ShotGeom {
     const int* recPos[4]; int nRec[4];
 };
 // all float arrays are device pointers
-void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], const ShotGeom& g);
+// wfld (device, [nts][5][nx][nz], zeroed by the caller) receives the coarse
+// samples of every fine step's new level when not null
+void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], const ShotGeom& g,
+               float* wfld = nullptr);
 void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5], float* const data[5],
                  const ShotGeom& g);
 // host-pointer convenience wrappers (copy in/out through the engine's staging buffers)
-void engine_nl_host(Engine* e, int adj, float* const model[5], float* const data[5], const ShotGeom& g);
+// wfld: host [nts][5][nx][nz], overwritten with the saved wavefield when not null
+void engine_nl_host(Engine* e, int adj, float* const model[5], float* const data[5], const ShotGeom& g,
+                    float* wfld = nullptr);
 void engine_born_host(Engine* e, int adj, float* const srcDtw[5], float* const dm[5], float* const data[5],
                       const ShotGeom& g);
 }  // namespace eio

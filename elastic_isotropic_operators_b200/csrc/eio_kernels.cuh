@@ -632,6 +632,39 @@ __global__ void __launch_bounds__(NT) k_imaging(ImagingArgs a)
     }
 }
 
+// Coarse-time sample of all five fields of the new level (interpWavefield,
+// K:1258-1291): W[its][f] += p[f] * w0 and W[its+1][f] += p[f] * w1 at every
+// interior cell, W laid out [nts][5][nx][nz].  One float4 of z per thread.
+struct SaveArgs {
+    const float* p[5];
+    float* W;
+    long long n;              // nx * nz
+    int nz, nx, its;
+    float w0, w1;
+};
+
+__global__ void __launch_bounds__(128) k_save_wavefield(SaveArgs a)
+{
+    const int gz = FAT + 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const int gx = FAT + blockIdx.y;
+    if (gz >= a.nz - FAT) return;
+    const long long gi = (long long)gx * a.nz + gz;
+#pragma unroll
+    for (int f = 0; f < 5; f++) {
+        const float4 v = ld4(a.p[f] + gi);
+        float* r0 = a.W + ((long long)a.its * 5 + f) * a.n + gi;
+        float* r1 = r0 + 5 * a.n;
+        float4 u0 = ld4(r0), u1 = ld4(r1);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            at(u0, j) = fmaf(at(v, j), a.w0, at(u0, j));
+            at(u1, j) = fmaf(at(v, j), a.w1, at(u1, j));
+        }
+        st4(r0, u0);
+        st4(r1, u1);
+    }
+}
+
 // time-major <-> trace-major transposes for the sparse signal matrices
 __global__ void k_transpose(const float* __restrict__ in, float* __restrict__ out, int rows, int cols)
 {

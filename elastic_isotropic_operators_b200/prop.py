@@ -312,6 +312,60 @@ class nonlinearPropElasticShotsGpu(_ElasticOp):
         if mm is not m:
             m[...] = mm
 
+    # ---- wavefield output (nonlinearPropElasticShotsGpu.cpp:185-300, 424-540):
+    # with par saveWavefield = 1 the shot wavefieldShotNumber (0-based) keeps its
+    # wavefield [nts][5][nx][nz]; the adjoint one is scaled like the adjoint sources.
+    def _wavefield_shot(self):
+        save = self.par.getInt("saveWavefield", 0)
+        shot = self.par.getInt("wavefieldShotNumber", 0)
+        return shot if save != 0 and 0 <= shot < self.nExp else -1
+
+    def _new_wavefield(self, shot):
+        if shot < 0:
+            return np.zeros((1, 1, 1, 1), np.float32)
+        return np.zeros((self.fd.nts, 5, self.fd.nx, self.fd.nz), np.float32)
+
+    def forwardWavefield(self, add, model, data):
+        self._check_time(model)
+        self._check_time(data)
+        m, d, nme = self._shapes(model, data)
+        mm = np.ascontiguousarray(m, dtype=np.float32)
+        dd = np.ascontiguousarray(d, dtype=np.float32)
+        shot = self._wavefield_shot()
+        w = self._new_wavefield(shot)
+        check(self._L.eio_nl_forward_wavefield(self._ctx, int(bool(add)), self.nExp, nme, fptr(mm), fptr(dd),
+                                               self._src_arr, self._rec_arr, self.nRecGeom, shot, fptr(w)))
+        if dd is not d:
+            d[...] = dd
+        self._wavefield = w
+
+    def adjointWavefield(self, add, model, data):
+        self._check_time(model)
+        self._check_time(data)
+        m, d, nme = self._shapes(model, data)
+        mm = np.ascontiguousarray(m, dtype=np.float32)
+        dd = np.ascontiguousarray(d, dtype=np.float32)
+        shot = self._wavefield_shot()
+        w = self._new_wavefield(shot)
+        check(self._L.eio_nl_adjoint_wavefield(self._ctx, int(bool(add)), self.nExp, nme, fptr(mm), fptr(dd),
+                                               self._src_arr, self._rec_arr, self.nRecGeom, shot, fptr(w)))
+        if mm is not m:
+            m[...] = mm
+        self._wavefield = w
+
+    def getWavefield(self):
+        """The wavefield kept by the last forwardWavefield / adjointWavefield call
+        (axes z, x, component, coarse time; numpy shape (nts, 5, nx, nz))."""
+        w = getattr(self, "_wavefield", None)
+        if w is None:
+            w = self._new_wavefield(-1)
+        if w.shape[0] == 1:
+            return floatVector(hypercube(ns=[1, 1, 1, 1]), w.copy())
+        t = axis(self.fd.nts, self.fd.ots, self.fd.dts)
+        hz = axis(self.fd.nz, self.fd.oz, self.fd.dz)
+        hx = axis(self.fd.nx, self.fd.ox, self.fd.dx)
+        return floatVector(hypercube(axes=[hz, hx, axis(5), t]), w.copy())
+
     def prepareShot(self, iExp, model):
         """Regular-grid inputs of shot iExp for the single-shot eio_nl_fwd_reg_dev
         entry point: the irregular source traces ``model`` [5][nSrc][nts] spread and
@@ -335,6 +389,30 @@ class nonlinearPropElasticShotsGpu(_ElasticOp):
 
     def dotTest(self, verbose=False, maxError=0.00001):
         return self._dot_test(self.modelSpace(), self.dataSpace(), verbose, maxError)
+
+
+class nonlinearFwiPropElasticShotsGpu(nonlinearPropElasticShotsGpu):
+    """Nonlinear modelling as a function of the elastic parameters, for FWI
+    (nonlinearFwiPropElasticShotsGpu, PF/Elastic_iso_float_prop.py:1107-1149):
+    forward(add, model, data) sets model [3][nx][nz] as the background and
+    propagates the fixed source signals ``sources`` [nts, nSrc, 5, 1].
+    It has no adjoint (the reference wrapper defines none either)."""
+
+    def __init__(self, elasticParam, par, sources, sourcesVectorCenterGrid, sourcesVectorXGrid,
+                 sourcesVectorZGrid, sourcesVectorXZGrid, receiversVectorCenterGrid, receiversVectorXGrid,
+                 receiversVectorZGrid, receiversVectorXZGrid):
+        super().__init__(elasticParam, par, sourcesVectorCenterGrid, sourcesVectorXGrid, sourcesVectorZGrid,
+                         sourcesVectorXZGrid, receiversVectorCenterGrid, receiversVectorXGrid, receiversVectorZGrid,
+                         receiversVectorXZGrid)
+        src = sources.getNdArray() if hasattr(sources, "getNdArray") else sources
+        self.sources = np.array(src, dtype=np.float32, copy=True)
+
+    def forward(self, add, model, data):
+        self.setBackground(model)
+        super().forward(add, self.sources, data)
+
+    def adjoint(self, add, model, data):
+        raise NotImplementedError("the nonlinear FWI operator has no adjoint; use BornElasticShotsGpu")
 
 
 class BornElasticShotsGpu(_ElasticOp):

@@ -199,6 +199,23 @@ int eio_nl_forward(eio_ctx *c, int add, int nExp, int nModelExp, const float *mo
                    eio_sinterp *const *src, eio_sinterp *const *rec, int nRecGeom);
 int eio_nl_adjoint(eio_ctx *c, int add, int nExp, int nModelExp, float *model, const float *data,
                    eio_sinterp *const *src, eio_sinterp *const *rec, int nRecGeom);
+/* Nonlinear operators that also save the wavefield of one shot: replace
+ * nonlinearPropElasticShotsGpu::forwardWavefield / adjointWavefield
+ * (F/src/nonlinearPropElasticShotsGpu.cpp:185-300, 424-540) with the
+ * saveWavefield / wavefieldShotNumber parameters, and the drivers
+ * propShotsElastic{Fwd,Adj}GpuWavefield (F/src/nonlinearPropElasticGpuFunctions.cu:649-760, 1029-1110).
+ * For shot wShot (0-based; < 0 saves nothing) wavefield [nts][5][nx][nz] is
+ * overwritten with the coarse-time samples of every fine step's new level
+ * (interpWavefield, K:1258-1291); the adjoint wavefield is then scaled like the
+ * adjoint sources (nonlinearPropElasticGpu.cpp:432-446).  Every interior cell
+ * is saved; the reference kernel indexes z without the FAT offset (K:1262) and
+ * so leaves the last four interior rows at zero. */
+int eio_nl_forward_wavefield(eio_ctx *c, int add, int nExp, int nModelExp, const float *model, float *data,
+                             eio_sinterp *const *src, eio_sinterp *const *rec, int nRecGeom, int wShot,
+                             float *wavefield);
+int eio_nl_adjoint_wavefield(eio_ctx *c, int add, int nExp, int nModelExp, float *model, const float *data,
+                             eio_sinterp *const *src, eio_sinterp *const *rec, int nRecGeom, int wShot,
+                             float *wavefield);
 int eio_born_forward(eio_ctx *c, int add, int nExp, const float *model, float *data,
                      const float *const *srcSignals, int nSignals,
                      eio_sinterp *const *src, eio_sinterp *const *rec, int nRecGeom);

@@ -133,18 +133,23 @@ class Oracle:
           s["w"].ctypes.data, reg.ctypes.data, irreg.ctypes.data)
 
     # ---------------------------------------------------------------- propagation
-    def nl_prop(self, adj, g, medium5, model5, data5, srcPos, recPos):
+    def nl_prop(self, adj, g, medium5, model5, data5, srcPos, recPos, wavefield=None):
         """g: dict(nz, nx, dz, dx, nts, dts, S, minPad, alphaCos).  model5/data5: lists of
-        [nPts][nts] arrays of self.dt (output ones are overwritten)."""
-        f = self._fn("orc_nl_prop")
+        [nPts][nts] arrays of self.dt (output ones are overwritten).  wavefield: None or a
+        [nts][5][nx][nz] array of self.dt, overwritten with the saved wavefield."""
+        f = self._fn("orc_nl_prop_wf")
         f.argtypes = [ctypes.c_int] * 3 + [ctypes.c_float] * 2 + [ctypes.c_int, ctypes.c_float, ctypes.c_int,
-                                                                   ctypes.c_int, ctypes.c_float] + [ctypes.c_void_p] * 7
+                                                                   ctypes.c_int, ctypes.c_float] + [ctypes.c_void_p] * 8
+        wp = None if wavefield is None else wavefield.ctypes.data
         ns = (ctypes.c_int * 4)(*[len(p) for p in srcPos])
         nr = (ctypes.c_int * 4)(*[len(p) for p in recPos])
         sp = [np.ascontiguousarray(p, np.int32) for p in srcPos]
         rp = [np.ascontiguousarray(p, np.int32) for p in recPos]
+        if wavefield is not None:
+            assert wavefield.dtype == self.dt and wavefield.flags["C_CONTIGUOUS"]
+            assert wavefield.shape == (g["nts"], 5, g["nx"], g["nz"])
         r = f(adj, g["nz"], g["nx"], g["dz"], g["dx"], g["nts"], g["dts"], g["S"], g["minPad"], g["alphaCos"],
-              _pp(medium5, None), _pp(model5, None), _pp(data5, None), _pp(sp, None), ns, _pp(rp, None), nr)
+              _pp(medium5, None), _pp(model5, None), _pp(data5, None), _pp(sp, None), ns, _pp(rp, None), nr, wp)
         assert r == 0, r
 
     def born_prop(self, adj, g, medium5, srcDtw5, dm5, data5, srcPos, recPos):
@@ -174,6 +179,8 @@ class RefGpu:
                                                                        R] + [ctypes.c_void_p] * 7
         self.born.ref_born_prop.argtypes = [ctypes.c_int] * 3 + [R] * 2 + [ctypes.c_int, R, ctypes.c_int,
                                                                            ctypes.c_int, R] + [ctypes.c_void_p] * 8
+        self.nl.ref_nl_prop_wf.argtypes = [ctypes.c_int] * 3 + [R] * 2 + [ctypes.c_int, R, ctypes.c_int,
+                                                                          ctypes.c_int, R] + [ctypes.c_void_p] * 8
 
     @staticmethod
     def available(prec="f"):
@@ -184,13 +191,27 @@ class RefGpu:
         return (g["nz"], g["nx"], float(np.float32(g["dz"])), float(np.float32(g["dx"])), g["nts"],
                 float(np.float32(g["dts"])), g["S"], g["minPad"], float(np.float32(g["alphaCos"])))
 
-    def nl_prop(self, adj, g, medium5, model5, data5, srcPos, recPos):
+    @staticmethod
+    def wavefield_supported(g):
+        """The reference's wavefield drivers size their device buffer with the
+        32-bit product 5*nz*nx*nts; larger sizes are never run."""
+        return 5 * int(g["nts"]) * int(g["nz"]) * int(g["nx"]) < 2 ** 31
+
+    def nl_prop(self, adj, g, medium5, model5, data5, srcPos, recPos, wavefield=None):
         ns = (ctypes.c_int * 4)(*[len(p) for p in srcPos])
         nr = (ctypes.c_int * 4)(*[len(p) for p in recPos])
         sp = [np.ascontiguousarray(p, np.int32) for p in srcPos]
         rp = [np.ascontiguousarray(p, np.int32) for p in recPos]
-        r = self.nl.ref_nl_prop(adj, *self._g(g), _pp(medium5, None), _pp(model5, None), _pp(data5, None),
-                                _pp(sp, None), ns, _pp(rp, None), nr)
+        if wavefield is None:
+            r = self.nl.ref_nl_prop(adj, *self._g(g), _pp(medium5, None), _pp(model5, None), _pp(data5, None),
+                                    _pp(sp, None), ns, _pp(rp, None), nr)
+        else:
+            if not self.wavefield_supported(g):
+                raise ValueError("reference wavefield drivers overflow their 32-bit buffer size at this size")
+            assert wavefield.dtype == self.dt and wavefield.flags["C_CONTIGUOUS"]
+            assert wavefield.shape == (g["nts"], 5, g["nx"], g["nz"])
+            r = self.nl.ref_nl_prop_wf(adj, *self._g(g), _pp(medium5, None), _pp(model5, None), _pp(data5, None),
+                                       _pp(sp, None), ns, _pp(rp, None), nr, wavefield.ctypes.data)
         assert r == 0
 
     @staticmethod
@@ -288,8 +309,22 @@ def _reg_pos(grids):
     return [G["uniq"] for G in grids]
 
 
-def nl_forward(orc, c, model, engine=None):
-    """model [nModelExp][5][nSrc][nts] -> data [nExp][5][nRec][nts] (add = False)."""
+def scale_adjoint_wavefield(orc, g, med, W):
+    """nonlinearPropElasticGpu.cpp:432-446: vx by rhoxDtw*area, vz by rhozDtw*area
+    (products in the working precision), the stresses by 2*dtw*area in double."""
+    dt = orc.dt
+    dtw = dt(np.float32(g["dts"])) / dt(g["S"])
+    area = dt(np.float64(1.0) / np.float64(np.float32(g["dx"]) * np.float32(g["dz"])))
+    W[:, 0] *= (med[0] * area).astype(dt)
+    W[:, 1] *= (med[1] * area).astype(dt)
+    fac = np.float64(2.0) * np.float64(dtw) * np.float64(area)
+    W[:, 2:] = (W[:, 2:].astype(np.float64) * fac).astype(dt)
+    return W
+
+
+def nl_forward(orc, c, model, engine=None, wshot=None):
+    """model [nModelExp][5][nSrc][nts] -> data [nExp][5][nRec][nts] (add = False).
+    wshot: shot index whose wavefield [nts][5][nx][nz] is saved and returned too."""
     g = c.grid()
     dt = orc.dt
     med = orc.medium(c.ep, g["dts"], g["S"])
@@ -309,16 +344,21 @@ def nl_forward(orc, c, model, engine=None):
             reg.append(r)
         _scale_sources(orc, g, med, src, reg)
         dreg = [np.zeros((len(rec[FIELD_GRID[f]]["uniq"]), nts), dt) for f in range(5)]
-        eng.nl_prop(0, g, med, reg, dreg, _reg_pos(src), _reg_pos(rec))
+        if e == wshot:
+            W = np.zeros((nts, 5, g["nx"], g["nz"]), dt)
+            eng.nl_prop(0, g, med, reg, dreg, _reg_pos(src), _reg_pos(rec), W)
+        else:
+            eng.nl_prop(0, g, med, reg, dreg, _reg_pos(src), _reg_pos(rec))
         for f in range(5):
             out = np.zeros((nrec, nts), dt)
             orc.sinterp_apply(rec[FIELD_GRID[f]], 0, 1, dreg[f], out)
             data[e, f] += out
-    return data
+    return data if wshot is None else (data, W)
 
 
-def nl_adjoint(orc, c, data, nModelExp=1, engine=None):
-    """data [nExp][5][nRec][nts] -> model [nModelExp][5][nSrc][nts] (add = False)."""
+def nl_adjoint(orc, c, data, nModelExp=1, engine=None, wshot=None):
+    """data [nExp][5][nRec][nts] -> model [nModelExp][5][nSrc][nts] (add = False).
+    wshot: shot index whose (scaled) adjoint wavefield is saved and returned too."""
     g = c.grid()
     dt = orc.dt
     med = orc.medium(c.ep, g["dts"], g["S"])
@@ -338,7 +378,12 @@ def nl_adjoint(orc, c, data, nModelExp=1, engine=None):
             orc.sinterp_apply(G, 1, 0, r, np.ascontiguousarray(d[f]))
             dreg.append(r)
         reg = [np.zeros((len(src[FIELD_GRID[f]]["uniq"]), nts), dt) for f in range(5)]
-        eng.nl_prop(1, g, med, reg, dreg, _reg_pos(src), _reg_pos(rec))
+        if e == wshot:
+            W = np.zeros((nts, 5, g["nx"], g["nz"]), dt)
+            eng.nl_prop(1, g, med, reg, dreg, _reg_pos(src), _reg_pos(rec), W)
+            scale_adjoint_wavefield(orc, g, med, W)
+        else:
+            eng.nl_prop(1, g, med, reg, dreg, _reg_pos(src), _reg_pos(rec))
         _scale_sources(orc, g, med, src, reg, adjoint_order=True)
         target = stack if nModelExp == 1 else np.zeros((5, nsrc, nts), dt)
         for f in range(5):
@@ -347,7 +392,7 @@ def nl_adjoint(orc, c, data, nModelExp=1, engine=None):
             model[e] += target
     if nModelExp == 1:
         model[0] += stack
-    return model
+    return model if wshot is None else (model, W)
 
 
 def born_sources(orc, c, g, med, src, sig):

@@ -482,9 +482,29 @@ static void FN(orc_inject_fine)(const FN(orc_grid_t) *g, REAL **p, REAL *const *
 /* model: 5 source arrays [nSrcReg(grid)][nts]; data: 5 [nRecReg][nts] */
 /* fwd overwrites data, adj overwrites model                           */
 /* ------------------------------------------------------------------ */
-int FN(orc_nl_prop)(int adj, int nz, int nx, float dz, float dx, int nts, float dts, int sub_int,
-                    int minPad, float alphaCos, REAL *const *medium5, REAL *const *model, REAL *const *data,
-                    const int *const *srcPos, const int *nSrc, const int *const *recPos, const int *nRec)
+/* interpWavefield (K:1258-1291): coarse-time samples of the new level of all
+ * five fields, W [nts][5][nx][nz]; every interior cell (the reference kernel
+ * omits the FAT offset in z at K:1262 and so never writes the last four
+ * interior rows; this restatement writes them). */
+static void FN(orc_save_wavefield)(const FN(orc_grid_t) *g, REAL **p, REAL *W, int its, int fi)
+{
+    const long n = (long)g->nz * g->nx;
+#pragma omp parallel for
+    for (int ix = ORC_FAT; ix < g->nx - ORC_FAT; ix++)
+        for (int f = 0; f < 5; f++)
+            for (int iz = ORC_FAT; iz < g->nz - ORC_FAT; iz++) {
+                const long i = (long)ix * g->nz + iz;
+                W[((long)its * 5 + f) * n + i] += p[f][i] * g->filt[fi];
+                W[((long)(its + 1) * 5 + f) * n + i] += p[f][i] * g->filt[g->h + fi];
+            }
+}
+
+/* wavefield: NULL, or [nts][5][nx][nz] overwritten with the saved wavefield
+ * (propShotsElastic{Fwd,Adj}GpuWavefield, F/prop/src/nonlinearPropElasticGpuFunctions.cu:649-760, 1029-1110) */
+int FN(orc_nl_prop_wf)(int adj, int nz, int nx, float dz, float dx, int nts, float dts, int sub_int,
+                       int minPad, float alphaCos, REAL *const *medium5, REAL *const *model, REAL *const *data,
+                       const int *const *srcPos, const int *nSrc, const int *const *recPos, const int *nRec,
+                       REAL *wavefield)
 {
     FN(orc_grid_t) g;
     if (FN(orc_grid_init)(&g, nz, nx, dz, dx, nts, dts, sub_int, minPad, alphaCos)) return -1;
@@ -495,6 +515,7 @@ int FN(orc_nl_prop)(int adj, int nz, int nx, float dz, float dx, int nts, float 
     REAL *p0[5], *p1[5], *scr[7];
     for (int f = 0; f < 5; f++) { p0[f] = buf + f * n; p1[f] = buf + (5 + f) * n; }
     for (int f = 0; f < 7; f++) scr[f] = buf + (10 + f) * n;
+    if (wavefield) memset(wavefield, 0, sizeof(REAL) * 5 * (size_t)nts * n);
     if (!adj) {
         for (int f = 0; f < 5; f++) memset(data[f], 0, sizeof(REAL) * nts * nRec[FN(orc_field_grid)[f]]);
         for (int its = 0; its < nts - 1; its++)
@@ -502,6 +523,7 @@ int FN(orc_nl_prop)(int adj, int nz, int nx, float dz, float dx, int nts, float 
                 FN(orc_step_fwd)(&g, &m, p0, p1);
                 FN(orc_inject_coarse)(&g, p0, model, srcPos, nSrc, its, it2 - 1);
                 FN(orc_damp)(&g, p0, p1);
+                if (wavefield) FN(orc_save_wavefield)(&g, p0, wavefield, its, it2);
                 FN(orc_extract_coarse)(&g, p0, data, recPos, nRec, its, it2);
                 FN(orc_swap)(p0, p1);
             }
@@ -512,12 +534,21 @@ int FN(orc_nl_prop)(int adj, int nz, int nx, float dz, float dx, int nts, float 
                 FN(orc_step_adj)(&g, &m, p0, p1, scr);
                 FN(orc_inject_coarse)(&g, p0, data, recPos, nRec, its, it2 + 1);
                 FN(orc_damp)(&g, p0, p1);
+                if (wavefield) FN(orc_save_wavefield)(&g, p0, wavefield, its, it2);
                 FN(orc_extract_coarse)(&g, p0, model, srcPos, nSrc, its, it2);
                 FN(orc_swap)(p0, p1);
             }
     }
     free(buf);
     return 0;
+}
+
+int FN(orc_nl_prop)(int adj, int nz, int nx, float dz, float dx, int nts, float dts, int sub_int,
+                    int minPad, float alphaCos, REAL *const *medium5, REAL *const *model, REAL *const *data,
+                    const int *const *srcPos, const int *nSrc, const int *const *recPos, const int *nRec)
+{
+    return FN(orc_nl_prop_wf)(adj, nz, nx, dz, dx, nts, dts, sub_int, minPad, alphaCos, medium5, model, data,
+                              srcPos, nSrc, recPos, nRec, NULL);
 }
 
 /* ------------------------------------------------------------------ */

@@ -47,6 +47,32 @@ EXPORT int ref_nl_prop(int adj, int nz, int nx, real dz, real dx, int nts, real 
     deallocateNonlinearElasticGpu(0, 0);
     return 0;
 }
+
+/* As ref_nl_prop, through the drivers that also save the wavefield
+ * (propShotsElastic{Fwd,Adj}GpuWavefield); wavefield [nts][5][nx][nz]. */
+EXPORT int ref_nl_prop_wf(int adj, int nz, int nx, real dz, real dx, int nts, real dts, int sub_int,
+                          int minPad, real alphaCos, real **medium, real **model, real **data,
+                          int **srcPos, const int *nSrc, int **recPos, const int *nRec, real *wavefield)
+{
+    /* the drivers size the device wavefield with the 32-bit product 5*nz*nx*nts */
+    if ((long long)5 * nts * nz * nx >= (1LL << 31)) return -2;
+    initNonlinearElasticGpu(dz, dx, nz, nx, nts, dts, sub_int, minPad, 16, alphaCos, 1, 0, 0);
+    allocateNonlinearElasticGpu(medium[0], medium[1], medium[2], medium[3], medium[4], 0, 0);
+    if (!adj)
+        propShotsElasticFwdGpuWavefield(model[0], model[1], model[2], model[3], model[4],
+                                        data[0], data[1], data[2], data[3], data[4],
+                                        srcPos[0], nSrc[0], srcPos[1], nSrc[1], srcPos[2], nSrc[2], srcPos[3], nSrc[3],
+                                        recPos[0], nRec[0], recPos[1], nRec[1], recPos[2], nRec[2], recPos[3], nRec[3],
+                                        wavefield, 0, 0, 0);
+    else
+        propShotsElasticAdjGpuWavefield(model[0], model[1], model[2], model[3], model[4],
+                                        data[0], data[1], data[2], data[3], data[4],
+                                        srcPos[0], nSrc[0], srcPos[1], nSrc[1], srcPos[2], nSrc[2], srcPos[3], nSrc[3],
+                                        recPos[0], nRec[0], recPos[1], nRec[1], recPos[2], nRec[2], recPos[3], nRec[3],
+                                        wavefield, 0, 0);
+    deallocateNonlinearElasticGpu(0, 0);
+    return 0;
+}
 #else
 /* srcDtw: 5 fine-time source arrays [nSrcReg][ntw]; dm: 5 [nx][nz]; data: 5 [nRecReg][nts].
  * Forward overwrites data; adjoint accumulates into dm. */

@@ -335,3 +335,93 @@ def test_sub2_running_sum_path_vs_oracle(kind):
         _nl_born_vs_oracle(c, w2, 13)
     finally:
         c.close()
+
+
+# ------------------------------------------------------------------ wavefield output
+def _wavefield_op(w, shot):
+    from elastic_isotropic_operators_b200.sepvec import paramObj
+    par = paramObj(w.par.as_dict())
+    par.set("saveWavefield", "1")
+    par.set("wavefieldShotNumber", str(shot))
+    src, rec = w.geometry()
+    return prop.nonlinearPropElasticShotsGpu(w.elastic, par, *src, *rec)
+
+
+@pytest.mark.parametrize("adj", [0, 1])
+def test_nl_wavefield_operator_vs_oracle(w, adj):
+    """forwardWavefield / adjointWavefield keep the wavefield of shot
+    wavefieldShotNumber; the adjoint one scaled like the adjoint sources."""
+    nl = _wavefield_op(w, 1)
+    c = O.Case.from_workload(w)
+    orc = O.Oracle("f")
+    rng = np.random.default_rng(8)
+    model, data = nl.modelSpace(), nl.dataSpace()
+    if not adj:
+        model.getNdArray()[...] = w.source_signal()[None]
+        nl.forwardWavefield(False, model, data)
+        want, wantW = O.nl_forward(orc, c, model.getNdArray(), wshot=1)
+        got = data.getNdArray()
+    else:
+        data.getNdArray()[...] = rng.standard_normal(data.getNdArray().shape).astype(np.float32)
+        nl.adjointWavefield(False, model, data)
+        want, wantW = O.nl_adjoint(orc, c, data.getNdArray(), wshot=1)
+        got = model.getNdArray()
+    W = nl.getWavefield().getNdArray()
+    assert W.shape == (w.nts, 5, w.nx, w.nz)
+    assert O.rel_l2(got, want) < TOL32
+    assert O.rel_l2(W, wantW) < TOL32, O.rel_l2(W, wantW)
+    assert np.abs(W).max() > 0
+
+
+def test_nl_wavefield_off_keeps_no_wavefield(w):
+    from elastic_isotropic_operators_b200.sepvec import paramObj
+    src, rec = w.geometry()
+    nl = prop.nonlinearPropElasticShotsGpu(w.elastic, paramObj(w.par.as_dict()), *src, *rec)
+    model, data = nl.modelSpace(), nl.dataSpace()
+    model.getNdArray()[...] = w.source_signal()[None]
+    nl.forwardWavefield(False, model, data)
+    assert nl.getWavefield().getNdArray().size == 1
+    ref = nl.dataSpace()
+    nl.forward(False, model, ref)
+    assert np.array_equal(ref.getNdArray(), data.getNdArray())
+
+
+@pytest.mark.skipif(not ref_available, reason="oracle/_ref not built")
+@pytest.mark.parametrize("adj", [0, 1])
+def test_reference_wavefield_pins_oracle(w, adj):
+    """The reference's own wavefield drivers agree with the oracle on every cell
+    they write; their kernel omits the FAT offset in z (K:1262), so the last four
+    interior rows stay zero there."""
+    for prec, tol in (("f", TOL32), ("d", 1e-10)):
+        r = reg_inputs(w, prec, seed=21)
+        g = r["g"]
+        orc, ref = r["orc"], O.RefGpu(prec)
+        Wo = np.zeros((g["nts"], 5, g["nx"], g["nz"]), orc.dt)
+        Wr = np.zeros_like(Wo)
+        mo, do_ = _copy(r["model"]), _copy(r["data"])
+        mr, dr = _copy(r["model"]), _copy(r["data"])
+        orc.nl_prop(adj, g, r["med"], mo, do_, r["sp"], r["rp"], Wo)
+        ref.nl_prop(adj, g, r["med"], mr, dr, r["sp"], r["rp"], Wr)
+        nz = g["nz"]
+        assert not Wr[..., nz - 8:nz - 4].any()
+        assert O.rel_l2(Wr[..., :nz - 8], Wo[..., :nz - 8]) < tol, (prec, adj)
+
+
+def test_nonlinear_fwi_operator_sets_background_then_propagates(w):
+    """nonlinearFwiPropElasticShotsGpu.forward(model) = setBackground(model) + forward(sources)."""
+    src, rec = w.geometry()
+    sig = w.source_signal()[None]
+    fwi = prop.nonlinearFwiPropElasticShotsGpu(w.elastic, w.par, sig, *src, *rec)
+    nl = prop.nonlinearPropElasticShotsGpu(w.elastic, w.par, *src, *rec)
+    model2 = w.elastic.clone()
+    model2.getNdArray()[...] = w.elastic.getNdArray() * np.float32(1.02)
+    d_fwi = fwi.dataSpace()
+    fwi.forward(False, model2, d_fwi)
+    nl.setBackground(model2)
+    d_nl = nl.dataSpace()
+    m = nl.modelSpace()
+    m.getNdArray()[...] = sig
+    nl.forward(False, m, d_nl)
+    assert np.array_equal(d_fwi.getNdArray(), d_nl.getNdArray())
+    with pytest.raises(NotImplementedError):
+        fwi.adjoint(False, model2, d_fwi)

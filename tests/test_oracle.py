@@ -173,3 +173,29 @@ def test_born_is_derivative_of_nonlinear(small_case):
         errs.append(O.rel_l2(born, fd))
     assert max(errs) < 3e-2
     assert abs(errs[0] - errs[1]) < 0.1 * errs[0]   # h-independent: no nonlinear residue left
+
+
+@pytest.mark.parametrize("adj", [0, 1])
+def test_saved_wavefield_equals_traces_at_the_devices(adj):
+    """The saved wavefield (interpWavefield, K:1258-1291) and the recorded traces
+    (K:7-60, 100-116) are the same coarse-time samples of the same level, so at
+    the receiver cells (forward) or source cells (adjoint, before scaling) they
+    agree exactly."""
+    from elastic_isotropic_operators_b200 import synthetic
+    from helpers import reg_inputs
+    w = synthetic.small(nts=60)
+    r = reg_inputs(w, "f", seed=3)
+    orc, g = r["orc"], r["g"]
+    W = np.zeros((g["nts"], 5, g["nx"], g["nz"]), np.float32)
+    m = [x.copy() for x in r["model"]]
+    d = [x.copy() for x in r["data"]]
+    orc.nl_prop(adj, g, r["med"], m, d, r["sp"], r["rp"], W)
+    traces, pos = (m, r["sp"]) if adj else (d, r["rp"])
+    flat = W.reshape(g["nts"], 5, -1)
+    for f in range(5):
+        got = flat[:, f, pos[O.FIELD_GRID[f]]].T
+        assert np.array_equal(got, traces[f]), f
+    assert np.abs(W).max() > 0
+    # nothing is written outside the updated interior
+    assert not W[:, :, :4].any() and not W[:, :, -4:].any()
+    assert not W[..., :4].any() and not W[..., -4:].any()
