@@ -21,6 +21,8 @@ import math
 
 import numpy as np
 
+from . import padding
+
 from .sepvec import axis, hypercube, floatVector, paramObj
 
 FAT = 4
@@ -39,21 +41,7 @@ def elastic_from_vpvsrho(vp, vs, rho):
 
 def pad_elastic(ep, zPad, xPad, fat=FAT, blockSize=16):
     """ep: [npar][nx][nz] -> padded array and the pad sizes (surfaceCondition = 0)."""
-    npar, nx, nz = ep.shape
-    nzTotal = zPad * 2 + nz
-    zPadPlus = int(math.ceil(float(nzTotal) / blockSize)) * blockSize - nz - zPad
-    nxTotal = xPad * 2 + nx
-    xPadPlus = int(math.ceil(float(nxTotal) / blockSize)) * blockSize - nx - xPad
-    nzN = zPad + zPadPlus + nz + 2 * fat
-    nxN = xPad + xPadPlus + nx + 2 * fat
-    out = np.zeros((npar, nxN, nzN), dtype=np.float32)
-    z0, x0 = fat + zPad, fat + xPad
-    out[:, x0:x0 + nx, z0:z0 + nz] = ep
-    out[:, x0:x0 + nx, :z0] = ep[:, :, :1]
-    out[:, x0:x0 + nx, z0 + nz:] = ep[:, :, -1:]
-    out[:, :x0, :] = out[:, x0:x0 + 1, :]
-    out[:, x0 + nx:, :] = out[:, x0 + nx - 1:x0 + nx, :]
-    return out, dict(zPadMinus=zPad, zPadPlus=zPadPlus, xPadMinus=xPad, xPadPlus=xPadPlus)
+    return padding.pad_elastic_array(ep, zPad, xPad, fat, blockSize, 0)
 
 
 def ricker(nts, dts, fdom, delay, ots=0.0):
