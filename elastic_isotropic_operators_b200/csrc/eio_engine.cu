@@ -80,7 +80,8 @@ struct Engine {
     std::vector<float> filt;
     float dts_inv = 0.f;
     int ntz = 0, ntx = 0, ntiles = 0;
-    int ckpt = 0;
+    int ckpt = 0;           // source-wavefield snapshots: 0 FP32, 1 BF16, 2 FP16 (scaled per snapshot)
+    DBuf Wq, wscale, wstage, wpmax;   // 16-bit history, scales [nts][2], FP32 staging row pair, warp maxima
     DBuf par[5], dampz, dampx, wf[10];
     DBuf inj_ts, inj_ent, ext_ts, ext_ent;
     DBuf sig_in[5], sig_out[5];
@@ -214,7 +215,8 @@ void engine_destroy(Engine* e) {
     cudaSetDevice(e->device);
     if (e->st) cudaStreamSynchronize(e->st);
     if (e->st2) cudaStreamSynchronize(e->st2);
-    DBuf* all[] = {&e->dampz, &e->dampx, &e->inj_ts, &e->inj_ent, &e->ext_ts, &e->ext_ent, &e->W, &e->err, &e->wsave};
+    DBuf* all[] = {&e->dampz, &e->dampx, &e->inj_ts, &e->inj_ent, &e->ext_ts, &e->ext_ent, &e->W, &e->err, &e->wsave,
+                   &e->Wq, &e->wscale, &e->wstage, &e->wpmax};
     for (DBuf* b : all) b->release();
     for (int f = 0; f < 5; f++) {
         e->par[f].release(); e->sig_in[f].release(); e->sig_out[f].release();
@@ -234,7 +236,7 @@ void engine_destroy(Engine* e) {
 }
 
 void engine_set_checkpoint(Engine* e, int mode) {
-    if (mode != 0) throw Error(EIO_ERR_UNSUPPORTED, "only FP32 source-wavefield snapshots are available");
+    if (mode < 0 || mode > 2) throw Error(EIO_ERR_ARG, "checkpoint precision must be 0 (FP32), 1 (BF16) or 2 (FP16)");
     e->ckpt = mode;
 }
 
@@ -680,16 +682,29 @@ static void launch_imaging(Engine* e, int adj, int its, float* const dm[5], floa
                            cudaStream_t st) {
     ImagingArgs ia;
     memset(&ia, 0, sizeof(ia));
-    ia.Wvx = e->W.f();
-    ia.Wvz = e->W.f() + (long long)e->nts * e->n;
+    if (e->ckpt) {
+        const unsigned short* wq = static_cast<const unsigned short*>(e->Wq.p);
+        ia.Wvx = wq;
+        ia.Wvz = wq + (long long)e->nts * e->n;
+        ia.wscale = e->wscale.f();
+    } else {
+        ia.Wvx = e->W.f();
+        ia.Wvz = e->W.f() + (long long)e->nts * e->n;
+    }
     ia.wstride = e->n;
     ia.nz = e->nz; ia.nx = e->nx; ia.nts = e->nts; ia.its = its;
     for (int i = 0; i < 4; i++) { ia.cz[i] = e->zc[i]; ia.cx[i] = e->xc[i]; }
     ia.dts_inv = e->dts_inv;
     for (int f = 0; f < 5; f++) { ia.dm[f] = dm[f]; ia.ss[f] = ss[f]; }
     const int ntiles = ((e->nz - 2 * FAT + TZ - 1) / TZ) * ((e->nx - 2 * FAT) / TX);
-    if (adj) k_imaging<1><<<ntiles, NT, 0, st>>>(ia);
-    else k_imaging<0><<<ntiles, NT, 0, st>>>(ia);
+    switch (e->ckpt * 2 + adj) {
+        case 0: k_imaging<0, 0><<<ntiles, NT, 0, st>>>(ia); break;
+        case 1: k_imaging<1, 0><<<ntiles, NT, 0, st>>>(ia); break;
+        case 2: k_imaging<0, 1><<<ntiles, NT, 0, st>>>(ia); break;
+        case 3: k_imaging<1, 1><<<ntiles, NT, 0, st>>>(ia); break;
+        case 4: k_imaging<0, 2><<<ntiles, NT, 0, st>>>(ia); break;
+        default: k_imaging<1, 2><<<ntiles, NT, 0, st>>>(ia); break;
+    }
     e->launches++;
 }
 
@@ -700,7 +715,98 @@ static void launch_imaging(Engine* e, int adj, int its, float* const dm[5], floa
 // that the step (its, it2 = 1) holds as its old, current and new level, so
 // that step writes the row once (EPI_TRI, same operation order) and the other
 // steps touch no history at all; other sub values keep the running sums.
+// 16-bit checkpoints: the coarse sample the EPI_TRI step just wrote to the
+// FP32 staging rows becomes row `row` of the 16-bit history
+static void quantize_row(Engine* e, int row) {
+    const int npart = e->ntiles * 16;
+    float* pm = e->wpmax.f();
+    QuantArgs q;
+    q.stage[0] = e->wstage.f();
+    q.stage[1] = e->wstage.f() + e->n;
+    unsigned short* wq = static_cast<unsigned short*>(e->Wq.p);
+    q.row[0] = wq + (long long)row * e->n;
+    q.row[1] = wq + ((long long)e->nts + row) * e->n;
+    q.scale = e->wscale.f() + 2 * row;
+    q.pmax = pm + (size_t)(row & 1) * 2 * npart;
+    q.pmax_next = pm + (size_t)((row + 1) & 1) * 2 * npart;
+    q.npart = npart;
+    q.nz = e->nz; q.nx = e->nx;
+    const int grid = 2 * e->nsm;
+    if (e->ckpt == 1) k_quantize<1><<<grid, 256, 0, e->st>>>(q);
+    else k_quantize<2><<<grid, 256, 0, e->st>>>(q);
+    e->launches++;
+}
+
+// Source wavefield with 16-bit snapshots (sub = 1 only): every coarse sample
+// goes through the FP32 staging rows, its scale comes from the warp maxima the
+// step leaves, and k_quantize stores the codes.  The tile kernels write the
+// maxima, so the sweep kernel is not used here.
+static void born_source_q(Engine* e, const PointList& src, StepArgs a) {
+    if (e->S != 2)
+        throw Error(EIO_ERR_UNSUPPORTED, "16-bit source-wavefield snapshots need sub = 1 (two fine steps per sample)");
+    const size_t qbytes = sizeof(unsigned short) * 2 * (size_t)e->nts * e->n;
+    if (e->Wq.cap < qbytes) {
+        e->Wq.ensure(qbytes);
+        EIO_CUDA(cudaMemsetAsync(e->Wq.p, 0, qbytes, e->st));   // the FAT frame is never written
+    }
+    if (e->wstage.cap < sizeof(float) * 2 * (size_t)e->n) {
+        e->wstage.ensure(sizeof(float) * 2 * (size_t)e->n);
+        EIO_CUDA(cudaMemsetAsync(e->wstage.p, 0, sizeof(float) * 2 * (size_t)e->n, e->st));
+    }
+    e->wscale.ensure(sizeof(float) * 2 * (size_t)e->nts);
+    const size_t pbytes = sizeof(float) * 2 * 2 * (size_t)e->ntiles * 16;
+    e->wpmax.ensure(pbytes);
+    EIO_CUDA(cudaMemsetAsync(e->wpmax.p, 0, pbytes, e->st));
+    const int kind = e->kind;
+    if (kind == 1) e->kind = 0;
+    zero_wavefields(e);
+    float* p0[5]; float* p1[5];
+    for (int f = 0; f < 5; f++) { p0[f] = e->wf[f].f(); p1[f] = e->wf[5 + f].f(); }
+    int cur = 0;
+    a.inj = upload_points(e, src, e->inj_ts, e->inj_ent, e->sig_in);
+    memset(&a.ext, 0, sizeof(a.ext));
+    a.W0 = e->wstage.f();
+    a.W1 = e->wstage.f() + e->n;
+    a.wt = 0;
+    const float* F = e->filt.data();
+    const int h = e->h;
+    const int npart = e->ntiles * 16;
+    try {
+        for (int its = 0; its < e->nts - 1; its++)
+            for (int it2 = 1; it2 < e->S + 1; it2++) {
+                const int itw = its * e->S + it2;
+                for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; }
+                a.inj.t0 = itw - 1; a.inj.w0 = 1.f; a.inj.w1 = 0.f;
+                const bool last = (its == e->nts - 2 && it2 == 2);
+                int row = -1;
+                if (it2 == 1) {
+                    a.tmode = 1; row = its; a.tw_o = F[h + 1]; a.tw_c = F[h + 2]; a.tw_n = F[1];
+                } else if (last) {
+                    a.tmode = 2; row = its + 1; a.tw_o = 0.f; a.tw_c = F[h + 1]; a.tw_n = F[h + 2];
+                }
+                if (row >= 0) {
+                    a.pmax = e->wpmax.f() + (size_t)(row & 1) * 2 * npart;
+                    launch_step<0, EPI_TRI>(e, a, cur);
+                    quantize_row(e, row);
+                } else {
+                    launch_step<0, EPI_NONE>(e, a, cur);
+                }
+                std::swap(p0, p1);
+                cur ^= 1;
+            }
+    } catch (...) {
+        e->kind = kind;
+        throw;
+    }
+    e->kind = kind;
+    check_launch();
+}
+
 static void born_source(Engine* e, const PointList& src, StepArgs a) {
+    if (e->ckpt) {
+        born_source_q(e, src, a);
+        return;
+    }
     const size_t wbytes = sizeof(float) * 2 * (size_t)e->nts * e->n;
     const bool fresh = e->W.cap < wbytes;
     e->W.ensure(wbytes);
@@ -750,7 +856,6 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
     EIO_CUDA(cudaSetDevice(e->device));
     if (!e->tuned) engine_autotune(e);
     err_reset(e);
-    if (e->ckpt != 0) throw Error(EIO_ERR_UNSUPPORTED, "checkpoint mode");
     PointList src, rec;
     build_points(e, g.srcPos, g.nSrc, src);
     build_points(e, g.recPos, g.nRec, rec);

@@ -28,6 +28,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 namespace eio {
 
 constexpr int FAT = 4;
@@ -81,6 +84,9 @@ struct StepArgs {
     // forward: vx, vz into row wt of W0 / W1;  adjoint: all five fields into eL[f]
     int tmode;
     float tw_o, tw_c, tw_n;
+    // 16-bit checkpoints: forward EPI_TRI also leaves, per tile and warp, the
+    // largest |sample| of vx and vz in pmax[(tile * 16 + warp) * 2 + {0, 1}]
+    float* pmax;
 };
 
 enum { EPI_NONE = 0, EPI_SAVE_W = 1, EPI_INJ_SS = 2, EPI_EXT_SS = 3, EPI_TRI = 4 };
@@ -282,6 +288,7 @@ __device__ __forceinline__ void step_tail(const StepArgs& a, float* scratch, int
                                           const float4 (&csave)[2])
 {
     float4 osave[5];      // old level (EPI_TRI)
+    float tri_max[2] = {0.f, 0.f};   // |max| of this thread's coarse samples (16-bit checkpoints)
     float dd[4];
     {
         const float dxc = __ldg(a.dampx + gx);
@@ -370,15 +377,29 @@ __device__ __forceinline__ void step_tail(const StepArgs& a, float* scratch, int
         if (EPI == EPI_TRI && a.tmode) {
             if (DIR == 0) {
                 if (F0 == 0) {
-                    st4(a.W0 + (long long)a.wt * a.wstride + gi,
-                        tri_sample(a.tmode, osave[0], csave[0], t[0], a.tw_o, a.tw_c, a.tw_n));
-                    st4(a.W1 + (long long)a.wt * a.wstride + gi,
-                        tri_sample(a.tmode, osave[1], csave[1], t[1], a.tw_o, a.tw_c, a.tw_n));
+                    const float4 s0 = tri_sample(a.tmode, osave[0], csave[0], t[0], a.tw_o, a.tw_c, a.tw_n);
+                    const float4 s1 = tri_sample(a.tmode, osave[1], csave[1], t[1], a.tw_o, a.tw_c, a.tw_n);
+                    st4(a.W0 + (long long)a.wt * a.wstride + gi, s0);
+                    st4(a.W1 + (long long)a.wt * a.wstride + gi, s1);
+                    tri_max[0] = fmaxf(fmaxf(fabsf(s0.x), fabsf(s0.y)), fmaxf(fabsf(s0.z), fabsf(s0.w)));
+                    tri_max[1] = fmaxf(fmaxf(fabsf(s1.x), fabsf(s1.y)), fmaxf(fabsf(s1.z), fabsf(s1.w)));
                 }
             } else {
 #pragma unroll
                 for (int f = F0; f < F1; f++)
                     st4(a.eL[f] + gi, tri_sample(a.tmode, osave[f], ldg4(a.c[f] + gi), t[f], a.tw_o, a.tw_c, a.tw_n));
+            }
+        }
+    }
+
+    if (EPI == EPI_TRI && DIR == 0 && F0 == 0) {
+        if (a.pmax && a.tmode) {              // uniform over the CTA
+#pragma unroll
+            for (int f = 0; f < 2; f++) {
+                float m = tri_max[f];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+                if ((tid & 31) == 0) a.pmax[((long long)tile * 16 + (tid >> 5)) * 2 + f] = m;
             }
         }
     }
@@ -524,7 +545,8 @@ __global__ void __launch_bounds__(NT2, 2) k_split(StepArgs a)
 // One thread per interior cell; W holds coarse Vx/Vz snapshots [nts][nx*nz].
 // ---------------------------------------------------------------------------
 struct ImagingArgs {
-    const float* Wvx; const float* Wvz;
+    const void* Wvx; const void* Wvz;     // float, or 16-bit codes for Q = 1 (BF16) / 2 (FP16)
+    const float* wscale;                  // Q > 0: [nts][2] scale of every snapshot (vx, vz)
     long long wstride;
     int nz, nx, nts, its;
     float cz[4], cx[4];
@@ -538,7 +560,29 @@ struct ImagingArgs {
 // coarse sample its.  64x16-cell tiles, 256 threads (one float4 of z x one column
 // each); the snapshot at its is staged with its 4-cell halo in shared memory for
 // the staggered derivatives, the neighbouring snapshots give the time difference.
-template <int ADJ>
+// Four consecutive history values of snapshot `its` at cell index i (float4
+// aligned) of field f (0 vx, 1 vz): FP32, or 16-bit codes times the snapshot scale.
+template <int Q>
+__device__ __forceinline__ float4 ldw(const ImagingArgs& a, int f, int its, long long i)
+{
+    const long long k = (long long)its * a.wstride + i;
+    const void* base = f ? a.Wvz : a.Wvx;
+    if (Q == 0) return ldg4(static_cast<const float*>(base) + k);
+    const uint2 u = __ldg(reinterpret_cast<const uint2*>(static_cast<const unsigned short*>(base) + k));
+    const float s = __ldg(a.wscale + 2 * its + f);
+    const unsigned h[4] = {u.x & 0xffffu, u.x >> 16, u.y & 0xffffu, u.y >> 16};
+    float4 r;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        float v;
+        if (Q == 1) v = __uint_as_float(h[j] << 16);                       // BF16: upper half of a float
+        else v = __half2float(__ushort_as_half((unsigned short)h[j]));     // FP16
+        at(r, j) = v * s;
+    }
+    return r;
+}
+
+template <int ADJ, int Q>
 __global__ void __launch_bounds__(NT) k_imaging(ImagingArgs a)
 {
     __shared__ __align__(16) float sm[2 * SMEM_FIELD];
@@ -547,8 +591,6 @@ __global__ void __launch_bounds__(NT) k_imaging(ImagingArgs a)
     const int bz = blockIdx.x % ntz, bx = blockIdx.x / ntz;
     const int z0 = FAT + bz * TZ, x0 = FAT + bx * TX;
     const long long nz = a.nz;
-    const float* vxc = a.Wvx + (long long)a.its * a.wstride;
-    const float* vzc = a.Wvz + (long long)a.its * a.wstride;
     {
         const int nq = SZ / 4;
         for (int q = tid; q < nq * SX; q += NT) {
@@ -557,8 +599,8 @@ __global__ void __launch_bounds__(NT) k_imaging(ImagingArgs a)
             float4 u = make_float4(0.f, 0.f, 0.f, 0.f), v = u;
             if (gz < a.nz) {
                 const long long gi = (long long)gx * nz + gz;
-                u = ldg4(vxc + gi);
-                v = ldg4(vzc + gi);
+                u = ldw<Q>(a, 0, a.its, gi);
+                v = ldw<Q>(a, 1, a.its, gi);
             }
             st4(sm + lx * SZ + lz4, u);
             st4(sm + SMEM_FIELD + lx * SZ + lz4, v);
@@ -587,10 +629,10 @@ __global__ void __launch_bounds__(NT) k_imaging(ImagingArgs a)
     float4 tx, tz;
     {
         const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 xo = a.its > 0 ? ldg4(a.Wvx + (long long)(a.its - 1) * a.wstride + gi) : zero;
-        const float4 zo = a.its > 0 ? ldg4(a.Wvz + (long long)(a.its - 1) * a.wstride + gi) : zero;
-        const float4 xn = a.its < a.nts - 1 ? ldg4(a.Wvx + (long long)(a.its + 1) * a.wstride + gi) : zero;
-        const float4 zn = a.its < a.nts - 1 ? ldg4(a.Wvz + (long long)(a.its + 1) * a.wstride + gi) : zero;
+        const float4 xo = a.its > 0 ? ldw<Q>(a, 0, a.its - 1, gi) : zero;
+        const float4 zo = a.its > 0 ? ldw<Q>(a, 1, a.its - 1, gi) : zero;
+        const float4 xn = a.its < a.nts - 1 ? ldw<Q>(a, 0, a.its + 1, gi) : zero;
+        const float4 zn = a.its < a.nts - 1 ? ldw<Q>(a, 1, a.its + 1, gi) : zero;
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             // one-sided at the ends like the reference: -W[its+1] at its = 0, W[its-1] at nts-1
@@ -662,6 +704,71 @@ __global__ void __launch_bounds__(128) k_save_wavefield(SaveArgs a)
         }
         st4(r0, u0);
         st4(r1, u1);
+    }
+}
+
+// 16-bit source-wavefield checkpoints: one coarse snapshot (vx, vz) from the
+// FP32 staging rows into codes with a scale per snapshot and field.  Every CTA
+// first reduces the per-(tile, warp) maxima the EPI_TRI step left in pmax
+// (npart entries of 2); the scale is max (BF16) or max / 2^15 (FP16, so the
+// codes use the normal range), 0 for an all-zero snapshot.  The CTAs also
+// clear pmax_next, the slots the next snapshot's step fills.
+struct QuantArgs {
+    const float* stage[2];        // FP32 snapshot of vx, vz, [nx][nz]
+    unsigned short* row[2];       // destination codes, [nx][nz]
+    float* scale;                 // 2 floats: this snapshot's vx, vz scale
+    const float* pmax;
+    float* pmax_next;
+    int npart;
+    int nz, nx;
+};
+
+template <int Q>
+__global__ void __launch_bounds__(256) k_quantize(QuantArgs a)
+{
+    __shared__ float red[2][8];
+    const int tid = threadIdx.x;
+    float m0 = 0.f, m1 = 0.f;
+    for (int i = tid; i < a.npart; i += blockDim.x) {
+        m0 = fmaxf(m0, a.pmax[2 * i]);
+        m1 = fmaxf(m1, a.pmax[2 * i + 1]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        m0 = fmaxf(m0, __shfl_xor_sync(0xffffffffu, m0, o));
+        m1 = fmaxf(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+    }
+    if ((tid & 31) == 0) { red[0][tid >> 5] = m0; red[1][tid >> 5] = m1; }
+    __syncthreads();
+    float amax[2] = {0.f, 0.f};
+#pragma unroll
+    for (int w = 0; w < 8; w++) { amax[0] = fmaxf(amax[0], red[0][w]); amax[1] = fmaxf(amax[1], red[1][w]); }
+    float sc[2], inv[2];
+#pragma unroll
+    for (int f = 0; f < 2; f++) {
+        sc[f] = (Q == 1) ? amax[f] : amax[f] * (1.0f / 32768.0f);
+        inv[f] = sc[f] > 0.f ? 1.0f / sc[f] : 0.f;
+    }
+    if (blockIdx.x == 0 && tid == 0) { a.scale[0] = sc[0]; a.scale[1] = sc[1]; }
+    const long long gtid = (long long)blockIdx.x * blockDim.x + tid;
+    const long long gstride = (long long)gridDim.x * blockDim.x;
+    for (long long i = gtid; i < 2LL * a.npart; i += gstride) a.pmax_next[i] = 0.f;
+    const int nq = (a.nz - 2 * FAT) / 4;
+    const long long total = (long long)nq * (a.nx - 2 * FAT);
+    for (long long q = gtid; q < total; q += gstride) {
+        const long long gi = (long long)(FAT + q / nq) * a.nz + FAT + 4 * (q % nq);
+#pragma unroll
+        for (int f = 0; f < 2; f++) {
+            const float4 v = ld4(a.stage[f] + gi);
+            unsigned h[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const float x = at(v, j) * inv[f];
+                if (Q == 1) h[j] = __bfloat16_as_ushort(__float2bfloat16_rn(x));
+                else h[j] = __half_as_ushort(__float2half_rn(x));
+            }
+            *reinterpret_cast<uint2*>(a.row[f] + gi) = make_uint2(h[0] | (h[1] << 16), h[2] | (h[3] << 16));
+        }
     }
 }
 

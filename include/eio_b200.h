@@ -123,8 +123,12 @@ int eio_ctx_create(const eio_fd_params *p, const float *elasticParam, int device
 /* setBackground: rebuild the medium (QC may fail) (PF/pyElastic_iso_float_nl.cpp:48) */
 int eio_ctx_set_background(eio_ctx *c, const float *elasticParam);
 void eio_ctx_destroy(eio_ctx *c);
-/* Source-wavefield snapshot storage for the Born operators:
- * 0 = FP32 (bit-faithful to the reference), 1 = BF16, 2 = FP16 (both scaled per snapshot). */
+/* Source-wavefield snapshot storage for the Born operators (no reference
+ * counterpart; the reference keeps FP32 snapshots): 0 = FP32 (bit-faithful to
+ * the reference), 1 = BF16, 2 = FP16, both as 16-bit codes with one scale per
+ * snapshot and field (BF16: the snapshot's max |value|, FP16: max / 2^15), half
+ * the history memory.  16-bit modes need sub = 1 (else EIO_ERR_UNSUPPORTED at
+ * the next Born call). */
 int eio_ctx_set_checkpoint_precision(eio_ctx *c, int mode);
 /* Scaled coefficient grids of the context (for inspection / tests). */
 int eio_ctx_get_medium(const eio_ctx *c, float *rhoxDtw, float *rhozDtw, float *lamb2MuDtw,
