@@ -280,7 +280,11 @@ def run_ours(args, ws, rank, local):
             "frac": round(achieved / peak, 4), "traffic": profile_traffic(),
             "peak_source": peak_kind, "kernel": kernel_name(L, ctx),
             "avg_launch_us": round(avg_launch_ms * 1e3, 3),
-            "algorithmic_bytes_per_launch": BYTES_PER_CELL * cells}
+            "algorithmic_bytes_per_launch": BYTES_PER_CELL * cells,
+            # whole job: every cell update of the timed region at 80 B (step kernels, imaging,
+            # sparse work and launch gaps included)
+            "job_gbs": round(BYTES_PER_CELL * value, 1),
+            "job_frac": round(BYTES_PER_CELL * value / peak, 4)}
 
     # ---- e2e through the reference-facing operator API (host buffers)
     e2e = None
@@ -304,10 +308,17 @@ def run_ours(args, ws, rank, local):
         torch.cuda.synchronize()
         t_e2e = max_over_ranks(ws, time.perf_counter() - t0)
         n = w.nz * w.nx
+        # per step: the perturbation grids once (forward) and the gradient grids once
+        # (adjoint); per shot and direction the fine source traces and the receiver
+        # interpolators; the irregular receiver traces out (forward) and in (adjoint)
         src_bytes = sum(4 * s["fine"][f].numel() for s in shots for f in range(5))
-        rec_bytes = sum(4 * s["data"][f].numel() for s in shots for f in range(5))
-        h2d = src_bytes * 2 + 4 * 5 * n * nsh * 2 + rec_bytes
-        d2h = rec_bytes + 4 * 5 * n * nsh
+        irr_bytes = 4 * int(np.prod(data.getNdArray().shape))
+        interp_bytes = 0
+        for k in range(4):
+            g = born.rec[k][0]
+            interp_bytes += 4 * (3 * g.nDeviceIrreg * g.nFiltTotal + g.nDeviceReg + 1)
+        h2d = 4 * 5 * n + src_bytes * 2 + irr_bytes + 2 * nsh * interp_bytes
+        d2h = irr_bytes + 4 * 5 * n
         e2e = {"value": round(ws * updates_per_step * args.steps / t_e2e / 1e9, 3), "unit": "Gcell-updates/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": round(1e3 * t_e2e / args.steps, 1)}

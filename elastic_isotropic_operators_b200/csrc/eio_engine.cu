@@ -88,6 +88,12 @@ struct Engine {
     DBuf stage_a[5], stage_b[5], stage_c[5];
     DBuf W, ss[20];         // secondary-source ring: 4 slots x 5 fields
     DBuf wsave;             // saved wavefield of the *Wavefield operators
+    // receiver interpolators of the current shot on the device (one per grid)
+    struct DevInterp {
+        DBuf slot, w, start, ent;
+        int nIrreg = 0, nReg = 0, nft = 0;
+    } rint[4];
+    DBuf stage_d[5];        // irregular receiver traces [nIrreg][nts] per field
     bool w_clean = false;   // history zeroed and only written by single stores since
     // step-kernel choice: kind 0 = shared-memory tile kernel (k_step),
     // kind 1 = TMA x-sweep (k_sweep) with strip height tz, chunk width cw and
@@ -218,7 +224,11 @@ void engine_destroy(Engine* e) {
     DBuf* all[] = {&e->dampz, &e->dampx, &e->inj_ts, &e->inj_ent, &e->ext_ts, &e->ext_ent, &e->W, &e->err, &e->wsave,
                    &e->Wq, &e->wscale, &e->wstage, &e->wpmax};
     for (DBuf* b : all) b->release();
+    for (int k = 0; k < 4; k++) {
+        e->rint[k].slot.release(); e->rint[k].w.release(); e->rint[k].start.release(); e->rint[k].ent.release();
+    }
     for (int f = 0; f < 5; f++) {
+        e->stage_d[f].release();
         e->par[f].release(); e->sig_in[f].release(); e->sig_out[f].release();
         e->stage_a[f].release(); e->stage_b[f].release(); e->stage_c[f].release();
     }
@@ -1038,6 +1048,136 @@ void engine_born_host(Engine* e, int adj, float* const srcDtw[5], float* const d
         if (!adj) d2h(e, data[f], e->stage_b[f], nr[f]);
         else d2h(e, dm[f], e->stage_c[f], e->n);
     }
+    EIO_CUDA(cudaStreamSynchronize(e->st));
+}
+
+// ---------------------------------------------------------------- multi-shot host paths
+// The multi-shot operators keep the Born perturbation (forward) or the
+// accumulating gradient (adjoint) on the device across shots, and interpolate
+// the receiver traces between the regular grid and the devices on the GPU, so
+// only the irregular traces cross PCIe.
+
+void engine_dm_upload(Engine* e, float* const dm[5]) {
+    EIO_CUDA(cudaSetDevice(e->device));
+    for (int f = 0; f < 5; f++) h2d(e, e->stage_c[f], dm[f], e->n);
+}
+void engine_dm_zero(Engine* e) {
+    EIO_CUDA(cudaSetDevice(e->device));
+    for (int f = 0; f < 5; f++) {
+        e->stage_c[f].ensure(sizeof(float) * e->n);
+        EIO_CUDA(cudaMemsetAsync(e->stage_c[f].p, 0, sizeof(float) * e->n, e->st));
+    }
+}
+void engine_dm_download(Engine* e, float* const dm[5]) {
+    for (int f = 0; f < 5; f++) d2h(e, dm[f], e->stage_c[f], e->n);
+    EIO_CUDA(cudaStreamSynchronize(e->st));
+}
+
+// receiver interpolators of one shot: weights, slots and the inverse (slot ->
+// entries in ascending device, filter order) on the device
+static void upload_interps(Engine* e, const SInterp* const rec[4]) {
+    for (int k = 0; k < 4; k++) {
+        const SInterp& s = *rec[k];
+        Engine::DevInterp& d = e->rint[k];
+        const size_t ne = (size_t)s.nIrreg * s.nft;
+        std::vector<int> start(s.nReg + 1, 0), ent(ne);
+        for (size_t i = 0; i < ne; i++) start[s.slot[i] + 1]++;
+        for (int r = 0; r < s.nReg; r++) start[r + 1] += start[r];
+        std::vector<int> fill(start.begin(), start.end() - 1);
+        for (size_t i = 0; i < ne; i++) ent[fill[s.slot[i]]++] = (int)i;
+        upload(d.slot, s.slot.data(), sizeof(int) * ne, e->st);
+        upload(d.w, s.w.data(), sizeof(float) * ne, e->st);
+        upload(d.start, start.data(), sizeof(int) * start.size(), e->st);
+        upload(d.ent, ent.data(), sizeof(int) * ne, e->st);
+        d.nIrreg = s.nIrreg; d.nReg = s.nReg; d.nft = s.nft;
+        // the host copies above are pageable and are read when the copies run
+        EIO_CUDA(cudaStreamSynchronize(e->st));
+    }
+}
+
+static void interp_fwd(Engine* e, int grid, const float* reg, float* irreg) {
+    const Engine::DevInterp& d = e->rint[grid];
+    const long long n = (long long)d.nIrreg * e->nts;
+    if (n == 0) return;
+    k_interp_fwd<<<(unsigned)((n + 255) / 256), 256, 0, e->st>>>(reg, irreg, static_cast<const int*>(d.slot.p),
+                                                                 d.w.f(), d.nIrreg, d.nft, e->nts);
+    e->launches++;
+}
+static void interp_adj(Engine* e, int grid, const float* irreg, float* reg) {
+    const Engine::DevInterp& d = e->rint[grid];
+    const long long n = (long long)d.nReg * e->nts;
+    if (n == 0) return;
+    k_interp_adj<<<(unsigned)((n + 255) / 256), 256, 0, e->st>>>(irreg, reg, static_cast<const int*>(d.start.p),
+                                                                 static_cast<const int*>(d.ent.p), d.w.f(), d.nReg,
+                                                                 d.nft, e->nts);
+    e->launches++;
+}
+
+// regular-grid receiver buffers (stage_b) and irregular ones (stage_d) of one shot;
+// the adjoint fills stage_b from the irregular host traces
+static void stage_receivers(Engine* e, int adj, const ShotGeom& g, const SInterp* const rec[4], const float* dataIrreg,
+                            float* dr[5]) {
+    upload_interps(e, rec);
+    const int nIrreg = rec[0]->nIrreg;
+    for (int f = 0; f < 5; f++) {
+        const int grid = kFieldGrid[f];
+        const size_t nr = (size_t)g.nRec[grid] * e->nts, ni = (size_t)nIrreg * e->nts;
+        e->stage_b[f].ensure(std::max<size_t>(16, sizeof(float) * nr));
+        e->stage_d[f].ensure(std::max<size_t>(16, sizeof(float) * ni));
+        if (adj) {
+            h2d(e, e->stage_d[f], dataIrreg + (size_t)f * ni, ni);
+            interp_adj(e, grid, e->stage_d[f].f(), e->stage_b[f].f());
+        }
+        dr[f] = e->stage_b[f].f();
+    }
+}
+static void return_receivers(Engine* e, const SInterp* const rec[4], float* dataIrreg) {
+    const size_t ni = (size_t)rec[0]->nIrreg * e->nts;
+    for (int f = 0; f < 5; f++) {
+        interp_fwd(e, kFieldGrid[f], e->stage_b[f].f(), e->stage_d[f].f());
+        d2h(e, dataIrreg + (size_t)f * ni, e->stage_d[f], ni);
+    }
+}
+
+void engine_born_shot(Engine* e, int adj, float* const srcDtw[5], const ShotGeom& g, const SInterp* const rec[4],
+                      float* dataIrreg) {
+    EIO_CUDA(cudaSetDevice(e->device));
+    float* ds[5]; float* dd[5]; float* dr[5];
+    for (int f = 0; f < 5; f++) {
+        h2d(e, e->stage_a[f], srcDtw[f], (size_t)g.nSrc[kFieldGrid[f]] * e->ntw);
+        ds[f] = e->stage_a[f].f();
+        dd[f] = e->stage_c[f].f();
+    }
+    stage_receivers(e, adj, g, rec, dataIrreg, dr);
+    engine_born(e, adj, ds, dd, dr, g);
+    if (!adj) return_receivers(e, rec, dataIrreg);
+    EIO_CUDA(cudaStreamSynchronize(e->st));
+}
+
+void engine_nl_shot(Engine* e, int adj, float* const modelReg[5], const ShotGeom& g, const SInterp* const rec[4],
+                    float* dataIrreg, float* wfld) {
+    EIO_CUDA(cudaSetDevice(e->device));
+    float* dm[5]; float* dr[5];
+    size_t nm[5];
+    for (int f = 0; f < 5; f++) {
+        nm[f] = (size_t)g.nSrc[kFieldGrid[f]] * e->nts;
+        if (!adj) h2d(e, e->stage_a[f], modelReg[f], nm[f]);
+        else e->stage_a[f].ensure(std::max<size_t>(16, sizeof(float) * nm[f]));
+        dm[f] = e->stage_a[f].f();
+    }
+    stage_receivers(e, adj, g, rec, dataIrreg, dr);
+    float* wdev = nullptr;
+    const size_t wcount = (size_t)5 * e->nts * e->n;
+    if (wfld) {
+        e->wsave.ensure(sizeof(float) * wcount);
+        EIO_CUDA(cudaMemsetAsync(e->wsave.p, 0, sizeof(float) * wcount, e->st));
+        wdev = e->wsave.f();
+    }
+    engine_nl(e, adj, dm, dr, g, wdev);
+    if (wfld) d2h(e, wfld, e->wsave, wcount);
+    if (!adj) return_receivers(e, rec, dataIrreg);
+    else
+        for (int f = 0; f < 5; f++) d2h(e, modelReg[f], e->stage_a[f], nm[f]);
     EIO_CUDA(cudaStreamSynchronize(e->st));
 }
 

@@ -35,6 +35,7 @@ void stagger_x(int adj, int add, int nz, int nx, float* model, float* data) {
     const long long n = (long long)nz * nx;
     if (!adj) {
         if (!add) std::fill(data, data + n, 0.f);
+#pragma omp parallel for schedule(static)
         for (int ix = 0; ix < nx - 1; ix++)
             for (int iz = 0; iz < nz; iz++) {
                 const long long i = (long long)ix * nz + iz;
@@ -43,6 +44,7 @@ void stagger_x(int adj, int add, int nz, int nx, float* model, float* data) {
         for (int iz = 0; iz < nz; iz++) data[(long long)(nx - 1) * nz + iz] += model[(long long)(nx - 1) * nz + iz];
     } else {
         if (!add) std::fill(model, model + n, 0.f);
+#pragma omp parallel for schedule(static)
         for (int ix = 1; ix < nx - 1; ix++)
             for (int iz = 0; iz < nz; iz++) {
                 const long long i = (long long)ix * nz + iz;
@@ -60,6 +62,7 @@ void stagger_z(int adj, int add, int nz, int nx, float* model, float* data) {
     const long long n = (long long)nz * nx;
     if (!adj) {
         if (!add) std::fill(data, data + n, 0.f);
+#pragma omp parallel for schedule(static)
         for (int ix = 0; ix < nx; ix++) {
             float* d = data + (long long)ix * nz;
             const float* m = model + (long long)ix * nz;
@@ -68,6 +71,7 @@ void stagger_z(int adj, int add, int nz, int nx, float* model, float* data) {
         }
     } else {
         if (!add) std::fill(model, model + n, 0.f);
+#pragma omp parallel for schedule(static)
         for (int ix = 0; ix < nx; ix++) {
             float* m = model + (long long)ix * nz;
             const float* d = data + (long long)ix * nz;
@@ -660,22 +664,18 @@ void check_nt(const ShotGrids& g, int nts) {
 // wfld (host [nts][5][nx][nz]) receives the saved wavefield when not null
 void nl_shot_forward(eio_ctx* c, const ShotGrids& g, const float* model, float* data, float* wfld = nullptr) {
     const int nts = c->fd.p.nts;
-    const int nsi = g.s[0]->nIrreg, nri = g.r[0]->nIrreg;
-    std::vector<float> reg[5], dreg[5];
-    float* mp[5]; float* dp[5];
+    const int nsi = g.s[0]->nIrreg;
+    std::vector<float> reg[5];
+    float* mp[5];
     for (int f = 0; f < 5; f++) {
         const SInterp& s = *g.s[kFG[f]];
         reg[f].assign((size_t)s.nReg * nts, 0.f);
         sinterp_adjoint(s, false, reg[f].data(), model + (size_t)f * nsi * nts);
     }
     scale_sources(c->fd, g, reg, nts);
-    for (int f = 0; f < 5; f++) {
-        dreg[f].assign((size_t)g.r[kFG[f]]->nReg * nts, 0.f);
-        mp[f] = reg[f].data(); dp[f] = dreg[f].data();
-    }
-    engine_nl_host(c->eng, 0, mp, dp, reg_geom(g), wfld);
-    std::fill(data, data + (size_t)5 * nri * nts, 0.f);
-    for (int f = 0; f < 5; f++) sinterp_forward(*g.r[kFG[f]], true, dreg[f].data(), data + (size_t)f * nri * nts);
+    for (int f = 0; f < 5; f++) mp[f] = reg[f].data();
+    // receivers are interpolated to the devices on the GPU (same sums as sinterp_forward)
+    engine_nl_shot(c->eng, 0, mp, reg_geom(g), g.r, data, wfld);
 }
 
 // The adjoint wavefield is scaled like the adjoint sources
@@ -685,6 +685,7 @@ static void scale_adjoint_wavefield(const FdParam& fd, float* w) {
     const float area = (float)(1.0 / (fd.p.dx * fd.p.dz));
     const size_t n = (size_t)fd.p.nz * fd.p.nx;
     const double tdtw = 2.0 * (double)fd.dtw * (double)area;
+#pragma omp parallel for schedule(static)
     for (int it = 0; it < fd.p.nts; it++) {
         float* slice = w + (size_t)it * 5 * n;
         for (size_t i = 0; i < n; i++) {
@@ -698,17 +699,15 @@ static void scale_adjoint_wavefield(const FdParam& fd, float* w) {
 // nonlinearPropElasticGpu::adjoint with add = true into model; wfld as for nl_shot_forward
 void nl_shot_adjoint(eio_ctx* c, const ShotGrids& g, float* model, const float* data, float* wfld = nullptr) {
     const int nts = c->fd.p.nts;
-    const int nsi = g.s[0]->nIrreg, nri = g.r[0]->nIrreg;
-    std::vector<float> reg[5], dreg[5];
-    float* mp[5]; float* dp[5];
+    const int nsi = g.s[0]->nIrreg;
+    std::vector<float> reg[5];
+    float* mp[5];
     for (int f = 0; f < 5; f++) {
-        const SInterp& r = *g.r[kFG[f]];
-        dreg[f].assign((size_t)r.nReg * nts, 0.f);
-        sinterp_adjoint(r, false, dreg[f].data(), data + (size_t)f * nri * nts);
         reg[f].assign((size_t)g.s[kFG[f]]->nReg * nts, 0.f);
-        mp[f] = reg[f].data(); dp[f] = dreg[f].data();
+        mp[f] = reg[f].data();
     }
-    engine_nl_host(c->eng, 1, mp, dp, reg_geom(g), wfld);
+    // the data are spread onto the regular grid on the GPU (same sums as sinterp_adjoint)
+    engine_nl_shot(c->eng, 1, mp, reg_geom(g), g.r, const_cast<float*>(data), wfld);
     if (wfld) scale_adjoint_wavefield(c->fd, wfld);
     scale_sources_adj(c->fd, g, reg, nts);
     for (int f = 0; f < 5; f++) sinterp_forward(*g.s[kFG[f]], true, reg[f].data(), model + (size_t)f * nsi * nts);
@@ -746,7 +745,8 @@ void born_model_slice(const FdParam& fd, const float* model, std::vector<float>*
     stagger_x(1, 0, nz, nx, tmp1.data(), tmp.data());
     stagger_z(1, 0, nz, nx, sl[4].data(), tmp1.data());
     const double tdtw = 2.0 * fd.dtw;
-    for (size_t i = 0; i < n; i++) {
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < (long long)n; i++) {
         sl[0][i] *= fd.par[0][i];
         sl[1][i] *= fd.par[1][i];
         sl[2][i] = (float)(sl[2][i] * tdtw);
@@ -825,7 +825,8 @@ static int nl_forward_impl(eio_ctx* c, int add, int nExp, int nModelExp, const f
             nl_shot_forward(c, g, model + (nModelExp == 1 ? 0 : (size_t)e * mslice), tmp.data(),
                             e == wShot ? wfld : nullptr);
             float* d = data + (size_t)e * dslice;
-            for (size_t i = 0; i < dslice; i++) d[i] += tmp[i];
+            #pragma omp parallel for schedule(static)
+            for (long long i = 0; i < (long long)dslice; i++) d[i] += tmp[i];
         }
     });
 }
@@ -908,23 +909,20 @@ EIO_API int eio_born_forward(eio_ctx* c, int add, int nExp, const float* model, 
         born_model_slice(c->fd, model, sl);
         float* dm[5];
         for (int f = 0; f < 5; f++) dm[f] = sl[f].data();
+        engine_dm_upload(c->eng, dm);        // stays on the device for every shot
+        std::vector<float> tmp(dslice);
         for (int e = 0; e < nExp; e++) {
             ShotGrids g = shot_grids(src, rec, nRecGeom, e);
             check_nt(g, nts);
             if ((size_t)5 * g.r[0]->nIrreg * nts != dslice) throw Error(EIO_ERR_ARG, "receiver counts differ");
-            std::vector<float> fine[5], dreg[5];
+            std::vector<float> fine[5];
             born_sources(c, g, sigs[nSignals == 1 ? 0 : e], fine);
-            float* sp[5]; float* dp[5];
-            for (int f = 0; f < 5; f++) {
-                dreg[f].assign((size_t)g.r[kFG[f]]->nReg * nts, 0.f);
-                sp[f] = fine[f].data(); dp[f] = dreg[f].data();
-            }
-            engine_born_host(c->eng, 0, sp, dm, dp, reg_geom(g));
+            float* sp[5];
+            for (int f = 0; f < 5; f++) sp[f] = fine[f].data();
+            engine_born_shot(c->eng, 0, sp, reg_geom(g), g.r, tmp.data());
             float* d = data + (size_t)e * dslice;
-            const int nri = g.r[0]->nIrreg;
-            std::vector<float> tmp(dslice, 0.f);
-            for (int f = 0; f < 5; f++) sinterp_forward(*g.r[kFG[f]], true, dreg[f].data(), tmp.data() + (size_t)f * nri * nts);
-            for (size_t i = 0; i < dslice; i++) d[i] += tmp[i];
+#pragma omp parallel for schedule(static)
+            for (long long i = 0; i < (long long)dslice; i++) d[i] += tmp[i];
         }
     });
 }
@@ -945,25 +943,22 @@ EIO_API int eio_born_adjoint(eio_ctx* c, int add, int nExp, float* model, const 
         std::vector<float> sl[5];
         float* dm[5];
         for (int f = 0; f < 5; f++) { sl[f].assign(n, 0.f); dm[f] = sl[f].data(); }
+        engine_dm_zero(c->eng);              // every shot's image accumulates on the device
         for (int e = 0; e < nExp; e++) {
             ShotGrids g = shot_grids(src, rec, nRecGeom, e);
             check_nt(g, nts);
             if ((size_t)5 * g.r[0]->nIrreg * nts != dslice) throw Error(EIO_ERR_ARG, "receiver counts differ");
-            std::vector<float> fine[5], dreg[5];
+            std::vector<float> fine[5];
             born_sources(c, g, sigs[nSignals == 1 ? 0 : e], fine);
-            float* sp[5]; float* dp[5];
-            const int nri = g.r[0]->nIrreg;
-            for (int f = 0; f < 5; f++) {
-                const SInterp& r = *g.r[kFG[f]];
-                dreg[f].assign((size_t)r.nReg * nts, 0.f);
-                sinterp_adjoint(r, false, dreg[f].data(), data + (size_t)e * dslice + (size_t)f * nri * nts);
-                sp[f] = fine[f].data(); dp[f] = dreg[f].data();
-            }
-            engine_born_host(c->eng, 1, sp, dm, dp, reg_geom(g));
+            float* sp[5];
+            for (int f = 0; f < 5; f++) sp[f] = fine[f].data();
+            engine_born_shot(c->eng, 1, sp, reg_geom(g), g.r, const_cast<float*>(data) + (size_t)e * dslice);
         }
+        engine_dm_download(c->eng, dm);
         // scaling and un-staggering, BornElasticShotsGpu.cpp:325-371
         const double tdtw = 2.0 * fd.dtw;
-        for (size_t i = 0; i < n; i++) {
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < (long long)n; i++) {
             sl[0][i] *= fd.par[0][i];
             sl[1][i] *= fd.par[1][i];
             sl[2][i] = (float)(sl[2][i] * tdtw);
@@ -978,7 +973,8 @@ EIO_API int eio_born_adjoint(eio_ctx* c, int add, int nExp, float* model, const 
         stagger_z(0, 0, nz, nx, sl[4].data(), t2.data());
         std::vector<float> t3(n);
         stagger_x(0, 0, nz, nx, t2.data(), t3.data());
-        for (size_t i = 0; i < n; i++) {
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < (long long)n; i++) {
             model[n + i] += sl[2][i];
             model[2 * n + i] += sl[3][i] + t3[i];
         }

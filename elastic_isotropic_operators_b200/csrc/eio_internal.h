@@ -86,6 +86,18 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
 // wfld: host [nts][5][nx][nz], overwritten with the saved wavefield when not null
 void engine_nl_host(Engine* e, int adj, float* const model[5], float* const data[5], const ShotGeom& g,
                     float* wfld = nullptr);
+// Multi-shot paths: the Born perturbation / gradient grids stay on the device
+// across shots (stage with engine_dm_upload or engine_dm_zero, read back with
+// engine_dm_download); receiver traces go in and out as irregular traces
+// [5][nIrreg][nts] on the host, interpolated on the device with rec[grid].
+void engine_dm_upload(Engine* e, float* const dm[5]);
+void engine_dm_zero(Engine* e);
+void engine_dm_download(Engine* e, float* const dm[5]);
+void engine_born_shot(Engine* e, int adj, float* const srcDtw[5], const ShotGeom& g, const SInterp* const rec[4],
+                      float* dataIrreg);
+// modelReg: regular source traces, read (forward) or written (adjoint)
+void engine_nl_shot(Engine* e, int adj, float* const modelReg[5], const ShotGeom& g, const SInterp* const rec[4],
+                    float* dataIrreg, float* wfld = nullptr);
 void engine_born_host(Engine* e, int adj, float* const srcDtw[5], float* const dm[5], float* const data[5],
                       const ShotGeom& g);
 }  // namespace eio

@@ -772,6 +772,40 @@ __global__ void __launch_bounds__(256) k_quantize(QuantArgs a)
     }
 }
 
+// Spatial interpolation of receiver traces on the device (spaceInterpGpu
+// forward / adjoint, F/src/spaceInterpGpu.cpp:288-361), trace-major [n][nt].
+// Forward gathers irreg[d][t] = sum_k w[d,k] * reg[slot[d,k]][t]; the adjoint
+// gathers reg[s][t] = sum of w * irreg[d][t] over the (d, k) that use slot s
+// (inverse CSR in ascending (d, k)), the order the host loops accumulate in,
+// with unfused multiply and add so the sums equal the host's bit for bit.
+__global__ void __launch_bounds__(256) k_interp_fwd(const float* reg, float* irreg, const int* slot, const float* w,
+                                                    int nIrreg, int nft, int nt)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)nIrreg * nt) return;
+    const int d = (int)(i / nt), t = (int)(i % nt);
+    float acc = 0.f;
+    for (int k = 0; k < nft; k++) {
+        const int e = d * nft + k;
+        acc = __fadd_rn(acc, __fmul_rn(__ldg(w + e), __ldg(reg + (long long)__ldg(slot + e) * nt + t)));
+    }
+    irreg[i] = acc;
+}
+
+__global__ void __launch_bounds__(256) k_interp_adj(const float* irreg, float* reg, const int* start, const int* ent,
+                                                    const float* w, int nReg, int nft, int nt)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)nReg * nt) return;
+    const int s = (int)(i / nt), t = (int)(i % nt);
+    float acc = 0.f;
+    for (int j = __ldg(start + s); j < __ldg(start + s + 1); j++) {
+        const int e = __ldg(ent + j);
+        acc = __fadd_rn(acc, __fmul_rn(__ldg(w + e), __ldg(irreg + (long long)(e / nft) * nt + t)));
+    }
+    reg[i] = acc;
+}
+
 // time-major <-> trace-major transposes for the sparse signal matrices
 __global__ void k_transpose(const float* __restrict__ in, float* __restrict__ out, int rows, int cols)
 {
