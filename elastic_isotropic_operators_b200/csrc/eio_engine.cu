@@ -478,14 +478,31 @@ static void launch_tile(Engine* e, const StepArgs& a, int cur) {
     k_tile<DIR, EPI><<<grid, NT, TileLayout<DIR>::BYTES, e->st>>>(t);
 }
 
+// step kernels go out with programmatic stream serialization (see pdl_begin)
+template <typename K>
+static void launch_pdl(K kern, int grid, int block, cudaStream_t st, const StepArgs& a) {
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    EIO_CUDA(cudaLaunchKernelEx(&cfg, kern, a));
+}
+
 template <int DIR, int EPI>
 static void launch_step(Engine* e, StepArgs& a, int cur) {
     const bool timed = e->stats && e->step_launches % STATS_PERIOD == 0;
     if (timed) stats_mark(e);
-    if (e->kind == 0) k_step<DIR, EPI><<<e->ntiles, NT, 0, e->st>>>(a);
+    if (e->kind == 0) launch_pdl(k_step<DIR, EPI, 3>, e->ntiles, NT, e->st, a);
     else if (e->kind == 2) launch_tile<DIR, EPI>(e, a, cur);
-    else if (e->kind == 3) k_step<DIR, EPI, 4><<<e->ntiles, NT, 0, e->st>>>(a);
-    else if (e->kind == 4) k_split<DIR, EPI><<<e->ntiles, NT2, 0, e->st>>>(a);
+    else if (e->kind == 3) launch_pdl(k_step<DIR, EPI, 4>, e->ntiles, NT, e->st, a);
+    else if (e->kind == 4) launch_pdl(k_split<DIR, EPI>, e->ntiles, NT2, e->st, a);
     else launch_sweep<DIR, EPI>(e, a, cur);
     if (timed) {
         stats_mark(e);

@@ -428,6 +428,22 @@ __device__ __forceinline__ void step_tail(const StepArgs& a, float* scratch, int
     }
 }
 
+// Programmatic dependent launch: a step kernel launched with the
+// programmatic-serialization attribute may start while the previous kernel of
+// the stream drains.  Before griddepcontrol.wait it touches only data no kernel
+// writes (the medium, prefetched to L2); every read of the wavefields comes
+// after the wait, which returns once the previous grid has completed and its
+// writes are visible.  Launched without the attribute, the wait returns at once.
+__device__ __forceinline__ void pdl_begin(const StepArgs& a, long long gi, bool valid)
+{
+    if (valid) {
+#pragma unroll
+        for (int k = 0; k < 5; k++) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.par[k] + gi));
+    }
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Stage the current level (forward) or its scaled combinations (adjoint) of
 // tile (z0, x0) with its 4-cell halo into sm [5][SX][SZ]; NTHR threads.
 template <int DIR, int NTHR>
@@ -472,10 +488,6 @@ __global__ void __launch_bounds__(NT, MINB) k_step(StepArgs a)
     const int bz = tile % a.ntz, bx = tile / a.ntz;
     const int z0 = FAT + bz * TZ, x0 = FAT + bx * TX;
     const int nz = a.nz;
-
-    stage_tile<DIR, NT>(a, sm, z0, x0, tid);
-    __syncthreads();
-
     const int tzi = tid % NTZ, txi = tid / NTZ;
     const int lz = FAT + 4 * tzi;              // local z of my float4
     const int lx = FAT + txi;                  // my local column
@@ -483,6 +495,11 @@ __global__ void __launch_bounds__(NT, MINB) k_step(StepArgs a)
     const int gx = x0 + txi;
     const bool valid = gz < nz - FAT;
     const long long gi = (long long)gx * nz + gz;
+
+    pdl_begin(a, gi, valid);
+    stage_tile<DIR, NT>(a, sm, z0, x0, tid);
+    __syncthreads();
+
     float4 t[5];                               // new values before the final taper
 
     stencil_core<DIR>(sm, lx, lz, a.cz, a.cx, valid, [&](int k) { return ldg4(a.par[k] + gi); }, t);
@@ -511,10 +528,6 @@ __global__ void __launch_bounds__(NT2, 2) k_split(StepArgs a)
     const int bz = tile % a.ntz, bx = tile / a.ntz;
     const int z0 = FAT + bz * TZ, x0 = FAT + bx * TX;
     const int nz = a.nz;
-
-    stage_tile<DIR, NT2>(a, sm, z0, x0, tid);
-    __syncthreads();
-
     const int lt = tid & (NT - 1);
     const int tzi = lt % NTZ, txi = lt / NTZ;
     const int lz = FAT + 4 * tzi;
@@ -523,6 +536,10 @@ __global__ void __launch_bounds__(NT2, 2) k_split(StepArgs a)
     const int gx = x0 + txi;
     const bool valid = gz < nz - FAT;
     const long long gi = (long long)gx * nz + gz;
+
+    pdl_begin(a, gi, valid && tid < NT);
+    stage_tile<DIR, NT2>(a, sm, z0, x0, tid);
+    __syncthreads();
     float4 t[5];
     float4 csave[2];
     auto par = [&](int k) { return ldg4(a.par[k] + gi); };
