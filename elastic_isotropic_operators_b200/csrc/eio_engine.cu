@@ -83,6 +83,11 @@ struct Engine {
     int ckpt = 0;           // source-wavefield snapshots: 0 FP32, 1 BF16, 2 FP16 (scaled per snapshot)
     DBuf Wq, wscale, wstage, wpmax;   // 16-bit history, scales [nts][2], FP32 staging row pair, warp maxima
     DBuf par[5], dampz, dampx, wf[10];
+    // free surface (nonlinear operators only, like the reference): taper
+    // without the top edge, sigmaxx coefficient of the surface row per column
+    int fs = 0;
+    bool fs_active = false;   // set while a free-surface propagation runs (k_step only)
+    DBuf dampz_fs, fsc;
     DBuf inj_ts, inj_ent, ext_ts, ext_ent;
     DBuf sig_in[5], sig_out[5];
     DBuf stage_a[5], stage_b[5], stage_c[5];
@@ -171,6 +176,17 @@ void engine_set_medium(Engine* e, const FdParam& fd) {
         if (fd.damp[i] < fd.damp[i - 1]) throw Error(EIO_ERR_ARG, "cosine taper table is not monotone");
     upload(e->dampz, dz.data(), sizeof(float) * nz, e->st);
     upload(e->dampx, dx.data(), sizeof(float) * nx, e->st);
+    e->fs = fd.p.surfaceCondition;
+    if (e->fs) {
+        std::vector<float> dzf(nz, 1.f);   // dampCosineEdge_freesurface, K:1223-1252: no top edge
+        for (int iz = FAT; iz < nz - FAT; iz++) {
+            const int d = nz - iz - 1 - FAT;
+            if (d < fd.minPad) dzf[iz] = fd.damp[d];
+        }
+        upload(e->dampz_fs, dzf.data(), sizeof(float) * nz, e->st);
+        upload(e->fsc, fd.fsc.data(), sizeof(float) * nx, e->st);
+        EIO_CUDA(cudaStreamSynchronize(e->st));   // the host tables are locals
+    }
     e->nts = fd.p.nts;
     e->S = fd.S;
     e->ntw = fd.ntw;
@@ -222,7 +238,7 @@ void engine_destroy(Engine* e) {
     if (e->st) cudaStreamSynchronize(e->st);
     if (e->st2) cudaStreamSynchronize(e->st2);
     DBuf* all[] = {&e->dampz, &e->dampx, &e->inj_ts, &e->inj_ent, &e->ext_ts, &e->ext_ent, &e->W, &e->err, &e->wsave,
-                   &e->Wq, &e->wscale, &e->wstage, &e->wpmax};
+                   &e->Wq, &e->wscale, &e->wstage, &e->wpmax, &e->dampz_fs, &e->fsc};
     for (DBuf* b : all) b->release();
     for (int k = 0; k < 4; k++) {
         e->rint[k].slot.release(); e->rint[k].w.release(); e->rint[k].start.release(); e->rint[k].ent.release();
@@ -263,13 +279,15 @@ void engine_stats(Engine* e, int enable, int reset, long long* launches, long lo
 
 // every kind but the sweep (1) uses the 64x16 tiles of k_step and their numbering
 static bool tiled(int kind) { return kind != 1; }
+// the free surface is built into k_step only
+static int eff_kind(const Engine* e) { return e->fs_active ? 0 : e->kind; }
 
 // tile geometry the sparse point lists are bucketed with
 struct TileGeom {
     int tz, tx, ntz;
 };
 static TileGeom tile_geom(const Engine* e) {
-    if (tiled(e->kind)) return {TZ, TX, e->ntz};
+    if (tiled(eff_kind(e))) return {TZ, TX, e->ntz};
     return {e->tz, e->cw, (e->nz - 2 * FAT + e->tz - 1) / e->tz};
 }
 
@@ -293,7 +311,7 @@ static void build_points(const Engine* e, const int* const pos[4], const int npo
             pe.key = (f << 16) | (((ix - FAT) % tg.tx) << 8) | ((iz - FAT) % tg.tz);
             pe.col = k;
             // k_step / k_tile number tiles z-fastest, k_sweep strip-major
-            tmp.push_back({tiled(e->kind) ? bx * tg.ntz + bz : bz * nchunks + bx, pe});
+            tmp.push_back({tiled(eff_kind(e)) ? bx * tg.ntz + bz : bz * nchunks + bx, pe});
         }
     }
     pl.any = !tmp.empty();
@@ -331,8 +349,10 @@ static StepArgs base_args(Engine* e) {
     StepArgs a;
     memset(&a, 0, sizeof(a));
     for (int f = 0; f < 5; f++) a.par[f] = e->par[f].f();
-    a.dampz = e->dampz.f();
+    a.dampz = e->fs_active ? e->dampz_fs.f() : e->dampz.f();
     a.dampx = e->dampx.f();
+    a.fs = e->fs_active ? 1 : 0;
+    a.fsc = e->fsc.f();
     a.nz = e->nz;
     a.nx = e->nx;
     a.ntz = e->ntz;
@@ -499,10 +519,19 @@ template <int DIR, int EPI>
 static void launch_step(Engine* e, StepArgs& a, int cur) {
     const bool timed = e->stats && e->step_launches % STATS_PERIOD == 0;
     if (timed) stats_mark(e);
-    if (e->kind == 0) launch_pdl(k_step<DIR, EPI, 3>, e->ntiles, NT, e->st, a);
-    else if (e->kind == 2) launch_tile<DIR, EPI>(e, a, cur);
-    else if (e->kind == 3) launch_pdl(k_step<DIR, EPI, 4>, e->ntiles, NT, e->st, a);
-    else if (e->kind == 4) launch_pdl(k_split<DIR, EPI>, e->ntiles, NT2, e->st, a);
+    const int kind = eff_kind(e);
+    bool done = false;
+    if constexpr (EPI == EPI_NONE) {   // the nonlinear operators are the only ones with a free surface
+        if (e->fs_active) {
+            launch_pdl(k_step<DIR, EPI, 3, true>, e->ntiles, NT, e->st, a);
+            done = true;
+        }
+    }
+    if (done) {
+    } else if (kind == 0) launch_pdl(k_step<DIR, EPI, 3>, e->ntiles, NT, e->st, a);
+    else if (kind == 2) launch_tile<DIR, EPI>(e, a, cur);
+    else if (kind == 3) launch_pdl(k_step<DIR, EPI, 4>, e->ntiles, NT, e->st, a);
+    else if (kind == 4) launch_pdl(k_split<DIR, EPI>, e->ntiles, NT2, e->st, a);
     else launch_sweep<DIR, EPI>(e, a, cur);
     if (timed) {
         stats_mark(e);
@@ -651,9 +680,22 @@ static void save_wavefield(Engine* e, float* W, float* const p[5], int its, floa
     e->launches++;
 }
 
+static void fs_top(Engine* e, float* const c[5]) {
+    k_fs_top<<<(e->nx - 2 * FAT + 127) / 128, 128, 0, e->st>>>(c[0], c[1], c[3], c[4], e->nz, e->nx);
+    e->launches++;
+}
+
+// free-surface propagations run with the effective kind 0 while the guard lives
+struct FsScope {
+    Engine* e;
+    explicit FsScope(Engine* en) : e(en) { e->fs_active = e->fs != 0; }
+    ~FsScope() { e->fs_active = false; }
+};
+
 void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], const ShotGeom& g, float* wfld) {
     EIO_CUDA(cudaSetDevice(e->device));
     if (!e->tuned) engine_autotune(e);
+    FsScope fs_scope(e);
     err_reset(e);
     PointList src, rec;
     build_points(e, g.srcPos, g.nSrc, src);
@@ -675,6 +717,7 @@ void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], 
                 for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; }
                 a.inj.t0 = its; a.inj.w0 = F[it2 - 1]; a.inj.w1 = F[h + it2 - 1];
                 a.ext.t0 = its; a.ext.w0 = F[it2]; a.ext.w1 = F[h + it2];
+                if (e->fs_active) fs_top(e, p1);
                 launch_step<0, EPI_NONE>(e, a, cur);
                 if (wfld) save_wavefield(e, wfld, p0, its, F[it2], F[h + it2]);
                 std::swap(p0, p1);

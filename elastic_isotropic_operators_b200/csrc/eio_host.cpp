@@ -92,8 +92,8 @@ void build_fdparam(const eio_fd_params& pin, const float* ep, FdParam& o) {
     eio_fd_params p = pin;
     if (p.nts < 2) throw Error(EIO_ERR_ARG, "nts must be >= 2");
     if (p.nz <= 0 || p.nx <= 0) throw Error(EIO_ERR_ARG, "nz and nx must be positive");
-    if (p.surfaceCondition != 0)
-        throw Error(EIO_ERR_UNSUPPORTED, "surfaceCondition=1 (free surface) is not available in this build");
+    if (p.surfaceCondition != 0 && p.surfaceCondition != 1)
+        throw Error(EIO_ERR_ARG, "surfaceCondition must be 0 or 1");
     o.S = 2 * p.sub;
     if (o.S > SUB_MAX || o.S >= SUB_MAX)
         throw Error(EIO_ERR_QC, "**** ERROR: 2*_sub is greater than the allowed SUB_MAX value. " +
@@ -102,7 +102,8 @@ void build_fdparam(const eio_fd_params& pin, const float* ep, FdParam& o) {
     o.ntw = (p.nts - 1) * o.S + 1;
     o.dtw = p.dts / float(o.S);
     if (p.mod_par == 2) { p.dz *= 1000.f; p.dx *= 1000.f; p.oz *= 1000.f; p.ox *= 1000.f; }
-    const int zPad = std::min(p.zPadMinus, p.zPadPlus);
+    // fdParamElastic.cpp:43-44: with the free surface the top pad is no taper
+    const int zPad = p.surfaceCondition ? p.zPadPlus : std::min(p.zPadMinus, p.zPadPlus);
     const int xPad = std::min(p.xPadMinus, p.xPadPlus);
     o.minPad = std::min(zPad, xPad);
     if (o.minPad >= PAD_MAX) throw Error(EIO_ERR_QC, "**** ERROR: Padding value is too high ****");
@@ -159,6 +160,14 @@ void build_fdparam(const eio_fd_params& pin, const float* ep, FdParam& o) {
         o.par[3][i] = (float)(2.0 * dtw * lam);
         o.par[4][i] = (float)(2.0 * dtw * o.par[4][i]);
     }
+    // free surface: sigmaxx on the surface row z = 2*fat is driven by
+    // lamb2MuDtw - lambDtw^2 / lamb2MuDtw (K:716-717, same float operations)
+    o.fsc.assign(nx, 0.f);
+    if (p.surfaceCondition)
+        for (int ix = 0; ix < nx; ix++) {
+            const long long i = (long long)ix * nz + 2 * fat;
+            o.fsc[ix] = o.par[2][i] - (o.par[3][i] * o.par[3][i] / o.par[2][i]);
+        }
     // FD coefficients, time filter and taper, nonlinearPropElasticGpuFunctions.cu:155-202
     static const double C[4] = {1.196289062541883, -0.079752604188901, 0.009570312506634, -6.975446437140719e-04};
     for (int k = 0; k < 4; k++) { o.zc[k] = (float)(C[k] / p.dz); o.xc[k] = (float)(C[k] / p.dx); }

@@ -34,6 +34,7 @@ struct FdParam {
     float dts_inv = 0.f;       // Born: 1/(2 dts)
     float minVpVs = 0.f, maxVpVs = 0.f;
     std::vector<float> par[5]; // rhoxDtw, rhozDtw, lamb2MuDtw, lambDtw, muxzDtw
+    std::vector<float> fsc;    // [nx] free surface: sigmaxx coefficient on the surface row
 };
 
 // Builds the FD parameters, checks the QC of fdParamElastic and prepares the

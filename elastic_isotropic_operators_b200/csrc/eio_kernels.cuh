@@ -87,7 +87,13 @@ struct StepArgs {
     // 16-bit checkpoints: forward EPI_TRI also leaves, per tile and warp, the
     // largest |sample| of vx and vz in pmax[(tile * 16 + warp) * 2 + {0, 1}]
     float* pmax;
+    // free surface at z = 2*FAT (surfaceCondition = 1, k_step only): fsc[ix] is
+    // the sigmaxx coefficient on the surface row
+    int fs;
+    const float* fsc;
 };
+
+constexpr int SURF = 2 * FAT;   // free-surface row
 
 enum { EPI_NONE = 0, EPI_SAVE_W = 1, EPI_INJ_SS = 2, EPI_EXT_SS = 3, EPI_TRI = 4 };
 
@@ -282,7 +288,7 @@ __device__ __forceinline__ void adj_products(float4 vx, float4 vz, float4 sxx, f
 // epilogues, sparse extraction.  NTHR threads of the CTA take part (every one
 // reaches the same barriers); scratch: >= 5*TX*TZ floats of shared memory that
 // the stencils no longer need.
-template <int DIR, int EPI, int F0, int F1, int NTHR, class Old>
+template <int DIR, int EPI, int F0, int F1, int NTHR, class Old, bool FS = false>
 __device__ __forceinline__ void step_tail(const StepArgs& a, float* scratch, int tile, int tid, int tzi, int txi,
                                           int gz, int gx, bool valid, long long gi, float4 (&t)[5], Old oload,
                                           const float4 (&csave)[2])
@@ -313,6 +319,42 @@ __device__ __forceinline__ void step_tail(const StepArgs& a, float* scratch, int
                 const float4 r = right ? ldg4(a.ssR[f] + gi) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
                 for (int j = 0; j < 4; j++) at(t[f], j) += at(l, j) * a.sw0 + at(r, j) * a.sw1;
+            }
+        }
+    }
+
+    // ---- free surface, adjoint: transpose of the top pass on the column
+    // (the mirrored stress rows return to their sources below the surface,
+    // the rows the top pass overwrites get nothing)
+    if (FS && DIR == 1 && a.fs && tile % a.ntz == 0) {   // CTA-uniform
+        __shared__ float fsv[2][5][TX];            // sigmazz, sigmaxz on rows SURF-4 .. SURF
+        if (valid && F0 <= 3 && F1 >= 5) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int row = gz + j;
+                if (row >= SURF - 4 && row <= SURF) {
+                    fsv[0][row - (SURF - 4)][txi] = at(t[3], j);
+                    fsv[1][row - (SURF - 4)][txi] = at(t[4], j);
+                }
+            }
+        }
+        __syncthreads();
+        if (valid) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int row = gz + j;
+                if (F0 <= 3 && F1 >= 5) {
+                    if (row > SURF && row <= SURF + 4) {
+                        at(t[3], j) -= fsv[0][(2 * SURF - row) - (SURF - 4)][txi];     // szz[S+k] -= szz[S-k]
+                        at(t[4], j) -= fsv[1][(2 * SURF + 1 - row) - (SURF - 4)][txi]; // sxz[S+1+k] -= sxz[S-k]
+                    }
+                    if (row >= SURF - 4 && row <= SURF) at(t[3], j) = 0.f;
+                    if (row >= SURF - 3 && row <= SURF) at(t[4], j) = 0.f;
+                }
+                if (F0 == 0) {
+                    if (row >= SURF - 4 && row < SURF) at(t[0], j) = 0.f;
+                    if (row >= SURF - 4 && row <= SURF) at(t[1], j) = 0.f;
+                }
             }
         }
     }
@@ -428,6 +470,51 @@ __device__ __forceinline__ void step_tail(const StepArgs& a, float* scratch, int
     }
 }
 
+// Free surface, top pass on the current level before each forward step
+// (ker_step_fwd_surface_top, K:543-587): sigmazz = 0 on the surface, sigmazz
+// and sigmaxz mirrored with opposite sign above it, vx and vz zero above it
+// (vz also on it).  One thread per interior column.
+__global__ void __launch_bounds__(128) k_fs_top(float* vx, float* vz, float* szz, float* sxz, int nz, int nx)
+{
+    const int ix = FAT + blockIdx.x * blockDim.x + threadIdx.x;
+    if (ix >= nx - FAT) return;
+    const long long b = (long long)ix * nz + SURF;
+    szz[b] = 0.f;
+#pragma unroll
+    for (int k = 1; k <= 4; k++) szz[b - k] = -szz[b + k];
+#pragma unroll
+    for (int k = 0; k < 4; k++) sxz[b - k] = -sxz[b + 1 + k];
+#pragma unroll
+    for (int k = 1; k <= 4; k++) vx[b - k] = 0.f;
+#pragma unroll
+    for (int k = 0; k <= 4; k++) vz[b - k] = 0.f;
+}
+
+// Free surface, forward update of the rows gz..gz+3 of a thread in the top
+// tile row (ker_step_fwd_surface_body, K:589-776): nothing above the surface;
+// on it only vx and sigmaxx, the latter with the reduced coefficient fsc.
+__device__ __forceinline__ void fs_forward_rows(const StepArgs& a, const float* sm, int lx, int lz, int gz, int gx,
+                                                float4 (&t)[5])
+{
+    if (gz > SURF) return;
+    float4 q[9];
+#pragma unroll
+    for (int m = 0; m < 9; m++) q[m] = ld4(sm + (lx - FAT + m) * SZ + lz);   // staged vx
+    const float4 dvx = dpx(q, 4, a.cx);
+    const float fc = __ldg(a.fsc + gx);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int row = gz + j;
+        if (row < SURF) {
+#pragma unroll
+            for (int f = 0; f < 5; f++) at(t[f], j) = 0.f;
+        } else if (row == SURF) {
+            at(t[1], j) = 0.f; at(t[3], j) = 0.f; at(t[4], j) = 0.f;
+            at(t[2], j) = fc * at(dvx, j);
+        }
+    }
+}
+
 // Programmatic dependent launch: a step kernel launched with the
 // programmatic-serialization attribute may start while the previous kernel of
 // the stream drains.  Before griddepcontrol.wait it touches only data no kernel
@@ -446,7 +533,7 @@ __device__ __forceinline__ void pdl_begin(const StepArgs& a, long long gi, bool 
 
 // Stage the current level (forward) or its scaled combinations (adjoint) of
 // tile (z0, x0) with its 4-cell halo into sm [5][SX][SZ]; NTHR threads.
-template <int DIR, int NTHR>
+template <int DIR, int NTHR, bool FS = false>
 __device__ __forceinline__ void stage_tile(const StepArgs& a, float* sm, int z0, int x0, int tid)
 {
     const int nz = a.nz;
@@ -461,9 +548,25 @@ __device__ __forceinline__ void stage_tile(const StepArgs& a, float* sm, int z0,
 #pragma unroll
                 for (int f = 0; f < 5; f++) v[f] = ldg4(a.c[f] + gi);
             } else {
-                adj_products(ldg4(a.c[0] + gi), ldg4(a.c[1] + gi), ldg4(a.c[2] + gi), ldg4(a.c[3] + gi),
+                const float4 sxx = ldg4(a.c[2] + gi);
+                adj_products(ldg4(a.c[0] + gi), ldg4(a.c[1] + gi), sxx, ldg4(a.c[3] + gi),
                              ldg4(a.c[4] + gi), ldg4(a.par[0] + gi), ldg4(a.par[1] + gi), ldg4(a.par[2] + gi),
                              ldg4(a.par[3] + gi), ldg4(a.par[4] + gi), v);
+                if (FS && a.fs && gz <= SURF) {
+                    // free surface: only what the forward update uses (see fs_forward_rows)
+                    const float fc = __ldg(a.fsc + gx);
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        const int row = gz + j;
+                        if (row < SURF) {
+#pragma unroll
+                            for (int f = 0; f < 5; f++) at(v[f], j) = 0.f;
+                        } else if (row == SURF) {
+                            at(v[0], j) = fc * at(sxx, j);
+                            at(v[1], j) = 0.f; at(v[2], j) = 0.f; at(v[4], j) = 0.f;
+                        }
+                    }
+                }
             }
         } else {
 #pragma unroll
@@ -478,7 +581,7 @@ __device__ __forceinline__ void stage_tile(const StepArgs& a, float* sm, int z0,
 // The current level (forward) or its scaled combinations (adjoint) are staged
 // with plain loads; the old level and the medium are read from global memory.
 // MINB CTAs per SM (3: <= 80 registers, 4: <= 64).
-template <int DIR, int EPI, int MINB = 3>
+template <int DIR, int EPI, int MINB = 3, bool FS = false>
 __global__ void __launch_bounds__(NT, MINB) k_step(StepArgs a)
 {
     __shared__ __align__(16) float sm[5 * SMEM_FIELD];
@@ -497,20 +600,21 @@ __global__ void __launch_bounds__(NT, MINB) k_step(StepArgs a)
     const long long gi = (long long)gx * nz + gz;
 
     pdl_begin(a, gi, valid);
-    stage_tile<DIR, NT>(a, sm, z0, x0, tid);
+    stage_tile<DIR, NT, FS>(a, sm, z0, x0, tid);
     __syncthreads();
 
     float4 t[5];                               // new values before the final taper
 
     stencil_core<DIR>(sm, lx, lz, a.cz, a.cx, valid, [&](int k) { return ldg4(a.par[k] + gi); }, t);
+    if (FS && DIR == 0 && a.fs && bz == 0) fs_forward_rows(a, sm, lx, lz, gz, gx, t);
 
     float4 csave[2];      // current vx, vz (forward EPI_TRI; shared memory is reused below)
     if (EPI == EPI_TRI && DIR == 0) {
         csave[0] = ld4(sm + lx * SZ + lz);
         csave[1] = ld4(sm + SMEM_FIELD + lx * SZ + lz);
     }
-    step_tail<DIR, EPI, 0, 5, NT>(a, sm, tile, tid, tzi, txi, gz, gx, valid, gi, t,
-                                  [&](int f) { return ld4(a.o[f] + gi); }, csave);
+    auto old = [&](int f) { return ld4(a.o[f] + gi); };
+    step_tail<DIR, EPI, 0, 5, NT, decltype(old), FS>(a, sm, tile, tid, tzi, txi, gz, gx, valid, gi, t, old, csave);
 }
 
 // Same step with two threads per float4: warps 0-7 update vx and vz, warps

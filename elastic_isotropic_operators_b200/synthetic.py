@@ -179,22 +179,25 @@ def born_600x1800(nts=4000, nshots=10, seed=2024):
                     w, nshots, extra=dict(dmodel=dmod))
 
 
-def small(nz=72, nx=104, nts=150, nshots=2, nrec=20, seed=7, sub=1, dz=10.0):
-    """Tiny layered case (parity tests): pads 12, random smooth perturbation."""
+def small(nz=72, nx=104, nts=150, nshots=2, nrec=20, seed=7, sub=1, dz=10.0, surface=0, alphaCos=0.99):
+    """Tiny layered case (parity tests): pads 12, random smooth perturbation.
+    surface = 1: free surface at the top (padding rule of padElasticFileGpuMain
+    with surfaceCondition = 1: a fat-cell top pad), devices a few cells below it."""
     pad = 12
     rng = np.random.default_rng(seed)
-    nzi, nxi = nz - 2 * FAT - 2 * pad, nx - 2 * FAT - 2 * pad
+    ztop = FAT if surface else pad
+    nzi, nxi = nz - 2 * FAT - ztop - pad, nx - 2 * FAT - 2 * pad
     assert nzi > 0 and nxi > 0
     depth = np.arange(nzi) / max(nzi - 1, 1)
     vp = np.tile(2000.0 + 1000.0 * depth, (nxi, 1)) + 100.0 * rng.standard_normal((nxi, nzi)).clip(-2, 2)
     vs = vp / 1.7
     ep = elastic_from_vpvsrho(vp, vs, gardner(vp))
-    epp, pads = pad_elastic(ep, pad, pad)
+    epp, pads = padding.pad_elastic_array(ep, pad, pad, FAT, 16, surface)
     assert epp.shape == (3, nx, nz), (epp.shape, nx, nz)
     dts = 1e-3
-    oz = -(FAT + pad) * dz
+    oz = -(FAT + pads["zPadMinus"]) * dz
     ox = -(FAT + pad) * dz
-    z0 = _grid_coord(oz, dz, FAT + pad + 2) + np.float32(3.0)     # off-grid: exercises bilinear weights
+    z0 = _grid_coord(oz, dz, FAT + pads["zPadMinus"] + 2) + np.float32(3.0)   # off-grid: exercises bilinear weights
     src_x = [_grid_coord(ox, dz, FAT + pad + 5 + 7 * e) + np.float32(4.0) for e in range(nshots)]
     rec_x = np.array([_grid_coord(ox, dz, FAT + pad + 2 + i * max(nxi - 4, 1) // nrec) + np.float32(2.5)
                       for i in range(nrec)], np.float32)
@@ -205,5 +208,8 @@ def small(nz=72, nx=104, nts=150, nshots=2, nrec=20, seed=7, sub=1, dz=10.0):
         f = gaussian_smooth(rng.standard_normal((nx, nz)), 2.0)
         f = f / np.sqrt(np.mean(f * f))
         dmod[k] = (0.05 * np.sqrt(np.mean(epp[k].astype(np.float64) ** 2)) * f).astype(np.float32)
-    return Workload("small", epp, pads, dz, dz, nts, dts, sub, 25.0, [z0] * nshots, src_x, rec_z, rec_x, w,
-                    nshots, extra=dict(dmodel=dmod))
+    wl = Workload("small", epp, pads, dz, dz, nts, dts, sub, 25.0, [z0] * nshots, src_x, rec_z, rec_x, w,
+                  nshots, extra=dict(dmodel=dmod))
+    wl.par.set("surfaceCondition", str(int(surface)))
+    wl.par.set("alphaCos", str(alphaCos))
+    return wl

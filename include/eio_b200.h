@@ -62,7 +62,7 @@ typedef struct eio_fd_params {
     int blockSize;      /* must be 16 (reference constraint) */
     int fat;            /* must be 4 */
     float alphaCos;     /* default 0.99 */
-    int surfaceCondition; /* 0 only */
+    int surfaceCondition; /* 0, or 1: free surface at z = 2*fat (nonlinear operators) */
     int mod_par;        /* 1: metres (default), 2: km in the par file */
     float errorTolerance; /* default 1e-6 */
 } eio_fd_params;

@@ -137,9 +137,10 @@ class Oracle:
         """g: dict(nz, nx, dz, dx, nts, dts, S, minPad, alphaCos).  model5/data5: lists of
         [nPts][nts] arrays of self.dt (output ones are overwritten).  wavefield: None or a
         [nts][5][nx][nz] array of self.dt, overwritten with the saved wavefield."""
-        f = self._fn("orc_nl_prop_wf")
+        f = self._fn("orc_nl_prop_fs")
         f.argtypes = [ctypes.c_int] * 3 + [ctypes.c_float] * 2 + [ctypes.c_int, ctypes.c_float, ctypes.c_int,
-                                                                   ctypes.c_int, ctypes.c_float] + [ctypes.c_void_p] * 8
+                                                                   ctypes.c_int, ctypes.c_float] + \
+            [ctypes.c_void_p] * 8 + [ctypes.c_int]
         wp = None if wavefield is None else wavefield.ctypes.data
         ns = (ctypes.c_int * 4)(*[len(p) for p in srcPos])
         nr = (ctypes.c_int * 4)(*[len(p) for p in recPos])
@@ -149,7 +150,8 @@ class Oracle:
             assert wavefield.dtype == self.dt and wavefield.flags["C_CONTIGUOUS"]
             assert wavefield.shape == (g["nts"], 5, g["nx"], g["nz"])
         r = f(adj, g["nz"], g["nx"], g["dz"], g["dx"], g["nts"], g["dts"], g["S"], g["minPad"], g["alphaCos"],
-              _pp(medium5, None), _pp(model5, None), _pp(data5, None), _pp(sp, None), ns, _pp(rp, None), nr, wp)
+              _pp(medium5, None), _pp(model5, None), _pp(data5, None), _pp(sp, None), ns, _pp(rp, None), nr, wp,
+              int(g.get("surface", 0)))
         assert r == 0, r
 
     def born_prop(self, adj, g, medium5, srcDtw5, dm5, data5, srcPos, recPos):
@@ -176,7 +178,7 @@ class RefGpu:
         self.nl = ctypes.CDLL(os.path.join(REF_DIR, "libref_nl_%s.so" % prec))
         self.born = ctypes.CDLL(os.path.join(REF_DIR, "libref_born_%s.so" % prec))
         self.nl.ref_nl_prop.argtypes = [ctypes.c_int] * 3 + [R] * 2 + [ctypes.c_int, R, ctypes.c_int, ctypes.c_int,
-                                                                       R] + [ctypes.c_void_p] * 7
+                                                                       R] + [ctypes.c_void_p] * 7 + [ctypes.c_int]
         self.born.ref_born_prop.argtypes = [ctypes.c_int] * 3 + [R] * 2 + [ctypes.c_int, R, ctypes.c_int,
                                                                            ctypes.c_int, R] + [ctypes.c_void_p] * 8
         self.nl.ref_nl_prop_wf.argtypes = [ctypes.c_int] * 3 + [R] * 2 + [ctypes.c_int, R, ctypes.c_int,
@@ -204,8 +206,10 @@ class RefGpu:
         rp = [np.ascontiguousarray(p, np.int32) for p in recPos]
         if wavefield is None:
             r = self.nl.ref_nl_prop(adj, *self._g(g), _pp(medium5, None), _pp(model5, None), _pp(data5, None),
-                                    _pp(sp, None), ns, _pp(rp, None), nr)
+                                    _pp(sp, None), ns, _pp(rp, None), nr, int(g.get("surface", 0)))
         else:
+            if g.get("surface", 0):
+                raise ValueError("the reference's wavefield drivers are driven here without the free surface")
             if not self.wavefield_supported(g):
                 raise ValueError("reference wavefield drivers overflow their 32-bit buffer size at this size")
             assert wavefield.dtype == self.dt and wavefield.flags["C_CONTIGUOUS"]
@@ -258,10 +262,13 @@ class Case:
     def grid(self):
         p = self.par
         S = 2 * int(p["sub"])
-        minPad = min(int(p["zPadMinus"]), int(p["zPadPlus"]), int(p["xPadMinus"]), int(p["xPadPlus"]))
+        surface = int(p.get("surfaceCondition", 0))
+        # fdParamElastic.cpp:43-44,74: with the free surface the top pad is not a taper
+        zPad = int(p["zPadPlus"]) if surface else min(int(p["zPadMinus"]), int(p["zPadPlus"]))
+        minPad = min(zPad, int(p["xPadMinus"]), int(p["xPadPlus"]))
         return dict(nz=int(p["nz"]), nx=int(p["nx"]), dz=float(p["dz"]), dx=float(p["dx"]), nts=int(p["nts"]),
                     dts=float(p["dts"]), S=S, minPad=minPad, alphaCos=float(p.get("alphaCos", 0.99)),
-                    ots=float(p.get("ots", 0.0)))
+                    ots=float(p.get("ots", 0.0)), surface=surface)
 
 
 def _stag_hypers(c):

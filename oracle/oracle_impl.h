@@ -427,6 +427,123 @@ static void FN(orc_damp)(const FN(orc_grid_t) *g, REAL **p0, REAL **p1)
     }
 }
 
+/* ---------------------------------------------------------------- */
+/* Free surface at z = 2*FAT (surfaceCondition = 1)                  */
+/* ---------------------------------------------------------------- */
+#define ORC_SURF (2 * ORC_FAT)
+
+/* ker_step_fwd_surface_top, K:543-587: on the current level, in place */
+static void FN(orc_fs_top)(const FN(orc_grid_t) *g, REAL **c)
+{
+    const int nz = g->nz, nx = g->nx;
+    for (int ix = ORC_FAT; ix < nx - ORC_FAT; ix++) {
+        REAL *vx = c[0] + (long)ix * nz, *vz = c[1] + (long)ix * nz, *szz = c[3] + (long)ix * nz,
+             *sxz = c[4] + (long)ix * nz;
+        const int s = ORC_SURF;
+        szz[s] = 0;
+        for (int k = 1; k <= 4; k++) szz[s - k] = -szz[s + k];
+        for (int k = 0; k < 4; k++) sxz[s - k] = -sxz[s + 1 + k];
+        for (int k = 1; k <= 4; k++) vx[s - k] = 0;
+        for (int k = 0; k <= 4; k++) vz[s - k] = 0;
+    }
+}
+
+/* ker_step_fwd_surface_body, K:589-776: the standard update below the
+ * surface, vx and the reduced sigmaxx coefficient (l2m - lam^2/l2m) on it,
+ * nothing above it */
+static void FN(orc_step_fwd_fs)(const FN(orc_grid_t) *g, const FN(orc_medium_t) *m, REAL **p0, REAL **p1)
+{
+    const int nz = g->nz, nx = g->nx;
+    const REAL *zc = g->zc, *xc = g->xc;
+    REAL *ovx = p0[0], *ovz = p0[1], *osxx = p0[2], *oszz = p0[3], *osxz = p0[4];
+    const REAL *cvx = p1[0], *cvz = p1[1], *csxx = p1[2], *cszz = p1[3], *csxz = p1[4];
+    #pragma omp parallel for schedule(static)
+    for (int ix = ORC_FAT; ix < nx - ORC_FAT; ix++) {
+        for (int iz = ORC_SURF; iz < nz - ORC_FAT; iz++) {
+            long i = (long)ix * nz + iz;
+            ovx[i] = ovx[i] + m->rhox[i] * (ORC_DM(csxx, i, nz, xc) + ORC_DP(csxz, i, 1, zc));
+            REAL dvxdx = ORC_DP(cvx, i, nz, xc);
+            if (iz == ORC_SURF) {
+                osxx[i] = osxx[i] + (m->l2m[i] - (m->lam[i] * m->lam[i] / m->l2m[i])) * dvxdx;
+                continue;
+            }
+            ovz[i] = ovz[i] + m->rhoz[i] * (ORC_DM(cszz, i, 1, zc) + ORC_DP(csxz, i, nz, xc));
+            REAL dvzdz = ORC_DP(cvz, i, 1, zc);
+            osxx[i] = osxx[i] + m->l2m[i] * dvxdx + m->lam[i] * dvzdz;
+            oszz[i] = oszz[i] + m->lam[i] * dvxdx + m->l2m[i] * dvzdz;
+            osxz[i] = osxz[i] + m->muxz[i] * (ORC_DM(cvx, i, 1, zc) + ORC_DM(cvz, i, nz, xc));
+        }
+    }
+}
+
+/* Adjoint of the free-surface step in the loop form of orc_step_adj:
+ * p0 <- M^T (p0 + U^T p1), with U the masked update above (its products
+ * vanish where U does not update) and M the top pass (M^T returns the mirrored
+ * stress rows to their sources below the surface and zeroes the rows M
+ * overwrites). */
+static void FN(orc_step_adj_fs)(const FN(orc_grid_t) *g, const FN(orc_medium_t) *m, REAL **p0, REAL **p1,
+                                REAL **scr)
+{
+    const int nz = g->nz, nx = g->nx;
+    const REAL *zc = g->zc, *xc = g->xc;
+    REAL *vxr = scr[0], *vzr = scr[1], *xxl2 = scr[2], *xxl = scr[3], *zzl2 = scr[4], *zzl = scr[5], *xzm = scr[6];
+    const REAL *cvx = p1[0], *cvz = p1[1], *csxx = p1[2], *cszz = p1[3], *csxz = p1[4];
+    #pragma omp parallel for schedule(static)
+    for (long ix = 0; ix < nx; ix++) {
+        for (long iz = 0; iz < nz; iz++) {
+            const long i = ix * nz + iz;
+            const int below = iz > ORC_SURF, on = iz == ORC_SURF;
+            vxr[i] = (below || on) ? m->rhox[i] * cvx[i] : 0;
+            vzr[i] = below ? m->rhoz[i] * cvz[i] : 0;
+            xxl2[i] = below ? m->l2m[i] * csxx[i]
+                            : on ? (m->l2m[i] - (m->lam[i] * m->lam[i] / m->l2m[i])) * csxx[i] : 0;
+            xxl[i] = below ? m->lam[i] * csxx[i] : 0;
+            zzl2[i] = below ? m->l2m[i] * cszz[i] : 0;
+            zzl[i] = below ? m->lam[i] * cszz[i] : 0;
+            xzm[i] = below ? m->muxz[i] * csxz[i] : 0;
+        }
+    }
+    REAL *ovx = p0[0], *ovz = p0[1], *osxx = p0[2], *oszz = p0[3], *osxz = p0[4];
+    #pragma omp parallel for schedule(static)
+    for (int ix = ORC_FAT; ix < nx - ORC_FAT; ix++) {
+        for (int iz = ORC_FAT; iz < nz - ORC_FAT; iz++) {
+            long i = (long)ix * nz + iz;
+            ovx[i] = ovx[i] - ORC_DM(xxl2, i, nz, xc) - ORC_DM(zzl, i, nz, xc) - ORC_DP(xzm, i, 1, zc);
+            ovz[i] = ovz[i] - ORC_DM(xxl, i, 1, zc) - ORC_DM(zzl2, i, 1, zc) - ORC_DP(xzm, i, nz, xc);
+            osxx[i] = osxx[i] - ORC_DP(vxr, i, nz, xc);
+            oszz[i] = oszz[i] - ORC_DP(vzr, i, 1, zc);
+            osxz[i] = osxz[i] - ORC_DM(vxr, i, 1, zc) - ORC_DM(vzr, i, nz, xc);
+        }
+        /* M^T on the column */
+        REAL *vx = ovx + (long)ix * nz, *vz = ovz + (long)ix * nz, *szz = oszz + (long)ix * nz,
+             *sxz = osxz + (long)ix * nz;
+        const int sf = ORC_SURF;
+        for (int k = 1; k <= 4; k++) { szz[sf + k] = szz[sf + k] - szz[sf - k]; szz[sf - k] = 0; }
+        szz[sf] = 0;
+        for (int k = 0; k < 4; k++) { sxz[sf + 1 + k] = sxz[sf + 1 + k] - sxz[sf - k]; sxz[sf - k] = 0; }
+        for (int k = 1; k <= 4; k++) vx[sf - k] = 0;
+        for (int k = 0; k <= 4; k++) vz[sf - k] = 0;
+    }
+}
+
+/* dampCosineEdge_freesurface, K:1223-1252: no taper at the top */
+static void FN(orc_damp_fs)(const FN(orc_grid_t) *g, REAL **p0, REAL **p1)
+{
+    const int nz = g->nz, nx = g->nx;
+    #pragma omp parallel for schedule(static)
+    for (int ix = ORC_FAT; ix < nx - ORC_FAT; ix++) {
+        for (int iz = ORC_FAT; iz < nz - ORC_FAT; iz++) {
+            int b = ix - ORC_FAT, c = nz - iz - 1 - ORC_FAT, d = nx - ix - 1 - ORC_FAT;
+            int dist = b; if (c < dist) dist = c; if (d < dist) dist = d;
+            if (dist < g->minPad) {
+                REAL dmp = g->damp[dist];
+                long i = (long)ix * nz + iz;
+                for (int f = 0; f < 5; f++) { p0[f][i] *= dmp; p1[f][i] *= dmp; }
+            }
+        }
+    }
+}
+
 static void FN(orc_swap)(REAL **p0, REAL **p1)
 {
     for (int f = 0; f < 5; f++) { REAL *t = p0[f]; p0[f] = p1[f]; p1[f] = t; }
@@ -501,10 +618,10 @@ static void FN(orc_save_wavefield)(const FN(orc_grid_t) *g, REAL **p, REAL *W, i
 
 /* wavefield: NULL, or [nts][5][nx][nz] overwritten with the saved wavefield
  * (propShotsElastic{Fwd,Adj}GpuWavefield, F/prop/src/nonlinearPropElasticGpuFunctions.cu:649-760, 1029-1110) */
-int FN(orc_nl_prop_wf)(int adj, int nz, int nx, float dz, float dx, int nts, float dts, int sub_int,
+int FN(orc_nl_prop_fs)(int adj, int nz, int nx, float dz, float dx, int nts, float dts, int sub_int,
                        int minPad, float alphaCos, REAL *const *medium5, REAL *const *model, REAL *const *data,
                        const int *const *srcPos, const int *nSrc, const int *const *recPos, const int *nRec,
-                       REAL *wavefield)
+                       REAL *wavefield, int surface)
 {
     FN(orc_grid_t) g;
     if (FN(orc_grid_init)(&g, nz, nx, dz, dx, nts, dts, sub_int, minPad, alphaCos)) return -1;
@@ -520,9 +637,15 @@ int FN(orc_nl_prop_wf)(int adj, int nz, int nx, float dz, float dx, int nts, flo
         for (int f = 0; f < 5; f++) memset(data[f], 0, sizeof(REAL) * nts * nRec[FN(orc_field_grid)[f]]);
         for (int its = 0; its < nts - 1; its++)
             for (int it2 = 1; it2 < g.S + 1; it2++) {
-                FN(orc_step_fwd)(&g, &m, p0, p1);
+                if (surface) {
+                    FN(orc_fs_top)(&g, p1);
+                    FN(orc_step_fwd_fs)(&g, &m, p0, p1);
+                } else {
+                    FN(orc_step_fwd)(&g, &m, p0, p1);
+                }
                 FN(orc_inject_coarse)(&g, p0, model, srcPos, nSrc, its, it2 - 1);
-                FN(orc_damp)(&g, p0, p1);
+                if (surface) FN(orc_damp_fs)(&g, p0, p1);
+                else FN(orc_damp)(&g, p0, p1);
                 if (wavefield) FN(orc_save_wavefield)(&g, p0, wavefield, its, it2);
                 FN(orc_extract_coarse)(&g, p0, data, recPos, nRec, its, it2);
                 FN(orc_swap)(p0, p1);
@@ -531,9 +654,11 @@ int FN(orc_nl_prop_wf)(int adj, int nz, int nx, float dz, float dx, int nts, flo
         for (int f = 0; f < 5; f++) memset(model[f], 0, sizeof(REAL) * nts * nSrc[FN(orc_field_grid)[f]]);
         for (int its = nts - 2; its > -1; its--)
             for (int it2 = g.S - 1; it2 > -1; it2--) {
-                FN(orc_step_adj)(&g, &m, p0, p1, scr);
+                if (surface) FN(orc_step_adj_fs)(&g, &m, p0, p1, scr);
+                else FN(orc_step_adj)(&g, &m, p0, p1, scr);
                 FN(orc_inject_coarse)(&g, p0, data, recPos, nRec, its, it2 + 1);
-                FN(orc_damp)(&g, p0, p1);
+                if (surface) FN(orc_damp_fs)(&g, p0, p1);
+                else FN(orc_damp)(&g, p0, p1);
                 if (wavefield) FN(orc_save_wavefield)(&g, p0, wavefield, its, it2);
                 FN(orc_extract_coarse)(&g, p0, model, srcPos, nSrc, its, it2);
                 FN(orc_swap)(p0, p1);
@@ -547,8 +672,17 @@ int FN(orc_nl_prop)(int adj, int nz, int nx, float dz, float dx, int nts, float 
                     int minPad, float alphaCos, REAL *const *medium5, REAL *const *model, REAL *const *data,
                     const int *const *srcPos, const int *nSrc, const int *const *recPos, const int *nRec)
 {
-    return FN(orc_nl_prop_wf)(adj, nz, nx, dz, dx, nts, dts, sub_int, minPad, alphaCos, medium5, model, data,
-                              srcPos, nSrc, recPos, nRec, NULL);
+    return FN(orc_nl_prop_fs)(adj, nz, nx, dz, dx, nts, dts, sub_int, minPad, alphaCos, medium5, model, data,
+                              srcPos, nSrc, recPos, nRec, NULL, 0);
+}
+
+int FN(orc_nl_prop_wf)(int adj, int nz, int nx, float dz, float dx, int nts, float dts, int sub_int,
+                       int minPad, float alphaCos, REAL *const *medium5, REAL *const *model, REAL *const *data,
+                       const int *const *srcPos, const int *nSrc, const int *const *recPos, const int *nRec,
+                       REAL *wavefield)
+{
+    return FN(orc_nl_prop_fs)(adj, nz, nx, dz, dx, nts, dts, sub_int, minPad, alphaCos, medium5, model, data,
+                              srcPos, nSrc, recPos, nRec, wavefield, 0);
 }
 
 /* ------------------------------------------------------------------ */

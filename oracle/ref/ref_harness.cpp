@@ -28,7 +28,7 @@ typedef REF_REAL real;
 /* model: 5 regular-grid source arrays [nSrcReg][nts]; data: 5 [nRecReg][nts]. */
 EXPORT int ref_nl_prop(int adj, int nz, int nx, real dz, real dx, int nts, real dts, int sub_int,
                        int minPad, real alphaCos, real **medium, real **model, real **data,
-                       int **srcPos, const int *nSrc, int **recPos, const int *nRec)
+                       int **srcPos, const int *nSrc, int **recPos, const int *nRec, int surface)
 {
     initNonlinearElasticGpu(dz, dx, nz, nx, nts, dts, sub_int, minPad, 16, alphaCos, 1, 0, 0);
     allocateNonlinearElasticGpu(medium[0], medium[1], medium[2], medium[3], medium[4], 0, 0);
@@ -37,13 +37,13 @@ EXPORT int ref_nl_prop(int adj, int nz, int nx, real dz, real dx, int nts, real 
                                data[0], data[1], data[2], data[3], data[4],
                                srcPos[0], nSrc[0], srcPos[1], nSrc[1], srcPos[2], nSrc[2], srcPos[3], nSrc[3],
                                recPos[0], nRec[0], recPos[1], nRec[1], recPos[2], nRec[2], recPos[3], nRec[3],
-                               0, 0, 0);
+                               0, 0, surface);
     else
         propShotsElasticAdjGpu(model[0], model[1], model[2], model[3], model[4],
                                data[0], data[1], data[2], data[3], data[4],
                                srcPos[0], nSrc[0], srcPos[1], nSrc[1], srcPos[2], nSrc[2], srcPos[3], nSrc[3],
                                recPos[0], nRec[0], recPos[1], nRec[1], recPos[2], nRec[2], recPos[3], nRec[3],
-                               0, 0, 0);
+                               0, 0, surface);
     deallocateNonlinearElasticGpu(0, 0);
     return 0;
 }

@@ -199,3 +199,33 @@ def test_saved_wavefield_equals_traces_at_the_devices(adj):
     # nothing is written outside the updated interior
     assert not W[:, :, :4].any() and not W[:, :, -4:].any()
     assert not W[..., :4].any() and not W[..., -4:].any()
+
+
+@pytest.mark.parametrize("alpha,tol", [(1.0, 1e-12), (0.99, 1e-6)])
+def test_free_surface_forward_adjoint_dot_product(alpha, tol):
+    """Free surface (surfaceCondition = 1): the oracle's adjoint step (masked
+    products, transposed stencils, transpose of the top mirroring) against its
+    forward step (top mirroring, masked update, reduced sigmaxx coefficient on
+    the surface).  Without the taper (alphaCos = 1) the pair is adjoint to
+    rounding; the taper brings the same small deviation as without the free
+    surface (the damping is applied after the update in both directions)."""
+    from elastic_isotropic_operators_b200 import synthetic
+    from helpers import reg_inputs
+    w = synthetic.small(nts=80, surface=1, alphaCos=alpha)
+    r = reg_inputs(w, "d", seed=9)
+    orc, g = r["orc"], r["g"]
+    assert g["surface"] == 1
+    m = [x.copy() for x in r["model"]]
+    d = [x.copy() for x in r["data"]]
+    fd = [np.zeros_like(x) for x in d]
+    orc.nl_prop(0, g, r["med"], m, fd, r["sp"], r["rp"])
+    am = [np.zeros_like(x) for x in m]
+    orc.nl_prop(1, g, r["med"], am, d, r["sp"], r["rp"])
+    lhs = sum(float(np.dot(a.ravel(), b.ravel())) for a, b in zip(fd, d))
+    rhs = sum(float(np.dot(a.ravel(), b.ravel())) for a, b in zip(m, am))
+    assert abs(lhs - rhs) <= tol * abs(lhs), (lhs, rhs, abs(lhs - rhs) / abs(lhs))
+    # the surface changes the result
+    g0 = dict(g, surface=0)
+    fd0 = [np.zeros_like(x) for x in d]
+    orc.nl_prop(0, g0, r["med"], m, fd0, r["sp"], r["rp"])
+    assert sum(float(np.abs(a - b).max()) for a, b in zip(fd, fd0)) > 0
