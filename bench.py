@@ -32,6 +32,7 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 BYTES_PER_CELL = 80.0    # read 5 current + 5 old + 5 medium, write 5 new (FP32)
+PAIR_BYTES_PER_CELL = 100.0   # two steps per launch: read 5 current + 5 old + 5 medium, write 2 x 5 new
 
 
 def parse():
@@ -45,9 +46,10 @@ def parse():
     ap.add_argument("--nts", type=int, default=4000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--kernel", type=int, default=-1, choices=[-1, 0, 1, 2, 3, 4],
+    ap.add_argument("--kernel", type=int, default=-1, choices=[-1, 0, 1, 2, 3, 4, 5],
                     help="-1: autotune (default); 0: tile kernel k_step; 1: TMA sweep kernel k_sweep; "
-                         "2: persistent TMA tile kernel k_tile; 3: k_step at 4 CTAs/SM; 4: split-field k_split")
+                         "2: persistent TMA tile kernel k_tile; 3: k_step at 4 CTAs/SM; 4: split-field k_split; "
+                         "5: two steps per launch k_pair")
     return ap.parse_args()
 
 
@@ -115,9 +117,11 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per k_step launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "k_step_traffic.txt")
+def profile_traffic(bytes_per_cell=BYTES_PER_CELL):
+    """DRAM bytes per launch of the dominant step kernel (k_step, or k_pair for
+    two steps per launch) from the committed ncu summary, if any."""
+    name = "k_pair_traffic.txt" if bytes_per_cell == PAIR_BYTES_PER_CELL else "k_step_traffic.txt"
+    path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_launch_full_size:"):
@@ -148,7 +152,28 @@ def kernel_name(L, ctx):
         return "k_step (fused 5-field update, 64x16 tiles, 4 CTAs/SM)"
     if kind == 4:
         return "k_split (fused 5-field update, 64x16 tiles, two threads per float4)"
+    if kind == 5:
+        return "k_pair (two fused 5-field steps per launch, 64x16 tiles widened by the stencil radius)"
     return "k_sweep (fused 5-field update, TMA x-sweep, tz=%d cw=%d cpr=%d)" % (tz, cw, cpr)
+
+
+def read_stats(L, ctx):
+    """Step-kernel counters of the timed region (and reset them): the dominant
+    kernel's mean launch time and its algorithmic bytes per launch.  With the
+    two-step kernel the dominant launches are the two-step ones (100 B per cell
+    for two updates); otherwise the single steps (80 B per cell)."""
+    import ctypes
+    pl, pms = ctypes.c_longlong(), ctypes.c_double()
+    L.eio_ctx_pair_stats(ctx, ctypes.byref(pl), ctypes.byref(pms))
+    launches, sl, sms = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_double()
+    L.eio_ctx_stats(ctx, 0, 1, ctypes.byref(launches), ctypes.byref(sl), ctypes.byref(sms))
+    singles, single_ms = sl.value - pl.value, sms.value - pms.value
+    if pl.value > 0 and pms.value >= single_ms:
+        avg, bpc, n = pms.value / pl.value, PAIR_BYTES_PER_CELL, pl.value
+    else:
+        avg, bpc, n = single_ms / max(singles, 1), BYTES_PER_CELL, singles
+    return {"launches": int(launches.value), "avg_ms": avg, "bytes_per_cell": bpc, "dominant_launches": int(n),
+            "step_launches": int(sl.value), "pair_launches": int(pl.value)}
 
 
 def dist_init(args):
@@ -267,20 +292,20 @@ def run_ours(args, ws, rank, local):
         t_ms += ev0.elapsed_time(ev1)
     barrier(ws)
     clk = clocks.stop()
-    launches, step_launches, step_ms = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_double()
-    L.eio_ctx_stats(ctx, 0, 1, ctypes.byref(launches), ctypes.byref(step_launches), ctypes.byref(step_ms))
+    st = read_stats(L, ctx)
     t_ms = max_over_ranks(ws, t_ms)
     value = ws * updates_per_step * args.steps / (t_ms * 1e-3) / 1e9
 
-    # roofline of the dominant kernel (fused step)
-    avg_launch_ms = step_ms.value / max(step_launches.value, 1)
-    achieved = BYTES_PER_CELL * cells / (avg_launch_ms * 1e-3) / 1e9
+    # roofline of the dominant kernel (fused step, or two fused steps per launch)
+    avg_launch_ms = st["avg_ms"]
+    achieved = st["bytes_per_cell"] * cells / (avg_launch_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peak()
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 4), "traffic": profile_traffic(),
+            "frac": round(achieved / peak, 4), "traffic": profile_traffic(st["bytes_per_cell"]),
             "peak_source": peak_kind, "kernel": kernel_name(L, ctx),
             "avg_launch_us": round(avg_launch_ms * 1e3, 3),
-            "algorithmic_bytes_per_launch": BYTES_PER_CELL * cells,
+            "algorithmic_bytes_per_launch": st["bytes_per_cell"] * cells,
+            "launches": {"step_kernel": st["step_launches"], "two_step": st["pair_launches"]},
             # whole job: every cell update of the timed region at 80 B (step kernels, imaging,
             # sparse work and launch gaps included)
             "job_gbs": round(BYTES_PER_CELL * value, 1),
@@ -340,7 +365,7 @@ def run_ours(args, ws, rank, local):
                          "L2 flush between timed steps"},
         "shot_gradients_per_s": round(ws * nsh * args.steps / (t_ms * 1e-3), 4),
         "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
-        "gpu_launches": int(launches.value),
+        "gpu_launches": st["launches"],
     }
     return out
 
@@ -568,12 +593,11 @@ def run_ours_nl(args, ws, rank, local):
         torch.cuda.synchronize()
         t_ms += ev0.elapsed_time(ev1)
     clk = clocks.stop()
-    launches, sl, sms = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_double()
-    L.eio_ctx_stats(ctx, 0, 1, ctypes.byref(launches), ctypes.byref(sl), ctypes.byref(sms))
+    st = read_stats(L, ctx)
     t_ms = max_over_ranks(ws, t_ms)
-    avg = sms.value / max(sl.value, 1)
+    avg = st["avg_ms"]
     peak, pk = measured_peak()
-    ach = BYTES_PER_CELL * cells / (avg * 1e-3) / 1e9
+    ach = st["bytes_per_cell"] * cells / (avg * 1e-3) / 1e9
     model = nl.modelSpace()
     model.getNdArray()[...] = w.source_signal()[None]
     data = nl.dataSpace()
@@ -603,8 +627,9 @@ def run_ours_nl(args, ws, rank, local):
                     "d2h_bytes_per_step": int(sum(4 * t.numel() for t in d_dev))},
             "roofline": {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(ach / peak, 4), "traffic": None, "peak_source": pk,
-                         "kernel": kernel_name(L, ctx), "avg_launch_us": round(avg * 1e3, 3)},
-            "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches.value)}
+                         "kernel": kernel_name(L, ctx), "avg_launch_us": round(avg * 1e3, 3),
+                         "algorithmic_bytes_per_launch": st["bytes_per_cell"] * cells},
+            "cpu_baseline": cpu, "clocks": clk, "gpu_launches": st["launches"]}
 
 
 def main():

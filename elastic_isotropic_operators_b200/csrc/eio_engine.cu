@@ -19,6 +19,7 @@
 
 #include "eio_internal.h"
 #include "eio_kernels.cuh"
+#include "eio_pair.cuh"
 #include "eio_sweep.cuh"
 #include "eio_tile.cuh"
 
@@ -63,6 +64,8 @@ struct PointList {
     std::vector<PointEntry> ent;
     int ld[5] = {0, 0, 0, 0, 0};
     bool any = false;
+    const int* const* pos = nullptr;   // the position lists the buckets came from
+    const int* npos = nullptr;
 };
 
 struct Engine {
@@ -82,13 +85,16 @@ struct Engine {
     int ntz = 0, ntx = 0, ntiles = 0;
     int ckpt = 0;           // source-wavefield snapshots: 0 FP32, 1 BF16, 2 FP16 (scaled per snapshot)
     DBuf Wq, wscale, wstage, wpmax;   // 16-bit history, scales [nts][2], FP32 staging row pair, warp maxima
-    DBuf par[5], dampz, dampx, wf[10];
+    // wavefield levels: two sets of 5 slices for the single-step kernels, four
+    // for the two-step kernel (it writes both new levels to the free sets)
+    DBuf par[5], dampz, dampx, wf[20];
     // free surface (nonlinear operators only, like the reference): taper
     // without the top edge, sigmaxx coefficient of the surface row per column
     int fs = 0;
     bool fs_active = false;   // set while a free-surface propagation runs (k_step only)
     DBuf dampz_fs, fsc;
     DBuf inj_ts, inj_ent, ext_ts, ext_ent;
+    DBuf inj_hts, inj_hent;   // source lists of the widened tiles (two-step kernel)
     DBuf sig_in[5], sig_out[5];
     DBuf stage_a[5], stage_b[5], stage_c[5];
     DBuf W, ss[20];         // secondary-source ring: 4 slots x 5 fields
@@ -103,7 +109,8 @@ struct Engine {
     // step-kernel choice: kind 0 = shared-memory tile kernel (k_step),
     // kind 1 = TMA x-sweep (k_sweep) with strip height tz, chunk width cw and
     // cpr chunks per CTA, kind 2 = persistent TMA-pipelined tile kernel (k_tile),
-    // kind 3 = k_step at 4 CTAs per SM, kind 4 = two threads per float4 (k_split)
+    // kind 3 = k_step at 4 CTAs per SM, kind 4 = two threads per float4 (k_split),
+    // kind 5 = two fine steps per launch (k_pair) with kind 3 for single steps
     int kind = 1, tz = 64, cw = 8, cpr = 8;
     bool tuned = false;
     // tensor maps of the sweep kernel (valid for mtz/mcw)
@@ -117,8 +124,11 @@ struct Engine {
     // launch statistics (bench instrumentation)
     long long launches = 0, step_launches = 0, sampled = 0;
     double step_ms = 0.0;
+    long long pair_launches = 0, pair_sampled = 0;   // two-step launches (also counted in step_launches)
+    double pair_ms = 0.0;
     bool stats = false;
     std::vector<cudaEvent_t> ev;
+    std::vector<unsigned char> ev_pair;   // per event pair: 1 = a two-step launch
     size_t ev_used = 0;
 };
 
@@ -131,11 +141,13 @@ static void stats_flush(Engine* e) {
     for (size_t k = 0; k + 1 < e->ev_used; k += 2) {
         float ms = 0.f;
         EIO_CUDA(cudaEventElapsedTime(&ms, e->ev[k], e->ev[k + 1]));
-        e->step_ms += ms;
+        if (e->ev_pair[k / 2]) e->pair_ms += ms;
+        else e->step_ms += ms;
     }
     e->ev_used = 0;
 }
-static void stats_mark(Engine* e) {
+// pair: the launch the mark opens (or closes) is a two-step launch
+static void stats_mark(Engine* e, bool pair = false) {
     if (!e->stats) return;
     if (e->ev_used == e->ev.size()) {
         if (e->ev.size() >= 65536) stats_flush(e);
@@ -146,8 +158,10 @@ static void stats_mark(Engine* e) {
                 EIO_CUDA(cudaEventCreate(&x));
                 e->ev.push_back(x);
             }
+            e->ev_pair.resize(e->ev.size() / 2);
         }
     }
+    e->ev_pair[e->ev_used / 2] = pair ? 1 : 0;
     EIO_CUDA(cudaEventRecord(e->ev[e->ev_used++], e->st));
 }
 
@@ -223,7 +237,10 @@ Engine* engine_create(int device, const FdParam& fd) {
             EIO_CUDA(cudaEventCreateWithFlags(&e->ev_free[k], cudaEventDisableTiming));
         }
         EIO_CUDA(cudaEventCreateWithFlags(&e->ev_sync, cudaEventDisableTiming));
-        for (int f = 0; f < 10; f++) e->wf[f].ensure(sizeof(float) * e->n);
+        for (int f = 0; f < 20; f++) {
+            e->wf[f].ensure(sizeof(float) * e->n);
+            EIO_CUDA(cudaMemsetAsync(e->wf[f].p, 0, sizeof(float) * e->n, e->st));
+        }
         engine_set_medium(e, fd);
     } catch (...) {
         engine_destroy(e);
@@ -237,7 +254,8 @@ void engine_destroy(Engine* e) {
     cudaSetDevice(e->device);
     if (e->st) cudaStreamSynchronize(e->st);
     if (e->st2) cudaStreamSynchronize(e->st2);
-    DBuf* all[] = {&e->dampz, &e->dampx, &e->inj_ts, &e->inj_ent, &e->ext_ts, &e->ext_ent, &e->W, &e->err, &e->wsave,
+    DBuf* all[] = {&e->dampz, &e->dampx, &e->inj_ts, &e->inj_ent, &e->inj_hts, &e->inj_hent, &e->ext_ts, &e->ext_ent,
+                   &e->W, &e->err, &e->wsave,
                    &e->Wq, &e->wscale, &e->wstage, &e->wpmax, &e->dampz_fs, &e->fsc};
     for (DBuf* b : all) b->release();
     for (int k = 0; k < 4; k++) {
@@ -248,7 +266,7 @@ void engine_destroy(Engine* e) {
         e->par[f].release(); e->sig_in[f].release(); e->sig_out[f].release();
         e->stage_a[f].release(); e->stage_b[f].release(); e->stage_c[f].release();
     }
-    for (int f = 0; f < 10; f++) e->wf[f].release();
+    for (int f = 0; f < 20; f++) e->wf[f].release();
     for (int f = 0; f < 20; f++) e->ss[f].release();
     for (cudaEvent_t x : e->ev) cudaEventDestroy(x);
     for (int k = 0; k < 4; k++) {
@@ -268,12 +286,22 @@ void engine_set_checkpoint(Engine* e, int mode) {
 
 void* engine_stream(Engine* e) { return (void*)e->st; }
 
-void engine_stats(Engine* e, int enable, int reset, long long* launches, long long* step_launches, double* step_ms) {
+// step_launches / step_ms cover every step-kernel launch (single- and two-step),
+// pair_launches / pair_ms the two-step ones alone; times are sampled means x counts
+void engine_stats(Engine* e, int enable, int reset, long long* launches, long long* step_launches, double* step_ms,
+                  long long* pair_launches, double* pair_ms) {
     stats_flush(e);
+    const double single = e->sampled ? e->step_ms * (double)e->step_launches / (double)e->sampled : 0.0;
+    const double pair = e->pair_sampled ? e->pair_ms * (double)e->pair_launches / (double)e->pair_sampled : 0.0;
     if (launches) *launches = e->launches;
-    if (step_launches) *step_launches = e->step_launches;
-    if (step_ms) *step_ms = e->sampled ? e->step_ms * (double)e->step_launches / (double)e->sampled : 0.0;
-    if (reset) { e->launches = 0; e->step_launches = 0; e->sampled = 0; e->step_ms = 0.0; }
+    if (step_launches) *step_launches = e->step_launches + e->pair_launches;
+    if (step_ms) *step_ms = single + pair;
+    if (pair_launches) *pair_launches = e->pair_launches;
+    if (pair_ms) *pair_ms = pair;
+    if (reset) {
+        e->launches = 0; e->step_launches = 0; e->sampled = 0; e->step_ms = 0.0;
+        e->pair_launches = 0; e->pair_sampled = 0; e->pair_ms = 0.0;
+    }
     if (enable >= 0) e->stats = enable != 0;
 }
 
@@ -291,8 +319,21 @@ static TileGeom tile_geom(const Engine* e) {
     return {e->tz, e->cw, (e->nz - 2 * FAT + e->tz - 1) / e->tz};
 }
 
+// CSR of (tile, entry) pairs, entries of a tile in their original order
+static void bucket(const std::vector<std::pair<int, PointEntry>>& tmp, int ntiles, PointList& pl) {
+    pl.any = !tmp.empty();
+    pl.tile_start.assign(ntiles + 1, 0);
+    for (auto& t : tmp) pl.tile_start[t.first + 1]++;
+    for (int i = 0; i < ntiles; i++) pl.tile_start[i + 1] += pl.tile_start[i];
+    pl.ent.resize(tmp.size());
+    std::vector<int> cur(pl.tile_start.begin(), pl.tile_start.end() - 1);
+    for (auto& t : tmp) pl.ent[cur[t.first]++] = t.second;
+}
+
 // Sort the points of the four position lists into per-tile buckets.
 static void build_points(const Engine* e, const int* const pos[4], const int npos[4], PointList& pl) {
+    pl.pos = pos;
+    pl.npos = npos;
     const TileGeom tg = tile_geom(e);
     const int nchunks = (e->nx - 2 * FAT) / tg.tx;
     const int ntiles = tg.ntz * nchunks;
@@ -314,13 +355,34 @@ static void build_points(const Engine* e, const int* const pos[4], const int npo
             tmp.push_back({tiled(eff_kind(e)) ? bx * tg.ntz + bz : bz * nchunks + bx, pe});
         }
     }
-    pl.any = !tmp.empty();
-    pl.tile_start.assign(ntiles + 1, 0);
-    for (auto& t : tmp) pl.tile_start[t.first + 1]++;
-    for (int i = 0; i < ntiles; i++) pl.tile_start[i + 1] += pl.tile_start[i];
-    pl.ent.resize(tmp.size());
-    std::vector<int> cur(pl.tile_start.begin(), pl.tile_start.end() - 1);
-    for (auto& t : tmp) pl.ent[cur[t.first]++] = t.second;
+    bucket(tmp, ntiles, pl);
+}
+
+// Sources of the widened tiles of the two-step kernel (k_pair): a point joins
+// the list of every tile whose widened tile (the tile plus the 4-cell stencil
+// radius) holds it, keyed from the widened tile's corner.  Bounds are checked
+// by build_points.
+static void build_halo_points(const Engine* e, const int* const pos[4], const int npos[4], PointList& pl) {
+    std::vector<std::pair<int, PointEntry>> tmp;
+    for (int f = 0; f < 5; f++) {
+        const int g = kFieldGrid[f];
+        pl.ld[f] = npos[g];
+        for (int k = 0; k < npos[g]; k++) {
+            const int cell = pos[g][k];
+            const int ix = cell / e->nz, iz = cell % e->nz;
+            const int bz0 = (iz - FAT) / TZ, bx0 = (ix - FAT) / TX;
+            for (int bz = std::max(bz0 - 1, 0); bz <= std::min(bz0 + 1, e->ntz - 1); bz++)
+                for (int bx = std::max(bx0 - 1, 0); bx <= std::min(bx0 + 1, e->ntx - 1); bx++) {
+                    const int lz = iz - bz * TZ, lx = ix - bx * TX;   // corner (FAT + bz*TZ - FAT, ...)
+                    if (lz < 0 || lz >= SZ || lx < 0 || lx >= SX) continue;
+                    PointEntry pe;
+                    pe.key = (f << 16) | (lx << 8) | lz;
+                    pe.col = k;
+                    tmp.push_back({bx * e->ntz + bz, pe});
+                }
+        }
+    }
+    bucket(tmp, e->ntiles, pl);
 }
 
 static SparseOp upload_points(Engine* e, const PointList& pl, DBuf& ts, DBuf& ent, DBuf* sig) {
@@ -517,7 +579,7 @@ static void launch_pdl(K kern, int grid, int block, cudaStream_t st, const StepA
 
 template <int DIR, int EPI>
 static void launch_step(Engine* e, StepArgs& a, int cur) {
-    const bool timed = e->stats && e->step_launches % STATS_PERIOD == 0;
+    const bool timed = e->stats && (e->step_launches + e->pair_launches) % STATS_PERIOD == 0;
     if (timed) stats_mark(e);
     const int kind = eff_kind(e);
     bool done = false;
@@ -530,7 +592,7 @@ static void launch_step(Engine* e, StepArgs& a, int cur) {
     if (done) {
     } else if (kind == 0) launch_pdl(k_step<DIR, EPI, 3>, e->ntiles, NT, e->st, a);
     else if (kind == 2) launch_tile<DIR, EPI>(e, a, cur);
-    else if (kind == 3) launch_pdl(k_step<DIR, EPI, 4>, e->ntiles, NT, e->st, a);
+    else if (kind == 3 || kind == 5) launch_pdl(k_step<DIR, EPI, 4>, e->ntiles, NT, e->st, a);
     else if (kind == 4) launch_pdl(k_split<DIR, EPI>, e->ntiles, NT2, e->st, a);
     else launch_sweep<DIR, EPI>(e, a, cur);
     if (timed) {
@@ -541,12 +603,90 @@ static void launch_step(Engine* e, StepArgs& a, int cur) {
     e->step_launches++;
 }
 
+// two fine steps in one launch (kind 5); the dynamic shared memory of each
+// instantiation is opened once per device
+template <int DIR, int EPI>
+static void launch_pair(Engine* e, const PairArgs& p) {
+    static_assert(sizeof(PairArgs) <= 4096, "kernel parameter block");
+    static unsigned char opened[64] = {};
+    if (e->device < 64 && !opened[e->device]) {
+        EIO_CUDA(cudaFuncSetAttribute(k_pair<DIR, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, PAIR_SMEM));
+        opened[e->device] = 1;
+    }
+    const bool timed = e->stats && (e->step_launches + e->pair_launches) % STATS_PERIOD == 0;
+    if (timed) stats_mark(e, true);
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(e->ntiles);
+    cfg.blockDim = dim3(NT);
+    cfg.dynamicSmemBytes = PAIR_SMEM;
+    cfg.stream = e->st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    EIO_CUDA(cudaLaunchKernelEx(&cfg, k_pair<DIR, EPI>, p));
+    if (timed) {
+        stats_mark(e, true);
+        e->pair_sampled++;
+    }
+    e->launches++;
+    e->pair_launches++;
+}
+
+// Wavefield levels of a propagation: o and c of the next step, and the two
+// free sets that a two-step launch writes its new levels to.
+struct Levels {
+    float* o[5]; float* c[5]; float* f0[5]; float* f1[5];
+    explicit Levels(Engine* e) {
+        for (int f = 0; f < 5; f++) {
+            o[f] = e->wf[f].f(); c[f] = e->wf[5 + f].f(); f0[f] = e->wf[10 + f].f(); f1[f] = e->wf[15 + f].f();
+        }
+    }
+    void set(StepArgs& a) const {
+        for (int f = 0; f < 5; f++) { a.o[f] = o[f]; a.c[f] = c[f]; }
+    }
+    void single() { std::swap(o, c); }                       // the new level replaced o
+    void pair() { std::swap(o, f0); std::swap(c, f1); }      // o, c = the two new levels
+};
+
+// one two-step launch: a0, a1 carry the per-step parameters of steps t+1 and
+// t+2 (a0.inj the time weights of step A); injh = the widened-tile source lists
+template <int DIR, int EPI>
+static void run_pair(Engine* e, StepArgs a0, StepArgs a1, const SparseOp& injh, Levels& L) {
+    PairArgs p;
+    for (int f = 0; f < 5; f++) {
+        a0.o[f] = L.o[f]; a0.c[f] = L.c[f];
+        a1.o[f] = L.f1[f]; a1.c[f] = L.f0[f];
+        p.n1[f] = L.f0[f];
+    }
+    SparseOp hi = injh;
+    hi.t0 = a0.inj.t0; hi.w0 = a0.inj.w0; hi.w1 = a0.inj.w1;
+    a0.inj = hi;
+    p.s[0] = a0;
+    p.s[1] = a1;
+    launch_pair<DIR, EPI>(e, p);
+    L.pair();
+}
+
+// the widened-tile source lists of a propagation (two-step kernel only)
+static SparseOp halo_sources(Engine* e, bool use_pair, const int* const pos[4], const int npos[4], DBuf* sig) {
+    SparseOp op;
+    memset(&op, 0, sizeof(op));
+    if (!use_pair) return op;
+    PointList pl;
+    build_halo_points(e, pos, npos, pl);
+    return upload_points(e, pl, e->inj_hts, e->inj_hent, sig);
+}
+
 // ---------------------------------------------------------------- autotuner
 struct KernelCfg {
     int kind, tz, cw, cpr;
 };
 static const KernelCfg kCandidates[] = {
     {0, TZ, TX, 0},
+    {5, TZ, TX, 0},
     {2, TZ, TX, 0},
     {3, TZ, TX, 0},
     {4, TZ, TX, 0},
@@ -600,12 +740,20 @@ void engine_autotune(Engine* e) {
         if (!cfg_valid(e, c)) continue;
         e->kind = c.kind;
         if (c.kind == 1) { e->tz = c.tz; e->cw = c.cw; e->cpr = c.cpr; }
-        float tot = 0.f;
+        float tot = 0.f;   // per fine step
         for (int dir = 0; dir < 2; dir++) {
             int cur = 0;
             const int reps = 12;
+            Levels L(e);
+            SparseOp none;
+            memset(&none, 0, sizeof(none));
             for (int r = 0; r < reps + 3; r++) {
                 if (r == 3) EIO_CUDA(cudaEventRecord(t0, e->st));
+                if (c.kind == 5) {
+                    if (dir == 0) run_pair<0, EPI_NONE>(e, a, a, none, L);
+                    else run_pair<1, EPI_NONE>(e, a, a, none, L);
+                    continue;
+                }
                 for (int f = 0; f < 5; f++) { a.o[f] = e->wf[cur * 5 + f].f(); a.c[f] = e->wf[(1 - cur) * 5 + f].f(); }
                 if (dir == 0) launch_step<0, EPI_NONE>(e, a, cur);
                 else launch_step<1, EPI_NONE>(e, a, cur);
@@ -615,7 +763,7 @@ void engine_autotune(Engine* e) {
             EIO_CUDA(cudaEventSynchronize(t1));
             float ms = 0.f;
             EIO_CUDA(cudaEventElapsedTime(&ms, t0, t1));
-            tot += ms / reps;
+            tot += ms / (c.kind == 5 ? 2 * reps : reps);
         }
         if (tot < best) { best = tot; bestc = c; }
     }
@@ -623,6 +771,7 @@ void engine_autotune(Engine* e) {
     cudaEventDestroy(t1);
     e->launches = 0;
     e->step_launches = 0;
+    e->pair_launches = 0;
     e->kind = bestc.kind;
     if (bestc.kind == 1) { e->tz = bestc.tz; e->cw = bestc.cw; e->cpr = bestc.cpr; }
     e->tuned = true;
@@ -633,7 +782,7 @@ void engine_autotune(Engine* e) {
 }
 
 static void zero_wavefields(Engine* e) {
-    for (int f = 0; f < 10; f++) EIO_CUDA(cudaMemsetAsync(e->wf[f].p, 0, sizeof(float) * e->n, e->st));
+    for (int f = 0; f < 20; f++) EIO_CUDA(cudaMemsetAsync(e->wf[f].p, 0, sizeof(float) * e->n, e->st));
 }
 
 static void check_launch() {
@@ -702,47 +851,68 @@ void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], 
     build_points(e, g.recPos, g.nRec, rec);
     StepArgs a = base_args(e);
     zero_wavefields(e);
-    float* p0[5]; float* p1[5];
-    for (int f = 0; f < 5; f++) { p0[f] = e->wf[f].f(); p1[f] = e->wf[5 + f].f(); }
-    int cur = 0;   // buffer holding the old level (p0)
+    Levels L(e);
+    int cur = 0;   // buffer set holding the old level (TMA kernels)
     const float* F = e->filt.data();
     const int h = e->h;
+    // two fine steps per launch unless a step needs work between the steps
+    const bool use_pair = e->kind == 5 && !wfld && !e->fs_active;
+    // the fine steps in propagation order: (its, it2)
+    std::vector<std::pair<int, int>> steps;
+    if (!adj) {
+        for (int its = 0; its < e->nts - 1; its++)
+            for (int it2 = 1; it2 < e->S + 1; it2++) steps.push_back({its, it2});
+    } else {
+        for (int its = e->nts - 2; its > -1; its--)
+            for (int it2 = e->S - 1; it2 > -1; it2--) steps.push_back({its, it2});
+    }
+    // time weights of the sparse injection and extraction of one step
+    auto weights = [&](StepArgs& x, int its, int it2) {
+        const int ki = adj ? it2 + 1 : it2 - 1;
+        x.inj.t0 = its; x.inj.w0 = F[ki]; x.inj.w1 = F[h + ki];
+        x.ext.t0 = its; x.ext.w0 = F[it2]; x.ext.w1 = F[h + it2];
+    };
+    SparseOp injh;
     if (!adj) {
         stage_in(e, model, src.ld, e->nts, e->sig_in);
         zero_out(e, rec.ld, e->nts, e->sig_out);
         a.inj = upload_points(e, src, e->inj_ts, e->inj_ent, e->sig_in);
         a.ext = upload_points(e, rec, e->ext_ts, e->ext_ent, e->sig_out);
-        for (int its = 0; its < e->nts - 1; its++)
-            for (int it2 = 1; it2 < e->S + 1; it2++) {
-                for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; }
-                a.inj.t0 = its; a.inj.w0 = F[it2 - 1]; a.inj.w1 = F[h + it2 - 1];
-                a.ext.t0 = its; a.ext.w0 = F[it2]; a.ext.w1 = F[h + it2];
-                if (e->fs_active) fs_top(e, p1);
-                launch_step<0, EPI_NONE>(e, a, cur);
-                if (wfld) save_wavefield(e, wfld, p0, its, F[it2], F[h + it2]);
-                std::swap(p0, p1);
-                cur ^= 1;
-            }
-        check_launch();
-        stage_out(e, rec.ld, e->nts, e->sig_out, data);
+        injh = halo_sources(e, use_pair, g.srcPos, g.nSrc, e->sig_in);
     } else {
         stage_in(e, data, rec.ld, e->nts, e->sig_in);
         zero_out(e, src.ld, e->nts, e->sig_out);
         a.inj = upload_points(e, rec, e->inj_ts, e->inj_ent, e->sig_in);
         a.ext = upload_points(e, src, e->ext_ts, e->ext_ent, e->sig_out);
-        for (int its = e->nts - 2; its > -1; its--)
-            for (int it2 = e->S - 1; it2 > -1; it2--) {
-                for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; }
-                a.inj.t0 = its; a.inj.w0 = F[it2 + 1]; a.inj.w1 = F[h + it2 + 1];
-                a.ext.t0 = its; a.ext.w0 = F[it2]; a.ext.w1 = F[h + it2];
-                launch_step<1, EPI_NONE>(e, a, cur);
-                if (wfld) save_wavefield(e, wfld, p0, its, F[it2], F[h + it2]);
-                std::swap(p0, p1);
-                cur ^= 1;
-            }
-        check_launch();
-        stage_out(e, src.ld, e->nts, e->sig_out, model);
+        injh = halo_sources(e, use_pair, g.recPos, g.nRec, e->sig_in);
     }
+    for (size_t i = 0; i < steps.size();) {
+        if (use_pair && i + 1 < steps.size()) {
+            StepArgs a0 = a, a1 = a;
+            weights(a0, steps[i].first, steps[i].second);
+            weights(a1, steps[i + 1].first, steps[i + 1].second);
+            if (!adj) run_pair<0, EPI_NONE>(e, a0, a1, injh, L);
+            else run_pair<1, EPI_NONE>(e, a0, a1, injh, L);
+            i += 2;
+            continue;
+        }
+        const int its = steps[i].first, it2 = steps[i].second;
+        L.set(a);
+        weights(a, its, it2);
+        if (!adj) {
+            if (e->fs_active) fs_top(e, L.c);
+            launch_step<0, EPI_NONE>(e, a, cur);
+        } else {
+            launch_step<1, EPI_NONE>(e, a, cur);
+        }
+        if (wfld) save_wavefield(e, wfld, L.o, its, F[it2], F[h + it2]);
+        L.single();
+        cur ^= 1;
+        i++;
+    }
+    check_launch();
+    if (!adj) stage_out(e, rec.ld, e->nts, e->sig_out, data);
+    else stage_out(e, src.ld, e->nts, e->sig_out, model);
     EIO_CUDA(cudaStreamSynchronize(e->st));
     stats_flush(e);
     err_check(e);
@@ -830,10 +1000,10 @@ static void born_source_q(Engine* e, const PointList& src, StepArgs a) {
     const int kind = e->kind;
     if (kind == 1) e->kind = 0;
     zero_wavefields(e);
-    float* p0[5]; float* p1[5];
-    for (int f = 0; f < 5; f++) { p0[f] = e->wf[f].f(); p1[f] = e->wf[5 + f].f(); }
+    Levels L(e);
     int cur = 0;
     a.inj = upload_points(e, src, e->inj_ts, e->inj_ent, e->sig_in);
+    const SparseOp injh = halo_sources(e, kind == 5, src.pos, src.npos, e->sig_in);
     memset(&a.ext, 0, sizeof(a.ext));
     a.W0 = e->wstage.f();
     a.W1 = e->wstage.f() + e->n;
@@ -842,10 +1012,23 @@ static void born_source_q(Engine* e, const PointList& src, StepArgs a) {
     const int h = e->h;
     const int npart = e->ntiles * 16;
     try {
-        for (int its = 0; its < e->nts - 1; its++)
+        for (int its = 0; its < e->nts - 1; its++) {
+            if (kind == 5 && its < e->nts - 2) {
+                // (its, 1) samples row its, (its, 2) only steps; the staging rows
+                // are quantized after the pair
+                StepArgs a0 = a, a1 = a;
+                a0.inj.t0 = 2 * its; a0.inj.w0 = 1.f; a0.inj.w1 = 0.f;
+                a0.tmode = 1; a0.wt = 0; a0.tw_o = F[h + 1]; a0.tw_c = F[h + 2]; a0.tw_n = F[1];
+                a0.pmax = e->wpmax.f() + (size_t)(its & 1) * 2 * npart;
+                a1.inj.t0 = 2 * its + 1; a1.inj.w0 = 1.f; a1.inj.w1 = 0.f;
+                a1.tmode = 0; a1.pmax = nullptr;
+                run_pair<0, EPI_TRI>(e, a0, a1, injh, L);
+                quantize_row(e, its);
+                continue;
+            }
             for (int it2 = 1; it2 < e->S + 1; it2++) {
                 const int itw = its * e->S + it2;
-                for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; }
+                L.set(a);
                 a.inj.t0 = itw - 1; a.inj.w0 = 1.f; a.inj.w1 = 0.f;
                 const bool last = (its == e->nts - 2 && it2 == 2);
                 int row = -1;
@@ -861,9 +1044,10 @@ static void born_source_q(Engine* e, const PointList& src, StepArgs a) {
                 } else {
                     launch_step<0, EPI_NONE>(e, a, cur);
                 }
-                std::swap(p0, p1);
+                L.single();
                 cur ^= 1;
             }
+        }
     } catch (...) {
         e->kind = kind;
         throw;
@@ -886,19 +1070,30 @@ static void born_source(Engine* e, const PointList& src, StepArgs a) {
     if (!tri || fresh || !e->w_clean) EIO_CUDA(cudaMemsetAsync(e->W.p, 0, wbytes, e->st));
     e->w_clean = tri;
     zero_wavefields(e);
-    float* p0[5]; float* p1[5];
-    for (int f = 0; f < 5; f++) { p0[f] = e->wf[f].f(); p1[f] = e->wf[5 + f].f(); }
+    Levels L(e);
     int cur = 0;
+    const bool use_pair = tri && e->kind == 5;
     a.inj = upload_points(e, src, e->inj_ts, e->inj_ent, e->sig_in);
+    const SparseOp injh = halo_sources(e, use_pair, src.pos, src.npos, e->sig_in);
     memset(&a.ext, 0, sizeof(a.ext));
     a.W0 = e->W.f();
     a.W1 = e->W.f() + (long long)e->nts * e->n;
     const float* F = e->filt.data();
     const int h = e->h;
-    for (int its = 0; its < e->nts - 1; its++)
+    for (int its = 0; its < e->nts - 1; its++) {
+        if (use_pair && its < e->nts - 2) {
+            // (its, 1) writes row its, (its, 2) only steps
+            StepArgs a0 = a, a1 = a;
+            a0.inj.t0 = 2 * its; a0.inj.w0 = 1.f; a0.inj.w1 = 0.f;
+            a0.tmode = 1; a0.wt = its; a0.tw_o = F[h + 1]; a0.tw_c = F[h + 2]; a0.tw_n = F[1];
+            a1.inj.t0 = 2 * its + 1; a1.inj.w0 = 1.f; a1.inj.w1 = 0.f;
+            a1.tmode = 0;
+            run_pair<0, EPI_TRI>(e, a0, a1, injh, L);
+            continue;
+        }
         for (int it2 = 1; it2 < e->S + 1; it2++) {
             const int itw = its * e->S + it2;
-            for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; }
+            L.set(a);
             a.inj.t0 = itw - 1; a.inj.w0 = 1.f; a.inj.w1 = 0.f;
             if (tri) {
                 const bool last = (its == e->nts - 2 && it2 == 2);
@@ -915,9 +1110,10 @@ static void born_source(Engine* e, const PointList& src, StepArgs a) {
                 a.wt = its; a.ww0 = F[it2]; a.ww1 = F[h + it2];
                 launch_step<0, EPI_SAVE_W>(e, a, cur);
             }
-            std::swap(p0, p1);
+            L.single();
             cur ^= 1;
         }
+    }
     check_launch();
 }
 
@@ -952,12 +1148,11 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
         EIO_CUDA(cudaEventRecord(e->ev_free[k], e->st2));
         EIO_CUDA(cudaEventRecord(e->ev_ready[k], e->st2));
     }
-    float* p0[5]; float* p1[5]; float* sL[5]; float* sR[5];
-    for (int f = 0; f < 5; f++) {
-        p0[f] = e->wf[f].f(); p1[f] = e->wf[5 + f].f();
-        sL[f] = e->ss[f].f(); sR[f] = e->ss[5 + f].f();
-    }
+    float* sL[5]; float* sR[5];
+    for (int f = 0; f < 5; f++) { sL[f] = e->ss[f].f(); sR[f] = e->ss[5 + f].f(); }
+    Levels L(e);
     int cur = 0;
+    const bool use_pair = e->kind == 5;
     StepArgs a = base;
     if (!adj) {
         zero_out(e, rec.ld, e->nts, e->sig_out);
@@ -977,13 +1172,26 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
             const int l = its % R, r = (its + 1) % R;
             EIO_CUDA(cudaStreamWaitEvent(e->st, e->ev_ready[l], 0));
             EIO_CUDA(cudaStreamWaitEvent(e->st, e->ev_ready[r], 0));
-            for (int it2 = 1; it2 < e->S + 1; it2++) {
-                for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; a.ssL[f] = ring[l][f]; a.ssR[f] = ring[r][f]; }
-                a.sw0 = F[it2 - 1]; a.sw1 = F[h + it2 - 1];
-                a.ext.t0 = its; a.ext.w0 = F[it2]; a.ext.w1 = F[h + it2];
+            for (int f = 0; f < 5; f++) { a.ssL[f] = ring[l][f]; a.ssR[f] = ring[r][f]; }
+            auto weights = [&](StepArgs& x, int it2) {
+                x.sw0 = F[it2 - 1]; x.sw1 = F[h + it2 - 1];
+                x.ext.t0 = its; x.ext.w0 = F[it2]; x.ext.w1 = F[h + it2];
+            };
+            for (int it2 = 1; it2 < e->S + 1;) {
+                if (use_pair && it2 + 1 < e->S + 1) {
+                    StepArgs a0 = a, a1 = a;
+                    weights(a0, it2);
+                    weights(a1, it2 + 1);
+                    run_pair<0, EPI_INJ_SS>(e, a0, a1, a.inj, L);   // no sparse sources
+                    it2 += 2;
+                    continue;
+                }
+                L.set(a);
+                weights(a, it2);
                 launch_step<0, EPI_INJ_SS>(e, a, cur);
-                std::swap(p0, p1);
+                L.single();
                 cur ^= 1;
+                it2++;
             }
             // the imaging kernel rewrites every interior cell of a slot, so the
             // reference's memset of the right slice (BornElasticGpuFunctions.cu:806-810) is not needed
@@ -1001,27 +1209,51 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
         // writes it once (EPI_TRI) and the imaging condition of T follows on the imaging stream.
         stage_in(e, data, rec.ld, e->nts, e->sig_in);
         a.inj = upload_points(e, rec, e->inj_ts, e->inj_ent, e->sig_in);
+        const SparseOp injh = halo_sources(e, use_pair, g.recPos, g.nRec, e->sig_in);
         // sample T goes to slot T % R; its imaging runs on the imaging stream
         // while the adjoint keeps stepping; the slot is rewritten R samples later
-        auto extract = [&](int T, int mode, float wo, float wc, float wn) {
+        auto imaging = [&](int T) {
             const int sl = T % R;
-            EIO_CUDA(cudaStreamWaitEvent(e->st, e->ev_free[sl], 0));
-            for (int f = 0; f < 5; f++) a.eL[f] = ring[sl][f];
-            a.tmode = mode; a.tw_o = wo; a.tw_c = wc; a.tw_n = wn;
-            launch_step<1, EPI_TRI>(e, a, cur);
             EIO_CUDA(cudaEventRecord(e->ev_ready[sl], e->st));
             EIO_CUDA(cudaStreamWaitEvent(e->st2, e->ev_ready[sl], 0));
             launch_imaging(e, 1, T, dm, ring[sl], e->st2);
             EIO_CUDA(cudaEventRecord(e->ev_free[sl], e->st2));
         };
+        auto tri = [&](StepArgs& x, int T, int mode, float wo, float wc, float wn) {
+            EIO_CUDA(cudaStreamWaitEvent(e->st, e->ev_free[T % R], 0));
+            for (int f = 0; f < 5; f++) x.eL[f] = ring[T % R][f];
+            x.tmode = mode; x.tw_o = wo; x.tw_c = wc; x.tw_n = wn;
+        };
+        auto weights = [&](StepArgs& x, int its, int it2) {
+            x.inj.t0 = its; x.inj.w0 = F[it2 + 1]; x.inj.w1 = F[h + it2 + 1];
+        };
         for (int its = e->nts - 2; its > -1; its--) {
+            if (use_pair && its > 0) {
+                // (its, 1) writes sample its+1, (its, 0) only steps
+                StepArgs a0 = a, a1 = a;
+                weights(a0, its, 1);
+                tri(a0, its + 1, 1, F[1], F[0], F[h + 1]);
+                weights(a1, its, 0);
+                a1.tmode = 0;
+                run_pair<1, EPI_TRI>(e, a0, a1, injh, L);
+                imaging(its + 1);
+                continue;
+            }
             for (int it2 = e->S - 1; it2 > -1; it2--) {
-                for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; }
-                a.inj.t0 = its; a.inj.w0 = F[it2 + 1]; a.inj.w1 = F[h + it2 + 1];
-                if (it2 == 1) extract(its + 1, 1, F[1], F[0], F[h + 1]);
-                else if (its == 0) extract(0, 2, 0.f, F[1], F[0]);   // sample 0 = p(1) f[1] + p(0) f[0]
-                else launch_step<1, EPI_NONE>(e, a, cur);
-                std::swap(p0, p1);
+                L.set(a);
+                weights(a, its, it2);
+                if (it2 == 1) {
+                    tri(a, its + 1, 1, F[1], F[0], F[h + 1]);
+                    launch_step<1, EPI_TRI>(e, a, cur);
+                    imaging(its + 1);
+                } else if (its == 0) {   // sample 0 = p(1) f[1] + p(0) f[0]
+                    tri(a, 0, 2, 0.f, F[1], F[0]);
+                    launch_step<1, EPI_TRI>(e, a, cur);
+                    imaging(0);
+                } else {
+                    launch_step<1, EPI_NONE>(e, a, cur);
+                }
+                L.single();
                 cur ^= 1;
             }
         }
@@ -1033,11 +1265,12 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
         a.inj = upload_points(e, rec, e->inj_ts, e->inj_ent, e->sig_in);
         for (int its = e->nts - 2; its > -1; its--) {
             for (int it2 = e->S - 1; it2 > -1; it2--) {
-                for (int f = 0; f < 5; f++) { a.o[f] = p0[f]; a.c[f] = p1[f]; a.eL[f] = sL[f]; a.eR[f] = sR[f]; }
+                L.set(a);
+                for (int f = 0; f < 5; f++) { a.eL[f] = sL[f]; a.eR[f] = sR[f]; }
                 a.inj.t0 = its; a.inj.w0 = F[it2 + 1]; a.inj.w1 = F[h + it2 + 1];
                 a.sw0 = F[it2]; a.sw1 = F[h + it2];
                 launch_step<1, EPI_EXT_SS>(e, a, cur);
-                std::swap(p0, p1);
+                L.single();
                 cur ^= 1;
             }
             launch_imaging(e, 1, its + 1, dm, sR, e->st);

@@ -546,7 +546,13 @@ EIO_API int eio_ctx_stats(eio_ctx* c, int enable, int reset, long long* launches
                           double* stepMs) {
     return guarded([&] {
         if (!c) throw Error(EIO_ERR_ARG, "null context");
-        engine_stats(c->eng, enable, reset, launches, stepLaunches, stepMs);
+        engine_stats(c->eng, enable, reset, launches, stepLaunches, stepMs, nullptr, nullptr);
+    });
+}
+EIO_API int eio_ctx_pair_stats(eio_ctx* c, long long* pairLaunches, double* pairMs) {
+    return guarded([&] {
+        if (!c) throw Error(EIO_ERR_ARG, "null context");
+        engine_stats(c->eng, -1, 0, nullptr, nullptr, nullptr, pairLaunches, pairMs);
     });
 }
 

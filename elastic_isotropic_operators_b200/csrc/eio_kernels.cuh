@@ -159,9 +159,11 @@ __device__ __forceinline__ float4 dpx(const float4* q, int m, const float* c)
 }
 
 // Load the 12-value z window for local column lx starting at local z lz (multiple of 4)
+// of a staged field with RZ floats per column
+template <int RZ = SZ>
 __device__ __forceinline__ void zwin(const float* s, int lx, int lz, float* w)
 {
-    const float* p = s + lx * SZ + lz - FAT;
+    const float* p = s + lx * RZ + lz - FAT;
     float4 a = ld4(p), b = ld4(p + 4), c = ld4(p + 8);
     w[0] = a.x; w[1] = a.y; w[2] = a.z; w[3] = a.w;
     w[4] = b.x; w[5] = b.y; w[6] = b.z; w[7] = b.w;
@@ -175,38 +177,38 @@ __device__ __forceinline__ void xwin(const float* s, int lx0, int lz, float4* q)
 }
 
 // Stencil part of one fused fine step for the float4 at local (lx, lz) of a
-// staged tile (5 fields [SX][SZ] at stride SMEM_FIELD): forward, the current
-// level and the medium at the cell from par(k); adjoint, the staged scaled
-// combinations.  t[f] receives the update of fields F0 <= f < F1 before the
-// old level is added; the field groups {vx, vz} and {sxx, szz, sxz} need four
-// derivatives each.
-template <int DIR, int F0, int F1, class Par>
+// staged tile (5 fields [..][RZ] at stride FSTR, by default [SX][SZ] at
+// SMEM_FIELD): forward, the current level and the medium at the cell from
+// par(k); adjoint, the staged scaled combinations.  t[f] receives the update
+// of fields F0 <= f < F1 before the old level is added; the field groups
+// {vx, vz} and {sxx, szz, sxz} need four derivatives each.
+template <int DIR, int F0, int F1, class Par, int RZ = SZ, int FSTR = SMEM_FIELD>
 __device__ __forceinline__ void stencil_fields(const float* sm, int lx, int lz, const float* cz, const float* cx,
                                                bool valid, Par par, float4 (&t)[5])
 {
     static_assert((F0 == 0 && F1 == 5) || (F0 == 0 && F1 == 2) || (F0 == 2 && F1 == 5), "field group");
     const float* s0 = sm;
-    const float* s1 = sm + SMEM_FIELD;
-    const float* s2 = sm + 2 * SMEM_FIELD;
-    const float* s3 = sm + 3 * SMEM_FIELD;
-    const float* s4 = sm + 4 * SMEM_FIELD;
+    const float* s1 = sm + FSTR;
+    const float* s2 = sm + 2 * FSTR;
+    const float* s3 = sm + 3 * FSTR;
+    const float* s4 = sm + 4 * FSTR;
     float4 q[9];
     float w[12];
     auto xw = [&](const float* sf) {
 #pragma unroll
-        for (int m = 0; m < 9; m++) q[m] = ld4(sf + (lx - FAT + m) * SZ + lz);
+        for (int m = 0; m < 9; m++) q[m] = ld4(sf + (lx - FAT + m) * RZ + lz);
     };
     if (DIR == 0) {
         // s0 vx, s1 vz, s2 sxx, s3 szz, s4 sxz; one output field at a time keeps few registers live
         if (F0 == 0) {
             xw(s2); float4 dx = dmx(q, 4, cx);
-            zwin(s4, lx, lz, w); float4 dz = dpz(w, cz);
+            zwin<RZ>(s4, lx, lz, w); float4 dz = dpz(w, cz);
             if (valid) {
                 const float4 rx = par(0);
 #pragma unroll
                 for (int j = 0; j < 4; j++) at(t[0], j) = at(rx, j) * (at(dx, j) + at(dz, j));
             }
-            zwin(s3, lx, lz, w); dz = dmz(w, cz);
+            zwin<RZ>(s3, lx, lz, w); dz = dmz(w, cz);
             xw(s4); dx = dpx(q, 4, cx);
             if (valid) {
                 const float4 rz = par(1);
@@ -216,7 +218,7 @@ __device__ __forceinline__ void stencil_fields(const float* sm, int lx, int lz, 
         }
         if (F1 == 5) {
             xw(s0); float4 dx = dpx(q, 4, cx);
-            zwin(s1, lx, lz, w); float4 dz = dpz(w, cz);
+            zwin<RZ>(s1, lx, lz, w); float4 dz = dpz(w, cz);
             if (valid) {
                 const float4 l2m = par(2), lam = par(3);
 #pragma unroll
@@ -225,7 +227,7 @@ __device__ __forceinline__ void stencil_fields(const float* sm, int lx, int lz, 
                     at(t[3], j) = at(lam, j) * at(dx, j) + at(l2m, j) * at(dz, j);
                 }
             }
-            zwin(s0, lx, lz, w); dz = dmz(w, cz);
+            zwin<RZ>(s0, lx, lz, w); dz = dmz(w, cz);
             xw(s1); dx = dmx(q, 4, cx);
             if (valid) {
                 const float4 mu = par(4);
@@ -237,10 +239,10 @@ __device__ __forceinline__ void stencil_fields(const float* sm, int lx, int lz, 
         // s0 A=l2m*sxx+lam*szz, s1 B=lam*sxx+l2m*szz, s2 M=mu*sxz, s3 P=rhox*vx, s4 Q=rhoz*vz
         if (F0 == 0) {
             xw(s0); float4 dx = dmx(q, 4, cx);
-            zwin(s2, lx, lz, w); float4 dz = dpz(w, cz);
+            zwin<RZ>(s2, lx, lz, w); float4 dz = dpz(w, cz);
 #pragma unroll
             for (int j = 0; j < 4; j++) at(t[0], j) = -(at(dx, j) + at(dz, j));
-            zwin(s1, lx, lz, w); dz = dmz(w, cz);
+            zwin<RZ>(s1, lx, lz, w); dz = dmz(w, cz);
             xw(s2); dx = dpx(q, 4, cx);
 #pragma unroll
             for (int j = 0; j < 4; j++) at(t[1], j) = -(at(dz, j) + at(dx, j));
@@ -249,10 +251,10 @@ __device__ __forceinline__ void stencil_fields(const float* sm, int lx, int lz, 
             xw(s3); float4 dx = dpx(q, 4, cx);
 #pragma unroll
             for (int j = 0; j < 4; j++) at(t[2], j) = -at(dx, j);
-            zwin(s4, lx, lz, w); float4 dz = dpz(w, cz);
+            zwin<RZ>(s4, lx, lz, w); float4 dz = dpz(w, cz);
 #pragma unroll
             for (int j = 0; j < 4; j++) at(t[3], j) = -at(dz, j);
-            zwin(s3, lx, lz, w); dz = dmz(w, cz);
+            zwin<RZ>(s3, lx, lz, w); dz = dmz(w, cz);
             xw(s4); dx = dmx(q, 4, cx);
 #pragma unroll
             for (int j = 0; j < 4; j++) at(t[4], j) = -(at(dz, j) + at(dx, j));
@@ -429,7 +431,7 @@ __device__ __forceinline__ void step_tail(const StepArgs& a, float* scratch, int
             } else {
 #pragma unroll
                 for (int f = F0; f < F1; f++)
-                    st4(a.eL[f] + gi, tri_sample(a.tmode, osave[f], ldg4(a.c[f] + gi), t[f], a.tw_o, a.tw_c, a.tw_n));
+                    st4(a.eL[f] + gi, tri_sample(a.tmode, osave[f], ld4(a.c[f] + gi), t[f], a.tw_o, a.tw_c, a.tw_n));
             }
         }
     }

@@ -140,8 +140,13 @@ void *eio_ctx_stream(eio_ctx *c);
 /* Step-kernel selection (no reference counterpart; the reference has one
  * 16x16-tile kernel).  kind 0: shared-memory tile kernel; kind 1: TMA-pipelined
  * x-sweep with strip height tz (64 or 128), chunk width cw (8 or 16) and cpr
- * chunks per CTA.  By default the first propagation of a context times every
- * candidate on its grid (eio_ctx_autotune) and keeps the fastest. */
+ * chunks per CTA; kind 2: persistent TMA tile kernel; kind 3: tile kernel at
+ * 4 CTAs per SM; kind 4: two threads per float4; kind 5: two fine steps per
+ * launch (the tile widened by the stencil radius, four wavefield levels), kind 3
+ * for the steps that run alone (free surface, saved wavefields, the last
+ * coarse interval of a Born source wavefield, running-sum epilogues).  By
+ * default the first propagation of a context times every candidate on its
+ * grid (eio_ctx_autotune) and keeps the fastest. */
 int eio_ctx_set_kernel(eio_ctx *c, int kind, int tz, int cw, int cpr);
 int eio_ctx_get_kernel(const eio_ctx *c, int *kind, int *tz, int *cw, int *cpr);
 int eio_ctx_autotune(eio_ctx *c, int *kind, int *tz, int *cw, int *cpr);
@@ -151,6 +156,11 @@ int eio_ctx_autotune(eio_ctx *c, int *kind, int *tz, int *cw, int *cpr);
  * enable: 1 on, 0 off, -1 unchanged; reset: zero the counters after reading. */
 int eio_ctx_stats(eio_ctx *c, int enable, int reset, long long *launches, long long *stepLaunches,
                   double *stepMs);
+/* The two-step launches (kind 5) alone, since the last reset: their count and
+ * their sampled mean duration times that count (no reference counterpart).
+ * They are also included in stepLaunches / stepMs of eio_ctx_stats; read this
+ * before an eio_ctx_stats call that resets. */
+int eio_ctx_pair_stats(eio_ctx *c, long long *pairLaunches, double *pairMs);
 
 /* ---------------------------------------------------------------------------
  * Single-shot propagation on the regular grid

@@ -204,7 +204,7 @@ def test_out_of_interior_point_rejected(w, ctx):
 
 
 # ------------------------------------------------------------------ every step-kernel variant
-KERNELS = [(0, 64, 16, 0), (2, 64, 16, 0), (3, 64, 16, 0), (4, 64, 16, 0), (1, 64, 8, 4), (1, 64, 8, 5), (1, 64, 16, 2), (1, 64, 16, 1), (1, 128, 8, 3)]
+KERNELS = [(0, 64, 16, 0), (2, 64, 16, 0), (3, 64, 16, 0), (4, 64, 16, 0), (5, 64, 16, 0), (1, 64, 8, 4), (1, 64, 8, 5), (1, 64, 16, 2), (1, 64, 16, 1), (1, 128, 8, 3)]
 
 
 @pytest.mark.parametrize("cfg", KERNELS, ids=lambda c: "k%d_tz%d_cw%d_cpr%d" % c)
@@ -232,7 +232,7 @@ def test_autotune_picks_a_valid_kernel(w):
     c = Ctx(w)
     try:
         kind, tz, cw, cpr = c.autotune()
-        assert kind in (0, 1, 2, 3, 4)
+        assert kind in (0, 1, 2, 3, 4, 5)
         if kind == 1:
             assert tz in (64, 128) and cw in (8, 16) and cpr >= 1
         with pytest.raises(prop.EioError):
@@ -310,7 +310,7 @@ def _nl_born_vs_oracle(c, w, seed):
         assert rel(pm if adj else pd, m if adj else d) < TOL32, ("nl", adj)
 
 
-@pytest.mark.parametrize("kind", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("kind", [0, 1, 2, 3, 4, 5])
 def test_ragged_tiles_vs_oracle(kind):
     """A grid whose interior (96 x 112) leaves a half-height last tile row, so the
     TMA boxes reach past the grid edge and read the zero fill."""
@@ -323,7 +323,7 @@ def test_ragged_tiles_vs_oracle(kind):
         c.close()
 
 
-@pytest.mark.parametrize("kind", [None, 0, 2, 3, 4])
+@pytest.mark.parametrize("kind", [None, 0, 2, 3, 4, 5])
 def test_sub2_running_sum_path_vs_oracle(kind):
     """sub = 2 (four fine steps per coarse sample) keeps the running-sum history
     and adjoint accumulation; sub = 1 (every other test) takes the single-write path."""
