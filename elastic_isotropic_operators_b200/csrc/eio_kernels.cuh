@@ -540,6 +540,36 @@ __device__ __forceinline__ void stage_tile(const StepArgs& a, float* sm, int z0,
 {
     const int nz = a.nz;
     const int nq = SZ / 4;                        // float4 per shared column
+    if (DIR == 0 && !FS && NTHR == NT) {
+        // forward: every load of the thread in flight before the first store
+        constexpr int NU = (SZ / 4) * SX;
+        constexpr int R = (NU + NT - 1) / NT;
+        float4 v[R][5];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int q = tid + r * NT;
+            const int lx = q / nq, lz4 = (q % nq) * 4;
+            const int gz = z0 - FAT + lz4, gx = x0 - FAT + lx;
+            if (q < NU && gz < nz) {
+                const long long gi = (long long)gx * nz + gz;
+#pragma unroll
+                for (int f = 0; f < 5; f++) v[r][f] = ldg4(a.c[f] + gi);
+            } else {
+#pragma unroll
+                for (int f = 0; f < 5; f++) v[r][f] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int q = tid + r * NT;
+            if (q < NU) {
+                const int lx = q / nq, lz4 = (q % nq) * 4;
+#pragma unroll
+                for (int f = 0; f < 5; f++) st4(sm + f * SMEM_FIELD + lx * SZ + lz4, v[r][f]);
+            }
+        }
+        return;
+    }
     for (int q = tid; q < nq * SX; q += NTHR) {
         const int lx = q / nq, lz4 = (q % nq) * 4;
         const int gz = z0 - FAT + lz4, gx = x0 - FAT + lx;
@@ -603,6 +633,14 @@ __global__ void __launch_bounds__(NT, MINB) k_step(StepArgs a)
 
     pdl_begin(a, gi, valid);
     stage_tile<DIR, NT, FS>(a, sm, z0, x0, tid);
+    // with 3 CTAs per SM the old level is loaded here, its latency hidden
+    // behind the barrier and the stencils
+    constexpr bool HOIST = MINB == 3 && !FS;
+    float4 oreg[5];
+    if (HOIST) {
+#pragma unroll
+        for (int f = 0; f < 5; f++) oreg[f] = valid ? ld4(a.o[f] + gi) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
     __syncthreads();
 
     float4 t[5];                               // new values before the final taper
@@ -615,7 +653,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step(StepArgs a)
         csave[0] = ld4(sm + lx * SZ + lz);
         csave[1] = ld4(sm + SMEM_FIELD + lx * SZ + lz);
     }
-    auto old = [&](int f) { return ld4(a.o[f] + gi); };
+    auto old = [&](int f) { return HOIST ? oreg[f] : ld4(a.o[f] + gi); };
     step_tail<DIR, EPI, 0, 5, NT, decltype(old), FS>(a, sm, tile, tid, tzi, txi, gz, gx, valid, gi, t, old, csave);
 }
 
