@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--nts", type=int, default=4000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--graphs", action="store_true", help="run the time loops as CUDA graphs (off by default)")
     ap.add_argument("--kernel", type=int, default=-1, choices=[-1, 0, 1, 2, 3, 4, 5],
                     help="-1: autotune (default); 0: tile kernel k_step; 1: TMA sweep kernel k_sweep; "
                          "2: persistent TMA tile kernel k_tile; 3: k_step at 4 CTAs/SM; 4: split-field k_split; "
@@ -132,10 +133,13 @@ def profile_traffic(bytes_per_cell=BYTES_PER_CELL):
 
 
 def pin_kernel(L, ctx, args):
-    """--kernel 0/1 fixes the step kernel (profiling runs); -1 keeps the autotuner."""
+    """--kernel k fixes the step kernel (profiling runs); -1 keeps the autotuner.
+    --graphs runs the time loops as CUDA graphs."""
     from elastic_isotropic_operators_b200 import _lib
     if args.kernel >= 0:
         _lib.check(L.eio_ctx_set_kernel(ctx, args.kernel, 64, 8, 8))
+    if args.graphs:
+        _lib.check(L.eio_ctx_set_graphs(ctx, 1))
 
 
 def kernel_name(L, ctx):

@@ -130,25 +130,77 @@ struct Engine {
     std::vector<cudaEvent_t> ev;
     std::vector<unsigned char> ev_pair;   // per event pair: 1 = a two-step launch
     size_t ev_used = 0;
+    // CUDA graphs of the time loops, one per distinct launch signature (key)
+    struct Graph {
+        uint64_t key = 0;
+        cudaGraphExec_t exec = nullptr;
+        // what one replay adds to the counters
+        long long launches = 0, step_launches = 0, sampled = 0, pair_launches = 0, pair_sampled = 0;
+        std::vector<cudaEvent_t> ev;          // timing events its event-record nodes write
+        std::vector<unsigned char> ev_pair;
+        size_t nev = 0;
+        bool pending = false;                 // replayed since its events were last read
+        unsigned long long used = 0;
+    };
+    std::vector<Graph*> graphs;
+    Graph* cap = nullptr;                     // graph being captured
+    bool use_graphs = false;  // measured slower than PDL stream launches on B200: opt-in
+    unsigned long long graph_clock = 0;
 };
+
+static void graph_free(Engine::Graph* g);
 
 // CUDA-event timing of every STATS_PERIOD-th launch of the fused step kernel
 // (only when enabled); sampling keeps the event records out of most gaps.
 constexpr long long STATS_PERIOD = 16;
+// the two-step kernels need more than 48 KB of dynamic shared memory
+static void open_pair_smem() {
+    EIO_CUDA(cudaFuncSetAttribute(k_pair<0, EPI_NONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, PAIR_SMEM));
+    EIO_CUDA(cudaFuncSetAttribute(k_pair<1, EPI_NONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, PAIR_SMEM));
+    EIO_CUDA(cudaFuncSetAttribute(k_pair<0, EPI_TRI>, cudaFuncAttributeMaxDynamicSharedMemorySize, PAIR_SMEM));
+    EIO_CUDA(cudaFuncSetAttribute(k_pair<1, EPI_TRI>, cudaFuncAttributeMaxDynamicSharedMemorySize, PAIR_SMEM));
+    EIO_CUDA(cudaFuncSetAttribute(k_pair<0, EPI_INJ_SS>, cudaFuncAttributeMaxDynamicSharedMemorySize, PAIR_SMEM));
+}
+
 static void stats_flush(Engine* e) {
-    if (!e->stats || e->ev_used == 0) return;
-    EIO_CUDA(cudaStreamSynchronize(e->st));
-    for (size_t k = 0; k + 1 < e->ev_used; k += 2) {
-        float ms = 0.f;
-        EIO_CUDA(cudaEventElapsedTime(&ms, e->ev[k], e->ev[k + 1]));
-        if (e->ev_pair[k / 2]) e->pair_ms += ms;
-        else e->step_ms += ms;
+    bool pending = false;
+    for (const Engine::Graph* g : e->graphs) pending = pending || g->pending;
+    if (e->ev_used == 0 && !pending) return;
+    if (!e->stats) {   // timing was switched off: drop what was recorded
+        e->ev_used = 0;
+        for (Engine::Graph* g : e->graphs) g->pending = false;
+        return;
     }
+    EIO_CUDA(cudaStreamSynchronize(e->st));
+    auto read = [&](const std::vector<cudaEvent_t>& ev, const std::vector<unsigned char>& is_pair, size_t n) {
+        for (size_t k = 0; k + 1 < n; k += 2) {
+            float ms = 0.f;
+            EIO_CUDA(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+            if (is_pair[k / 2]) e->pair_ms += ms;
+            else e->step_ms += ms;
+        }
+    };
+    read(e->ev, e->ev_pair, e->ev_used);
     e->ev_used = 0;
+    for (Engine::Graph* g : e->graphs)
+        if (g->pending) {
+            read(g->ev, g->ev_pair, g->nev);
+            g->pending = false;
+        }
 }
 // pair: the launch the mark opens (or closes) is a two-step launch
 static void stats_mark(Engine* e, bool pair = false) {
     if (!e->stats) return;
+    if (e->cap) {   // capturing: the graph's own events (created before the capture)
+        Engine::Graph* g = e->cap;
+        if (g->nev < g->ev.size()) {
+            g->ev_pair[g->nev / 2] = pair ? 1 : 0;
+            // external: an event-record node that records the event at every replay (a plain
+            // record inside a capture only orders the captured work)
+            EIO_CUDA(cudaEventRecordWithFlags(g->ev[g->nev++], e->st, cudaEventRecordExternal));
+        }
+        return;
+    }
     if (e->ev_used == e->ev.size()) {
         if (e->ev.size() >= 65536) stats_flush(e);
         else {
@@ -237,6 +289,7 @@ Engine* engine_create(int device, const FdParam& fd) {
             EIO_CUDA(cudaEventCreateWithFlags(&e->ev_free[k], cudaEventDisableTiming));
         }
         EIO_CUDA(cudaEventCreateWithFlags(&e->ev_sync, cudaEventDisableTiming));
+        open_pair_smem();
         for (int f = 0; f < 20; f++) {
             e->wf[f].ensure(sizeof(float) * e->n);
             EIO_CUDA(cudaMemsetAsync(e->wf[f].p, 0, sizeof(float) * e->n, e->st));
@@ -269,6 +322,8 @@ void engine_destroy(Engine* e) {
     for (int f = 0; f < 20; f++) e->wf[f].release();
     for (int f = 0; f < 20; f++) e->ss[f].release();
     for (cudaEvent_t x : e->ev) cudaEventDestroy(x);
+    for (Engine::Graph* g : e->graphs) graph_free(g);
+    e->graphs.clear();
     for (int k = 0; k < 4; k++) {
         if (e->ev_ready[k]) cudaEventDestroy(e->ev_ready[k]);
         if (e->ev_free[k]) cudaEventDestroy(e->ev_free[k]);
@@ -604,15 +659,10 @@ static void launch_step(Engine* e, StepArgs& a, int cur) {
 }
 
 // two fine steps in one launch (kind 5); the dynamic shared memory of each
-// instantiation is opened once per device
+// instantiation is opened when the context is created (open_pair_smem)
 template <int DIR, int EPI>
 static void launch_pair(Engine* e, const PairArgs& p) {
     static_assert(sizeof(PairArgs) <= 4096, "kernel parameter block");
-    static unsigned char opened[64] = {};
-    if (e->device < 64 && !opened[e->device]) {
-        EIO_CUDA(cudaFuncSetAttribute(k_pair<DIR, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, PAIR_SMEM));
-        opened[e->device] = 1;
-    }
     const bool timed = e->stats && (e->step_launches + e->pair_launches) % STATS_PERIOD == 0;
     if (timed) stats_mark(e, true);
     cudaLaunchConfig_t cfg;
@@ -670,6 +720,131 @@ static void run_pair(Engine* e, StepArgs a0, StepArgs a1, const SparseOp& injh, 
     L.pair();
 }
 
+// ---------------------------------------------------------------- CUDA graphs
+// FNV-1a over the values that fix a time loop's launch sequence (kernel
+// arguments, buffer addresses, step counts, the kernel choice)
+struct LoopKey {
+    uint64_t h = 1469598103934665603ull;
+    void add(const void* p, size_t n) {
+        const unsigned char* b = static_cast<const unsigned char*>(p);
+        for (size_t i = 0; i < n; i++) { h ^= b[i]; h *= 1099511628211ull; }
+    }
+    template <class T> LoopKey& operator<<(const T& v) { add(&v, sizeof(v)); return *this; }
+};
+
+static LoopKey loop_key(const Engine* e, int loop) {
+    LoopKey k;
+    k << loop << e->kind << e->tz << e->cw << e->cpr << e->fs_active << e->nts << e->S << e->ckpt << e->stats;
+    k.add(e->filt.data(), sizeof(float) * e->filt.size());
+    for (int f = 0; f < 20; f++) k << e->wf[f].p;
+    return k;
+}
+
+static void graph_free(Engine::Graph* g) {
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    for (cudaEvent_t x : g->ev) cudaEventDestroy(x);
+    delete g;
+}
+
+constexpr size_t MAX_GRAPHS = 8;
+
+// Run one time loop (body issues its launches on e->st, and on e->st2 after
+// joining it through an event) as a CUDA graph: captured the first time its key
+// is seen, replayed afterwards.  max_steps bounds the step launches (sizes the
+// graph's timing events).  Falls back to direct launches if capture fails.
+template <class Body>
+static void run_graph(Engine* e, uint64_t key, long long max_steps, Body&& body) {
+    if (!e->use_graphs) {
+        body();
+        return;
+    }
+    Engine::Graph* g = nullptr;
+    for (Engine::Graph* x : e->graphs)
+        if (x->key == key) g = x;
+    if (!g) {
+        g = new Engine::Graph();
+        g->key = key;
+        try {
+            if (e->stats) {
+                const size_t nev = 2 * (size_t)(max_steps / STATS_PERIOD + 2);
+                for (size_t i = 0; i < nev; i++) {
+                    cudaEvent_t x;
+                    EIO_CUDA(cudaEventCreate(&x));
+                    g->ev.push_back(x);
+                }
+                g->ev_pair.assign(nev / 2, 0);
+            }
+        } catch (...) {
+            graph_free(g);
+            throw;
+        }
+        const long long l0 = e->launches, s0 = e->step_launches, m0 = e->sampled, p0 = e->pair_launches,
+                        q0 = e->pair_sampled;
+        cudaError_t err = cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal);
+        if (err == cudaSuccess) {
+            e->cap = g;
+            bool failed = false;
+            try {
+                body();
+            } catch (const Error& x) {
+                if (x.code != EIO_ERR_CUDA) {
+                    e->cap = nullptr;
+                    cudaGraph_t gr = nullptr;
+                    cudaStreamEndCapture(e->st, &gr);
+                    if (gr) cudaGraphDestroy(gr);
+                    e->launches = l0; e->step_launches = s0; e->sampled = m0; e->pair_launches = p0;
+                    e->pair_sampled = q0;
+                    graph_free(g);
+                    throw;
+                }
+                failed = true;   // a call the capture does not take: direct launches below
+            }
+            if (failed) {
+                e->cap = nullptr;
+                cudaGraph_t gr = nullptr;
+                cudaStreamEndCapture(e->st, &gr);
+                if (gr) cudaGraphDestroy(gr);
+                cudaGetLastError();
+                e->launches = l0; e->step_launches = s0; e->sampled = m0; e->pair_launches = p0; e->pair_sampled = q0;
+                graph_free(g);
+                e->use_graphs = false;
+                body();   // every level set is still zero, so the body may start from any of them
+                return;
+            }
+            e->cap = nullptr;
+            cudaGraph_t gr = nullptr;
+            err = cudaStreamEndCapture(e->st, &gr);
+            if (err == cudaSuccess) err = cudaGraphInstantiate(&g->exec, gr, 0);
+            if (gr) cudaGraphDestroy(gr);
+        }
+        g->launches = e->launches - l0; g->step_launches = e->step_launches - s0; g->sampled = e->sampled - m0;
+        g->pair_launches = e->pair_launches - p0; g->pair_sampled = e->pair_sampled - q0;
+        e->launches = l0; e->step_launches = s0; e->sampled = m0; e->pair_launches = p0; e->pair_sampled = q0;
+        if (err != cudaSuccess) {   // no graphs on this device / driver: launch directly from now on
+            cudaGetLastError();
+            graph_free(g);
+            e->use_graphs = false;
+            body();
+            return;
+        }
+        if (e->graphs.size() >= MAX_GRAPHS) {
+            size_t old = 0;
+            for (size_t i = 1; i < e->graphs.size(); i++)
+                if (e->graphs[i]->used < e->graphs[old]->used) old = i;
+            stats_flush(e);
+            graph_free(e->graphs[old]);
+            e->graphs.erase(e->graphs.begin() + old);
+        }
+        e->graphs.push_back(g);
+    }
+    if (g->pending) stats_flush(e);   // its events still hold the previous replay
+    EIO_CUDA(cudaGraphLaunch(g->exec, e->st));
+    g->used = ++e->graph_clock;
+    e->launches += g->launches; e->step_launches += g->step_launches; e->sampled += g->sampled;
+    e->pair_launches += g->pair_launches; e->pair_sampled += g->pair_sampled;
+    g->pending = e->stats && g->nev > 0;
+}
+
 // the widened-tile source lists of a propagation (two-step kernel only)
 static SparseOp halo_sources(Engine* e, bool use_pair, const int* const pos[4], const int npos[4], DBuf* sig) {
     SparseOp op;
@@ -709,6 +884,11 @@ void engine_set_kernel(Engine* e, int kind, int tz, int cw, int cpr) {
     e->kind = kind;
     if (kind == 1) { e->tz = tz; e->cw = cw; e->cpr = cpr; }
     e->tuned = true;
+}
+
+void engine_set_graphs(Engine* e, int enable) {
+    stats_flush(e);
+    e->use_graphs = enable != 0;
 }
 
 void engine_get_kernel(const Engine* e, int* kind, int* tz, int* cw, int* cpr) {
@@ -886,30 +1066,36 @@ void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], 
         a.ext = upload_points(e, src, e->ext_ts, e->ext_ent, e->sig_out);
         injh = halo_sources(e, use_pair, g.recPos, g.nRec, e->sig_in);
     }
-    for (size_t i = 0; i < steps.size();) {
-        if (use_pair && i + 1 < steps.size()) {
-            StepArgs a0 = a, a1 = a;
-            weights(a0, steps[i].first, steps[i].second);
-            weights(a1, steps[i + 1].first, steps[i + 1].second);
-            if (!adj) run_pair<0, EPI_NONE>(e, a0, a1, injh, L);
-            else run_pair<1, EPI_NONE>(e, a0, a1, injh, L);
-            i += 2;
-            continue;
+    LoopKey key = loop_key(e, 1);
+    key << adj << wfld << use_pair;
+    key.add(&a, sizeof(a));
+    key.add(&injh, sizeof(injh));
+    run_graph(e, key.h, (long long)steps.size(), [&] {
+        for (size_t i = 0; i < steps.size();) {
+            if (use_pair && i + 1 < steps.size()) {
+                StepArgs a0 = a, a1 = a;
+                weights(a0, steps[i].first, steps[i].second);
+                weights(a1, steps[i + 1].first, steps[i + 1].second);
+                if (!adj) run_pair<0, EPI_NONE>(e, a0, a1, injh, L);
+                else run_pair<1, EPI_NONE>(e, a0, a1, injh, L);
+                i += 2;
+                continue;
+            }
+            const int its = steps[i].first, it2 = steps[i].second;
+            L.set(a);
+            weights(a, its, it2);
+            if (!adj) {
+                if (e->fs_active) fs_top(e, L.c);
+                launch_step<0, EPI_NONE>(e, a, cur);
+            } else {
+                launch_step<1, EPI_NONE>(e, a, cur);
+            }
+            if (wfld) save_wavefield(e, wfld, L.o, its, F[it2], F[h + it2]);
+            L.single();
+            cur ^= 1;
+            i++;
         }
-        const int its = steps[i].first, it2 = steps[i].second;
-        L.set(a);
-        weights(a, its, it2);
-        if (!adj) {
-            if (e->fs_active) fs_top(e, L.c);
-            launch_step<0, EPI_NONE>(e, a, cur);
-        } else {
-            launch_step<1, EPI_NONE>(e, a, cur);
-        }
-        if (wfld) save_wavefield(e, wfld, L.o, its, F[it2], F[h + it2]);
-        L.single();
-        cur ^= 1;
-        i++;
-    }
+    });
     check_launch();
     if (!adj) stage_out(e, rec.ld, e->nts, e->sig_out, data);
     else stage_out(e, src.ld, e->nts, e->sig_out, model);
@@ -1011,7 +1197,12 @@ static void born_source_q(Engine* e, const PointList& src, StepArgs a) {
     const float* F = e->filt.data();
     const int h = e->h;
     const int npart = e->ntiles * 16;
+    LoopKey key = loop_key(e, 2);
+    key << e->Wq.p << e->wscale.p << e->wstage.p << e->wpmax.p;
+    key.add(&a, sizeof(a));
+    key.add(&injh, sizeof(injh));
     try {
+      run_graph(e, key.h, (long long)(e->nts - 1) * e->S, [&] {
         for (int its = 0; its < e->nts - 1; its++) {
             if (kind == 5 && its < e->nts - 2) {
                 // (its, 1) samples row its, (its, 2) only steps; the staging rows
@@ -1048,6 +1239,7 @@ static void born_source_q(Engine* e, const PointList& src, StepArgs a) {
                 cur ^= 1;
             }
         }
+      });
     } catch (...) {
         e->kind = kind;
         throw;
@@ -1080,6 +1272,11 @@ static void born_source(Engine* e, const PointList& src, StepArgs a) {
     a.W1 = e->W.f() + (long long)e->nts * e->n;
     const float* F = e->filt.data();
     const int h = e->h;
+    LoopKey key = loop_key(e, 3);
+    key << tri << use_pair;
+    key.add(&a, sizeof(a));
+    key.add(&injh, sizeof(injh));
+    run_graph(e, key.h, (long long)(e->nts - 1) * e->S, [&] {
     for (int its = 0; its < e->nts - 1; its++) {
         if (use_pair && its < e->nts - 2) {
             // (its, 1) writes row its, (its, 2) only steps
@@ -1114,6 +1311,7 @@ static void born_source(Engine* e, const PointList& src, StepArgs a) {
             cur ^= 1;
         }
     }
+    });
     check_launch();
 }
 
@@ -1141,22 +1339,35 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
         }
     for (int f = 0; f < 10; f++) EIO_CUDA(cudaMemsetAsync(e->ss[f].p, 0, sizeof(float) * e->n, e->st));
     zero_wavefields(e);
-    // the imaging stream starts after everything queued so far (history, model, clears)
-    EIO_CUDA(cudaEventRecord(e->ev_sync, e->st));
-    EIO_CUDA(cudaStreamWaitEvent(e->st2, e->ev_sync, 0));
-    for (int k = 0; k < R; k++) {       // no slot is in use at the start
-        EIO_CUDA(cudaEventRecord(e->ev_free[k], e->st2));
-        EIO_CUDA(cudaEventRecord(e->ev_ready[k], e->st2));
-    }
+    // the imaging stream joins a time loop after everything queued before it
+    // (history, model, clears) and the step stream waits for it at the end
+    auto fork = [&] {
+        EIO_CUDA(cudaEventRecord(e->ev_sync, e->st));
+        EIO_CUDA(cudaStreamWaitEvent(e->st2, e->ev_sync, 0));
+        for (int k = 0; k < R; k++) {       // no slot is in use at the start
+            EIO_CUDA(cudaEventRecord(e->ev_free[k], e->st2));
+            EIO_CUDA(cudaEventRecord(e->ev_ready[k], e->st2));
+        }
+    };
+    auto join = [&] {
+        EIO_CUDA(cudaEventRecord(e->ev_sync, e->st2));
+        EIO_CUDA(cudaStreamWaitEvent(e->st, e->ev_sync, 0));
+    };
     float* sL[5]; float* sR[5];
     for (int f = 0; f < 5; f++) { sL[f] = e->ss[f].f(); sR[f] = e->ss[5 + f].f(); }
     Levels L(e);
     int cur = 0;
     const bool use_pair = e->kind == 5;
     StepArgs a = base;
+    LoopKey key = loop_key(e, adj ? (e->S == 2 ? 5 : 6) : 4);
+    key << use_pair << e->W.p << e->Wq.p << e->wscale.p;
+    for (int f = 0; f < 5; f++) key << dm[f];
+    for (int f = 0; f < 20; f++) key << e->ss[f].p;
+    const long long nsteps = (long long)(e->nts - 1) * e->S;
     if (!adj) {
         zero_out(e, rec.ld, e->nts, e->sig_out);
         a.ext = upload_points(e, rec, e->ext_ts, e->ext_ent, e->sig_out);
+        key.add(&a, sizeof(a));
         // secondary sources of coarse sample k go to slot k % R on the imaging
         // stream, up to R-1 samples ahead of the step kernels that inject them;
         // slot k is free once coarse interval k - R (its last reader) is done
@@ -1166,6 +1377,8 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
             launch_imaging(e, 0, k, dm, ring[sl], e->st2);
             EIO_CUDA(cudaEventRecord(e->ev_ready[sl], e->st2));
         };
+        run_graph(e, key.h, nsteps, [&] {
+        fork();
         for (int k = 0; k < R - 1 && k < e->nts; k++) image(k);
         for (int its = 0; its < e->nts - 1; its++) {
             if (its + R - 1 < e->nts) image(its + R - 1);
@@ -1197,8 +1410,8 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
             // reference's memset of the right slice (BornElasticGpuFunctions.cu:806-810) is not needed
             EIO_CUDA(cudaEventRecord(e->ev_free[l], e->st));
         }
-        EIO_CUDA(cudaEventRecord(e->ev_sync, e->st2));
-        EIO_CUDA(cudaStreamWaitEvent(e->st, e->ev_sync, 0));
+        join();
+        });
         check_launch();
         stage_out(e, rec.ld, e->nts, e->sig_out, data);
     } else if (e->S == 2) {
@@ -1227,6 +1440,10 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
         auto weights = [&](StepArgs& x, int its, int it2) {
             x.inj.t0 = its; x.inj.w0 = F[it2 + 1]; x.inj.w1 = F[h + it2 + 1];
         };
+        key.add(&a, sizeof(a));
+        key.add(&injh, sizeof(injh));
+        run_graph(e, key.h, nsteps, [&] {
+        fork();
         for (int its = e->nts - 2; its > -1; its--) {
             if (use_pair && its > 0) {
                 // (its, 1) writes sample its+1, (its, 0) only steps
@@ -1257,12 +1474,14 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
                 cur ^= 1;
             }
         }
-        EIO_CUDA(cudaEventRecord(e->ev_sync, e->st2));
-        EIO_CUDA(cudaStreamWaitEvent(e->st, e->ev_sync, 0));
+        join();
+        });
         check_launch();
     } else {
         stage_in(e, data, rec.ld, e->nts, e->sig_in);
         a.inj = upload_points(e, rec, e->inj_ts, e->inj_ent, e->sig_in);
+        key.add(&a, sizeof(a));
+        run_graph(e, key.h, nsteps, [&] {
         for (int its = e->nts - 2; its > -1; its--) {
             for (int it2 = e->S - 1; it2 > -1; it2--) {
                 L.set(a);
@@ -1278,6 +1497,7 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
             for (int f = 0; f < 5; f++) EIO_CUDA(cudaMemsetAsync(sL[f], 0, sizeof(float) * e->n, e->st));
         }
         launch_imaging(e, 1, 0, dm, sR, e->st);
+        });
         check_launch();
     }
     EIO_CUDA(cudaStreamSynchronize(e->st));

@@ -549,6 +549,12 @@ EIO_API int eio_ctx_stats(eio_ctx* c, int enable, int reset, long long* launches
         engine_stats(c->eng, enable, reset, launches, stepLaunches, stepMs, nullptr, nullptr);
     });
 }
+EIO_API int eio_ctx_set_graphs(eio_ctx* c, int enable) {
+    return guarded([&] {
+        if (!c) throw Error(EIO_ERR_ARG, "null context");
+        engine_set_graphs(c->eng, enable);
+    });
+}
 EIO_API int eio_ctx_pair_stats(eio_ctx* c, long long* pairLaunches, double* pairMs) {
     return guarded([&] {
         if (!c) throw Error(EIO_ERR_ARG, "null context");

@@ -70,6 +70,7 @@ void engine_get_kernel(const Engine* e, int* kind, int* tz, int* cw, int* cpr);
 void engine_autotune(Engine* e);
 void* engine_stream(Engine* e);
 // launch statistics: enable = 1/0 (-1 leaves it), reset = 1 zeroes the counters after reading
+void engine_set_graphs(Engine* e, int enable);
 void engine_stats(Engine* e, int enable, int reset, long long* launches, long long* step_launches, double* step_ms,
                   long long* pair_launches, double* pair_ms);
 
