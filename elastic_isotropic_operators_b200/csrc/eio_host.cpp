@@ -549,6 +549,13 @@ EIO_API int eio_ctx_stats(eio_ctx* c, int enable, int reset, long long* launches
         engine_stats(c->eng, enable, reset, launches, stepLaunches, stepMs, nullptr, nullptr);
     });
 }
+EIO_API int eio_reduce64(int device, int op, int dtype, const void* x, const void* y, long long n, int onDevice,
+                         double* result) {
+    return guarded([&] {
+        if (!result) throw Error(EIO_ERR_ARG, "null result");
+        *result = reduce64(device, op, dtype, x, y, n, onDevice != 0);
+    });
+}
 EIO_API int eio_ctx_set_graphs(eio_ctx* c, int enable) {
     return guarded([&] {
         if (!c) throw Error(EIO_ERR_ARG, "null context");

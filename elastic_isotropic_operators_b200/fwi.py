@@ -15,29 +15,63 @@ pieces that script composes, on top of ``nonlinearFwiPropElasticShotsGpu``
   search and projection onto the bounds.
 
 Reductions that decide the optimisation (misfit, dot products, gradient norm)
-run in FP64 on the GPU when one is present (``dot64``); the fields stay FP32.
+run in FP64 on the GPU through the library's own reduction kernels
+(``eio_reduce64``: ``dot64``, ``misfit64``); the fields stay FP32.  Without a
+visible CUDA device (host-only tests of the solver logic) they are formed in
+FP64 with numpy.
 """
+import ctypes
+
 import numpy as np
 
-__all__ = ["dot64", "ElasticDatComp", "ElasticConv", "ElasticConvJab", "FwiObjective", "lbfgs"]
+__all__ = ["dot64", "misfit64", "ElasticDatComp", "ElasticConv", "ElasticConvJab", "FwiObjective", "lbfgs"]
 
 
 def _nd(v):
     return v.getNdArray() if hasattr(v, "getNdArray") else v
 
 
+_HAS_GPU = None
+
+
+def _gpu():
+    global _HAS_GPU
+    if _HAS_GPU is None:
+        try:
+            import torch
+            _HAS_GPU = bool(torch.cuda.is_available())
+        except ImportError:
+            _HAS_GPU = False
+    return _HAS_GPU
+
+
+def _reduce64(op, a, b, device=0):
+    a = np.asarray(_nd(a))
+    b = a if b is None else np.asarray(_nd(b))
+    if a.size != b.size:
+        raise ValueError("reduction over arrays of different sizes (%d, %d)" % (a.size, b.size))
+    dt = np.float32 if (a.dtype == np.float32 and b.dtype == np.float32) else np.float64
+    same = b is a
+    a = np.ascontiguousarray(a, dtype=dt)
+    b = a if same else np.ascontiguousarray(b, dtype=dt)
+    if not _gpu():
+        a64, b64 = a.ravel().astype(np.float64), b.ravel().astype(np.float64)
+        return float(np.dot(a64, b64)) if op == 0 else float(np.dot(a64 - b64, a64 - b64))
+    from . import _lib
+    r = ctypes.c_double()
+    _lib.check(_lib.lib().eio_reduce64(device, op, 0 if dt == np.float32 else 1, a.ctypes.data, b.ctypes.data,
+                                       a.size, 0, ctypes.byref(r)))
+    return r.value
+
+
 def dot64(a, b):
-    """FP64 dot product of two arrays, on the GPU when available."""
-    a, b = _nd(a), _nd(b)
-    try:
-        import torch
-        if torch.cuda.is_available():
-            ta = torch.from_numpy(np.ascontiguousarray(a)).to("cuda").double().ravel()
-            tb = ta if b is a else torch.from_numpy(np.ascontiguousarray(b)).to("cuda").double().ravel()
-            return float(torch.dot(ta, tb).item())
-    except ImportError:
-        pass
-    return float(np.dot(np.ravel(a).astype(np.float64), np.ravel(b).astype(np.float64)))
+    """FP64 dot product of two arrays (FP32 or FP64 values), summed on the GPU."""
+    return _reduce64(0, a, None if b is a else b)
+
+
+def misfit64(a, b):
+    """FP64 sum of (a - b)^2, summed on the GPU."""
+    return _reduce64(1, a, b)
 
 
 # --------------------------------------------------------------------- data components

@@ -247,13 +247,14 @@ class _ElasticOp:
         r1 = data_space.clone().rand(4321)
         d2 = model_space.clone()
         r2 = data_space.clone()
+        from .fwi import dot64   # FP64 sums on the GPU
         self.forward(False, d1, r2)
         self.adjoint(False, d2, r1)
-        dot1, dot2 = r1.dot(r2), d1.dot(d2)
+        dot1, dot2 = dot64(r1, r2), dot64(d1, d2)
         err_no_add = abs((dot1 - dot2) / dot2)
         self.forward(True, d1, r2)
         self.adjoint(True, d2, r1)
-        dot3, dot4 = r1.dot(r2), d1.dot(d2)
+        dot3, dot4 = dot64(r1, r2), dot64(d1, d2)
         err_add = abs((dot3 - dot4) / dot4)
         if verbose:
             print("WITHOUT ADD:\ndot1: %.16g\ndot2: %.16g\nerror WITHOUT ADD: %.16g" % (dot1, dot2, err_no_add))

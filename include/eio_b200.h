@@ -156,6 +156,15 @@ int eio_ctx_autotune(eio_ctx *c, int *kind, int *tz, int *cw, int *cpr);
  * enable: 1 on, 0 off, -1 unchanged; reset: zero the counters after reading. */
 int eio_ctx_stats(eio_ctx *c, int enable, int reset, long long *launches, long long *stepLaunches,
                   double *stepMs);
+/* FP64 reductions on the GPU (no reference counterpart; the reference sums on
+ * the host in pySolver, operator.h:50-89 for the dot-product test).
+ * op 0: sum x[i]*y[i] (dot product, or squared norm with y == x);
+ * op 1: sum (x[i]-y[i])^2 (data misfit). x, y: n values of type dtype
+ * (0: float, 1: double), device pointers when onDevice != 0, else host arrays
+ * staged through the device in chunks. The summation order is fixed, so the
+ * result is reproducible. */
+int eio_reduce64(int device, int op, int dtype, const void *x, const void *y, long long n, int onDevice,
+                 double *result);
 /* CUDA graphs of the time loops (no reference counterpart; off by default).
  * Each time loop is captured as a graph the first time its launch sequence
  * (kernel choice, step counts, buffer addresses, point-list sizes) is seen and
