@@ -79,6 +79,7 @@ _SIGS = {
     "eio_ctx_stats": (I, [P, I, I, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
                           ctypes.POINTER(ctypes.c_double)]),
     "eio_ctx_set_graphs": (I, [P, I]),
+    "eio_ctx_set_shot_windows": (I, [P, I, IP, IP]),
     "eio_reduce64": (I, [I, I, I, P, P, ctypes.c_longlong, I, ctypes.POINTER(ctypes.c_double)]),
     "eio_ctx_pair_stats": (I, [P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]),
     "eio_nl_fwd_reg": (I, [P, P, P, P, IP, P, IP]),

@@ -92,6 +92,13 @@ struct Engine {
     // without the top edge, sigmaxx coefficient of the surface row per column
     int fs = 0;
     bool fs_active = false;   // set while a free-surface propagation runs (k_step only)
+    // shot window: the propagations run on columns [win_ix0, win_ix0 + nx) of the
+    // full_nx-column grid (one contiguous block of every [nx][nz] array)
+    int full_nx = 0, win_ix0 = 0;
+    bool windowed = false;
+    std::vector<float> damp;  // taper table of the grid (minPad entries)
+    int minPad = 0;
+    DBuf dampx_w;
     DBuf dampz_fs, fsc;
     DBuf inj_ts, inj_ent, ext_ts, ext_ent;
     DBuf inj_hts, inj_hent;   // source lists of the widened tiles (two-step kernel)
@@ -106,6 +113,9 @@ struct Engine {
     } rint[4];
     DBuf stage_d[5];        // irregular receiver traces [nIrreg][nts] per field
     bool w_clean = false;   // history zeroed and only written by single stores since
+    // grid size (nz * nx) the history buffers were last cleared for: their FAT
+    // frame is never written, so a new layout (another shot window) clears them
+    long long w_n = -1, wq_n = -1, ws_n = -1;
     // step-kernel choice: kind 0 = shared-memory tile kernel (k_step),
     // kind 1 = TMA x-sweep (k_sweep) with strip height tz, chunk width cw and
     // cpr chunks per CTA, kind 2 = persistent TMA-pipelined tile kernel (k_tile),
@@ -225,7 +235,10 @@ static void upload(DBuf& b, const void* h, size_t bytes, cudaStream_t st) {
 void engine_set_medium(Engine* e, const FdParam& fd) {
     EIO_CUDA(cudaSetDevice(e->device));
     const int nz = fd.p.nz, nx = fd.p.nx;
-    if (nz != e->nz || nx != e->nx) throw Error(EIO_ERR_ARG, "setBackground: grid size changed");
+    if (nz != e->nz || nx != e->full_nx) throw Error(EIO_ERR_ARG, "setBackground: grid size changed");
+    engine_set_window(e, 0, 0);
+    e->damp.assign(fd.damp.begin(), fd.damp.begin() + std::min<size_t>(fd.damp.size(), (size_t)std::max(fd.minPad, 0)));
+    e->minPad = fd.minPad;
     for (int f = 0; f < 5; f++) upload(e->par[f], fd.par[f].data(), sizeof(float) * e->n, e->st);
     // per-axis taper tables: the taper of a cell is damp[min(distance to any edge)]
     // and damp[] is non-decreasing, so it equals min(dampz[iz], dampx[ix]).
@@ -274,6 +287,7 @@ Engine* engine_create(int device, const FdParam& fd) {
         EIO_CUDA(cudaDeviceGetAttribute(&e->nsm, cudaDevAttrMultiProcessorCount, device));
         e->nz = fd.p.nz;
         e->nx = fd.p.nx;
+        e->full_nx = e->nx;
         e->n = (long long)e->nz * e->nx;
         if ((e->nz - 2 * FAT) % 16 || (e->nx - 2 * FAT) % 16 || e->nz % 4)
             throw Error(EIO_ERR_QC, "nz-2*fat and nx-2*fat must be multiples of 16");
@@ -309,7 +323,7 @@ void engine_destroy(Engine* e) {
     if (e->st2) cudaStreamSynchronize(e->st2);
     DBuf* all[] = {&e->dampz, &e->dampx, &e->inj_ts, &e->inj_ent, &e->inj_hts, &e->inj_hent, &e->ext_ts, &e->ext_ent,
                    &e->W, &e->err, &e->wsave,
-                   &e->Wq, &e->wscale, &e->wstage, &e->wpmax, &e->dampz_fs, &e->fsc};
+                   &e->Wq, &e->wscale, &e->wstage, &e->wpmax, &e->dampz_fs, &e->fsc, &e->dampx_w};
     for (DBuf* b : all) b->release();
     for (int k = 0; k < 4; k++) {
         e->rint[k].slot.release(); e->rint[k].w.release(); e->rint[k].start.release(); e->rint[k].ent.release();
@@ -362,8 +376,13 @@ void engine_stats(Engine* e, int enable, int reset, long long* launches, long lo
 
 // every kind but the sweep (1) uses the 64x16 tiles of k_step and their numbering
 static bool tiled(int kind) { return kind != 1; }
-// the free surface is built into k_step only
-static int eff_kind(const Engine* e) { return e->fs_active ? 0 : e->kind; }
+// the free surface is built into k_step only; the TMA kernels' tensor maps
+// cover the whole grid, so a shot window runs them as kind 3
+static int eff_kind(const Engine* e) {
+    if (e->fs_active) return 0;
+    if (e->windowed && (e->kind == 1 || e->kind == 2)) return 3;
+    return e->kind;
+}
 
 // tile geometry the sparse point lists are bucketed with
 struct TileGeom {
@@ -465,11 +484,12 @@ static void transpose(Engine* e, const float* in, float* out, int rows, int cols
 static StepArgs base_args(Engine* e) {
     StepArgs a;
     memset(&a, 0, sizeof(a));
-    for (int f = 0; f < 5; f++) a.par[f] = e->par[f].f();
+    const long long off = (long long)e->win_ix0 * e->nz;   // shot window
+    for (int f = 0; f < 5; f++) a.par[f] = e->par[f].f() + off;
     a.dampz = e->fs_active ? e->dampz_fs.f() : e->dampz.f();
-    a.dampx = e->dampx.f();
+    a.dampx = e->windowed ? e->dampx_w.f() : e->dampx.f();
     a.fs = e->fs_active ? 1 : 0;
-    a.fsc = e->fsc.f();
+    a.fsc = e->fsc.f() ? e->fsc.f() + e->win_ix0 : nullptr;
     a.nz = e->nz;
     a.nx = e->nx;
     a.ntz = e->ntz;
@@ -886,6 +906,38 @@ void engine_set_kernel(Engine* e, int kind, int tz, int cw, int cpr) {
     e->tuned = true;
 }
 
+// Columns [ix0, ix0 + nxw) of the grid as the grid of the next propagations
+// (nxw = 0: the whole grid).  The window keeps the grid's taper table: its
+// first and last FAT columns are the frozen frame and the taper runs from its
+// own edges.  The medium, the Born perturbation and the gradient are the
+// grid's arrays offset by ix0 * nz; wavefield levels use the first nz * nxw
+// values of their buffers.
+void engine_set_window(Engine* e, int ix0, int nxw) {
+    if (nxw == 0) { ix0 = 0; nxw = e->full_nx; }
+    if (ix0 < 0 || nxw < 2 * FAT + 16 || (nxw - 2 * FAT) % 16 || ix0 + nxw > e->full_nx)
+        throw Error(EIO_ERR_ARG, "shot window [" + std::to_string(ix0) + ", " + std::to_string(ix0 + nxw) +
+                                     ") must lie in the grid and hold 2*fat + a multiple of 16 columns");
+    if (ix0 == e->win_ix0 && nxw == e->nx) return;
+    EIO_CUDA(cudaSetDevice(e->device));
+    e->win_ix0 = ix0;
+    e->nx = nxw;
+    e->n = (long long)e->nz * nxw;
+    e->ntx = (nxw - 2 * FAT) / TX;
+    e->ntiles = e->ntz * e->ntx;
+    e->windowed = !(ix0 == 0 && nxw == e->full_nx);
+    if (e->windowed) {
+        std::vector<float> dx(nxw, 1.f);
+        for (int ix = FAT; ix < nxw - FAT; ix++) {
+            const int d = std::min(ix - FAT, nxw - ix - 1 - FAT);
+            if (d < e->minPad && d < (int)e->damp.size()) dx[ix] = e->damp[d];
+        }
+        upload(e->dampx_w, dx.data(), sizeof(float) * nxw, e->st);
+        EIO_CUDA(cudaStreamSynchronize(e->st));   // dx is a local
+    }
+}
+
+int engine_window_ix0(const Engine* e) { return e->win_ix0; }
+
 void engine_set_graphs(Engine* e, int enable) {
     stats_flush(e);
     e->use_graphs = enable != 0;
@@ -1023,6 +1075,7 @@ struct FsScope {
 
 void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], const ShotGeom& g, float* wfld) {
     EIO_CUDA(cudaSetDevice(e->device));
+    if (wfld && e->windowed) throw Error(EIO_ERR_UNSUPPORTED, "saved wavefields cover the whole grid: no shot windows");
     if (!e->tuned) engine_autotune(e);
     FsScope fs_scope(e);
     err_reset(e);
@@ -1171,13 +1224,15 @@ static void born_source_q(Engine* e, const PointList& src, StepArgs a) {
     if (e->S != 2)
         throw Error(EIO_ERR_UNSUPPORTED, "16-bit source-wavefield snapshots need sub = 1 (two fine steps per sample)");
     const size_t qbytes = sizeof(unsigned short) * 2 * (size_t)e->nts * e->n;
-    if (e->Wq.cap < qbytes) {
+    if (e->Wq.cap < qbytes || e->wq_n != e->n) {
         e->Wq.ensure(qbytes);
         EIO_CUDA(cudaMemsetAsync(e->Wq.p, 0, qbytes, e->st));   // the FAT frame is never written
+        e->wq_n = e->n;
     }
-    if (e->wstage.cap < sizeof(float) * 2 * (size_t)e->n) {
+    if (e->wstage.cap < sizeof(float) * 2 * (size_t)e->n || e->ws_n != e->n) {
         e->wstage.ensure(sizeof(float) * 2 * (size_t)e->n);
         EIO_CUDA(cudaMemsetAsync(e->wstage.p, 0, sizeof(float) * 2 * (size_t)e->n, e->st));
+        e->ws_n = e->n;
     }
     e->wscale.ensure(sizeof(float) * 2 * (size_t)e->nts);
     const size_t pbytes = sizeof(float) * 2 * 2 * (size_t)e->ntiles * 16;
@@ -1259,8 +1314,9 @@ static void born_source(Engine* e, const PointList& src, StepArgs a) {
     const bool tri = (e->S == 2);
     // running sums need a zeroed history; single writes only need the never
     // written FAT frame to be zero, which holds from the first clear on
-    if (!tri || fresh || !e->w_clean) EIO_CUDA(cudaMemsetAsync(e->W.p, 0, wbytes, e->st));
+    if (!tri || fresh || !e->w_clean || e->w_n != e->n) EIO_CUDA(cudaMemsetAsync(e->W.p, 0, wbytes, e->st));
     e->w_clean = tri;
+    e->w_n = e->n;
     zero_wavefields(e);
     Levels L(e);
     int cur = 0;
@@ -1570,19 +1626,23 @@ void engine_born_host(Engine* e, int adj, float* const srcDtw[5], float* const d
 // the receiver traces between the regular grid and the devices on the GPU, so
 // only the irregular traces cross PCIe.
 
+// the perturbation / image always covers the whole grid (shot windows are views of it)
 void engine_dm_upload(Engine* e, float* const dm[5]) {
     EIO_CUDA(cudaSetDevice(e->device));
-    for (int f = 0; f < 5; f++) h2d(e, e->stage_c[f], dm[f], e->n);
+    const size_t n = (size_t)e->nz * e->full_nx;
+    for (int f = 0; f < 5; f++) h2d(e, e->stage_c[f], dm[f], n);
 }
 void engine_dm_zero(Engine* e) {
     EIO_CUDA(cudaSetDevice(e->device));
+    const size_t n = (size_t)e->nz * e->full_nx;
     for (int f = 0; f < 5; f++) {
-        e->stage_c[f].ensure(sizeof(float) * e->n);
-        EIO_CUDA(cudaMemsetAsync(e->stage_c[f].p, 0, sizeof(float) * e->n, e->st));
+        e->stage_c[f].ensure(sizeof(float) * n);
+        EIO_CUDA(cudaMemsetAsync(e->stage_c[f].p, 0, sizeof(float) * n, e->st));
     }
 }
 void engine_dm_download(Engine* e, float* const dm[5]) {
-    for (int f = 0; f < 5; f++) d2h(e, dm[f], e->stage_c[f], e->n);
+    const size_t n = (size_t)e->nz * e->full_nx;
+    for (int f = 0; f < 5; f++) d2h(e, dm[f], e->stage_c[f], n);
     EIO_CUDA(cudaStreamSynchronize(e->st));
 }
 
@@ -1659,7 +1719,7 @@ void engine_born_shot(Engine* e, int adj, float* const srcDtw[5], const ShotGeom
     for (int f = 0; f < 5; f++) {
         h2d(e, e->stage_a[f], srcDtw[f], (size_t)g.nSrc[kFieldGrid[f]] * e->ntw);
         ds[f] = e->stage_a[f].f();
-        dd[f] = e->stage_c[f].f();
+        dd[f] = e->stage_c[f].f() + (long long)e->win_ix0 * e->nz;   // the shot window of the image
     }
     stage_receivers(e, adj, g, rec, dataIrreg, dr);
     engine_born(e, adj, ds, dd, dr, g);

@@ -368,6 +368,8 @@ struct eio_ctx {
     FdParam fd;
     Engine* eng = nullptr;
     int device = 0;
+    // per-shot windows of the multi-shot operators (eio_ctx_set_shot_windows); empty: whole grid
+    std::vector<int> win_ix0, win_nx;
 };
 
 template <class F>
@@ -556,6 +558,20 @@ EIO_API int eio_reduce64(int device, int op, int dtype, const void* x, const voi
         *result = reduce64(device, op, dtype, x, y, n, onDevice != 0);
     });
 }
+EIO_API int eio_ctx_set_shot_windows(eio_ctx* c, int nShots, const int* ix0, const int* nxw) {
+    return guarded([&] {
+        if (!c) throw Error(EIO_ERR_ARG, "null context");
+        if (nShots < 0 || (nShots > 0 && (!ix0 || !nxw))) throw Error(EIO_ERR_ARG, "null window list");
+        const int nx = c->fd.p.nx, fat = c->fd.p.fat;
+        for (int i = 0; i < nShots; i++)
+            if (ix0[i] < 0 || nxw[i] < 2 * fat + 16 || (nxw[i] - 2 * fat) % 16 || ix0[i] + nxw[i] > nx)
+                throw Error(EIO_ERR_ARG, "shot window " + std::to_string(i) + " [" + std::to_string(ix0[i]) + ", " +
+                                             std::to_string(ix0[i] + nxw[i]) +
+                                             ") must lie in the grid and hold 2*fat + a multiple of 16 columns");
+        c->win_ix0.assign(ix0, ix0 + nShots);
+        c->win_nx.assign(nxw, nxw + nShots);
+    });
+}
 EIO_API int eio_ctx_set_graphs(eio_ctx* c, int enable) {
     return guarded([&] {
         if (!c) throw Error(EIO_ERR_ARG, "null context");
@@ -679,6 +695,47 @@ ShotGeom reg_geom(const ShotGrids& g) {
     return sg;
 }
 
+// Shot `shot` of a multi-shot call on its window (eio_ctx_set_shot_windows):
+// the engine crops to columns [ix0, ix0 + nxw) and the regular positions shift
+// by ix0 * nz.  Every device must lie in the window's updated interior.  The
+// whole grid comes back when the guard goes.
+struct ShotWindow {
+    eio_ctx* c;
+    std::vector<int> pos[8];
+    ShotGeom sg;
+    ShotWindow(eio_ctx* ctx, const ShotGrids& g, int shot, int nShots) : c(ctx) {
+        sg = reg_geom(g);
+        if (c->win_nx.empty()) return;
+        if ((int)c->win_nx.size() != nShots)
+            throw Error(EIO_ERR_ARG, "shot windows were set for " + std::to_string(c->win_nx.size()) + " shots, the call has " +
+                                         std::to_string(nShots));
+        const int ix0 = c->win_ix0[shot], nxw = c->win_nx[shot], nz = c->fd.p.nz, fat = c->fd.p.fat;
+        const long long off = (long long)ix0 * nz;
+        for (int k = 0; k < 8; k++) {
+            const int* p = k < 4 ? sg.srcPos[k] : sg.recPos[k - 4];
+            const int n = k < 4 ? sg.nSrc[k] : sg.nRec[k - 4];
+            pos[k].resize(n);
+            for (int i = 0; i < n; i++) {
+                const int ix = p[i] / nz;
+                if (ix < ix0 + fat || ix >= ix0 + nxw - fat)
+                    throw Error(EIO_ERR_BOUNDS, "a device of shot " + std::to_string(shot) + " (column " +
+                                                    std::to_string(ix) + ") lies outside the updated interior of its window");
+                pos[k][i] = (int)(p[i] - off);
+            }
+            if (k < 4) sg.srcPos[k] = pos[k].data();
+            else sg.recPos[k - 4] = pos[k].data();
+        }
+        engine_set_window(c->eng, ix0, nxw);
+    }
+    ~ShotWindow() {
+        if (!c->win_nx.empty()) {
+            try { engine_set_window(c->eng, 0, 0); } catch (...) {}
+        }
+    }
+    ShotWindow(const ShotWindow&) = delete;
+    ShotWindow& operator=(const ShotWindow&) = delete;
+};
+
 void check_nt(const ShotGrids& g, int nts) {
     for (int k = 0; k < 4; k++)
         if (g.s[k]->nt != nts || g.r[k]->nt != nts)
@@ -690,7 +747,8 @@ void check_nt(const ShotGrids& g, int nts) {
 
 // nonlinearPropElasticGpu::forward with add = false: irregular source -> data slice;
 // wfld (host [nts][5][nx][nz]) receives the saved wavefield when not null
-void nl_shot_forward(eio_ctx* c, const ShotGrids& g, const float* model, float* data, float* wfld = nullptr) {
+void nl_shot_forward(eio_ctx* c, const ShotGrids& g, const ShotGeom& sg, const float* model, float* data,
+                     float* wfld = nullptr) {
     const int nts = c->fd.p.nts;
     const int nsi = g.s[0]->nIrreg;
     std::vector<float> reg[5];
@@ -703,7 +761,7 @@ void nl_shot_forward(eio_ctx* c, const ShotGrids& g, const float* model, float* 
     scale_sources(c->fd, g, reg, nts);
     for (int f = 0; f < 5; f++) mp[f] = reg[f].data();
     // receivers are interpolated to the devices on the GPU (same sums as sinterp_forward)
-    engine_nl_shot(c->eng, 0, mp, reg_geom(g), g.r, data, wfld);
+    engine_nl_shot(c->eng, 0, mp, sg, g.r, data, wfld);
 }
 
 // The adjoint wavefield is scaled like the adjoint sources
@@ -725,7 +783,8 @@ static void scale_adjoint_wavefield(const FdParam& fd, float* w) {
 }
 
 // nonlinearPropElasticGpu::adjoint with add = true into model; wfld as for nl_shot_forward
-void nl_shot_adjoint(eio_ctx* c, const ShotGrids& g, float* model, const float* data, float* wfld = nullptr) {
+void nl_shot_adjoint(eio_ctx* c, const ShotGrids& g, const ShotGeom& sg, float* model, const float* data,
+                     float* wfld = nullptr) {
     const int nts = c->fd.p.nts;
     const int nsi = g.s[0]->nIrreg;
     std::vector<float> reg[5];
@@ -735,7 +794,7 @@ void nl_shot_adjoint(eio_ctx* c, const ShotGrids& g, float* model, const float* 
         mp[f] = reg[f].data();
     }
     // the data are spread onto the regular grid on the GPU (same sums as sinterp_adjoint)
-    engine_nl_shot(c->eng, 1, mp, reg_geom(g), g.r, const_cast<float*>(data), wfld);
+    engine_nl_shot(c->eng, 1, mp, sg, g.r, const_cast<float*>(data), wfld);
     if (wfld) scale_adjoint_wavefield(c->fd, wfld);
     scale_sources_adj(c->fd, g, reg, nts);
     for (int f = 0; f < 5; f++) sinterp_forward(*g.s[kFG[f]], true, reg[f].data(), model + (size_t)f * nsi * nts);
@@ -850,7 +909,8 @@ static int nl_forward_impl(eio_ctx* c, int add, int nExp, int nModelExp, const f
             check_nt(g, nts);
             if ((size_t)5 * g.s[0]->nIrreg * nts != mslice || (size_t)5 * g.r[0]->nIrreg * nts != dslice)
                 throw Error(EIO_ERR_ARG, "device counts differ between shots");
-            nl_shot_forward(c, g, model + (nModelExp == 1 ? 0 : (size_t)e * mslice), tmp.data(),
+            ShotWindow win(c, g, e, nExp);
+            nl_shot_forward(c, g, win.sg, model + (nModelExp == 1 ? 0 : (size_t)e * mslice), tmp.data(),
                             e == wShot ? wfld : nullptr);
             float* d = data + (size_t)e * dslice;
             #pragma omp parallel for schedule(static)
@@ -876,12 +936,13 @@ static int nl_adjoint_impl(eio_ctx* c, int add, int nExp, int nModelExp, float* 
             check_nt(g, nts);
             if ((size_t)5 * g.s[0]->nIrreg * nts != mslice || (size_t)5 * g.r[0]->nIrreg * nts != dslice)
                 throw Error(EIO_ERR_ARG, "device counts differ between shots");
+            ShotWindow win(c, g, e, nExp);
             if (nModelExp == 1) {
                 // constant source signal: stack every shot (nonlinearPropElasticShotsGpu.cpp:384-417)
-                nl_shot_adjoint(c, g, slice.data(), data + (size_t)e * dslice, e == wShot ? wfld : nullptr);
+                nl_shot_adjoint(c, g, win.sg, slice.data(), data + (size_t)e * dslice, e == wShot ? wfld : nullptr);
             } else {
                 std::fill(slice.begin(), slice.end(), 0.f);
-                nl_shot_adjoint(c, g, slice.data(), data + (size_t)e * dslice, e == wShot ? wfld : nullptr);
+                nl_shot_adjoint(c, g, win.sg, slice.data(), data + (size_t)e * dslice, e == wShot ? wfld : nullptr);
                 float* m = model + (size_t)e * mslice;
                 for (size_t i = 0; i < mslice; i++) m[i] += slice[i];
             }
@@ -947,7 +1008,8 @@ EIO_API int eio_born_forward(eio_ctx* c, int add, int nExp, const float* model, 
             born_sources(c, g, sigs[nSignals == 1 ? 0 : e], fine);
             float* sp[5];
             for (int f = 0; f < 5; f++) sp[f] = fine[f].data();
-            engine_born_shot(c->eng, 0, sp, reg_geom(g), g.r, tmp.data());
+            ShotWindow win(c, g, e, nExp);
+            engine_born_shot(c->eng, 0, sp, win.sg, g.r, tmp.data());
             float* d = data + (size_t)e * dslice;
 #pragma omp parallel for schedule(static)
             for (long long i = 0; i < (long long)dslice; i++) d[i] += tmp[i];
@@ -980,7 +1042,8 @@ EIO_API int eio_born_adjoint(eio_ctx* c, int add, int nExp, float* model, const 
             born_sources(c, g, sigs[nSignals == 1 ? 0 : e], fine);
             float* sp[5];
             for (int f = 0; f < 5; f++) sp[f] = fine[f].data();
-            engine_born_shot(c->eng, 1, sp, reg_geom(g), g.r, const_cast<float*>(data) + (size_t)e * dslice);
+            ShotWindow win(c, g, e, nExp);
+            engine_born_shot(c->eng, 1, sp, win.sg, g.r, const_cast<float*>(data) + (size_t)e * dslice);
         }
         engine_dm_download(c->eng, dm);
         // scaling and un-staggering, BornElasticShotsGpu.cpp:325-371

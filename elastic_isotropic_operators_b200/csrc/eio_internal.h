@@ -71,6 +71,8 @@ void engine_autotune(Engine* e);
 void* engine_stream(Engine* e);
 // launch statistics: enable = 1/0 (-1 leaves it), reset = 1 zeroes the counters after reading
 void engine_set_graphs(Engine* e, int enable);
+void engine_set_window(Engine* e, int ix0, int nxw);   // nxw = 0: the whole grid
+int engine_window_ix0(const Engine* e);
 // FP64 sum of x*y (op 0) or (x-y)^2 (op 1) over n values (dtype 0 FP32, 1 FP64) on GPU `device`
 double reduce64(int device, int op, int dtype, const void* x, const void* y, long long n, bool on_device);
 void engine_stats(Engine* e, int enable, int reset, long long* launches, long long* step_launches, double* step_ms,

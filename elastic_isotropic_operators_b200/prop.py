@@ -217,6 +217,50 @@ class _ElasticOp:
     def ctx(self):
         return self._ctx
 
+    # ---- cropped shots (no reference counterpart)
+    def setShotWindows(self, ix0, nxw):
+        """Propagate shot i on grid columns [ix0[i], ix0[i] + nxw[i]) only
+        (eio_ctx_set_shot_windows): a window holds 2*fat + a multiple of 16
+        columns and the shot's devices in its updated interior, and the grid's
+        cosine taper runs from its edges."""
+        ix0 = np.ascontiguousarray(ix0, dtype=np.int32)
+        nxw = np.ascontiguousarray(nxw, dtype=np.int32)
+        if ix0.shape != (self.nExp,) or nxw.shape != (self.nExp,):
+            raise EioError(-1, "one window per shot (nExp = %d)" % self.nExp)
+        check(self._L.eio_ctx_set_shot_windows(self._ctx, self.nExp, _lib.iptr(ix0), _lib.iptr(nxw)))
+        self.shotWindows = (ix0, nxw)
+
+    def clearShotWindows(self):
+        check(self._L.eio_ctx_set_shot_windows(self._ctx, 0, None, None))
+        self.shotWindows = None
+
+    def autoShotWindows(self, margin=None):
+        """Set per-shot windows spanning each shot's sources and receivers plus
+        ``margin`` columns on both sides (default: the grid's wider x pad), plus
+        the fat frame, widened to 2*fat + a multiple of 16 columns and kept in
+        the grid.  Returns (ix0, nxw)."""
+        nz, nx, fat = self.fd.nz, self.fd.nx, self.fd.fat
+        if margin is None:
+            margin = max(self.fd.xPadMinus, self.fd.xPadPlus)
+        ix0s, nxws = [], []
+        for e in range(self.nExp):
+            cols = []
+            for g in self.src:
+                cols.append(np.asarray(g[e].getRegPosUnique()) // nz)
+            for g in self.rec:
+                cols.append(np.asarray(g[0 if self.nRecGeom == 1 else e].getRegPosUnique()) // nz)
+            cols = np.concatenate([c for c in cols if c.size])
+            lo = max(int(cols.min()) - margin - fat, 0)
+            hi = min(int(cols.max()) + margin + fat + 1, nx)
+            w = hi - lo
+            w = 2 * fat + 16 * int(np.ceil(max(w - 2 * fat, 16) / 16.0))
+            w = min(w, nx)
+            lo = min(max(lo - (w - (hi - lo)) // 2, 0), nx - w)
+            ix0s.append(lo)
+            nxws.append(w)
+        self.setShotWindows(ix0s, nxws)
+        return np.array(ix0s, np.int32), np.array(nxws, np.int32)
+
     def setBackground(self, elasticParam):
         """Rebuild the medium (fdParamElastic QC runs again and may raise)."""
         ep = _arr(elasticParam)

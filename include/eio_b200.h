@@ -156,6 +156,18 @@ int eio_ctx_autotune(eio_ctx *c, int *kind, int *tz, int *cw, int *cpr);
  * enable: 1 on, 0 off, -1 unchanged; reset: zero the counters after reading. */
 int eio_ctx_stats(eio_ctx *c, int enable, int reset, long long *launches, long long *stepLaunches,
                   double *stepMs);
+/* Cropped shots (no reference counterpart; the reference propagates every shot
+ * on the whole grid). Shot i of the next multi-shot calls (eio_nl_forward,
+ * eio_nl_adjoint, eio_born_forward, eio_born_adjoint with nExp == nShots)
+ * propagates on columns [ix0[i], ix0[i] + nxw[i]) of the grid only: the
+ * medium, the Born perturbation and the gradient are viewed through the
+ * window. Its first and last fat columns are the frozen frame, and the
+ * grid's cosine taper runs from the window's edges. Each window must lie in
+ * the grid, hold 2*fat + a multiple of 16 columns, and contain the shot's
+ * sources and receivers in its updated interior (EIO_ERR_BOUNDS otherwise).
+ * Wavefield saving is not available on windows. nShots = 0 restores
+ * whole-grid shots. */
+int eio_ctx_set_shot_windows(eio_ctx *c, int nShots, const int *ix0, const int *nxw);
 /* FP64 reductions on the GPU (no reference counterpart; the reference sums on
  * the host in pySolver, operator.h:50-89 for the dot-product test).
  * op 0: sum x[i]*y[i] (dot product, or squared norm with y == x);
