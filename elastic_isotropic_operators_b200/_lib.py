@@ -80,6 +80,9 @@ _SIGS = {
                           ctypes.POINTER(ctypes.c_double)]),
     "eio_ctx_set_graphs": (I, [P, I]),
     "eio_ctx_set_shot_windows": (I, [P, I, IP, IP]),
+    "eio_ctx_set_lanes": (I, [P, I]),
+    "eio_ctx_get_lanes": (I, [P, IP, IP]),
+    "eio_born_shots_dev": (I, [P, I, I, P, P, P, P, IP, P, IP]),
     "eio_reduce64": (I, [I, I, I, P, P, ctypes.c_longlong, I, ctypes.POINTER(ctypes.c_double)]),
     "eio_ctx_pair_stats": (I, [P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]),
     "eio_nl_fwd_reg": (I, [P, P, P, P, IP, P, IP]),

@@ -1626,6 +1626,44 @@ void engine_born_host(Engine* e, int adj, float* const srcDtw[5], float* const d
 // the receiver traces between the regular grid and the devices on the GPU, so
 // only the irregular traces cross PCIe.
 
+// dst += src over n floats (n a multiple of 4, 16-byte aligned arrays)
+__global__ void __launch_bounds__(256) k_add4(float* __restrict__ dst, const float* __restrict__ src, long long n4)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+        float4 a = reinterpret_cast<float4*>(dst)[i];
+        const float4 b = reinterpret_cast<const float4*>(src)[i];
+        a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w;
+        reinterpret_cast<float4*>(dst)[i] = a;
+    }
+}
+
+bool engine_is_tuned(const Engine* e) { return e->tuned; }
+int engine_get_checkpoint(const Engine* e) { return e->ckpt; }
+int engine_get_graphs(const Engine* e) { return e->use_graphs ? 1 : 0; }
+size_t engine_cells(const Engine* e) { return (size_t)e->nz * e->full_nx; }
+
+// the lane's own image (whole grid), zeroed, for a lane other than the first
+void engine_dm_ptrs(Engine* e, float* out[5]) {
+    const size_t n = (size_t)e->nz * e->full_nx;
+    for (int f = 0; f < 5; f++) {
+        e->stage_c[f].ensure(sizeof(float) * n);
+        out[f] = e->stage_c[f].f();
+    }
+}
+
+// dst (device, whole grid, 5 components) += this lane's image
+void engine_dm_add(Engine* e, float* const dst[5]) {
+    EIO_CUDA(cudaSetDevice(e->device));
+    const long long n4 = (long long)e->nz * e->full_nx / 4;
+    for (int f = 0; f < 5; f++) {
+        k_add4<<<4 * e->nsm, 256, 0, e->st>>>(dst[f], e->stage_c[f].f(), n4);
+        e->launches++;
+    }
+    check_launch();
+    EIO_CUDA(cudaStreamSynchronize(e->st));
+}
+
 // the perturbation / image always covers the whole grid (shot windows are views of it)
 void engine_dm_upload(Engine* e, float* const dm[5]) {
     EIO_CUDA(cudaSetDevice(e->device));

@@ -16,9 +16,13 @@
 #include <cstring>
 #include <memory>
 #include <sstream>
+#include <exception>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
+
+#include <cuda_runtime.h>
 
 #include "eio_internal.h"
 
@@ -370,7 +374,79 @@ struct eio_ctx {
     int device = 0;
     // per-shot windows of the multi-shot operators (eio_ctx_set_shot_windows); empty: whole grid
     std::vector<int> win_ix0, win_nx;
+    // shot lanes: further engines (own streams and buffers) on the same device that
+    // run shots of a multi-shot call concurrently with eng (eio_ctx_set_lanes)
+    std::vector<Engine*> extra;
+    int lanes = 2;
 };
+
+static Engine* lane_engine(eio_ctx* c, int k) { return k == 0 ? c->eng : c->extra[k - 1]; }
+
+// Lanes for a call over nShots shots, each new lane needing about lane_bytes of
+// device memory: at most c->lanes and nShots, fewer when the free memory would
+// not hold the new lanes.  New lanes take the first lane's kernel choice (tuned
+// first), checkpoint precision and graph setting.
+static int ensure_lanes(eio_ctx* c, int nShots, size_t lane_bytes) {
+    int n = std::max(1, std::min(c->lanes, nShots));
+    const int have = 1 + (int)c->extra.size();
+    if (n > have) {
+        size_t fr = 0, tot = 0;
+        if (cudaSetDevice(c->device) == cudaSuccess && cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+            const size_t need = lane_bytes + lane_bytes / 5 + ((size_t)256 << 20);
+            while (n > have && (size_t)(n - have) * need > fr) n--;
+        } else {
+            n = have;
+        }
+    }
+    if (n > 1 && !engine_is_tuned(c->eng)) engine_autotune(c->eng);
+    while ((int)c->extra.size() < n - 1) {
+        Engine* e = engine_create(c->device, c->fd);
+        try {
+            int kind, tz, cw, cpr;
+            engine_get_kernel(c->eng, &kind, &tz, &cw, &cpr);
+            engine_set_kernel(e, kind, tz, cw, cpr);
+            engine_set_checkpoint(e, engine_get_checkpoint(c->eng));
+            engine_set_graphs(e, engine_get_graphs(c->eng));
+        } catch (...) {
+            engine_destroy(e);
+            throw;
+        }
+        c->extra.push_back(e);
+    }
+    return n;
+}
+
+// Shots 0..nShots-1 over n lanes: lane k takes shots k, k + n, ... in order, on
+// its own host thread; the first error is rethrown after every lane stopped.
+template <class F>
+static void run_lanes(eio_ctx* c, int n, int nShots, F&& f) {
+    if (n <= 1) {
+        for (int s = 0; s < nShots; s++) f(0, c->eng, s);
+        return;
+    }
+    std::vector<std::exception_ptr> err(n);
+    std::vector<std::thread> th;
+    th.reserve(n);
+    for (int k = 0; k < n; k++)
+        th.emplace_back([&, k] {
+            try {
+                for (int s = k; s < nShots; s += n) f(k, lane_engine(c, k), s);
+            } catch (...) {
+                err[k] = std::current_exception();
+            }
+        });
+    for (auto& t : th) t.join();
+    for (auto& x : err)
+        if (x) std::rethrow_exception(x);
+}
+
+// device bytes a lane needs for a shot: wavefield levels, secondary sources and, for Born, the history
+static size_t lane_bytes(const eio_ctx* c, bool born) {
+    const size_t n = (size_t)c->fd.p.nz * c->fd.p.nx;
+    size_t b = sizeof(float) * n * 40;
+    if (born) b += (size_t)2 * c->fd.p.nts * n * (engine_get_checkpoint(c->eng) ? 2 : 4);
+    return b;
+}
 
 template <class F>
 static int guarded(F&& f) {
@@ -495,11 +571,13 @@ EIO_API int eio_ctx_set_background(eio_ctx* c, const float* ep) {
         FdParam fd;
         build_fdparam(c->fd.p, ep, fd);   // QC may throw; the context keeps its old medium then
         engine_set_medium(c->eng, fd);
+        for (Engine* e : c->extra) engine_set_medium(e, fd);
         c->fd = std::move(fd);
     });
 }
 EIO_API void eio_ctx_destroy(eio_ctx* c) {
     if (!c) return;
+    for (Engine* e : c->extra) engine_destroy(e);
     engine_destroy(c->eng);
     delete c;
 }
@@ -507,6 +585,7 @@ EIO_API int eio_ctx_set_checkpoint_precision(eio_ctx* c, int mode) {
     return guarded([&] {
         if (!c) throw Error(EIO_ERR_ARG, "null context");
         engine_set_checkpoint(c->eng, mode);
+        for (Engine* e : c->extra) engine_set_checkpoint(e, mode);
     });
 }
 EIO_API int eio_ctx_get_medium(const eio_ctx* c, float* rx, float* rz, float* l2m, float* lam, float* mu) {
@@ -529,12 +608,16 @@ EIO_API int eio_ctx_set_kernel(eio_ctx* c, int kind, int tz, int cw, int cpr) {
     return guarded([&] {
         if (!c) throw Error(EIO_ERR_ARG, "null context");
         engine_set_kernel(c->eng, kind, tz, cw, cpr);
+        for (Engine* e : c->extra) engine_set_kernel(e, kind, tz, cw, cpr);
     });
 }
 EIO_API int eio_ctx_autotune(eio_ctx* c, int* kind, int* tz, int* cw, int* cpr) {
     return guarded([&] {
         if (!c) throw Error(EIO_ERR_ARG, "null context");
         engine_autotune(c->eng);
+        int k, t, w, r;
+        engine_get_kernel(c->eng, &k, &t, &w, &r);
+        for (Engine* e : c->extra) engine_set_kernel(e, k, t, w, r);
         engine_get_kernel(c->eng, kind, tz, cw, cpr);
     });
 }
@@ -548,7 +631,18 @@ EIO_API int eio_ctx_stats(eio_ctx* c, int enable, int reset, long long* launches
                           double* stepMs) {
     return guarded([&] {
         if (!c) throw Error(EIO_ERR_ARG, "null context");
-        engine_stats(c->eng, enable, reset, launches, stepLaunches, stepMs, nullptr, nullptr);
+        // summed over the lanes
+        long long la = 0, sl = 0;
+        double ms = 0.0;
+        for (int k = 0; k <= (int)c->extra.size(); k++) {
+            long long a = 0, b = 0;
+            double m = 0.0;
+            engine_stats(lane_engine(c, k), enable, reset, &a, &b, &m, nullptr, nullptr);
+            la += a; sl += b; ms += m;
+        }
+        if (launches) *launches = la;
+        if (stepLaunches) *stepLaunches = sl;
+        if (stepMs) *stepMs = ms;
     });
 }
 EIO_API int eio_reduce64(int device, int op, int dtype, const void* x, const void* y, long long n, int onDevice,
@@ -556,6 +650,51 @@ EIO_API int eio_reduce64(int device, int op, int dtype, const void* x, const voi
     return guarded([&] {
         if (!result) throw Error(EIO_ERR_ARG, "null result");
         *result = reduce64(device, op, dtype, x, y, n, onDevice != 0);
+    });
+}
+EIO_API int eio_ctx_set_lanes(eio_ctx* c, int lanes) {
+    return guarded([&] {
+        if (!c) throw Error(EIO_ERR_ARG, "null context");
+        if (lanes < 1 || lanes > 8) throw Error(EIO_ERR_ARG, "lanes must be 1 .. 8");
+        c->lanes = lanes;
+        while ((int)c->extra.size() > lanes - 1) {   // release the lanes beyond the new count
+            engine_destroy(c->extra.back());
+            c->extra.pop_back();
+        }
+    });
+}
+EIO_API int eio_ctx_get_lanes(const eio_ctx* c, int* lanes, int* active) {
+    return guarded([&] {
+        if (!c) throw Error(EIO_ERR_ARG, "null context");
+        if (lanes) *lanes = c->lanes;
+        if (active) *active = 1 + (int)c->extra.size();
+    });
+}
+static ShotGeom make_geom(const int* const srcPos[4], const int nSrc[4], const int* const recPos[4],
+                          const int nRec[4]);
+EIO_API int eio_born_shots_dev(eio_ctx* c, int adj, int nShots, float* const* srcDtw, float* const dm[5],
+                               float* const* data, const int* const* srcPos, const int* nSrc,
+                               const int* const* recPos, const int* nRec) {
+    return guarded([&] {
+        if (!c || !srcDtw || !dm || !data || !srcPos || !nSrc || !recPos || !nRec || nShots < 1)
+            throw Error(EIO_ERR_ARG, "null argument");
+        const int nl = ensure_lanes(c, nShots, lane_bytes(c, true));
+        std::vector<float*> lane_dm((size_t)5 * nl);
+        for (int k = 0; k < nl; k++) {
+            if (adj && k > 0) {   // the other lanes image into their own buffers, added below
+                engine_dm_zero(lane_engine(c, k));
+                engine_dm_ptrs(lane_engine(c, k), lane_dm.data() + 5 * k);
+            } else {
+                for (int f = 0; f < 5; f++) lane_dm[5 * k + f] = dm[f];
+            }
+        }
+        run_lanes(c, nl, nShots, [&](int k, Engine* eng, int s) {
+            engine_born(eng, adj, srcDtw + 5 * (size_t)s, lane_dm.data() + 5 * k, data + 5 * (size_t)s,
+                        make_geom(srcPos + 4 * (size_t)s, nSrc + 4 * (size_t)s, recPos + 4 * (size_t)s,
+                                  nRec + 4 * (size_t)s));
+        });
+        if (adj)
+            for (int k = 1; k < nl; k++) engine_dm_add(lane_engine(c, k), dm);
     });
 }
 EIO_API int eio_ctx_set_shot_windows(eio_ctx* c, int nShots, const int* ix0, const int* nxw) {
@@ -576,12 +715,22 @@ EIO_API int eio_ctx_set_graphs(eio_ctx* c, int enable) {
     return guarded([&] {
         if (!c) throw Error(EIO_ERR_ARG, "null context");
         engine_set_graphs(c->eng, enable);
+        for (Engine* e : c->extra) engine_set_graphs(e, enable);
     });
 }
 EIO_API int eio_ctx_pair_stats(eio_ctx* c, long long* pairLaunches, double* pairMs) {
     return guarded([&] {
         if (!c) throw Error(EIO_ERR_ARG, "null context");
-        engine_stats(c->eng, -1, 0, nullptr, nullptr, nullptr, pairLaunches, pairMs);
+        long long pl = 0;
+        double pm = 0.0;
+        for (int k = 0; k <= (int)c->extra.size(); k++) {
+            long long a = 0;
+            double m = 0.0;
+            engine_stats(lane_engine(c, k), -1, 0, nullptr, nullptr, nullptr, &a, &m);
+            pl += a; pm += m;
+        }
+        if (pairLaunches) *pairLaunches = pl;
+        if (pairMs) *pairMs = pm;
     });
 }
 
@@ -701,9 +850,10 @@ ShotGeom reg_geom(const ShotGrids& g) {
 // whole grid comes back when the guard goes.
 struct ShotWindow {
     eio_ctx* c;
+    Engine* eng;
     std::vector<int> pos[8];
     ShotGeom sg;
-    ShotWindow(eio_ctx* ctx, const ShotGrids& g, int shot, int nShots) : c(ctx) {
+    ShotWindow(eio_ctx* ctx, Engine* lane, const ShotGrids& g, int shot, int nShots) : c(ctx), eng(lane) {
         sg = reg_geom(g);
         if (c->win_nx.empty()) return;
         if ((int)c->win_nx.size() != nShots)
@@ -725,11 +875,11 @@ struct ShotWindow {
             if (k < 4) sg.srcPos[k] = pos[k].data();
             else sg.recPos[k - 4] = pos[k].data();
         }
-        engine_set_window(c->eng, ix0, nxw);
+        engine_set_window(eng, ix0, nxw);
     }
     ~ShotWindow() {
         if (!c->win_nx.empty()) {
-            try { engine_set_window(c->eng, 0, 0); } catch (...) {}
+            try { engine_set_window(eng, 0, 0); } catch (...) {}
         }
     }
     ShotWindow(const ShotWindow&) = delete;
@@ -747,8 +897,8 @@ void check_nt(const ShotGrids& g, int nts) {
 
 // nonlinearPropElasticGpu::forward with add = false: irregular source -> data slice;
 // wfld (host [nts][5][nx][nz]) receives the saved wavefield when not null
-void nl_shot_forward(eio_ctx* c, const ShotGrids& g, const ShotGeom& sg, const float* model, float* data,
-                     float* wfld = nullptr) {
+void nl_shot_forward(eio_ctx* c, Engine* eng, const ShotGrids& g, const ShotGeom& sg, const float* model,
+                     float* data, float* wfld = nullptr) {
     const int nts = c->fd.p.nts;
     const int nsi = g.s[0]->nIrreg;
     std::vector<float> reg[5];
@@ -761,7 +911,7 @@ void nl_shot_forward(eio_ctx* c, const ShotGrids& g, const ShotGeom& sg, const f
     scale_sources(c->fd, g, reg, nts);
     for (int f = 0; f < 5; f++) mp[f] = reg[f].data();
     // receivers are interpolated to the devices on the GPU (same sums as sinterp_forward)
-    engine_nl_shot(c->eng, 0, mp, sg, g.r, data, wfld);
+    engine_nl_shot(eng, 0, mp, sg, g.r, data, wfld);
 }
 
 // The adjoint wavefield is scaled like the adjoint sources
@@ -783,8 +933,8 @@ static void scale_adjoint_wavefield(const FdParam& fd, float* w) {
 }
 
 // nonlinearPropElasticGpu::adjoint with add = true into model; wfld as for nl_shot_forward
-void nl_shot_adjoint(eio_ctx* c, const ShotGrids& g, const ShotGeom& sg, float* model, const float* data,
-                     float* wfld = nullptr) {
+void nl_shot_adjoint(eio_ctx* c, Engine* eng, const ShotGrids& g, const ShotGeom& sg, float* model,
+                     const float* data, float* wfld = nullptr) {
     const int nts = c->fd.p.nts;
     const int nsi = g.s[0]->nIrreg;
     std::vector<float> reg[5];
@@ -794,7 +944,7 @@ void nl_shot_adjoint(eio_ctx* c, const ShotGrids& g, const ShotGeom& sg, float* 
         mp[f] = reg[f].data();
     }
     // the data are spread onto the regular grid on the GPU (same sums as sinterp_adjoint)
-    engine_nl_shot(c->eng, 1, mp, sg, g.r, const_cast<float*>(data), wfld);
+    engine_nl_shot(eng, 1, mp, sg, g.r, const_cast<float*>(data), wfld);
     if (wfld) scale_adjoint_wavefield(c->fd, wfld);
     scale_sources_adj(c->fd, g, reg, nts);
     for (int f = 0; f < 5; f++) sinterp_forward(*g.s[kFG[f]], true, reg[f].data(), model + (size_t)f * nsi * nts);
@@ -903,19 +1053,22 @@ static int nl_forward_impl(eio_ctx* c, int add, int nExp, int nModelExp, const f
         const size_t dslice = (size_t)5 * g0.r[0]->nIrreg * nts;
         const size_t mslice = (size_t)5 * g0.s[0]->nIrreg * nts;
         if (!add) std::fill(data, data + dslice * nExp, 0.f);
-        std::vector<float> tmp(dslice);
         for (int e = 0; e < nExp; e++) {
             ShotGrids g = shot_grids(src, rec, nRecGeom, e);
             check_nt(g, nts);
             if ((size_t)5 * g.s[0]->nIrreg * nts != mslice || (size_t)5 * g.r[0]->nIrreg * nts != dslice)
                 throw Error(EIO_ERR_ARG, "device counts differ between shots");
-            ShotWindow win(c, g, e, nExp);
-            nl_shot_forward(c, g, win.sg, model + (nModelExp == 1 ? 0 : (size_t)e * mslice), tmp.data(),
+        }
+        const int nl = ensure_lanes(c, nExp, lane_bytes(c, false));
+        std::vector<std::vector<float>> tmp(nl, std::vector<float>(dslice));
+        run_lanes(c, nl, nExp, [&](int k, Engine* eng, int e) {
+            ShotGrids g = shot_grids(src, rec, nRecGeom, e);
+            ShotWindow win(c, eng, g, e, nExp);
+            nl_shot_forward(c, eng, g, win.sg, model + (nModelExp == 1 ? 0 : (size_t)e * mslice), tmp[k].data(),
                             e == wShot ? wfld : nullptr);
             float* d = data + (size_t)e * dslice;
-            #pragma omp parallel for schedule(static)
-            for (long long i = 0; i < (long long)dslice; i++) d[i] += tmp[i];
-        }
+            for (size_t i = 0; i < dslice; i++) d[i] += tmp[k][i];
+        });
     });
 }
 
@@ -930,25 +1083,33 @@ static int nl_adjoint_impl(eio_ctx* c, int add, int nExp, int nModelExp, float* 
         const size_t dslice = (size_t)5 * g0.r[0]->nIrreg * nts;
         const size_t mslice = (size_t)5 * g0.s[0]->nIrreg * nts;
         if (!add) std::fill(model, model + mslice * nModelExp, 0.f);
-        std::vector<float> slice(mslice, 0.f);
         for (int e = 0; e < nExp; e++) {
             ShotGrids g = shot_grids(src, rec, nRecGeom, e);
             check_nt(g, nts);
             if ((size_t)5 * g.s[0]->nIrreg * nts != mslice || (size_t)5 * g.r[0]->nIrreg * nts != dslice)
                 throw Error(EIO_ERR_ARG, "device counts differ between shots");
-            ShotWindow win(c, g, e, nExp);
-            if (nModelExp == 1) {
-                // constant source signal: stack every shot (nonlinearPropElasticShotsGpu.cpp:384-417)
-                nl_shot_adjoint(c, g, win.sg, slice.data(), data + (size_t)e * dslice, e == wShot ? wfld : nullptr);
-            } else {
-                std::fill(slice.begin(), slice.end(), 0.f);
-                nl_shot_adjoint(c, g, win.sg, slice.data(), data + (size_t)e * dslice, e == wShot ? wfld : nullptr);
-                float* m = model + (size_t)e * mslice;
-                for (size_t i = 0; i < mslice; i++) m[i] += slice[i];
-            }
         }
+        const int nl = ensure_lanes(c, nExp, lane_bytes(c, false));
+        // constant source signal: every shot stacks into one model (nonlinearPropElasticShotsGpu.cpp:384-417),
+        // here one partial stack per lane, added in lane order
+        std::vector<std::vector<float>> slice(nl, std::vector<float>(mslice, 0.f));
+        run_lanes(c, nl, nExp, [&](int k, Engine* eng, int e) {
+            ShotGrids g = shot_grids(src, rec, nRecGeom, e);
+            ShotWindow win(c, eng, g, e, nExp);
+            if (nModelExp == 1) {
+                nl_shot_adjoint(c, eng, g, win.sg, slice[k].data(), data + (size_t)e * dslice,
+                                e == wShot ? wfld : nullptr);
+            } else {
+                std::fill(slice[k].begin(), slice[k].end(), 0.f);
+                nl_shot_adjoint(c, eng, g, win.sg, slice[k].data(), data + (size_t)e * dslice,
+                                e == wShot ? wfld : nullptr);
+                float* m = model + (size_t)e * mslice;
+                for (size_t i = 0; i < mslice; i++) m[i] += slice[k][i];
+            }
+        });
         if (nModelExp == 1)
-            for (size_t i = 0; i < mslice; i++) model[i] += slice[i];
+            for (int k = 0; k < nl; k++)
+                for (size_t i = 0; i < mslice; i++) model[i] += slice[k][i];
     });
 }
 
@@ -998,22 +1159,25 @@ EIO_API int eio_born_forward(eio_ctx* c, int add, int nExp, const float* model, 
         born_model_slice(c->fd, model, sl);
         float* dm[5];
         for (int f = 0; f < 5; f++) dm[f] = sl[f].data();
-        engine_dm_upload(c->eng, dm);        // stays on the device for every shot
-        std::vector<float> tmp(dslice);
         for (int e = 0; e < nExp; e++) {
             ShotGrids g = shot_grids(src, rec, nRecGeom, e);
             check_nt(g, nts);
             if ((size_t)5 * g.r[0]->nIrreg * nts != dslice) throw Error(EIO_ERR_ARG, "receiver counts differ");
+        }
+        const int nl = ensure_lanes(c, nExp, lane_bytes(c, true));
+        for (int k = 0; k < nl; k++) engine_dm_upload(lane_engine(c, k), dm);   // stays on the device for every shot
+        std::vector<std::vector<float>> tmp(nl, std::vector<float>(dslice));
+        run_lanes(c, nl, nExp, [&](int k, Engine* eng, int e) {
+            ShotGrids g = shot_grids(src, rec, nRecGeom, e);
             std::vector<float> fine[5];
             born_sources(c, g, sigs[nSignals == 1 ? 0 : e], fine);
             float* sp[5];
             for (int f = 0; f < 5; f++) sp[f] = fine[f].data();
-            ShotWindow win(c, g, e, nExp);
-            engine_born_shot(c->eng, 0, sp, win.sg, g.r, tmp.data());
+            ShotWindow win(c, eng, g, e, nExp);
+            engine_born_shot(eng, 0, sp, win.sg, g.r, tmp[k].data());
             float* d = data + (size_t)e * dslice;
-#pragma omp parallel for schedule(static)
-            for (long long i = 0; i < (long long)dslice; i++) d[i] += tmp[i];
-        }
+            for (size_t i = 0; i < dslice; i++) d[i] += tmp[k][i];
+        });
     });
 }
 
@@ -1033,17 +1197,27 @@ EIO_API int eio_born_adjoint(eio_ctx* c, int add, int nExp, float* model, const 
         std::vector<float> sl[5];
         float* dm[5];
         for (int f = 0; f < 5; f++) { sl[f].assign(n, 0.f); dm[f] = sl[f].data(); }
-        engine_dm_zero(c->eng);              // every shot's image accumulates on the device
         for (int e = 0; e < nExp; e++) {
             ShotGrids g = shot_grids(src, rec, nRecGeom, e);
             check_nt(g, nts);
             if ((size_t)5 * g.r[0]->nIrreg * nts != dslice) throw Error(EIO_ERR_ARG, "receiver counts differ");
+        }
+        const int nl = ensure_lanes(c, nExp, lane_bytes(c, true));
+        for (int k = 0; k < nl; k++) engine_dm_zero(lane_engine(c, k));   // each lane's shots accumulate on its device
+        run_lanes(c, nl, nExp, [&](int, Engine* eng, int e) {
+            ShotGrids g = shot_grids(src, rec, nRecGeom, e);
             std::vector<float> fine[5];
             born_sources(c, g, sigs[nSignals == 1 ? 0 : e], fine);
             float* sp[5];
             for (int f = 0; f < 5; f++) sp[f] = fine[f].data();
-            ShotWindow win(c, g, e, nExp);
-            engine_born_shot(c->eng, 1, sp, win.sg, g.r, const_cast<float*>(data) + (size_t)e * dslice);
+            ShotWindow win(c, eng, g, e, nExp);
+            engine_born_shot(eng, 1, sp, win.sg, g.r, const_cast<float*>(data) + (size_t)e * dslice);
+        });
+        // the lanes' images, added in lane order on the first lane's device
+        if (nl > 1) {
+            float* d0[5];
+            engine_dm_ptrs(c->eng, d0);
+            for (int k = 1; k < nl; k++) engine_dm_add(lane_engine(c, k), d0);
         }
         engine_dm_download(c->eng, dm);
         // scaling and un-staggering, BornElasticShotsGpu.cpp:325-371

@@ -72,6 +72,12 @@ void* engine_stream(Engine* e);
 // launch statistics: enable = 1/0 (-1 leaves it), reset = 1 zeroes the counters after reading
 void engine_set_graphs(Engine* e, int enable);
 void engine_set_window(Engine* e, int ix0, int nxw);   // nxw = 0: the whole grid
+bool engine_is_tuned(const Engine* e);
+int engine_get_checkpoint(const Engine* e);
+int engine_get_graphs(const Engine* e);
+size_t engine_cells(const Engine* e);
+void engine_dm_ptrs(Engine* e, float* out[5]);          // this lane's own image buffers
+void engine_dm_add(Engine* e, float* const dst[5]);     // dst += this lane's image (device)
 int engine_window_ix0(const Engine* e);
 // FP64 sum of x*y (op 0) or (x-y)^2 (op 1) over n values (dtype 0 FP32, 1 FP64) on GPU `device`
 double reduce64(int device, int op, int dtype, const void* x, const void* y, long long n, bool on_device);

@@ -156,6 +156,27 @@ int eio_ctx_autotune(eio_ctx *c, int *kind, int *tz, int *cw, int *cpr);
  * enable: 1 on, 0 off, -1 unchanged; reset: zero the counters after reading. */
 int eio_ctx_stats(eio_ctx *c, int enable, int reset, long long *launches, long long *stepLaunches,
                   double *stepMs);
+/* Shot lanes (no reference counterpart; the reference runs one shot per GPU at
+ * a time). The multi-shot operators (eio_nl_forward/adjoint,
+ * eio_born_forward/adjoint, eio_born_shots_dev) run their shots on up to
+ * `lanes` engines of the same GPU concurrently. Each lane has its own
+ * streams, wavefields and Born history. Lane k takes shots k, k + n, ... in
+ * order, and the lanes' images and stacked adjoint sources are added in lane
+ * order, so results do not depend on timing. A new lane is created only while
+ * the free device memory holds its buffers (for Born, the source-wavefield
+ * history). Default 2, range 1 .. 8; lowering the count releases lanes.
+ * eio_ctx_get_lanes reports the setting and the lanes that exist. */
+int eio_ctx_set_lanes(eio_ctx *c, int lanes);
+int eio_ctx_get_lanes(const eio_ctx *c, int *lanes, int *active);
+/* Many Born shots with device-resident inputs (no reference counterpart).
+ * Shot s: fine-time regular sources srcDtw[5*s + f] and receiver traces
+ * data[5*s + f] (device pointers, as eio_born_fwd_reg_dev), positions
+ * srcPos[4*s + k] / nSrc[4*s + k] and recPos[4*s + k] / nRec[4*s + k] (host).
+ * dm[5]: the device perturbation (adj = 0) or the device image every shot
+ * adds into (adj = 1). The shots run on the context's lanes. */
+int eio_born_shots_dev(eio_ctx *c, int adj, int nShots, float *const *srcDtw, float *const dm[5],
+                       float *const *data, const int *const *srcPos, const int *nSrc,
+                       const int *const *recPos, const int *nRec);
 /* Cropped shots (no reference counterpart; the reference propagates every shot
  * on the whole grid). Shot i of the next multi-shot calls (eio_nl_forward,
  * eio_nl_adjoint, eio_born_forward, eio_born_adjoint with nExp == nShots)
