@@ -378,7 +378,15 @@ struct eio_ctx {
     // run shots of a multi-shot call concurrently with eng (eio_ctx_set_lanes)
     std::vector<Engine*> extra;
     int lanes = 2;
+    std::vector<std::vector<float>> lane_tmp;   // per-lane host staging of one shot's data (kept across calls)
 };
+
+// lane k's staging buffer of at least n floats (contents undefined)
+static float* lane_staging(eio_ctx* c, int k, size_t n) {
+    if ((int)c->lane_tmp.size() <= k) c->lane_tmp.resize(k + 1);
+    if (c->lane_tmp[k].size() < n) c->lane_tmp[k].resize(n);
+    return c->lane_tmp[k].data();
+}
 
 static Engine* lane_engine(eio_ctx* c, int k) { return k == 0 ? c->eng : c->extra[k - 1]; }
 
@@ -1052,7 +1060,6 @@ static int nl_forward_impl(eio_ctx* c, int add, int nExp, int nModelExp, const f
         ShotGrids g0 = shot_grids(src, rec, nRecGeom, 0);
         const size_t dslice = (size_t)5 * g0.r[0]->nIrreg * nts;
         const size_t mslice = (size_t)5 * g0.s[0]->nIrreg * nts;
-        if (!add) std::fill(data, data + dslice * nExp, 0.f);
         for (int e = 0; e < nExp; e++) {
             ShotGrids g = shot_grids(src, rec, nRecGeom, e);
             check_nt(g, nts);
@@ -1060,14 +1067,20 @@ static int nl_forward_impl(eio_ctx* c, int add, int nExp, int nModelExp, const f
                 throw Error(EIO_ERR_ARG, "device counts differ between shots");
         }
         const int nl = ensure_lanes(c, nExp, lane_bytes(c, false));
-        std::vector<std::vector<float>> tmp(nl, std::vector<float>(dslice));
+        std::vector<float*> tmp(nl);
+        for (int k = 0; k < nl; k++) tmp[k] = add ? lane_staging(c, k, dslice) : nullptr;
         run_lanes(c, nl, nExp, [&](int k, Engine* eng, int e) {
             ShotGrids g = shot_grids(src, rec, nRecGeom, e);
             ShotWindow win(c, eng, g, e, nExp);
-            nl_shot_forward(c, eng, g, win.sg, model + (nModelExp == 1 ? 0 : (size_t)e * mslice), tmp[k].data(),
-                            e == wShot ? wfld : nullptr);
             float* d = data + (size_t)e * dslice;
-            for (size_t i = 0; i < dslice; i++) d[i] += tmp[k][i];
+            // add = false: straight into the shot's slice; add = true: staged, then added
+            nl_shot_forward(c, eng, g, win.sg, model + (nModelExp == 1 ? 0 : (size_t)e * mslice), add ? tmp[k] : d,
+                            e == wShot ? wfld : nullptr);
+            if (add) {
+                const float* t = tmp[k];
+#pragma omp parallel for schedule(static)
+                for (long long i = 0; i < (long long)dslice; i++) d[i] += t[i];
+            }
         });
     });
 }
@@ -1104,12 +1117,17 @@ static int nl_adjoint_impl(eio_ctx* c, int add, int nExp, int nModelExp, float* 
                 nl_shot_adjoint(c, eng, g, win.sg, slice[k].data(), data + (size_t)e * dslice,
                                 e == wShot ? wfld : nullptr);
                 float* m = model + (size_t)e * mslice;
-                for (size_t i = 0; i < mslice; i++) m[i] += slice[k][i];
+                const float* sk = slice[k].data();
+#pragma omp parallel for schedule(static)
+                for (long long i = 0; i < (long long)mslice; i++) m[i] += sk[i];
             }
         });
         if (nModelExp == 1)
-            for (int k = 0; k < nl; k++)
-                for (size_t i = 0; i < mslice; i++) model[i] += slice[k][i];
+            for (int k = 0; k < nl; k++) {
+                const float* sk = slice[k].data();
+#pragma omp parallel for schedule(static)
+                for (long long i = 0; i < (long long)mslice; i++) model[i] += sk[i];
+            }
     });
 }
 
@@ -1154,8 +1172,7 @@ EIO_API int eio_born_forward(eio_ctx* c, int add, int nExp, const float* model, 
         const int nts = c->fd.p.nts;
         ShotGrids g0 = shot_grids(src, rec, nRecGeom, 0);
         const size_t dslice = (size_t)5 * g0.r[0]->nIrreg * nts;
-        if (!add) std::fill(data, data + dslice * nExp, 0.f);
-        std::vector<float> sl[5];
+        std::vector<float> sl[5];   // add = false: each shot's slice is written whole below
         born_model_slice(c->fd, model, sl);
         float* dm[5];
         for (int f = 0; f < 5; f++) dm[f] = sl[f].data();
@@ -1166,7 +1183,8 @@ EIO_API int eio_born_forward(eio_ctx* c, int add, int nExp, const float* model, 
         }
         const int nl = ensure_lanes(c, nExp, lane_bytes(c, true));
         for (int k = 0; k < nl; k++) engine_dm_upload(lane_engine(c, k), dm);   // stays on the device for every shot
-        std::vector<std::vector<float>> tmp(nl, std::vector<float>(dslice));
+        std::vector<float*> tmp(nl);
+        for (int k = 0; k < nl; k++) tmp[k] = add ? lane_staging(c, k, dslice) : nullptr;
         run_lanes(c, nl, nExp, [&](int k, Engine* eng, int e) {
             ShotGrids g = shot_grids(src, rec, nRecGeom, e);
             std::vector<float> fine[5];
@@ -1174,9 +1192,13 @@ EIO_API int eio_born_forward(eio_ctx* c, int add, int nExp, const float* model, 
             float* sp[5];
             for (int f = 0; f < 5; f++) sp[f] = fine[f].data();
             ShotWindow win(c, eng, g, e, nExp);
-            engine_born_shot(eng, 0, sp, win.sg, g.r, tmp[k].data());
             float* d = data + (size_t)e * dslice;
-            for (size_t i = 0; i < dslice; i++) d[i] += tmp[k][i];
+            engine_born_shot(eng, 0, sp, win.sg, g.r, add ? tmp[k] : d);
+            if (add) {
+                const float* t = tmp[k];
+#pragma omp parallel for schedule(static)
+                for (long long i = 0; i < (long long)dslice; i++) d[i] += t[i];
+            }
         });
     });
 }
