@@ -656,20 +656,25 @@ template <int DIR, int EPI>
 static void launch_step(Engine* e, StepArgs& a, int cur) {
     const bool timed = e->stats && (e->step_launches + e->pair_launches) % STATS_PERIOD == 0;
     if (timed) stats_mark(e);
-    const int kind = eff_kind(e);
-    bool done = false;
-    if constexpr (EPI == EPI_NONE) {   // the nonlinear operators are the only ones with a free surface
-        if (e->fs_active) {
-            launch_pdl(k_step<DIR, EPI, 3, true>, e->ntiles, NT, e->st, a);
-            done = true;
+    if constexpr (EPI >= EPI_TRI_IMG) {   // the fused imaging condition is built into k_step only
+        // 3 CTAs per SM; 2 for the 16-bit histories, whose decoding would spill at 80 registers
+        launch_pdl(k_step<DIR, EPI, EPI == EPI_TRI_IMG ? 3 : 2>, e->ntiles, NT, e->st, a);
+    } else {
+        const int kind = eff_kind(e);
+        bool done = false;
+        if constexpr (EPI == EPI_NONE) {   // the nonlinear operators are the only ones with a free surface
+            if (e->fs_active) {
+                launch_pdl(k_step<DIR, EPI, 3, true>, e->ntiles, NT, e->st, a);
+                done = true;
+            }
         }
+        if (done) {
+        } else if (kind == 0) launch_pdl(k_step<DIR, EPI, 3>, e->ntiles, NT, e->st, a);
+        else if (kind == 2) launch_tile<DIR, EPI>(e, a, cur);
+        else if (kind == 3 || kind == 5) launch_pdl(k_step<DIR, EPI, 4>, e->ntiles, NT, e->st, a);
+        else if (kind == 4) launch_pdl(k_split<DIR, EPI>, e->ntiles, NT2, e->st, a);
+        else launch_sweep<DIR, EPI>(e, a, cur);
     }
-    if (done) {
-    } else if (kind == 0) launch_pdl(k_step<DIR, EPI, 3>, e->ntiles, NT, e->st, a);
-    else if (kind == 2) launch_tile<DIR, EPI>(e, a, cur);
-    else if (kind == 3 || kind == 5) launch_pdl(k_step<DIR, EPI, 4>, e->ntiles, NT, e->st, a);
-    else if (kind == 4) launch_pdl(k_split<DIR, EPI>, e->ntiles, NT2, e->st, a);
-    else launch_sweep<DIR, EPI>(e, a, cur);
     if (timed) {
         stats_mark(e);
         e->sampled++;
@@ -1157,21 +1162,30 @@ void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], 
     err_check(e);
 }
 
+// the source-wavefield history of the current shot (FP32 or 16-bit codes)
+static WHist whist(const Engine* e) {
+    WHist h;
+    memset(&h, 0, sizeof(h));
+    if (e->ckpt) {
+        const unsigned short* wq = static_cast<const unsigned short*>(e->Wq.p);
+        h.Wvx = wq;
+        h.Wvz = wq + (long long)e->nts * e->n;
+        h.wscale = e->wscale.f();
+    } else {
+        h.Wvx = e->W.f();
+        h.Wvz = e->W.f() + (long long)e->nts * e->n;
+    }
+    h.wstride = e->n;
+    h.nts = e->nts;
+    return h;
+}
+
 static void launch_imaging(Engine* e, int adj, int its, float* const dm[5], float* const ss[5],
                            cudaStream_t st) {
     ImagingArgs ia;
     memset(&ia, 0, sizeof(ia));
-    if (e->ckpt) {
-        const unsigned short* wq = static_cast<const unsigned short*>(e->Wq.p);
-        ia.Wvx = wq;
-        ia.Wvz = wq + (long long)e->nts * e->n;
-        ia.wscale = e->wscale.f();
-    } else {
-        ia.Wvx = e->W.f();
-        ia.Wvz = e->W.f() + (long long)e->nts * e->n;
-    }
-    ia.wstride = e->n;
-    ia.nz = e->nz; ia.nx = e->nx; ia.nts = e->nts; ia.its = its;
+    ia.h = whist(e);
+    ia.nz = e->nz; ia.nx = e->nx; ia.its = its;
     for (int i = 0; i < 4; i++) { ia.cz[i] = e->zc[i]; ia.cx[i] = e->xc[i]; }
     ia.dts_inv = e->dts_inv;
     for (int f = 0; f < 5; f++) { ia.dm[f] = dm[f]; ia.ss[f] = ss[f]; }
@@ -1496,6 +1510,19 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
         auto weights = [&](StepArgs& x, int its, int it2) {
             x.inj.t0 = its; x.inj.w0 = F[it2 + 1]; x.inj.w1 = F[h + it2 + 1];
         };
+        // single steps image inside the sample step (EPI_TRI_IMG): the adjoint sample
+        // never leaves the registers.  That step is a k_step, so the point lists must
+        // use its tiles (not the sweep kernel's); the two-step kernel keeps the sample ring
+        const bool fuse_img = !use_pair && tiled(eff_kind(e));
+        const WHist wh = whist(e);
+        auto fused = [&](StepArgs& x, int T, int mode, float wo, float wc, float wn) {
+            x.tmode = mode; x.tw_o = wo; x.tw_c = wc; x.tw_n = wn;
+            x.wh = wh; x.img_its = T; x.dts_inv = e->dts_inv;
+            for (int f = 0; f < 5; f++) x.img[f] = dm[f];
+            if (e->ckpt == 0) launch_step<1, EPI_TRI_IMG>(e, x, cur);
+            else if (e->ckpt == 1) launch_step<1, EPI_TRI_IMG + 1>(e, x, cur);
+            else launch_step<1, EPI_TRI_IMG + 2>(e, x, cur);
+        };
         key.add(&a, sizeof(a));
         key.add(&injh, sizeof(injh));
         run_graph(e, key.h, nsteps, [&] {
@@ -1516,13 +1543,21 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
                 L.set(a);
                 weights(a, its, it2);
                 if (it2 == 1) {
-                    tri(a, its + 1, 1, F[1], F[0], F[h + 1]);
-                    launch_step<1, EPI_TRI>(e, a, cur);
-                    imaging(its + 1);
+                    if (fuse_img) {
+                        fused(a, its + 1, 1, F[1], F[0], F[h + 1]);
+                    } else {
+                        tri(a, its + 1, 1, F[1], F[0], F[h + 1]);
+                        launch_step<1, EPI_TRI>(e, a, cur);
+                        imaging(its + 1);
+                    }
                 } else if (its == 0) {   // sample 0 = p(1) f[1] + p(0) f[0]
-                    tri(a, 0, 2, 0.f, F[1], F[0]);
-                    launch_step<1, EPI_TRI>(e, a, cur);
-                    imaging(0);
+                    if (fuse_img) {
+                        fused(a, 0, 2, 0.f, F[1], F[0]);
+                    } else {
+                        tri(a, 0, 2, 0.f, F[1], F[0]);
+                        launch_step<1, EPI_TRI>(e, a, cur);
+                        imaging(0);
+                    }
                 } else {
                     launch_step<1, EPI_NONE>(e, a, cur);
                 }

@@ -59,6 +59,14 @@ struct SparseOp {
     float w0, w1;             // time-interpolation weights for rows t0, t0+1
 };
 
+// source-wavefield history (coarse Vx / Vz snapshots)
+struct WHist {
+    const void* Wvx; const void* Wvz;     // float, or 16-bit codes for Q = 1 (BF16) / 2 (FP16)
+    const float* wscale;                  // Q > 0: [nts][2] scale of every snapshot (vx, vz)
+    long long wstride;
+    int nts;
+};
+
 struct StepArgs {
     float* o[5];              // old level, overwritten with the new level
     const float* c[5];        // current level
@@ -91,11 +99,19 @@ struct StepArgs {
     // the sigmaxx coefficient on the surface row
     int fs;
     const float* fsc;
+    // EPI_TRI_IMG (adjoint, k_step only): the coarse adjoint sample of this step
+    // goes straight into the imaging condition of coarse sample img_its against
+    // the history wh, accumulated into img[5]; no sample buffer is written
+    WHist wh;
+    int img_its;
+    float dts_inv;
+    float* img[5];
 };
 
 constexpr int SURF = 2 * FAT;   // free-surface row
 
-enum { EPI_NONE = 0, EPI_SAVE_W = 1, EPI_INJ_SS = 2, EPI_EXT_SS = 3, EPI_TRI = 4 };
+enum { EPI_NONE = 0, EPI_SAVE_W = 1, EPI_INJ_SS = 2, EPI_EXT_SS = 3, EPI_TRI = 4, EPI_TRI_IMG = 5 };
+// EPI_TRI_IMG + Q: the history holds FP32 (Q = 0), BF16 (1) or FP16 (2) snapshots
 
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
@@ -283,6 +299,106 @@ __device__ __forceinline__ void adj_products(float4 vx, float4 vz, float4 sxx, f
     }
 }
 
+// Four consecutive history values of snapshot `its` at cell index i (float4
+// aligned) of field f (0 vx, 1 vz): FP32, or 16-bit codes times the snapshot scale.
+template <int Q>
+__device__ __forceinline__ float4 ldw(const WHist& a, int f, int its, long long i)
+{
+    const long long k = (long long)its * a.wstride + i;
+    const void* base = f ? a.Wvz : a.Wvx;
+    if (Q == 0) return ldg4(static_cast<const float*>(base) + k);
+    const uint2 u = __ldg(reinterpret_cast<const uint2*>(static_cast<const unsigned short*>(base) + k));
+    const float s = __ldg(a.wscale + 2 * its + f);
+    const unsigned h[4] = {u.x & 0xffffu, u.x >> 16, u.y & 0xffffu, u.y >> 16};
+    float4 r;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        float v;
+        if (Q == 1) v = __uint_as_float(h[j] << 16);                       // BF16: upper half of a float
+        else v = __half2float(__ushort_as_half((unsigned short)h[j]));     // FP16
+        at(r, j) = v * s;
+    }
+    return r;
+}
+
+// snapshot `its` (vx, vz) of tile (z0, x0) with its 4-cell halo into sm [2][SX][SZ]; NT threads
+template <int Q>
+__device__ __forceinline__ void stage_snapshot(const WHist& h, int its, int nz, float* sm, int z0, int x0, int tid)
+{
+    const int nq = SZ / 4;
+    for (int q = tid; q < nq * SX; q += NT) {
+        const int lx = q / nq, lz4 = (q % nq) * 4;
+        const int gz = z0 - FAT + lz4, gx = x0 - FAT + lx;
+        float4 u = make_float4(0.f, 0.f, 0.f, 0.f), v = u;
+        if (gz < nz) {
+            const long long gi = (long long)gx * nz + gz;
+            u = ldw<Q>(h, 0, its, gi);
+            v = ldw<Q>(h, 1, its, gi);
+        }
+        st4(sm + lx * SZ + lz4, u);
+        st4(sm + SMEM_FIELD + lx * SZ + lz4, v);
+    }
+}
+
+// The source-wavefield terms of both imaging kernels at the float4 (lx, lz) of a
+// staged snapshot: staggered derivatives of Vx, Vz and their time difference
+// W[its-1] - W[its+1] (one-sided at the ends like the reference).
+struct ImgTerms {
+    float4 dvx_dx, dvx_dz, dvz_dx, dvz_dz, tx, tz;
+};
+template <int Q>
+__device__ __forceinline__ ImgTerms imaging_terms(const WHist& h, const float* sm, int lx, int lz, long long gi,
+                                                  int its, const float* cz, const float* cx)
+{
+    ImgTerms r;
+    const float* svx = sm;
+    const float* svz = sm + SMEM_FIELD;
+    float4 q[9];
+    float w[12];
+#pragma unroll
+    for (int m = 0; m < 9; m++) q[m] = ld4(svx + (lx - FAT + m) * SZ + lz);
+    r.dvx_dx = dpx(q, 4, cx);
+    zwin(svx, lx, lz, w);
+    r.dvx_dz = dmz(w, cz);
+#pragma unroll
+    for (int m = 0; m < 9; m++) q[m] = ld4(svz + (lx - FAT + m) * SZ + lz);
+    r.dvz_dx = dmx(q, 4, cx);
+    zwin(svz, lx, lz, w);
+    r.dvz_dz = dpz(w, cz);
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 xo = its > 0 ? ldw<Q>(h, 0, its - 1, gi) : zero;
+    const float4 zo = its > 0 ? ldw<Q>(h, 1, its - 1, gi) : zero;
+    const float4 xn = its < h.nts - 1 ? ldw<Q>(h, 0, its + 1, gi) : zero;
+    const float4 zn = its < h.nts - 1 ? ldw<Q>(h, 1, its + 1, gi) : zero;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        // one-sided at the ends like the reference: -W[its+1] at its = 0, W[its-1] at nts-1
+        at(r.tx, j) = (its == 0) ? -at(xn, j) : (its == h.nts - 1) ? at(xo, j) : at(xo, j) - at(xn, j);
+        at(r.tz, j) = (its == 0) ? -at(zn, j) : (its == h.nts - 1) ? at(zo, j) : at(zo, j) - at(zn, j);
+    }
+    return r;
+}
+
+// imaging condition (imagingElaAdjGpu, K:1538-1613): the images at gi += the
+// adjoint sample s[5] against the source-wavefield terms
+__device__ __forceinline__ void imaging_accumulate(float* const dm[5], long long gi, const float4 (&s)[5],
+                                                   const ImgTerms& t, float dts_inv)
+{
+    float4 d0 = ld4(dm[0] + gi), d1 = ld4(dm[1] + gi), d2 = ld4(dm[2] + gi), d3 = ld4(dm[3] + gi),
+           d4 = ld4(dm[4] + gi);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const float dvx = at(t.dvx_dx, j), dvz = at(t.dvz_dz, j);
+        at(d0, j) += at(s[0], j) * at(t.tx, j) * dts_inv;
+        at(d1, j) += at(s[1], j) * at(t.tz, j) * dts_inv;
+        at(d2, j) += (at(s[2], j) + at(s[3], j)) * (dvx + dvz);
+        at(d3, j) += 2.0f * (dvx * at(s[2], j) + dvz * at(s[3], j));
+        at(d4, j) += at(s[4], j) * (at(t.dvx_dz, j) + at(t.dvz_dx, j));
+    }
+    st4(dm[0] + gi, d0); st4(dm[1] + gi, d1); st4(dm[2] + gi, d2);
+    st4(dm[3] + gi, d3); st4(dm[4] + gi, d4);
+}
+
 // Everything of one fused fine step after the stencils, for the float4 of
 // thread (tzi, txi) of tile `tile` and the fields F0 <= f < F1: deferred taper
 // of the old level (o(f) returns it), leapfrog sum, scattered-field source,
@@ -295,7 +411,11 @@ __device__ __forceinline__ void step_tail(const StepArgs& a, float* scratch, int
                                           int gz, int gx, bool valid, long long gi, float4 (&t)[5], Old oload,
                                           const float4 (&csave)[2])
 {
+    constexpr bool IMG = EPI >= EPI_TRI_IMG;                 // sample straight into the imaging condition
+    constexpr bool TRI = EPI == EPI_TRI || IMG;
+    static_assert(!IMG || (DIR == 1 && NTHR == NT && F0 == 0 && F1 == 5), "fused imaging: adjoint k_step only");
     float4 osave[5];      // old level (EPI_TRI)
+    float4 smp[5];        // coarse adjoint samples (EPI_TRI_IMG)
     float tri_max[2] = {0.f, 0.f};   // |max| of this thread's coarse samples (16-bit checkpoints)
     float dd[4];
     {
@@ -307,7 +427,7 @@ __device__ __forceinline__ void step_tail(const StepArgs& a, float* scratch, int
 #pragma unroll
         for (int f = F0; f < F1; f++) {
             const float4 o = oload(f);
-            if (EPI == EPI_TRI) osave[f] = o;
+            if (TRI) osave[f] = o;
 #pragma unroll
             for (int j = 0; j < 4; j++) at(t[f], j) = dd[j] * at(o, j) + at(t[f], j);
         }
@@ -418,7 +538,7 @@ __device__ __forceinline__ void step_tail(const StepArgs& a, float* scratch, int
                 st4(a.eL[f] + gi, l); st4(a.eR[f] + gi, r);
             }
         }
-        if (EPI == EPI_TRI && a.tmode) {
+        if (TRI && a.tmode) {
             if (DIR == 0) {
                 if (F0 == 0) {
                     const float4 s0 = tri_sample(a.tmode, osave[0], csave[0], t[0], a.tw_o, a.tw_c, a.tw_n);
@@ -430,8 +550,10 @@ __device__ __forceinline__ void step_tail(const StepArgs& a, float* scratch, int
                 }
             } else {
 #pragma unroll
-                for (int f = F0; f < F1; f++)
-                    st4(a.eL[f] + gi, tri_sample(a.tmode, osave[f], ld4(a.c[f] + gi), t[f], a.tw_o, a.tw_c, a.tw_n));
+                for (int f = F0; f < F1; f++) {
+                    smp[f] = tri_sample(a.tmode, osave[f], ld4(a.c[f] + gi), t[f], a.tw_o, a.tw_c, a.tw_n);
+                    if (!IMG) st4(a.eL[f] + gi, smp[f]);
+                }
             }
         }
     }
@@ -468,6 +590,19 @@ __device__ __forceinline__ void step_tail(const StepArgs& a, float* scratch, int
                 sg[(long long)a.ext.t0 * ld + pe.col] += v * a.ext.w0;
                 sg[(long long)(a.ext.t0 + 1) * ld + pe.col] += v * a.ext.w1;
             }
+        }
+    }
+
+    // ---- imaging condition of coarse sample img_its (EPI_TRI_IMG): the snapshot
+    // with its halo in the scratch, then the same terms as k_imaging<1>
+    if (IMG && a.tmode) {   // uniform over the CTA
+        constexpr int Q = EPI - EPI_TRI_IMG;
+        __syncthreads();   // the scratch is free
+        stage_snapshot<Q>(a.wh, a.img_its, a.nz, scratch, gz - 4 * tzi, gx - txi, tid);
+        __syncthreads();
+        if (valid) {
+            const ImgTerms it = imaging_terms<Q>(a.wh, scratch, FAT + txi, FAT + 4 * tzi, gi, a.img_its, a.cz, a.cx);
+            imaging_accumulate(a.img, gi, smp, it, a.dts_inv);
         }
     }
 }
@@ -540,7 +675,7 @@ __device__ __forceinline__ void stage_tile(const StepArgs& a, float* sm, int z0,
 {
     const int nz = a.nz;
     const int nq = SZ / 4;                        // float4 per shared column
-    if (DIR == 0 && !FS && NTHR == NT) {
+    if constexpr (DIR == 0 && !FS && NTHR == NT) {
         // forward: every load of the thread in flight before the first store
         constexpr int NU = (SZ / 4) * SX;
         constexpr int R = (NU + NT - 1) / NT;
@@ -568,8 +703,7 @@ __device__ __forceinline__ void stage_tile(const StepArgs& a, float* sm, int z0,
                 for (int f = 0; f < 5; f++) st4(sm + f * SMEM_FIELD + lx * SZ + lz4, v[r][f]);
             }
         }
-        return;
-    }
+    } else {
     for (int q = tid; q < nq * SX; q += NTHR) {
         const int lx = q / nq, lz4 = (q % nq) * 4;
         const int gz = z0 - FAT + lz4, gx = x0 - FAT + lx;
@@ -606,6 +740,7 @@ __device__ __forceinline__ void stage_tile(const StepArgs& a, float* sm, int z0,
         }
 #pragma unroll
         for (int f = 0; f < 5; f++) st4(sm + f * SMEM_FIELD + lx * SZ + lz4, v[f]);
+    }
     }
 }
 
@@ -706,10 +841,8 @@ __global__ void __launch_bounds__(NT2, 2) k_split(StepArgs a)
 // One thread per interior cell; W holds coarse Vx/Vz snapshots [nts][nx*nz].
 // ---------------------------------------------------------------------------
 struct ImagingArgs {
-    const void* Wvx; const void* Wvz;     // float, or 16-bit codes for Q = 1 (BF16) / 2 (FP16)
-    const float* wscale;                  // Q > 0: [nts][2] scale of every snapshot (vx, vz)
-    long long wstride;
-    int nz, nx, nts, its;
+    WHist h;
+    int nz, nx, its;
     float cz[4], cx[4];
     float dts_inv;
     float* dm[5];   // fwd: read; adj: accumulated
@@ -721,28 +854,6 @@ struct ImagingArgs {
 // coarse sample its.  64x16-cell tiles, 256 threads (one float4 of z x one column
 // each); the snapshot at its is staged with its 4-cell halo in shared memory for
 // the staggered derivatives, the neighbouring snapshots give the time difference.
-// Four consecutive history values of snapshot `its` at cell index i (float4
-// aligned) of field f (0 vx, 1 vz): FP32, or 16-bit codes times the snapshot scale.
-template <int Q>
-__device__ __forceinline__ float4 ldw(const ImagingArgs& a, int f, int its, long long i)
-{
-    const long long k = (long long)its * a.wstride + i;
-    const void* base = f ? a.Wvz : a.Wvx;
-    if (Q == 0) return ldg4(static_cast<const float*>(base) + k);
-    const uint2 u = __ldg(reinterpret_cast<const uint2*>(static_cast<const unsigned short*>(base) + k));
-    const float s = __ldg(a.wscale + 2 * its + f);
-    const unsigned h[4] = {u.x & 0xffffu, u.x >> 16, u.y & 0xffffu, u.y >> 16};
-    float4 r;
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        float v;
-        if (Q == 1) v = __uint_as_float(h[j] << 16);                       // BF16: upper half of a float
-        else v = __half2float(__ushort_as_half((unsigned short)h[j]));     // FP16
-        at(r, j) = v * s;
-    }
-    return r;
-}
-
 template <int ADJ, int Q>
 __global__ void __launch_bounds__(NT) k_imaging(ImagingArgs a)
 {
@@ -752,86 +863,33 @@ __global__ void __launch_bounds__(NT) k_imaging(ImagingArgs a)
     const int bz = blockIdx.x % ntz, bx = blockIdx.x / ntz;
     const int z0 = FAT + bz * TZ, x0 = FAT + bx * TX;
     const long long nz = a.nz;
-    {
-        const int nq = SZ / 4;
-        for (int q = tid; q < nq * SX; q += NT) {
-            const int lx = q / nq, lz4 = (q % nq) * 4;
-            const int gz = z0 - FAT + lz4, gx = x0 - FAT + lx;
-            float4 u = make_float4(0.f, 0.f, 0.f, 0.f), v = u;
-            if (gz < a.nz) {
-                const long long gi = (long long)gx * nz + gz;
-                u = ldw<Q>(a, 0, a.its, gi);
-                v = ldw<Q>(a, 1, a.its, gi);
-            }
-            st4(sm + lx * SZ + lz4, u);
-            st4(sm + SMEM_FIELD + lx * SZ + lz4, v);
-        }
-    }
+    stage_snapshot<Q>(a.h, a.its, a.nz, sm, z0, x0, tid);
     __syncthreads();
     const int tzi = tid % NTZ, txi = tid / NTZ;
     const int lz = FAT + 4 * tzi, lx = FAT + txi;
     const int gz = z0 + 4 * tzi;
     if (gz >= a.nz - FAT) return;
     const long long gi = (long long)(x0 + txi) * nz + gz;
-    const float* svx = sm;
-    const float* svz = sm + SMEM_FIELD;
-    float4 q[9];
-    float w[12];
-#pragma unroll
-    for (int m = 0; m < 9; m++) q[m] = ld4(svx + (lx - FAT + m) * SZ + lz);
-    const float4 dvx_dx = dpx(q, 4, a.cx);
-    zwin(svx, lx, lz, w);
-    const float4 dvx_dz = dmz(w, a.cz);
-#pragma unroll
-    for (int m = 0; m < 9; m++) q[m] = ld4(svz + (lx - FAT + m) * SZ + lz);
-    const float4 dvz_dx = dmx(q, 4, a.cx);
-    zwin(svz, lx, lz, w);
-    const float4 dvz_dz = dpz(w, a.cz);
-    float4 tx, tz;
-    {
-        const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 xo = a.its > 0 ? ldw<Q>(a, 0, a.its - 1, gi) : zero;
-        const float4 zo = a.its > 0 ? ldw<Q>(a, 1, a.its - 1, gi) : zero;
-        const float4 xn = a.its < a.nts - 1 ? ldw<Q>(a, 0, a.its + 1, gi) : zero;
-        const float4 zn = a.its < a.nts - 1 ? ldw<Q>(a, 1, a.its + 1, gi) : zero;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            // one-sided at the ends like the reference: -W[its+1] at its = 0, W[its-1] at nts-1
-            at(tx, j) = (a.its == 0) ? -at(xn, j) : (a.its == a.nts - 1) ? at(xo, j) : at(xo, j) - at(xn, j);
-            at(tz, j) = (a.its == 0) ? -at(zn, j) : (a.its == a.nts - 1) ? at(zo, j) : at(zo, j) - at(zn, j);
-        }
-    }
+    const ImgTerms t = imaging_terms<Q>(a.h, sm, lx, lz, gi, a.its, a.cz, a.cx);
     if (!ADJ) {
         const float4 d0 = ldg4(a.dm[0] + gi), d1 = ldg4(a.dm[1] + gi), dl = ldg4(a.dm[2] + gi),
                      du = ldg4(a.dm[3] + gi), d4 = ldg4(a.dm[4] + gi);
         float4 s0, s1, s2, s3, s4;
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-            at(s0, j) = at(d0, j) * at(tx, j) * a.dts_inv;
-            at(s1, j) = at(d1, j) * at(tz, j) * a.dts_inv;
-            const float dvx = at(dvx_dx, j), dvz = at(dvz_dz, j);
+            at(s0, j) = at(d0, j) * at(t.tx, j) * a.dts_inv;
+            at(s1, j) = at(d1, j) * at(t.tz, j) * a.dts_inv;
+            const float dvx = at(t.dvx_dx, j), dvz = at(t.dvz_dz, j);
             at(s2, j) = at(dl, j) * (dvx + dvz) + 2.0f * at(du, j) * dvx;
             at(s3, j) = at(dl, j) * (dvx + dvz) + 2.0f * at(du, j) * dvz;
-            at(s4, j) = at(d4, j) * (at(dvx_dz, j) + at(dvz_dx, j));
+            at(s4, j) = at(d4, j) * (at(t.dvx_dz, j) + at(t.dvz_dx, j));
         }
         st4(a.ss[0] + gi, s0); st4(a.ss[1] + gi, s1); st4(a.ss[2] + gi, s2);
         st4(a.ss[3] + gi, s3); st4(a.ss[4] + gi, s4);
     } else {
-        const float4 s0 = ldg4(a.ss[0] + gi), s1 = ldg4(a.ss[1] + gi), s2 = ldg4(a.ss[2] + gi),
-                     s3 = ldg4(a.ss[3] + gi), s4 = ldg4(a.ss[4] + gi);
-        float4 d0 = ld4(a.dm[0] + gi), d1 = ld4(a.dm[1] + gi), d2 = ld4(a.dm[2] + gi), d3 = ld4(a.dm[3] + gi),
-               d4 = ld4(a.dm[4] + gi);
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const float dvx = at(dvx_dx, j), dvz = at(dvz_dz, j);
-            at(d0, j) += at(s0, j) * at(tx, j) * a.dts_inv;
-            at(d1, j) += at(s1, j) * at(tz, j) * a.dts_inv;
-            at(d2, j) += (at(s2, j) + at(s3, j)) * (dvx + dvz);
-            at(d3, j) += 2.0f * (dvx * at(s2, j) + dvz * at(s3, j));
-            at(d4, j) += at(s4, j) * (at(dvx_dz, j) + at(dvz_dx, j));
-        }
-        st4(a.dm[0] + gi, d0); st4(a.dm[1] + gi, d1); st4(a.dm[2] + gi, d2);
-        st4(a.dm[3] + gi, d3); st4(a.dm[4] + gi, d4);
+        const float4 s[5] = {ldg4(a.ss[0] + gi), ldg4(a.ss[1] + gi), ldg4(a.ss[2] + gi), ldg4(a.ss[3] + gi),
+                             ldg4(a.ss[4] + gi)};
+        imaging_accumulate(a.dm, gi, s, t, a.dts_inv);
     }
 }
 
