@@ -393,6 +393,10 @@ def run_ours(args, ws, rank, local):
                    "l2": "inputs larger than L2 (34.6 GB FP32 source-wavefield history per shot) and a 256 MB "
                          "L2 flush between timed steps"},
         "shot_gradients_per_s": round(ws * nsh * args.steps / (t_ms * 1e-3), 4),
+        # (algorithmic bytes of one shot's Born forward + adjoint: 4 propagations at 80 B per cell
+        # update) / measured HBM peak / measured time per shot gradient
+        "shot_gradients_roofline_frac": round(
+            (4.0 * fine_steps * cells * BYTES_PER_CELL / (peak * 1e9)) / ((t_ms * 1e-3) / (ws * nsh * args.steps)), 4),
         "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
         "gpu_launches": st["launches"],
     }
