@@ -1674,6 +1674,8 @@ __global__ void __launch_bounds__(256) k_add4(float* __restrict__ dst, const flo
 }
 
 bool engine_is_tuned(const Engine* e) { return e->tuned; }
+// device bytes of source-wavefield history this engine already holds
+size_t engine_history_bytes(const Engine* e) { return e->W.cap + e->Wq.cap; }
 int engine_get_checkpoint(const Engine* e) { return e->ckpt; }
 int engine_get_graphs(const Engine* e) { return e->use_graphs ? 1 : 0; }
 size_t engine_cells(const Engine* e) { return (size_t)e->nz * e->full_nx; }

@@ -390,20 +390,30 @@ static float* lane_staging(eio_ctx* c, int k, size_t n) {
 
 static Engine* lane_engine(eio_ctx* c, int k) { return k == 0 ? c->eng : c->extra[k - 1]; }
 
-// Lanes for a call over nShots shots, each new lane needing about lane_bytes of
-// device memory: at most c->lanes and nShots, fewer when the free memory would
-// not hold the new lanes.  New lanes take the first lane's kernel choice (tuned
-// first), checkpoint precision and graph setting.
+// Lanes for a call over nShots shots, each lane needing about lane_bytes of
+// device memory for the call: at most c->lanes and nShots, fewer when the free
+// memory would not hold what the lanes still have to allocate (a new lane all
+// of it; an existing one its Born history, which is allocated at first use).
+// New lanes take the first lane's kernel choice (tuned first), checkpoint
+// precision and graph setting.
 static int ensure_lanes(eio_ctx* c, int nShots, size_t lane_bytes) {
     int n = std::max(1, std::min(c->lanes, nShots));
     const int have = 1 + (int)c->extra.size();
-    if (n > have) {
+    if (n > 1) {
         size_t fr = 0, tot = 0;
         if (cudaSetDevice(c->device) == cudaSuccess && cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
-            const size_t need = lane_bytes + lane_bytes / 5 + ((size_t)256 << 20);
-            while (n > have && (size_t)(n - have) * need > fr) n--;
+            auto need = [&](int lanes) {
+                size_t b = 0;
+                for (int k = 0; k < lanes; k++) {
+                    const size_t held = k < have ? engine_history_bytes(lane_engine(c, k)) : 0;
+                    const size_t want = k < have ? (lane_bytes > held ? lane_bytes - held : 0) : lane_bytes;
+                    b += want + want / 5;
+                }
+                return b + ((size_t)256 << 20);
+            };
+            while (n > 1 && need(n) > fr) n--;
         } else {
-            n = have;
+            n = std::min(n, have);
         }
     }
     if (n > 1 && !engine_is_tuned(c->eng)) engine_autotune(c->eng);

@@ -73,6 +73,7 @@ void* engine_stream(Engine* e);
 void engine_set_graphs(Engine* e, int enable);
 void engine_set_window(Engine* e, int ix0, int nxw);   // nxw = 0: the whole grid
 bool engine_is_tuned(const Engine* e);
+size_t engine_history_bytes(const Engine* e);
 int engine_get_checkpoint(const Engine* e);
 int engine_get_graphs(const Engine* e);
 size_t engine_cells(const Engine* e);
