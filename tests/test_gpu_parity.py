@@ -413,6 +413,10 @@ def test_nonlinear_fwi_operator_sets_background_then_propagates(w):
     sig = w.source_signal()[None]
     fwi = prop.nonlinearFwiPropElasticShotsGpu(w.elastic, w.par, sig, *src, *rec)
     nl = prop.nonlinearPropElasticShotsGpu(w.elastic, w.par, *src, *rec)
+    # bitwise comparison: both contexts on the same kernel (each would autotune on its own)
+    from elastic_isotropic_operators_b200 import _lib
+    for op in (fwi, nl):
+        _lib.check(op._L.eio_ctx_set_kernel(op.ctx, 0, 64, 16, 0))
     model2 = w.elastic.clone()
     model2.getNdArray()[...] = w.elastic.getNdArray() * np.float32(1.02)
     d_fwi = fwi.dataSpace()
