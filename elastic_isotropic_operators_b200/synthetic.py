@@ -15,6 +15,12 @@ Workloads (all seeded, no external data):
                  vp gradient 1800..4000 m/s, vs=vp/1.8, Gardner rho, seeded
                  Gaussian-random drho/dlambda/dmu smoothed at 50 m with 5% RMS,
                  10 shots (12 Hz Ricker), 900 receivers
+  fwi_1000x3400  batched FWI gradient: 1000x3400 total (50-cell pads), dx=dz=12.5 m,
+                 dt=1 ms, nts=5000, flat layers vp 1800..4000 m/s with a seeded
+                 irregular 4500 m/s inclusion (true model) and its Gaussian-smoothed
+                 version (starting model), vs=vp/1.8, Gardner rho, 10 Hz Ricker,
+                 120 shots whose receivers (same count) span an offset window of
+                 2..8 km drawn per shot (uneven apertures, so cropped windows differ)
   small          tiny grid for parity tests
 """
 import math
@@ -120,6 +126,11 @@ class Workload:
             xc = self.src_x[e:e + 1].copy()
             for k, h in enumerate(hyps):
                 src[k].append(spaceInterpGpu(zc, xc, h, self.nts, method, nfilt, 0, 0.0, 0.0))
+        if "rec_x_shots" in self.extra:   # per-shot receivers (same count, own positions)
+            rec = [[spaceInterpGpu(np.full(len(rx), self.rec_z[0], np.float32), np.asarray(rx, np.float32), h,
+                                   self.nts, method, nfilt, 0, 0.0, 0.0) for rx in self.extra["rec_x_shots"]]
+                   for h in hyps]
+            return src, rec
         rec = [[spaceInterpGpu(self.rec_z, self.rec_x, h, self.nts, method, nfilt, 0, 0.0, 0.0)] for h in hyps]
         return src, rec
 
@@ -177,6 +188,46 @@ def born_600x1800(nts=4000, nshots=10, seed=2024):
     w = ricker(nts, dts, 12.0, 0.12)
     return Workload("born_600x1800", epp, pads, dz, dz, nts, dts, 1, 30.0, [z0] * nshots, src_x, rec_z, rec_x,
                     w, nshots, extra=dict(dmodel=dmod))
+
+
+def fwi_1000x3400(nts=5000, nshots=120, nrec=200, seed=2025, nz=1000, nx=3400, dz=12.5, pad=50,
+                  window_km=(2.0, 8.0)):
+    """Batched-FWI case (see the module docstring); other sizes for tests.
+    extra: true_model / start_model ([3][nx][nz] padded), rec_x_shots."""
+    nzi, nxi = nz - 2 * FAT - 2 * pad, nx - 2 * FAT - 2 * pad
+    rng = np.random.default_rng(seed)
+    depth = np.arange(nzi) / max(nzi - 1, 1)
+    layers = np.array([1800, 2100, 2400, 2700, 3000, 3300, 3600, 4000], np.float64)
+    vp0 = np.tile(layers[np.minimum((depth * len(layers)).astype(int), len(layers) - 1)], (nxi, 1))
+    blob = gaussian_smooth(rng.standard_normal((nxi, nzi)), max(nzi, nxi) / 40.0)
+    xx, zz = np.meshgrid(np.arange(nxi) / nxi, depth, indexing="ij")
+    inside = (blob > 0.2 * blob.std()) & ((xx - 0.5) ** 2 / 0.06 + (zz - 0.55) ** 2 / 0.04 < 1.0)
+    vp_true = np.where(inside, 4500.0, vp0)
+    vp_start = gaussian_smooth(vp_true, max(nzi, nxi) / 60.0)
+    models = []
+    for vp in (vp_true, vp_start):
+        ep = elastic_from_vpvsrho(vp, vp / 1.8, gardner(vp))
+        epp, pads = pad_elastic(ep, pad, pad)
+        assert epp.shape == (3, nx, nz), epp.shape
+        models.append(epp)
+    dts = 1e-3
+    oz = -(FAT + pad) * dz
+    ox = -(FAT + pad) * dz
+    z0 = _grid_coord(oz, dz, FAT + pad + 2)
+    first, last = FAT + pad + 10, FAT + pad + nxi - 11
+    xs = np.linspace(first, last, nshots).round().astype(int)
+    src_x = [_grid_coord(ox, dz, i) for i in xs]
+    rec_shots = []
+    for i in xs:
+        half = 0.5 * rng.uniform(*window_km) * 1000.0 / dz            # cells
+        lo, hi = max(first, int(round(i - half))), min(last, int(round(i + half)))
+        rec_shots.append(np.array([_grid_coord(ox, dz, c) for c in np.linspace(lo, hi, nrec)], np.float32)
+                         + np.float32(0.5 * dz))
+    w = ricker(nts, dts, 10.0, 0.15)
+    wl = Workload("fwi_%dx%d" % (nz, nx), models[1], pads, dz, dz, nts, dts, 1, 20.0, [z0] * nshots, src_x,
+                  np.full(nrec, z0, np.float32), rec_shots[0], w, nshots,
+                  extra=dict(true_model=models[0], start_model=models[1], rec_x_shots=rec_shots))
+    return wl
 
 
 def small(nz=72, nx=104, nts=150, nshots=2, nrec=20, seed=7, sub=1, dz=10.0, surface=0, alphaCos=0.99):
