@@ -41,8 +41,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="born_600x1800", choices=["born_600x1800", "nl_312x520"])
-    ap.add_argument("--shots", type=int, default=10)
+    ap.add_argument("--workload", default="born_600x1800", choices=["born_600x1800", "nl_312x520", "fwi_1000x3400"])
+    ap.add_argument("--shots", type=int, default=None,
+                    help="shots per GPU (default: 10 for born_600x1800; a bounded sample of 16 of the 120 shots "
+                         "for fwi_1000x3400)")
     ap.add_argument("--nts", type=int, default=4000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -227,7 +229,7 @@ def run_ours(args, ws, rank, local):
     import torch
     from elastic_isotropic_operators_b200 import _lib, prop, synthetic
 
-    w = synthetic.born_600x1800(nts=args.nts, nshots=args.shots, seed=2024 + rank)
+    w = synthetic.born_600x1800(nts=args.nts, nshots=args.shots or 10, seed=2024 + rank)
     src, rec = w.geometry()
     sig = [w.source_signal()]
     dev = torch.device("cuda", local)
@@ -440,6 +442,10 @@ def run_reference(args, ws, rank, local):
         if not O.RefGpu.available("f"):
             return {"impl": "reference", "unavailable": "oracle/_ref not built (reference tree absent at build time)"}
         return run_reference_nl(args)
+    if args.workload == "fwi_1000x3400":
+        return {"impl": "reference", "unavailable": "the reference propagates every shot on the whole grid and its "
+                "Born drivers index the history with the 32-bit product its*nz*nx (kernelsGpuElastic.cu:1342), "
+                "which overflows here (5000*1000*3400 >= 2^31)"}
     w = synthetic.born_600x1800(nts=args.nts, nshots=1, seed=2024)
     if not O.RefGpu.available("f"):
         return run_reference_port(args, w, "oracle/_ref not built (reference tree absent at build time)")
@@ -665,6 +671,86 @@ def run_ours_nl(args, ws, rank, local):
             "cpu_baseline": cpu, "clocks": clk, "gpu_launches": st["launches"]}
 
 
+def run_ours_fwi(args, ws, rank, local):
+    """FWI gradients of the batched-FWI case: per step, the misfit and gradient
+    (nonlinear forward residual + Born adjoint) of a bounded sample of its
+    shots through the operator API, with cropped shots, BF16 source-wavefield
+    checkpoints and shot lanes.  One shot-gradient = 3 propagations of its
+    window's cells."""
+    import ctypes
+    import torch
+    from elastic_isotropic_operators_b200 import _lib, fwi, prop, synthetic
+    nsh = args.shots or 16
+    # a bounded sample of the 120 shots, spread over the line; each rank its own shots
+    pick = np.linspace(0, 119, nsh * ws).round().astype(int)[rank::ws]
+    w = synthetic.fwi_1000x3400(nshots=120, select=list(pick))
+    w.par.set("iGpu", str(local))
+    dev = torch.device("cuda", local)
+    src, rec = w.geometry()
+    sig = w.source_signal()[None]
+    nl = prop.nonlinearFwiPropElasticShotsGpu(w.elastic, w.par, sig, *src, *rec)
+    born = prop.BornElasticShotsGpu(w.elastic, w.par, [w.source_signal()], *src, *rec)
+    born.setCheckpointPrecision(1)
+    for op in (nl, born):
+        pin_kernel(op._L, op.ctx, args)
+    ix0, nxw = nl.autoShotWindows()
+    born.setShotWindows(ix0, nxw)
+    d_obs = nl.dataSpace()
+    nl.forward(False, w.extra["true_model"], d_obs)          # observed data, untimed
+    obj = fwi.FwiObjective(nl, born, d_obs)
+    m0 = w.extra["start_model"]
+    L = _lib.lib()
+    est = torch.cuda.ExternalStream(L.eio_ctx_stream(born.ctx), device=dev)
+    fine_steps = (w.nts - 1) * 2
+    updates = float(sum(3 * fine_steps * (w.nz - 8) * (int(n) - 8) for n in nxw))
+    for _ in range(args.warmup):
+        obj.value_and_gradient(m0)
+    torch.cuda.synchronize()
+    for op in (nl, born):
+        L.eio_ctx_stats(op.ctx, 1, 1, None, None, None)
+    barrier(ws)
+    clocks = ClockSampler(None)
+    clocks.start()
+    t_ms = 0.0
+    for _ in range(args.steps):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record(est)
+        obj.value_and_gradient(m0)
+        ev1.record(est)
+        torch.cuda.synchronize()
+        t_ms += ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    launches = 0
+    for op in (nl, born):
+        launches += read_stats(L, op.ctx)["launches"]
+    t_ms = max_over_ranks(ws, t_ms)
+    value = ws * updates * args.steps / (t_ms * 1e-3) / 1e9
+    peak, pk = measured_peak()
+    n_data = int(np.prod(d_obs.getNdArray().shape))
+    h2d = 4 * (3 * w.nz * w.nx) * 2 + 4 * n_data         # model (forward, Born background), residual
+    d2h = 4 * n_data + 4 * 3 * w.nz * w.nx               # modelled data, gradient
+    return {"metric": "Gcells/s", "value": round(value, 3), "unit": "Gcell-updates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_ms / args.steps, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "fwi_1000x3400: FWI misfit + gradient (nonlinear forward + Born adjoint), "
+                                   "%d of the 120 shots per GPU (bounded sample), 1000x3400 grid, nts=5000, "
+                                   "cropped shots (uneven 2-8 km windows, mean %d columns), BF16 checkpoints"
+                                   % (nsh, int(np.mean(nxw))),
+                       "shots_per_gpu": nsh, "shot_lanes": lanes_used(L, born.ctx),
+                       "cell_updates_per_step": updates * ws,
+                       "l2": "inputs larger than L2 (BF16 history of a window: several GB per shot)"},
+            "shot_gradients_per_s": round(ws * nsh * args.steps / (t_ms * 1e-3), 4),
+            "e2e": {"value": round(value, 3), "unit": "Gcell-updates/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "note": "the operator API with host buffers is the only path"},
+            "roofline": {"bound": "hbm", "achieved": round(BYTES_PER_CELL * value, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(BYTES_PER_CELL * value / peak, 4), "traffic": None, "peak_source": pk,
+                         "basis": "80 B per cell update over the timed region (job level)",
+                         "kernel": kernel_name(L, born.ctx)},
+            "cpu_baseline": None, "clocks": clk, "gpu_launches": int(launches)}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -676,6 +762,8 @@ def main():
     ws, rank, local = dist_init(args)
     if args.workload == "nl_312x520":
         out = run_ours_nl(args, ws, rank, local)
+    elif args.workload == "fwi_1000x3400":
+        out = run_ours_fwi(args, ws, rank, local)
     else:
         out = run_ours(args, ws, rank, local)
     if rank == 0:

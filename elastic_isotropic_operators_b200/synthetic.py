@@ -191,8 +191,10 @@ def born_600x1800(nts=4000, nshots=10, seed=2024):
 
 
 def fwi_1000x3400(nts=5000, nshots=120, nrec=200, seed=2025, nz=1000, nx=3400, dz=12.5, pad=50,
-                  window_km=(2.0, 8.0)):
+                  window_km=(2.0, 8.0), select=None):
     """Batched-FWI case (see the module docstring); other sizes for tests.
+    select: indices of the shots to keep (the acquisition of the others is drawn
+    all the same, so a subset is the same shots as in the full case).
     extra: true_model / start_model ([3][nx][nz] padded), rec_x_shots."""
     nzi, nxi = nz - 2 * FAT - 2 * pad, nx - 2 * FAT - 2 * pad
     rng = np.random.default_rng(seed)
@@ -223,9 +225,13 @@ def fwi_1000x3400(nts=5000, nshots=120, nrec=200, seed=2025, nz=1000, nx=3400, d
         lo, hi = max(first, int(round(i - half))), min(last, int(round(i + half)))
         rec_shots.append(np.array([_grid_coord(ox, dz, c) for c in np.linspace(lo, hi, nrec)], np.float32)
                          + np.float32(0.5 * dz))
+    if select is not None:
+        src_x = [src_x[i] for i in select]
+        rec_shots = [rec_shots[i] for i in select]
+    n = len(src_x)
     w = ricker(nts, dts, 10.0, 0.15)
-    wl = Workload("fwi_%dx%d" % (nz, nx), models[1], pads, dz, dz, nts, dts, 1, 20.0, [z0] * nshots, src_x,
-                  np.full(nrec, z0, np.float32), rec_shots[0], w, nshots,
+    wl = Workload("fwi_%dx%d" % (nz, nx), models[1], pads, dz, dz, nts, dts, 1, 20.0, [z0] * n, src_x,
+                  np.full(nrec, z0, np.float32), rec_shots[0], w, n,
                   extra=dict(true_model=models[0], start_model=models[1], rec_x_shots=rec_shots))
     return wl
 
