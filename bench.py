@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--graphs", action="store_true", help="run the time loops as CUDA graphs (off by default)")
+    ap.add_argument("--fwi-unfused", action="store_true",
+                    help="fwi_1000x3400: nonlinear forward + Born adjoint (3 propagations per shot) instead of "
+                         "the fused gradient (2)")
     ap.add_argument("--lanes", type=int, default=0,
                     help="shot lanes (concurrent shots on the GPU); 0 keeps the library default")
     ap.add_argument("--kernel", type=int, default=-1, choices=[-1, 0, 1, 2, 3, 4, 5],
@@ -673,10 +676,12 @@ def run_ours_nl(args, ws, rank, local):
 
 def run_ours_fwi(args, ws, rank, local):
     """FWI gradients of the batched-FWI case: per step, the misfit and gradient
-    (nonlinear forward residual + Born adjoint) of a bounded sample of its
-    shots through the operator API, with cropped shots, BF16 source-wavefield
-    checkpoints and shot lanes.  One shot-gradient = 3 propagations of its
-    window's cells."""
+    of a bounded sample of its shots through the operator API (FwiObjective),
+    with cropped shots, BF16 source-wavefield checkpoints and shot lanes.  The
+    fused gradient runs 2 propagations of a shot's window (nonlinear forward
+    recording the source wavefield, Born adjoint); --fwi-unfused runs the
+    reference's 3 (nonlinear forward, Born adjoint with its own source
+    propagation).  Cell updates count the propagations actually run."""
     import ctypes
     import torch
     from elastic_isotropic_operators_b200 import _lib, fwi, prop, synthetic
@@ -697,12 +702,13 @@ def run_ours_fwi(args, ws, rank, local):
     born.setShotWindows(ix0, nxw)
     d_obs = nl.dataSpace()
     nl.forward(False, w.extra["true_model"], d_obs)          # observed data, untimed
-    obj = fwi.FwiObjective(nl, born, d_obs)
+    obj = fwi.FwiObjective(nl, born, d_obs, fused=not args.fwi_unfused)
+    props = 2 if obj.fused else 3
     m0 = w.extra["start_model"]
     L = _lib.lib()
     est = torch.cuda.ExternalStream(L.eio_ctx_stream(born.ctx), device=dev)
     fine_steps = (w.nts - 1) * 2
-    updates = float(sum(3 * fine_steps * (w.nz - 8) * (int(n) - 8) for n in nxw))
+    updates = float(sum(props * fine_steps * (w.nz - 8) * (int(n) - 8) for n in nxw))
     for _ in range(args.warmup):
         obj.value_and_gradient(m0)
     torch.cuda.synchronize()
@@ -728,16 +734,19 @@ def run_ours_fwi(args, ws, rank, local):
     value = ws * updates * args.steps / (t_ms * 1e-3) / 1e9
     peak, pk = measured_peak()
     n_data = int(np.prod(d_obs.getNdArray().shape))
-    h2d = 4 * (3 * w.nz * w.nx) * 2 + 4 * n_data         # model (forward, Born background), residual
+    # model (forward and Born background, or the one fused background), residual
+    h2d = 4 * (3 * w.nz * w.nx) * (1 if obj.fused else 2) + 4 * n_data
     d2h = 4 * n_data + 4 * 3 * w.nz * w.nx               # modelled data, gradient
     return {"metric": "Gcells/s", "value": round(value, 3), "unit": "Gcell-updates/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_ms / args.steps, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": "fwi_1000x3400: FWI misfit + gradient (nonlinear forward + Born adjoint), "
+            "config": {"workload": "fwi_1000x3400: FWI misfit + gradient (%s), "
                                    "%d of the 120 shots per GPU (bounded sample), 1000x3400 grid, nts=5000, "
                                    "cropped shots (uneven 2-8 km windows, mean %d columns), BF16 checkpoints"
-                                   % (nsh, int(np.mean(nxw))),
+                                   % ("fused: nonlinear forward recording the source wavefield + Born adjoint"
+                                      if obj.fused else "nonlinear forward + Born adjoint", nsh, int(np.mean(nxw))),
+                       "propagations_per_shot": props,
                        "shots_per_gpu": nsh, "shot_lanes": lanes_used(L, born.ctx),
                        "cell_updates_per_step": updates * ws,
                        "l2": "inputs larger than L2 (BF16 history of a window: several GB per shot)"},

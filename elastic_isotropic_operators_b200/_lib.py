@@ -83,6 +83,7 @@ _SIGS = {
     "eio_ctx_set_lanes": (I, [P, I]),
     "eio_ctx_get_lanes": (I, [P, IP, IP]),
     "eio_born_shots_dev": (I, [P, I, I, P, P, P, P, IP, P, IP]),
+    "eio_fwi_gradient": (I, [P, I, I, FP, FP, I, IP, P, P, I, P, FP, ctypes.POINTER(ctypes.c_double)]),
     "eio_reduce64": (I, [I, I, I, P, P, ctypes.c_longlong, I, ctypes.POINTER(ctypes.c_double)]),
     "eio_ctx_pair_stats": (I, [P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]),
     "eio_nl_fwd_reg": (I, [P, P, P, P, IP, P, IP]),

@@ -1234,7 +1234,26 @@ static void quantize_row(Engine* e, int row) {
 // goes through the FP32 staging rows, its scale comes from the warp maxima the
 // step leaves, and k_quantize stores the codes.  The tile kernels write the
 // maxima, so the sweep kernel is not used here.
-static void born_source_q(Engine* e, const PointList& src, StepArgs a) {
+// Injection (and, for the nonlinear forward, extraction) time weights of the
+// source-wavefield propagation at fine step (its, it2): the Born operators
+// inject fine-time sources (row itw - 1), the nonlinear forward coarse traces
+// with the filter weights and records its receivers (engine_nl_record).
+struct SrcWeights {
+    const Engine* e;
+    bool nl;
+    void operator()(StepArgs& x, int its, int it2) const {
+        const float* F = e->filt.data();
+        const int h = e->h;
+        if (nl) {
+            x.inj.t0 = its; x.inj.w0 = F[it2 - 1]; x.inj.w1 = F[h + it2 - 1];
+            x.ext.t0 = its; x.ext.w0 = F[it2]; x.ext.w1 = F[h + it2];
+        } else {
+            x.inj.t0 = its * e->S + it2 - 1; x.inj.w0 = 1.f; x.inj.w1 = 0.f;
+        }
+    }
+};
+
+static void born_source_q(Engine* e, const PointList& src, StepArgs a, const SparseOp* ext) {
     if (e->S != 2)
         throw Error(EIO_ERR_UNSUPPORTED, "16-bit source-wavefield snapshots need sub = 1 (two fine steps per sample)");
     const size_t qbytes = sizeof(unsigned short) * 2 * (size_t)e->nts * e->n;
@@ -1259,7 +1278,9 @@ static void born_source_q(Engine* e, const PointList& src, StepArgs a) {
     int cur = 0;
     a.inj = upload_points(e, src, e->inj_ts, e->inj_ent, e->sig_in);
     const SparseOp injh = halo_sources(e, kind == 5, src.pos, src.npos, e->sig_in);
-    memset(&a.ext, 0, sizeof(a.ext));
+    if (ext) a.ext = *ext;
+    else memset(&a.ext, 0, sizeof(a.ext));
+    const SrcWeights weights{e, ext != nullptr};
     a.W0 = e->wstage.f();
     a.W1 = e->wstage.f() + e->n;
     a.wt = 0;
@@ -1267,7 +1288,7 @@ static void born_source_q(Engine* e, const PointList& src, StepArgs a) {
     const int h = e->h;
     const int npart = e->ntiles * 16;
     LoopKey key = loop_key(e, 2);
-    key << e->Wq.p << e->wscale.p << e->wstage.p << e->wpmax.p;
+    key << e->Wq.p << e->wscale.p << e->wstage.p << e->wpmax.p << (ext != nullptr);
     key.add(&a, sizeof(a));
     key.add(&injh, sizeof(injh));
     try {
@@ -1277,19 +1298,18 @@ static void born_source_q(Engine* e, const PointList& src, StepArgs a) {
                 // (its, 1) samples row its, (its, 2) only steps; the staging rows
                 // are quantized after the pair
                 StepArgs a0 = a, a1 = a;
-                a0.inj.t0 = 2 * its; a0.inj.w0 = 1.f; a0.inj.w1 = 0.f;
+                weights(a0, its, 1);
                 a0.tmode = 1; a0.wt = 0; a0.tw_o = F[h + 1]; a0.tw_c = F[h + 2]; a0.tw_n = F[1];
                 a0.pmax = e->wpmax.f() + (size_t)(its & 1) * 2 * npart;
-                a1.inj.t0 = 2 * its + 1; a1.inj.w0 = 1.f; a1.inj.w1 = 0.f;
+                weights(a1, its, 2);
                 a1.tmode = 0; a1.pmax = nullptr;
                 run_pair<0, EPI_TRI>(e, a0, a1, injh, L);
                 quantize_row(e, its);
                 continue;
             }
             for (int it2 = 1; it2 < e->S + 1; it2++) {
-                const int itw = its * e->S + it2;
                 L.set(a);
-                a.inj.t0 = itw - 1; a.inj.w0 = 1.f; a.inj.w1 = 0.f;
+                weights(a, its, it2);
                 const bool last = (its == e->nts - 2 && it2 == 2);
                 int row = -1;
                 if (it2 == 1) {
@@ -1317,9 +1337,11 @@ static void born_source_q(Engine* e, const PointList& src, StepArgs a) {
     check_launch();
 }
 
-static void born_source(Engine* e, const PointList& src, StepArgs a) {
+// ext: the receiver lists of the nonlinear forward (engine_nl_record), whose
+// source traces are coarse; nullptr for the Born operators' fine-time sources
+static void born_source(Engine* e, const PointList& src, StepArgs a, const SparseOp* ext = nullptr) {
     if (e->ckpt) {
-        born_source_q(e, src, a);
+        born_source_q(e, src, a, ext);
         return;
     }
     const size_t wbytes = sizeof(float) * 2 * (size_t)e->nts * e->n;
@@ -1337,13 +1359,15 @@ static void born_source(Engine* e, const PointList& src, StepArgs a) {
     const bool use_pair = tri && e->kind == 5;
     a.inj = upload_points(e, src, e->inj_ts, e->inj_ent, e->sig_in);
     const SparseOp injh = halo_sources(e, use_pair, src.pos, src.npos, e->sig_in);
-    memset(&a.ext, 0, sizeof(a.ext));
+    if (ext) a.ext = *ext;
+    else memset(&a.ext, 0, sizeof(a.ext));
+    const SrcWeights weights{e, ext != nullptr};
     a.W0 = e->W.f();
     a.W1 = e->W.f() + (long long)e->nts * e->n;
     const float* F = e->filt.data();
     const int h = e->h;
     LoopKey key = loop_key(e, 3);
-    key << tri << use_pair;
+    key << tri << use_pair << (ext != nullptr);
     key.add(&a, sizeof(a));
     key.add(&injh, sizeof(injh));
     run_graph(e, key.h, (long long)(e->nts - 1) * e->S, [&] {
@@ -1351,17 +1375,16 @@ static void born_source(Engine* e, const PointList& src, StepArgs a) {
         if (use_pair && its < e->nts - 2) {
             // (its, 1) writes row its, (its, 2) only steps
             StepArgs a0 = a, a1 = a;
-            a0.inj.t0 = 2 * its; a0.inj.w0 = 1.f; a0.inj.w1 = 0.f;
+            weights(a0, its, 1);
             a0.tmode = 1; a0.wt = its; a0.tw_o = F[h + 1]; a0.tw_c = F[h + 2]; a0.tw_n = F[1];
-            a1.inj.t0 = 2 * its + 1; a1.inj.w0 = 1.f; a1.inj.w1 = 0.f;
+            weights(a1, its, 2);
             a1.tmode = 0;
             run_pair<0, EPI_TRI>(e, a0, a1, injh, L);
             continue;
         }
         for (int it2 = 1; it2 < e->S + 1; it2++) {
-            const int itw = its * e->S + it2;
             L.set(a);
-            a.inj.t0 = itw - 1; a.inj.w0 = 1.f; a.inj.w1 = 0.f;
+            weights(a, its, it2);
             if (tri) {
                 const bool last = (its == e->nts - 2 && it2 == 2);
                 if (it2 == 1) {          // row its = o*f[h+1] + c*f[h+2] + n*f[1]
@@ -1385,8 +1408,35 @@ static void born_source(Engine* e, const PointList& src, StepArgs a) {
     check_launch();
 }
 
+// Nonlinear forward of one shot that also leaves the coarse Vx/Vz history the
+// Born operators build in their first phase (the source wavefield of the
+// imaging condition), for an adjoint that follows with reuse_history.  The
+// nonlinear operators inject the coarse traces with the time filter, the Born
+// operators fine-time traces interpolated on the host from the same coarse
+// traces: the two source wavefields agree to rounding.  model: regular coarse
+// source traces [nReg][nts] per field (device); data: regular receiver traces
+// (device), as engine_nl.  No free surface (the Born operators have none).
+void engine_nl_record(Engine* e, float* const model[5], float* const data[5], const ShotGeom& g) {
+    EIO_CUDA(cudaSetDevice(e->device));
+    if (!e->tuned) engine_autotune(e);
+    if (e->fs) throw Error(EIO_ERR_UNSUPPORTED, "the Born operators ignore the free surface: no shared history");
+    err_reset(e);
+    PointList src, rec;
+    build_points(e, g.srcPos, g.nSrc, src);
+    build_points(e, g.recPos, g.nRec, rec);
+    StepArgs base = base_args(e);
+    stage_in(e, model, src.ld, e->nts, e->sig_in);
+    zero_out(e, rec.ld, e->nts, e->sig_out);
+    const SparseOp ext = upload_points(e, rec, e->ext_ts, e->ext_ent, e->sig_out);
+    born_source(e, src, base, &ext);
+    stage_out(e, rec.ld, e->nts, e->sig_out, data);
+    EIO_CUDA(cudaStreamSynchronize(e->st));
+    stats_flush(e);
+    err_check(e);
+}
+
 void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5], float* const data[5],
-                 const ShotGeom& g) {
+                 const ShotGeom& g, bool reuse_history) {
     EIO_CUDA(cudaSetDevice(e->device));
     if (!e->tuned) engine_autotune(e);
     err_reset(e);
@@ -1396,9 +1446,11 @@ void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5],
     StepArgs base = base_args(e);
     const float* F = e->filt.data();
     const int h = e->h;
-    // phase 1: source wavefield
-    stage_in(e, srcDtw, src.ld, e->ntw, e->sig_in);
-    born_source(e, src, base);
+    // phase 1: source wavefield (kept from engine_nl_record when reuse_history)
+    if (!reuse_history) {
+        stage_in(e, srcDtw, src.ld, e->ntw, e->sig_in);
+        born_source(e, src, base);
+    }
     // phase 2
     constexpr int R = 4;                 // secondary-source ring slots
     float* ring[R][5];
@@ -1800,6 +1852,39 @@ void engine_born_shot(Engine* e, int adj, float* const srcDtw[5], const ShotGeom
     engine_born(e, adj, ds, dd, dr, g);
     if (!adj) return_receivers(e, rec, dataIrreg);
     EIO_CUDA(cudaStreamSynchronize(e->st));
+}
+
+// One shot of an FWI gradient: the nonlinear forward of the regular coarse
+// sources modelReg recording the Born history (engine_nl_record), the modelled
+// irregular data to dataIrreg (host [5][nIrreg][nts]), then the host callback
+// residual(dataIrreg, resid) that fills resid (host, same layout: S^T of the
+// sampled residual) and returns its misfit, then the Born adjoint of resid on
+// the recorded history into the image dm (device).  Two propagations instead
+// of the three of a nonlinear forward followed by a Born adjoint.
+double engine_fwi_shot(Engine* e, float* const modelReg[5], const ShotGeom& g, const SInterp* const rec[4],
+                       float* dataIrreg, float* resid, double (*residual)(void*, const float*, float*), void* ctx,
+                       float* const dm[5]) {
+    EIO_CUDA(cudaSetDevice(e->device));
+    float* ms[5]; float* dr[5];
+    for (int f = 0; f < 5; f++) {
+        h2d(e, e->stage_a[f], modelReg[f], (size_t)g.nSrc[kFieldGrid[f]] * e->nts);
+        ms[f] = e->stage_a[f].f();
+    }
+    stage_receivers(e, 0, g, rec, nullptr, dr);
+    engine_nl_record(e, ms, dr, g);
+    return_receivers(e, rec, dataIrreg);
+    EIO_CUDA(cudaStreamSynchronize(e->st));
+    const double phi = residual(ctx, dataIrreg, resid);
+    stage_receivers(e, 1, g, rec, resid, dr);
+    float* none[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    engine_born(e, 1, none, dm, dr, g, true);
+    EIO_CUDA(cudaStreamSynchronize(e->st));
+    return phi;
+}
+
+// the image buffers of this lane, offset to the current shot window
+void engine_dm_window(Engine* e, float* out[5]) {
+    for (int f = 0; f < 5; f++) out[f] = e->stage_c[f].f() + (long long)e->win_ix0 * e->nz;
 }
 
 void engine_nl_shot(Engine* e, int adj, float* const modelReg[5], const ShotGeom& g, const SInterp* const rec[4],

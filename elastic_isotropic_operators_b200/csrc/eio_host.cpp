@@ -1213,6 +1213,45 @@ EIO_API int eio_born_forward(eio_ctx* c, int add, int nExp, const float* model, 
     });
 }
 
+// The lanes' images (added in lane order on the first lane's device) downloaded
+// into sl (dm: its pointers), scaled and un-staggered into model (added):
+// BornElasticShotsGpu.cpp:325-371
+static void image_to_model(eio_ctx* c, int nl, float* const dm[5], std::vector<float>* sl, float* model) {
+    const FdParam& fd = c->fd;
+    const int nz = fd.p.nz, nx = fd.p.nx;
+    const size_t n = (size_t)nz * nx;
+    {
+        if (nl > 1) {
+            float* d0[5];
+            engine_dm_ptrs(c->eng, d0);
+            for (int k = 1; k < nl; k++) engine_dm_add(lane_engine(c, k), d0);
+        }
+        engine_dm_download(c->eng, dm);
+        const double tdtw = 2.0 * fd.dtw;
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < (long long)n; i++) {
+            sl[0][i] *= fd.par[0][i];
+            sl[1][i] *= fd.par[1][i];
+            sl[2][i] = (float)(sl[2][i] * tdtw);
+            sl[3][i] = (float)(sl[3][i] * tdtw);
+            sl[4][i] = (float)(sl[4][i] * tdtw);
+        }
+        std::vector<float> t1(model, model + n);
+        stagger_x(0, 1, nz, nx, sl[0].data(), t1.data());
+        stagger_z(0, 1, nz, nx, sl[1].data(), t1.data());
+        std::copy(t1.begin(), t1.end(), model);
+        std::vector<float> t2(n);
+        stagger_z(0, 0, nz, nx, sl[4].data(), t2.data());
+        std::vector<float> t3(n);
+        stagger_x(0, 0, nz, nx, t2.data(), t3.data());
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < (long long)n; i++) {
+            model[n + i] += sl[2][i];
+            model[2 * n + i] += sl[3][i] + t3[i];
+        }
+    }
+}
+
 EIO_API int eio_born_adjoint(eio_ctx* c, int add, int nExp, float* model, const float* data,
                              const float* const* sigs, int nSignals, eio_sinterp* const* src, eio_sinterp* const* rec,
                              int nRecGeom) {
@@ -1245,35 +1284,124 @@ EIO_API int eio_born_adjoint(eio_ctx* c, int add, int nExp, float* model, const 
             ShotWindow win(c, eng, g, e, nExp);
             engine_born_shot(eng, 1, sp, win.sg, g.r, const_cast<float*>(data) + (size_t)e * dslice);
         });
-        // the lanes' images, added in lane order on the first lane's device
-        if (nl > 1) {
-            float* d0[5];
-            engine_dm_ptrs(c->eng, d0);
-            for (int k = 1; k < nl; k++) engine_dm_add(lane_engine(c, k), d0);
+        image_to_model(c, nl, dm, sl, model);
+    });
+}
+
+
+
+// ------------------------------------------------------------ FWI gradient
+namespace {
+
+// residual of one shot: r_k = S_k d - d_obs_k for the sampled components
+// (codes 0..4 the fields, 5 the pressure 0.5 (sxx + szz)), its misfit
+// 0.5 r.r in FP64, and S^T r into the five fields
+struct ShotResidual {
+    int nComp, nri, nts;
+    const int* comps;
+    const float* dobs;          // [nComp][nri][nts] of this shot
+    std::vector<float> r;       // [nComp][nri][nts]
+};
+
+double shot_residual(void* p, const float* d, float* rt) {
+    ShotResidual& s = *static_cast<ShotResidual*>(p);
+    const size_t m = (size_t)s.nri * s.nts;
+    s.r.resize((size_t)s.nComp * m);
+    for (int k = 0; k < s.nComp; k++) {
+        const int code = s.comps[k];
+        float* rk = s.r.data() + (size_t)k * m;
+        const float* ok = s.dobs + (size_t)k * m;
+        if (code < 5) {
+            const float* df = d + (size_t)code * m;
+            for (size_t i = 0; i < m; i++) rk[i] = df[i] - ok[i];
+        } else {
+            const float* d2 = d + 2 * m;
+            const float* d3 = d + 3 * m;
+            for (size_t i = 0; i < m; i++) rk[i] = 0.5f * (d2[i] + d3[i]) - ok[i];
         }
-        engine_dm_download(c->eng, dm);
-        // scaling and un-staggering, BornElasticShotsGpu.cpp:325-371
-        const double tdtw = 2.0 * fd.dtw;
-#pragma omp parallel for schedule(static)
-        for (long long i = 0; i < (long long)n; i++) {
-            sl[0][i] *= fd.par[0][i];
-            sl[1][i] *= fd.par[1][i];
-            sl[2][i] = (float)(sl[2][i] * tdtw);
-            sl[3][i] = (float)(sl[3][i] * tdtw);
-            sl[4][i] = (float)(sl[4][i] * tdtw);
+    }
+    std::fill(rt, rt + 5 * m, 0.f);
+    for (int k = 0; k < s.nComp; k++) {
+        const int code = s.comps[k];
+        const float* rk = s.r.data() + (size_t)k * m;
+        if (code < 5) {
+            float* tf = rt + (size_t)code * m;
+            for (size_t i = 0; i < m; i++) tf[i] += rk[i];
+        } else {
+            float* t2 = rt + 2 * m;
+            float* t3 = rt + 3 * m;
+            for (size_t i = 0; i < m; i++) { t2[i] += 0.5f * rk[i]; t3[i] += 0.5f * rk[i]; }
         }
-        std::vector<float> t1(model, model + n);
-        stagger_x(0, 1, nz, nx, sl[0].data(), t1.data());
-        stagger_z(0, 1, nz, nx, sl[1].data(), t1.data());
-        std::copy(t1.begin(), t1.end(), model);
-        std::vector<float> t2(n);
-        stagger_z(0, 0, nz, nx, sl[4].data(), t2.data());
-        std::vector<float> t3(n);
-        stagger_x(0, 0, nz, nx, t2.data(), t3.data());
-#pragma omp parallel for schedule(static)
-        for (long long i = 0; i < (long long)n; i++) {
-            model[n + i] += sl[2][i];
-            model[2 * n + i] += sl[3][i] + t3[i];
+    }
+    // FP64 sum in index order on the host thread of the lane: a device
+    // reduction here would allocate and free on the device, which waits for
+    // the other lanes' kernels
+    double acc = 0.0;
+    for (float v : s.r) acc += (double)v * (double)v;
+    return 0.5 * acc;
+}
+
+}  // namespace
+
+EIO_API int eio_fwi_gradient(eio_ctx* c, int nExp, int nModelExp, const float* model, const float* dobs, int nComp,
+                             const int* comps, eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom,
+                             float* data, float* grad, double* misfit) {
+    return guarded([&] {
+        if (!c || !model || !dobs || !src || !rec || !grad || !misfit || nExp < 1) throw Error(EIO_ERR_ARG, "null argument");
+        if (nModelExp != 1 && nModelExp != nExp) throw Error(EIO_ERR_ARG, "model shot axis must be 1 or nExp");
+        if (nRecGeom != 1 && nRecGeom != nExp) throw Error(EIO_ERR_ARG, "receiver geometry count must be 1 or nExp");
+        if (nComp < 1 || nComp > 6 || !comps) throw Error(EIO_ERR_ARG, "1 .. 6 data components");
+        for (int k = 0; k < nComp; k++)
+            if (comps[k] < 0 || comps[k] > 5) throw Error(EIO_ERR_ARG, "component codes are 0..4 (fields) or 5 (pressure)");
+        if (c->fd.p.surfaceCondition) throw Error(EIO_ERR_UNSUPPORTED, "the Born operators ignore the free surface");
+        const FdParam& fd = c->fd;
+        const int nts = fd.p.nts;
+        const size_t n = (size_t)fd.p.nz * fd.p.nx;
+        ShotGrids g0 = shot_grids(src, rec, nRecGeom, 0);
+        const int nri = g0.r[0]->nIrreg, nsi = g0.s[0]->nIrreg;
+        const size_t dslice = (size_t)5 * nri * nts, oslice = (size_t)nComp * nri * nts;
+        const size_t mslice = (size_t)5 * nsi * nts;
+        for (int e = 0; e < nExp; e++) {
+            ShotGrids g = shot_grids(src, rec, nRecGeom, e);
+            check_nt(g, nts);
+            if ((size_t)5 * g.s[0]->nIrreg * nts != mslice || (size_t)5 * g.r[0]->nIrreg * nts != dslice)
+                throw Error(EIO_ERR_ARG, "device counts differ between shots");
         }
+        const int nl = ensure_lanes(c, nExp, lane_bytes(c, true));
+        for (int k = 0; k < nl; k++) engine_dm_zero(lane_engine(c, k));
+        std::vector<std::vector<float>> dtmp(nl), rtmp(nl);
+        std::vector<double> phi(nExp, 0.0);
+        run_lanes(c, nl, nExp, [&](int k, Engine* eng, int e) {
+            ShotGrids g = shot_grids(src, rec, nRecGeom, e);
+            const float* ms = model + (nModelExp == 1 ? 0 : (size_t)e * mslice);
+            std::vector<float> reg[5];
+            float* mp[5];
+            for (int f = 0; f < 5; f++) {
+                const SInterp& s = *g.s[kFG[f]];
+                reg[f].assign((size_t)s.nReg * nts, 0.f);
+                sinterp_adjoint(s, false, reg[f].data(), ms + (size_t)f * nsi * nts);
+            }
+            scale_sources(fd, g, reg, nts);
+            for (int f = 0; f < 5; f++) mp[f] = reg[f].data();
+            float* d = data ? data + (size_t)e * dslice : nullptr;
+            if (!d) {
+                dtmp[k].resize(dslice);
+                d = dtmp[k].data();
+            }
+            rtmp[k].resize(dslice);
+            ShotResidual sr{nComp, nri, nts, comps, dobs + (size_t)e * oslice, {}};
+            ShotWindow win(c, eng, g, e, nExp);
+            float* img[5];
+            engine_dm_window(eng, img);
+            phi[e] = engine_fwi_shot(eng, mp, win.sg, g.r, d, rtmp[k].data(), shot_residual, &sr, img);
+        });
+        double total = 0.0;
+        for (int e = 0; e < nExp; e++) total += phi[e];   // shot order
+        *misfit = total;
+        std::fill(grad, grad + 3 * n, 0.f);
+        std::vector<float> sl[5];
+        float* dm[5];
+        for (int f = 0; f < 5; f++) { sl[f].assign(n, 0.f); dm[f] = sl[f].data(); }
+        image_to_model(c, nl, dm, sl, grad);
     });
 }

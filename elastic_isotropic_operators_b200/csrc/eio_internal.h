@@ -94,8 +94,10 @@ struct ShotGeom {
 // samples of every fine step's new level when not null
 void engine_nl(Engine* e, int adj, float* const model[5], float* const data[5], const ShotGeom& g,
                float* wfld = nullptr);
+void engine_nl_record(Engine* e, float* const model[5], float* const data[5], const ShotGeom& g);
+// reuse_history: the history of the shot is already in place (engine_nl_record); srcDtw unused
 void engine_born(Engine* e, int adj, float* const srcDtw[5], float* const dm[5], float* const data[5],
-                 const ShotGeom& g);
+                 const ShotGeom& g, bool reuse_history = false);
 // host-pointer convenience wrappers (copy in/out through the engine's staging buffers)
 // wfld: host [nts][5][nx][nz], overwritten with the saved wavefield when not null
 void engine_nl_host(Engine* e, int adj, float* const model[5], float* const data[5], const ShotGeom& g,
@@ -110,6 +112,10 @@ void engine_dm_download(Engine* e, float* const dm[5]);
 void engine_born_shot(Engine* e, int adj, float* const srcDtw[5], const ShotGeom& g, const SInterp* const rec[4],
                       float* dataIrreg);
 // modelReg: regular source traces, read (forward) or written (adjoint)
+double engine_fwi_shot(Engine* e, float* const modelReg[5], const ShotGeom& g, const SInterp* const rec[4],
+                       float* dataIrreg, float* resid, double (*residual)(void*, const float*, float*), void* ctx,
+                       float* const dm[5]);
+void engine_dm_window(Engine* e, float* out[5]);
 void engine_nl_shot(Engine* e, int adj, float* const modelReg[5], const ShotGeom& g, const SInterp* const rec[4],
                     float* dataIrreg, float* wfld = nullptr);
 void engine_born_host(Engine* e, int adj, float* const srcDtw[5], float* const dm[5], float* const data[5],

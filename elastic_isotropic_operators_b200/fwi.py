@@ -184,12 +184,21 @@ class FwiObjective:
     born: BornElasticShotsGpu on the same acquisition (setBackground(m) makes it
     the Jacobian at m); sampler: optional ElasticDatComp S; conv: optional
     ElasticConv (conv_type 1 or 2): m is then VpVsRho and the gradient goes
-    through ElasticConvJab^T; mask: optional gradient weights [3][nx][nz]."""
+    through ElasticConvJab^T; mask: optional gradient weights [3][nx][nz].
 
-    def __init__(self, nl, born, d_obs, sampler=None, conv=None, mask=None):
+    fused (default): gradients come from BornElasticShotsGpu.fwiGradient, which
+    reuses the source wavefield of the nonlinear forward in the Born adjoint
+    (two propagations per shot instead of three; the misfit and gradient agree
+    with the unfused evaluation to FP32 rounding).  It needs the Born
+    operator's source signals to be the nonlinear operator's sources and no
+    free surface; fused=False, or a free surface, takes the unfused path."""
+
+    def __init__(self, nl, born, d_obs, sampler=None, conv=None, mask=None, fused=True):
         self.nl, self.born, self.sampler, self.conv = nl, born, sampler, conv
         self.d_obs = np.asarray(_nd(d_obs), dtype=np.float32)
         self.mask = None if mask is None else np.asarray(_nd(mask), dtype=np.float32)
+        self.fused = bool(fused) and hasattr(born, "fwiGradient") and hasattr(nl, "sources") and \
+            not getattr(getattr(born, "fd", None), "surfaceCondition", 1)
         self.nfev = 0
 
     def _elastic(self, m):
@@ -217,16 +226,21 @@ class FwiObjective:
 
     def value_and_gradient(self, m):
         self.nfev += 1
-        ep, r = self.residual(m)
-        phi = 0.5 * dot64(r, r)
-        rfull = r
-        if self.sampler is not None:
-            rfull = np.zeros(self.nl.dataSpace().getNdArray().shape, np.float32)
-            self.sampler.adjoint(False, rfull, r)
-        self.born.setBackground(ep)
-        g = self.born.modelSpace()
-        self.born.adjoint(False, g, np.ascontiguousarray(rfull, dtype=np.float32))
-        g = np.array(_nd(g), dtype=np.float32)
+        if self.fused:
+            ep = self._elastic(m)
+            comps = None if self.sampler is None else ",".join(self.sampler.comp_list)
+            phi, g = self.born.fwiGradient(ep, self.nl.sources, self.d_obs, comps)
+        else:
+            ep, r = self.residual(m)
+            phi = 0.5 * dot64(r, r)
+            rfull = r
+            if self.sampler is not None:
+                rfull = np.zeros(self.nl.dataSpace().getNdArray().shape, np.float32)
+                self.sampler.adjoint(False, rfull, r)
+            self.born.setBackground(ep)
+            g = self.born.modelSpace()
+            self.born.adjoint(False, g, np.ascontiguousarray(rfull, dtype=np.float32))
+            g = np.array(_nd(g), dtype=np.float32)
         if self.conv is not None:
             jab = ElasticConvJab(m, self.conv.conv_type)
             gm = np.zeros_like(g)

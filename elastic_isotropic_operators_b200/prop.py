@@ -270,6 +270,11 @@ class _ElasticOp:
         """Born source-wavefield snapshots: 0 FP32, 1 BF16, 2 FP16."""
         check(self._L.eio_ctx_set_checkpoint_precision(self._ctx, int(mode)))
 
+    def setLanes(self, lanes):
+        """Shots of one multi-shot call run on up to ``lanes`` engines of this
+        context (default 2), each on its own stream and host thread."""
+        check(self._L.eio_ctx_set_lanes(self._ctx, int(lanes)))
+
     def getMedium(self):
         n = self.fd.nz * self.fd.nx
         out = [np.zeros((self.fd.nx, self.fd.nz), np.float32) for _ in range(5)]
@@ -511,6 +516,49 @@ class BornElasticShotsGpu(_ElasticOp):
                                        len(self._sigs), self._src_arr, self._rec_arr, self.nRecGeom))
         if mm is not m:
             m[...] = mm
+
+    _COMP_CODES = {"vx": 0, "vz": 1, "sxx": 2, "szz": 3, "sxz": 4, "p": 5}
+
+    def fwiGradient(self, elasticModel, sources, dObs, components=None, data=None):
+        """Misfit and gradient of 0.5 ||S F(m) - dObs||^2 in one pass per shot.
+
+        Sets elasticModel [3][nx][nz] as the background, then per shot runs the
+        nonlinear forward of ``sources`` (the source traces of
+        nonlinearFwiPropElasticShotsGpu, [nModelExp][5][nSrc][nts], nModelExp 1
+        or nExp) while recording the Born source wavefield, forms the residual
+        of the sampled components and runs the Born adjoint on the recorded
+        wavefield (two propagations per shot; the reference runs the nonlinear
+        forward, then BornElasticShotsGpu's adjoint, which propagates the source
+        again).  ``components``: a comma-separated list of vx, vz, sxx, szz, sxz,
+        p (ElasticDatComp's), all five fields when None; dObs has the sampled
+        shape [nExp][nComp][nRec][nts].  ``data`` (optional, [nExp][5][nRec][nts])
+        receives the modelled data.  Returns (misfit, gradient [3][nx][nz]).
+        No free surface (the Born operator has none)."""
+        comps = ["vx", "vz", "sxx", "szz", "sxz"] if components is None else \
+            [c.strip().lower() for c in components.split(",")]
+        if len(set(comps)) != len(comps) or any(c not in self._COMP_CODES for c in comps):
+            raise EioError(-1, "unknown or repeated data component in %r" % (components,))
+        codes = np.array([self._COMP_CODES[c] for c in comps], np.int32)
+        self.setBackground(elasticModel)
+        src = np.ascontiguousarray(_arr(sources), dtype=np.float32)
+        per = 5 * self.nSrcIrreg * self.fd.nts
+        if src.size % per or src.size // per not in (1, self.nExp):
+            raise EioError(-1, "sources must hold 1 or nExp shots of [5][nSrc][nts] traces")
+        d_obs = np.ascontiguousarray(_arr(dObs), dtype=np.float32)
+        if d_obs.shape != (self.nExp, len(comps), self.nRecIrreg, self.fd.nts):
+            raise EioError(-1, "dObs shape %s, expected %s" % (d_obs.shape, (self.nExp, len(comps),
+                                                                               self.nRecIrreg, self.fd.nts)))
+        dd = None
+        if data is not None:
+            dd = _arr(data)
+            if dd.shape != (self.nExp, 5, self.nRecIrreg, self.fd.nts) or not dd.flags["C_CONTIGUOUS"]:
+                raise EioError(-1, "data must be a contiguous float32 [nExp][5][nRec][nts] array")
+        grad = np.zeros((3, self.fd.nx, self.fd.nz), np.float32)
+        phi = ctypes.c_double()
+        check(self._L.eio_fwi_gradient(self._ctx, self.nExp, src.size // per, fptr(src), fptr(d_obs), len(codes),
+                                       _lib.iptr(codes), self._src_arr, self._rec_arr, self.nRecGeom,
+                                       None if dd is None else dd.ctypes.data, fptr(grad), ctypes.byref(phi)))
+        return phi.value, grad
 
     def prepareShot(self, iExp):
         """Regular-grid inputs of shot iExp for the single-shot *_reg_dev entry

@@ -177,6 +177,24 @@ int eio_ctx_get_lanes(const eio_ctx *c, int *lanes, int *active);
 int eio_born_shots_dev(eio_ctx *c, int adj, int nShots, float *const *srcDtw, float *const dm[5],
                        float *const *data, const int *const *srcPos, const int *nSrc,
                        const int *const *recPos, const int *nRec);
+/* FWI misfit and gradient in one pass per shot (no reference counterpart:
+ * the reference runs nonlinearFwiPropElasticShotsGpu, then BornElasticShotsGpu
+ * adjoint, three propagations per shot). Per shot, the nonlinear forward of
+ * the source traces `model` (irregular, as eio_nl_forward) records the Born
+ * source-wavefield history. The sampled residual r = S d - dObs follows, then
+ * the Born adjoint of S^T r on that history: two propagations per shot. The
+ * nonlinear forward injects the coarse traces with the time filter, where the
+ * Born operators inject host-interpolated fine traces of the same signal, so
+ * the history agrees with theirs to rounding. S picks nComp components, codes
+ * 0..4 = vx, vz, sxx, szz, sxz and 5 = pressure 0.5 (sxx + szz) (the data
+ * component sampler of the FWI scripts).
+ * dObs: [nExp][nComp][nRecIrreg][nts]; data (optional, may be NULL):
+ * [nExp][5][nRecIrreg][nts] modelled; grad: [3][nx][nz], overwritten with
+ * the Born adjoint image of the residual; misfit: 0.5 r.r (FP64 sum, shots in order).
+ * Runs on the context's lanes and shot windows; no free surface. */
+int eio_fwi_gradient(eio_ctx *c, int nExp, int nModelExp, const float *model, const float *dObs, int nComp,
+                     const int *comps, eio_sinterp *const *src, eio_sinterp *const *rec, int nRecGeom,
+                     float *data, float *grad, double *misfit);
 /* Cropped shots (no reference counterpart; the reference propagates every shot
  * on the whole grid). Shot i of the next multi-shot calls (eio_nl_forward,
  * eio_nl_adjoint, eio_born_forward, eio_born_adjoint with nExp == nShots)
