@@ -85,6 +85,12 @@ _SIGS = {
     "eio_born_shots_dev": (I, [P, I, I, P, P, P, P, IP, P, IP]),
     "eio_fwi_gradient": (I, [P, I, I, FP, FP, I, IP, P, P, I, P, FP, ctypes.POINTER(ctypes.c_double)]),
     "eio_reduce64": (I, [I, I, I, P, P, ctypes.c_longlong, I, ctypes.POINTER(ctypes.c_double)]),
+    "eio_cnn_conv3x3": (I, [I, I, I, I, I, P, P, P, I, P, P, P]),
+    "eio_cnn_wgrad_scratch": (I, [I, I, I, I, I, ctypes.POINTER(ctypes.c_longlong)]),
+    "eio_cnn_conv3x3_wgrad": (I, [I, I, I, I, I, P, P, P, P, ctypes.c_longlong, P]),
+    "eio_cnn_flip": (I, [I, I, P, P, P]),
+    "eio_cnn_mse": (I, [ctypes.c_longlong, I, I, P, P, P, P, P, P]),
+    "eio_cnn_adam": (I, [ctypes.c_longlong, P, P, P, P, F, F, F, F, I, P, P]),
     "eio_ctx_pair_stats": (I, [P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]),
     "eio_nl_fwd_reg": (I, [P, P, P, P, IP, P, IP]),
     "eio_nl_adj_reg": (I, [P, P, P, P, IP, P, IP]),

@@ -1,0 +1,483 @@
+// Kernels of the learned FWI preconditioner: a small fully convolutional
+// network (3x3 convolutions, stride 1, zero padding 1, no biases, ReLU between
+// layers) that maps an FWI gradient to an approximate Gauss-Newton model
+// update.  The reference has no learned component; this network is trained on
+// pairs (J^T J dm, dm) that the Born operators of this library produce.
+//
+// Layout: activations NHWC in BF16, C = 16 or 32 channels per pixel (32 or
+// 64 bytes, so a pixel is whole 16-byte vectors); weights [9][Cout][Cin] BF16
+// (tap = 3 dy + dx) with FP32 master copies for the optimiser.  Products run
+// on the tensor cores as implicit GEMMs with FP32 accumulation
+// (mma.sync m16n8k16 BF16):
+//
+// * k_conv3: y[p][co] = sum_tap sum_ci x[p + off(tap)][ci] w[tap][co][ci],
+//   off(tap) = (dy - 1, dx - 1).  M = pixels (16 per fragment), N = Cout,
+//   K = 9 Cin.  A CTA computes 8 rows x 32 columns of output pixels, one warp
+//   per row; the input tile with its one-pixel halo and all weights sit in
+//   shared memory, each pixel row padded by 8 BF16 so that the 32-bit
+//   fragment loads of 8 consecutive pixels hit 32 distinct banks.  Epilogue:
+//   optional ReLU, or a multiply by (mask > 0) (the ReLU derivative of the
+//   layer below, for the backward pass), BF16 store and an optional FP32 copy.
+// * the data gradient is the same kernel on the flipped, transposed weights
+//   wt[tap][ci][co] = w[8 - tap][co][ci] (k_flip).
+// * k_conv3_wgrad: dw[tap][co][ci] = sum_p dy[p][co] x[p + off(tap)][ci],
+//   M = Cout, N = Cin, K = pixels; one warp per tap, both operands fetched
+//   with ldmatrix.trans from the staged tiles.  A persistent grid keeps its
+//   partial sums in registers over all its tiles and writes them once; the
+//   partials are then summed block by block in a fixed order, so the weight
+//   gradient does not change from run to run.
+// * k_mse: loss 0.5 sum (y - t)^2 / count over the first nc channels, its
+//   derivative in BF16; k_adam: Adam step on the FP32 master weights with the
+//   BF16 copy written alongside.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <string>
+
+#include "eio_internal.h"
+
+namespace eio {
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+constexpr int CT_H = 8;     // output rows of a CTA (one warp each)
+constexpr int CT_W = 32;    // output columns of a CTA (two 16-pixel fragments per warp)
+constexpr int SR = CT_H + 2, SC = CT_W + 2;   // staged input tile with its halo
+constexpr int FWD_THREADS = 32 * CT_H;
+constexpr int WG_THREADS = 32 * 9;            // weight gradient: one warp per tap
+
+__device__ __forceinline__ void mma_bf16(float* d, const uint32_t* a, uint32_t b0, uint32_t b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ void ldsm_x4_trans(uint32_t* r, const bf16* p)
+{
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+
+__device__ __forceinline__ uint32_t lds32(const bf16* p) { return *reinterpret_cast<const uint32_t*>(p); }
+
+// rows x cols pixels of image n starting at (y0 - halo, x0 - halo) into shared
+// memory (pixel stride C + 8); pixels outside the image are zero
+template <int C>
+__device__ __forceinline__ void stage_pixels(const bf16* __restrict__ x, int H, int W, int n, int y0, int x0,
+                                             int halo, int rows, int cols, bf16* s, int nthr)
+{
+    constexpr int V = C / 8;
+    constexpr int CP = C + 8;
+    const int total = rows * cols * V;
+    for (int i = threadIdx.x; i < total; i += nthr) {
+        const int v = i % V, p = i / V;
+        const int r = p / cols, c = p - r * cols;
+        const int gy = y0 - halo + r, gx = x0 - halo + c;
+        uint4 val = make_uint4(0u, 0u, 0u, 0u);
+        if (gy >= 0 && gy < H && gx >= 0 && gx < W)
+            val = *reinterpret_cast<const uint4*>(x + (((size_t)n * H + gy) * W + gx) * C + v * 8);
+        *reinterpret_cast<uint4*>(s + (size_t)p * CP + v * 8) = val;
+    }
+}
+
+template <int CIN, int COUT>
+constexpr int conv_smem() { return (SR * SC * (CIN + 8) + 9 * COUT * (CIN + 8)) * 2; }
+
+template <int CIN, int COUT>
+constexpr int wgrad_smem() { return (SR * SC * (CIN + 8) + CT_H * CT_W * (COUT + 8)) * 2; }
+
+// EPI 0: optional ReLU; EPI 1: multiply by (mask > 0), mask NHWC with COUT channels
+template <int CIN, int COUT, int EPI>
+__global__ void __launch_bounds__(FWD_THREADS) k_conv3(const bf16* __restrict__ x, const bf16* __restrict__ w,
+                                                      const bf16* __restrict__ mask, int relu, int H, int W,
+                                                      bf16* __restrict__ y, float* __restrict__ y32)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int CP = CIN + 8;
+    constexpr int NT = COUT / 8;
+    bf16* sx = reinterpret_cast<bf16*>(smem);
+    bf16* sw = sx + SR * SC * CP;
+    const int n = blockIdx.z, y0 = blockIdx.y * CT_H, x0 = blockIdx.x * CT_W;
+    for (int i = threadIdx.x; i < 9 * COUT * (CIN / 8); i += FWD_THREADS) {
+        const int v = i % (CIN / 8), row = i / (CIN / 8);
+        *reinterpret_cast<uint4*>(sw + row * CP + v * 8) = *reinterpret_cast<const uint4*>(w + row * CIN + v * 8);
+    }
+    stage_pixels<CIN>(x, H, W, n, y0, x0, 1, SR, SC, sx, FWD_THREADS);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    float acc[2][NT][4];
+#pragma unroll
+    for (int m = 0; m < 2; m++)
+#pragma unroll
+        for (int j = 0; j < NT; j++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[m][j][q] = 0.f;
+#pragma unroll 1
+    for (int tap = 0; tap < 9; tap++) {
+        const int dy = tap / 3, dx = tap - 3 * dy;
+        const bf16* srow = sx + ((warp + dy) * SC + dx) * CP;
+#pragma unroll
+        for (int kc = 0; kc < CIN / 16; kc++) {
+            uint32_t a[2][4];
+#pragma unroll
+            for (int m = 0; m < 2; m++) {
+                const bf16* p0 = srow + (m * 16 + g) * CP + kc * 16 + 2 * t;
+                const bf16* p1 = p0 + 8 * CP;
+                a[m][0] = lds32(p0);
+                a[m][1] = lds32(p1);
+                a[m][2] = lds32(p0 + 8);
+                a[m][3] = lds32(p1 + 8);
+            }
+#pragma unroll
+            for (int j = 0; j < NT; j++) {
+                const bf16* pw = sw + (tap * COUT + j * 8 + g) * CP + kc * 16 + 2 * t;
+                const uint32_t b0 = lds32(pw), b1 = lds32(pw + 8);
+                mma_bf16(acc[0][j], a[0], b0, b1);
+                mma_bf16(acc[1][j], a[1], b0, b1);
+            }
+        }
+    }
+    const int oy = y0 + warp;
+    if (oy >= H) return;
+#pragma unroll
+    for (int m = 0; m < 2; m++)
+#pragma unroll
+        for (int half = 0; half < 2; half++) {
+            const int ox = x0 + m * 16 + g + 8 * half;
+            if (ox >= W) continue;
+            const size_t pix = ((size_t)n * H + oy) * W + ox;
+#pragma unroll
+            for (int j = 0; j < NT; j++) {
+                const int co = j * 8 + 2 * t;
+                float v0 = acc[m][j][2 * half], v1 = acc[m][j][2 * half + 1];
+                if constexpr (EPI == 0) {
+                    if (relu) { v0 = fmaxf(v0, 0.f); v1 = fmaxf(v1, 0.f); }
+                } else {
+                    const __nv_bfloat162 mk = *reinterpret_cast<const __nv_bfloat162*>(mask + pix * COUT + co);
+                    if (!(__bfloat162float(mk.x) > 0.f)) v0 = 0.f;
+                    if (!(__bfloat162float(mk.y) > 0.f)) v1 = 0.f;
+                }
+                *reinterpret_cast<__nv_bfloat162*>(y + pix * COUT + co) = __floats2bfloat162_rn(v0, v1);
+                if (y32) *reinterpret_cast<float2*>(y32 + pix * COUT + co) = make_float2(v0, v1);
+            }
+        }
+}
+
+// partial weight gradients of the tiles tile = blockIdx.x, + gridDim.x, ...
+// into part[blockIdx.x][9][COUT][CIN]
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(WG_THREADS) k_conv3_wgrad(const bf16* __restrict__ x, const bf16* __restrict__ dy,
+                                                           int N, int H, int W, float* __restrict__ part)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int CPX = CIN + 8, CPY = COUT + 8;
+    constexpr int MT = COUT / 16, NT = CIN / 8;
+    bf16* sx = reinterpret_cast<bf16*>(smem);
+    bf16* sd = sx + SR * SC * CPX;
+    const int tap = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int ty = tap / 3, tx = tap - 3 * ty;
+    const int tilesX = (W + CT_W - 1) / CT_W, tilesY = (H + CT_H - 1) / CT_H;
+    const int ntiles = tilesX * tilesY * N;
+    float acc[MT][NT][4];
+#pragma unroll
+    for (int m = 0; m < MT; m++)
+#pragma unroll
+        for (int j = 0; j < NT; j++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[m][j][q] = 0.f;
+    const int mat = lane >> 3, mrow = lane & 7;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int n = tile / (tilesX * tilesY);
+        const int rem = tile - n * tilesX * tilesY;
+        const int y0 = (rem / tilesX) * CT_H, x0 = (rem % tilesX) * CT_W;
+        __syncthreads();   // the previous tile's fragments are read
+        stage_pixels<CIN>(x, H, W, n, y0, x0, 1, SR, SC, sx, WG_THREADS);
+        stage_pixels<COUT>(dy, H, W, n, y0, x0, 0, CT_H, CT_W, sd, WG_THREADS);
+        __syncthreads();
+#pragma unroll 1
+        for (int chunk = 0; chunk < CT_H * CT_W / 16; chunk++) {
+            const int r = chunk / (CT_W / 16), c0 = (chunk % (CT_W / 16)) * 16;
+            uint32_t a[MT][4];
+#pragma unroll
+            for (int m = 0; m < MT; m++)
+                ldsm_x4_trans(a[m], sd + (r * CT_W + c0 + (mat >> 1) * 8 + mrow) * CPY + m * 16 + (mat & 1) * 8);
+            uint32_t b[NT][2];
+#pragma unroll
+            for (int j2 = 0; j2 < NT / 2; j2++) {
+                uint32_t q[4];
+                ldsm_x4_trans(q, sx + ((r + ty) * SC + c0 + tx + (mat & 1) * 8 + mrow) * CPX + (2 * j2 + (mat >> 1)) * 8);
+                b[2 * j2][0] = q[0];
+                b[2 * j2][1] = q[1];
+                b[2 * j2 + 1][0] = q[2];
+                b[2 * j2 + 1][1] = q[3];
+            }
+#pragma unroll
+            for (int m = 0; m < MT; m++)
+#pragma unroll
+                for (int j = 0; j < NT; j++) mma_bf16(acc[m][j], a[m], b[j][0], b[j][1]);
+        }
+    }
+    float* out = part + (size_t)blockIdx.x * 9 * COUT * CIN + (size_t)tap * COUT * CIN;
+#pragma unroll
+    for (int m = 0; m < MT; m++)
+#pragma unroll
+        for (int j = 0; j < NT; j++) {
+            const int co = m * 16 + g, ci = j * 8 + 2 * t;
+            *reinterpret_cast<float2*>(out + co * CIN + ci) = make_float2(acc[m][j][0], acc[m][j][1]);
+            *reinterpret_cast<float2*>(out + (co + 8) * CIN + ci) = make_float2(acc[m][j][2], acc[m][j][3]);
+        }
+}
+
+// out[j] = sum over blocks b (in order) of part[b][j]
+__global__ void k_sum_partials(const float* __restrict__ part, int nblk, int len, float* __restrict__ out)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= len) return;
+    float s = 0.f;
+    for (int b = 0; b < nblk; b++) s += part[(size_t)b * len + j];
+    out[j] = s;
+}
+
+// wt[tap][ci][co] = w[8 - tap][co][ci]
+__global__ void k_flip(const bf16* __restrict__ w, int cin, int cout, bf16* __restrict__ wt)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 9 * cin * cout) return;
+    const int tap = i / (cin * cout), rem = i - tap * cin * cout;
+    const int ci = rem / cout, co = rem - ci * cout;
+    wt[i] = w[((size_t)(8 - tap) * cout + co) * cin + ci];
+}
+
+constexpr int MSE_THREADS = 256;
+
+// dz = (y - t) * scale on channels < nc (0 elsewhere), partial sums of (y - t)^2 per block
+__global__ void __launch_bounds__(MSE_THREADS) k_mse(const float* __restrict__ y, const float* __restrict__ tgt,
+                                                     long long npix, int C, int nc, float scale,
+                                                     bf16* __restrict__ dz, double* __restrict__ part)
+{
+    double acc = 0.0;
+    const long long n = npix * C;
+    for (long long i = (long long)blockIdx.x * MSE_THREADS + threadIdx.x; i < n;
+         i += (long long)gridDim.x * MSE_THREADS) {
+        const long long p = i / C;
+        const int c = (int)(i - p * C);
+        float d = 0.f;
+        if (c < nc) {
+            d = y[i] - tgt[p * nc + c];
+            acc += (double)d * d;
+        }
+        dz[i] = __float2bfloat16_rn(d * scale);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    __shared__ double ws[MSE_THREADS / 32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int k = 0; k < MSE_THREADS / 32; k++) s += ws[k];
+        part[blockIdx.x] = s;
+    }
+}
+
+__global__ void k_sum_double(const double* __restrict__ part, int m, double scale, double* __restrict__ out)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s = 0.0;
+        for (int i = 0; i < m; i++) s += part[i];
+        *out = s * scale;
+    }
+}
+
+__global__ void k_adam(float* __restrict__ p, float* __restrict__ m, float* __restrict__ v,
+                       const float* __restrict__ g, long long n, float lr, float b1, float b2, float eps, float c1,
+                       float c2, bf16* __restrict__ pb)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float pi = p[i] - lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+    p[i] = pi;
+    if (pb) pb[i] = __float2bfloat16_rn(pi);
+}
+
+#define CCUDA(x)                                                                                       \
+    do {                                                                                               \
+        cudaError_t e_ = (x);                                                                          \
+        if (e_ != cudaSuccess) throw Error(EIO_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+void check_channels(int cin, int cout)
+{
+    if ((cin != 16 && cin != 32) || (cout != 16 && cout != 32))
+        throw Error(EIO_ERR_ARG, "convolution channels must be 16 or 32 (got " + std::to_string(cin) + " -> " +
+                                     std::to_string(cout) + ")");
+}
+
+void check_dims(int n, int h, int w)
+{
+    if (n < 1 || h < 1 || w < 1 || n > 65535 || (h + CT_H - 1) / CT_H > 65535)
+        throw Error(EIO_ERR_ARG, "bad batch or image size");
+}
+
+void check_ptr(const void* p, const char* what)
+{
+    if (!p) throw Error(EIO_ERR_ARG, std::string("null ") + what);
+    if (reinterpret_cast<uintptr_t>(p) % 16) throw Error(EIO_ERR_ARG, std::string(what) + " not 16-byte aligned");
+}
+
+template <int CIN, int COUT, int EPI>
+void launch_conv(int n, int h, int w, const bf16* x, const bf16* wt, const bf16* mask, int relu, bf16* y,
+                 float* y32, cudaStream_t st)
+{
+    constexpr int sm = conv_smem<CIN, COUT>();
+    static bool opened = false;   // the attribute is per function and device-independent in value
+    if (!opened) {
+        CCUDA(cudaFuncSetAttribute(k_conv3<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        opened = true;
+    }
+    const dim3 grid((w + CT_W - 1) / CT_W, (h + CT_H - 1) / CT_H, n);
+    k_conv3<CIN, COUT, EPI><<<grid, FWD_THREADS, sm, st>>>(x, wt, mask, relu, h, w, y, y32);
+    CCUDA(cudaGetLastError());
+}
+
+template <int CIN, int COUT>
+int wgrad_blocks(int n, int h, int w)
+{
+    static int per_sm = 0, nsm = 0;
+    if (!per_sm) {
+        constexpr int sm = wgrad_smem<CIN, COUT>();
+        CCUDA(cudaFuncSetAttribute(k_conv3_wgrad<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        int dev = 0;
+        CCUDA(cudaGetDevice(&dev));
+        CCUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        CCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv3_wgrad<CIN, COUT>, WG_THREADS, sm));
+        if (per_sm < 1) per_sm = 1;
+    }
+    const long long tiles = (long long)((w + CT_W - 1) / CT_W) * ((h + CT_H - 1) / CT_H) * n;
+    return (int)std::min<long long>(tiles, (long long)per_sm * nsm);
+}
+
+}  // namespace
+
+void cnn_conv3x3(int n, int h, int w, int cin, int cout, const void* x, const void* wt, const void* mask, int relu,
+                 void* y, float* y32, void* stream)
+{
+    check_channels(cin, cout);
+    check_dims(n, h, w);
+    check_ptr(x, "input");
+    check_ptr(wt, "weights");
+    check_ptr(y, "output");
+    if (mask) check_ptr(mask, "mask");
+    if (y32) check_ptr(y32, "FP32 output");
+    auto st = static_cast<cudaStream_t>(stream);
+    auto X = static_cast<const bf16*>(x);
+    auto Wt = static_cast<const bf16*>(wt);
+    auto M = static_cast<const bf16*>(mask);
+    auto Y = static_cast<bf16*>(y);
+#define CONV_CASE(CI, CO)                                                            \
+    if (cin == CI && cout == CO) {                                                   \
+        if (M) launch_conv<CI, CO, 1>(n, h, w, X, Wt, M, 0, Y, y32, st);             \
+        else launch_conv<CI, CO, 0>(n, h, w, X, Wt, nullptr, relu, Y, y32, st);      \
+        return;                                                                      \
+    }
+    CONV_CASE(16, 16)
+    CONV_CASE(16, 32)
+    CONV_CASE(32, 16)
+    CONV_CASE(32, 32)
+#undef CONV_CASE
+}
+
+long long cnn_wgrad_scratch(int n, int h, int w, int cin, int cout)
+{
+    check_channels(cin, cout);
+    check_dims(n, h, w);
+    int nb = 0;
+    if (cin == 16 && cout == 16) nb = wgrad_blocks<16, 16>(n, h, w);
+    if (cin == 16 && cout == 32) nb = wgrad_blocks<16, 32>(n, h, w);
+    if (cin == 32 && cout == 16) nb = wgrad_blocks<32, 16>(n, h, w);
+    if (cin == 32 && cout == 32) nb = wgrad_blocks<32, 32>(n, h, w);
+    return (long long)nb * 9 * cin * cout;
+}
+
+void cnn_conv3x3_wgrad(int n, int h, int w, int cin, int cout, const void* x, const void* dy, float* dw,
+                       float* scratch, long long scratchFloats, void* stream)
+{
+    check_channels(cin, cout);
+    check_dims(n, h, w);
+    check_ptr(x, "input");
+    check_ptr(dy, "output gradient");
+    check_ptr(dw, "weight gradient");
+    check_ptr(scratch, "scratch");
+    const long long need = cnn_wgrad_scratch(n, h, w, cin, cout);
+    if (scratchFloats < need)
+        throw Error(EIO_ERR_ARG, "weight-gradient scratch holds " + std::to_string(scratchFloats) + " floats, needs " +
+                                     std::to_string(need));
+    const int nb = (int)(need / (9LL * cin * cout));
+    auto st = static_cast<cudaStream_t>(stream);
+    auto X = static_cast<const bf16*>(x);
+    auto D = static_cast<const bf16*>(dy);
+#define WG_CASE(CI, CO)                                                                                     \
+    if (cin == CI && cout == CO)                                                                            \
+        k_conv3_wgrad<CI, CO><<<nb, WG_THREADS, wgrad_smem<CI, CO>(), st>>>(X, D, n, h, w, scratch);
+    WG_CASE(16, 16)
+    WG_CASE(16, 32)
+    WG_CASE(32, 16)
+    WG_CASE(32, 32)
+#undef WG_CASE
+    CCUDA(cudaGetLastError());
+    const int len = 9 * cin * cout;
+    k_sum_partials<<<(len + 255) / 256, 256, 0, st>>>(scratch, nb, len, dw);
+    CCUDA(cudaGetLastError());
+}
+
+void cnn_flip(int cin, int cout, const void* w, void* wt, void* stream)
+{
+    check_channels(cin, cout);
+    if (!w || !wt) throw Error(EIO_ERR_ARG, "null weights");
+    const int len = 9 * cin * cout;
+    k_flip<<<(len + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<const bf16*>(w), cin,
+                                                                             cout, static_cast<bf16*>(wt));
+    CCUDA(cudaGetLastError());
+}
+
+void cnn_mse(long long npix, int c, int nc, const float* y32, const float* target, void* dz, double* part,
+             double* loss, void* stream)
+{
+    constexpr int nPart = CNN_MSE_PARTIALS;   // fixed, so the summation order does not depend on the device
+    if (npix < 1 || c < 1 || nc < 1 || nc > c) throw Error(EIO_ERR_ARG, "bad loss sizes");
+    if (!y32 || !target || !dz || !part || !loss) throw Error(EIO_ERR_ARG, "null loss buffer");
+    auto st = static_cast<cudaStream_t>(stream);
+    const double cnt = (double)npix * nc;
+    k_mse<<<nPart, MSE_THREADS, 0, st>>>(y32, target, npix, c, nc, (float)(1.0 / cnt), static_cast<bf16*>(dz), part);
+    CCUDA(cudaGetLastError());
+    k_sum_double<<<1, 32, 0, st>>>(part, nPart, 0.5 / cnt, loss);
+    CCUDA(cudaGetLastError());
+}
+
+void cnn_adam(long long n, float* p, float* m, float* v, const float* g, float lr, float b1, float b2, float eps,
+              int step, void* pb, void* stream)
+{
+    if (n < 1 || !p || !m || !v || !g || step < 1) throw Error(EIO_ERR_ARG, "bad Adam arguments");
+    const float c1 = (float)(1.0 / (1.0 - std::pow((double)b1, step)));
+    const float c2 = (float)(1.0 / (1.0 - std::pow((double)b2, step)));
+    k_adam<<<(unsigned)((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        p, m, v, g, n, lr, b1, b2, eps, c1, c2, static_cast<bf16*>(pb));
+    CCUDA(cudaGetLastError());
+}
+
+}  // namespace eio

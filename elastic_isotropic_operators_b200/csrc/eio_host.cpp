@@ -1405,3 +1405,30 @@ EIO_API int eio_fwi_gradient(eio_ctx* c, int nExp, int nModelExp, const float* m
         image_to_model(c, nl, dm, sl, grad);
     });
 }
+
+// ------------------------------------------------------------ learned preconditioner
+EIO_API int eio_cnn_conv3x3(int n, int h, int w, int cin, int cout, const void* x, const void* wt, const void* mask,
+                            int relu, void* y, float* y32, void* stream) {
+    return guarded([&] { cnn_conv3x3(n, h, w, cin, cout, x, wt, mask, relu, y, y32, stream); });
+}
+EIO_API int eio_cnn_wgrad_scratch(int n, int h, int w, int cin, int cout, long long* floats) {
+    return guarded([&] {
+        if (!floats) throw Error(EIO_ERR_ARG, "null result");
+        *floats = cnn_wgrad_scratch(n, h, w, cin, cout);
+    });
+}
+EIO_API int eio_cnn_conv3x3_wgrad(int n, int h, int w, int cin, int cout, const void* x, const void* dy, float* dw,
+                                  float* scratch, long long scratchFloats, void* stream) {
+    return guarded([&] { cnn_conv3x3_wgrad(n, h, w, cin, cout, x, dy, dw, scratch, scratchFloats, stream); });
+}
+EIO_API int eio_cnn_flip(int cin, int cout, const void* w, void* wt, void* stream) {
+    return guarded([&] { cnn_flip(cin, cout, w, wt, stream); });
+}
+EIO_API int eio_cnn_mse(long long npix, int c, int nc, const float* y32, const float* target, void* dz,
+                        double* scratch, double* loss, void* stream) {
+    return guarded([&] { cnn_mse(npix, c, nc, y32, target, dz, scratch, loss, stream); });
+}
+EIO_API int eio_cnn_adam(long long n, float* p, float* m, float* v, const float* g, float lr, float b1, float b2,
+                         float eps, int step, void* pb, void* stream) {
+    return guarded([&] { cnn_adam(n, p, m, v, g, lr, b1, b2, eps, step, pb, stream); });
+}

@@ -82,6 +82,19 @@ void engine_dm_add(Engine* e, float* const dst[5]);     // dst += this lane's im
 int engine_window_ix0(const Engine* e);
 // FP64 sum of x*y (op 0) or (x-y)^2 (op 1) over n values (dtype 0 FP32, 1 FP64) on GPU `device`
 double reduce64(int device, int op, int dtype, const void* x, const void* y, long long n, bool on_device);
+
+// learned preconditioner (eio_cnn.cu); device pointers, work queued on `stream`
+constexpr int CNN_MSE_PARTIALS = 1024;
+void cnn_conv3x3(int n, int h, int w, int cin, int cout, const void* x, const void* wt, const void* mask, int relu,
+                 void* y, float* y32, void* stream);
+long long cnn_wgrad_scratch(int n, int h, int w, int cin, int cout);
+void cnn_conv3x3_wgrad(int n, int h, int w, int cin, int cout, const void* x, const void* dy, float* dw,
+                       float* scratch, long long scratchFloats, void* stream);
+void cnn_flip(int cin, int cout, const void* w, void* wt, void* stream);
+void cnn_mse(long long npix, int c, int nc, const float* y32, const float* target, void* dz, double* part,
+             double* loss, void* stream);
+void cnn_adam(long long n, float* p, float* m, float* v, const float* g, float lr, float b1, float b2, float eps,
+              int step, void* pb, void* stream);
 void engine_stats(Engine* e, int enable, int reset, long long* launches, long long* step_launches, double* step_ms,
                   long long* pair_launches, double* pair_ms);
 

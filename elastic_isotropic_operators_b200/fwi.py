@@ -286,25 +286,50 @@ class _Scaled:
 
 
 def lbfgs(objective, m0, niter=10, memory=5, minBound=None, maxBound=None, init_step=None, c1=1e-4,
-          max_backtrack=8, callback=None, scale=None):
+          max_backtrack=8, callback=None, scale=None, precond=None, stats=None):
     """Minimise ``objective``; with ``scale`` (an array of m's shape, e.g. the
     starting model) the search runs on m / scale so that parameters of very
-    different units weigh alike.  See _lbfgs for the method."""
+    different units weigh alike.  ``precond(m, g)`` (e.g. a
+    precond.LearnedPreconditioner) proposes a model update that is tried before
+    each L-BFGS step and kept only when the exact misfit accepts it; ``stats``
+    (a dict) receives the counts of accepted and rejected learned steps.  See
+    _lbfgs for the method."""
     if scale is None:
-        return _lbfgs(objective, m0, niter, memory, minBound, maxBound, init_step, c1, max_backtrack, callback)
+        return _lbfgs(objective, m0, niter, memory, minBound, maxBound, init_step, c1, max_backtrack, callback,
+                      precond, stats)
     sc = np.where(np.asarray(scale) != 0, np.asarray(scale), 1.0).astype(np.float32)
     lo = None if minBound is None else minBound / sc
     hi = None if maxBound is None else maxBound / sc
     if lo is not None and hi is not None:
         lo, hi = np.minimum(lo, hi), np.maximum(lo, hi)
     cb = None if callback is None else (lambda it, x, f, g: callback(it, x * sc, f, g / sc))
+    pc = None if precond is None else (lambda x, gx: precond((x * sc).astype(np.float32), gx / sc) / sc)
     x, hist = _lbfgs(_Scaled(objective, sc), np.asarray(m0) / sc, niter, memory, lo, hi, init_step, c1,
-                     max_backtrack, cb)
+                     max_backtrack, cb, pc, stats)
     return (x * sc).astype(np.float32), hist
 
 
+def _learned_step(objective, precond, m, f, g, minBound, maxBound, c1, tries=3):
+    """Try the update proposed by precond(m, g) at full, half and quarter
+    length; the exact misfit decides: the first trial point that lowers it
+    (with the Armijo condition when the proposal is a descent direction) is
+    returned with its misfit, else None."""
+    d = np.asarray(precond(m, g), dtype=np.float64)
+    if not np.isfinite(d).all() or not d.any():
+        return None
+    descent = dot64(g, d) < 0
+    step = 1.0
+    for _ in range(tries):
+        mt = _project((m + step * d).astype(np.float32), minBound, maxBound)
+        ft = objective.value(mt)
+        if ft < f and (not descent or ft <= f + c1 * dot64(g, mt - m)):
+            return mt, ft
+        step *= 0.5
+    return None
+
+
 def _lbfgs(objective, m0, niter=10, memory=5, minBound=None, maxBound=None, init_step=None, c1=1e-4,
-           max_backtrack=8, callback=None):
+           max_backtrack=8, callback=None, precond=None, stats=None):
     """Minimise ``objective`` (value_and_gradient(m), value(m)) from m0.
 
     Two-loop recursion over the last ``memory`` pairs on the variables that no
@@ -314,6 +339,9 @@ def _lbfgs(objective, m0, niter=10, memory=5, minBound=None, maxBound=None, init
     itself (default 1 %); trial points are projected onto [minBound,
     maxBound]; backtracking halves the step until the Armijo condition holds,
     and a failed search restarts once from the projected steepest descent.
+    With ``precond``, each iteration first tries the proposed update
+    (_learned_step) and falls back to the L-BFGS step when the misfit rejects
+    it; accepted learned steps enter the L-BFGS memory like any other.
     Returns (m, history) with history the objective values (FP64)."""
     m = _project(np.array(m0, dtype=np.float32, copy=True), minBound, maxBound)
     f, g = objective.value_and_gradient(m)
@@ -321,7 +349,30 @@ def _lbfgs(objective, m0, niter=10, memory=5, minBound=None, maxBound=None, init
     S, Y, rho = [], [], []
     it = 0
     restarted = False
+    if stats is not None:
+        stats.setdefault("learned", 0)
+        stats.setdefault("rejected", 0)
     while it < niter:
+        if precond is not None:
+            trial = _learned_step(objective, precond, m, f, g, minBound, maxBound, c1)
+            if stats is not None:
+                stats["learned" if trial is not None else "rejected"] += 1
+            if trial is not None:
+                mt = trial[0]
+                ft, gt = objective.value_and_gradient(mt)
+                s = (mt - m).astype(np.float64)
+                y = (gt - g).astype(np.float64)
+                sy = dot64(s, y)
+                if sy > 1e-10 * np.sqrt(dot64(s, s) * dot64(y, y)):
+                    S.append(s); Y.append(y); rho.append(1.0 / sy)
+                    if len(S) > memory:
+                        S.pop(0); Y.pop(0); rho.pop(0)
+                m, f, g = mt, ft, gt
+                hist.append(f)
+                if callback is not None:
+                    callback(it, m, f, g)
+                it += 1
+                continue
         free = _free(m, g, minBound, maxBound)
         q = np.where(free, g, 0).astype(np.float64)
         alpha = []

@@ -1,0 +1,285 @@
+"""Learned FWI preconditioner: a small convolutional network that maps an FWI
+gradient to an approximate Gauss-Newton model update, trained on pairs that
+the Born operators produce, with the exact misfit accepting or rejecting each
+learned step (``fwi.lbfgs(..., precond=...)``).
+
+The reference has no learned component (its FWI scripts run pySolver's
+L-BFGS on the plain gradient); the network and its kernels are this
+library's.  Training pairs: for a background m0 and seeded smooth
+perturbations dm, the Born forward then adjoint gives g = J^T J dm, the
+Gauss-Newton Hessian applied to dm; the network learns dm from g.  Near m0
+the FWI gradient is g = J^T J (m - m_true) to first order, so the learned
+update is -net(g).
+
+Features per pixel (16 input channels, 4 used): the three gradient channels
+relative to the background scale (g_c * mean(m0_c)), divided by their RMS
+over the model, and an illumination map (the Born normal operator applied to
+a constant relative perturbation, normalised to a maximum of 1).  Targets:
+the relative perturbation dm_c / mean(m0_c) times K / RMS(features), K fixed
+on the training set so that the targets are O(1).  The network: 3x3
+convolutions 16 -> 32 -> ... -> 32 -> 16 (3 outputs used), ReLU between
+layers, no biases; BF16 weights and activations, FP32 accumulation, FP32
+master weights with Adam.  Every product runs in the library's kernels
+(``eio_cnn_*``); torch only holds the device memory and the stream.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+__all__ = ["ConvNet", "LearnedPreconditioner", "smooth_perturbation"]
+
+_CIN = 16    # input channels of the first layer (4 features used)
+_COUT = 16   # output channels of the last layer (3 used)
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise _lib.EioError(-3, "the learned preconditioner needs a CUDA device")
+    return torch
+
+
+def _p(t):
+    return ctypes.c_void_p(int(t.data_ptr()))
+
+
+class ConvNet:
+    """The network: ``hidden`` channels, ``depth`` 3x3 convolutions (depth >= 2).
+    Weights [9][Cout][Cin]: FP32 master copies, BF16 working copies, Adam moments."""
+
+    def __init__(self, depth=6, hidden=32, nin=4, nout=3, device=0, seed=0):
+        torch = _torch()
+        if depth < 2 or hidden not in (16, 32) or not (1 <= nin <= _CIN) or not (1 <= nout <= _COUT):
+            raise ValueError("depth >= 2, hidden 16 or 32, 1 <= nin <= 16, 1 <= nout <= 16")
+        self.dev = torch.device("cuda", device)
+        self.nin, self.nout = nin, nout
+        self.chans = [_CIN] + [hidden] * (depth - 1) + [_COUT]
+        rng = np.random.default_rng(seed)
+        self.w32, self.wb, self.wt, self.m, self.v, self.dw = [], [], [], [], [], []
+        for l in range(depth):
+            ci, co = self.chans[l], self.chans[l + 1]
+            fan = 9 * (nin if l == 0 else ci)
+            w = rng.standard_normal((9, co, ci)) * np.sqrt(2.0 / fan)
+            if l == 0:
+                w[:, :, nin:] = 0.0
+            if l == depth - 1:
+                w *= 0.1
+                w[:, nout:, :] = 0.0
+            w32 = torch.tensor(w, dtype=torch.float32, device=self.dev)
+            self.w32.append(w32)
+            self.wb.append(w32.to(torch.bfloat16))
+            self.wt.append(torch.empty((9, ci, co), dtype=torch.bfloat16, device=self.dev))
+            self.m.append(torch.zeros_like(w32))
+            self.v.append(torch.zeros_like(w32))
+            self.dw.append(torch.zeros_like(w32))
+        self.step = 0
+        self._shape = None
+        self._loss = torch.zeros(1, dtype=torch.float64, device=self.dev)
+        self._part = torch.zeros(1024, dtype=torch.float64, device=self.dev)
+
+    # ------------------------------------------------------------ buffers
+    def _buffers(self, n, h, w):
+        if self._shape == (n, h, w):
+            return
+        torch = _torch()
+        bf = torch.bfloat16
+        self.act = [None] + [torch.empty((n, h, w, c), dtype=bf, device=self.dev) for c in self.chans[1:]]
+        self.y32 = torch.empty((n, h, w, _COUT), dtype=torch.float32, device=self.dev)
+        self.dz = [torch.empty((n, h, w, c), dtype=bf, device=self.dev) for c in self.chans[1:]]
+        need = ctypes.c_longlong()
+        nmax = 0
+        for l in range(len(self.chans) - 1):
+            check(_lib.lib().eio_cnn_wgrad_scratch(n, h, w, self.chans[l], self.chans[l + 1], ctypes.byref(need)))
+            nmax = max(nmax, need.value)
+        self.scratch = torch.empty(nmax, dtype=torch.float32, device=self.dev)
+        self._shape = (n, h, w)
+
+    def _stream(self):
+        return ctypes.c_void_p(_torch().cuda.current_stream(self.dev).cuda_stream)
+
+    # ------------------------------------------------------------ passes
+    def forward(self, x):
+        """x: BF16 [N][H][W][16] (device) -> FP32 [N][H][W][16] (device; the
+        first ``nout`` channels are the output)."""
+        L = _lib.lib()
+        n, h, w, c = x.shape
+        if c != _CIN:
+            raise ValueError("input needs %d channels" % _CIN)
+        self._buffers(n, h, w)
+        st = self._stream()
+        self.act[0] = x
+        last = len(self.chans) - 2
+        for l in range(last + 1):
+            check(L.eio_cnn_conv3x3(n, h, w, self.chans[l], self.chans[l + 1], _p(self.act[l]), _p(self.wb[l]),
+                                    None, int(l < last), _p(self.act[l + 1]),
+                                    _p(self.y32) if l == last else None, st))
+        return self.y32
+
+    def backward(self, target):
+        """Weight gradients of 0.5 mean((y - target)^2) over the first nout
+        channels (target FP32 [N][H][W][nout], device) after ``forward``.
+        Returns the loss as a device scalar (FP64)."""
+        L = _lib.lib()
+        n, h, w = self._shape
+        st = self._stream()
+        depth = len(self.chans) - 1
+        check(L.eio_cnn_mse(n * h * w, _COUT, self.nout, _p(self.y32), _p(target), _p(self.dz[-1]),
+                            _p(self._part), _p(self._loss), st))
+        for l in range(depth - 1, -1, -1):
+            ci, co = self.chans[l], self.chans[l + 1]
+            check(L.eio_cnn_conv3x3_wgrad(n, h, w, ci, co, _p(self.act[l]), _p(self.dz[l]), _p(self.dw[l]),
+                                          _p(self.scratch), self.scratch.numel(), st))
+            if l > 0:
+                check(L.eio_cnn_flip(ci, co, _p(self.wb[l]), _p(self.wt[l]), st))
+                check(L.eio_cnn_conv3x3(n, h, w, co, ci, _p(self.dz[l]), _p(self.wt[l]), _p(self.act[l]), 0,
+                                        _p(self.dz[l - 1]), None, st))
+        return self._loss
+
+    def adam(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
+        L = _lib.lib()
+        st = self._stream()
+        self.step += 1
+        for l in range(len(self.w32)):
+            check(L.eio_cnn_adam(self.w32[l].numel(), _p(self.w32[l]), _p(self.m[l]), _p(self.v[l]),
+                                 _p(self.dw[l]), lr, b1, b2, eps, self.step, _p(self.wb[l]), st))
+
+    def weights(self):
+        """FP32 master weights as numpy arrays [9][Cout][Cin]."""
+        return [w.cpu().numpy() for w in self.w32]
+
+    def set_weights(self, ws):
+        torch = _torch()
+        for l, w in enumerate(ws):
+            self.w32[l].copy_(torch.as_tensor(np.asarray(w, np.float32)))
+            self.wb[l].copy_(self.w32[l].to(torch.bfloat16))
+
+
+def smooth_perturbation(shape, rng, sigma, interior=None):
+    """Unit-RMS smooth random field [nx][nz] (Gaussian-filtered white noise),
+    zero outside ``interior`` = (x0, x1, z0, z1) when given."""
+    from .synthetic import gaussian_smooth
+    f = gaussian_smooth(rng.standard_normal(shape), sigma)
+    if interior is not None:
+        x0, x1, z0, z1 = interior
+        mask = np.zeros(shape)
+        mask[x0:x1, z0:z1] = 1.0
+        f = gaussian_smooth(mask, 2.0) * f
+    return (f / np.sqrt(np.mean(f * f))).astype(np.float32)
+
+
+class LearnedPreconditioner:
+    """Learned approximate inverse of the Gauss-Newton Hessian at a background.
+
+    born: a BornElasticShotsGpu on the FWI's acquisition; m0: the background
+    (elastic parameters [3][nx][nz]) the pairs are generated at; interior:
+    (x0, x1, z0, z1) cells where perturbations live (default: inside the
+    absorbing pads).  ``__call__(m, g)`` returns the learned model update
+    (a descent candidate) for the gradient g, for ``fwi.lbfgs(precond=...)``."""
+
+    def __init__(self, born, m0, interior=None, net=None, sigma=3.0, rel_rms=0.02, seed=0):
+        self.born = born
+        self.m0 = np.ascontiguousarray(m0, dtype=np.float32)
+        self.scale = np.abs(self.m0.reshape(3, -1)).mean(axis=1).astype(np.float64)
+        self.scale[self.scale == 0] = 1.0
+        nx, nz = self.m0.shape[1:]
+        if interior is None:
+            fd = born.fd
+            interior = (fd.xPadMinus + fd.fat, nx - fd.xPadPlus - fd.fat, fd.zPadMinus + fd.fat,
+                        nz - fd.zPadPlus - fd.fat)
+        self.interior = interior
+        self.sigma, self.rel_rms = sigma, rel_rms
+        self.net = net if net is not None else ConvNet(seed=seed)
+        self.K = None
+        self.born.setBackground(self.m0)
+        self.illum = self._illumination()
+
+    # ------------------------------------------------------------ Born pairs
+    def _normal(self, dm):
+        """J^T J dm at the background (Born forward, then adjoint)."""
+        d = np.zeros(self.born.dataSpace().getNdArray().shape, np.float32)
+        self.born.forward(False, np.ascontiguousarray(dm, np.float32), d)
+        g = np.zeros_like(self.m0)
+        self.born.adjoint(False, g, d)
+        return g
+
+    def _illumination(self):
+        x0, x1, z0, z1 = self.interior
+        u = np.zeros_like(self.m0)
+        u[:, x0:x1, z0:z1] = (self.rel_rms * self.scale)[:, None, None]
+        h = self._normal(u) * self.scale[:, None, None]
+        e = np.sqrt((h.astype(np.float64) ** 2).sum(axis=0))
+        return (e / max(e.max(), 1e-30)).astype(np.float32)
+
+    def _rel_gradient(self, g):
+        return np.asarray(g, np.float64) * self.scale[:, None, None]
+
+    def features(self, g):
+        """(NHWC feature image [nx][nz][16] FP32, RMS used) of a gradient [3][nx][nz]."""
+        gr = self._rel_gradient(g)
+        s = float(np.sqrt(np.mean(gr * gr)))
+        s = s if s > 0 else 1.0
+        f = np.zeros(self.m0.shape[1:] + (_CIN,), np.float32)
+        f[..., :3] = np.moveaxis(gr / s, 0, -1)
+        f[..., 3] = self.illum
+        return f, s
+
+    def make_pairs(self, nsamples, seed=1):
+        """Features and targets of ``nsamples`` seeded perturbations: (X
+        [n][nx][nz][16], T [n][nx][nz][3], feature RMS [n], dm [n][3][nx][nz])."""
+        rng = np.random.default_rng(seed)
+        shape = self.m0.shape[1:]
+        X, S, D = [], [], []
+        for _ in range(nsamples):
+            rel = np.stack([smooth_perturbation(shape, rng, self.sigma, self.interior) for _ in range(3)])
+            dm = (rel * (self.rel_rms * self.scale)[:, None, None]).astype(np.float32)
+            f, s = self.features(self._normal(dm))
+            X.append(f)
+            S.append(s)
+            D.append(dm)
+        X, S, D = np.stack(X), np.array(S), np.stack(D)
+        rel = D.astype(np.float64) / self.scale[None, :, None, None]
+        if self.K is None:
+            self.K = float(np.median(S / np.sqrt(np.mean(rel * rel, axis=(1, 2, 3)))))
+        T = np.moveaxis(rel * (self.K / S)[:, None, None, None], 1, -1).astype(np.float32)
+        return X, T, S, D
+
+    # ------------------------------------------------------------ training
+    def train(self, X, T, epochs=40, batch=8, lr=2e-3, seed=0):
+        """Adam on mini-batches of (X, T) (numpy, as make_pairs gives them);
+        returns the mean loss of each epoch."""
+        torch = _torch()
+        dev = self.net.dev
+        Xd = torch.as_tensor(X, device=dev).to(torch.bfloat16)
+        Td = torch.as_tensor(np.ascontiguousarray(T), device=dev)
+        n = X.shape[0]
+        rng = np.random.default_rng(seed)
+        hist = []
+        for ep in range(epochs):
+            order = rng.permutation(n)
+            tot = torch.zeros((), dtype=torch.float64, device=dev)
+            nb = 0
+            for b0 in range(0, n - batch + 1, batch):
+                idx = torch.as_tensor(order[b0:b0 + batch], device=dev)
+                xb = Xd.index_select(0, idx).contiguous()
+                tb = Td.index_select(0, idx).contiguous()
+                self.net.forward(xb)
+                tot += self.net.backward(tb)[0]
+                self.net.adam(lr=lr * (0.5 * (1 + np.cos(np.pi * ep / epochs))))
+                nb += 1
+            hist.append(float(tot.item()) / max(nb, 1))
+        return hist
+
+    def predict(self, g):
+        """Learned estimate of dm with J^T J dm = g ([3][nx][nz])."""
+        torch = _torch()
+        f, s = self.features(g)
+        x = torch.as_tensor(f[None], device=self.net.dev).to(torch.bfloat16).contiguous()
+        y = self.net.forward(x)[0, ..., :3].double().cpu().numpy()
+        rel = np.moveaxis(y, -1, 0) * (s / self.K)
+        return (rel * self.scale[:, None, None]).astype(np.float32)
+
+    def __call__(self, m, g):
+        return -self.predict(g)

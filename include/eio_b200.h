@@ -353,6 +353,38 @@ int eio_nl_fwd_noalloc(const eio_fd_params *p, float *const medium[5], float *co
                        const int *const srcPos[4], const int nSrc[4], const int *const recPos[4], const int nRec[4],
                        void *stream);
 
+/* ---- Learned FWI preconditioner (no reference counterpart) ------------------
+ * Kernels of a small convolutional network that maps an FWI gradient to an
+ * approximate Gauss-Newton update, trained on (J^T J dm, dm) pairs from the
+ * Born operators.  All pointers are device pointers, 16-byte aligned; work is
+ * queued on `stream` (a cudaStream_t, NULL = the default stream) and nothing
+ * synchronises.  Activations are NHWC BF16 with 16 or 32 channels; weights
+ * [9][cout][cin] BF16, tap = 3 dy + dx; products on the tensor cores with FP32
+ * accumulation. */
+/* y = conv3x3(x, wt) (stride 1, zero padding 1, no bias), then ReLU when relu
+ * != 0, or, when mask != NULL, y *= (mask > 0) (mask: NHWC, cout channels: the
+ * ReLU derivative for the backward pass).  y: BF16 NHWC [n][h][w][cout];
+ * y32 (optional): the same values in FP32. */
+int eio_cnn_conv3x3(int n, int h, int w, int cin, int cout, const void *x, const void *wt, const void *mask,
+                    int relu, void *y, float *y32, void *stream);
+/* floats of scratch the weight gradient needs for this shape */
+int eio_cnn_wgrad_scratch(int n, int h, int w, int cin, int cout, long long *floats);
+/* dw[tap][co][ci] = sum_p dy[p][co] x[p + (dy-1, dx-1)][ci] (FP32, overwritten;
+ * fixed summation order) */
+int eio_cnn_conv3x3_wgrad(int n, int h, int w, int cin, int cout, const void *x, const void *dy, float *dw,
+                          float *scratch, long long scratchFloats, void *stream);
+/* wt[tap][ci][co] = w[8 - tap][co][ci]: the weights of the data gradient */
+int eio_cnn_flip(int cin, int cout, const void *w, void *wt, void *stream);
+/* loss = 0.5 sum_{p, c < nc} (y32 - target)^2 / (npix nc) into *loss (device
+ * double); dz (BF16 NHWC, c channels) = its derivative, 0 on channels >= nc.
+ * target: FP32 [npix][nc]; scratch: 1024 device doubles. */
+int eio_cnn_mse(long long npix, int c, int nc, const float *y32, const float *target, void *dz, double *scratch,
+                double *loss, void *stream);
+/* one Adam step (bias-corrected, step >= 1) on the FP32 parameters p with
+ * moments m, v and gradient g; pb (optional): BF16 copy of the result */
+int eio_cnn_adam(long long n, float *p, float *m, float *v, const float *g, float lr, float b1, float b2, float eps,
+                 int step, void *pb, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
