@@ -41,7 +41,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="born_600x1800", choices=["born_600x1800", "nl_312x520", "fwi_1000x3400"])
+    ap.add_argument("--workload", default="born_600x1800",
+                    choices=["born_600x1800", "nl_312x520", "fwi_1000x3400", "fwi_learned"])
+    ap.add_argument("--pairs", type=int, default=64, help="fwi_learned: Born training pairs")
+    ap.add_argument("--epochs", type=int, default=60, help="fwi_learned: training epochs")
     ap.add_argument("--shots", type=int, default=None,
                     help="shots per GPU (default: 10 for born_600x1800; a bounded sample of 16 of the 120 shots "
                          "for fwi_1000x3400)")
@@ -445,6 +448,10 @@ def run_reference(args, ws, rank, local):
         if not O.RefGpu.available("f"):
             return {"impl": "reference", "unavailable": "oracle/_ref not built (reference tree absent at build time)"}
         return run_reference_nl(args)
+    if args.workload == "fwi_learned":
+        return {"impl": "reference", "unavailable": "the reference has no learned preconditioner and no FWI driver "
+                "(its scripts call pySolver, which is not in the reference tree); the plain L-BFGS arm of this "
+                "workload is the method without the learned part"}
     if args.workload == "fwi_1000x3400":
         return {"impl": "reference", "unavailable": "the reference propagates every shot on the whole grid and its "
                 "Born drivers index the history with the 32-bit product its*nz*nx (kernelsGpuElastic.cu:1342), "
@@ -760,6 +767,140 @@ def run_ours_fwi(args, ws, rank, local):
             "cpu_baseline": None, "clocks": clk, "gpu_launches": int(launches)}
 
 
+class _CountedObjective:
+    """Counts the shot propagations an FWI objective runs (misfit: 1 per shot;
+    gradient: 2 fused, 3 unfused)."""
+
+    def __init__(self, obj, nshots):
+        self.obj, self.n, self.props = obj, nshots, 0
+
+    def value(self, m):
+        self.props += self.n
+        return self.obj.value(m)
+
+    def value_and_gradient(self, m):
+        self.props += (2 if self.obj.fused else 3) * self.n
+        return self.obj.value_and_gradient(m)
+
+
+class _Reached(Exception):
+    pass
+
+
+def run_ours_learned(args, ws, rank, local):
+    """Learned vs plain FWI: wall-clock to the misfit that plain L-BFGS reaches in
+    --steps iterations, plain against learned (Born training pairs + training +
+    L-BFGS with learned steps the exact misfit accepts or rejects), on a reduced
+    grid of the batched-FWI model (layered background, 4500 m/s inclusion,
+    smoothed start model).  Each GPU runs the same comparison (replicas)."""
+    import torch
+    from elastic_isotropic_operators_b200 import _lib, fwi, precond, prop, synthetic
+    nsh = args.shots or 8
+    w = synthetic.fwi_1000x3400(nz=136, nx=520, nts=1200, nshots=nsh, nrec=60, pad=20, window_km=(2.0, 4.0))
+    w.par.set("iGpu", str(local))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    src, rec = w.geometry()
+    sig = w.source_signal()
+    nl = prop.nonlinearFwiPropElasticShotsGpu(w.elastic, w.par, sig[None], *src, *rec)
+    born = prop.BornElasticShotsGpu(w.elastic, w.par, [sig], *src, *rec)
+    for op in (nl, born):
+        pin_kernel(op._L, op.ctx, args)
+    d_obs = nl.dataSpace()
+    nl.forward(False, w.extra["true_model"], d_obs)          # observed data, untimed
+    m0 = w.extra["start_model"]
+    obj = _CountedObjective(fwi.FwiObjective(nl, born, d_obs), nsh)
+    for _ in range(args.warmup):
+        obj.value_and_gradient(m0)
+    obj.props = 0
+    L = _lib.lib()
+    for op in (nl, born):
+        L.eio_ctx_stats(op.ctx, 1, 1, None, None, None)
+    cells = (w.nz - 8) * (w.nx - 8) * (w.nts - 1) * 2
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1) / 1e3
+
+    barrier(ws)
+    clocks = ClockSampler(None)
+    clocks.start()
+    (_, plain), t_plain = timed(lambda: fwi.lbfgs(obj, m0, niter=args.steps, scale=m0))
+    props_plain = obj.props
+    target = plain[-1]
+    obj.props = 0
+    P = None
+
+    def train():
+        nonlocal P
+        P = precond.LearnedPreconditioner(born, m0, seed=0)
+        X, T, _, _ = P.make_pairs(args.pairs, seed=1)
+        P.train(X, T, epochs=args.epochs, batch=8, lr=3e-3)
+
+    _, t_train = timed(train)
+    pair_props = (args.pairs + 1) * 4 * nsh                   # Born forward + adjoint (+ the illumination pair)
+    trace = []
+    t_start = [0.0]
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+
+    def cb(it, m, f, g):
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record()
+        torch.cuda.synchronize()
+        trace.append((it + 1, f, ev0.elapsed_time(ev) / 1e3))
+        if f <= target:
+            raise _Reached()
+
+    stats = {}
+    try:
+        fwi.lbfgs(obj, m0, niter=2 * args.steps, scale=m0, precond=P, stats=stats, callback=cb)
+    except _Reached:
+        pass
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = sum(read_stats(L, op.ctx)["launches"] for op in (nl, born))
+    reached = bool(trace) and trace[-1][1] <= target
+    t_iter = trace[-1][2] if trace else float("nan")
+    t_learned = t_train + t_iter
+    t_plain = max_over_ranks(ws, t_plain)
+    t_learned = max_over_ranks(ws, t_learned)
+    speedup = t_plain / t_learned if reached else 0.0
+    props_learned = obj.props + pair_props
+    gcells_plain = props_plain * cells / t_plain / 1e9
+    peak, pk = measured_peak()
+    return {"metric": "FWI wall-clock speed-up to the plain method's final misfit (learned vs plain)",
+            "value": round(speedup, 3), "unit": "x", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * t_plain / args.steps, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 propagation, bf16 network", "data": "synthetic",
+            "config": {"workload": "fwi_learned: 136x520 grid of the batched-FWI model (12.5 m, nts=1200, %d shots, "
+                                   "60 receivers each), plain L-BFGS for %d iterations vs learned steps "
+                                   "(%d Born pairs, %d epochs)" % (nsh, args.steps, args.pairs, args.epochs),
+                       "l2": "each gradient streams the FP32 source history of a shot (about 1.1 GB) through HBM"},
+            "plain": {"iterations": args.steps, "seconds": round(t_plain, 3), "final_misfit": target,
+                      "misfit_history": [float(v) for v in plain], "propagations": props_plain},
+            "learned": {"reached": reached, "iterations": trace[-1][0] if trace else 0,
+                        "seconds_total": round(t_learned, 3), "seconds_training": round(t_train, 3),
+                        "seconds_iterations": round(t_iter, 3),
+                        "misfit_history": [float(x[1]) for x in trace], "accepted": stats.get("learned", 0),
+                        "rejected": stats.get("rejected", 0), "propagations": props_learned},
+            "iterations_ratio": round(args.steps / trace[-1][0], 3) if reached else None,
+            "speedup_excluding_training": round(t_plain / t_iter, 3) if reached else None,
+            "e2e": {"value": round(speedup, 3), "unit": "x", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                    "note": "the FWI API with host buffers is the only path"},
+            "roofline": {"bound": "hbm", "achieved": round(BYTES_PER_CELL * gcells_plain, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(BYTES_PER_CELL * gcells_plain / peak, 4), "traffic": None,
+                         "peak_source": pk, "basis": "80 B per cell update of the plain run over its wall-clock",
+                         "kernel": kernel_name(L, born.ctx)},
+            "cpu_baseline": None, "clocks": clk, "gpu_launches": int(launches)}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -773,6 +914,8 @@ def main():
         out = run_ours_nl(args, ws, rank, local)
     elif args.workload == "fwi_1000x3400":
         out = run_ours_fwi(args, ws, rank, local)
+    elif args.workload == "fwi_learned":
+        out = run_ours_learned(args, ws, rank, local)
     else:
         out = run_ours(args, ws, rank, local)
     if rank == 0:

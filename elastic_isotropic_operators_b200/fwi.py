@@ -309,27 +309,41 @@ def lbfgs(objective, m0, niter=10, memory=5, minBound=None, maxBound=None, init_
     return (x * sc).astype(np.float32), hist
 
 
-def _learned_step(objective, precond, m, f, g, minBound, maxBound, c1, tries=3):
-    """Try the update proposed by precond(m, g) at full, half and quarter
-    length; the exact misfit decides: the first trial point that lowers it
-    (with the Armijo condition when the proposal is a descent direction) is
-    returned with its misfit, else None."""
-    d = np.asarray(precond(m, g), dtype=np.float64)
-    if not np.isfinite(d).all() or not d.any():
-        return None
-    descent = dot64(g, d) < 0
-    step = 1.0
-    for _ in range(tries):
-        mt = _project((m + step * d).astype(np.float32), minBound, maxBound)
-        ft = objective.value(mt)
-        if ft < f and (not descent or ft <= f + c1 * dot64(g, mt - m)):
-            return mt, ft
-        step *= 0.5
-    return None
+def _trial_value(objective, mt):
+    """Misfit at a trial point of a line search; +inf when the propagator's
+    stability or dispersion check refuses the model (the search backtracks)."""
+    from ._lib import EioError
+    try:
+        return objective.value(mt)
+    except EioError as e:
+        if e.code != -2:              # anything but a refused model is an error
+            raise
+        return np.inf
+
+
+def _two_loop(g, free, S, Y, rho, h0):
+    """L-BFGS direction -H g on the free variables: the two-loop recursion over
+    the stored pairs around the initial inverse Hessian h0 (a function)."""
+    q = np.where(free, g, 0).astype(np.float64)
+    alpha = []
+    for s, y, r in reversed(list(zip(S, Y, rho))):
+        a = r * dot64(s, q)
+        alpha.append(a)
+        q = q - a * y
+    q = np.asarray(h0(q), dtype=np.float64)
+    for (s, y, r), a in zip(zip(S, Y, rho), reversed(alpha)):
+        b = r * dot64(y, q)
+        q = q + (a - b) * s
+    return np.where(free, -q, 0)
+
+
+def _max_rel(d, m):
+    am = np.abs(m).astype(np.float64)
+    return float((np.abs(d) / np.where(am > 0, am, max(float(am.max()), 1e-30))).max())
 
 
 def _lbfgs(objective, m0, niter=10, memory=5, minBound=None, maxBound=None, init_step=None, c1=1e-4,
-           max_backtrack=8, callback=None, precond=None, stats=None):
+           max_backtrack=8, callback=None, precond=None, stats=None, max_rel=0.1, learned_c1=0.2):
     """Minimise ``objective`` (value_and_gradient(m), value(m)) from m0.
 
     Two-loop recursion over the last ``memory`` pairs on the variables that no
@@ -337,11 +351,15 @@ def _lbfgs(objective, m0, niter=10, memory=5, minBound=None, maxBound=None, init
     for the projected problem); the first step, and every step after a restart,
     is scaled so that no model value changes by more than ``init_step`` of
     itself (default 1 %); trial points are projected onto [minBound,
-    maxBound]; backtracking halves the step until the Armijo condition holds,
-    and a failed search restarts once from the projected steepest descent.
-    With ``precond``, each iteration first tries the proposed update
-    (_learned_step) and falls back to the L-BFGS step when the misfit rejects
-    it; accepted learned steps enter the L-BFGS memory like any other.
+    maxBound]; backtracking halves the step until the Armijo condition holds
+    (a model the propagator's checks refuse counts as a failed trial), and a
+    failed search restarts once from the projected steepest descent.
+    With ``precond`` (a learned approximate inverse Hessian, precond(m, g) ~
+    -H^-1 g), the recursion runs around it, scaled by the latest curvature
+    pair, instead of the scalar initial Hessian; the exact misfit judges the
+    step (sufficient decrease with learned_c1, two trials), and when it
+    rejects the learned direction, or that is no descent direction, the
+    iteration falls back to the plain L-BFGS step.
     Returns (m, history) with history the objective values (FP64)."""
     m = _project(np.array(m0, dtype=np.float32, copy=True), minBound, maxBound)
     f, g = objective.value_and_gradient(m)
@@ -352,60 +370,65 @@ def _lbfgs(objective, m0, niter=10, memory=5, minBound=None, maxBound=None, init
     if stats is not None:
         stats.setdefault("learned", 0)
         stats.setdefault("rejected", 0)
+    plain_only = False
     while it < niter:
-        if precond is not None:
-            trial = _learned_step(objective, precond, m, f, g, minBound, maxBound, c1)
-            if stats is not None:
-                stats["learned" if trial is not None else "rejected"] += 1
-            if trial is not None:
-                mt = trial[0]
-                ft, gt = objective.value_and_gradient(mt)
-                s = (mt - m).astype(np.float64)
-                y = (gt - g).astype(np.float64)
-                sy = dot64(s, y)
-                if sy > 1e-10 * np.sqrt(dot64(s, s) * dot64(y, y)):
-                    S.append(s); Y.append(y); rho.append(1.0 / sy)
-                    if len(S) > memory:
-                        S.pop(0); Y.pop(0); rho.pop(0)
-                m, f, g = mt, ft, gt
-                hist.append(f)
-                if callback is not None:
-                    callback(it, m, f, g)
-                it += 1
-                continue
         free = _free(m, g, minBound, maxBound)
-        q = np.where(free, g, 0).astype(np.float64)
-        alpha = []
-        for s, y, r in reversed(list(zip(S, Y, rho))):
-            a = r * dot64(s, q)
-            alpha.append(a)
-            q = q - a * y
-        if S:
-            q = q * (dot64(S[-1], Y[-1]) / dot64(Y[-1], Y[-1]))
-        for (s, y, r), a in zip(zip(S, Y, rho), reversed(alpha)):
-            b = r * dot64(y, q)
-            q = q + (a - b) * s
-        d = np.where(free, -q, 0)
-        if dot64(g, d) >= 0:  # not a descent direction: restart from steepest descent
-            S, Y, rho = [], [], []
-            d = np.where(free, -g, 0).astype(np.float64)
-        if not S:
-            # parameters of very different scales (kg/m3 and Pa): bound the
-            # largest relative change of any model value by init_step
-            frac = 0.01 if init_step is None else init_step
-            am = np.abs(m).astype(np.float64)
-            rel = np.abs(d) / np.where(am > 0, am, max(float(am.max()), 1e-30))
-            step = frac / max(float(rel.max()), 1e-300)
-        else:
-            step = 1.0
+        learned = False
+        d = None
+        if precond is not None and not plain_only:
+            # the learned operator as the initial inverse Hessian, scaled by the
+            # latest curvature pair (gamma = s.y / y.P y, P = -precond) once
+            # there is one; the search starts at the full step, capped at a
+            # max_rel relative change of any model value
+            def P(q):
+                return -np.asarray(precond(m, np.asarray(q, np.float32)), np.float64)
+            gamma = 1.0
+            if S:
+                yPy = dot64(Y[-1], P(Y[-1]))
+                if yPy > 0:
+                    gamma = dot64(S[-1], Y[-1]) / yPy
+            d = _two_loop(g, free, S, Y, rho, lambda q: gamma * P(q))
+            if np.isfinite(d).all() and d.any() and dot64(g, d) < 0:
+                learned = True
+                step = min(1.0, max_rel / max(_max_rel(d, m), 1e-300)) if not S else 1.0
+            else:
+                d = None
+                if stats is not None:
+                    stats["rejected"] += 1
+        plain_only = False
+        if d is None:
+            d = _two_loop(g, free, S, Y, rho,
+                          lambda q: q * (dot64(S[-1], Y[-1]) / dot64(Y[-1], Y[-1])) if S else q)
+            if dot64(g, d) >= 0:  # not a descent direction: restart from steepest descent
+                S, Y, rho = [], [], []
+                d = np.where(free, -g, 0).astype(np.float64)
+            if not S:
+                # parameters of very different scales (kg/m3 and Pa): bound the
+                # largest relative change of any model value by init_step
+                frac = 0.01 if init_step is None else init_step
+                step = frac / max(_max_rel(d, m), 1e-300)
+            else:
+                step = 1.0
         accepted = False
-        for _ in range(max_backtrack + 1):
+        # a learned step must deliver a fifth of the decrease its slope
+        # predicts (a Newton step on a quadratic delivers half), within two
+        # trials; a plain step the Armijo condition with c1
+        cl = learned_c1 if learned else c1
+        for _ in range(2 if learned else max_backtrack + 1):
             mt = _project((m + step * d).astype(np.float32), minBound, maxBound)
-            ft = objective.value(mt)
-            if ft <= f + c1 * dot64(g, mt - m) and ft < f:
+            ft = _trial_value(objective, mt)
+            if ft <= f + cl * dot64(g, mt - m) and ft < f:
                 accepted = True
                 break
             step *= 0.5
+        if not accepted and learned:
+            # the exact misfit rejected the learned direction: plain step instead
+            if stats is not None:
+                stats["rejected"] += 1
+            plain_only = True
+            continue
+        if learned and stats is not None:
+            stats["learned"] += 1
         if not accepted:
             if S and not restarted:
                 S, Y, rho = [], [], []
