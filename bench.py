@@ -42,8 +42,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="born_600x1800",
-                    choices=["born_600x1800", "nl_312x520", "fwi_1000x3400", "fwi_learned"])
+                    choices=["born_600x1800", "nl_312x520", "fwi_1000x3400", "fwi_learned", "cnn_train"])
     ap.add_argument("--pairs", type=int, default=64, help="fwi_learned: Born training pairs")
+    ap.add_argument("--conv-path", type=int, default=-1, choices=[-1, 0, 1],
+                    help="cnn_train: forward convolutions on mma.sync (0) or tcgen05 (1); "
+                         "-1 keeps the library default (mma.sync)")
     ap.add_argument("--epochs", type=int, default=60, help="fwi_learned: training epochs")
     ap.add_argument("--shots", type=int, default=None,
                     help="shots per GPU (default: 10 for born_600x1800; a bounded sample of 16 of the 120 shots "
@@ -448,7 +451,7 @@ def run_reference(args, ws, rank, local):
         if not O.RefGpu.available("f"):
             return {"impl": "reference", "unavailable": "oracle/_ref not built (reference tree absent at build time)"}
         return run_reference_nl(args)
-    if args.workload == "fwi_learned":
+    if args.workload in ("fwi_learned", "cnn_train"):
         return {"impl": "reference", "unavailable": "the reference has no learned preconditioner and no FWI driver "
                 "(its scripts call pySolver, which is not in the reference tree); the plain L-BFGS arm of this "
                 "workload is the method without the learned part"}
@@ -901,6 +904,85 @@ def run_ours_learned(args, ws, rank, local):
             "cpu_baseline": None, "clocks": clk, "gpu_launches": int(launches)}
 
 
+def cnn_step_flops(chans, npix):
+    """Tensor-core FLOPs of one training step of the preconditioner network:
+    forward convolutions of every layer, data gradients of all but the first,
+    weight gradients of every layer (2 * 9 * cin * cout per pixel each)."""
+    per = [2 * 9 * ci * co for ci, co in zip(chans[:-1], chans[1:])]
+    return float(npix) * (2 * sum(per) + sum(per[1:]))
+
+
+def run_ours_cnn(args, ws, rank, local):
+    """Training throughput of the learned preconditioner's network: per step,
+    forward, loss, data and weight gradients and the Adam update of a batch of
+    --shots 256 x 256 patches (4 features in 16 channels, 32 hidden, 6 layers)
+    through the library's kernels.  Inputs are resident on the device; each
+    step reads them fresh from a pool larger than L2."""
+    import ctypes
+    import torch
+    from elastic_isotropic_operators_b200 import _lib, precond
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if args.conv_path >= 0:
+        _lib.check(_lib.lib().eio_cnn_set_conv_path(args.conv_path))
+    path = ctypes.c_int()
+    _lib.check(_lib.lib().eio_cnn_get_conv_path(ctypes.byref(path)))
+    batch = args.shots or 16
+    h = w = 256
+    net = precond.ConvNet(depth=6, hidden=32, device=local, seed=0)
+    g = torch.Generator(device=dev)
+    g.manual_seed(1)
+    pool = 4                                                  # 4 batches: 4 x 64 MB of BF16 inputs
+    X = torch.zeros((pool * batch, h, w, 16), dtype=torch.bfloat16, device=dev)
+    X[..., :4] = torch.randn((pool * batch, h, w, 4), generator=g, device=dev).to(torch.bfloat16)
+    T = torch.randn((pool * batch, h, w, 3), generator=g, device=dev)
+    for i in range(args.warmup):
+        k = i % pool
+        net.forward(X[k * batch:(k + 1) * batch])
+        net.backward(T[k * batch:(k + 1) * batch])
+        net.adam()
+    torch.cuda.synchronize()
+    barrier(ws)
+    clocks = ClockSampler(None)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(args.steps):
+        k = i % pool
+        net.forward(X[k * batch:(k + 1) * batch])
+        loss = net.backward(T[k * batch:(k + 1) * batch])
+        net.adam()
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t_ms = max_over_ranks(ws, e0.elapsed_time(e1))
+    depth = len(net.chans) - 1
+    launches_per_step = depth + 2 * depth + 2 * (depth - 1) + 2 + depth   # conv, wgrad+sum, flip+conv, mse+sum, adam
+    flops = cnn_step_flops(net.chans, batch * h * w)
+    tflops = flops * args.steps / (t_ms * 1e-3) / 1e12
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak, pk = float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        peak, pk = 1590.0, "fallback"
+    samples = ws * batch * args.steps / (t_ms * 1e-3)
+    return {"metric": "preconditioner training throughput", "value": round(samples, 2), "unit": "patches/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_ms / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (FP32 accumulate)",
+            "data": "synthetic", "loss": float(loss.item()),
+            "config": {"workload": "cnn_train: %d patches of 256x256 per step, 6 conv layers 16-32-32-32-32-32-16"
+                                   % batch, "l2": "inputs read from a pool of 4 batches (256 MB) larger than L2"},
+            "e2e": {"value": round(samples, 2), "unit": "patches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                    "note": "training consumes device-resident pairs that the Born operators produce"},
+            "roofline": {"bound": "tensor", "achieved": round(tflops, 2), "peak": peak, "unit": "TFLOP/s",
+                         "frac": round(tflops / peak, 4), "traffic": None, "peak_source": pk,
+                         "basis": "tensor-core FLOPs of a training step (forward, data and weight gradients) over "
+                                  "the timed region",
+                         "kernel": ("k_conv3_tc (tcgen05, TMEM accumulator)" if path.value == 1 else
+                                    "k_conv3 (mma.sync m16n8k16)") + " + k_conv3_wgrad (mma.sync m16n8k16)"},
+            "cpu_baseline": None, "clocks": clk, "gpu_launches": int(launches_per_step * args.steps)}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -916,6 +998,8 @@ def main():
         out = run_ours_fwi(args, ws, rank, local)
     elif args.workload == "fwi_learned":
         out = run_ours_learned(args, ws, rank, local)
+    elif args.workload == "cnn_train":
+        out = run_ours_cnn(args, ws, rank, local)
     else:
         out = run_ours(args, ws, rank, local)
     if rank == 0:

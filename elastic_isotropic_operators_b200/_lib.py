@@ -86,6 +86,9 @@ _SIGS = {
     "eio_fwi_gradient": (I, [P, I, I, FP, FP, I, IP, P, P, I, P, FP, ctypes.POINTER(ctypes.c_double)]),
     "eio_reduce64": (I, [I, I, I, P, P, ctypes.c_longlong, I, ctypes.POINTER(ctypes.c_double)]),
     "eio_cnn_conv3x3": (I, [I, I, I, I, I, P, P, P, I, P, P, P]),
+    "eio_cnn_set_conv_path": (I, [I]),
+    "eio_cnn_get_conv_path": (I, [IP]),
+    "eio_cnn_status": (I, [I, IP]),
     "eio_cnn_wgrad_scratch": (I, [I, I, I, I, I, ctypes.POINTER(ctypes.c_longlong)]),
     "eio_cnn_conv3x3_wgrad": (I, [I, I, I, I, I, P, P, P, P, ctypes.c_longlong, P]),
     "eio_cnn_flip": (I, [I, I, P, P, P]),

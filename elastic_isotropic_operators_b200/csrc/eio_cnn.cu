@@ -24,8 +24,9 @@
 //   M = Cout, N = Cin, K = pixels; one warp per tap, both operands fetched
 //   with ldmatrix.trans from the staged tiles.  A persistent grid keeps its
 //   partial sums in registers over all its tiles and writes them once; the
-//   partials are then summed block by block in a fixed order, so the weight
-//   gradient does not change from run to run.
+//   partials are then summed in a fixed order (16 chunks of consecutive
+//   blocks in parallel, then the chunks), so the weight gradient does not
+//   change from run to run.
 // * k_mse: loss 0.5 sum (y - t)^2 / count over the first nc channels, its
 //   derivative in BF16; k_adam: Adam step on the FP32 master weights with the
 //   BF16 copy written alongside.
@@ -173,6 +174,279 @@ __global__ void __launch_bounds__(FWD_THREADS) k_conv3(const bf16* __restrict__ 
         }
 }
 
+// ---------------------------------------------------------------- tcgen05 path
+// The same convolution on the 5th-generation tensor cores.  A CTA (4 warps)
+// walks down a strip of TC_STRIP image rows, 128 output pixels wide; a
+// persistent grid loops over the strips.  Input rows (with a one-pixel halo)
+// sit in a ring of four shared-memory slots as [8-channel chunk][130
+// pixels][8 BF16], which is the K-major, non-swizzled operand layout of
+// tcgen05.mma: the A operand of tap (dy, dx) and 16 channels is a descriptor
+// onto slot (y - 1 + dy) shifted by dx pixels (8 pixels x 16 B core matrices,
+// the next 8 pixels 128 B on, the next 8 channels one chunk = 2080 B on), so
+// no im2col copy is made and each input row is loaded once per strip.  The
+// weights sit as [tap][chunk][Cout][8 BF16] (B operand, K-major).  One thread
+// issues the 9 * Cin / 16 MMAs (M = 128, N = Cout, K = 16) of a row into one of
+// two 32-column TMEM accumulators and commits them to that accumulator's
+// mbarrier.  Software pipeline per row y: wait for input row y + 2 (cp.async),
+// barrier, issue the MMAs of row y + 1, wait (bounded) for those of row y,
+// start the copies of row y + 3 into the slot those MMAs have released,
+// epilogue of row y (each warp reads its 32 lanes = pixels with tcgen05.ld):
+// the copies and the tensor cores run under the epilogue.
+// Operand and descriptor layout follow the PTX ISA's tcgen05 matrix
+// descriptor (start, leading and stride byte offsets >> 4, version 1 at bit
+// 46, no swizzle) and instruction descriptor (F32 accumulator, BF16 A and B,
+// both K-major, N >> 3 at bit 17, M >> 4 at bit 24).
+constexpr int TC_PIX = 128;                 // output pixels of a row tile
+constexpr int TC_HP = TC_PIX + 2;           // staged pixels of a row (halo)
+constexpr int TC_THREADS = 128;
+constexpr int TC_STRIP = 16;                // rows of a strip
+constexpr int TC_SLOTS = 4;                 // input-row ring
+constexpr long long TC_WAIT_LIMIT = 1LL << 22;
+constexpr int TC_TMEM_COLS = 64;            // two 32-column accumulators
+
+__device__ int g_cnn_err;                   // set when an mbarrier wait gives up
+
+template <int CIN, int COUT>
+struct TcLayout {
+    static constexpr int ROW_BYTES = (CIN / 8) * TC_HP * 16;
+    static constexpr int A_BYTES = TC_SLOTS * ROW_BYTES;
+    static constexpr int B_OFF = (A_BYTES + 127) / 128 * 128;
+    static constexpr int B_BYTES = 9 * (CIN / 8) * COUT * 16;
+    static constexpr int BAR_OFF = B_OFF + B_BYTES;   // 2 mbarriers, then the TMEM address
+    static constexpr int SMEM = BAR_OFF + 32;
+};
+
+__device__ __forceinline__ unsigned cnn_smem_u32(const void* p)
+{
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long umma_desc(unsigned addr, unsigned lbo, unsigned sbo)
+{
+    return (unsigned long long)((addr >> 4) & 0x3FFF) | ((unsigned long long)((lbo >> 4) & 0x3FFF) << 16) |
+           ((unsigned long long)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+template <int COUT>
+__device__ __forceinline__ constexpr unsigned umma_idesc()
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(COUT >> 3) << 17) | ((unsigned)(TC_PIX >> 4) << 24);
+}
+
+template <int N>
+__device__ __forceinline__ void tmem_ld(unsigned taddr, float* v);
+
+template <>
+__device__ __forceinline__ void tmem_ld<16>(unsigned taddr, float* v)
+{
+    unsigned r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+template <>
+__device__ __forceinline__ void tmem_ld<32>(unsigned taddr, float* v)
+{
+    tmem_ld<16>(taddr, v);
+    tmem_ld<16>(taddr + 16, v + 16);
+}
+
+// input row gy of image n, pixels x0-1 .. x0+128, into ring slot `slot` by
+// 16-byte cp.async copies (zero-filled outside the image); the caller waits
+template <int CIN>
+__device__ __forceinline__ void tc_stage_row(const bf16* __restrict__ x, int H, int W, int n, int gy, int x0,
+                                             unsigned char* slot)
+{
+    constexpr int KC = CIN / 8;
+    const bool row_in = gy >= 0 && gy < H;
+    for (int i = threadIdx.x; i < KC * TC_HP; i += TC_THREADS) {
+        const int kc = i % KC, c = i / KC;
+        const int gx = x0 - 1 + c;
+        const bool in = row_in && gx >= 0 && gx < W;
+        const bf16* src = in ? x + (((size_t)n * H + gy) * W + gx) * CIN + kc * 8 : x;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                         cnn_smem_u32(slot + ((size_t)kc * TC_HP + c) * 16)),
+                     "l"(src), "r"(in ? 16 : 0)
+                     : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_rows_landed()
+{
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic writes -> tensor-core reads
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+}
+
+// the MMAs of output row y (ring slots of rows y-1 .. y+1) into accumulator buf, committed to bar
+template <int CIN, int COUT>
+__device__ __forceinline__ void tc_issue_row(unsigned a0, unsigned b0, int y, unsigned tmem_buf, unsigned bar)
+{
+    using Ly = TcLayout<CIN, COUT>;
+    constexpr int KC = CIN / 8;
+    constexpr unsigned idesc = umma_idesc<COUT>();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll 1
+    for (int tap = 0; tap < 9; tap++) {
+        const int dy = tap / 3, dx = tap - 3 * dy;
+        const unsigned slot = a0 + (unsigned)(((y + 3 + dy) & (TC_SLOTS - 1)) * Ly::ROW_BYTES);
+#pragma unroll
+        for (int kk = 0; kk < CIN / 16; kk++) {
+            const unsigned long long ad = umma_desc(slot + (2 * kk * TC_HP + dx) * 16, TC_HP * 16, 128);
+            const unsigned long long bd = umma_desc(b0 + ((tap * KC + 2 * kk) * COUT) * 16, COUT * 16, 128);
+            const unsigned acc = (tap | kk) ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                :
+                : "r"(tmem_buf), "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                : "memory");
+        }
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+template <int CIN, int COUT, int EPI>
+__global__ void __launch_bounds__(TC_THREADS) k_conv3_tc(const bf16* __restrict__ x, const bf16* __restrict__ w,
+                                                        const bf16* __restrict__ mask, int relu, int N, int H,
+                                                        int W, bf16* __restrict__ y, float* __restrict__ y32)
+{
+    using Ly = TcLayout<CIN, COUT>;
+    constexpr int KC = CIN / 8;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char* sA = smem;
+    unsigned char* sB = smem + Ly::B_OFF;
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem + Ly::BAR_OFF);
+    unsigned* tslot = reinterpret_cast<unsigned*>(smem + Ly::BAR_OFF + 16);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    for (int i = tid; i < 9 * COUT * KC; i += TC_THREADS) {   // weights -> [tap][chunk][co][8]
+        const int kc = i % KC, row = i / KC;                   // row = tap * COUT + co
+        const int tap = row / COUT, co = row - tap * COUT;
+        *reinterpret_cast<uint4*>(sB + (((size_t)tap * KC + kc) * COUT + co) * 16) =
+            *reinterpret_cast<const uint4*>(w + (size_t)row * CIN + kc * 8);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(cnn_smem_u32(bar)), "r"(1) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(cnn_smem_u32(bar + 1)), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(cnn_smem_u32(tslot)),
+                     "r"(TC_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const unsigned tmem = *tslot;
+    const unsigned a0 = cnn_smem_u32(sA), b0 = cnn_smem_u32(sB);
+    const unsigned bar0 = cnn_smem_u32(bar);
+
+    const int tilesX = (W + TC_PIX - 1) / TC_PIX, strips = (H + TC_STRIP - 1) / TC_STRIP;
+    const long long units = (long long)N * strips * tilesX;
+    unsigned phase[2] = {0u, 0u};
+    unsigned k = 0;                          // rows done by this CTA: accumulator k & 1
+    bool bad = false;
+    for (long long u = blockIdx.x; u < units && !bad; u += gridDim.x) {
+        const int xt = (int)(u % tilesX);
+        const long long r = u / tilesX;
+        const int sy = (int)(r % strips), n = (int)(r / strips);
+        const int x0 = xt * TC_PIX, yb = sy * TC_STRIP, ye = min(H, yb + TC_STRIP);
+        // prologue: rows yb-1 .. yb+1, the MMAs of row yb, then row yb+2 in flight
+        for (int gy = yb - 1; gy <= yb + 1; gy++)
+            tc_stage_row<CIN>(x, H, W, n, gy, x0, sA + ((gy + 4) & (TC_SLOTS - 1)) * Ly::ROW_BYTES);
+        tc_rows_landed();
+        if (tid == 0) tc_issue_row<CIN, COUT>(a0, b0, yb, tmem + (k & 1) * 32, bar0 + (k & 1) * 8);
+        if (yb + 1 < ye) tc_stage_row<CIN>(x, H, W, n, yb + 2, x0, sA + ((yb + 2) & (TC_SLOTS - 1)) * Ly::ROW_BYTES);
+        for (int yy = yb; yy < ye; yy++, k++) {
+            // row yy+2 has landed (and the epilogue of row yy-1 is done): MMAs of row yy+1
+            tc_rows_landed();
+            if (yy + 1 < ye && tid == 0)
+                tc_issue_row<CIN, COUT>(a0, b0, yy + 1, tmem + ((k + 1) & 1) * 32, bar0 + ((k + 1) & 1) * 8);
+            // bounded wait for the accumulator of row yy
+            const unsigned b = k & 1;
+            bool ok = false;
+            for (long long it = 0; it < TC_WAIT_LIMIT && !ok; it++) {
+                unsigned done;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                    "selp.u32 %0, 1, 0, p;\n\t}"
+                    : "=r"(done)
+                    : "r"(bar0 + b * 8), "r"(phase[b])
+                    : "memory");
+                ok = done != 0;
+            }
+            if (__syncthreads_or(!ok)) {
+                if (tid == 0) atomicExch(&g_cnn_err, 1);
+                bad = true;
+                break;
+            }
+            phase[b] ^= 1u;
+            // the MMAs of row yy have read slot (yy-1): row yy+3 goes there, under the epilogue
+            if (yy + 2 < ye)
+                tc_stage_row<CIN>(x, H, W, n, yy + 3, x0, sA + ((yy + 3) & (TC_SLOTS - 1)) * Ly::ROW_BYTES);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            float v[COUT];
+            tmem_ld<COUT>(tmem + b * 32 + ((unsigned)(warp * 32) << 16), v);
+            const int gx = x0 + warp * 32 + lane;
+            if (gx < W) {
+                const size_t pix = ((size_t)n * H + yy) * W + gx;
+                if constexpr (EPI == 0) {
+                    if (relu) {
+#pragma unroll
+                        for (int c = 0; c < COUT; c++) v[c] = fmaxf(v[c], 0.f);
+                    }
+                } else {
+#pragma unroll
+                    for (int c8 = 0; c8 < COUT / 8; c8++) {
+                        const uint4 mk = *reinterpret_cast<const uint4*>(mask + pix * COUT + c8 * 8);
+                        const __nv_bfloat162* m2 = reinterpret_cast<const __nv_bfloat162*>(&mk);
+#pragma unroll
+                        for (int q = 0; q < 4; q++) {
+                            if (!(__bfloat162float(m2[q].x) > 0.f)) v[c8 * 8 + 2 * q] = 0.f;
+                            if (!(__bfloat162float(m2[q].y) > 0.f)) v[c8 * 8 + 2 * q + 1] = 0.f;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int c8 = 0; c8 < COUT / 8; c8++) {
+                    uint4 o;
+                    __nv_bfloat162* o2 = reinterpret_cast<__nv_bfloat162*>(&o);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) o2[q] = __floats2bfloat162_rn(v[c8 * 8 + 2 * q], v[c8 * 8 + 2 * q + 1]);
+                    *reinterpret_cast<uint4*>(y + pix * COUT + c8 * 8) = o;
+                }
+                if (y32) {
+#pragma unroll
+                    for (int c4 = 0; c4 < COUT / 4; c4++)
+                        *reinterpret_cast<float4*>(y32 + pix * COUT + c4 * 4) =
+                            make_float4(v[4 * c4], v[4 * c4 + 1], v[4 * c4 + 2], v[4 * c4 + 3]);
+                }
+            }
+        }
+        // the next strip's prologue overwrites the ring: its barrier orders the
+        // last epilogue's TMEM reads before the next MMAs
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS)
+                     : "memory");
+}
+
 // partial weight gradients of the tiles tile = blockIdx.x, + gridDim.x, ...
 // into part[blockIdx.x][9][COUT][CIN]
 template <int CIN, int COUT>
@@ -238,13 +512,26 @@ __global__ void __launch_bounds__(WG_THREADS) k_conv3_wgrad(const bf16* __restri
         }
 }
 
-// out[j] = sum over blocks b (in order) of part[b][j]
-__global__ void k_sum_partials(const float* __restrict__ part, int nblk, int len, float* __restrict__ out)
+constexpr int SUM_CHUNKS = 16;   // the block partials are summed in 16 chunks, then the chunks in order
+
+// mid[c][j] = sum over the blocks b of chunk c (in order) of part[b][j]
+__global__ void k_sum_partials(const float* __restrict__ part, int nblk, int len, float* __restrict__ mid)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.y;
+    if (j >= len) return;
+    const int b0 = (int)((long long)nblk * c / SUM_CHUNKS), b1 = (int)((long long)nblk * (c + 1) / SUM_CHUNKS);
+    float s = 0.f;
+    for (int b = b0; b < b1; b++) s += part[(size_t)b * len + j];
+    mid[(size_t)c * len + j] = s;
+}
+
+__global__ void k_sum_chunks(const float* __restrict__ mid, int len, float* __restrict__ out)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= len) return;
     float s = 0.f;
-    for (int b = 0; b < nblk; b++) s += part[(size_t)b * len + j];
+    for (int c = 0; c < SUM_CHUNKS; c++) s += mid[(size_t)c * len + j];
     out[j] = s;
 }
 
@@ -290,13 +577,14 @@ __global__ void __launch_bounds__(MSE_THREADS) k_mse(const float* __restrict__ y
     }
 }
 
+// one warp: lane l sums part[l], part[l + 32], ... in order, then a fixed shuffle tree
 __global__ void k_sum_double(const double* __restrict__ part, int m, double scale, double* __restrict__ out)
 {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        double s = 0.0;
-        for (int i = 0; i < m; i++) s += part[i];
-        *out = s * scale;
-    }
+    double s = 0.0;
+    for (int i = threadIdx.x; i < m; i += 32) s += part[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) *out = s * scale;
 }
 
 __global__ void k_adam(float* __restrict__ p, float* __restrict__ m, float* __restrict__ v,
@@ -355,6 +643,27 @@ void launch_conv(int n, int h, int w, const bf16* x, const bf16* wt, const bf16*
     CCUDA(cudaGetLastError());
 }
 
+template <int CIN, int COUT, int EPI>
+void launch_conv_tc(int n, int h, int w, const bf16* x, const bf16* wt, const bf16* mask, int relu, bf16* y,
+                    float* y32, cudaStream_t st)
+{
+    constexpr int sm = TcLayout<CIN, COUT>::SMEM;
+    static int grid_cap = 0;
+    if (!grid_cap) {
+        CCUDA(cudaFuncSetAttribute(k_conv3_tc<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        int dev = 0, nsm = 0, per = 0;
+        CCUDA(cudaGetDevice(&dev));
+        CCUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        CCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_conv3_tc<CIN, COUT, EPI>, TC_THREADS, sm));
+        // each resident CTA holds TC_TMEM_COLS TMEM columns of the SM's 512
+        grid_cap = nsm * std::max(1, std::min(per, 512 / TC_TMEM_COLS));
+    }
+    const long long tiles = (long long)n * ((h + TC_STRIP - 1) / TC_STRIP) * ((w + TC_PIX - 1) / TC_PIX);
+    const int grid = (int)std::min<long long>(tiles, grid_cap);
+    k_conv3_tc<CIN, COUT, EPI><<<grid, TC_THREADS, sm, st>>>(x, wt, mask, relu, n, h, w, y, y32);
+    CCUDA(cudaGetLastError());
+}
+
 template <int CIN, int COUT>
 int wgrad_blocks(int n, int h, int w)
 {
@@ -374,6 +683,29 @@ int wgrad_blocks(int n, int h, int w)
 
 }  // namespace
 
+namespace {
+int g_conv_path = 0;   // 0: mma.sync kernel (measured faster on these channel counts), 1: tcgen05 kernel
+}
+
+void cnn_set_conv_path(int path)
+{
+    if (path != 0 && path != 1) throw Error(EIO_ERR_ARG, "convolution path must be 0 (mma.sync) or 1 (tcgen05)");
+    g_conv_path = path;
+}
+
+int cnn_get_conv_path() { return g_conv_path; }
+
+int cnn_status(int reset)
+{
+    int e = 0;
+    CCUDA(cudaMemcpyFromSymbol(&e, g_cnn_err, sizeof(int)));
+    if (reset) {
+        const int z = 0;
+        CCUDA(cudaMemcpyToSymbol(g_cnn_err, &z, sizeof(int)));
+    }
+    return e;
+}
+
 void cnn_conv3x3(int n, int h, int w, int cin, int cout, const void* x, const void* wt, const void* mask, int relu,
                  void* y, float* y32, void* stream)
 {
@@ -389,11 +721,16 @@ void cnn_conv3x3(int n, int h, int w, int cin, int cout, const void* x, const vo
     auto Wt = static_cast<const bf16*>(wt);
     auto M = static_cast<const bf16*>(mask);
     auto Y = static_cast<bf16*>(y);
-#define CONV_CASE(CI, CO)                                                            \
-    if (cin == CI && cout == CO) {                                                   \
-        if (M) launch_conv<CI, CO, 1>(n, h, w, X, Wt, M, 0, Y, y32, st);             \
-        else launch_conv<CI, CO, 0>(n, h, w, X, Wt, nullptr, relu, Y, y32, st);      \
-        return;                                                                      \
+#define CONV_CASE(CI, CO)                                                                 \
+    if (cin == CI && cout == CO) {                                                        \
+        if (g_conv_path == 1) {                                                           \
+            if (M) launch_conv_tc<CI, CO, 1>(n, h, w, X, Wt, M, 0, Y, y32, st);           \
+            else launch_conv_tc<CI, CO, 0>(n, h, w, X, Wt, nullptr, relu, Y, y32, st);    \
+        } else {                                                                          \
+            if (M) launch_conv<CI, CO, 1>(n, h, w, X, Wt, M, 0, Y, y32, st);              \
+            else launch_conv<CI, CO, 0>(n, h, w, X, Wt, nullptr, relu, Y, y32, st);       \
+        }                                                                                 \
+        return;                                                                           \
     }
     CONV_CASE(16, 16)
     CONV_CASE(16, 32)
@@ -411,7 +748,7 @@ long long cnn_wgrad_scratch(int n, int h, int w, int cin, int cout)
     if (cin == 16 && cout == 32) nb = wgrad_blocks<16, 32>(n, h, w);
     if (cin == 32 && cout == 16) nb = wgrad_blocks<32, 16>(n, h, w);
     if (cin == 32 && cout == 32) nb = wgrad_blocks<32, 32>(n, h, w);
-    return (long long)nb * 9 * cin * cout;
+    return ((long long)nb + SUM_CHUNKS) * 9 * cin * cout;   // block partials, then the chunk sums
 }
 
 void cnn_conv3x3_wgrad(int n, int h, int w, int cin, int cout, const void* x, const void* dy, float* dw,
@@ -427,7 +764,7 @@ void cnn_conv3x3_wgrad(int n, int h, int w, int cin, int cout, const void* x, co
     if (scratchFloats < need)
         throw Error(EIO_ERR_ARG, "weight-gradient scratch holds " + std::to_string(scratchFloats) + " floats, needs " +
                                      std::to_string(need));
-    const int nb = (int)(need / (9LL * cin * cout));
+    const int nb = (int)(need / (9LL * cin * cout)) - SUM_CHUNKS;
     auto st = static_cast<cudaStream_t>(stream);
     auto X = static_cast<const bf16*>(x);
     auto D = static_cast<const bf16*>(dy);
@@ -441,7 +778,10 @@ void cnn_conv3x3_wgrad(int n, int h, int w, int cin, int cout, const void* x, co
 #undef WG_CASE
     CCUDA(cudaGetLastError());
     const int len = 9 * cin * cout;
-    k_sum_partials<<<(len + 255) / 256, 256, 0, st>>>(scratch, nb, len, dw);
+    float* mid = scratch + (size_t)nb * len;
+    k_sum_partials<<<dim3((len + 255) / 256, SUM_CHUNKS), 256, 0, st>>>(scratch, nb, len, mid);
+    CCUDA(cudaGetLastError());
+    k_sum_chunks<<<(len + 255) / 256, 256, 0, st>>>(mid, len, dw);
     CCUDA(cudaGetLastError());
 }
 

@@ -1411,6 +1411,21 @@ EIO_API int eio_cnn_conv3x3(int n, int h, int w, int cin, int cout, const void* 
                             int relu, void* y, float* y32, void* stream) {
     return guarded([&] { cnn_conv3x3(n, h, w, cin, cout, x, wt, mask, relu, y, y32, stream); });
 }
+EIO_API int eio_cnn_set_conv_path(int path) {
+    return guarded([&] { cnn_set_conv_path(path); });
+}
+EIO_API int eio_cnn_get_conv_path(int* path) {
+    return guarded([&] {
+        if (!path) throw Error(EIO_ERR_ARG, "null result");
+        *path = cnn_get_conv_path();
+    });
+}
+EIO_API int eio_cnn_status(int reset, int* err) {
+    return guarded([&] {
+        if (!err) throw Error(EIO_ERR_ARG, "null result");
+        *err = cnn_status(reset);
+    });
+}
 EIO_API int eio_cnn_wgrad_scratch(int n, int h, int w, int cin, int cout, long long* floats) {
     return guarded([&] {
         if (!floats) throw Error(EIO_ERR_ARG, "null result");

@@ -88,6 +88,9 @@ constexpr int CNN_MSE_PARTIALS = 1024;
 void cnn_conv3x3(int n, int h, int w, int cin, int cout, const void* x, const void* wt, const void* mask, int relu,
                  void* y, float* y32, void* stream);
 long long cnn_wgrad_scratch(int n, int h, int w, int cin, int cout);
+void cnn_set_conv_path(int path);
+int cnn_get_conv_path();
+int cnn_status(int reset);
 void cnn_conv3x3_wgrad(int n, int h, int w, int cin, int cout, const void* x, const void* dy, float* dw,
                        float* scratch, long long scratchFloats, void* stream);
 void cnn_flip(int cin, int cout, const void* w, void* wt, void* stream);

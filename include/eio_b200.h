@@ -367,6 +367,15 @@ int eio_nl_fwd_noalloc(const eio_fd_params *p, float *const medium[5], float *co
  * y32 (optional): the same values in FP32. */
 int eio_cnn_conv3x3(int n, int h, int w, int cin, int cout, const void *x, const void *wt, const void *mask,
                     int relu, void *y, float *y32, void *stream);
+/* forward-convolution kernel of eio_cnn_conv3x3 (process-wide): 0 = mma.sync
+ * (m16n8k16; default, faster at 16-32 channels), 1 = tcgen05 (M = 128 pixels,
+ * TMEM accumulator, strips of rows through a cp.async ring) */
+int eio_cnn_set_conv_path(int path);
+int eio_cnn_get_conv_path(int *path);
+/* *err = 1 when a tcgen05 kernel gave up waiting for its accumulator (the
+ * output of that call is incomplete); reset != 0 clears the flag.  Synchronises
+ * the device. */
+int eio_cnn_status(int reset, int *err);
 /* floats of scratch the weight gradient needs for this shape */
 int eio_cnn_wgrad_scratch(int n, int h, int w, int cin, int cout, long long *floats);
 /* dw[tap][co][ci] = sum_p dy[p][co] x[p + (dy-1, dx-1)][ci] (FP32, overwritten;

@@ -38,9 +38,27 @@ def _np(t):
     return t.float().cpu().numpy()
 
 
+@pytest.fixture
+def conv_path():
+    """Runs a test with the given forward-convolution kernel, then restores the default."""
+    L = _lib.lib()
+    old = ctypes.c_int()
+    _lib.check(L.eio_cnn_get_conv_path(ctypes.byref(old)))
+    yield lambda p: _lib.check(L.eio_cnn_set_conv_path(p))
+    _lib.check(L.eio_cnn_set_conv_path(old.value))
+
+
+def _status():
+    err = ctypes.c_int()
+    _lib.check(_lib.lib().eio_cnn_status(1, ctypes.byref(err)))
+    return err.value
+
+
+@pytest.mark.parametrize("path", [0, 1])
 @pytest.mark.parametrize("cin,cout", [(16, 16), (16, 32), (32, 16), (32, 32)])
-@pytest.mark.parametrize("shape", [(2, 37, 45), (1, 8, 32), (3, 5, 70)])
-def test_conv_forward_relu_and_mask(cin, cout, shape):
+@pytest.mark.parametrize("shape", [(2, 37, 45), (1, 8, 32), (3, 5, 70), (1, 3, 300)])
+def test_conv_forward_relu_and_mask(cin, cout, shape, path, conv_path):
+    conv_path(path)
     n, h, w = shape
     rng = np.random.default_rng(cin * 100 + cout + h)
     L = _lib.lib()
@@ -61,6 +79,7 @@ def test_conv_forward_relu_and_mask(cin, cout, shape):
     torch.cuda.synchronize()
     r = ref * (mk > 0)
     assert _rel(_np(y32), r) < 2e-5
+    assert _status() == 0
 
 
 @pytest.mark.parametrize("cin,cout", [(16, 16), (16, 32), (32, 16), (32, 32)])
