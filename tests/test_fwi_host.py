@@ -83,3 +83,36 @@ def test_lbfgs_converges_and_respects_bounds():
     assert mb.min() >= 0.0
     want = np.maximum(q.ms, 0.0)
     assert np.max(np.abs(mb - want)) < 5e-2
+
+
+class _SpreadQuadratic:
+    """phi(m) = 0.5 (m - m*)^T A (m - m*) with a diagonal A of widely spread scales."""
+
+    def __init__(self, n=60, seed=3):
+        rng = np.random.default_rng(seed)
+        self.a = np.exp(rng.uniform(-3, 3, n))
+        self.mstar = rng.standard_normal(n)
+
+    def value(self, m):
+        d = np.asarray(m, np.float64) - self.mstar
+        return 0.5 * float(d @ (self.a * d))
+
+    def value_and_gradient(self, m):
+        d = np.asarray(m, np.float64) - self.mstar
+        return 0.5 * float(d @ (self.a * d)), (self.a * d).astype(np.float32)
+
+
+def test_lbfgs_takes_good_learned_steps_and_rejects_bad_ones():
+    q = _SpreadQuadratic()
+    m0 = np.zeros(60, np.float32) + 0.5
+    _, plain = fwi.lbfgs(q, m0, niter=6)
+    # an (approximate) inverse Hessian: accepted, and it converges much faster
+    good = {}
+    _, learned = fwi.lbfgs(q, m0, niter=6, precond=lambda m, g: -g / (q.a * (1 + 0.05 * np.cos(np.arange(60)))),
+                           stats=good)
+    assert good["learned"] >= 1 and learned[2] < 1e-3 * plain[2]
+    # a direction that increases the misfit is rejected; the plain steps still converge
+    bad = {}
+    _, fallback = fwi.lbfgs(q, m0, niter=6, precond=lambda m, g: g.astype(np.float64), stats=bad)
+    assert bad["learned"] == 0 and bad["rejected"] >= 6
+    assert fallback[-1] <= plain[-1] * 1.0001
