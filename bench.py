@@ -43,11 +43,14 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="born_600x1800",
                     choices=["born_600x1800", "nl_312x520", "fwi_1000x3400", "fwi_learned", "cnn_train"])
-    ap.add_argument("--pairs", type=int, default=64, help="fwi_learned: Born training pairs")
+    ap.add_argument("--pairs", type=int, default=48, help="fwi_learned: Born training pairs")
     ap.add_argument("--conv-path", type=int, default=-1, choices=[-1, 0, 1],
                     help="cnn_train: forward convolutions on mma.sync (0) or tcgen05 (1); "
                          "-1 keeps the library default (mma.sync)")
-    ap.add_argument("--epochs", type=int, default=60, help="fwi_learned: training epochs")
+    ap.add_argument("--epochs", type=int, default=80, help="fwi_learned: training epochs")
+    ap.add_argument("--depth", type=int, default=6, help="fwi_learned: convolution layers of the network")
+    ap.add_argument("--sigma", type=float, default=3.0,
+                    help="fwi_learned: smoothing length (cells) of the training perturbations")
     ap.add_argument("--shots", type=int, default=None,
                     help="shots per GPU (default: 10 for born_600x1800; a bounded sample of 16 of the 120 shots "
                          "for fwi_1000x3400)")
@@ -841,7 +844,8 @@ def run_ours_learned(args, ws, rank, local):
 
     def train():
         nonlocal P
-        P = precond.LearnedPreconditioner(born, m0, seed=0)
+        P = precond.LearnedPreconditioner(born, m0, sigma=args.sigma, seed=0,
+                                          net=precond.ConvNet(depth=args.depth, device=local, seed=0))
         X, T, _, _ = P.make_pairs(args.pairs, seed=1)
         P.train(X, T, epochs=args.epochs, batch=8, lr=3e-3)
 
@@ -884,7 +888,8 @@ def run_ours_learned(args, ws, rank, local):
             "vs_baseline": None, "dtype": "f32 propagation, bf16 network", "data": "synthetic",
             "config": {"workload": "fwi_learned: 136x520 grid of the batched-FWI model (12.5 m, nts=1200, %d shots, "
                                    "60 receivers each), plain L-BFGS for %d iterations vs learned steps "
-                                   "(%d Born pairs, %d epochs)" % (nsh, args.steps, args.pairs, args.epochs),
+                                   "(%d Born pairs, %d epochs, %d layers, perturbation smoothing %.1f cells)"
+                                   % (nsh, args.steps, args.pairs, args.epochs, args.depth, args.sigma),
                        "l2": "each gradient streams the FP32 source history of a shot (about 1.1 GB) through HBM"},
             "plain": {"iterations": args.steps, "seconds": round(t_plain, 3), "final_misfit": target,
                       "misfit_history": [float(v) for v in plain], "propagations": props_plain},
