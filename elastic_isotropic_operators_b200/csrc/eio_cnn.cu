@@ -628,16 +628,36 @@ void check_ptr(const void* p, const char* what)
     if (reinterpret_cast<uintptr_t>(p) % 16) throw Error(EIO_ERR_ARG, std::string(what) + " not 16-byte aligned");
 }
 
+// Launch shape of kernel `K` on the current device: the dynamic shared-memory
+// attribute set once per device, and the SM count times the CTAs that fit on
+// an SM (at most `cap`).  Cached per device.
+struct KernelSlots {
+    int resident[64] = {};   // 0: not opened on that device yet
+};
+
+template <class K>
+int open_kernel(KernelSlots& ks, K kernel, int threads, int smem, int cap)
+{
+    int dev = 0;
+    CCUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw Error(EIO_ERR_ARG, "device index above 63");
+    if (!ks.resident[dev]) {
+        CCUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        int nsm = 0, per = 0;
+        CCUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        CCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem));
+        ks.resident[dev] = nsm * std::max(1, std::min(per, cap));
+    }
+    return ks.resident[dev];
+}
+
 template <int CIN, int COUT, int EPI>
 void launch_conv(int n, int h, int w, const bf16* x, const bf16* wt, const bf16* mask, int relu, bf16* y,
                  float* y32, cudaStream_t st)
 {
     constexpr int sm = conv_smem<CIN, COUT>();
-    static bool opened = false;   // the attribute is per function and device-independent in value
-    if (!opened) {
-        CCUDA(cudaFuncSetAttribute(k_conv3<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        opened = true;
-    }
+    static KernelSlots ks;
+    open_kernel(ks, k_conv3<CIN, COUT, EPI>, FWD_THREADS, sm, 1 << 20);
     const dim3 grid((w + CT_W - 1) / CT_W, (h + CT_H - 1) / CT_H, n);
     k_conv3<CIN, COUT, EPI><<<grid, FWD_THREADS, sm, st>>>(x, wt, mask, relu, h, w, y, y32);
     CCUDA(cudaGetLastError());
@@ -648,16 +668,9 @@ void launch_conv_tc(int n, int h, int w, const bf16* x, const bf16* wt, const bf
                     float* y32, cudaStream_t st)
 {
     constexpr int sm = TcLayout<CIN, COUT>::SMEM;
-    static int grid_cap = 0;
-    if (!grid_cap) {
-        CCUDA(cudaFuncSetAttribute(k_conv3_tc<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        int dev = 0, nsm = 0, per = 0;
-        CCUDA(cudaGetDevice(&dev));
-        CCUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        CCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_conv3_tc<CIN, COUT, EPI>, TC_THREADS, sm));
-        // each resident CTA holds TC_TMEM_COLS TMEM columns of the SM's 512
-        grid_cap = nsm * std::max(1, std::min(per, 512 / TC_TMEM_COLS));
-    }
+    static KernelSlots ks;
+    // each resident CTA holds TC_TMEM_COLS TMEM columns of the SM's 512
+    const int grid_cap = open_kernel(ks, k_conv3_tc<CIN, COUT, EPI>, TC_THREADS, sm, 512 / TC_TMEM_COLS);
     const long long tiles = (long long)n * ((h + TC_STRIP - 1) / TC_STRIP) * ((w + TC_PIX - 1) / TC_PIX);
     const int grid = (int)std::min<long long>(tiles, grid_cap);
     k_conv3_tc<CIN, COUT, EPI><<<grid, TC_THREADS, sm, st>>>(x, wt, mask, relu, n, h, w, y, y32);
@@ -667,18 +680,10 @@ void launch_conv_tc(int n, int h, int w, const bf16* x, const bf16* wt, const bf
 template <int CIN, int COUT>
 int wgrad_blocks(int n, int h, int w)
 {
-    static int per_sm = 0, nsm = 0;
-    if (!per_sm) {
-        constexpr int sm = wgrad_smem<CIN, COUT>();
-        CCUDA(cudaFuncSetAttribute(k_conv3_wgrad<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        int dev = 0;
-        CCUDA(cudaGetDevice(&dev));
-        CCUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-        CCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv3_wgrad<CIN, COUT>, WG_THREADS, sm));
-        if (per_sm < 1) per_sm = 1;
-    }
+    static KernelSlots ks;
+    const int resident = open_kernel(ks, k_conv3_wgrad<CIN, COUT>, WG_THREADS, wgrad_smem<CIN, COUT>(), 1 << 20);
     const long long tiles = (long long)((w + CT_W - 1) / CT_W) * ((h + CT_H - 1) / CT_H) * n;
-    return (int)std::min<long long>(tiles, (long long)per_sm * nsm);
+    return (int)std::min<long long>(tiles, resident);
 }
 
 }  // namespace
