@@ -174,10 +174,12 @@ class LearnedPreconditioner:
     """Learned approximate inverse of the Gauss-Newton Hessian at a background.
 
     born: a BornElasticShotsGpu on the FWI's acquisition; m0: the background
-    (elastic parameters [3][nx][nz]) the pairs are generated at; interior:
-    (x0, x1, z0, z1) cells where perturbations live (default: inside the
-    absorbing pads).  ``__call__(m, g)`` returns the learned model update
-    (a descent candidate) for the gradient g, for ``fwi.lbfgs(precond=...)``."""
+    (elastic parameters [3][nx][nz]) the pairs are generated at (it becomes
+    born's background); interior: (x0, x1, z0, z1) cells where perturbations
+    live (default: inside the absorbing pads).  ``__call__(m, g)`` returns the
+    learned model update (a descent candidate) for the gradient g, for
+    ``fwi.lbfgs(precond=...)``; it needs make_pairs (which fixes the target
+    scale K) and train first."""
 
     def __init__(self, born, m0, interior=None, net=None, sigma=3.0, rel_rms=0.02, seed=0):
         self.born = born
@@ -248,8 +250,11 @@ class LearnedPreconditioner:
 
     # ------------------------------------------------------------ training
     def train(self, X, T, epochs=40, batch=8, lr=2e-3, seed=0):
-        """Adam on mini-batches of (X, T) (numpy, as make_pairs gives them);
-        returns the mean loss of each epoch."""
+        """Adam on shuffled mini-batches of (X, T) (numpy, as make_pairs gives
+        them), the learning rate on a cosine schedule from lr to 0; returns the
+        mean loss of each epoch."""
+        if X.shape[0] < batch:
+            raise ValueError("need at least one batch of %d pairs (got %d)" % (batch, X.shape[0]))
         torch = _torch()
         dev = self.net.dev
         Xd = torch.as_tensor(X, device=dev).to(torch.bfloat16)
@@ -274,6 +279,8 @@ class LearnedPreconditioner:
 
     def predict(self, g):
         """Learned estimate of dm with J^T J dm = g ([3][nx][nz])."""
+        if self.K is None:
+            raise RuntimeError("make_pairs (and train) before predict: the target scale is not set")
         torch = _torch()
         f, s = self.features(g)
         x = torch.as_tensor(f[None], device=self.net.dev).to(torch.bfloat16).contiguous()
