@@ -105,9 +105,10 @@ class ConvNet:
         """x: BF16 [N][H][W][16] (device) -> FP32 [N][H][W][16] (device; the
         first ``nout`` channels are the output)."""
         L = _lib.lib()
+        torch = _torch()
         n, h, w, c = x.shape
-        if c != _CIN:
-            raise ValueError("input needs %d channels" % _CIN)
+        if c != _CIN or x.dtype != torch.bfloat16 or not x.is_contiguous() or x.device != self.dev:
+            raise ValueError("input must be a contiguous BF16 [N][H][W][%d] tensor on %s" % (_CIN, self.dev))
         self._buffers(n, h, w)
         st = self._stream()
         self.act[0] = x
@@ -123,7 +124,11 @@ class ConvNet:
         channels (target FP32 [N][H][W][nout], device) after ``forward``.
         Returns the loss as a device scalar (FP64)."""
         L = _lib.lib()
+        torch = _torch()
         n, h, w = self._shape
+        if tuple(target.shape) != (n, h, w, self.nout) or target.dtype != torch.float32 or \
+                not target.is_contiguous():
+            raise ValueError("target must be a contiguous FP32 [%d][%d][%d][%d] tensor" % (n, h, w, self.nout))
         st = self._stream()
         depth = len(self.chans) - 1
         check(L.eio_cnn_mse(n * h * w, _COUT, self.nout, _p(self.y32), _p(target), _p(self.dz[-1]),
