@@ -356,7 +356,7 @@ def _lbfgs(objective, m0, niter=10, memory=5, minBound=None, maxBound=None, init
     failed search restarts once from the projected steepest descent.
     With ``precond`` (a learned approximate inverse Hessian, precond(m, g) ~
     -H^-1 g), the recursion runs around it, scaled by the latest curvature
-    pair, instead of the scalar initial Hessian; the exact misfit judges the
+    pair, instead of the scalar initial Hessian; the exact misfit decides the
     step (sufficient decrease with learned_c1, two trials), and when it
     rejects the learned direction, or that is no descent direction, the
     iteration falls back to the plain L-BFGS step.

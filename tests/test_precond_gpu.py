@@ -4,7 +4,7 @@ network gains over the plain gradient.
 
 * On held-out perturbations, the Born data of the learned update fit those of
   the true perturbation better than the data of the gradient do (each at its
-  best scale: the exact Born residual judges).
+  best scale: the exact Born residual decides).
 * In FWI from a perturbed start, L-BFGS with learned steps (each accepted only
   when the exact misfit drops) reaches a lower misfit in the same number of
   iterations than plain L-BFGS."""
