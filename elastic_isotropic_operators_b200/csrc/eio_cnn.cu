@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(FWD_THREADS) k_conv3(const bf16* __restrict__ 
 // The same convolution on the 5th-generation tensor cores.  A CTA (4 warps)
 // walks down a strip of TC_STRIP image rows, 128 output pixels wide; a
 // persistent grid loops over the strips.  Input rows (with a one-pixel halo)
-// sit in a ring of four shared-memory slots as [8-channel chunk][130
+// sit in a ring of five shared-memory slots as [8-channel chunk][130
 // pixels][8 BF16], which is the K-major, non-swizzled operand layout of
 // tcgen05.mma: the A operand of tap (dy, dx) and 16 channels is a descriptor
 // onto slot (y - 1 + dy) shifted by dx pixels (8 pixels x 16 B core matrices,
@@ -187,11 +187,12 @@ __global__ void __launch_bounds__(FWD_THREADS) k_conv3(const bf16* __restrict__ 
 // weights sit as [tap][chunk][Cout][8 BF16] (B operand, K-major).  One thread
 // issues the 9 * Cin / 16 MMAs (M = 128, N = Cout, K = 16) of a row into one of
 // two 32-column TMEM accumulators and commits them to that accumulator's
-// mbarrier.  Software pipeline per row y: wait for input row y + 2 (cp.async),
-// barrier, issue the MMAs of row y + 1, wait (bounded) for those of row y,
-// start the copies of row y + 3 into the slot those MMAs have released,
-// epilogue of row y (each warp reads its 32 lanes = pixels with tcgen05.ld):
-// the copies and the tensor cores run under the epilogue.
+// mbarrier.  Software pipeline per row y: wait for input row y + 2 (cp.async;
+// row y + 3 may still be in flight), barrier, issue the MMAs of row y + 1,
+// wait (bounded) for those of row y, start the copies of row y + 4 into the
+// slot those MMAs have released, epilogue of row y (each warp reads its 32
+// lanes = pixels with tcgen05.ld): copies run two rows ahead, the tensor
+// cores one row ahead of the epilogue.
 // Operand and descriptor layout follow the PTX ISA's tcgen05 matrix
 // descriptor (start, leading and stride byte offsets >> 4, version 1 at bit
 // 46, no swizzle) and instruction descriptor (F32 accumulator, BF16 A and B,
@@ -200,7 +201,7 @@ constexpr int TC_PIX = 128;                 // output pixels of a row tile
 constexpr int TC_HP = TC_PIX + 2;           // staged pixels of a row (halo)
 constexpr int TC_THREADS = 128;
 constexpr int TC_STRIP = 16;                // rows of a strip
-constexpr int TC_SLOTS = 4;                 // input-row ring
+constexpr int TC_SLOTS = 5;                 // input-row ring: rows y-1 .. y+3 of output row y
 constexpr long long TC_WAIT_LIMIT = 1LL << 22;
 constexpr int TC_TMEM_COLS = 64;            // two 32-column accumulators
 
@@ -278,9 +279,15 @@ __device__ __forceinline__ void tc_stage_row(const bf16* __restrict__ x, int H, 
     asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
+__device__ __forceinline__ int tc_slot(int row) { return (row + TC_SLOTS) % TC_SLOTS; }   // row >= -1
+
+__device__ __forceinline__ void tc_commit_empty() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+// copy groups up to all but the newest `pending` have landed, then a barrier
+template <int PENDING>
 __device__ __forceinline__ void tc_rows_landed()
 {
-    asm volatile("cp.async.wait_all;" ::: "memory");
+    asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic writes -> tensor-core reads
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -294,10 +301,10 @@ __device__ __forceinline__ void tc_issue_row(unsigned a0, unsigned b0, int y, un
     constexpr int KC = CIN / 8;
     constexpr unsigned idesc = umma_idesc<COUT>();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll 1
+#pragma unroll
     for (int tap = 0; tap < 9; tap++) {
         const int dy = tap / 3, dx = tap - 3 * dy;
-        const unsigned slot = a0 + (unsigned)(((y + 3 + dy) & (TC_SLOTS - 1)) * Ly::ROW_BYTES);
+        const unsigned slot = a0 + (unsigned)(tc_slot(y - 1 + dy) * Ly::ROW_BYTES);
 #pragma unroll
         for (int kk = 0; kk < CIN / 16; kk++) {
             const unsigned long long ad = umma_desc(slot + (2 * kk * TC_HP + dx) * 16, TC_HP * 16, 128);
@@ -364,15 +371,20 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3_tc(const bf16* __restrict_
         const long long r = u / tilesX;
         const int sy = (int)(r % strips), n = (int)(r / strips);
         const int x0 = xt * TC_PIX, yb = sy * TC_STRIP, ye = min(H, yb + TC_STRIP);
-        // prologue: rows yb-1 .. yb+1, the MMAs of row yb, then row yb+2 in flight
+        // prologue: rows yb-1 .. yb+1, the MMAs of row yb, then rows yb+2 and
+        // yb+3 in flight, one copy group each (empty past the strip)
         for (int gy = yb - 1; gy <= yb + 1; gy++)
-            tc_stage_row<CIN>(x, H, W, n, gy, x0, sA + ((gy + 4) & (TC_SLOTS - 1)) * Ly::ROW_BYTES);
-        tc_rows_landed();
+            tc_stage_row<CIN>(x, H, W, n, gy, x0, sA + tc_slot(gy) * Ly::ROW_BYTES);
+        tc_rows_landed<0>();
         if (tid == 0) tc_issue_row<CIN, COUT>(a0, b0, yb, tmem + (k & 1) * 32, bar0 + (k & 1) * 8);
-        if (yb + 1 < ye) tc_stage_row<CIN>(x, H, W, n, yb + 2, x0, sA + ((yb + 2) & (TC_SLOTS - 1)) * Ly::ROW_BYTES);
+        for (int gy = yb + 2; gy <= yb + 3; gy++) {
+            if (gy - 1 < ye) tc_stage_row<CIN>(x, H, W, n, gy, x0, sA + tc_slot(gy) * Ly::ROW_BYTES);
+            else tc_commit_empty();
+        }
         for (int yy = yb; yy < ye; yy++, k++) {
-            // row yy+2 has landed (and the epilogue of row yy-1 is done): MMAs of row yy+1
-            tc_rows_landed();
+            // row yy+2 has landed (its group is the second newest; the epilogue
+            // of row yy-1 is done): MMAs of row yy+1
+            tc_rows_landed<1>();
             if (yy + 1 < ye && tid == 0)
                 tc_issue_row<CIN, COUT>(a0, b0, yy + 1, tmem + ((k + 1) & 1) * 32, bar0 + ((k + 1) & 1) * 8);
             // bounded wait for the accumulator of row yy
@@ -395,9 +407,10 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3_tc(const bf16* __restrict_
                 break;
             }
             phase[b] ^= 1u;
-            // the MMAs of row yy have read slot (yy-1): row yy+3 goes there, under the epilogue
-            if (yy + 2 < ye)
-                tc_stage_row<CIN>(x, H, W, n, yy + 3, x0, sA + ((yy + 3) & (TC_SLOTS - 1)) * Ly::ROW_BYTES);
+            // the MMAs of row yy have read slot (yy-1): row yy+4 goes there, under
+            // the epilogue and the next row (one group per row, empty past the strip)
+            if (yy + 3 < ye) tc_stage_row<CIN>(x, H, W, n, yy + 4, x0, sA + tc_slot(yy + 4) * Ly::ROW_BYTES);
+            else tc_commit_empty();
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             float v[COUT];
             tmem_ld<COUT>(tmem + b * 32 + ((unsigned)(warp * 32) << 16), v);
