@@ -12,7 +12,11 @@ pieces that script composes, on top of ``nonlinearFwiPropElasticShotsGpu``
   J^T S^T (S F(m) - d) through the Born adjoint, with an optional gradient mask
   and bound vectors (efwiMain.py:120-177, 248-256);
 * ``lbfgs``          -- limited-memory BFGS with a backtracking (Armijo) line
-  search and projection onto the bounds.
+  search and projection onto the bounds, optionally with learned steps;
+* ``band_objective`` / ``multiscale`` -- the multiscale loop of the FWI
+  scripts (efwiMain.py is run once per band with band-limited wavelets): the
+  objective on band-limited sources and data, and L-BFGS band after band,
+  each band starting from the previous band's model.
 
 Reductions that decide the optimisation (misfit, dot products, gradient norm)
 run in FP64 on the GPU through the library's own reduction kernels
@@ -24,7 +28,8 @@ import ctypes
 
 import numpy as np
 
-__all__ = ["dot64", "misfit64", "ElasticDatComp", "ElasticConv", "ElasticConvJab", "FwiObjective", "lbfgs"]
+__all__ = ["dot64", "misfit64", "ElasticDatComp", "ElasticConv", "ElasticConvJab", "FwiObjective", "lbfgs",
+           "band_objective", "multiscale"]
 
 
 def _nd(v):
@@ -450,3 +455,35 @@ def _lbfgs(objective, m0, niter=10, memory=5, minBound=None, maxBound=None, init
             callback(it, m, f, g)
         it += 1
     return m, hist
+
+
+# --------------------------------------------------------------------- multiscale
+def band_objective(nl, born, d_obs, sources, dts, band, **objective_kw):
+    """FwiObjective of one frequency band: the source traces ``sources`` (the
+    nonlinear FWI operator's, [nModelExp][5][nSrc][nts]) and the observed data
+    filtered with the zero-phase trapezoid ``band`` = (f1, f2, f3, f4)
+    (wavelet.band_limit); both operators get the filtered sources."""
+    from .wavelet import band_limit
+    src = np.asarray(_nd(sources), dtype=np.float32)
+    src_b = band_limit(src, dts, *band, axis=-1).astype(np.float32)
+    d_b = band_limit(np.asarray(_nd(d_obs), dtype=np.float32), dts, *band, axis=-1).astype(np.float32)
+    nl.sources = np.ascontiguousarray(src_b)
+    per = src_b.reshape(-1, *src_b.shape[-3:])
+    born.setSourceSignals([per[i] for i in range(per.shape[0])])
+    return FwiObjective(nl, born, d_b, **objective_kw)
+
+
+def multiscale(objective_for_band, m0, bands, niter=10, callback=None, **lbfgs_kw):
+    """L-BFGS band after band: ``objective_for_band(band)`` gives the objective
+    of a band (e.g. band_objective), each band starts from the model the
+    previous one reached.  ``callback(k, band, m, history)`` after each band.
+    Returns (m, [history of each band])."""
+    m = np.array(m0, dtype=np.float32, copy=True)
+    hists = []
+    for k, band in enumerate(bands):
+        obj = objective_for_band(band)
+        m, hist = lbfgs(obj, m, niter=niter, **lbfgs_kw)
+        hists.append(hist)
+        if callback is not None:
+            callback(k, band, m, hist)
+    return m, hists

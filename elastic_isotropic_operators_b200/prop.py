@@ -481,13 +481,20 @@ class BornElasticShotsGpu(_ElasticOp):
                          [receiversVectorCenterGrid, receiversVectorXGrid, receiversVectorZGrid,
                           receiversVectorXZGrid])
         self.elasticHyper = _hyper_of(elasticParam)
-        self._sigs = []
+        self.setSourceSignals(sourcesSignalsVector)
+
+    def setSourceSignals(self, sourcesSignalsVector):
+        """Replace the source signals (1 or nExp of [nts, nSrc, 5]), e.g. by
+        band-limited ones between the bands of a multiscale inversion.  The
+        reference fixes them at construction; this is an extension."""
+        sigs = []
         for s in sourcesSignalsVector:
             self._check_time(s)
             a = _arr(s).reshape(5, self.nSrcIrreg, self.fd.nts)
-            self._sigs.append(np.ascontiguousarray(a))
-        if len(self._sigs) not in (1, self.nExp):
+            sigs.append(np.ascontiguousarray(a, dtype=np.float32))
+        if len(sigs) not in (1, self.nExp):
             raise EioError(-1, "sourcesSignalsVector must hold 1 or nExp signals")
+        self._sigs = sigs
         self._sig_arr = _lib.ptr_array([a.ctypes.data for a in self._sigs])
 
     def _shapes(self, model, data):

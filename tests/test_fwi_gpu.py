@@ -65,3 +65,25 @@ def test_lbfgs_reduces_the_misfit_with_bounds_mask_and_components():
     err0 = np.linalg.norm((m0 - true)[1:])
     err1 = np.linalg.norm((m - true)[1:])
     assert err1 < err0
+
+
+def test_multiscale_bands_reduce_the_misfit_of_each_band():
+    from elastic_isotropic_operators_b200 import wavelet
+    w = synthetic.small(nts=120)
+    src, rec = w.geometry()
+    sig = w.source_signal()
+    true = w.elastic.getNdArray().copy()
+    nl = prop.nonlinearFwiPropElasticShotsGpu(w.elastic, w.par, sig[None], *src, *rec)
+    born = prop.BornElasticShotsGpu(w.elastic, w.par, [sig], *src, *rec)
+    d = nl.dataSpace()
+    nl.forward(False, true, d)
+    d_obs = d.getNdArray().copy()
+    _, m0, _ = _problem()
+    sources = nl.sources.copy()
+    bands = wavelet.multiscale_bands(4.0, 20.0, 2, ramp=2.0)
+    m, hists = fwi.multiscale(lambda band: fwi.band_objective(nl, born, d_obs, sources, w.dts, band), m0, bands,
+                              niter=2, scale=m0)
+    assert len(hists) == 2
+    assert all(h[-1] < h[0] for h in hists), hists
+    # the Born operator took the band-limited signals
+    assert not np.allclose(born._sigs[0], sig.reshape(born._sigs[0].shape))

@@ -116,3 +116,32 @@ def test_lbfgs_takes_good_learned_steps_and_rejects_bad_ones():
     _, fallback = fwi.lbfgs(q, m0, niter=6, precond=lambda m, g: g.astype(np.float64), stats=bad)
     assert bad["learned"] == 0 and bad["rejected"] >= 6
     assert fallback[-1] <= plain[-1] * 1.0001
+
+
+def test_multiscale_runs_each_band_from_the_previous_model():
+    seen = []
+
+    class Band:
+        def __init__(self, target):
+            self.t = np.asarray(target, np.float64)
+
+        def value(self, m):
+            return 0.5 * float(np.sum((np.asarray(m, np.float64) - self.t) ** 2))
+
+        def value_and_gradient(self, m):
+            d = np.asarray(m, np.float64) - self.t
+            return 0.5 * float(d @ d), d.astype(np.float32)
+
+    targets = {(1, 2, 3, 4): np.full(8, 1.0), (1, 2, 6, 7): np.full(8, 2.0)}
+
+    def for_band(band):
+        seen.append(band)
+        return Band(targets[band])
+
+    starts = []
+    m, hists = fwi.multiscale(for_band, np.full(8, 0.5, np.float32), list(targets), niter=20, init_step=0.5,
+                              callback=lambda k, band, mk, h: starts.append(mk.copy()))
+    assert seen == list(targets) and len(hists) == 2
+    assert np.allclose(starts[0], 1.0, atol=1e-3) and np.allclose(m, 2.0, atol=1e-3)
+    # the second band started where the first ended: its first misfit is that of m = 1
+    assert abs(hists[1][0] - 0.5 * 8 * 1.0) < 1e-2
