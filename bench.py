@@ -42,7 +42,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="born_600x1800",
-                    choices=["born_600x1800", "nl_312x520", "fwi_1000x3400", "fwi_learned", "cnn_train"])
+                    choices=["born_600x1800", "nl_312x520", "nl_shots", "fwi_1000x3400", "fwi_learned",
+                             "cnn_train"])
+    ap.add_argument("--batch", type=int, default=8,
+                    help="nl_shots: shots per lockstep launch (1 = one shot at a time on the lanes)")
     ap.add_argument("--pairs", type=int, default=48, help="fwi_learned: Born training pairs")
     ap.add_argument("--conv-path", type=int, default=-1, choices=[-1, 0, 1],
                     help="cnn_train: forward convolutions on mma.sync (0) or tcgen05 (1); "
@@ -454,6 +457,9 @@ def run_reference(args, ws, rank, local):
         if not O.RefGpu.available("f"):
             return {"impl": "reference", "unavailable": "oracle/_ref not built (reference tree absent at build time)"}
         return run_reference_nl(args)
+    if args.workload == "nl_shots":
+        return {"impl": "reference", "unavailable": "the reference arm of the nonlinear path is timed on one shot "
+                "(--workload nl_312x520); its drivers propagate the shots of a call one after another"}
     if args.workload in ("fwi_learned", "cnn_train"):
         return {"impl": "reference", "unavailable": "the reference has no learned preconditioner and no FWI driver "
                 "(its scripts call pySolver, which is not in the reference tree); the plain L-BFGS arm of this "
@@ -988,6 +994,64 @@ def run_ours_cnn(args, ws, rank, local):
             "cpu_baseline": None, "clocks": clk, "gpu_launches": int(launches_per_step * args.steps)}
 
 
+def run_ours_nl_shots(args, ws, rank, local):
+    """Nonlinear forward of --shots (default 8) shots of the 312x520 case per
+    step through nonlinearPropElasticShotsGpu.forward with host buffers, the
+    shots batched --batch per lockstep launch (1: one at a time on the lanes)."""
+    import torch
+    from elastic_isotropic_operators_b200 import _lib, prop, synthetic
+    nsh = args.shots or 8
+    w = synthetic.nl_312x520(nshots=nsh)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    w.par.set("iGpu", str(local))
+    src, rec = w.geometry()
+    nl = prop.nonlinearPropElasticShotsGpu(w.elastic, w.par, *src, *rec)
+    L = _lib.lib()
+    pin_kernel(L, nl.ctx, args)
+    nl.setShotBatch(max(1, min(args.batch, 8)))   # the library default is 8
+    model = nl.modelSpace()
+    model.getNdArray()[...] = w.source_signal()[None]
+    data = nl.dataSpace()
+    upd = float(nsh * (w.nts - 1) * 2 * (w.nz - 8) * (w.nx - 8))
+    est = torch.cuda.ExternalStream(L.eio_ctx_stream(nl.ctx), device=dev)
+    for _ in range(args.warmup):
+        nl.forward(False, model, data)
+    L.eio_ctx_stats(nl.ctx, 1, 1, None, None, None)
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(None)
+    clocks.start()
+    t_ms = 0.0
+    for _ in range(args.steps):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record(est)
+        nl.forward(False, model, data)
+        ev1.record(est)
+        torch.cuda.synchronize()
+        t_ms += ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    t_ms = max_over_ranks(ws, t_ms)
+    value = ws * upd * args.steps / (t_ms * 1e-3) / 1e9
+    peak, pk = measured_peak()
+    n_model = int(np.prod(model.getNdArray().shape))
+    n_data = int(np.prod(data.getNdArray().shape))
+    return {"metric": "Gcells/s", "value": round(value, 3), "unit": "Gcell-updates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_ms / args.steps, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "nl_shots: nonlinear forward of %d shots of the 312x520 case (nts=2000) per step, "
+                                   "%s" % (nsh, "%d shots per lockstep launch" % args.batch if args.batch > 1
+                                           else "one shot at a time on the lanes"),
+                       "shots_per_gpu": nsh, "l2": "host buffers in and out every step (operator API)"},
+            "e2e": {"value": round(value, 3), "unit": "Gcell-updates/s", "h2d_bytes_per_step": 4 * n_model,
+                    "d2h_bytes_per_step": 4 * n_data, "note": "the operator API with host buffers"},
+            "roofline": {"bound": "hbm", "achieved": round(BYTES_PER_CELL * value, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(BYTES_PER_CELL * value / peak, 4), "traffic": None, "peak_source": pk,
+                         "basis": "80 B per cell update over the timed region (job level)"},
+            "cpu_baseline": None, "clocks": clk, "gpu_launches": int(read_stats(L, nl.ctx)["launches"])}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -1001,6 +1065,8 @@ def main():
         out = run_ours_nl(args, ws, rank, local)
     elif args.workload == "fwi_1000x3400":
         out = run_ours_fwi(args, ws, rank, local)
+    elif args.workload == "nl_shots":
+        out = run_ours_nl_shots(args, ws, rank, local)
     elif args.workload == "fwi_learned":
         out = run_ours_learned(args, ws, rank, local)
     elif args.workload == "cnn_train":

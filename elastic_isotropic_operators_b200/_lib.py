@@ -81,6 +81,7 @@ _SIGS = {
     "eio_ctx_set_graphs": (I, [P, I]),
     "eio_ctx_set_shot_windows": (I, [P, I, IP, IP]),
     "eio_ctx_set_lanes": (I, [P, I]),
+    "eio_ctx_set_shot_batch": (I, [P, I]),
     "eio_ctx_get_lanes": (I, [P, IP, IP]),
     "eio_born_shots_dev": (I, [P, I, I, P, P, P, P, IP, P, IP]),
     "eio_fwi_gradient": (I, [P, I, I, FP, FP, I, IP, P, P, I, P, FP, ctypes.POINTER(ctypes.c_double)]),

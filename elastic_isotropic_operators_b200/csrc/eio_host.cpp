@@ -378,6 +378,7 @@ struct eio_ctx {
     // run shots of a multi-shot call concurrently with eng (eio_ctx_set_lanes)
     std::vector<Engine*> extra;
     int lanes = 2;
+    int batch = STEP_BATCH;   // nonlinear forward: shots per lockstep launch (1 = lanes)
     std::vector<std::vector<float>> lane_tmp;   // per-lane host staging of one shot's data (kept across calls)
 };
 
@@ -396,8 +397,8 @@ static Engine* lane_engine(eio_ctx* c, int k) { return k == 0 ? c->eng : c->extr
 // of it; an existing one its Born history, which is allocated at first use).
 // New lanes take the first lane's kernel choice (tuned first), checkpoint
 // precision and graph setting.
-static int ensure_lanes(eio_ctx* c, int nShots, size_t lane_bytes) {
-    int n = std::max(1, std::min(c->lanes, nShots));
+static int ensure_lanes(eio_ctx* c, int nShots, size_t lane_bytes, int want = 0) {
+    int n = std::max(1, std::min(want > 0 ? want : c->lanes, nShots));
     const int have = 1 + (int)c->extra.size();
     if (n > 1) {
         size_t fr = 0, tot = 0;
@@ -668,6 +669,13 @@ EIO_API int eio_reduce64(int device, int op, int dtype, const void* x, const voi
     return guarded([&] {
         if (!result) throw Error(EIO_ERR_ARG, "null result");
         *result = reduce64(device, op, dtype, x, y, n, onDevice != 0);
+    });
+}
+EIO_API int eio_ctx_set_shot_batch(eio_ctx* c, int shots) {
+    return guarded([&] {
+        if (!c) throw Error(EIO_ERR_ARG, "null context");
+        if (shots < 1 || shots > STEP_BATCH) throw Error(EIO_ERR_ARG, "shot batch must be 1 .. 8");
+        c->batch = shots;
     });
 }
 EIO_API int eio_ctx_set_lanes(eio_ctx* c, int lanes) {
@@ -1060,6 +1068,55 @@ EIO_API int eio_born_prepare_model(eio_ctx* c, const float* model, float* const 
     });
 }
 
+// Nonlinear forward of every shot in groups of c->batch engines advanced in
+// lockstep (engine_nl_shots_batch): one launch per fine step for the group.
+static void nl_forward_batched(eio_ctx* c, int add, int nExp, int nModelExp, const float* model, float* data,
+                               eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom, size_t dslice,
+                               size_t mslice) {
+    const int nts = c->fd.p.nts;
+    const int nb = ensure_lanes(c, nExp, lane_bytes(c, false), std::min(c->batch, (int)STEP_BATCH));
+    for (int s0 = 0; s0 < nExp; s0 += nb) {
+        const int cnt = std::min(nb, nExp - s0);
+        std::vector<ShotGrids> gs;
+        std::vector<std::unique_ptr<ShotWindow>> wins;
+        std::vector<ShotGeom> geo(cnt);
+        std::vector<std::vector<float>> reg((size_t)5 * cnt);
+        std::vector<float*> mp((size_t)5 * cnt), dp(cnt);
+        std::vector<const SInterp*> rp((size_t)4 * cnt);
+        std::vector<Engine*> eng(cnt);
+        for (int i = 0; i < cnt; i++) {
+            const int e = s0 + i;
+            eng[i] = lane_engine(c, i);
+            gs.push_back(shot_grids(src, rec, nRecGeom, e));
+        }
+        for (int i = 0; i < cnt; i++) {
+            const int e = s0 + i;
+            const ShotGrids& g = gs[i];
+            wins.emplace_back(new ShotWindow(c, eng[i], g, e, nExp));
+            geo[i] = wins.back()->sg;
+            const float* ms = model + (nModelExp == 1 ? 0 : (size_t)e * mslice);
+            const int nsi = g.s[0]->nIrreg;
+            for (int f = 0; f < 5; f++) {
+                const SInterp& si = *g.s[kFG[f]];
+                reg[(size_t)5 * i + f].assign((size_t)si.nReg * nts, 0.f);
+                sinterp_adjoint(si, false, reg[(size_t)5 * i + f].data(), ms + (size_t)f * nsi * nts);
+            }
+            scale_sources(c->fd, g, &reg[(size_t)5 * i], nts);
+            for (int f = 0; f < 5; f++) mp[(size_t)5 * i + f] = reg[(size_t)5 * i + f].data();
+            for (int k = 0; k < 4; k++) rp[(size_t)4 * i + k] = g.r[k];
+            dp[i] = add ? lane_staging(c, i, dslice) : data + (size_t)e * dslice;
+        }
+        engine_nl_shots_batch(eng.data(), cnt, mp.data(), geo.data(), rp.data(), dp.data());
+        if (add)
+            for (int i = 0; i < cnt; i++) {
+                float* d = data + (size_t)(s0 + i) * dslice;
+                const float* t = dp[i];
+#pragma omp parallel for schedule(static)
+                for (long long j = 0; j < (long long)dslice; j++) d[j] += t[j];
+            }
+    }
+}
+
 static int nl_forward_impl(eio_ctx* c, int add, int nExp, int nModelExp, const float* model, float* data,
                            eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom, int wShot, float* wfld) {
     return guarded([&] {
@@ -1075,6 +1132,10 @@ static int nl_forward_impl(eio_ctx* c, int add, int nExp, int nModelExp, const f
             check_nt(g, nts);
             if ((size_t)5 * g.s[0]->nIrreg * nts != mslice || (size_t)5 * g.r[0]->nIrreg * nts != dslice)
                 throw Error(EIO_ERR_ARG, "device counts differ between shots");
+        }
+        if (c->batch > 1 && nExp > 1 && !(wShot >= 0 && wShot < nExp && wfld) && !c->fd.p.surfaceCondition) {
+            nl_forward_batched(c, add, nExp, nModelExp, model, data, src, rec, nRecGeom, dslice, mslice);
+            return;
         }
         const int nl = ensure_lanes(c, nExp, lane_bytes(c, false));
         std::vector<float*> tmp(nl);

@@ -748,13 +748,12 @@ __device__ __forceinline__ void stage_tile(const StepArgs& a, float* sm, int z0,
 // The current level (forward) or its scaled combinations (adjoint) are staged
 // with plain loads; the old level and the medium are read from global memory.
 // MINB CTAs per SM (3: <= 80 registers, 4: <= 64).
-template <int DIR, int EPI, int MINB = 3, bool FS = false>
-__global__ void __launch_bounds__(NT, MINB) k_step(StepArgs a)
+template <int DIR, int EPI, int MINB, bool FS>
+__device__ __forceinline__ void step_body(const StepArgs& a, int tile)
 {
     __shared__ __align__(16) float sm[5 * SMEM_FIELD];
 
     const int tid = threadIdx.x;
-    const int tile = blockIdx.x;
     const int bz = tile % a.ntz, bx = tile / a.ntz;
     const int z0 = FAT + bz * TZ, x0 = FAT + bx * TX;
     const int nz = a.nz;
@@ -790,6 +789,27 @@ __global__ void __launch_bounds__(NT, MINB) k_step(StepArgs a)
     }
     auto old = [&](int f) { return HOIST ? oreg[f] : ld4(a.o[f] + gi); };
     step_tail<DIR, EPI, 0, 5, NT, decltype(old), FS>(a, sm, tile, tid, tzi, txi, gz, gx, valid, gi, t, old, csave);
+}
+
+template <int DIR, int EPI, int MINB = 3, bool FS = false>
+__global__ void __launch_bounds__(NT, MINB) k_step(StepArgs a)
+{
+    step_body<DIR, EPI, MINB, FS>(a, blockIdx.x);
+}
+
+// The same step for up to STEP_BATCH shots in one launch: blockIdx.y picks the
+// shot, blockIdx.x its tile.  Shots may have different windows (nx, taper):
+// a shot's tiles beyond its own count leave at once, before touching memory.
+struct StepBatch {
+    StepArgs a[STEP_BATCH];
+};
+
+template <int DIR, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_step_batch(const __grid_constant__ StepBatch b)
+{
+    const StepArgs& a = b.a[blockIdx.y];
+    if ((int)blockIdx.x >= a.ntz * ((a.nx - 2 * FAT) / TX)) return;   // CTA-uniform
+    step_body<DIR, EPI_NONE, MINB, false>(a, blockIdx.x);
 }
 
 // Same step with two threads per float4: warps 0-7 update vx and vz, warps

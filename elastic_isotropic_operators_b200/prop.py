@@ -275,6 +275,12 @@ class _ElasticOp:
         context (default 2), each on its own stream and host thread."""
         check(self._L.eio_ctx_set_lanes(self._ctx, int(lanes)))
 
+    def setShotBatch(self, shots):
+        """Nonlinear forward: advance up to ``shots`` (1 .. 8, default 8) shots in
+        lockstep with one step launch for all of them; 1 runs the shots one at
+        a time on the lanes."""
+        check(self._L.eio_ctx_set_shot_batch(self._ctx, int(shots)))
+
     def getMedium(self):
         n = self.fd.nz * self.fd.nx
         out = [np.zeros((self.fd.nx, self.fd.nz), np.float32) for _ in range(5)]

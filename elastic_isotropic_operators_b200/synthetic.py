@@ -139,7 +139,10 @@ def _grid_coord(o, d, idx):
     return np.float32(o + idx * d)
 
 
-def nl_312x520(nts=2000):
+def nl_312x520(nts=2000, nshots=1):
+    """Plain nonlinear modelling case: 200x400 interior with 50-cell pads, six
+    flat layers, 15 Hz Ricker at 20 m depth, 400 receivers.  nshots > 1 spreads
+    further sources along the line (the first one stays mid-line)."""
     nzi, nxi, dz = 200, 400, 10.0
     vps = np.array([1500, 1900, 2300, 2700, 3100, 3500], np.float64)
     layer = np.minimum((np.arange(nzi) * len(vps)) // nzi, len(vps) - 1)
@@ -153,11 +156,13 @@ def nl_312x520(nts=2000):
     ox = -(FAT + 50) * dz
     # z = 20 m below the top of the interior; source mid-line
     z0 = _grid_coord(oz, dz, FAT + 50 + 2)
-    src_x = [_grid_coord(ox, dz, FAT + 50 + nxi // 2)]
+    cols = [nxi // 2] + [int(round(c)) for c in np.linspace(20, nxi - 21, max(nshots - 1, 1))][:nshots - 1]
+    src_x = [_grid_coord(ox, dz, FAT + 50 + c) for c in cols]
     rec_x = np.array([_grid_coord(ox, dz, FAT + 50 + i) for i in range(nxi)], np.float32)
     rec_z = np.full(nxi, z0, np.float32)
     w = ricker(nts, dts, 15.0, 0.1)
-    return Workload("nl_312x520", epp, pads, dz, dz, nts, dts, 1, 30.0, [z0], src_x, rec_z, rec_x, w, 1)
+    return Workload("nl_312x520", epp, pads, dz, dz, nts, dts, 1, 30.0, [z0] * nshots, src_x, rec_z, rec_x, w,
+                    nshots)
 
 
 def born_600x1800(nts=4000, nshots=10, seed=2024):
