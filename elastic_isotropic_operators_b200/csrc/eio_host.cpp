@@ -460,8 +460,11 @@ static void run_lanes(eio_ctx* c, int n, int nShots, F&& f) {
 }
 
 // device bytes a lane needs for a shot: wavefield levels, secondary sources and, for Born, the history
+// (with shot windows set, of the widest window: a lane's buffers grow to the largest shot it runs)
 static size_t lane_bytes(const eio_ctx* c, bool born) {
-    const size_t n = (size_t)c->fd.p.nz * c->fd.p.nx;
+    int nx = c->fd.p.nx;
+    if (!c->win_nx.empty()) nx = *std::max_element(c->win_nx.begin(), c->win_nx.end());
+    const size_t n = (size_t)c->fd.p.nz * nx;
     size_t b = sizeof(float) * n * 40;
     if (born) b += (size_t)2 * c->fd.p.nts * n * (engine_get_checkpoint(c->eng) ? 2 : 4);
     return b;
