@@ -717,6 +717,9 @@ def run_ours_fwi(args, ws, rank, local):
     born.setCheckpointPrecision(1)
     for op in (nl, born):
         pin_kernel(op._L, op.ctx, args)
+    if args.lanes <= 0:
+        # cropped shots are small: four in flight beat two (3.59 -> 3.87 shot gradients/s measured)
+        _lib.check(_lib.lib().eio_ctx_set_lanes(born.ctx, 4))
     ix0, nxw = nl.autoShotWindows()
     born.setShotWindows(ix0, nxw)
     d_obs = nl.dataSpace()
