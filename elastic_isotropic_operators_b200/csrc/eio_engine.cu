@@ -1882,16 +1882,19 @@ double engine_fwi_shot(Engine* e, float* const modelReg[5], const ShotGeom& g, c
     return phi;
 }
 
-// Nonlinear forward of nb shots, one engine each (own wavefields, point lists,
-// windows), advanced in lockstep: one k_step_batch launch per fine step covers
-// the tiles of every shot (blockIdx.y = shot), so small grids fill the GPU
-// and the per-step launch cost is paid once for all of them.  The steps, time
-// weights and arithmetic are those of engine_nl (same stencil body), so each
-// shot's traces equal its single-shot propagation bit for bit.  No free
-// surface, no wavefield output; the launches go to the first engine's stream,
-// which waits for every engine's preparation, and every engine waits for the
-// loop before returning its traces.
-void engine_nl_shots_batch(Engine* const* es, int nb, float* const* modelReg, const ShotGeom* g,
+// Nonlinear forward (adj = 0) or adjoint (adj = 1) of nb shots, one engine
+// each (own wavefields, point lists, windows), advanced in lockstep: one
+// k_step_batch launch per fine step covers the tiles of every shot
+// (blockIdx.y = shot), so small grids fill the GPU and the per-step launch
+// cost is paid once for all of them.  The steps, time weights and arithmetic
+// are those of engine_nl (same stencil body), so each shot's result equals its
+// single-shot propagation with the tile kernel bit for bit.  No free surface,
+// no wavefield output; the launches go to the first engine's stream, which
+// waits for every engine's preparation, and every engine waits for the loop
+// before returning its traces.  modelReg: regular source traces, nb x 5 host
+// arrays (read by the forward, written by the adjoint); dataIrreg: irregular
+// receiver traces, nb host arrays (written by the forward, read by the adjoint).
+void engine_nl_shots_batch(Engine* const* es, int nb, int adj, float* const* modelReg, const ShotGeom* g,
                            const SInterp* const* rec, float* const* dataIrreg) {
     if (nb < 1 || nb > STEP_BATCH) throw Error(EIO_ERR_ARG, "batch of 1 .. 8 shots");
     Engine* e0 = es[0];
@@ -1900,6 +1903,7 @@ void engine_nl_shots_batch(Engine* const* es, int nb, float* const* modelReg, co
     const int minb = (e0->kind == 3 || e0->kind == 5) ? 4 : 3;
     std::vector<PointList> src(nb), recp(nb);
     std::vector<Levels> lv;
+    lv.reserve(nb);
     StepBatch b;
     memset(&b, 0, sizeof(b));
     int max_tiles = 0;
@@ -1911,20 +1915,29 @@ void engine_nl_shots_batch(Engine* const* es, int nb, float* const* modelReg, co
         err_reset(e);
         float* dm[5]; float* dr[5];
         for (int f = 0; f < 5; f++) {
-            h2d(e, e->stage_a[f], modelReg[5 * i + f], (size_t)g[i].nSrc[kFieldGrid[f]] * e->nts);
+            const size_t nm = (size_t)g[i].nSrc[kFieldGrid[f]] * e->nts;
+            if (!adj) h2d(e, e->stage_a[f], modelReg[5 * i + f], nm);
+            else e->stage_a[f].ensure(std::max<size_t>(16, sizeof(float) * nm));
             dm[f] = e->stage_a[f].f();
         }
-        stage_receivers(e, 0, g[i], rec + 4 * i, nullptr, dr);
+        stage_receivers(e, adj, g[i], rec + 4 * i, adj ? dataIrreg[i] : nullptr, dr);
         build_points(e, g[i].srcPos, g[i].nSrc, src[i]);
         build_points(e, g[i].recPos, g[i].nRec, recp[i]);
         StepArgs& a = b.a[i];
         a = base_args(e);
         zero_wavefields(e);
         lv.emplace_back(e);
-        stage_in(e, dm, src[i].ld, e->nts, e->sig_in);
-        zero_out(e, recp[i].ld, e->nts, e->sig_out);
-        a.inj = upload_points(e, src[i], e->inj_ts, e->inj_ent, e->sig_in);
-        a.ext = upload_points(e, recp[i], e->ext_ts, e->ext_ent, e->sig_out);
+        if (!adj) {
+            stage_in(e, dm, src[i].ld, e->nts, e->sig_in);
+            zero_out(e, recp[i].ld, e->nts, e->sig_out);
+            a.inj = upload_points(e, src[i], e->inj_ts, e->inj_ent, e->sig_in);
+            a.ext = upload_points(e, recp[i], e->ext_ts, e->ext_ent, e->sig_out);
+        } else {
+            stage_in(e, dr, recp[i].ld, e->nts, e->sig_in);
+            zero_out(e, src[i].ld, e->nts, e->sig_out);
+            a.inj = upload_points(e, recp[i], e->inj_ts, e->inj_ent, e->sig_in);
+            a.ext = upload_points(e, src[i], e->ext_ts, e->ext_ent, e->sig_out);
+        }
         max_tiles = std::max(max_tiles, e->ntiles);
         if (i > 0) {
             EIO_CUDA(cudaEventRecord(e->ev_sync, e->st));
@@ -1943,28 +1956,52 @@ void engine_nl_shots_batch(Engine* const* es, int nb, float* const* modelReg, co
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    for (int its = 0; its < e0->nts - 1; its++)
-        for (int it2 = 1; it2 < e0->S + 1; it2++) {
-            for (int i = 0; i < nb; i++) {
-                StepArgs& a = b.a[i];
-                lv[i].set(a);
-                a.inj.t0 = its; a.inj.w0 = F[it2 - 1]; a.inj.w1 = F[h + it2 - 1];
-                a.ext.t0 = its; a.ext.w0 = F[it2]; a.ext.w1 = F[h + it2];
-                lv[i].single();
-            }
+    auto launch = [&] {
+        if (!adj) {
             if (minb == 4) EIO_CUDA(cudaLaunchKernelEx(&cfg, k_step_batch<0, 4>, b));
             else EIO_CUDA(cudaLaunchKernelEx(&cfg, k_step_batch<0, 3>, b));
-            e0->step_launches++;
+        } else {
+            if (minb == 4) EIO_CUDA(cudaLaunchKernelEx(&cfg, k_step_batch<1, 4>, b));
+            else EIO_CUDA(cudaLaunchKernelEx(&cfg, k_step_batch<1, 3>, b));
         }
+        e0->step_launches++;
+    };
+    // the fine steps in propagation order, with the time weights of engine_nl
+    auto step = [&](int its, int it2) {
+        const int ki = adj ? it2 + 1 : it2 - 1;
+        for (int i = 0; i < nb; i++) {
+            StepArgs& a = b.a[i];
+            lv[i].set(a);
+            a.inj.t0 = its; a.inj.w0 = F[ki]; a.inj.w1 = F[h + ki];
+            a.ext.t0 = its; a.ext.w0 = F[it2]; a.ext.w1 = F[h + it2];
+            lv[i].single();
+        }
+        launch();
+    };
+    if (!adj) {
+        for (int its = 0; its < e0->nts - 1; its++)
+            for (int it2 = 1; it2 < e0->S + 1; it2++) step(its, it2);
+    } else {
+        for (int its = e0->nts - 2; its > -1; its--)
+            for (int it2 = e0->S - 1; it2 > -1; it2--) step(its, it2);
+    }
     check_launch();
     EIO_CUDA(cudaEventRecord(e0->ev_sync, e0->st));
     for (int i = 0; i < nb; i++) {
         Engine* e = es[i];
         if (i > 0) EIO_CUDA(cudaStreamWaitEvent(e->st, e0->ev_sync, 0));
-        float* dr[5];
-        for (int f = 0; f < 5; f++) dr[f] = e->stage_b[f].f();
-        stage_out(e, recp[i].ld, e->nts, e->sig_out, dr);
-        return_receivers(e, rec + 4 * i, dataIrreg[i]);
+        if (!adj) {
+            float* dr[5];
+            for (int f = 0; f < 5; f++) dr[f] = e->stage_b[f].f();
+            stage_out(e, recp[i].ld, e->nts, e->sig_out, dr);
+            return_receivers(e, rec + 4 * i, dataIrreg[i]);
+        } else {
+            float* dm[5];
+            for (int f = 0; f < 5; f++) dm[f] = e->stage_a[f].f();
+            stage_out(e, src[i].ld, e->nts, e->sig_out, dm);
+            for (int f = 0; f < 5; f++)
+                d2h(e, modelReg[5 * i + f], e->stage_a[f], (size_t)g[i].nSrc[kFieldGrid[f]] * e->nts);
+        }
     }
     for (int i = 0; i < nb; i++) {
         EIO_CUDA(cudaStreamSynchronize(es[i]->st));

@@ -1109,7 +1109,7 @@ static void nl_forward_batched(eio_ctx* c, int add, int nExp, int nModelExp, con
             for (int k = 0; k < 4; k++) rp[(size_t)4 * i + k] = g.r[k];
             dp[i] = add ? lane_staging(c, i, dslice) : data + (size_t)e * dslice;
         }
-        engine_nl_shots_batch(eng.data(), cnt, mp.data(), geo.data(), rp.data(), dp.data());
+        engine_nl_shots_batch(eng.data(), cnt, 0, mp.data(), geo.data(), rp.data(), dp.data());
         if (add)
             for (int i = 0; i < cnt; i++) {
                 float* d = data + (size_t)(s0 + i) * dslice;
@@ -1159,6 +1159,53 @@ static int nl_forward_impl(eio_ctx* c, int add, int nExp, int nModelExp, const f
     });
 }
 
+// Nonlinear adjoint of every shot in groups of c->batch engines advanced in
+// lockstep (engine_nl_shots_batch); each shot's source traces are scaled and
+// interpolated as in nl_shot_adjoint and added to its model slice, shots in
+// order (one stack over every shot for a constant source signal).
+static void nl_adjoint_batched(eio_ctx* c, int nExp, int nModelExp, float* model, const float* data,
+                               eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom, size_t dslice,
+                               size_t mslice) {
+    const int nts = c->fd.p.nts;
+    const int nb = ensure_lanes(c, nExp, lane_bytes(c, false), std::min(c->batch, (int)STEP_BATCH));
+    for (int s0 = 0; s0 < nExp; s0 += nb) {
+        const int cnt = std::min(nb, nExp - s0);
+        std::vector<ShotGrids> gs;
+        std::vector<std::unique_ptr<ShotWindow>> wins;
+        std::vector<ShotGeom> geo(cnt);
+        std::vector<std::vector<float>> reg((size_t)5 * cnt);
+        std::vector<float*> mp((size_t)5 * cnt), dp(cnt);
+        std::vector<const SInterp*> rp((size_t)4 * cnt);
+        std::vector<Engine*> eng(cnt);
+        for (int i = 0; i < cnt; i++) {
+            eng[i] = lane_engine(c, i);
+            gs.push_back(shot_grids(src, rec, nRecGeom, s0 + i));
+        }
+        for (int i = 0; i < cnt; i++) {
+            const int e = s0 + i;
+            const ShotGrids& g = gs[i];
+            wins.emplace_back(new ShotWindow(c, eng[i], g, e, nExp));
+            geo[i] = wins.back()->sg;
+            for (int f = 0; f < 5; f++) {
+                reg[(size_t)5 * i + f].assign((size_t)g.s[kFG[f]]->nReg * nts, 0.f);
+                mp[(size_t)5 * i + f] = reg[(size_t)5 * i + f].data();
+            }
+            for (int k = 0; k < 4; k++) rp[(size_t)4 * i + k] = g.r[k];
+            dp[i] = const_cast<float*>(data) + (size_t)e * dslice;
+        }
+        engine_nl_shots_batch(eng.data(), cnt, 1, mp.data(), geo.data(), rp.data(), dp.data());
+        for (int i = 0; i < cnt; i++) {
+            const int e = s0 + i;
+            const ShotGrids& g = gs[i];
+            const int nsi = g.s[0]->nIrreg;
+            scale_sources_adj(c->fd, g, &reg[(size_t)5 * i], nts);
+            float* m = model + (nModelExp == 1 ? 0 : (size_t)e * mslice);
+            for (int f = 0; f < 5; f++) sinterp_forward(*g.s[kFG[f]], true, reg[(size_t)5 * i + f].data(),
+                                                        m + (size_t)f * nsi * nts);
+        }
+    }
+}
+
 static int nl_adjoint_impl(eio_ctx* c, int add, int nExp, int nModelExp, float* model, const float* data,
                            eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom, int wShot, float* wfld) {
     return guarded([&] {
@@ -1175,6 +1222,10 @@ static int nl_adjoint_impl(eio_ctx* c, int add, int nExp, int nModelExp, float* 
             check_nt(g, nts);
             if ((size_t)5 * g.s[0]->nIrreg * nts != mslice || (size_t)5 * g.r[0]->nIrreg * nts != dslice)
                 throw Error(EIO_ERR_ARG, "device counts differ between shots");
+        }
+        if (c->batch > 1 && nExp > 1 && !(wShot >= 0 && wShot < nExp && wfld) && !c->fd.p.surfaceCondition) {
+            nl_adjoint_batched(c, nExp, nModelExp, model, data, src, rec, nRecGeom, dslice, mslice);
+            return;
         }
         const int nl = ensure_lanes(c, nExp, lane_bytes(c, false));
         // constant source signal: every shot stacks into one model (nonlinearPropElasticShotsGpu.cpp:384-417),

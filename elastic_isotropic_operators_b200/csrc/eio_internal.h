@@ -133,7 +133,7 @@ double engine_fwi_shot(Engine* e, float* const modelReg[5], const ShotGeom& g, c
                        float* const dm[5]);
 void engine_dm_window(Engine* e, float* out[5]);
 constexpr int STEP_BATCH = 8;   // shots of one lockstep launch (k_step_batch)
-void engine_nl_shots_batch(Engine* const* es, int nb, float* const* modelReg, const ShotGeom* g,
+void engine_nl_shots_batch(Engine* const* es, int nb, int adj, float* const* modelReg, const ShotGeom* g,
                            const SInterp* const* rec, float* const* dataIrreg);
 void engine_nl_shot(Engine* e, int adj, float* const modelReg[5], const ShotGeom& g, const SInterp* const rec[4],
                     float* dataIrreg, float* wfld = nullptr);

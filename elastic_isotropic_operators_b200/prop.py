@@ -276,9 +276,9 @@ class _ElasticOp:
         check(self._L.eio_ctx_set_lanes(self._ctx, int(lanes)))
 
     def setShotBatch(self, shots):
-        """Nonlinear forward: advance up to ``shots`` (1 .. 8, default 8) shots in
-        lockstep with one step launch for all of them; 1 runs the shots one at
-        a time on the lanes."""
+        """Nonlinear forward and adjoint: advance up to ``shots`` (1 .. 8, default
+        8) shots in lockstep with one step launch for all of them; 1 runs the
+        shots one at a time on the lanes."""
         check(self._L.eio_ctx_set_shot_batch(self._ctx, int(shots)))
 
     def getMedium(self):

@@ -156,13 +156,13 @@ int eio_ctx_autotune(eio_ctx *c, int *kind, int *tz, int *cw, int *cpr);
  * enable: 1 on, 0 off, -1 unchanged; reset: zero the counters after reading. */
 int eio_ctx_stats(eio_ctx *c, int enable, int reset, long long *launches, long long *stepLaunches,
                   double *stepMs);
-/* Shot batching of the nonlinear forward (no reference counterpart): with
- * shots > 1 (default 8), eio_nl_forward advances up to `shots` (<= 8) shots in
- * lockstep, one engine each, with one step launch per fine step for all of
- * them (blockIdx.y = shot, each shot on its own window and point lists); 1
- * runs the shots one at a time on the lanes.  Traces equal the one-shot
- * propagation with the tile kernel bit for bit.  Not used with the free
- * surface or when a wavefield is saved. */
+/* Shot batching of the nonlinear operators (no reference counterpart): with
+ * shots > 1 (default 8), eio_nl_forward and eio_nl_adjoint advance up to
+ * `shots` (<= 8) shots in lockstep, one engine each, with one step launch per
+ * fine step for all of them (blockIdx.y = shot, each shot on its own window
+ * and point lists); 1 runs the shots one at a time on the lanes.  Results equal
+ * the one-shot propagation with the tile kernel bit for bit.  Not used with
+ * the free surface or when a wavefield is saved. */
 int eio_ctx_set_shot_batch(eio_ctx *c, int shots);
 /* Shot lanes (no reference counterpart; the reference runs one shot per GPU at
  * a time). The multi-shot operators (eio_nl_forward/adjoint,
