@@ -15,7 +15,7 @@ gloo on CPU).  Shots are independent, so the forward needs no exchange at all;
 """
 import numpy as np
 
-__all__ = ["shot_partition", "local_vectors", "stack_model", "gather_data", "ShotParallel"]
+__all__ = ["shot_partition", "local_vectors", "stack_model", "gather_data", "sum_in_rank_order", "ShotParallel"]
 
 
 def shot_partition(nExp, world, rank):
@@ -85,6 +85,23 @@ def gather_data(local, nExp, group=None):
     return out
 
 
+def sum_in_rank_order(value, group=None):
+    """Sum of a float over the ranks of ``group``, added in rank order (FP64),
+    so that every rank gets the same bits whatever the collective's order."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_initialized() or dist.get_world_size(group) == 1:
+        return float(value)
+    dev = _group_device(group)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    parts = [torch.empty_like(t) for _ in range(dist.get_world_size(group))]
+    dist.all_gather(parts, t, group=group)
+    total = 0.0
+    for p in parts:
+        total += float(p.item())
+    return total
+
+
 class ShotParallel:
     """An operator over nExp shots split across the ranks of a process group.
 
@@ -110,6 +127,22 @@ class ShotParallel:
     def forward(self, add, model, data):
         if self.local is not None:
             self.local.forward(add, model, data)
+
+    def fwiGradient(self, model, sources, dObs, components=None, shape=None):
+        """FWI misfit and gradient over every rank's shots: this rank's local
+        operator (a BornElasticShotsGpu) runs the fused gradient of its block
+        (``sources`` and ``dObs`` are this rank's entries), the gradients are
+        summed over the ranks (stack_model) and the misfits added in rank order.
+        ``shape``: the gradient's shape, needed on a rank without shots."""
+        if self.local is not None:
+            phi, g = self.local.fwiGradient(model, sources, dObs, components)
+            g = np.ascontiguousarray(g, np.float32)
+        else:
+            if shape is None:
+                raise ValueError("a rank without shots needs the gradient shape")
+            phi, g = 0.0, np.zeros(shape, np.float32)
+        stack_model(g, self.group)
+        return sum_in_rank_order(phi, self.group), g
 
     def adjoint(self, add, model, data):
         m = model.getNdArray() if hasattr(model, "getNdArray") else model

@@ -113,3 +113,45 @@ def test_two_gloo_ranks_match_serial_oracle(tmp_path):
         # the stacked model differs from the serial sum only by summation order
         assert O.rel_l2(r["grad"], want_grad) < 1e-6
     assert np.array_equal(res[0]["grad"], res[1]["grad"])
+
+
+class _FakeGradient:
+    """Test-only local operator: shot e contributes misfit 0.1 * (e + 1) and
+    gradient (e + 1) * ones to the sum over its block."""
+
+    def __init__(self, shots, shape):
+        self.shots, self.shape = list(shots), shape
+
+    def fwiGradient(self, model, sources, dObs, components=None):
+        assert dObs.shape[0] == len(self.shots)
+        w = sum(e + 1 for e in self.shots)
+        return 0.1 * w, np.full(self.shape, float(w), np.float32)
+
+
+def _rank_fwi(rank, world, port, out_dir):
+    import datetime
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        nExp, shape = 5, (3, 4, 6)
+        op = ShotParallel(lambda shots: _FakeGradient(shots, shape), nExp)
+        d_obs = np.zeros((len(op.shots), 2, 3, 7), np.float32)
+        phi, g = op.fwiGradient(None, None, d_obs, shape=shape)
+        np.savez(os.path.join(out_dir, "fwi%d.npz" % rank), phi=phi, g=g)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_shot_parallel_fwi_gradient_sums_over_ranks(tmp_path, world):
+    import torch.multiprocessing as mp
+    mp.start_processes(_rank_fwi, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    want = sum(e + 1 for e in range(5))
+    res = [np.load(tmp_path / ("fwi%d.npz" % r)) for r in range(world)]
+    for r in res:
+        assert abs(float(r["phi"]) - 0.1 * want) < 1e-12
+        assert np.array_equal(r["g"], np.full((3, 4, 6), float(want), np.float32))
+    assert all(float(r["phi"]) == float(res[0]["phi"]) for r in res)
