@@ -1071,6 +1071,41 @@ EIO_API int eio_born_prepare_model(eio_ctx* c, const float* model, float* const 
     });
 }
 
+// One group of up to c->batch shots for engine_nl_shots_batch: the engines
+// (lanes 0..cnt-1) set to the shots' windows, their geometries, receiver
+// interpolators and one regular source buffer per shot and field.
+struct ShotGroup {
+    int s0, cnt;
+    std::vector<ShotGrids> gs;
+    std::vector<std::unique_ptr<ShotWindow>> wins;
+    std::vector<ShotGeom> geo;
+    std::vector<std::vector<float>> reg;     // [cnt * 5]
+    std::vector<float*> mp;                  // [cnt * 5] -> reg
+    std::vector<float*> dp;                  // [cnt] irregular traces of each shot
+    std::vector<const SInterp*> rp;          // [cnt * 4]
+    std::vector<Engine*> eng;
+    ShotGroup(eio_ctx* c, int first, int n, int nExp, eio_sinterp* const* src, eio_sinterp* const* rec,
+              int nRecGeom)
+        : s0(first), cnt(n), geo(n), reg((size_t)5 * n), mp((size_t)5 * n), dp(n), rp((size_t)4 * n), eng(n) {
+        const int nts = c->fd.p.nts;
+        for (int i = 0; i < cnt; i++) {
+            eng[i] = lane_engine(c, i);
+            gs.push_back(shot_grids(src, rec, nRecGeom, s0 + i));
+        }
+        for (int i = 0; i < cnt; i++) {
+            const ShotGrids& g = gs[i];
+            wins.emplace_back(new ShotWindow(c, eng[i], g, s0 + i, nExp));
+            geo[i] = wins.back()->sg;
+            for (int f = 0; f < 5; f++) {
+                reg[(size_t)5 * i + f].assign((size_t)g.s[kFG[f]]->nReg * nts, 0.f);
+                mp[(size_t)5 * i + f] = reg[(size_t)5 * i + f].data();
+            }
+            for (int k = 0; k < 4; k++) rp[(size_t)4 * i + k] = g.r[k];
+        }
+    }
+    void run(int adj) { engine_nl_shots_batch(eng.data(), cnt, adj, mp.data(), geo.data(), rp.data(), dp.data()); }
+};
+
 // Nonlinear forward of every shot in groups of c->batch engines advanced in
 // lockstep (engine_nl_shots_batch): one launch per fine step for the group.
 static void nl_forward_batched(eio_ctx* c, int add, int nExp, int nModelExp, const float* model, float* data,
@@ -1079,41 +1114,22 @@ static void nl_forward_batched(eio_ctx* c, int add, int nExp, int nModelExp, con
     const int nts = c->fd.p.nts;
     const int nb = ensure_lanes(c, nExp, lane_bytes(c, false), std::min(c->batch, (int)STEP_BATCH));
     for (int s0 = 0; s0 < nExp; s0 += nb) {
-        const int cnt = std::min(nb, nExp - s0);
-        std::vector<ShotGrids> gs;
-        std::vector<std::unique_ptr<ShotWindow>> wins;
-        std::vector<ShotGeom> geo(cnt);
-        std::vector<std::vector<float>> reg((size_t)5 * cnt);
-        std::vector<float*> mp((size_t)5 * cnt), dp(cnt);
-        std::vector<const SInterp*> rp((size_t)4 * cnt);
-        std::vector<Engine*> eng(cnt);
-        for (int i = 0; i < cnt; i++) {
+        ShotGroup grp(c, s0, std::min(nb, nExp - s0), nExp, src, rec, nRecGeom);
+        for (int i = 0; i < grp.cnt; i++) {
             const int e = s0 + i;
-            eng[i] = lane_engine(c, i);
-            gs.push_back(shot_grids(src, rec, nRecGeom, e));
-        }
-        for (int i = 0; i < cnt; i++) {
-            const int e = s0 + i;
-            const ShotGrids& g = gs[i];
-            wins.emplace_back(new ShotWindow(c, eng[i], g, e, nExp));
-            geo[i] = wins.back()->sg;
+            const ShotGrids& g = grp.gs[i];
             const float* ms = model + (nModelExp == 1 ? 0 : (size_t)e * mslice);
             const int nsi = g.s[0]->nIrreg;
-            for (int f = 0; f < 5; f++) {
-                const SInterp& si = *g.s[kFG[f]];
-                reg[(size_t)5 * i + f].assign((size_t)si.nReg * nts, 0.f);
-                sinterp_adjoint(si, false, reg[(size_t)5 * i + f].data(), ms + (size_t)f * nsi * nts);
-            }
-            scale_sources(c->fd, g, &reg[(size_t)5 * i], nts);
-            for (int f = 0; f < 5; f++) mp[(size_t)5 * i + f] = reg[(size_t)5 * i + f].data();
-            for (int k = 0; k < 4; k++) rp[(size_t)4 * i + k] = g.r[k];
-            dp[i] = add ? lane_staging(c, i, dslice) : data + (size_t)e * dslice;
+            for (int f = 0; f < 5; f++)
+                sinterp_adjoint(*g.s[kFG[f]], false, grp.mp[(size_t)5 * i + f], ms + (size_t)f * nsi * nts);
+            scale_sources(c->fd, g, &grp.reg[(size_t)5 * i], nts);
+            grp.dp[i] = add ? lane_staging(c, i, dslice) : data + (size_t)e * dslice;
         }
-        engine_nl_shots_batch(eng.data(), cnt, 0, mp.data(), geo.data(), rp.data(), dp.data());
+        grp.run(0);
         if (add)
-            for (int i = 0; i < cnt; i++) {
+            for (int i = 0; i < grp.cnt; i++) {
                 float* d = data + (size_t)(s0 + i) * dslice;
-                const float* t = dp[i];
+                const float* t = grp.dp[i];
 #pragma omp parallel for schedule(static)
                 for (long long j = 0; j < (long long)dslice; j++) d[j] += t[j];
             }
@@ -1169,39 +1185,17 @@ static void nl_adjoint_batched(eio_ctx* c, int nExp, int nModelExp, float* model
     const int nts = c->fd.p.nts;
     const int nb = ensure_lanes(c, nExp, lane_bytes(c, false), std::min(c->batch, (int)STEP_BATCH));
     for (int s0 = 0; s0 < nExp; s0 += nb) {
-        const int cnt = std::min(nb, nExp - s0);
-        std::vector<ShotGrids> gs;
-        std::vector<std::unique_ptr<ShotWindow>> wins;
-        std::vector<ShotGeom> geo(cnt);
-        std::vector<std::vector<float>> reg((size_t)5 * cnt);
-        std::vector<float*> mp((size_t)5 * cnt), dp(cnt);
-        std::vector<const SInterp*> rp((size_t)4 * cnt);
-        std::vector<Engine*> eng(cnt);
-        for (int i = 0; i < cnt; i++) {
-            eng[i] = lane_engine(c, i);
-            gs.push_back(shot_grids(src, rec, nRecGeom, s0 + i));
-        }
-        for (int i = 0; i < cnt; i++) {
+        ShotGroup grp(c, s0, std::min(nb, nExp - s0), nExp, src, rec, nRecGeom);
+        for (int i = 0; i < grp.cnt; i++) grp.dp[i] = const_cast<float*>(data) + (size_t)(s0 + i) * dslice;
+        grp.run(1);
+        for (int i = 0; i < grp.cnt; i++) {
             const int e = s0 + i;
-            const ShotGrids& g = gs[i];
-            wins.emplace_back(new ShotWindow(c, eng[i], g, e, nExp));
-            geo[i] = wins.back()->sg;
-            for (int f = 0; f < 5; f++) {
-                reg[(size_t)5 * i + f].assign((size_t)g.s[kFG[f]]->nReg * nts, 0.f);
-                mp[(size_t)5 * i + f] = reg[(size_t)5 * i + f].data();
-            }
-            for (int k = 0; k < 4; k++) rp[(size_t)4 * i + k] = g.r[k];
-            dp[i] = const_cast<float*>(data) + (size_t)e * dslice;
-        }
-        engine_nl_shots_batch(eng.data(), cnt, 1, mp.data(), geo.data(), rp.data(), dp.data());
-        for (int i = 0; i < cnt; i++) {
-            const int e = s0 + i;
-            const ShotGrids& g = gs[i];
+            const ShotGrids& g = grp.gs[i];
             const int nsi = g.s[0]->nIrreg;
-            scale_sources_adj(c->fd, g, &reg[(size_t)5 * i], nts);
+            scale_sources_adj(c->fd, g, &grp.reg[(size_t)5 * i], nts);
             float* m = model + (nModelExp == 1 ? 0 : (size_t)e * mslice);
-            for (int f = 0; f < 5; f++) sinterp_forward(*g.s[kFG[f]], true, reg[(size_t)5 * i + f].data(),
-                                                        m + (size_t)f * nsi * nts);
+            for (int f = 0; f < 5; f++)
+                sinterp_forward(*g.s[kFG[f]], true, grp.mp[(size_t)5 * i + f], m + (size_t)f * nsi * nts);
         }
     }
 }
