@@ -145,3 +145,38 @@ def test_multiscale_runs_each_band_from_the_previous_model():
     assert np.allclose(starts[0], 1.0, atol=1e-3) and np.allclose(m, 2.0, atol=1e-3)
     # the second band started where the first ended: its first misfit is that of m = 1
     assert abs(hists[1][0] - 0.5 * 8 * 1.0) < 1e-2
+
+
+def test_band_objective_filters_sources_and_data_for_both_operators():
+    from elastic_isotropic_operators_b200 import wavelet
+
+    class NL:
+        sources = None
+
+    class Born:
+        fd = type("fd", (), {"surfaceCondition": 0})()
+        sigs = None
+
+        def setSourceSignals(self, s):
+            self.sigs = [np.array(x) for x in s]
+
+        def fwiGradient(self, *a):       # makes FwiObjective consider the fused path
+            raise AssertionError("not called here")
+
+    rng = np.random.default_rng(0)
+    dts, nts = 1e-3, 256
+    src = rng.standard_normal((2, 5, 1, nts)).astype(np.float32)
+    d_obs = rng.standard_normal((2, 5, 3, nts)).astype(np.float32)
+    nl, born = NL(), Born()
+    nl.sources = src.copy()
+    band = (2.0, 4.0, 20.0, 25.0)
+    obj = fwi.band_objective(nl, born, d_obs, src, dts, band)
+    want_src = wavelet.band_limit(src, dts, *band)
+    assert np.allclose(nl.sources, want_src, atol=1e-6)
+    assert len(born.sigs) == 2 and np.allclose(born.sigs[1], want_src[1], atol=1e-6)
+    assert np.allclose(obj.d_obs, wavelet.band_limit(d_obs, dts, *band), atol=1e-6)
+    # the band removes energy above 25 Hz
+    spec = np.abs(np.fft.rfft(obj.d_obs, axis=-1))
+    f = np.fft.rfftfreq(nts, dts)
+    assert spec[..., f > 26].max() < 1e-4 * spec.max()
+    assert obj.fused
