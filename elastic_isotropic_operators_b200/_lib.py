@@ -20,6 +20,7 @@ _ERRORS = {
     -4: "acquisition device out of bounds",
     -5: "unsupported option",
     -6: "out of memory",
+    -7: "device wait timed out",
 }
 
 F = ctypes.c_float
@@ -76,6 +77,8 @@ _SIGS = {
     "eio_ctx_set_kernel": (I, [P, I, I, I, I]),
     "eio_ctx_get_kernel": (I, [P, IP, IP, IP, IP]),
     "eio_ctx_autotune": (I, [P, IP, IP, IP, IP]),
+    "eio_ctx_set_wait_limit": (I, [P, ctypes.c_longlong]),
+    "eio_ctx_get_wait_limit": (I, [P, ctypes.POINTER(ctypes.c_longlong)]),
     "eio_ctx_stats": (I, [P, I, I, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
                           ctypes.POINTER(ctypes.c_double)]),
     "eio_ctx_set_graphs": (I, [P, I]),
@@ -90,6 +93,8 @@ _SIGS = {
     "eio_cnn_set_conv_path": (I, [I]),
     "eio_cnn_get_conv_path": (I, [IP]),
     "eio_cnn_status": (I, [I, IP]),
+    "eio_cnn_set_wait_limit": (I, [ctypes.c_longlong]),
+    "eio_cnn_get_wait_limit": (I, [ctypes.POINTER(ctypes.c_longlong)]),
     "eio_cnn_wgrad_scratch": (I, [I, I, I, I, I, ctypes.POINTER(ctypes.c_longlong)]),
     "eio_cnn_conv3x3_wgrad": (I, [I, I, I, I, I, P, P, P, P, ctypes.c_longlong, P]),
     "eio_cnn_flip": (I, [I, I, P, P, P]),

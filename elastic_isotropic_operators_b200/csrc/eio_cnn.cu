@@ -202,10 +202,31 @@ constexpr int TC_HP = TC_PIX + 2;           // staged pixels of a row (halo)
 constexpr int TC_THREADS = 128;
 constexpr int TC_STRIP = 16;                // rows of a strip
 constexpr int TC_SLOTS = 5;                 // input-row ring: rows y-1 .. y+3 of output row y
-constexpr long long TC_WAIT_LIMIT = 1LL << 22;
+constexpr long long TC_WAIT_LIMIT = 1LL << 22;   // default try_wait polls of an accumulator wait
+constexpr long long TC_DRAIN_LIMIT = 1LL << 24;  // polls of a drain wait after a timeout (never shortened)
 constexpr int TC_TMEM_COLS = 64;            // two 32-column accumulators
 
-__device__ int g_cnn_err;                   // set when an mbarrier wait gives up
+// set when an mbarrier wait gives up: 1 = an accumulator wait timed out (the
+// CTA drained its MMAs and copies and stopped; that call's output is
+// incomplete), 2 = even the drain timed out (the context should be dropped)
+__device__ int g_cnn_err;
+
+// bounded wait on phase `parity` of the mbarrier at shared address `bar`
+__device__ __forceinline__ bool tc_wait(unsigned bar, unsigned parity, long long limit)
+{
+    for (long long it = 0; it < limit; it++) {
+        unsigned done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
 
 template <int CIN, int COUT>
 struct TcLayout {
@@ -326,7 +347,8 @@ __device__ __forceinline__ void tc_issue_row(unsigned a0, unsigned b0, int y, un
 template <int CIN, int COUT, int EPI>
 __global__ void __launch_bounds__(TC_THREADS) k_conv3_tc(const bf16* __restrict__ x, const bf16* __restrict__ w,
                                                         const bf16* __restrict__ mask, int relu, int N, int H,
-                                                        int W, bf16* __restrict__ y, float* __restrict__ y32)
+                                                        int W, bf16* __restrict__ y, float* __restrict__ y32,
+                                                        long long wait_limit)
 {
     using Ly = TcLayout<CIN, COUT>;
     constexpr int KC = CIN / 8;
@@ -389,20 +411,18 @@ __global__ void __launch_bounds__(TC_THREADS) k_conv3_tc(const bf16* __restrict_
                 tc_issue_row<CIN, COUT>(a0, b0, yy + 1, tmem + ((k + 1) & 1) * 32, bar0 + ((k + 1) & 1) * 8);
             // bounded wait for the accumulator of row yy
             const unsigned b = k & 1;
-            bool ok = false;
-            for (long long it = 0; it < TC_WAIT_LIMIT && !ok; it++) {
-                unsigned done;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\t"
-                    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                    "selp.u32 %0, 1, 0, p;\n\t}"
-                    : "=r"(done)
-                    : "r"(bar0 + b * 8), "r"(phase[b])
-                    : "memory");
-                ok = done != 0;
-            }
+            const bool ok = tc_wait(bar0 + b * 8, phase[b], wait_limit);
             if (__syncthreads_or(!ok)) {
-                if (tid == 0) atomicExch(&g_cnn_err, 1);
+                // Timed out.  The MMAs of row yy (buffer b) and, when issued,
+                // of row yy+1 (buffer b^1) may still be running and write TMEM
+                // and arrive on the barriers; the cp.async copies of the ring
+                // may still be landing.  Drain both before the CTA frees TMEM
+                // and leaves, with a long fixed bound.
+                bool drained = tc_wait(bar0 + b * 8, phase[b], TC_DRAIN_LIMIT);
+                if (yy + 1 < ye) drained = tc_wait(bar0 + (b ^ 1) * 8, phase[b ^ 1], TC_DRAIN_LIMIT) && drained;
+                asm volatile("cp.async.wait_all;" ::: "memory");
+                drained = !__syncthreads_or(!drained);
+                if (tid == 0) atomicMax(&g_cnn_err, drained ? 1 : 2);
                 bad = true;
                 break;
             }
@@ -676,6 +696,9 @@ void launch_conv(int n, int h, int w, const bf16* x, const bf16* wt, const bf16*
     CCUDA(cudaGetLastError());
 }
 
+// try_wait polls of the tcgen05 kernel's accumulator waits (process-wide)
+long long g_tc_wait_limit = TC_WAIT_LIMIT;
+
 template <int CIN, int COUT, int EPI>
 void launch_conv_tc(int n, int h, int w, const bf16* x, const bf16* wt, const bf16* mask, int relu, bf16* y,
                     float* y32, cudaStream_t st)
@@ -686,7 +709,7 @@ void launch_conv_tc(int n, int h, int w, const bf16* x, const bf16* wt, const bf
     const int grid_cap = open_kernel(ks, k_conv3_tc<CIN, COUT, EPI>, TC_THREADS, sm, 512 / TC_TMEM_COLS);
     const long long tiles = (long long)n * ((h + TC_STRIP - 1) / TC_STRIP) * ((w + TC_PIX - 1) / TC_PIX);
     const int grid = (int)std::min<long long>(tiles, grid_cap);
-    k_conv3_tc<CIN, COUT, EPI><<<grid, TC_THREADS, sm, st>>>(x, wt, mask, relu, n, h, w, y, y32);
+    k_conv3_tc<CIN, COUT, EPI><<<grid, TC_THREADS, sm, st>>>(x, wt, mask, relu, n, h, w, y, y32, g_tc_wait_limit);
     CCUDA(cudaGetLastError());
 }
 
@@ -712,6 +735,9 @@ void cnn_set_conv_path(int path)
 }
 
 int cnn_get_conv_path() { return g_conv_path; }
+
+void cnn_set_wait_limit(long long polls) { g_tc_wait_limit = polls < 0 ? TC_WAIT_LIMIT : polls; }
+long long cnn_get_wait_limit() { return g_tc_wait_limit; }
 
 int cnn_status(int reset)
 {

@@ -131,6 +131,9 @@ struct Engine {
     const void* tbase[15] = {};
     int tile_ctas[2] = {0, 0};    // persistent k_tile grid per direction (0 = not yet queried)
     DBuf err;
+    // try_wait polls of a TMA pipeline wait in the sweep and tile kernels before
+    // it gives up (error flag, drain, EIO_ERR_TIMEOUT); their drains keep DRAIN_LIMIT
+    long long wait_limit = WAIT_LIMIT;
     // launch statistics (bench instrumentation)
     long long launches = 0, step_launches = 0, sampled = 0;
     double step_ms = 0.0;
@@ -578,6 +581,7 @@ static void launch_sweep(Engine* e, const StepArgs& a, int cur) {
     s.tmode = a.tmode; s.tw_o = a.tw_o; s.tw_c = a.tw_c; s.tw_n = a.tw_n;
     for (int f = 0; f < 5; f++) s.c[f] = a.c[f];
     s.err = static_cast<int*>(e->err.p);
+    s.wait_limit = e->wait_limit;
     const int nb = s.nstrips * s.nranges;
     if (e->tz == 64 && e->cw == 8) launch_sweep_t<DIR, EPI, 64, 8>(e, s, nb);
     else if (e->tz == 64 && e->cw == 16) launch_sweep_t<DIR, EPI, 64, 16>(e, s, nb);
@@ -631,6 +635,7 @@ static void launch_tile(Engine* e, const StepArgs& a, int cur) {
     t.s = a;
     t.ntiles = e->ntiles;
     t.err = static_cast<int*>(e->err.p);
+    t.wait_limit = e->wait_limit;
     const int grid = std::min(e->ntiles, e->tile_ctas[DIR]);
     k_tile<DIR, EPI><<<grid, NT, TileLayout<DIR>::BYTES, e->st>>>(t);
 }
@@ -1015,7 +1020,7 @@ void engine_autotune(Engine* e) {
     e->stats = stats;
     int flag = 0;
     EIO_CUDA(cudaMemcpy(&flag, e->err.p, sizeof(int), cudaMemcpyDeviceToHost));
-    if (flag) throw Error(EIO_ERR_CUDA, "a TMA pipeline wait timed out while tuning");
+    if (flag) throw Error(EIO_ERR_TIMEOUT, "a TMA pipeline wait timed out while tuning");
 }
 
 static void zero_wavefields(Engine* e) {
@@ -1052,8 +1057,11 @@ static void err_reset(Engine* e) {
 static void err_check(Engine* e) {
     int flag = 0;
     EIO_CUDA(cudaMemcpy(&flag, e->err.p, sizeof(int), cudaMemcpyDeviceToHost));
-    if (flag) throw Error(EIO_ERR_CUDA, "a TMA pipeline wait timed out in the step kernel");
+    if (flag) throw Error(EIO_ERR_TIMEOUT, "a TMA pipeline wait timed out in the step kernel (output incomplete)");
 }
+
+void engine_set_wait_limit(Engine* e, long long polls) { e->wait_limit = polls < 0 ? WAIT_LIMIT : polls; }
+long long engine_get_wait_limit(const Engine* e) { return e->wait_limit; }
 
 // new level (in p) into coarse rows its, its+1 of the saved wavefield
 static void save_wavefield(Engine* e, float* W, float* const p[5], int its, float w0, float w1) {
@@ -2081,23 +2089,67 @@ constexpr long long TOTAL = OFF_ENT + 2LL * MAX_POINTS * 2;          // in 4-byt
 static __device__ __align__(256) float g_noalloc_scratch[TOTAL];
 
 static std::mutex g_mu;
-static float* g_dev_addr[256];
+// per device ordinal: the address found at set-up and the id of the CUDA
+// context it belongs to (a cudaDeviceReset ends that context; the next one
+// loads the library's device code anew, possibly at another address)
+struct ScratchSlot {
+    unsigned long long ctx = 0;
+    float* p = nullptr;
+};
+static ScratchSlot g_dev_addr[256];
 
-// Device address of the scratch array on the current device.  The first call on
-// a device looks it up (cudaGetSymbolAddress); later calls reuse it.
+// id of the context current on this thread (driver entry points through the
+// runtime, so nothing links libcuda); false when there is none or the driver
+// cannot tell
+static bool current_context_id(unsigned long long* id) {
+    static PFN_cuCtxGetCurrent_v4000 get_cur = nullptr;
+    static PFN_cuCtxGetId_v12000 get_id = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_cur = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(p);
+    }
+    if (!get_cur || !get_id) return false;
+    CUcontext c = nullptr;
+    if (get_cur(&c) != CUDA_SUCCESS || !c) return false;
+    return get_id(c, id) == CUDA_SUCCESS;
+}
+
+// Device address of the scratch array on the current device.  Set-up, once
+// per device: the first call looks it up with cudaGetSymbolAddress (the host
+// symbol itself is only a stand-in, never a device address) and keeps it
+// with the id of the device's context; later calls in that context reuse it.
+// After a cudaDeviceReset the context id differs and the address is looked
+// up again.  Where the driver cannot report context ids, every call looks it
+// up (cheap: no allocation).
 static float* scratch_on_current_device() {
     int dev = 0;
     EIO_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 256) throw Error(EIO_ERR_ARG, "device ordinal out of range");
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_dev_addr[dev]) {
-        void* p = nullptr;
-        cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (err != cudaSuccess || !p)
-            throw Error(EIO_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(err));
-        g_dev_addr[dev] = static_cast<float*>(p);
+    unsigned long long id = 0;
+    ScratchSlot& slot = g_dev_addr[dev];
+    if (slot.p && current_context_id(&id) && id == slot.ctx) return slot.p;
+    void* p = nullptr;
+    cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (err != cudaSuccess || !p)
+        throw Error(EIO_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(err));
+    // the lookup made the device's primary context current on this thread
+    if (current_context_id(&id)) {
+        slot.ctx = id;
+        slot.p = static_cast<float*>(p);
+    } else {
+        slot = ScratchSlot();
     }
-    return g_dev_addr[dev];
+    return static_cast<float*>(p);
 }
 
 // Per-tile buckets of the tile kernel (TZ x TX tiles numbered z-fastest).

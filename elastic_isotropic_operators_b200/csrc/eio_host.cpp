@@ -426,6 +426,7 @@ static int ensure_lanes(eio_ctx* c, int nShots, size_t lane_bytes, int want = 0)
             engine_set_kernel(e, kind, tz, cw, cpr);
             engine_set_checkpoint(e, engine_get_checkpoint(c->eng));
             engine_set_graphs(e, engine_get_graphs(c->eng));
+            engine_set_wait_limit(e, engine_get_wait_limit(c->eng));
         } catch (...) {
             engine_destroy(e);
             throw;
@@ -631,6 +632,19 @@ EIO_API int eio_ctx_set_kernel(eio_ctx* c, int kind, int tz, int cw, int cpr) {
         if (!c) throw Error(EIO_ERR_ARG, "null context");
         engine_set_kernel(c->eng, kind, tz, cw, cpr);
         for (Engine* e : c->extra) engine_set_kernel(e, kind, tz, cw, cpr);
+    });
+}
+EIO_API int eio_ctx_set_wait_limit(eio_ctx* c, long long polls) {
+    return guarded([&] {
+        if (!c) throw Error(EIO_ERR_ARG, "null context");
+        engine_set_wait_limit(c->eng, polls);
+        for (Engine* e : c->extra) engine_set_wait_limit(e, polls);
+    });
+}
+EIO_API int eio_ctx_get_wait_limit(const eio_ctx* c, long long* polls) {
+    return guarded([&] {
+        if (!c || !polls) throw Error(EIO_ERR_ARG, "null context or output");
+        *polls = engine_get_wait_limit(c->eng);
     });
 }
 EIO_API int eio_ctx_autotune(eio_ctx* c, int* kind, int* tz, int* cw, int* cpr) {
@@ -1527,6 +1541,15 @@ EIO_API int eio_cnn_get_conv_path(int* path) {
     return guarded([&] {
         if (!path) throw Error(EIO_ERR_ARG, "null result");
         *path = cnn_get_conv_path();
+    });
+}
+EIO_API int eio_cnn_set_wait_limit(long long polls) {
+    return guarded([&] { cnn_set_wait_limit(polls); });
+}
+EIO_API int eio_cnn_get_wait_limit(long long* polls) {
+    return guarded([&] {
+        if (!polls) throw Error(EIO_ERR_ARG, "null output");
+        *polls = cnn_get_wait_limit();
     });
 }
 EIO_API int eio_cnn_status(int reset, int* err) {

@@ -66,6 +66,8 @@ void engine_set_medium(Engine* e, const FdParam& fd);
 void engine_set_checkpoint(Engine* e, int mode);
 // step-kernel selection: kind 0 tile kernel, 1 TMA sweep (tz, cw, cpr); autotune times the candidates
 void engine_set_kernel(Engine* e, int kind, int tz, int cw, int cpr);
+void engine_set_wait_limit(Engine* e, long long polls);   // < 0: the default
+long long engine_get_wait_limit(const Engine* e);
 void engine_get_kernel(const Engine* e, int* kind, int* tz, int* cw, int* cpr);
 void engine_autotune(Engine* e);
 void* engine_stream(Engine* e);
@@ -91,6 +93,8 @@ long long cnn_wgrad_scratch(int n, int h, int w, int cin, int cout);
 void cnn_set_conv_path(int path);
 int cnn_get_conv_path();
 int cnn_status(int reset);
+void cnn_set_wait_limit(long long polls);   // < 0: the default
+long long cnn_get_wait_limit();
 void cnn_conv3x3_wgrad(int n, int h, int w, int cin, int cout, const void* x, const void* dy, float* dw,
                        float* scratch, long long scratchFloats, void* stream);
 void cnn_flip(int cin, int cout, const void* w, void* wt, void* stream);

@@ -19,7 +19,8 @@
 
 namespace eio {
 
-constexpr long long WAIT_LIMIT = 1LL << 20;   // try_wait polls before an mbarrier wait gives up
+constexpr long long WAIT_LIMIT = 1LL << 20;   // default try_wait polls before a pipeline wait gives up
+constexpr long long DRAIN_LIMIT = 1LL << 24;  // polls of a drain wait after a timeout (never shortened)
 constexpr int SWEEP_MAXK = 64;                // chunks per CTA range (upper bound)
 
 struct SweepArgs {
@@ -43,6 +44,7 @@ struct SweepArgs {
     int tmode; float tw_o, tw_c, tw_n;   // EPI_TRI, see StepArgs
     const float* c[5];                  // current level (adjoint EPI_TRI reads it directly)
     int* err;
+    long long wait_limit;   // try_wait polls of a pipeline wait (the drain always gets DRAIN_LIMIT)
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -55,10 +57,10 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
 }
-// bounded wait on phase `parity`; returns false on timeout
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+// bounded wait on phase `parity` (at most `limit` polls); returns false on timeout
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, long long limit) {
     const unsigned a = smem_u32(bar);
-    for (long long it = 0; it < WAIT_LIMIT; it++) {
+    for (long long it = 0; it < limit; it++) {
         unsigned done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -228,14 +230,14 @@ __global__ void __launch_bounds__(SweepLayout<TZ, CW, DIR>::NT) k_sweep(const __
     }
     if (DIR == 1) {
         for (int u = 0; u < 2; u++) {
-            if (!mbar_wait(rbar + (u % 2), (u / 2) & 1)) fail();
+            if (!mbar_wait(rbar + (u % 2), (u / 2) & 1, a.wait_limit)) fail();
             transform(u);
             __syncthreads();
             if (abort_flag) break;
             if (tid == 0) issue_unit(u + 2);
         }
     } else {
-        if (!mbar_wait(rbar, 0)) fail();
+        if (!mbar_wait(rbar, 0, a.wait_limit)) fail();
     }
 
     const int zg = tid % NZG, jc = tid / NZG;
@@ -271,9 +273,9 @@ __global__ void __launch_bounds__(SweepLayout<TZ, CW, DIR>::NT) k_sweep(const __
             pre[0] = ld4(w0p); pre[1] = ld4(w0p + a.wstride); pre[2] = ld4(w1p); pre[3] = ld4(w1p + a.wstride);
         }
         if (DIR == 0) {
-            if (!mbar_wait(rbar + ((k + 1) % RU), ((k + 1) / RU) & 1)) fail();
+            if (!mbar_wait(rbar + ((k + 1) % RU), ((k + 1) / RU) & 1, a.wait_limit)) fail();
         }
-        if (!mbar_wait(sbar + (k & 1), (k >> 1) & 1)) fail();
+        if (!mbar_wait(sbar + (k & 1), (k >> 1) & 1, a.wait_limit)) fail();
         // (the adjoint product units k, k+1 were completed by earlier iterations / the prologue)
         const float* u0 = prod + (k % RU) * (5 * UNIT);
         const float* u1 = prod + ((k + 1) % RU) * (5 * UNIT);
@@ -459,7 +461,7 @@ __global__ void __launch_bounds__(SweepLayout<TZ, CW, DIR>::NT) k_sweep(const __
             if (tid == 0) issue_stage(k + 2);
             // product unit k+2 replaces unit k-1; its raw copy was issued two iterations ago
             if (k + 2 <= K) {
-                if (!mbar_wait(rbar + (k % 2), ((k + 2) / 2) & 1)) fail();
+                if (!mbar_wait(rbar + (k % 2), ((k + 2) / 2) & 1, a.wait_limit)) fail();
                 transform(k + 2);
                 __syncthreads();
                 if (tid == 0 && !abort_flag) issue_unit(k + 4);
@@ -471,7 +473,7 @@ __global__ void __launch_bounds__(SweepLayout<TZ, CW, DIR>::NT) k_sweep(const __
         // drain: wait (bounded) for the last phase issued on every barrier
         for (int i = 0; i < Ly::NBAR; i++) {
             if (!pend[i]) continue;
-            mbar_wait(bar + i, ppar[i]);
+            mbar_wait(bar + i, ppar[i], DRAIN_LIMIT);
         }
     }
 }

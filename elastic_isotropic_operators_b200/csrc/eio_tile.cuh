@@ -29,6 +29,7 @@ struct TileArgs {
     StepArgs s;           // everything else, as for k_step
     int ntiles;
     int* err;
+    long long wait_limit;   // try_wait polls of a pipeline wait (the drain always gets DRAIN_LIMIT)
 };
 
 template <int DIR>
@@ -45,9 +46,9 @@ struct TileLayout {
 };
 
 // bounded, CTA-uniform wait; false after a timeout (error flag set)
-__device__ __forceinline__ bool tile_wait(unsigned long long* bar, unsigned parity, int* err)
+__device__ __forceinline__ bool tile_wait(unsigned long long* bar, unsigned parity, int* err, long long limit)
 {
-    const bool ok = mbar_wait(bar, parity);
+    const bool ok = mbar_wait(bar, parity, limit);
     if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0 && err) atomicExch(err, 1);
         return false;
@@ -108,10 +109,10 @@ __global__ void __launch_bounds__(NT, 1) k_tile(const __grid_constant__ TileArgs
         float* st = sm + s * Ly::STAGE;
         const int next = tile + gridDim.x;
         if (tid == 0 && next < ta.ntiles) tile_issue<DIR>(ta, sm + (s ^ 1) * Ly::STAGE, bar + (s ^ 1), next);
-        if (!tile_wait(bar + s, (i >> 1) & 1, ta.err)) {
+        if (!tile_wait(bar + s, (i >> 1) & 1, ta.err, ta.wait_limit)) {
             // drain: this stage and, if issued, the next one
-            mbar_wait(bar + s, (i >> 1) & 1);
-            if (next < ta.ntiles) mbar_wait(bar + (s ^ 1), ((i + 1) >> 1) & 1);
+            mbar_wait(bar + s, (i >> 1) & 1, DRAIN_LIMIT);
+            if (next < ta.ntiles) mbar_wait(bar + (s ^ 1), ((i + 1) >> 1) & 1, DRAIN_LIMIT);
             return;
         }
         const int z0 = FAT + (tile % a.ntz) * TZ, x0 = FAT + (tile / a.ntz) * TX;

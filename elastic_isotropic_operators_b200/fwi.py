@@ -462,9 +462,20 @@ def band_objective(nl, born, d_obs, sources, dts, band, **objective_kw):
     """FwiObjective of one frequency band: the source traces ``sources`` (the
     nonlinear FWI operator's, [nModelExp][5][nSrc][nts]) and the observed data
     filtered with the zero-phase trapezoid ``band`` = (f1, f2, f3, f4)
-    (wavelet.band_limit); both operators get the filtered sources."""
+    (wavelet.band_limit); both operators get the filtered sources.
+
+    ``nl.sources`` holds the filtered traces afterwards.  The first call keeps
+    a copy of the broadband traces the operator was built with
+    (``nl._broadband_sources``); passing ``sources=None`` or ``nl.sources``
+    itself filters that copy, so a band loop never filters traces that an
+    earlier band already filtered."""
     from .wavelet import band_limit
-    src = np.asarray(_nd(sources), dtype=np.float32)
+    if not hasattr(nl, "_broadband_sources"):
+        nl._broadband_sources = np.array(_nd(nl.sources), dtype=np.float32, copy=True)
+    if sources is None or sources is nl.sources:
+        src = nl._broadband_sources
+    else:
+        src = np.asarray(_nd(sources), dtype=np.float32)
     src_b = band_limit(src, dts, *band, axis=-1).astype(np.float32)
     d_b = band_limit(np.asarray(_nd(d_obs), dtype=np.float32), dts, *band, axis=-1).astype(np.float32)
     nl.sources = np.ascontiguousarray(src_b)

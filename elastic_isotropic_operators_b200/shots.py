@@ -15,7 +15,8 @@ gloo on CPU).  Shots are independent, so the forward needs no exchange at all;
 """
 import numpy as np
 
-__all__ = ["shot_partition", "local_vectors", "stack_model", "gather_data", "sum_in_rank_order", "ShotParallel"]
+__all__ = ["shot_partition", "local_vectors", "stack_model", "gather_data", "sum_in_rank_order", "all_ranks_ok",
+           "ShotParallel"]
 
 
 def shot_partition(nExp, world, rank):
@@ -102,6 +103,19 @@ def sum_in_rank_order(value, group=None):
     return total
 
 
+def all_ranks_ok(ok, group=None):
+    """True on every rank when ``ok`` holds on every rank of ``group``: one
+    all-reduce (MIN) of a flag, so that the ranks agree on an error before any
+    of them enters a collective that a failed rank would never join."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_initialized() or dist.get_world_size(group) == 1:
+        return bool(ok)
+    t = torch.tensor([1 if ok else 0], dtype=torch.int32, device=_group_device(group))
+    dist.all_reduce(t, op=dist.ReduceOp.MIN, group=group)
+    return bool(t.item())
+
+
 class ShotParallel:
     """An operator over nExp shots split across the ranks of a process group.
 
@@ -133,14 +147,34 @@ class ShotParallel:
         operator (a BornElasticShotsGpu) runs the fused gradient of its block
         (``sources`` and ``dObs`` are this rank's entries), the gradients are
         summed over the ranks (stack_model) and the misfits added in rank order.
-        ``shape``: the gradient's shape, needed on a rank without shots."""
-        if self.local is not None:
-            phi, g = self.local.fwiGradient(model, sources, dObs, components)
-            g = np.ascontiguousarray(g, np.float32)
-        else:
-            if shape is None:
-                raise ValueError("a rank without shots needs the gradient shape")
-            phi, g = 0.0, np.zeros(shape, np.float32)
+
+        ``shape``: the gradient's shape; by default the shape of ``model``
+        (the gradient lives in the elastic model's space).  Every rank resolves
+        it and runs its own block before any collective; the ranks then agree
+        on success (all_ranks_ok), so an error on one rank -- a missing shape on
+        a rank without shots, a failed propagation -- raises on every rank
+        instead of leaving the others waiting in the sum."""
+        err = None
+        phi, g = 0.0, None
+        try:
+            if shape is None and model is not None:
+                m = model.getNdArray() if hasattr(model, "getNdArray") else model
+                shape = np.shape(m)
+            if self.local is not None:
+                phi, g = self.local.fwiGradient(model, sources, dObs, components)
+                g = np.ascontiguousarray(g, np.float32)
+                if shape is not None and g.shape != tuple(shape):
+                    raise ValueError("local gradient shape %s, expected %s" % (g.shape, tuple(shape)))
+            elif shape is None:
+                raise ValueError("a rank without shots needs the gradient shape (give model or shape)")
+            else:
+                g = np.zeros(shape, np.float32)
+        except Exception as ex:   # re-raised below, after every rank knows
+            err = ex
+        if not all_ranks_ok(err is None, self.group):
+            if err is not None:
+                raise err
+            raise RuntimeError("fwiGradient failed on another rank of the group")
         stack_model(g, self.group)
         return sum_in_rank_order(phi, self.group), g
 

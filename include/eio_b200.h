@@ -43,6 +43,9 @@ extern "C" {
 #define EIO_ERR_BOUNDS -4  /* acquisition device outside the usable grid */
 #define EIO_ERR_UNSUPPORTED -5
 #define EIO_ERR_NOMEM -6
+#define EIO_ERR_TIMEOUT -7 /* a bounded device wait gave up: that call's output is incomplete; the kernel
+                              drained its copies before returning, so the context stays usable (the
+                              reference exits the process on any CUDA error, F/src/cudaErrors.cu:4-29) */
 
 typedef struct eio_sinterp eio_sinterp;
 typedef struct eio_ctx eio_ctx;
@@ -150,6 +153,16 @@ void *eio_ctx_stream(eio_ctx *c);
 int eio_ctx_set_kernel(eio_ctx *c, int kind, int tz, int cw, int cpr);
 int eio_ctx_get_kernel(const eio_ctx *c, int *kind, int *tz, int *cw, int *cpr);
 int eio_ctx_autotune(eio_ctx *c, int *kind, int *tz, int *cw, int *cpr);
+/* Bound of the TMA-pipeline waits of the sweep (kind 1) and tile (kind 2)
+ * kernels, in mbarrier try_wait polls (no reference counterpart: the
+ * reference's kernels have no device-side waits).  A wait that runs out sets
+ * the context's error flag; the CTA then waits for its copies still in flight
+ * (with a fixed long bound that this setting does not shorten) and returns,
+ * and the call fails with EIO_ERR_TIMEOUT.  polls < 0 restores the default
+ * (2^20); 0 makes every pipeline wait give up at once (used by the tests of
+ * the timeout path). */
+int eio_ctx_set_wait_limit(eio_ctx *c, long long polls);
+int eio_ctx_get_wait_limit(const eio_ctx *c, long long *polls);
 /* Instrumentation (no reference counterpart): kernel launch counters and,
  * when enabled, CUDA-event timing of every 16th fused step-kernel launch;
  * stepMs is the sampled mean duration times stepLaunches.
@@ -352,8 +365,10 @@ int eio_nl_prepare_sources(eio_ctx *c, const float *model, eio_sinterp *const sr
  *   nz*nx <= 262144 cells, nz, nx <= 16384, source + receiver traces <=
  *   4194304 floats (sum over the 5 fields of points x nts), <= 65536 points
  *   per list.
- * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * Set-up: the first call on a device (and the first after a
+ * cudaDeviceReset) looks up the array's device address with
+ * cudaGetSymbolAddress; make that first call on each device before any
+ * stream capture begins there.
  * Every call reuses the same array and clears what must start at zero;
  * calls that overlap on the GPU (other threads or streams) race on it and
  * must be serialised by the caller. */
@@ -381,9 +396,17 @@ int eio_cnn_conv3x3(int n, int h, int w, int cin, int cout, const void *x, const
 int eio_cnn_set_conv_path(int path);
 int eio_cnn_get_conv_path(int *path);
 /* *err = 1 when a tcgen05 kernel gave up waiting for its accumulator (the
- * output of that call is incomplete); reset != 0 clears the flag.  Synchronises
- * the device. */
+ * output of that call is incomplete), 2 when its drain also ran out; reset !=
+ * 0 clears the flag.  Synchronises the device. */
 int eio_cnn_status(int reset, int *err);
+/* Bound of the tcgen05 convolution's accumulator waits, in try_wait polls
+ * (process-wide; < 0 restores the default 2^22; 0 makes the first wait of
+ * every CTA give up).  After a timeout the CTA waits, with a fixed long
+ * bound, for its MMAs and copies still in flight before it frees its tensor
+ * memory and returns; eio_cnn_status then reports 1 (2 if even that drain
+ * ran out). */
+int eio_cnn_set_wait_limit(long long polls);
+int eio_cnn_get_wait_limit(long long *polls);
 /* floats of scratch the weight gradient needs for this shape */
 int eio_cnn_wgrad_scratch(int n, int h, int w, int cin, int cout, long long *floats);
 /* dw[tap][co][ci] = sum_p dy[p][co] x[p + (dy-1, dx-1)][ci] (FP32, overwritten;

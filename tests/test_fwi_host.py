@@ -180,3 +180,35 @@ def test_band_objective_filters_sources_and_data_for_both_operators():
     f = np.fft.rfftfreq(nts, dts)
     assert spec[..., f > 26].max() < 1e-4 * spec.max()
     assert obj.fused
+
+
+def test_band_objective_never_filters_twice():
+    """A band loop that passes ``nl.sources`` (or None) each time filters the
+    broadband traces the operator was built with, not the previous band's."""
+    from elastic_isotropic_operators_b200 import wavelet
+
+    class NL:
+        sources = None
+
+    class Born:
+        fd = type("fd", (), {"surfaceCondition": 0})()
+
+        def setSourceSignals(self, s):
+            self.sigs = [np.array(x) for x in s]
+
+        def fwiGradient(self, *a):
+            raise AssertionError("not called here")
+
+    rng = np.random.default_rng(1)
+    dts, nts = 1e-3, 256
+    broadband = rng.standard_normal((1, 5, 1, nts)).astype(np.float32)
+    d_obs = rng.standard_normal((1, 5, 3, nts)).astype(np.float32)
+    nl, born = NL(), Born()
+    nl.sources = broadband.copy()
+    b1, b2 = (2.0, 4.0, 10.0, 14.0), (2.0, 4.0, 30.0, 36.0)
+    fwi.band_objective(nl, born, d_obs, nl.sources, dts, b1)
+    fwi.band_objective(nl, born, d_obs, nl.sources, dts, b2)
+    assert np.allclose(nl.sources, wavelet.band_limit(broadband, dts, *b2), atol=1e-6)
+    fwi.band_objective(nl, born, d_obs, None, dts, b1)
+    assert np.allclose(nl.sources, wavelet.band_limit(broadband, dts, *b1), atol=1e-6)
+    assert np.array_equal(nl._broadband_sources, broadband)

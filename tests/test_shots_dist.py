@@ -155,3 +155,72 @@ def test_shot_parallel_fwi_gradient_sums_over_ranks(tmp_path, world):
         assert abs(float(r["phi"]) - 0.1 * want) < 1e-12
         assert np.array_equal(r["g"], np.full((3, 4, 6), float(want), np.float32))
     assert all(float(r["phi"]) == float(res[0]["phi"]) for r in res)
+
+
+def _rank_fwi_no_shape(rank, world, port, out_dir):
+    import datetime
+    import time
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        # one shot, three ranks: ranks 1 and 2 own none, and neither a model nor a shape is given
+        op = ShotParallel(lambda shots: _FakeGradient(shots, (3, 4, 6)), 1)
+        d_obs = np.zeros((len(op.shots), 2, 3, 7), np.float32)
+        t0 = time.monotonic()
+        try:
+            op.fwiGradient(None, None, d_obs)
+            outcome = "returned"
+        except ValueError as ex:
+            outcome = "ValueError: %s" % ex
+        except RuntimeError as ex:
+            outcome = "RuntimeError: %s" % ex
+        np.savez(os.path.join(out_dir, "nf%d.npz" % rank), outcome=outcome, dt=time.monotonic() - t0)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_shot_parallel_fwi_gradient_fails_fast_on_every_rank(tmp_path):
+    """A rank without shots and without a shape cannot form its part of the
+    sum: every rank must raise (the owner of the shot included), well before
+    the process group's timeout, instead of the owner waiting in the
+    all-reduce."""
+    import torch.multiprocessing as mp
+    world = 3
+    mp.start_processes(_rank_fwi_no_shape, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    res = [np.load(tmp_path / ("nf%d.npz" % r)) for r in range(world)]
+    assert str(res[0]["outcome"]).startswith("RuntimeError"), str(res[0]["outcome"])
+    for r in res[1:]:
+        assert str(r["outcome"]).startswith("ValueError"), str(r["outcome"])
+    assert all(float(r["dt"]) < 30.0 for r in res)
+
+
+def _rank_fwi_model_shape(rank, world, port, out_dir):
+    import datetime
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        shape = (3, 4, 6)
+        op = ShotParallel(lambda shots: _FakeGradient(shots, shape), 1)
+        d_obs = np.zeros((len(op.shots), 2, 3, 7), np.float32)
+        phi, g = op.fwiGradient(np.zeros(shape, np.float32), None, d_obs)
+        np.savez(os.path.join(out_dir, "ms%d.npz" % rank), phi=phi, g=g)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_shot_parallel_fwi_gradient_shape_from_model(tmp_path):
+    """Without ``shape`` the gradient takes the model's shape on every rank,
+    so ranks without shots still join the sum."""
+    import torch.multiprocessing as mp
+    world = 3
+    mp.start_processes(_rank_fwi_model_shape, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    for r in range(world):
+        res = np.load(tmp_path / ("ms%d.npz" % r))
+        assert abs(float(res["phi"]) - 0.1) < 1e-12
+        assert np.array_equal(res["g"], np.ones((3, 4, 6), np.float32))
