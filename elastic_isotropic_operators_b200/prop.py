@@ -65,6 +65,8 @@ class spaceInterpGpu:
         self._L = L
         self.nt = int(nt)
         self.gridHyper = gridHyper
+        self.zCoord, self.xCoord = z.copy(), x.copy()   # the irregular device coordinates
+        self.method, self.nFilt = method, int(nFilt)
         ni, nr, nf = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         check(L.eio_sinterp_sizes(h, ctypes.byref(ni), ctypes.byref(nr), ctypes.byref(nf)))
         self.nDeviceIrreg, self.nDeviceReg, self.nFiltTotal = ni.value, nr.value, nf.value
@@ -625,6 +627,20 @@ def _four_grids(zc, xc, hypers, nts, method, nfilt, dipole, zds, xds):
     return [spaceInterpGpu(zc, xc, h, nts, method, nfilt, dipole, zds, xds) for h in hypers]
 
 
+def _geometry_array(geom):
+    """A geometry file's coordinates [3][nPoints][nExp] (numpy order; x, y, z
+    along the slowest axis): a SEP dataset read with ndims = 3, as the
+    reference reads it (genericIO.defaultIO.getVector(file, ndims=3),
+    python_float/Elastic_iso_float_prop.py:269-270), a ``.npy`` array, or an
+    array given directly."""
+    if isinstance(geom, str):
+        if geom.endswith(".npy"):
+            return np.load(geom)
+        from .sepio import readSep
+        return np.asarray(readSep(geom, ndims=3).getNdArray())
+    return np.asarray(geom)
+
+
 def buildSourceGeometry(parObject, elasticParam):
     """Sources on the four staggered grids, one set per shot.
     Returns (center, x, z, xz) lists and the shot axis."""
@@ -645,7 +661,7 @@ def buildSourceGeometry(parObject, elasticParam):
     geom = parObject.getString("sourceGeomFile", "None")
     if geom != "None":
         # numpy array [3][nSimSou][nExp] (x, y, z coordinates), as read from the geometry file
-        g = np.load(geom) if isinstance(geom, str) else np.asarray(geom)
+        g = _geometry_array(geom)
         if g.shape[2] != nExp:
             raise ValueError("ERROR! nExp (%d) not consistent with number of shots provided within "
                              "sourceGeomFile (%d)" % (nExp, g.shape[2]))
@@ -686,7 +702,7 @@ def buildReceiversGeometry(parObject, elasticParam):
     nfilt = parObject.getInt("recInterpNumFilters", 4)
     geom = parObject.getString("recGeomFile", "none")
     if geom != "none":
-        g = np.load(geom) if isinstance(geom, str) else np.asarray(geom)
+        g = _geometry_array(geom)
         xc = np.ascontiguousarray(g[0, :, 0], dtype=np.float32)
         zc = np.ascontiguousarray(g[2, :, 0], dtype=np.float32)
         nRec = parObject.getInt("nReceiver")

@@ -5,7 +5,7 @@ vectors, ``SEP::hypercube`` and ``paramObj`` (genericIO / sepVector, not
 vendored with the reference).  These classes provide the part of that API the
 operator path uses: axes with (n, o, d), numpy-backed storage whose numpy
 shape is the axis list reversed (axis 1 fastest), ``getNdArray``,
-``getHyper``, ``clone``, ``scale``, ``dot``, ``rand``/``random``, and a
+``getHyper``, ``clone``, ``scale``, ``dot``, ``rand``/``random``, ``writeVec``, and a
 ``paramObj`` with ``getInt``/``getFloat``/``getString``/``getInts`` over a
 par-file or a dict.
 """
@@ -112,6 +112,11 @@ class floatVector:
 
     def checkSame(self, other):
         return self.hyper.checkSame(other.hyper)
+
+    def writeVec(self, filename, data_format="xdr_float"):
+        """Write the vector as a SEP dataset (``filename`` header + ``filename@`` binary)."""
+        from .sepio import writeSep
+        writeSep(filename, self, data_format)
 
 
 class doubleVector(floatVector):

@@ -165,7 +165,11 @@ def nl_312x520(nts=2000, nshots=1):
                     nshots)
 
 
-def born_600x1800(nts=4000, nshots=10, seed=2024):
+def born_600x1800(nts=4000, nshots=10, seed=2024, select=None):
+    """Born benchmark case: 600x1800 grid (50-cell pads), vp gradient
+    1800-4000 m/s, vs = vp/1.8, Gardner density, seeded smoothed 5 % RMS
+    perturbations of rho, lambda, mu, nshots 12 Hz Ricker shots spread over the
+    line, 900 receivers centred on it.  select: indices of the shots to keep."""
     nz, nx, dz = 600, 1800, 10.0
     pad = 50
     nzi, nxi = nz - 2 * FAT - 2 * pad, nx - 2 * FAT - 2 * pad
@@ -186,6 +190,9 @@ def born_600x1800(nts=4000, nshots=10, seed=2024):
     ox = -(FAT + pad) * dz
     z0 = _grid_coord(oz, dz, FAT + pad + 2)
     xs = np.linspace(FAT + pad + 20, FAT + pad + nxi - 21, nshots).round().astype(int)
+    if select is not None:
+        xs = xs[list(select)]
+        nshots = len(xs)
     src_x = [_grid_coord(ox, dz, i) for i in xs]
     first = FAT + pad + (nxi - 900) // 2
     rec_x = np.array([_grid_coord(ox, dz, first + i) for i in range(900)], np.float32)

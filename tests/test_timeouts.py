@@ -18,7 +18,7 @@ import numpy as np
 import pytest
 
 from elastic_isotropic_operators_b200 import _lib, prop, synthetic
-from tests.helpers import Ctx, reg_inputs
+from helpers import Ctx, reg_inputs
 
 pytestmark = pytest.mark.gpu
 
