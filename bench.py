@@ -44,8 +44,9 @@ def parse():
     ap.add_argument("--workload", default="born_600x1800",
                     choices=["born_600x1800", "nl_312x520", "nl_shots", "fwi_1000x3400", "fwi_learned",
                              "cnn_train"])
-    ap.add_argument("--batch", type=int, default=8,
-                    help="nl_shots: shots per lockstep launch (1 = one shot at a time on the lanes)")
+    ap.add_argument("--batch", type=int, default=None,
+                    help="shots per lockstep launch (1 = one shot at a time on the lanes); nl_shots default 8, "
+                         "born_600x1800 default: the library's (as wide as the lanes and memory allow)")
     ap.add_argument("--pairs", type=int, default=48, help="fwi_learned: Born training pairs")
     ap.add_argument("--conv-path", type=int, default=-1, choices=[-1, 0, 1],
                     help="cnn_train: forward convolutions on mma.sync (0) or tcgen05 (1); "
@@ -192,21 +193,28 @@ def lanes_used(L, ctx):
 
 def read_stats(L, ctx):
     """Step-kernel counters of the timed region (and reset them): the dominant
-    kernel's mean launch time and its algorithmic bytes per launch.  With the
-    two-step kernel the dominant launches are the two-step ones (100 B per cell
-    for two updates); otherwise the single steps (80 B per cell)."""
+    kernel's mean launch time, how many cell updates one of its launches
+    makes (several shots per launch with shot batching) and its algorithmic
+    bytes per cell update.  With the two-step kernel the dominant launches are
+    the two-step ones (100 B per cell for two updates); otherwise the single
+    steps (80 B per cell)."""
     import ctypes
     pl, pms = ctypes.c_longlong(), ctypes.c_double()
     L.eio_ctx_pair_stats(ctx, ctypes.byref(pl), ctypes.byref(pms))
+    cells = ctypes.c_longlong()
+    L.eio_ctx_step_cells(ctx, ctypes.byref(cells))
     launches, sl, sms = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_double()
     L.eio_ctx_stats(ctx, 0, 1, ctypes.byref(launches), ctypes.byref(sl), ctypes.byref(sms))
     singles, single_ms = sl.value - pl.value, sms.value - pms.value
+    cells_per_launch = cells.value / max(singles, 1)
     if pl.value > 0 and pms.value >= single_ms:
         avg, bpc, n = pms.value / pl.value, PAIR_BYTES_PER_CELL, pl.value
+        cells_per_launch = None
     else:
         avg, bpc, n = single_ms / max(singles, 1), BYTES_PER_CELL, singles
     return {"launches": int(launches.value), "avg_ms": avg, "bytes_per_cell": bpc, "dominant_launches": int(n),
-            "step_launches": int(sl.value), "pair_launches": int(pl.value)}
+            "step_launches": int(sl.value), "pair_launches": int(pl.value), "step_cells": int(cells.value),
+            "cells_per_launch": cells_per_launch}
 
 
 def dist_init(args):
@@ -253,6 +261,8 @@ def run_ours(args, ws, rank, local):
     L = _lib.lib()
     ctx = born.ctx
     pin_kernel(L, ctx, args)
+    if args.batch is not None:
+        _lib.check(L.eio_ctx_set_shot_batch(ctx, args.batch))
     est = torch.cuda.ExternalStream(L.eio_ctx_stream(ctx), device=dev)   # the engine's launch stream
     nsh = w.nExp
     fine_steps, cells = ctypes.c_longlong(), ctypes.c_longlong()
@@ -335,9 +345,13 @@ def run_ours(args, ws, rank, local):
     # roofline of the dominant kernel (fused step, or two fused steps per launch)
     avg_launch_ms = st["avg_ms"]
     lanes = lanes_used(L, ctx)
-    if lanes == 1:
-        achieved = st["bytes_per_cell"] * cells / (avg_launch_ms * 1e-3) / 1e9
-        basis = "algorithmic bytes per launch / mean CUDA-event duration of the step launches (engine stream)"
+    cpl = st["cells_per_launch"] or cells
+    batched = cpl > 1.01 * cells             # launches that advance several shots (one stream)
+    bytes_per_launch = st["bytes_per_cell"] * cpl
+    if lanes == 1 or batched:
+        achieved = bytes_per_launch / (avg_launch_ms * 1e-3) / 1e9
+        basis = ("algorithmic bytes per launch (%.2f shots x 80 B x interior cells) / mean CUDA-event duration of "
+                 "the step launches (engine stream)" % (cpl / cells))
     else:
         # the lanes' step kernels overlap, so a launch's event time includes the other lanes' work:
         # the step launches' algorithmic bytes over the timed region instead
@@ -349,7 +363,8 @@ def run_ours(args, ws, rank, local):
             "frac": round(achieved / peak, 4), "traffic": profile_traffic(st["bytes_per_cell"]),
             "peak_source": peak_kind, "kernel": kernel_name(L, ctx), "basis": basis,
             "avg_launch_us": round(avg_launch_ms * 1e3, 3),
-            "algorithmic_bytes_per_launch": st["bytes_per_cell"] * cells,
+            "algorithmic_bytes_per_launch": bytes_per_launch,
+            "shots_per_launch": round(cpl / cells, 3),
             "launches": {"step_kernel": st["step_launches"], "two_step": st["pair_launches"]},
             # whole job: every cell update of the timed region at 80 B (step kernels, imaging,
             # sparse work and launch gaps included)
@@ -1004,6 +1019,8 @@ def run_ours_nl_shots(args, ws, rank, local):
     import torch
     from elastic_isotropic_operators_b200 import _lib, prop, synthetic
     nsh = args.shots or 8
+    if args.batch is None:
+        args.batch = 8
     w = synthetic.nl_312x520(nshots=nsh)
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)

@@ -78,6 +78,7 @@ _SIGS = {
     "eio_ctx_get_kernel": (I, [P, IP, IP, IP, IP]),
     "eio_ctx_autotune": (I, [P, IP, IP, IP, IP]),
     "eio_ctx_set_wait_limit": (I, [P, ctypes.c_longlong]),
+    "eio_ctx_step_cells": (I, [P, ctypes.POINTER(ctypes.c_longlong)]),
     "eio_ctx_get_wait_limit": (I, [P, ctypes.POINTER(ctypes.c_longlong)]),
     "eio_ctx_stats": (I, [P, I, I, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
                           ctypes.POINTER(ctypes.c_double)]),

@@ -136,6 +136,7 @@ struct Engine {
     long long wait_limit = WAIT_LIMIT;
     // launch statistics (bench instrumentation)
     long long launches = 0, step_launches = 0, sampled = 0;
+    long long step_cells = 0;   // cell updates of the single-step launches (a batch launch: all its shots)
     double step_ms = 0.0;
     long long pair_launches = 0, pair_sampled = 0;   // two-step launches (also counted in step_launches)
     double pair_ms = 0.0;
@@ -372,10 +373,13 @@ void engine_stats(Engine* e, int enable, int reset, long long* launches, long lo
     if (pair_ms) *pair_ms = pair;
     if (reset) {
         e->launches = 0; e->step_launches = 0; e->sampled = 0; e->step_ms = 0.0;
-        e->pair_launches = 0; e->pair_sampled = 0; e->pair_ms = 0.0;
+        e->pair_launches = 0; e->pair_sampled = 0; e->pair_ms = 0.0; e->step_cells = 0;
     }
     if (enable >= 0) e->stats = enable != 0;
 }
+long long engine_step_cells(const Engine* e) { return e->step_cells; }
+// the Born operators ignore the free surface (like the reference's Born drivers)
+bool engine_batchable(const Engine* e) { return e->S == 2 && e->ckpt == 0; }
 
 // every kind but the sweep (1) uses the 64x16 tiles of k_step and their numbering
 static bool tiled(int kind) { return kind != 1; }
@@ -686,6 +690,7 @@ static void launch_step(Engine* e, StepArgs& a, int cur) {
     }
     e->launches++;
     e->step_launches++;
+    e->step_cells += (long long)(e->nz - 2 * FAT) * (e->nx - 2 * FAT);
 }
 
 // two fine steps in one launch (kind 5); the dynamic shared memory of each
@@ -1890,11 +1895,58 @@ double engine_fwi_shot(Engine* e, float* const modelReg[5], const ShotGeom& g, c
     return phi;
 }
 
+// ---------------------------------------------------------------- Born shots in lockstep
+// The Born operators and the fused FWI gradient for nb shots at once, one
+// engine per shot (own wavefields, history, secondary-source ring, point
+// lists, window), every fine step one k_step_shots launch for all of them
+// (CTA b: tile b / nb of shot b % nb).  All shots read the first engine's
+// medium arrays (every engine of a context holds the same medium), so the
+// shots' CTAs of one tile read a medium tile from HBM once.  The phases, time
+// weights and epilogues are those of born_source and engine_born (FP32
+// history, two fine steps per coarse sample), so every shot's traces and
+// image equal its one-shot propagation with the tile kernel (k_step, 4 CTAs
+// per SM; 3 for the fused adjoint imaging step) bit for bit.  Launches go to
+// the first engine's streams (imaging on its second stream); that stream
+// waits for every engine's preparation and every engine waits for it before
+// reading results back.
+
+// the batch launch of one fine step; grid = nb x the largest shot's tile count
+template <int DIR, int EPI, int MINB>
+static void launch_shots(Engine* e0, const StepBatch& b, int nb, int max_tiles) {
+    const bool timed = e0->stats && (e0->step_launches + e0->pair_launches) % STATS_PERIOD == 0;
+    if (timed) stats_mark(e0);
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3((unsigned)(nb * max_tiles));
+    cfg.blockDim = dim3(NT);
+    cfg.stream = e0->st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    EIO_CUDA(cudaLaunchKernelEx(&cfg, k_step_shots<DIR, EPI, MINB>, b, nb));
+    if (timed) {
+        stats_mark(e0);
+        e0->sampled++;
+    }
+    e0->launches++;
+    e0->step_launches++;
+}
+
+// a batch launch updates the interior cells of every shot once
+static void batch_count(Engine* e0, Engine* const* es, int nb, long long launches) {
+    long long cells = 0;
+    for (int i = 0; i < nb; i++) cells += (long long)(es[i]->nz - 2 * FAT) * (es[i]->nx - 2 * FAT);
+    e0->step_cells += cells * launches;
+}
+
 // Nonlinear forward (adj = 0) or adjoint (adj = 1) of nb shots, one engine
 // each (own wavefields, point lists, windows), advanced in lockstep: one
-// k_step_batch launch per fine step covers the tiles of every shot
-// (blockIdx.y = shot), so small grids fill the GPU and the per-step launch
-// cost is paid once for all of them.  The steps, time weights and arithmetic
+// k_step_shots launch per fine step covers the tiles of every shot (the
+// shots of a tile next to each other, reading one copy of the medium), so
+// small grids fill the GPU and the per-step launch cost is paid once for all
+// of them.  The steps, time weights and arithmetic
 // are those of engine_nl (same stencil body), so each shot's result equals its
 // single-shot propagation with the tile kernel bit for bit.  No free surface,
 // no wavefield output; the launches go to the first engine's stream, which
@@ -1933,6 +1985,9 @@ void engine_nl_shots_batch(Engine* const* es, int nb, int adj, float* const* mod
         build_points(e, g[i].recPos, g[i].nRec, recp[i]);
         StepArgs& a = b.a[i];
         a = base_args(e);
+        // every engine of a context holds the same medium: all shots read the first
+        // engine's, so the shots' CTAs of one tile share it through L2
+        for (int f = 0; f < 5; f++) a.par[f] = e0->par[f].f() + (long long)e->win_ix0 * e->nz;
         zero_wavefields(e);
         lv.emplace_back(e);
         if (!adj) {
@@ -1954,25 +2009,16 @@ void engine_nl_shots_batch(Engine* const* es, int nb, int adj, float* const* mod
     }
     const float* F = e0->filt.data();
     const int h = e0->h;
-    cudaLaunchConfig_t cfg;
-    memset(&cfg, 0, sizeof(cfg));
-    cfg.gridDim = dim3(max_tiles, nb);
-    cfg.blockDim = dim3(NT);
-    cfg.stream = e0->st;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
+    Engine* const* engines = es;
     auto launch = [&] {
         if (!adj) {
-            if (minb == 4) EIO_CUDA(cudaLaunchKernelEx(&cfg, k_step_batch<0, 4>, b));
-            else EIO_CUDA(cudaLaunchKernelEx(&cfg, k_step_batch<0, 3>, b));
+            if (minb == 4) launch_shots<0, EPI_NONE, 4>(e0, b, nb, max_tiles);
+            else launch_shots<0, EPI_NONE, 3>(e0, b, nb, max_tiles);
         } else {
-            if (minb == 4) EIO_CUDA(cudaLaunchKernelEx(&cfg, k_step_batch<1, 4>, b));
-            else EIO_CUDA(cudaLaunchKernelEx(&cfg, k_step_batch<1, 3>, b));
+            if (minb == 4) launch_shots<1, EPI_NONE, 4>(e0, b, nb, max_tiles);
+            else launch_shots<1, EPI_NONE, 3>(e0, b, nb, max_tiles);
         }
-        e0->step_launches++;
+        batch_count(e0, engines, nb, 1);
     };
     // the fine steps in propagation order, with the time weights of engine_nl
     auto step = [&](int its, int it2) {
@@ -2015,6 +2061,291 @@ void engine_nl_shots_batch(Engine* const* es, int nb, int adj, float* const* mod
         EIO_CUDA(cudaStreamSynchronize(es[i]->st));
         err_check(es[i]);
     }
+}
+
+// ---------------------------------------------------------------- Born shots in lockstep (phases)
+struct ShotBatch {
+    Engine* const* es;
+    int nb;
+    int max_tiles = 0;
+    StepBatch b;
+    std::vector<Levels> lv;
+    ShotBatch(Engine* const* engines, int n) : es(engines), nb(n) {
+        if (nb < 1 || nb > STEP_BATCH) throw Error(EIO_ERR_ARG, "batch of 1 .. 8 shots");
+        memset(&b, 0, sizeof(b));
+        Engine* e0 = es[0];
+        for (int i = 0; i < nb; i++) {
+            Engine* e = es[i];
+            if (e->device != e0->device || e->nts != e0->nts || e->S != e0->S || e->nz != e0->nz)
+                throw Error(EIO_ERR_ARG, "batched shots need engines of one device and one time axis");
+            if (e->S != 2 || e->ckpt)
+                throw Error(EIO_ERR_UNSUPPORTED, "batched Born shots need sub = 1 and an FP32 history");
+            max_tiles = std::max(max_tiles, e->ntiles);
+        }
+    }
+    Engine* e0() const { return es[0]; }
+    // base arguments of every shot, reading the first engine's medium at its own window
+    void base() {
+        Engine* e0 = es[0];
+        for (int i = 0; i < nb; i++) {
+            Engine* e = es[i];
+            b.a[i] = base_args(e);
+            const long long off = (long long)e->win_ix0 * e->nz;
+            for (int f = 0; f < 5; f++) b.a[i].par[f] = e0->par[f].f() + off;
+        }
+    }
+    void levels() {
+        lv.clear();
+        for (int i = 0; i < nb; i++) {
+            zero_wavefields(es[i]);
+            lv.emplace_back(es[i]);
+        }
+    }
+    // the first engine's stream waits for the work queued on the others, and back
+    void join_in() {
+        for (int i = 1; i < nb; i++) {
+            EIO_CUDA(cudaEventRecord(es[i]->ev_sync, es[i]->st));
+            EIO_CUDA(cudaStreamWaitEvent(es[0]->st, es[i]->ev_sync, 0));
+        }
+    }
+    void join_out() {
+        EIO_CUDA(cudaEventRecord(es[0]->ev_sync, es[0]->st));
+        for (int i = 1; i < nb; i++) EIO_CUDA(cudaStreamWaitEvent(es[i]->st, es[0]->ev_sync, 0));
+    }
+    template <int DIR, int EPI, int MINB>
+    void step() {
+        launch_shots<DIR, EPI, MINB>(es[0], b, nb, max_tiles);
+        batch_count(es[0], es, nb, 1);
+        for (int i = 0; i < nb; i++) lv[i].single();
+    }
+};
+
+// Phase 1 of every shot: the source wavefield and its coarse Vx/Vz history
+// (born_source with two fine steps per sample).  src: per-shot source lists
+// (fine-time Born sources, or the nonlinear operators' coarse traces when ext
+// holds the receiver lists of a nonlinear forward that also records).
+static void batch_source(ShotBatch& B, std::vector<PointList>& src, const SparseOp* ext) {
+    Engine* e0 = B.e0();
+    for (int i = 0; i < B.nb; i++) {
+        Engine* e = B.es[i];
+        const size_t wbytes = sizeof(float) * 2 * (size_t)e->nts * e->n;
+        const bool fresh = e->W.cap < wbytes;
+        e->W.ensure(wbytes);
+        if (fresh || !e->w_clean || e->w_n != e->n) EIO_CUDA(cudaMemsetAsync(e->W.p, 0, wbytes, e->st));
+        e->w_clean = true;
+        e->w_n = e->n;
+        StepArgs& a = B.b.a[i];
+        a.inj = upload_points(e, src[i], e->inj_ts, e->inj_ent, e->sig_in);
+        if (ext) a.ext = ext[i];
+        else memset(&a.ext, 0, sizeof(a.ext));
+        a.W0 = e->W.f();
+        a.W1 = e->W.f() + (long long)e->nts * e->n;
+    }
+    B.levels();
+    B.join_in();
+    const SrcWeights weights{e0, ext != nullptr};
+    const float* F = e0->filt.data();
+    const int h = e0->h;
+    for (int its = 0; its < e0->nts - 1; its++)
+        for (int it2 = 1; it2 < 3; it2++) {
+            const bool last = (its == e0->nts - 2 && it2 == 2);
+            for (int i = 0; i < B.nb; i++) {
+                StepArgs& a = B.b.a[i];
+                B.lv[i].set(a);
+                weights(a, its, it2);
+                if (it2 == 1) {          // row its = o*f[h+1] + c*f[h+2] + n*f[1]
+                    a.tmode = 1; a.wt = its; a.tw_o = F[h + 1]; a.tw_c = F[h + 2]; a.tw_n = F[1];
+                } else if (last) {       // row nts-1 = c*f[h+1] + n*f[h+2]
+                    a.tmode = 2; a.wt = its + 1; a.tw_o = 0.f; a.tw_c = F[h + 1]; a.tw_n = F[h + 2];
+                }
+            }
+            if (it2 == 1 || last) B.step<0, EPI_TRI, 4>();
+            else B.step<0, EPI_NONE, 4>();
+        }
+    check_launch();
+    B.join_out();   // phase 2 prepares on the engines' own streams
+}
+
+// Phase 2 of the Born forward for every shot: the scattered wavefield with the
+// secondary sources of the perturbation dm[i] (per shot, windowed views);
+// imaging kernels on the first engine's imaging stream fill each shot's ring
+// up to R-1 coarse samples ahead; rec: receiver lists (extraction).
+static void batch_scatter(ShotBatch& B, std::vector<PointList>& rec, float* const* dm) {
+    Engine* e0 = B.e0();
+    constexpr int R = 4;
+    ImagingBatch ib;
+    memset(&ib, 0, sizeof(ib));
+    int img_tiles = 0;
+    for (int i = 0; i < B.nb; i++) {
+        Engine* e = B.es[i];
+        for (int k = 0; k < R; k++)
+            for (int f = 0; f < 5; f++) e->ss[k * 5 + f].ensure(sizeof(float) * e->n);
+        for (int f = 0; f < 10; f++) EIO_CUDA(cudaMemsetAsync(e->ss[f].p, 0, sizeof(float) * e->n, e->st));
+        zero_out(e, rec[i].ld, e->nts, e->sig_out);
+        StepArgs& a = B.b.a[i];
+        memset(&a.inj, 0, sizeof(a.inj));
+        a.ext = upload_points(e, rec[i], e->ext_ts, e->ext_ent, e->sig_out);
+        ImagingArgs& ia = ib.a[i];
+        ia.h = whist(e);
+        ia.nz = e->nz; ia.nx = e->nx;
+        for (int q = 0; q < 4; q++) { ia.cz[q] = e->zc[q]; ia.cx[q] = e->xc[q]; }
+        ia.dts_inv = e->dts_inv;
+        for (int f = 0; f < 5; f++) ia.dm[f] = dm[5 * i + f];
+        img_tiles = std::max(img_tiles, ((e->nz - 2 * FAT + TZ - 1) / TZ) * ((e->nx - 2 * FAT) / TX));
+    }
+    B.levels();
+    B.join_in();
+    EIO_CUDA(cudaEventRecord(e0->ev_sync, e0->st));
+    EIO_CUDA(cudaStreamWaitEvent(e0->st2, e0->ev_sync, 0));
+    for (int k = 0; k < R; k++) {
+        EIO_CUDA(cudaEventRecord(e0->ev_free[k], e0->st2));
+        EIO_CUDA(cudaEventRecord(e0->ev_ready[k], e0->st2));
+    }
+    auto image = [&](int k) {
+        const int sl = k % R;
+        EIO_CUDA(cudaStreamWaitEvent(e0->st2, e0->ev_free[sl], 0));
+        for (int i = 0; i < B.nb; i++) {
+            ib.a[i].its = k;
+            for (int f = 0; f < 5; f++) ib.a[i].ss[f] = B.es[i]->ss[sl * 5 + f].f();
+        }
+        k_imaging_shots<0, 0><<<B.nb * img_tiles, NT, 0, e0->st2>>>(ib, B.nb);
+        e0->launches++;
+        EIO_CUDA(cudaEventRecord(e0->ev_ready[sl], e0->st2));
+    };
+    const float* F = e0->filt.data();
+    const int h = e0->h;
+    for (int k = 0; k < R - 1 && k < e0->nts; k++) image(k);
+    for (int its = 0; its < e0->nts - 1; its++) {
+        if (its + R - 1 < e0->nts) image(its + R - 1);
+        const int l = its % R, r = (its + 1) % R;
+        EIO_CUDA(cudaStreamWaitEvent(e0->st, e0->ev_ready[l], 0));
+        EIO_CUDA(cudaStreamWaitEvent(e0->st, e0->ev_ready[r], 0));
+        for (int it2 = 1; it2 < 3; it2++) {
+            for (int i = 0; i < B.nb; i++) {
+                StepArgs& a = B.b.a[i];
+                B.lv[i].set(a);
+                for (int f = 0; f < 5; f++) { a.ssL[f] = B.es[i]->ss[l * 5 + f].f(); a.ssR[f] = B.es[i]->ss[r * 5 + f].f(); }
+                a.sw0 = F[it2 - 1]; a.sw1 = F[h + it2 - 1];
+                a.ext.t0 = its; a.ext.w0 = F[it2]; a.ext.w1 = F[h + it2];
+            }
+            B.step<0, EPI_INJ_SS, 4>();
+        }
+        EIO_CUDA(cudaEventRecord(e0->ev_free[l], e0->st));
+    }
+    EIO_CUDA(cudaEventRecord(e0->ev_sync, e0->st2));
+    EIO_CUDA(cudaStreamWaitEvent(e0->st, e0->ev_sync, 0));
+    check_launch();
+}
+
+// Phase 2 of the Born adjoint for every shot: the adjoint wavefield of the
+// regular receiver traces (inj), the imaging condition fused into the
+// coarse-sample steps (EPI_TRI_IMG) against each shot's history, into the
+// per-shot images img[i] (windowed views; shots of a batch never share one).
+static void batch_adjoint(ShotBatch& B, std::vector<PointList>& rec, float* const* img) {
+    Engine* e0 = B.e0();
+    for (int i = 0; i < B.nb; i++) {
+        Engine* e = B.es[i];
+        StepArgs& a = B.b.a[i];
+        a.inj = upload_points(e, rec[i], e->inj_ts, e->inj_ent, e->sig_in);
+        memset(&a.ext, 0, sizeof(a.ext));
+        a.wh = whist(e);
+        a.dts_inv = e->dts_inv;
+        for (int f = 0; f < 5; f++) a.img[f] = img[5 * i + f];
+    }
+    B.levels();
+    B.join_in();
+    const float* F = e0->filt.data();
+    const int h = e0->h;
+    for (int its = e0->nts - 2; its > -1; its--)
+        for (int it2 = 1; it2 > -1; it2--) {
+            int T = -1;
+            for (int i = 0; i < B.nb; i++) {
+                StepArgs& a = B.b.a[i];
+                B.lv[i].set(a);
+                a.inj.t0 = its; a.inj.w0 = F[it2 + 1]; a.inj.w1 = F[h + it2 + 1];
+                if (it2 == 1) {          // sample its+1 = (p(2T+1) f[1] + p(2T) f[0]) + p(2T-1) f[h+1]
+                    T = its + 1; a.tmode = 1; a.tw_o = F[1]; a.tw_c = F[0]; a.tw_n = F[h + 1];
+                } else if (its == 0) {   // sample 0 = p(1) f[1] + p(0) f[0]
+                    T = 0; a.tmode = 2; a.tw_o = 0.f; a.tw_c = F[1]; a.tw_n = F[0];
+                }
+                a.img_its = T;
+            }
+            if (T >= 0) B.step<1, EPI_TRI_IMG, 3>();
+            else B.step<1, EPI_NONE, 4>();
+        }
+    check_launch();
+}
+
+// Born forward (adj = 0) or adjoint (adj = 1) of nb shots in lockstep, device
+// inputs and outputs.  ds: per shot 5 device arrays of fine-time regular
+// source traces (trace-major); dm: per shot 5 device pointers (forward: the
+// perturbation slices; adjoint: the shot's own image, accumulated), both
+// already offset to the shot's window; dr: per shot 5 device arrays of regular
+// receiver traces (trace-major; written by the forward, read by the adjoint).
+// Returns with the work queued on every engine's stream.
+static void born_batch_queue(Engine* const* es, int nb, int adj, float* const* ds, float* const* dm,
+                             float* const* dr, const ShotGeom* g) {
+    Engine* e0 = es[0];
+    if (!e0->tuned) engine_autotune(e0);
+    ShotBatch B(es, nb);
+    std::vector<PointList> src(nb), recp(nb);
+    for (int i = 0; i < nb; i++) {
+        Engine* e = es[i];
+        err_reset(e);
+        build_points(e, g[i].srcPos, g[i].nSrc, src[i]);
+        build_points(e, g[i].recPos, g[i].nRec, recp[i]);
+        stage_in(e, ds + 5 * i, src[i].ld, e->ntw, e->sig_in);
+    }
+    B.base();
+    batch_source(B, src, nullptr);
+    B.base();
+    if (!adj) {
+        batch_scatter(B, recp, dm);
+    } else {
+        for (int i = 0; i < nb; i++)   // on each engine's stream, after phase 1 (batch_source joined out)
+            stage_in(es[i], dr + 5 * i, recp[i].ld, es[i]->nts, es[i]->sig_in);
+        batch_adjoint(B, recp, dm);
+    }
+    B.join_out();
+    if (!adj)
+        for (int i = 0; i < nb; i++) stage_out(es[i], recp[i].ld, es[i]->nts, es[i]->sig_out, dr + 5 * i);
+}
+
+static void batch_finish(Engine* const* es, int nb) {
+    for (int i = 0; i < nb; i++) {
+        EIO_CUDA(cudaStreamSynchronize(es[i]->st));
+        stats_flush(es[i]);
+        err_check(es[i]);
+    }
+}
+
+void engine_born_batch_dev(Engine* const* es, int nb, int adj, float* const* ds, float* const* dm, float* const* dr,
+                           const ShotGeom* g) {
+    EIO_CUDA(cudaSetDevice(es[0]->device));
+    born_batch_queue(es, nb, adj, ds, dm, dr, g);
+    batch_finish(es, nb);
+}
+
+// The same with host inputs and outputs, as engine_born_shot: srcDtw per shot
+// 5 host arrays of fine-time regular source traces; rec per shot 4 receiver
+// interpolators; dataIrreg per shot host traces [5][nIrreg][nts] (written by
+// the forward, read by the adjoint).  The receivers are interpolated on the GPU.
+void engine_born_shots_batch(Engine* const* es, int nb, int adj, float* const* srcDtw, float* const* dm,
+                             const ShotGeom* g, const SInterp* const* rec, float* const* dataIrreg) {
+    EIO_CUDA(cudaSetDevice(es[0]->device));
+    std::vector<float*> ds((size_t)5 * nb), dr((size_t)5 * nb);
+    for (int i = 0; i < nb; i++) {
+        Engine* e = es[i];
+        for (int f = 0; f < 5; f++) {
+            h2d(e, e->stage_a[f], srcDtw[5 * i + f], (size_t)g[i].nSrc[kFieldGrid[f]] * e->ntw);
+            ds[5 * i + f] = e->stage_a[f].f();
+        }
+        stage_receivers(e, adj, g[i], rec + 4 * i, adj ? dataIrreg[i] : nullptr, dr.data() + 5 * i);
+    }
+    born_batch_queue(es, nb, adj, ds.data(), dm, dr.data(), g);
+    if (!adj)
+        for (int i = 0; i < nb; i++) return_receivers(es[i], rec + 4 * i, dataIrreg[i]);
+    batch_finish(es, nb);
 }
 
 // the image buffers of this lane, offset to the current shot window

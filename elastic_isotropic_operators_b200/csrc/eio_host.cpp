@@ -460,6 +460,31 @@ static void run_lanes(eio_ctx* c, int n, int nShots, F&& f) {
         if (x) std::rethrow_exception(x);
 }
 
+// Born shots in lockstep groups (engine_born_shots_batch / engine_born_batch_dev):
+// each shot of a group runs on a lane of its own (its buffers and its own
+// history), so the group is as wide as the shot batch setting, the lane count
+// and the free memory allow; 0 when the shots run on the lanes instead (a
+// single shot or lane, a 16-bit history, sub > 1, or a shot batch of 1).
+static size_t lane_bytes(const eio_ctx* c, bool born);
+static int born_batch_width(eio_ctx* c, int nShots) {
+    const int want = std::min(std::min(c->batch, c->lanes), (int)STEP_BATCH);
+    if (want < 2 || nShots < 2 || !engine_batchable(c->eng)) return 0;
+    const int nb = ensure_lanes(c, nShots, lane_bytes(c, true), want);
+    return nb >= 2 ? nb : 0;
+}
+
+// consecutive groups of at most nb shots with sizes as even as possible: (first shot, count)
+static std::vector<std::pair<int, int>> shot_groups(int nShots, int nb) {
+    const int ng = (nShots + nb - 1) / nb;
+    std::vector<std::pair<int, int>> out;
+    for (int k = 0, s = 0; k < ng; k++) {
+        const int n = nShots / ng + (k < nShots % ng ? 1 : 0);
+        out.emplace_back(s, n);
+        s += n;
+    }
+    return out;
+}
+
 // device bytes a lane needs for a shot: wavefield levels, secondary sources and, for Born, the history
 // (with shot windows set, of the widest window: a lane's buffers grow to the largest shot it runs)
 static size_t lane_bytes(const eio_ctx* c, bool born) {
@@ -681,6 +706,14 @@ EIO_API int eio_ctx_stats(eio_ctx* c, int enable, int reset, long long* launches
         if (stepMs) *stepMs = ms;
     });
 }
+EIO_API int eio_ctx_step_cells(const eio_ctx* c, long long* cells) {
+    return guarded([&] {
+        if (!c || !cells) throw Error(EIO_ERR_ARG, "null context or output");
+        long long n = engine_step_cells(c->eng);
+        for (Engine* e : c->extra) n += engine_step_cells(e);
+        *cells = n;
+    });
+}
 EIO_API int eio_reduce64(int device, int op, int dtype, const void* x, const void* y, long long n, int onDevice,
                          double* result) {
     return guarded([&] {
@@ -721,7 +754,8 @@ EIO_API int eio_born_shots_dev(eio_ctx* c, int adj, int nShots, float* const* sr
     return guarded([&] {
         if (!c || !srcDtw || !dm || !data || !srcPos || !nSrc || !recPos || !nRec || nShots < 1)
             throw Error(EIO_ERR_ARG, "null argument");
-        const int nl = ensure_lanes(c, nShots, lane_bytes(c, true));
+        const int nb = born_batch_width(c, nShots);
+        const int nl = nb ? nb : ensure_lanes(c, nShots, lane_bytes(c, true));
         std::vector<float*> lane_dm((size_t)5 * nl);
         for (int k = 0; k < nl; k++) {
             if (adj && k > 0) {   // the other lanes image into their own buffers, added below
@@ -730,6 +764,25 @@ EIO_API int eio_born_shots_dev(eio_ctx* c, int adj, int nShots, float* const* sr
             } else {
                 for (int f = 0; f < 5; f++) lane_dm[5 * k + f] = dm[f];
             }
+        }
+        if (nb) {   // groups of shots in lockstep: shot i of a group on lane i
+            std::vector<Engine*> es(nb);
+            for (int k = 0; k < nb; k++) es[k] = lane_engine(c, k);
+            for (const auto& grp : shot_groups(nShots, nb)) {
+                const int s0 = grp.first, n = grp.second;
+                std::vector<ShotGeom> g(n);
+                std::vector<float*> dmv((size_t)5 * n);
+                for (int i = 0; i < n; i++) {
+                    const size_t s = (size_t)(s0 + i);
+                    g[i] = make_geom(srcPos + 4 * s, nSrc + 4 * s, recPos + 4 * s, nRec + 4 * s);
+                    for (int f = 0; f < 5; f++) dmv[5 * i + f] = adj ? lane_dm[5 * i + f] : dm[f];
+                }
+                engine_born_batch_dev(es.data(), n, adj, srcDtw + 5 * (size_t)s0, dmv.data(), data + 5 * (size_t)s0,
+                                      g.data());
+            }
+            if (adj)
+                for (int k = 1; k < nl; k++) engine_dm_add(lane_engine(c, k), dm);
+            return;
         }
         run_lanes(c, nl, nShots, [&](int k, Engine* eng, int s) {
             engine_born(eng, adj, srcDtw + 5 * (size_t)s, lane_dm.data() + 5 * k, data + 5 * (size_t)s,
@@ -1295,6 +1348,45 @@ EIO_API int eio_nl_adjoint_wavefield(eio_ctx* c, int add, int nExp, int nModelEx
     return nl_adjoint_impl(c, add, nExp, nModelExp, model, data, src, rec, nRecGeom, wShot, wfld);
 }
 
+// One group of Born shots in lockstep through the operator path: shot s0 + i
+// runs on lane i (its window, fine-time sources from the host preparation,
+// receivers interpolated on the GPU).  Forward: every shot reads the first
+// lane's perturbation at its window; adjoint: shot i images into lane i's
+// own buffers (summed by image_to_model).  dataIrreg: per shot host traces.
+static void born_group(eio_ctx* c, int adj, int s0, int n, int nExp, eio_sinterp* const* src,
+                       eio_sinterp* const* rec, int nRecGeom, const float* const* sigs, int nSignals,
+                       float* const* dataIrreg) {
+    std::vector<Engine*> es(n);
+    std::vector<std::vector<float>> fine((size_t)5 * n);
+    std::vector<float*> sp((size_t)5 * n), dmv((size_t)5 * n);
+    std::vector<std::unique_ptr<ShotWindow>> wins;
+    std::vector<ShotGeom> g(n);
+    std::vector<const SInterp*> recs((size_t)4 * n);
+    float* base0[5];
+    engine_dm_ptrs(lane_engine(c, 0), base0);
+    for (int i = 0; i < n; i++) {
+        const int e = s0 + i;
+        es[i] = lane_engine(c, i);
+        ShotGrids gg = shot_grids(src, rec, nRecGeom, e);
+        std::vector<float> f5[5];
+        born_sources(c, gg, sigs[nSignals == 1 ? 0 : e], f5);
+        for (int f = 0; f < 5; f++) {
+            fine[5 * i + f] = std::move(f5[f]);
+            sp[5 * i + f] = fine[5 * i + f].data();
+        }
+        wins.emplace_back(new ShotWindow(c, es[i], gg, e, nExp));
+        g[i] = wins.back()->sg;
+        for (int k = 0; k < 4; k++) recs[4 * i + k] = gg.r[k];
+        if (adj) {
+            engine_dm_window(es[i], dmv.data() + 5 * i);
+        } else {
+            const long long off = c->win_nx.empty() ? 0 : (long long)c->win_ix0[e] * c->fd.p.nz;
+            for (int f = 0; f < 5; f++) dmv[5 * i + f] = base0[f] + off;
+        }
+    }
+    engine_born_shots_batch(es.data(), n, adj, sp.data(), dmv.data(), g.data(), recs.data(), dataIrreg);
+}
+
 EIO_API int eio_born_forward(eio_ctx* c, int add, int nExp, const float* model, float* data,
                              const float* const* sigs, int nSignals, eio_sinterp* const* src, eio_sinterp* const* rec,
                              int nRecGeom) {
@@ -1314,10 +1406,26 @@ EIO_API int eio_born_forward(eio_ctx* c, int add, int nExp, const float* model, 
             check_nt(g, nts);
             if ((size_t)5 * g.r[0]->nIrreg * nts != dslice) throw Error(EIO_ERR_ARG, "receiver counts differ");
         }
-        const int nl = ensure_lanes(c, nExp, lane_bytes(c, true));
+        const int nb = born_batch_width(c, nExp);
+        const int nl = nb ? nb : ensure_lanes(c, nExp, lane_bytes(c, true));
         for (int k = 0; k < nl; k++) engine_dm_upload(lane_engine(c, k), dm);   // stays on the device for every shot
         std::vector<float*> tmp(nl);
         for (int k = 0; k < nl; k++) tmp[k] = add ? lane_staging(c, k, dslice) : nullptr;
+        if (nb) {
+            for (const auto& grp : shot_groups(nExp, nb)) {
+                std::vector<float*> out(grp.second);
+                for (int i = 0; i < grp.second; i++) out[i] = add ? tmp[i] : data + (size_t)(grp.first + i) * dslice;
+                born_group(c, 0, grp.first, grp.second, nExp, src, rec, nRecGeom, sigs, nSignals, out.data());
+                if (add)
+                    for (int i = 0; i < grp.second; i++) {
+                        float* d = data + (size_t)(grp.first + i) * dslice;
+                        const float* t = tmp[i];
+#pragma omp parallel for schedule(static)
+                        for (long long q = 0; q < (long long)dslice; q++) d[q] += t[q];
+                    }
+            }
+            return;
+        }
         run_lanes(c, nl, nExp, [&](int k, Engine* eng, int e) {
             ShotGrids g = shot_grids(src, rec, nRecGeom, e);
             std::vector<float> fine[5];
@@ -1396,8 +1504,19 @@ EIO_API int eio_born_adjoint(eio_ctx* c, int add, int nExp, float* model, const 
             check_nt(g, nts);
             if ((size_t)5 * g.r[0]->nIrreg * nts != dslice) throw Error(EIO_ERR_ARG, "receiver counts differ");
         }
-        const int nl = ensure_lanes(c, nExp, lane_bytes(c, true));
+        const int nb = born_batch_width(c, nExp);
+        const int nl = nb ? nb : ensure_lanes(c, nExp, lane_bytes(c, true));
         for (int k = 0; k < nl; k++) engine_dm_zero(lane_engine(c, k));   // each lane's shots accumulate on its device
+        if (nb) {
+            for (const auto& grp : shot_groups(nExp, nb)) {
+                std::vector<float*> in(grp.second);
+                for (int i = 0; i < grp.second; i++)
+                    in[i] = const_cast<float*>(data) + (size_t)(grp.first + i) * dslice;
+                born_group(c, 1, grp.first, grp.second, nExp, src, rec, nRecGeom, sigs, nSignals, in.data());
+            }
+            image_to_model(c, nl, dm, sl, model);
+            return;
+        }
         run_lanes(c, nl, nExp, [&](int, Engine* eng, int e) {
             ShotGrids g = shot_grids(src, rec, nRecGeom, e);
             std::vector<float> fine[5];

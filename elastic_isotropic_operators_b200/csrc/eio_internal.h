@@ -139,6 +139,17 @@ void engine_dm_window(Engine* e, float* out[5]);
 constexpr int STEP_BATCH = 8;   // shots of one lockstep launch (k_step_batch)
 void engine_nl_shots_batch(Engine* const* es, int nb, int adj, float* const* modelReg, const ShotGeom* g,
                            const SInterp* const* rec, float* const* dataIrreg);
+// Born forward / adjoint of nb shots in lockstep (one engine per shot; sub = 1,
+// FP32 history, no free surface); dm: per shot 5 device pointers (the
+// perturbation, or the shot's own image), offset to the shot's window.
+// Host traces (receivers interpolated on the GPU, like engine_born_shot):
+void engine_born_shots_batch(Engine* const* es, int nb, int adj, float* const* srcDtw, float* const* dm,
+                             const ShotGeom* g, const SInterp* const* rec, float* const* dataIrreg);
+// device traces: ds fine-time regular sources, dr regular receiver traces, per shot 5 arrays each
+void engine_born_batch_dev(Engine* const* es, int nb, int adj, float* const* ds, float* const* dm, float* const* dr,
+                           const ShotGeom* g);
+bool engine_batchable(const Engine* e);   // sub = 1 and an FP32 history
+long long engine_step_cells(const Engine* e);
 void engine_nl_shot(Engine* e, int adj, float* const modelReg[5], const ShotGeom& g, const SInterp* const rec[4],
                     float* dataIrreg, float* wfld = nullptr);
 void engine_born_host(Engine* e, int adj, float* const srcDtw[5], float* const dm[5], float* const data[5],

@@ -797,19 +797,25 @@ __global__ void __launch_bounds__(NT, MINB) k_step(StepArgs a)
     step_body<DIR, EPI, MINB, FS>(a, blockIdx.x);
 }
 
-// The same step for up to STEP_BATCH shots in one launch: blockIdx.y picks the
-// shot, blockIdx.x its tile.  Shots may have different windows (nx, taper):
-// a shot's tiles beyond its own count leave at once, before touching memory.
+// Argument block of the step launches that cover several shots (k_step_shots).
 struct StepBatch {
     StepArgs a[STEP_BATCH];
 };
 
-template <int DIR, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_step_batch(const __grid_constant__ StepBatch b)
+// The same step for nb <= STEP_BATCH shots in one launch, with the shots of a
+// tile next to each other in the launch order: CTA b runs tile b / nb of shot
+// b % nb.  The CTAs of one tile are then resident at the same time; shots that
+// share the medium arrays (and the Born perturbation) read a tile of them from
+// HBM once, the other shots' reads hit in L2.  Each shot keeps its own
+// wavefields, window, taper, point lists and epilogue buffers in its StepArgs;
+// a shot's tiles beyond its own count leave before touching memory.
+template <int DIR, int EPI, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_step_shots(const __grid_constant__ StepBatch b, int nb)
 {
-    const StepArgs& a = b.a[blockIdx.y];
-    if ((int)blockIdx.x >= a.ntz * ((a.nx - 2 * FAT) / TX)) return;   // CTA-uniform
-    step_body<DIR, EPI_NONE, MINB, false>(a, blockIdx.x);
+    const int shot = blockIdx.x % nb, tile = blockIdx.x / nb;
+    const StepArgs& a = b.a[shot];
+    if (tile >= a.ntz * ((a.nx - 2 * FAT) / TX)) return;   // CTA-uniform
+    step_body<DIR, EPI, MINB, false>(a, tile);
 }
 
 // Same step with two threads per float4: warps 0-7 update vx and vz, warps
@@ -875,12 +881,12 @@ struct ImagingArgs {
 // each); the snapshot at its is staged with its 4-cell halo in shared memory for
 // the staggered derivatives, the neighbouring snapshots give the time difference.
 template <int ADJ, int Q>
-__global__ void __launch_bounds__(NT) k_imaging(ImagingArgs a)
+__device__ __forceinline__ void imaging_body(const ImagingArgs& a, int tile)
 {
     __shared__ __align__(16) float sm[2 * SMEM_FIELD];
     const int tid = threadIdx.x;
     const int ntz = (a.nz - 2 * FAT + TZ - 1) / TZ;
-    const int bz = blockIdx.x % ntz, bx = blockIdx.x / ntz;
+    const int bz = tile % ntz, bx = tile / ntz;
     const int z0 = FAT + bz * TZ, x0 = FAT + bx * TX;
     const long long nz = a.nz;
     stage_snapshot<Q>(a.h, a.its, a.nz, sm, z0, x0, tid);
@@ -911,6 +917,28 @@ __global__ void __launch_bounds__(NT) k_imaging(ImagingArgs a)
                              ldg4(a.ss[4] + gi)};
         imaging_accumulate(a.dm, gi, s, t, a.dts_inv);
     }
+}
+
+template <int ADJ, int Q>
+__global__ void __launch_bounds__(NT) k_imaging(ImagingArgs a)
+{
+    imaging_body<ADJ, Q>(a, blockIdx.x);
+}
+
+// k_imaging for nb <= STEP_BATCH shots, the shots of a tile next to each other
+// in the launch order (CTA b: tile b / nb of shot b % nb), so that the Born
+// perturbation the forward kernels of all shots read comes from HBM once.
+struct ImagingBatch {
+    ImagingArgs a[STEP_BATCH];
+};
+
+template <int ADJ, int Q>
+__global__ void __launch_bounds__(NT) k_imaging_shots(const __grid_constant__ ImagingBatch b, int nb)
+{
+    const int shot = blockIdx.x % nb, tile = blockIdx.x / nb;
+    const ImagingArgs& a = b.a[shot];
+    if (tile >= ((a.nz - 2 * FAT + TZ - 1) / TZ) * ((a.nx - 2 * FAT) / TX)) return;   // CTA-uniform
+    imaging_body<ADJ, Q>(a, tile);
 }
 
 // Coarse-time sample of all five fields of the new level (interpWavefield,

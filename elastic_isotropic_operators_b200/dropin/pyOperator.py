@@ -36,16 +36,16 @@ class Operator:
 
     def dotTest(self, verb=False, maxError=1e-4):
         """<A x, y> against <x, A^T y> for random x, y (FP64 sums), with add
-        off and on; raises RuntimeError when a relative error exceeds maxError."""
+        off and on; raises RuntimeError when a relative error exceeds maxError.
+        The add pass starts from the outputs of the first pass, so the
+        accumulated vectors keep the operator's own scale (an O(1) random start
+        would swamp a small-valued output in FP32)."""
         x = self.domain.clone().rand()
         y = self.range.clone().rand()
         Ax = self.range.clone().zero()
         ATy = self.domain.clone().zero()
         results = []
         for add in (False, True):
-            if add:
-                Ax.rand()
-                ATy.rand()
             ax0, aty0 = Ax.clone(), ATy.clone()
             self.forward(add, x, Ax)
             self.adjoint(add, ATy, y)

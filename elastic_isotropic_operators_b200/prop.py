@@ -278,9 +278,10 @@ class _ElasticOp:
         check(self._L.eio_ctx_set_lanes(self._ctx, int(lanes)))
 
     def setShotBatch(self, shots):
-        """Nonlinear forward and adjoint: advance up to ``shots`` (1 .. 8, default
-        8) shots in lockstep with one step launch for all of them; 1 runs the
-        shots one at a time on the lanes."""
+        """Advance up to ``shots`` (1 .. 8, default 8) shots in lockstep with one
+        step launch for all of them (the nonlinear operators; the Born operators
+        in groups as wide as the device memory holds their histories); 1 runs
+        the shots one at a time on the lanes."""
         check(self._L.eio_ctx_set_shot_batch(self._ctx, int(shots)))
 
     def getMedium(self):

@@ -169,13 +169,26 @@ int eio_ctx_get_wait_limit(const eio_ctx *c, long long *polls);
  * enable: 1 on, 0 off, -1 unchanged; reset: zero the counters after reading. */
 int eio_ctx_stats(eio_ctx *c, int enable, int reset, long long *launches, long long *stepLaunches,
                   double *stepMs);
-/* Shot batching of the nonlinear operators (no reference counterpart): with
- * shots > 1 (default 8), eio_nl_forward and eio_nl_adjoint advance up to
- * `shots` (<= 8) shots in lockstep, one engine each, with one step launch per
- * fine step for all of them (blockIdx.y = shot, each shot on its own window
- * and point lists); 1 runs the shots one at a time on the lanes.  Results equal
- * the one-shot propagation with the tile kernel bit for bit.  Not used with
- * the free surface or when a wavefield is saved. */
+/* Cell updates of the single-step launches since the last eio_ctx_stats reset,
+ * summed over the lanes (a launch that advances several shots counts each
+ * shot's interior cells); call it before eio_ctx_stats resets the counters. */
+int eio_ctx_step_cells(const eio_ctx *c, long long *cells);
+/* Shot batching (no reference counterpart; the reference runs one shot per GPU
+ * at a time, BornElasticShotsGpu.cpp:178-207): with shots > 1 (default 8) the
+ * multi-shot operators advance up to `shots` (<= 8) shots in lockstep, one
+ * engine each, with one step launch per fine step for all of them.  The
+ * launch orders the shots of a tile next to each other and every shot reads
+ * one copy of the medium, so a medium tile comes from HBM once per step for
+ * the whole group.  eio_nl_forward / eio_nl_adjoint: each shot on its own
+ * window and point lists; not used with the free surface or when a wavefield
+ * is saved.  eio_born_forward / eio_born_adjoint / eio_born_shots_dev: groups
+ * of as many shots as the free device memory holds (each needs its own
+ * source-wavefield history), sizes as even as possible, the imaging of a
+ * group in one launch per coarse sample; used with sub = 1 and FP32
+ * histories, otherwise the lanes run the shots.  Per-shot traces equal the
+ * one-shot propagation with the tile kernel (kind 3) bit for bit; the Born
+ * image adds the shots in another order (each shot of a group into its own
+ * buffer).  1 runs the shots one at a time on the lanes. */
 int eio_ctx_set_shot_batch(eio_ctx *c, int shots);
 /* Shot lanes (no reference counterpart; the reference runs one shot per GPU at
  * a time). The multi-shot operators (eio_nl_forward/adjoint,
