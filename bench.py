@@ -46,7 +46,7 @@ def parse():
                              "cnn_train"])
     ap.add_argument("--batch", type=int, default=None,
                     help="shots per lockstep launch (1 = one shot at a time on the lanes); nl_shots default 8, "
-                         "born_600x1800 default: the library's (as wide as the lanes and memory allow)")
+                         "born_600x1800 default: the library's (1)")
     ap.add_argument("--pairs", type=int, default=48, help="fwi_learned: Born training pairs")
     ap.add_argument("--conv-path", type=int, default=-1, choices=[-1, 0, 1],
                     help="cnn_train: forward convolutions on mma.sync (0) or tcgen05 (1); "
@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--fwi-unfused", action="store_true",
                     help="fwi_1000x3400: nonlinear forward + Born adjoint (3 propagations per shot) instead of "
                          "the fused gradient (2)")
+    ap.add_argument("--persistent", type=int, default=None,
+                    help="Born shot groups: phases run as persistent time loops (bits 1 source, 2 scattered, "
+                         "4 adjoint; 0 = one launch per fine step); default: the library's")
     ap.add_argument("--lanes", type=int, default=0,
                     help="shot lanes (concurrent shots on the GPU); 0 keeps the library default")
     ap.add_argument("--kernel", type=int, default=-1, choices=[-1, 0, 1, 2, 3, 4, 5],
@@ -262,7 +265,9 @@ def run_ours(args, ws, rank, local):
     ctx = born.ctx
     pin_kernel(L, ctx, args)
     if args.batch is not None:
-        _lib.check(L.eio_ctx_set_shot_batch(ctx, args.batch))
+        _lib.check(L.eio_ctx_set_born_batch(ctx, args.batch))
+    if args.persistent is not None:
+        _lib.check(L.eio_ctx_set_persistent(ctx, args.persistent))
     est = torch.cuda.ExternalStream(L.eio_ctx_stream(ctx), device=dev)   # the engine's launch stream
     nsh = w.nExp
     fine_steps, cells = ctypes.c_longlong(), ctypes.c_longlong()

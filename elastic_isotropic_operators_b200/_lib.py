@@ -79,6 +79,9 @@ _SIGS = {
     "eio_ctx_autotune": (I, [P, IP, IP, IP, IP]),
     "eio_ctx_set_wait_limit": (I, [P, ctypes.c_longlong]),
     "eio_ctx_step_cells": (I, [P, ctypes.POINTER(ctypes.c_longlong)]),
+    "eio_ctx_set_persistent": (I, [P, I]),
+    "eio_ctx_set_born_batch": (I, [P, I]),
+    "eio_ctx_get_persistent": (I, [P, IP]),
     "eio_ctx_get_wait_limit": (I, [P, ctypes.POINTER(ctypes.c_longlong)]),
     "eio_ctx_stats": (I, [P, I, I, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
                           ctypes.POINTER(ctypes.c_double)]),

@@ -22,6 +22,7 @@
 #include "eio_pair.cuh"
 #include "eio_sweep.cuh"
 #include "eio_tile.cuh"
+#include "eio_wave.cuh"
 
 namespace eio {
 
@@ -88,6 +89,10 @@ struct Engine {
     // wavefield levels: two sets of 5 slices for the single-step kernels, four
     // for the two-step kernel (it writes both new levels to the free sets)
     DBuf par[5], dampz, dampx, wf[20];
+    // the engine whose medium arrays the kernels read (nullptr: its own).  The
+    // shot lanes of a context read the first lane's copy, so that lanes running
+    // at once share one medium in L2 instead of evicting each other's
+    const Engine* med = nullptr;
     // free surface (nonlinear operators only, like the reference): taper
     // without the top edge, sigmaxx coefficient of the surface row per column
     int fs = 0;
@@ -131,6 +136,13 @@ struct Engine {
     const void* tbase[15] = {};
     int tile_ctas[2] = {0, 0};    // persistent k_tile grid per direction (0 = not yet queried)
     DBuf err;
+    // persistent time loop (eio_wave.cuh) of the lockstep shot groups: on by
+    // default; the per-step plan, modes, secondary-source samples and unit counters
+    // phases of the Born shot groups run as persistent loops (bits: 1 source, 2 scattered, 4 adjoint);
+    // 0 by default: measured slower than the per-step launches (eio_ctx_set_persistent)
+    int use_wave = 0;
+    DBuf wave_plan, wave_mode, wave_ssk, wave_done;
+    int wave_ctas[8] = {};   // resident CTAs per k_wave instantiation (0 = not queried)
     // try_wait polls of a TMA pipeline wait in the sweep and tile kernels before
     // it gives up (error flag, drain, EIO_ERR_TIMEOUT); their drains keep DRAIN_LIMIT
     long long wait_limit = WAIT_LIMIT;
@@ -163,6 +175,9 @@ struct Engine {
 };
 
 static void graph_free(Engine::Graph* g);
+
+// medium array f (rhoxDtw, rhozDtw, lamb2MuDtw, lambDtw, muxzDtw) the kernels of e read
+static float* mpar(const Engine* e, int f) { return (e->med ? e->med : e)->par[f].f(); }
 
 // CUDA-event timing of every STATS_PERIOD-th launch of the fused step kernel
 // (only when enabled); sampling keeps the event records out of most gaps.
@@ -492,7 +507,7 @@ static StepArgs base_args(Engine* e) {
     StepArgs a;
     memset(&a, 0, sizeof(a));
     const long long off = (long long)e->win_ix0 * e->nz;   // shot window
-    for (int f = 0; f < 5; f++) a.par[f] = e->par[f].f() + off;
+    for (int f = 0; f < 5; f++) a.par[f] = mpar(e, f) + off;
     a.dampz = e->fs_active ? e->dampz_fs.f() : e->dampz.f();
     a.dampx = e->windowed ? e->dampx_w.f() : e->dampx.f();
     a.fs = e->fs_active ? 1 : 0;
@@ -539,8 +554,8 @@ static void ensure_maps(Engine* e) {
         e->mwf_int[b] = make_map(e->wf[b].f(), e->nz, e->nx, e->tz, e->cw);
     }
     for (int f = 0; f < 5; f++) {
-        e->mpar_halo[f] = make_map(e->par[f].f(), e->nz, e->nx, e->tz + 2 * FAT, e->cw);
-        e->mpar_int[f] = make_map(e->par[f].f(), e->nz, e->nx, e->tz, e->cw);
+        e->mpar_halo[f] = make_map(mpar(e, f), e->nz, e->nx, e->tz + 2 * FAT, e->cw);
+        e->mpar_int[f] = make_map(mpar(e, f), e->nz, e->nx, e->tz, e->cw);
     }
     e->mtz = e->tz;
     e->mcw = e->cw;
@@ -596,7 +611,7 @@ static void launch_sweep(Engine* e, const StepArgs& a, int cur) {
 static void ensure_tile_maps(Engine* e) {
     bool same = true;
     for (int b = 0; b < 10; b++) same = same && e->tbase[b] == e->wf[b].p;
-    for (int f = 0; f < 5; f++) same = same && e->tbase[10 + f] == e->par[f].p;
+    for (int f = 0; f < 5; f++) same = same && e->tbase[10 + f] == mpar(e, f);
     if (same) return;
     for (int b = 0; b < 10; b++) {
         e->twf_halo[b] = make_map(e->wf[b].f(), e->nz, e->nx, SZ, SX);
@@ -604,9 +619,9 @@ static void ensure_tile_maps(Engine* e) {
         e->tbase[b] = e->wf[b].p;
     }
     for (int f = 0; f < 5; f++) {
-        e->tpar_halo[f] = make_map(e->par[f].f(), e->nz, e->nx, SZ, SX);
-        e->tpar_int[f] = make_map(e->par[f].f(), e->nz, e->nx, TZ, TX);
-        e->tbase[10 + f] = e->par[f].p;
+        e->tpar_halo[f] = make_map(mpar(e, f), e->nz, e->nx, SZ, SX);
+        e->tpar_int[f] = make_map(mpar(e, f), e->nz, e->nx, TZ, TX);
+        e->tbase[10 + f] = mpar(e, f);
     }
 }
 
@@ -1066,6 +1081,19 @@ static void err_check(Engine* e) {
 }
 
 void engine_set_wait_limit(Engine* e, long long polls) { e->wait_limit = polls < 0 ? WAIT_LIMIT : polls; }
+void engine_share_medium(Engine* e, const Engine* from) {
+    if (from == e) from = nullptr;
+    if (from && (from->nz != e->nz || from->full_nx != e->full_nx || from->device != e->device))
+        throw Error(EIO_ERR_ARG, "engines of different grids or devices cannot share a medium");
+    e->med = from;
+    memset(e->tbase, 0, sizeof(e->tbase));   // tensor maps of the TMA tile kernel are rebuilt
+    e->mtz = -1;                             // ... and those of the sweep kernel
+}
+void engine_set_persistent(Engine* e, int mask) {
+    if (mask < 0 || mask > 7) throw Error(EIO_ERR_ARG, "persistent-loop mask must be 0 .. 7");
+    e->use_wave = mask;
+}
+int engine_get_persistent(const Engine* e) { return e->use_wave; }
 long long engine_get_wait_limit(const Engine* e) { return e->wait_limit; }
 
 // new level (in p) into coarse rows its, its+1 of the saved wavefield
@@ -1987,7 +2015,7 @@ void engine_nl_shots_batch(Engine* const* es, int nb, int adj, float* const* mod
         a = base_args(e);
         // every engine of a context holds the same medium: all shots read the first
         // engine's, so the shots' CTAs of one tile share it through L2
-        for (int f = 0; f < 5; f++) a.par[f] = e0->par[f].f() + (long long)e->win_ix0 * e->nz;
+        for (int f = 0; f < 5; f++) a.par[f] = mpar(e0, f) + (long long)e->win_ix0 * e->nz;
         zero_wavefields(e);
         lv.emplace_back(e);
         if (!adj) {
@@ -2070,6 +2098,10 @@ struct ShotBatch {
     int max_tiles = 0;
     StepBatch b;
     std::vector<Levels> lv;
+    // persistent time loop: the steps of a phase are recorded here and run as one k_wave launch
+    bool wave = false;
+    std::vector<StepArgs> plan;
+    std::vector<int> modes, ssk;
     ShotBatch(Engine* const* engines, int n) : es(engines), nb(n) {
         if (nb < 1 || nb > STEP_BATCH) throw Error(EIO_ERR_ARG, "batch of 1 .. 8 shots");
         memset(&b, 0, sizeof(b));
@@ -2091,7 +2123,7 @@ struct ShotBatch {
             Engine* e = es[i];
             b.a[i] = base_args(e);
             const long long off = (long long)e->win_ix0 * e->nz;
-            for (int f = 0; f < 5; f++) b.a[i].par[f] = e0->par[f].f() + off;
+            for (int f = 0; f < 5; f++) b.a[i].par[f] = mpar(e0, f) + off;
         }
     }
     void levels() {
@@ -2112,13 +2144,98 @@ struct ShotBatch {
         EIO_CUDA(cudaEventRecord(es[0]->ev_sync, es[0]->st));
         for (int i = 1; i < nb; i++) EIO_CUDA(cudaStreamWaitEvent(es[i]->st, es[0]->ev_sync, 0));
     }
+    // one fine step: launched now, or recorded for the persistent loop (whose
+    // phase runs one epilogue: EPI_TRI / EPI_TRI_IMG steps without a coarse
+    // sample carry tmode 0 and are plain steps)
     template <int DIR, int EPI, int MINB>
-    void step() {
-        launch_shots<DIR, EPI, MINB>(es[0], b, nb, max_tiles);
-        batch_count(es[0], es, nb, 1);
+    void step(int ss_k = -1) {
+        if (wave) {
+            plan.insert(plan.end(), b.a, b.a + nb);
+            modes.push_back(ss_k >= 0 ? WAVE_SS : 0);
+            ssk.push_back(ss_k);
+        } else {
+            launch_shots<DIR, EPI, MINB>(es[0], b, nb, max_tiles);
+            batch_count(es[0], es, nb, 1);
+        }
         for (int i = 0; i < nb; i++) lv[i].single();
     }
+    // start recording a phase (bit `phase` of the first engine's persistent-loop mask)
+    void begin(int phase) {
+        wave = (es[0]->use_wave & phase) != 0;
+        plan.clear();
+        modes.clear();
+        ssk.clear();
+    }
+    // run the recorded phase as one persistent launch of k_wave<DIR, EPI, MINB>;
+    // ia / slots: the secondary-source inputs of the forward scattered phase
+    template <int DIR, int EPI, int MINB>
+    void run(const ImagingArgs* ia = nullptr, float* const* slots = nullptr);
 };
+
+template <int DIR, int EPI, int MINB>
+static int wave_resident(Engine* e, int slot) {
+    int& n = e->wave_ctas[slot];
+    if (!n) {
+        int per = 0;
+        EIO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_wave<DIR, EPI, MINB>, NT, 0));
+        if (per < 1) throw Error(EIO_ERR_CUDA, "the persistent step kernel does not fit on an SM");
+        n = per * e->nsm;
+    }
+    return n;
+}
+// the wave_ctas slot of each instantiation
+template <int DIR, int EPI, int MINB>
+constexpr int wave_slot() {
+    return EPI == EPI_TRI ? 0 : EPI == EPI_INJ_SS ? 1 : EPI == EPI_TRI_IMG ? 2 : (DIR == 0 ? 3 : 4) + (MINB == 4 ? 2 : 0);
+}
+
+template <int DIR, int EPI, int MINB>
+void ShotBatch::run(const ImagingArgs* ia, float* const* slots) {
+    if (!wave || modes.empty()) return;
+    Engine* e0 = es[0];
+    const int nsteps = (int)modes.size();
+    const size_t pbytes = sizeof(StepArgs) * plan.size();
+    e0->wave_plan.ensure(pbytes);
+    e0->wave_mode.ensure(sizeof(int) * nsteps);
+    e0->wave_ssk.ensure(sizeof(int) * nsteps);
+    e0->wave_done.ensure(sizeof(int) * (size_t)nb * max_tiles);
+    EIO_CUDA(cudaMemcpyAsync(e0->wave_plan.p, plan.data(), pbytes, cudaMemcpyHostToDevice, e0->st));
+    EIO_CUDA(cudaMemcpyAsync(e0->wave_mode.p, modes.data(), sizeof(int) * nsteps, cudaMemcpyHostToDevice, e0->st));
+    EIO_CUDA(cudaMemcpyAsync(e0->wave_ssk.p, ssk.data(), sizeof(int) * nsteps, cudaMemcpyHostToDevice, e0->st));
+    EIO_CUDA(cudaMemsetAsync(e0->wave_done.p, 0, sizeof(int) * (size_t)nb * max_tiles, e0->st));
+    WaveArgs w;
+    memset(&w, 0, sizeof(w));
+    w.plan = static_cast<const StepArgs*>(e0->wave_plan.p);
+    w.mode = static_cast<const int*>(e0->wave_mode.p);
+    w.ss_k = static_cast<const int*>(e0->wave_ssk.p);
+    for (int i = 0; i < nb; i++) {
+        if (ia) w.img[i] = ia[i];
+        if (slots)
+            for (int k = 0; k < 2; k++)
+                for (int f = 0; f < 5; f++) w.ss[i][k][f] = slots[(i * 2 + k) * 5 + f];
+    }
+    w.done = static_cast<int*>(e0->wave_done.p);
+    w.err = static_cast<int*>(e0->err.p);
+    w.wait_limit = e0->wait_limit * 4;
+    w.nsteps = nsteps;
+    w.nb = nb;
+    w.max_tiles = max_tiles;
+    const int units = nb * max_tiles;
+    const bool timed = e0->stats;
+    if (timed) stats_mark(e0);
+    void* args[] = {&w};
+    const int g = std::min(units, wave_resident<DIR, EPI, MINB>(e0, wave_slot<DIR, EPI, MINB>()));
+    EIO_CUDA(cudaLaunchCooperativeKernel((const void*)k_wave<DIR, EPI, MINB>, g, NT, args, 0, e0->st));
+    if (timed) {
+        stats_mark(e0);
+        e0->sampled += nsteps;   // the event pair covers every step of the phase
+    }
+    e0->launches++;
+    e0->step_launches += nsteps;
+    batch_count(e0, es, nb, nsteps);
+    // the host arrays are read by the copies above: keep them until the stream has passed them
+    EIO_CUDA(cudaStreamSynchronize(e0->st));
+}
 
 // Phase 1 of every shot: the source wavefield and its coarse Vx/Vz history
 // (born_source with two fine steps per sample).  src: per-shot source lists
@@ -2146,6 +2263,7 @@ static void batch_source(ShotBatch& B, std::vector<PointList>& src, const Sparse
     const SrcWeights weights{e0, ext != nullptr};
     const float* F = e0->filt.data();
     const int h = e0->h;
+    B.begin(1);
     for (int its = 0; its < e0->nts - 1; its++)
         for (int it2 = 1; it2 < 3; it2++) {
             const bool last = (its == e0->nts - 2 && it2 == 2);
@@ -2157,11 +2275,14 @@ static void batch_source(ShotBatch& B, std::vector<PointList>& src, const Sparse
                     a.tmode = 1; a.wt = its; a.tw_o = F[h + 1]; a.tw_c = F[h + 2]; a.tw_n = F[1];
                 } else if (last) {       // row nts-1 = c*f[h+1] + n*f[h+2]
                     a.tmode = 2; a.wt = its + 1; a.tw_o = 0.f; a.tw_c = F[h + 1]; a.tw_n = F[h + 2];
+                } else {
+                    a.tmode = 0;         // no coarse sample: a plain step
                 }
             }
-            if (it2 == 1 || last) B.step<0, EPI_TRI, 4>();
+            if (it2 == 1 || last || B.wave) B.step<0, EPI_TRI, 4>();
             else B.step<0, EPI_NONE, 4>();
         }
+    B.run<0, EPI_TRI, 3>();
     check_launch();
     B.join_out();   // phase 2 prepares on the engines' own streams
 }
@@ -2195,6 +2316,36 @@ static void batch_scatter(ShotBatch& B, std::vector<PointList>& rec, float* cons
     }
     B.levels();
     B.join_in();
+    const float* F = e0->filt.data();
+    const int h = e0->h;
+    B.begin(2);
+    if (B.wave) {
+        // persistent loop: the owning CTA computes the secondary sources of sample k
+        // for its tile into ring slot k % 2 right before the first step that uses them
+        std::vector<float*> slots((size_t)B.nb * 2 * 5);
+        for (int i = 0; i < B.nb; i++)
+            for (int k = 0; k < 2; k++)
+                for (int f = 0; f < 5; f++) slots[(i * 2 + k) * 5 + f] = B.es[i]->ss[k * 5 + f].f();
+        for (int its = 0; its < e0->nts - 1; its++)
+            for (int it2 = 1; it2 < 3; it2++) {
+                for (int i = 0; i < B.nb; i++) {
+                    StepArgs& a = B.b.a[i];
+                    B.lv[i].set(a);
+                    for (int f = 0; f < 5; f++) {
+                        a.ssL[f] = slots[(i * 2 + (its & 1)) * 5 + f];
+                        a.ssR[f] = slots[(i * 2 + ((its + 1) & 1)) * 5 + f];
+                    }
+                    a.sw0 = F[it2 - 1]; a.sw1 = F[h + it2 - 1];
+                    a.ext.t0 = its; a.ext.w0 = F[it2]; a.ext.w1 = F[h + it2];
+                }
+                // sample 0 before the first step; sample its+1 before (its, 2), its first reader
+                const int k = (its == 0 && it2 == 1) ? 0 : (it2 == 2 ? its + 1 : -1);
+                B.step<0, EPI_INJ_SS, 4>(k);
+            }
+        B.run<0, EPI_INJ_SS, 3>(ib.a, slots.data());
+        check_launch();
+        return;
+    }
     EIO_CUDA(cudaEventRecord(e0->ev_sync, e0->st));
     EIO_CUDA(cudaStreamWaitEvent(e0->st2, e0->ev_sync, 0));
     for (int k = 0; k < R; k++) {
@@ -2212,8 +2363,6 @@ static void batch_scatter(ShotBatch& B, std::vector<PointList>& rec, float* cons
         e0->launches++;
         EIO_CUDA(cudaEventRecord(e0->ev_ready[sl], e0->st2));
     };
-    const float* F = e0->filt.data();
-    const int h = e0->h;
     for (int k = 0; k < R - 1 && k < e0->nts; k++) image(k);
     for (int its = 0; its < e0->nts - 1; its++) {
         if (its + R - 1 < e0->nts) image(its + R - 1);
@@ -2256,6 +2405,7 @@ static void batch_adjoint(ShotBatch& B, std::vector<PointList>& rec, float* cons
     B.join_in();
     const float* F = e0->filt.data();
     const int h = e0->h;
+    B.begin(4);
     for (int its = e0->nts - 2; its > -1; its--)
         for (int it2 = 1; it2 > -1; it2--) {
             int T = -1;
@@ -2267,12 +2417,15 @@ static void batch_adjoint(ShotBatch& B, std::vector<PointList>& rec, float* cons
                     T = its + 1; a.tmode = 1; a.tw_o = F[1]; a.tw_c = F[0]; a.tw_n = F[h + 1];
                 } else if (its == 0) {   // sample 0 = p(1) f[1] + p(0) f[0]
                     T = 0; a.tmode = 2; a.tw_o = 0.f; a.tw_c = F[1]; a.tw_n = F[0];
+                } else {
+                    a.tmode = 0;         // no coarse sample: a plain step
                 }
                 a.img_its = T;
             }
-            if (T >= 0) B.step<1, EPI_TRI_IMG, 3>();
+            if (T >= 0 || B.wave) B.step<1, EPI_TRI_IMG, 3>();
             else B.step<1, EPI_NONE, 4>();
         }
+    B.run<1, EPI_TRI_IMG, 3>();
     check_launch();
 }
 

@@ -378,7 +378,8 @@ struct eio_ctx {
     // run shots of a multi-shot call concurrently with eng (eio_ctx_set_lanes)
     std::vector<Engine*> extra;
     int lanes = 2;
-    int batch = STEP_BATCH;   // nonlinear forward: shots per lockstep launch (1 = lanes)
+    int batch = STEP_BATCH;   // nonlinear operators: shots per lockstep launch (1 = lanes)
+    int born_batch = 1;       // Born operators: shots per lockstep group (1 = lanes, measured faster)
     std::vector<std::vector<float>> lane_tmp;   // per-lane host staging of one shot's data (kept across calls)
 };
 
@@ -427,6 +428,8 @@ static int ensure_lanes(eio_ctx* c, int nShots, size_t lane_bytes, int want = 0)
             engine_set_checkpoint(e, engine_get_checkpoint(c->eng));
             engine_set_graphs(e, engine_get_graphs(c->eng));
             engine_set_wait_limit(e, engine_get_wait_limit(c->eng));
+            engine_set_persistent(e, engine_get_persistent(c->eng));
+            engine_share_medium(e, c->eng);   // one copy of the medium for every lane (L2)
         } catch (...) {
             engine_destroy(e);
             throw;
@@ -467,7 +470,7 @@ static void run_lanes(eio_ctx* c, int n, int nShots, F&& f) {
 // single shot or lane, a 16-bit history, sub > 1, or a shot batch of 1).
 static size_t lane_bytes(const eio_ctx* c, bool born);
 static int born_batch_width(eio_ctx* c, int nShots) {
-    const int want = std::min(std::min(c->batch, c->lanes), (int)STEP_BATCH);
+    const int want = std::min(std::min(c->born_batch, c->lanes), (int)STEP_BATCH);
     if (want < 2 || nShots < 2 || !engine_batchable(c->eng)) return 0;
     const int nb = ensure_lanes(c, nShots, lane_bytes(c, true), want);
     return nb >= 2 ? nb : 0;
@@ -666,6 +669,19 @@ EIO_API int eio_ctx_set_wait_limit(eio_ctx* c, long long polls) {
         for (Engine* e : c->extra) engine_set_wait_limit(e, polls);
     });
 }
+EIO_API int eio_ctx_set_persistent(eio_ctx* c, int mask) {
+    return guarded([&] {
+        if (!c) throw Error(EIO_ERR_ARG, "null context");
+        engine_set_persistent(c->eng, mask);
+        for (Engine* e : c->extra) engine_set_persistent(e, mask);
+    });
+}
+EIO_API int eio_ctx_get_persistent(const eio_ctx* c, int* mask) {
+    return guarded([&] {
+        if (!c || !mask) throw Error(EIO_ERR_ARG, "null context or output");
+        *mask = engine_get_persistent(c->eng);
+    });
+}
 EIO_API int eio_ctx_get_wait_limit(const eio_ctx* c, long long* polls) {
     return guarded([&] {
         if (!c || !polls) throw Error(EIO_ERR_ARG, "null context or output");
@@ -719,6 +735,13 @@ EIO_API int eio_reduce64(int device, int op, int dtype, const void* x, const voi
     return guarded([&] {
         if (!result) throw Error(EIO_ERR_ARG, "null result");
         *result = reduce64(device, op, dtype, x, y, n, onDevice != 0);
+    });
+}
+EIO_API int eio_ctx_set_born_batch(eio_ctx* c, int shots) {
+    return guarded([&] {
+        if (!c) throw Error(EIO_ERR_ARG, "null context");
+        if (shots < 1 || shots > STEP_BATCH) throw Error(EIO_ERR_ARG, "Born shot batch must be 1 .. 8");
+        c->born_batch = shots;
     });
 }
 EIO_API int eio_ctx_set_shot_batch(eio_ctx* c, int shots) {

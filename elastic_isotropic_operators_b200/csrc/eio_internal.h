@@ -67,6 +67,9 @@ void engine_set_checkpoint(Engine* e, int mode);
 // step-kernel selection: kind 0 tile kernel, 1 TMA sweep (tz, cw, cpr); autotune times the candidates
 void engine_set_kernel(Engine* e, int kind, int tz, int cw, int cpr);
 void engine_set_wait_limit(Engine* e, long long polls);   // < 0: the default
+void engine_share_medium(Engine* e, const Engine* from);   // e's kernels read from's medium arrays
+void engine_set_persistent(Engine* e, int mask);          // phases of the shot groups run as persistent loops
+int engine_get_persistent(const Engine* e);
 long long engine_get_wait_limit(const Engine* e);
 void engine_get_kernel(const Engine* e, int* kind, int* tz, int* cw, int* cpr);
 void engine_autotune(Engine* e);

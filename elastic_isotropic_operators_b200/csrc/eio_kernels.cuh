@@ -115,6 +115,13 @@ enum { EPI_NONE = 0, EPI_SAVE_W = 1, EPI_INJ_SS = 2, EPI_EXT_SS = 3, EPI_TRI = 4
 
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+// L2-coherent load (bypasses L1 and the read-only path): for data that other
+// CTAs of the same launch write (the persistent time loop, eio_wave.cuh)
+__device__ __forceinline__ float4 ldcg4(const float* p) { return __ldcg(reinterpret_cast<const float4*>(p)); }
+// a wavefield value another CTA of this launch may have written (COH), or one
+// that is constant for the launch
+template <bool COH>
+__device__ __forceinline__ float4 ldw4(const float* p) { return COH ? ldcg4(p) : ldg4(p); }
 __device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
 __device__ __forceinline__ float& at(float4& v, int j) { return reinterpret_cast<float*>(&v)[j]; }
 __device__ __forceinline__ float at(const float4& v, int j) { return reinterpret_cast<const float*>(&v)[j]; }
@@ -381,11 +388,13 @@ __device__ __forceinline__ ImgTerms imaging_terms(const WHist& h, const float* s
 
 // imaging condition (imagingElaAdjGpu, K:1538-1613): the images at gi += the
 // adjoint sample s[5] against the source-wavefield terms
+template <bool COH = false>
 __device__ __forceinline__ void imaging_accumulate(float* const dm[5], long long gi, const float4 (&s)[5],
                                                    const ImgTerms& t, float dts_inv)
 {
-    float4 d0 = ld4(dm[0] + gi), d1 = ld4(dm[1] + gi), d2 = ld4(dm[2] + gi), d3 = ld4(dm[3] + gi),
-           d4 = ld4(dm[4] + gi);
+    auto ld = [&](const float* p) { return COH ? ldcg4(p) : ld4(p); };
+    float4 d0 = ld(dm[0] + gi), d1 = ld(dm[1] + gi), d2 = ld(dm[2] + gi), d3 = ld(dm[3] + gi),
+           d4 = ld(dm[4] + gi);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
         const float dvx = at(t.dvx_dx, j), dvz = at(t.dvz_dz, j);
@@ -406,7 +415,7 @@ __device__ __forceinline__ void imaging_accumulate(float* const dm[5], long long
 // epilogues, sparse extraction.  NTHR threads of the CTA take part (every one
 // reaches the same barriers); scratch: >= 5*TX*TZ floats of shared memory that
 // the stencils no longer need.
-template <int DIR, int EPI, int F0, int F1, int NTHR, class Old, bool FS = false>
+template <int DIR, int EPI, int F0, int F1, int NTHR, class Old, bool FS = false, bool COH = false>
 __device__ __forceinline__ void step_tail(const StepArgs& a, float* scratch, int tile, int tid, int tzi, int txi,
                                           int gz, int gx, bool valid, long long gi, float4 (&t)[5], Old oload,
                                           const float4 (&csave)[2])
@@ -437,8 +446,8 @@ __device__ __forceinline__ void step_tail(const StepArgs& a, float* scratch, int
             const bool right = a.sw1 != 0.f;
 #pragma unroll
             for (int f = F0; f < F1; f++) {
-                const float4 l = ldg4(a.ssL[f] + gi);
-                const float4 r = right ? ldg4(a.ssR[f] + gi) : make_float4(0.f, 0.f, 0.f, 0.f);
+                const float4 l = ldw4<COH>(a.ssL[f] + gi);
+                const float4 r = right ? ldw4<COH>(a.ssR[f] + gi) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
                 for (int j = 0; j < 4; j++) at(t[f], j) += at(l, j) * a.sw0 + at(r, j) * a.sw1;
             }
@@ -551,7 +560,8 @@ __device__ __forceinline__ void step_tail(const StepArgs& a, float* scratch, int
             } else {
 #pragma unroll
                 for (int f = F0; f < F1; f++) {
-                    smp[f] = tri_sample(a.tmode, osave[f], ld4(a.c[f] + gi), t[f], a.tw_o, a.tw_c, a.tw_n);
+                    smp[f] = tri_sample(a.tmode, osave[f], COH ? ldcg4(a.c[f] + gi) : ld4(a.c[f] + gi), t[f],
+                                        a.tw_o, a.tw_c, a.tw_n);
                     if (!IMG) st4(a.eL[f] + gi, smp[f]);
                 }
             }
@@ -602,7 +612,7 @@ __device__ __forceinline__ void step_tail(const StepArgs& a, float* scratch, int
         __syncthreads();
         if (valid) {
             const ImgTerms it = imaging_terms<Q>(a.wh, scratch, FAT + txi, FAT + 4 * tzi, gi, a.img_its, a.cz, a.cx);
-            imaging_accumulate(a.img, gi, smp, it, a.dts_inv);
+            imaging_accumulate<COH>(a.img, gi, smp, it, a.dts_inv);
         }
     }
 }
@@ -670,7 +680,7 @@ __device__ __forceinline__ void pdl_begin(const StepArgs& a, long long gi, bool 
 
 // Stage the current level (forward) or its scaled combinations (adjoint) of
 // tile (z0, x0) with its 4-cell halo into sm [5][SX][SZ]; NTHR threads.
-template <int DIR, int NTHR, bool FS = false>
+template <int DIR, int NTHR, bool FS = false, bool COH = false>
 __device__ __forceinline__ void stage_tile(const StepArgs& a, float* sm, int z0, int x0, int tid)
 {
     const int nz = a.nz;
@@ -688,7 +698,7 @@ __device__ __forceinline__ void stage_tile(const StepArgs& a, float* sm, int z0,
             if (q < NU && gz < nz) {
                 const long long gi = (long long)gx * nz + gz;
 #pragma unroll
-                for (int f = 0; f < 5; f++) v[r][f] = ldg4(a.c[f] + gi);
+                for (int f = 0; f < 5; f++) v[r][f] = ldw4<COH>(a.c[f] + gi);
             } else {
 #pragma unroll
                 for (int f = 0; f < 5; f++) v[r][f] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -712,11 +722,11 @@ __device__ __forceinline__ void stage_tile(const StepArgs& a, float* sm, int z0,
             const long long gi = (long long)gx * nz + gz;
             if (DIR == 0) {
 #pragma unroll
-                for (int f = 0; f < 5; f++) v[f] = ldg4(a.c[f] + gi);
+                for (int f = 0; f < 5; f++) v[f] = ldw4<COH>(a.c[f] + gi);
             } else {
-                const float4 sxx = ldg4(a.c[2] + gi);
-                adj_products(ldg4(a.c[0] + gi), ldg4(a.c[1] + gi), sxx, ldg4(a.c[3] + gi),
-                             ldg4(a.c[4] + gi), ldg4(a.par[0] + gi), ldg4(a.par[1] + gi), ldg4(a.par[2] + gi),
+                const float4 sxx = ldw4<COH>(a.c[2] + gi);
+                adj_products(ldw4<COH>(a.c[0] + gi), ldw4<COH>(a.c[1] + gi), sxx, ldw4<COH>(a.c[3] + gi),
+                             ldw4<COH>(a.c[4] + gi), ldg4(a.par[0] + gi), ldg4(a.par[1] + gi), ldg4(a.par[2] + gi),
                              ldg4(a.par[3] + gi), ldg4(a.par[4] + gi), v);
                 if (FS && a.fs && gz <= SURF) {
                     // free surface: only what the forward update uses (see fs_forward_rows)
@@ -748,11 +758,12 @@ __device__ __forceinline__ void stage_tile(const StepArgs& a, float* sm, int z0,
 // The current level (forward) or its scaled combinations (adjoint) are staged
 // with plain loads; the old level and the medium are read from global memory.
 // MINB CTAs per SM (3: <= 80 registers, 4: <= 64).
-template <int DIR, int EPI, int MINB, bool FS>
-__device__ __forceinline__ void step_body(const StepArgs& a, int tile)
+// COH: the persistent time loop (eio_wave.cuh), where other CTAs of the same
+// launch write the wavefields: no programmatic-dependent-launch handshake, and
+// every wavefield read goes through L2 (ldcg4).
+template <int DIR, int EPI, int MINB, bool FS, bool COH = false>
+__device__ __forceinline__ void step_body_sm(const StepArgs& a, int tile, float* sm)
 {
-    __shared__ __align__(16) float sm[5 * SMEM_FIELD];
-
     const int tid = threadIdx.x;
     const int bz = tile % a.ntz, bx = tile / a.ntz;
     const int z0 = FAT + bz * TZ, x0 = FAT + bx * TX;
@@ -765,15 +776,16 @@ __device__ __forceinline__ void step_body(const StepArgs& a, int tile)
     const bool valid = gz < nz - FAT;
     const long long gi = (long long)gx * nz + gz;
 
-    pdl_begin(a, gi, valid);
-    stage_tile<DIR, NT, FS>(a, sm, z0, x0, tid);
+    if (!COH) pdl_begin(a, gi, valid);
+    stage_tile<DIR, NT, FS, COH>(a, sm, z0, x0, tid);
     // with 3 CTAs per SM the old level is loaded here, its latency hidden
     // behind the barrier and the stencils
     constexpr bool HOIST = MINB == 3 && !FS;
+    auto ldo = [&](int f) { return COH ? ldcg4(a.o[f] + gi) : ld4(a.o[f] + gi); };
     float4 oreg[5];
     if (HOIST) {
 #pragma unroll
-        for (int f = 0; f < 5; f++) oreg[f] = valid ? ld4(a.o[f] + gi) : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int f = 0; f < 5; f++) oreg[f] = valid ? ldo(f) : make_float4(0.f, 0.f, 0.f, 0.f);
     }
     __syncthreads();
 
@@ -787,8 +799,16 @@ __device__ __forceinline__ void step_body(const StepArgs& a, int tile)
         csave[0] = ld4(sm + lx * SZ + lz);
         csave[1] = ld4(sm + SMEM_FIELD + lx * SZ + lz);
     }
-    auto old = [&](int f) { return HOIST ? oreg[f] : ld4(a.o[f] + gi); };
-    step_tail<DIR, EPI, 0, 5, NT, decltype(old), FS>(a, sm, tile, tid, tzi, txi, gz, gx, valid, gi, t, old, csave);
+    auto old = [&](int f) { return HOIST ? oreg[f] : ldo(f); };
+    step_tail<DIR, EPI, 0, 5, NT, decltype(old), FS, COH>(a, sm, tile, tid, tzi, txi, gz, gx, valid, gi, t, old,
+                                                          csave);
+}
+
+template <int DIR, int EPI, int MINB, bool FS>
+__device__ __forceinline__ void step_body(const StepArgs& a, int tile)
+{
+    __shared__ __align__(16) float sm[5 * SMEM_FIELD];
+    step_body_sm<DIR, EPI, MINB, FS>(a, tile, sm);
 }
 
 template <int DIR, int EPI, int MINB = 3, bool FS = false>
@@ -880,23 +900,25 @@ struct ImagingArgs {
 // coarse sample its.  64x16-cell tiles, 256 threads (one float4 of z x one column
 // each); the snapshot at its is staged with its 4-cell halo in shared memory for
 // the staggered derivatives, the neighbouring snapshots give the time difference.
+// sm: >= 2 * SMEM_FIELD floats of shared memory.  Every thread returns
+// through the end (no barrier after the early exit of the threads past the grid).
 template <int ADJ, int Q>
-__device__ __forceinline__ void imaging_body(const ImagingArgs& a, int tile)
+__device__ __forceinline__ void imaging_body_sm(const ImagingArgs& a, int tile, float* sm, int its,
+                                                float* const* ss)
 {
-    __shared__ __align__(16) float sm[2 * SMEM_FIELD];
     const int tid = threadIdx.x;
     const int ntz = (a.nz - 2 * FAT + TZ - 1) / TZ;
     const int bz = tile % ntz, bx = tile / ntz;
     const int z0 = FAT + bz * TZ, x0 = FAT + bx * TX;
     const long long nz = a.nz;
-    stage_snapshot<Q>(a.h, a.its, a.nz, sm, z0, x0, tid);
+    stage_snapshot<Q>(a.h, its, a.nz, sm, z0, x0, tid);
     __syncthreads();
     const int tzi = tid % NTZ, txi = tid / NTZ;
     const int lz = FAT + 4 * tzi, lx = FAT + txi;
     const int gz = z0 + 4 * tzi;
     if (gz >= a.nz - FAT) return;
     const long long gi = (long long)(x0 + txi) * nz + gz;
-    const ImgTerms t = imaging_terms<Q>(a.h, sm, lx, lz, gi, a.its, a.cz, a.cx);
+    const ImgTerms t = imaging_terms<Q>(a.h, sm, lx, lz, gi, its, a.cz, a.cx);
     if (!ADJ) {
         const float4 d0 = ldg4(a.dm[0] + gi), d1 = ldg4(a.dm[1] + gi), dl = ldg4(a.dm[2] + gi),
                      du = ldg4(a.dm[3] + gi), d4 = ldg4(a.dm[4] + gi);
@@ -910,13 +932,20 @@ __device__ __forceinline__ void imaging_body(const ImagingArgs& a, int tile)
             at(s3, j) = at(dl, j) * (dvx + dvz) + 2.0f * at(du, j) * dvz;
             at(s4, j) = at(d4, j) * (at(t.dvx_dz, j) + at(t.dvz_dx, j));
         }
-        st4(a.ss[0] + gi, s0); st4(a.ss[1] + gi, s1); st4(a.ss[2] + gi, s2);
-        st4(a.ss[3] + gi, s3); st4(a.ss[4] + gi, s4);
+        st4(ss[0] + gi, s0); st4(ss[1] + gi, s1); st4(ss[2] + gi, s2);
+        st4(ss[3] + gi, s3); st4(ss[4] + gi, s4);
     } else {
-        const float4 s[5] = {ldg4(a.ss[0] + gi), ldg4(a.ss[1] + gi), ldg4(a.ss[2] + gi), ldg4(a.ss[3] + gi),
-                             ldg4(a.ss[4] + gi)};
+        const float4 s[5] = {ldg4(ss[0] + gi), ldg4(ss[1] + gi), ldg4(ss[2] + gi), ldg4(ss[3] + gi),
+                             ldg4(ss[4] + gi)};
         imaging_accumulate(a.dm, gi, s, t, a.dts_inv);
     }
+}
+
+template <int ADJ, int Q>
+__device__ __forceinline__ void imaging_body(const ImagingArgs& a, int tile)
+{
+    __shared__ __align__(16) float sm[2 * SMEM_FIELD];
+    imaging_body_sm<ADJ, Q>(a, tile, sm, a.its, a.ss);
 }
 
 template <int ADJ, int Q>

@@ -278,11 +278,23 @@ class _ElasticOp:
         check(self._L.eio_ctx_set_lanes(self._ctx, int(lanes)))
 
     def setShotBatch(self, shots):
-        """Advance up to ``shots`` (1 .. 8, default 8) shots in lockstep with one
-        step launch for all of them (the nonlinear operators; the Born operators
-        in groups as wide as the device memory holds their histories); 1 runs
-        the shots one at a time on the lanes."""
+        """Nonlinear operators: advance up to ``shots`` (1 .. 8, default 8) shots
+        in lockstep with one step launch for all of them; 1 runs the shots one
+        at a time on the lanes."""
         check(self._L.eio_ctx_set_shot_batch(self._ctx, int(shots)))
+
+    def setBornBatch(self, shots):
+        """Born operators: run the shots in lockstep groups of up to ``shots``
+        (1 .. 8, capped by the lanes and the device memory); default 1, the
+        shots one at a time on the lanes."""
+        check(self._L.eio_ctx_set_born_batch(self._ctx, int(shots)))
+
+    def setPersistent(self, mask):
+        """Shot groups of the Born operators: the propagation phases that run
+        every fine step in one persistent launch (bits: 1 source wavefield, 2
+        scattered wavefield, 4 adjoint; True = 7, False = 0 = one launch per step)."""
+        mask = 7 if mask is True else 0 if mask is False else int(mask)
+        check(self._L.eio_ctx_set_persistent(self._ctx, mask))
 
     def getMedium(self):
         n = self.fd.nz * self.fd.nx

@@ -162,6 +162,21 @@ int eio_ctx_autotune(eio_ctx *c, int *kind, int *tz, int *cw, int *cpr);
  * (2^20); 0 makes every pipeline wait give up at once (used by the tests of
  * the timeout path). */
 int eio_ctx_set_wait_limit(eio_ctx *c, long long polls);
+/* Persistent time loop (no reference counterpart; the reference launches 4-12
+ * kernels per fine step, BornElasticGpuFunctions.cu:744-849): the shot groups
+ * of the Born operators (eio_ctx_set_born_batch) run every fine step of a
+ * propagation phase in one cooperative launch, the CTAs advancing tile by tile
+ * behind per-tile step counters instead of a grid-wide boundary per step, the
+ * forward's secondary sources computed per tile inside the loop.  Results are
+ * bitwise those of the per-step launches.  A tile whose neighbours do not
+ * arrive within 4 x the wait limit (eio_ctx_set_wait_limit) polls sets the
+ * error flag and the call fails with EIO_ERR_TIMEOUT.  mask: the phases that
+ * run as persistent loops, 1 the source wavefield, 2 the Born forward's
+ * scattered wavefield, 4 the Born adjoint; 0 (default) launches per step, which
+ * measured faster on the 600x1800 benchmark (the per-tile completion fence and
+ * neighbour polls cost more than the launch boundaries they remove). */
+int eio_ctx_set_persistent(eio_ctx *c, int mask);
+int eio_ctx_get_persistent(const eio_ctx *c, int *mask);
 int eio_ctx_get_wait_limit(const eio_ctx *c, long long *polls);
 /* Instrumentation (no reference counterpart): kernel launch counters and,
  * when enabled, CUDA-event timing of every 16th fused step-kernel launch;
@@ -173,23 +188,28 @@ int eio_ctx_stats(eio_ctx *c, int enable, int reset, long long *launches, long l
  * summed over the lanes (a launch that advances several shots counts each
  * shot's interior cells); call it before eio_ctx_stats resets the counters. */
 int eio_ctx_step_cells(const eio_ctx *c, long long *cells);
-/* Shot batching (no reference counterpart; the reference runs one shot per GPU
- * at a time, BornElasticShotsGpu.cpp:178-207): with shots > 1 (default 8) the
- * multi-shot operators advance up to `shots` (<= 8) shots in lockstep, one
- * engine each, with one step launch per fine step for all of them.  The
- * launch orders the shots of a tile next to each other and every shot reads
- * one copy of the medium, so a medium tile comes from HBM once per step for
- * the whole group.  eio_nl_forward / eio_nl_adjoint: each shot on its own
- * window and point lists; not used with the free surface or when a wavefield
- * is saved.  eio_born_forward / eio_born_adjoint / eio_born_shots_dev: groups
- * of as many shots as the free device memory holds (each needs its own
- * source-wavefield history), sizes as even as possible, the imaging of a
- * group in one launch per coarse sample; used with sub = 1 and FP32
- * histories, otherwise the lanes run the shots.  Per-shot traces equal the
- * one-shot propagation with the tile kernel (kind 3) bit for bit; the Born
- * image adds the shots in another order (each shot of a group into its own
- * buffer).  1 runs the shots one at a time on the lanes. */
+/* Shot batching of the nonlinear operators (no reference counterpart; the
+ * reference runs one shot per GPU at a time, nonlinearPropElasticShotsGpu.cpp:80-422):
+ * with shots > 1 (default 8), eio_nl_forward and eio_nl_adjoint advance up to
+ * `shots` (<= 8) shots in lockstep, one engine each, with one step launch per
+ * fine step for all of them (the shots of a tile next to each other in the
+ * launch, every shot reading one copy of the medium; each shot on its own
+ * window and point lists); 1 runs the shots one at a time on the lanes.
+ * Results equal the one-shot propagation with the tile kernel bit for bit.
+ * Not used with the free surface or when a wavefield is saved. */
 int eio_ctx_set_shot_batch(eio_ctx *c, int shots);
+/* Shot batching of the Born operators (eio_born_forward / eio_born_adjoint /
+ * eio_born_shots_dev; no reference counterpart, BornElasticShotsGpu.cpp:178-207
+ * runs one shot per GPU): with shots > 1 the shots of a call run in groups of
+ * up to min(shots, lanes) that the free device memory holds (each shot needs
+ * its own source-wavefield history), sizes as even as possible, one engine per
+ * shot, one step launch per fine step for the group and the imaging of the
+ * group in one launch per coarse sample (sub = 1 and FP32 histories; otherwise
+ * the lanes run the shots).  Per-shot traces equal the one-shot propagation
+ * with the tile kernel (kind 3) bit for bit; the image adds the shots in
+ * another order.  Default 1 (the shots on the lanes): on the 600x1800 Born
+ * benchmark two concurrent lanes measured faster than groups of 2-5. */
+int eio_ctx_set_born_batch(eio_ctx *c, int shots);
 /* Shot lanes (no reference counterpart; the reference runs one shot per GPU at
  * a time). The multi-shot operators (eio_nl_forward/adjoint,
  * eio_born_forward/adjoint, eio_born_shots_dev) run their shots on up to

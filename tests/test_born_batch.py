@@ -1,5 +1,5 @@
-"""Born operators with shots in lockstep (eio_ctx_set_shot_batch > 1, the
-default): the shots of a call run in groups, one k_step_shots launch per fine
+"""Born operators with shots in lockstep (eio_ctx_set_born_batch > 1): the
+shots of a call run in groups, one k_step_shots launch per fine
 step for every shot of a group (the shots of a tile next to each other, one
 copy of the medium), the imaging of a group's shots in one launch.
 
@@ -26,7 +26,7 @@ TOL32 = 1e-5
 def _ops(w, batch):
     src, rec = w.geometry()
     born = prop.BornElasticShotsGpu(w.elastic, w.par, [w.source_signal()], *src, *rec)
-    born.setShotBatch(batch)
+    born.setBornBatch(batch)
     born.setLanes(3)
     _lib.check(born._L.eio_ctx_set_kernel(born.ctx, 3, 64, 16, 0))
     return born
@@ -77,7 +77,7 @@ def test_batched_born_with_cropped_shots():
     for batch in (1, 2):
         src, rec = TW._geometry(w, w.elastic, src_x, recs, [0, 1])
         born = prop.BornElasticShotsGpu(w.elastic, w.par, [w.source_signal()], *src, *rec)
-        born.setShotBatch(batch)
+        born.setBornBatch(batch)
         born.setShotWindows([24, 104], [88, 120])
         _lib.check(born._L.eio_ctx_set_kernel(born.ctx, 3, 64, 16, 0))
         dm = born.modelSpace()
@@ -144,3 +144,28 @@ def test_batched_born_device_entry_matches_oracle():
         orc.born_prop(1, r["g"], r["med"], r["fine"], want, d_in, r["sp"], r["rp"])
     got = np.concatenate([t.cpu().numpy().ravel() for t in grad5])
     assert O.rel_l2(got, np.concatenate([x.ravel() for x in want])) < TOL32
+
+
+@pytest.mark.parametrize("nshots,batch", [(3, 3), (5, 2)])
+def test_persistent_time_loop_equals_per_step_launches(nshots, batch):
+    """The shot groups' persistent loop (one launch per propagation phase, tiles
+    advancing behind per-tile step counters, secondary sources computed per
+    tile) gives the bits of the per-step launches, forward and adjoint."""
+    w = synthetic.small(nts=90, nshots=nshots)
+    out = []
+    for persistent in (0, 7):
+        op = _ops(w, batch)
+        op.setPersistent(persistent)
+        dm = op.modelSpace()
+        dm.getNdArray()[...] = w.extra["dmodel"]
+        d = op.dataSpace()
+        op.forward(False, dm, d)
+        rng = np.random.default_rng(7)
+        dd = op.dataSpace()
+        dd.getNdArray()[...] = rng.standard_normal(dd.getNdArray().shape).astype(np.float32)
+        g = op.modelSpace()
+        op.adjoint(False, g, dd)
+        out.append((d.getNdArray().copy(), g.getNdArray().copy()))
+    assert np.abs(out[0][0]).max() > 0
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
