@@ -35,6 +35,28 @@ BYTES_PER_CELL = 80.0    # read 5 current + 5 old + 5 medium, write 5 new (FP32)
 PAIR_BYTES_PER_CELL = 100.0   # two steps per launch: read 5 current + 5 old + 5 medium, write 2 x 5 new
 
 
+def born_pair_bytes(cells, fine_steps, nts):
+    """Algorithmic bytes of one shot's Born forward + adjoint (FP32 source
+    history, two fine steps per coarse sample): the four propagations (source
+    wavefield in both calls, scattered wavefield, adjoint wavefield) at 80 B
+    per cell update, plus per coarse sample and cell the history written twice
+    (Vx, Vz: 2 x 8 B), the forward imaging (3 history samples 24 B, the
+    perturbation 20 B, the secondary sources written 20 B), the scattered steps
+    reading the secondary sources (3 x 20 B: the left sample on both fine
+    steps, the right one on the second), and the adjoint imaging (3 history
+    samples 24 B, read-modify-write of the five images 40 B)."""
+    return cells * (4 * BYTES_PER_CELL * fine_steps + (16 + 64 + 60 + 64) * nts)
+
+
+def shot_gradient_bytes(cells, fine_steps, nts, propagations=2):
+    """Algorithmic bytes of one FWI shot gradient: the propagations at 80 B per
+    cell update (2 fused: the nonlinear forward recording the source wavefield
+    and the Born adjoint; 3 unfused), plus per coarse sample and cell the 16-bit
+    snapshot written and read (4 + 4 B) and the read-modify-write of the five
+    FP32 images (40 B)."""
+    return cells * (propagations * BYTES_PER_CELL * fine_steps + (4 + 4 + 40) * nts)
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -61,6 +83,8 @@ def parse():
     ap.add_argument("--nts", type=int, default=4000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fwi", action="store_true",
+                    help="born_600x1800: skip the bounded FWI-gradient sample (the 'fwi' keys of the line)")
     ap.add_argument("--graphs", action="store_true", help="run the time loops as CUDA graphs (off by default)")
     ap.add_argument("--fwi-unfused", action="store_true",
                     help="fwi_1000x3400: nonlinear forward + Born adjoint (3 propagations per shot) instead of "
@@ -429,11 +453,13 @@ def run_ours(args, ws, rank, local):
                    "shot_lanes": lanes_used(L, ctx),
                    "l2": "inputs larger than L2 (34.6 GB FP32 source-wavefield history per shot) and a 256 MB "
                          "L2 flush between timed steps"},
-        "shot_gradients_per_s": round(ws * nsh * args.steps / (t_ms * 1e-3), 4),
-        # (algorithmic bytes of one shot's Born forward + adjoint: 4 propagations at 80 B per cell
-        # update) / measured HBM peak / measured time per shot gradient
-        "shot_gradients_roofline_frac": round(
-            (4.0 * fine_steps * cells * BYTES_PER_CELL / (peak * 1e9)) / ((t_ms * 1e-3) / (ws * nsh * args.steps)), 4),
+        # Born forward + adjoint pairs of one shot per second, and their algorithmic bytes
+        # (born_pair_bytes) over the measured HBM peak per measured time of a pair
+        "born_pairs_per_s": round(ws * nsh * args.steps / (t_ms * 1e-3), 4),
+        "born_pair_bytes": born_pair_bytes(cells, fine_steps, w.nts),
+        "born_pair_roofline_frac": round(
+            (born_pair_bytes(cells, fine_steps, w.nts) / (peak * 1e9)) / ((t_ms * 1e-3) / (ws * nsh * args.steps)),
+            4),
         "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
         "gpu_launches": st["launches"],
     }
@@ -491,12 +517,21 @@ def run_reference(args, ws, rank, local):
     w = synthetic.born_600x1800(nts=args.nts, nshots=1, seed=2024)
     if not O.RefGpu.available("f"):
         return run_reference_port(args, w, "oracle/_ref not built (reference tree absent at build time)")
+    import torch
+    if not torch.cuda.is_available():
+        return run_reference_port(args, w, "no CUDA device on this machine")
+    sample_note = ""
     if not O.RefGpu.born_supported(O.Case.from_workload(w).grid()):
-        return run_reference_port(
-            args, w, "the reference Born drivers index their Vx/Vz history with the 32-bit product its*nz*nx "
-                     "(kernelsGpuElastic.cu:1342), which overflows for nts*nz*nx >= 2^31 (here 4000*600*1800); "
-                     "on this grid they faulted with an illegal memory access at BornElasticGpuFunctions.cu:763, "
-                     "so they are not run again")
+        # The reference's Born drivers index their Vx/Vz history with the 32-bit product
+        # its*nz*nx (kernelsGpuElastic.cu:1342), which overflows for nts*nz*nx >= 2^31 (here
+        # 4000*600*1800; on this grid they faulted with an illegal memory access at
+        # BornElasticGpuFunctions.cu:763 and are not run at that length again).  The bounded
+        # sample is the same grid, shot and perturbation with the record cut to the longest
+        # their index admits, nts = 1900 (1900*600*1800 < 2^31); Gcell-updates/s is per cell
+        # update, so the record length does not enter the comparison.
+        w = synthetic.born_600x1800(nts=1900, nshots=1, seed=2024)
+        sample_note = ("; record cut from nts=%d to nts=1900, the longest the reference's 32-bit history "
+                       "index admits on this grid (its*nz*nx < 2^31, kernelsGpuElastic.cu:1342)" % args.nts)
     orc = O.Oracle("f")
     c = O.Case.from_workload(w)
     g = c.grid()
@@ -526,10 +561,13 @@ def run_reference(args, ws, rank, local):
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * dt / args.steps, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "born_600x1800: Born forward + adjoint, 1 shot per step (bounded sample of the "
-                                   "10-shot workload), nts=%d" % g["nts"], "nz": g["nz"], "nx": g["nx"]},
+                                   "10-shot workload), nts=%d%s" % (g["nts"], sample_note), "nz": g["nz"],
+                       "nx": g["nx"], "nts": g["nts"]},
             "cpu_baseline": {"value": round(v, 3), "unit": "Gcell-updates/s", "cores": 1, "kind": "reference",
-                             "sample": "reference CUDA drivers (elastic_iso_float, built for sm_100a) on the B200; "
-                                       "the reference has no CPU implementation of this path"},
+                             "sample": "reference CUDA drivers (elastic_iso_float, built for sm_100a) on the B200, "
+                                       "1 shot of the 600x1800 grid, nts=%d, each call a full init/alloc/propagate/"
+                                       "free as BornElasticGpu::forward/adjoint; the reference has no CPU "
+                                       "implementation of this path" % g["nts"]},
             "e2e": {"value": round(v, 3), "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 
@@ -775,6 +813,10 @@ def run_ours_fwi(args, ws, rank, local):
     t_ms = max_over_ranks(ws, t_ms)
     value = ws * updates * args.steps / (t_ms * 1e-3) / 1e9
     peak, pk = measured_peak()
+    sg_per_s = ws * nsh * args.steps / (t_ms * 1e-3)
+    # algorithmic bytes of the mean shot gradient (each shot on its own window)
+    sg_bytes = float(np.mean([shot_gradient_bytes((w.nz - 8) * (int(n) - 8), fine_steps, w.nts, props)
+                              for n in nxw]))
     n_data = int(np.prod(d_obs.getNdArray().shape))
     # model (forward and Born background, or the one fused background), residual
     h2d = 4 * (3 * w.nz * w.nx) * (1 if obj.fused else 2) + 4 * n_data
@@ -792,7 +834,9 @@ def run_ours_fwi(args, ws, rank, local):
                        "shots_per_gpu": nsh, "shot_lanes": lanes_used(L, born.ctx),
                        "cell_updates_per_step": updates * ws,
                        "l2": "inputs larger than L2 (BF16 history of a window: several GB per shot)"},
-            "shot_gradients_per_s": round(ws * nsh * args.steps / (t_ms * 1e-3), 4),
+            "shot_gradients_per_s": round(sg_per_s, 4),
+            "shot_gradient_bytes": sg_bytes,
+            "shot_gradient_roofline_frac": round(sg_bytes / (peak * 1e9) * sg_per_s, 4),
             "e2e": {"value": round(value, 3), "unit": "Gcell-updates/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "note": "the operator API with host buffers is the only path"},
             "roofline": {"bound": "hbm", "achieved": round(BYTES_PER_CELL * value, 1), "peak": peak, "unit": "GB/s",
@@ -1077,6 +1121,28 @@ def run_ours_nl_shots(args, ws, rank, local):
             "cpu_baseline": None, "clocks": clk, "gpu_launches": int(read_stats(L, nl.ctx)["launches"])}
 
 
+def fwi_sample(args, ws, rank, local):
+    """A bounded FWI-gradient measurement beside the default Born line: the
+    batched-FWI case (1000x3400, nts = 5000, cropped shots of uneven 2-8 km
+    windows, BF16 source-wavefield checkpoints, fused gradient), 8 of its 120
+    shots per GPU, 1 warm-up and 2 timed steps whatever --steps says."""
+    import copy
+    import gc
+    import torch
+    gc.collect()
+    torch.cuda.empty_cache()
+    a = copy.copy(args)
+    a.shots, a.steps, a.warmup, a.fwi_unfused = 8, 2, 1, False
+    r = run_ours_fwi(a, ws, rank, local)
+    return {"metric": "shot-gradients/s", "value": r["shot_gradients_per_s"], "unit": "shot-gradients/s",
+            "roofline_frac": r["shot_gradient_roofline_frac"], "bytes_per_shot_gradient": r["shot_gradient_bytes"],
+            "gcell_updates_per_s": r["value"], "ms_per_step": r["ms_per_step"], "steps": a.steps, "warmup": a.warmup,
+            "workload": r["config"]["workload"], "shot_lanes": r["config"]["shot_lanes"],
+            "peak": r["roofline"]["peak"], "clocks": r["clocks"],
+            "basis": "per shot gradient: 2 propagations x 80 B x window cells x fine steps + window cells x nts x "
+                     "(4 B BF16 snapshot write + 4 B read + 40 B image read-modify-write)"}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -1098,6 +1164,8 @@ def main():
         out = run_ours_cnn(args, ws, rank, local)
     else:
         out = run_ours(args, ws, rank, local)
+        if not args.no_fwi:
+            out["fwi"] = fwi_sample(args, ws, rank, local)
     if rank == 0:
         print(json.dumps(out))
     if ws > 1:
