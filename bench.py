@@ -74,7 +74,10 @@ def parse():
                     help="cnn_train: forward convolutions on mma.sync (0) or tcgen05 (1); "
                          "-1 keeps the library default (mma.sync)")
     ap.add_argument("--epochs", type=int, default=80, help="fwi_learned: training epochs")
-    ap.add_argument("--depth", type=int, default=6, help="fwi_learned: convolution layers of the network")
+    ap.add_argument("--depth", type=int, default=6, help="fwi_learned: convolution layers of the ConvNet")
+    ap.add_argument("--net", default=None, choices=["unet", "convnet"],
+                    help="preconditioner network: the four-level U-Net (cnn_train default) or the plain ConvNet "
+                         "(fwi_learned default)")
     ap.add_argument("--sigma", type=float, default=3.0,
                     help="fwi_learned: smoothing length (cells) of the training perturbations")
     ap.add_argument("--shots", type=int, default=None,
@@ -917,8 +920,9 @@ def run_ours_learned(args, ws, rank, local):
 
     def train():
         nonlocal P
-        P = precond.LearnedPreconditioner(born, m0, sigma=args.sigma, seed=0,
-                                          net=precond.ConvNet(depth=args.depth, device=local, seed=0))
+        net = (precond.UNet(device=local, seed=0) if args.net == "unet" else
+               precond.ConvNet(depth=args.depth, device=local, seed=0))
+        P = precond.LearnedPreconditioner(born, m0, sigma=args.sigma, seed=0, net=net)
         X, T, _, _ = P.make_pairs(args.pairs, seed=1)
         P.train(X, T, epochs=args.epochs, batch=8, lr=3e-3)
 
@@ -990,12 +994,35 @@ def cnn_step_flops(chans, npix):
     return float(npix) * (2 * sum(per) + sum(per[1:]))
 
 
+def unet_step_cost(chans, levels, batch, h, w):
+    """(tensor-core FLOPs, algorithmic HBM bytes) of one U-Net training step.
+    FLOPs: forward, data gradient (all but the first layer) and weight
+    gradient of each 3x3 convolution, 2 * 9 * cin * cout per pixel of its
+    level.  Bytes: each BF16 activation read or written once per pass it
+    enters -- forward input + output; backward output gradient + ReLU mask +
+    input (weight gradient) and input gradient (data gradient) -- and the
+    pooling, upsampling and concatenation copies with their adjoints."""
+    fl, by = 0.0, 0.0
+    for k, ((ci, co), lv) in enumerate(zip(chans, levels)):
+        npx = batch * (h >> lv) * (w >> lv)
+        fl += 2.0 * 9 * ci * co * npx * (2 if k == 0 else 3)
+        by += 2.0 * npx * ((ci + co) + (2 * co + ci) + (0 if k == 0 else ci + co))
+    b = chans[0][1]
+    for lv, c in ((0, b), (1, 2 * b), (2, 4 * b)):
+        npx = batch * (h >> lv) * (w >> lv)
+        by += 2.0 * npx * c * (1.25 + 1.25)           # pooling (read 4, write 1 per 4) and its adjoint
+        by += 2.0 * npx * (3 * c) * 2 * 2             # upsampling + concatenation, their adjoints
+    return fl, by
+
+
 def run_ours_cnn(args, ws, rank, local):
     """Training throughput of the learned preconditioner's network: per step,
     forward, loss, data and weight gradients and the Adam update of a batch of
-    --shots 256 x 256 patches (4 features in 16 channels, 32 hidden, 6 layers)
-    through the library's kernels.  Inputs are resident on the device; each
-    step reads them fresh from a pool larger than L2."""
+    --shots 256 x 256 patches (4 features in 16 channels) through the
+    library's kernels -- the four-level U-Net (32 / 64 / 128 / 256 channels,
+    1.17 M parameters; every convolution an implicit GEMM on tcgen05) or, with
+    --net convnet, the 6-layer 32-channel ConvNet.  Inputs are resident on the
+    device; each step reads them fresh from a pool larger than L2."""
     import ctypes
     import torch
     from elastic_isotropic_operators_b200 import _lib, precond
@@ -1007,7 +1034,8 @@ def run_ours_cnn(args, ws, rank, local):
     _lib.check(_lib.lib().eio_cnn_get_conv_path(ctypes.byref(path)))
     batch = args.shots or 16
     h = w = 256
-    net = precond.ConvNet(depth=6, hidden=32, device=local, seed=0)
+    unet = (args.net or "unet") == "unet"
+    net = precond.UNet(device=local, seed=0) if unet else precond.ConvNet(depth=6, hidden=32, device=local, seed=0)
     g = torch.Generator(device=dev)
     g.manual_seed(1)
     pool = 4                                                  # 4 batches: 4 x 64 MB of BF16 inputs
@@ -1034,30 +1062,52 @@ def run_ours_cnn(args, ws, rank, local):
     torch.cuda.synchronize()
     clk = clocks.stop()
     t_ms = max_over_ranks(ws, e0.elapsed_time(e1))
-    depth = len(net.chans) - 1
-    launches_per_step = depth + 2 * depth + 2 * (depth - 1) + 2 + depth   # conv, wgrad+sum, flip+conv, mse+sum, adam
-    flops = cnn_step_flops(net.chans, batch * h * w)
+    if unet:
+        nl = len(net.chans)
+        # per conv: the forward GEMM; the ReLU adjoint (not the head), the weight-gradient GEMM and its split
+        # sum, the weight flip and the data-gradient GEMM (not the first layer); 3 poolings, 3 x (upsampling +
+        # concatenation), 3 x (concatenation adjoint + upsampling adjoint), 3 pooling adjoints; the loss and its
+        # sum; Adam per layer
+        launches_per_step = nl + (nl - 1) + 2 * nl + 2 * (nl - 1) + 3 + 6 + 6 + 3 + 2 + nl
+        flops, alg_bytes = unet_step_cost(net.chans, net._lvl(), batch, h, w)
+    else:
+        depth = len(net.chans) - 1
+        launches_per_step = depth + 2 * depth + 2 * (depth - 1) + 2 + depth   # conv, wgrad+sum, flip+conv, mse+sum, adam
+        flops, alg_bytes = cnn_step_flops(net.chans, batch * h * w), None
     tflops = flops * args.steps / (t_ms * 1e-3) / 1e12
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peak, pk = float(json.load(f)["bf16_tflops"]), "measured"
+            mp = json.load(f)
+            peak, pk, hbm = float(mp["bf16_tflops"]), "measured", float(mp["hbm_gbs"])
     except Exception:
-        peak, pk = 1590.0, "fallback"
+        peak, pk, hbm = 1590.0, "fallback", 6650.0
     samples = ws * batch * args.steps / (t_ms * 1e-3)
+    gbs = alg_bytes * args.steps / (t_ms * 1e-3) / 1e9 if alg_bytes else None
+    if gbs is not None and gbs / hbm > tflops / peak:
+        roof = {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s", "frac": round(gbs / hbm, 4)}
+    else:
+        roof = {"bound": "tensor", "achieved": round(tflops, 2), "peak": peak, "unit": "TFLOP/s",
+                "frac": round(tflops / peak, 4)}
+    if unet:
+        desc = ("cnn_train: %d patches of 256x256 per step, U-Net 32/64/128/256 channels (%d parameters), "
+                "2x2 average pooling, nearest upsampling, concatenated skips" % (batch, net.n_params()))
+        kern = "k_gemm_tc (tcgen05, TMEM accumulators; implicit 3x3 gathers) for forward, data and weight gradients"
+    else:
+        desc = "cnn_train: %d patches of 256x256 per step, 6 conv layers 16-32-32-32-32-32-16" % batch
+        kern = (("k_conv3_tc (tcgen05, TMEM accumulator)" if path.value == 1 else
+                 "k_conv3 (mma.sync m16n8k16)") + " + k_conv3_wgrad (mma.sync m16n8k16)")
     return {"metric": "preconditioner training throughput", "value": round(samples, 2), "unit": "patches/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_ms / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (FP32 accumulate)",
             "data": "synthetic", "loss": float(loss.item()),
-            "config": {"workload": "cnn_train: %d patches of 256x256 per step, 6 conv layers 16-32-32-32-32-32-16"
-                                   % batch, "l2": "inputs read from a pool of 4 batches (256 MB) larger than L2"},
+            "config": {"workload": desc, "l2": "inputs read from a pool of 4 batches (256 MB) larger than L2"},
             "e2e": {"value": round(samples, 2), "unit": "patches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
                     "note": "training consumes device-resident pairs that the Born operators produce"},
-            "roofline": {"bound": "tensor", "achieved": round(tflops, 2), "peak": peak, "unit": "TFLOP/s",
-                         "frac": round(tflops / peak, 4), "traffic": None, "peak_source": pk,
-                         "basis": "tensor-core FLOPs of a training step (forward, data and weight gradients) over "
-                                  "the timed region",
-                         "kernel": ("k_conv3_tc (tcgen05, TMEM accumulator)" if path.value == 1 else
-                                    "k_conv3 (mma.sync m16n8k16)") + " + k_conv3_wgrad (mma.sync m16n8k16)"},
+            "roofline": dict(roof, traffic=None, peak_source=pk, tensor_tflops=round(tflops, 2),
+                             tensor_frac=round(tflops / peak, 4), hbm_gbs=round(gbs, 1) if gbs else None,
+                             basis="tensor-core FLOPs of a training step (forward, data and weight gradients) and, "
+                                   "for the U-Net, its algorithmic activation bytes, over the timed region; the "
+                                   "bound is the larger fraction", kernel=kern),
             "cpu_baseline": None, "clocks": clk, "gpu_launches": int(launches_per_step * args.steps)}
 
 

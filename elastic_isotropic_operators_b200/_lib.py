@@ -104,6 +104,17 @@ _SIGS = {
     "eio_cnn_flip": (I, [I, I, P, P, P]),
     "eio_cnn_mse": (I, [ctypes.c_longlong, I, I, P, P, P, P, P, P]),
     "eio_cnn_adam": (I, [ctypes.c_longlong, P, P, P, P, F, F, F, F, I, P, P]),
+    "eio_gemm_bf16": (I, [ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong, P, ctypes.c_longlong, P,
+                          ctypes.c_longlong, P, P, P, I, I, P, P]),
+    "eio_gemm_set_wait_limit": (I, [ctypes.c_longlong]),
+    "eio_gemm_status": (I, [I, P]),
+    "eio_unet_conv3x3": (I, [I, I, I, I, I, P, P, P, P, I, P]),
+    "eio_unet_wgrad_scratch": (I, [I, I, I, I, I, P]),
+    "eio_unet_conv3x3_wgrad": (I, [I, I, I, I, I, P, P, P, P, ctypes.c_longlong, P]),
+    "eio_unet_flip": (I, [I, I, P, P, P]),
+    "eio_unet_resample": (I, [I, I, I, I, I, P, P, I, P]),
+    "eio_unet_concat": (I, [I, ctypes.c_longlong, I, I, P, I, P, I, P, P]),
+    "eio_unet_relu_adj": (I, [ctypes.c_longlong, P, P, P, I, P]),
     "eio_ctx_pair_stats": (I, [P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]),
     "eio_nl_fwd_reg": (I, [P, P, P, P, IP, P, IP]),
     "eio_nl_adj_reg": (I, [P, P, P, P, IP, P, IP]),

@@ -1721,3 +1721,46 @@ EIO_API int eio_cnn_adam(long long n, float* p, float* m, float* v, const float*
                          float eps, int step, void* pb, void* stream) {
     return guarded([&] { cnn_adam(n, p, m, v, g, lr, b1, b2, eps, step, pb, stream); });
 }
+
+// ---- U-Net preconditioner kernels ------------------------------------------
+EIO_API int eio_gemm_bf16(long long M, long long N, long long K, const void* A, long long lda, const void* B,
+                          long long ldb, float* C32, void* C16, const void* mask, int relu, int splits, float* scratch,
+                          void* stream) {
+    return guarded([&] { gemm_bf16(M, N, K, A, lda, B, ldb, C32, C16, mask, relu, splits, scratch, stream); });
+}
+EIO_API int eio_gemm_set_wait_limit(long long polls) {
+    return guarded([&] { gemm_set_wait_limit(polls); });
+}
+EIO_API int eio_gemm_status(int reset, int* err) {
+    return guarded([&] {
+        if (!err) throw Error(EIO_ERR_ARG, "null result");
+        *err = gemm_status(reset);
+    });
+}
+EIO_API int eio_unet_conv3x3(int n, int h, int w, int cin, int cout, const void* x, const void* wt, float* y32,
+                             void* y16, int relu, void* stream) {
+    return guarded([&] { unet_conv3x3(n, h, w, cin, cout, x, wt, y32, y16, relu, stream); });
+}
+EIO_API int eio_unet_wgrad_scratch(int n, int h, int w, int cin, int cout, long long* floats) {
+    return guarded([&] {
+        if (!floats) throw Error(EIO_ERR_ARG, "null result");
+        *floats = unet_wgrad_scratch(n, h, w, cin, cout);
+    });
+}
+EIO_API int eio_unet_conv3x3_wgrad(int n, int h, int w, int cin, int cout, const void* x, const void* dz, float* dw,
+                                   float* scratch, long long scratchFloats, void* stream) {
+    return guarded([&] { unet_conv3x3_wgrad(n, h, w, cin, cout, x, dz, dw, scratch, scratchFloats, stream); });
+}
+EIO_API int eio_unet_flip(int cout, int cin, const void* w, void* wf, void* stream) {
+    return guarded([&] { unet_flip(cout, cin, w, wf, stream); });
+}
+EIO_API int eio_unet_resample(int op, int n, int h, int w, int c, const void* in, void* out, int add, void* stream) {
+    return guarded([&] { unet_resample(op, n, h, w, c, in, out, add, stream); });
+}
+EIO_API int eio_unet_concat(int adj, long long pixels, int ca, int cb, void* a, int addA, void* b, int addB, void* z,
+                            void* stream) {
+    return guarded([&] { unet_concat(adj, pixels, ca, cb, a, addA, b, addB, z, stream); });
+}
+EIO_API int eio_unet_relu_adj(long long n, const void* src, const void* mask, void* dst, int add, void* stream) {
+    return guarded([&] { unet_relu_adj(n, src, mask, dst, add, stream); });
+}

@@ -157,4 +157,20 @@ void engine_nl_shot(Engine* e, int adj, float* const modelReg[5], const ShotGeom
                     float* dataIrreg, float* wfld = nullptr);
 void engine_born_host(Engine* e, int adj, float* const srcDtw[5], float* const dm[5], float* const data[5],
                       const ShotGeom& g);
+
+// U-Net layers (eio_gemm.cu)
+void gemm_bf16(long long M, long long N, long long K, const void* A, long long lda, const void* B, long long ldb,
+               float* C32, void* C16, const void* mask, int relu, int splits, float* scratch, void* stream);
+void gemm_set_wait_limit(long long polls);
+int gemm_status(int reset);
+void unet_conv3x3(int n, int h, int w, int cin, int cout, const void* x, const void* wt, float* y32, void* y16,
+                  int relu, void* stream);
+long long unet_wgrad_scratch(int n, int h, int w, int cin, int cout);
+void unet_conv3x3_wgrad(int n, int h, int w, int cin, int cout, const void* x, const void* dz, float* dw,
+                        float* scratch, long long scratch_floats, void* stream);
+void unet_flip(int cout, int cin, const void* w, void* wf, void* stream);
+void unet_resample(int op, int n, int h, int w, int c, const void* in, void* out, int add, void* stream);
+void unet_concat(int adj, long long pixels, int ca, int cb, void* a, int add_a, void* b, int add_b, void* z,
+                 void* stream);
+void unet_relu_adj(long long n, const void* src, const void* mask, void* dst, int add, void* stream);
 }  // namespace eio

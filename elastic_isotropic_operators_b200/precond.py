@@ -16,11 +16,16 @@ relative to the background scale (g_c * mean(m0_c)), divided by their RMS
 over the model, and an illumination map (the Born normal operator applied to
 a constant relative perturbation, normalised to a maximum of 1).  Targets:
 the relative perturbation dm_c / mean(m0_c) times K / RMS(features), K fixed
-on the training set so that the targets are O(1).  The network: 3x3
-convolutions 16 -> 32 -> ... -> 32 -> 16 (3 outputs used), ReLU between
-layers, no biases; BF16 weights and activations, FP32 accumulation, FP32
-master weights with Adam.  Every product runs in the library's kernels
-(``eio_cnn_*``); torch only holds the device memory and the stream.
+on the training set so that the targets are O(1).  Two networks, both with
+BF16 weights and activations, FP32 accumulation, FP32 master weights with
+Adam, no biases, 3 of 16 output channels used:
+  * ConvNet: a plain stack of 3x3 convolutions 16 -> 32 -> ... -> 32 -> 16
+    with ReLU between layers (``eio_cnn_*`` kernels);
+  * UNet: the four-level U-Net (32 / 64 / 128 / 256 channels, pooling,
+    upsampling, concatenated skips), every convolution an implicit GEMM on
+    tcgen05 (``eio_unet_*`` kernels); ``LearnedPreconditioner(arch="unet")``.
+Every product runs in the library's kernels; torch only holds the device
+memory and the stream.
 """
 import ctypes
 
@@ -29,7 +34,7 @@ import numpy as np
 from . import _lib
 from ._lib import check
 
-__all__ = ["ConvNet", "LearnedPreconditioner", "smooth_perturbation"]
+__all__ = ["ConvNet", "UNet", "unet_channels", "LearnedPreconditioner", "smooth_perturbation"]
 
 _CIN = 16    # input channels of the first layer (4 features used)
 _COUT = 16   # output channels of the last layer (3 used)
@@ -162,6 +167,239 @@ class ConvNet:
             self.wb[l].copy_(self.w32[l].to(torch.bfloat16))
 
 
+def unet_channels(base=32):
+    """(cin, cout) of the U-Net's eleven 3x3 convolutions: two per encoder level
+    (base, 2 base, 4 base channels), the bottleneck (8 base), one per decoder
+    level on the concatenation [upsampled, skip], and the head."""
+    b = base
+    return [(_CIN, b), (b, b), (b, 2 * b), (2 * b, 2 * b), (2 * b, 4 * b), (4 * b, 4 * b), (4 * b, 8 * b),
+            (8 * b + 4 * b, 4 * b), (4 * b + 2 * b, 2 * b), (2 * b + b, b), (b, _COUT)]
+
+
+class UNet:
+    """Four-level U-Net: 3x3 convolutions with ReLU, 2x2 average pooling down,
+    nearest 2x upsampling up, skip connections by concatenation; base 32 gives
+    channels 32 / 64 / 128 / 256 and 1.17 M parameters.  Input BF16 NHWC
+    [N][H][W][16] (the gradient's three channels and the illumination, as
+    ConvNet), output FP32 [N][H][W][16] (the first ``nout`` channels used); H
+    and W multiples of 8 (three poolings).
+
+    Every convolution is an implicit GEMM on the library's tcgen05 kernel
+    (eio_unet_conv3x3: the 3x3 neighbourhoods gathered by the GEMM's copy
+    loop) -- forward with the weights, data gradient with the flipped weights,
+    weight gradient (eio_unet_conv3x3_wgrad) with both operands read in place,
+    split over the pixels (fixed summation order).  Weights [Cout][9][Cin]:
+    FP32 master copies with Adam, BF16 working copies.  The same interface as
+    ConvNet (forward, backward, adam, weights, set_weights)."""
+
+    multiple = 8
+
+    def __init__(self, base=32, nin=4, nout=3, device=0, seed=0):
+        torch = _torch()
+        if base % 8 or base < 8 or not (1 <= nin <= _CIN) or not (1 <= nout <= _COUT):
+            raise ValueError("base a multiple of 8, 1 <= nin <= 16, 1 <= nout <= 16")
+        self.dev = torch.device("cuda", device)
+        self.nin, self.nout, self.base = nin, nout, base
+        self.chans = unet_channels(base)
+        rng = np.random.default_rng(seed)
+        self.w32, self.wb, self.wf, self.m, self.v, self.dw = [], [], [], [], [], []
+        last = len(self.chans) - 1
+        for l, (ci, co) in enumerate(self.chans):
+            fan = 9 * (nin if l == 0 else ci)
+            w = rng.standard_normal((co, 9, ci)) * np.sqrt(2.0 / fan)
+            if l == 0:
+                w[:, :, nin:] = 0.0
+            if l == last:
+                w *= 0.1
+                w[nout:] = 0.0
+            w32 = torch.tensor(w, dtype=torch.float32, device=self.dev)
+            self.w32.append(w32)
+            self.wb.append(w32.to(torch.bfloat16))
+            self.wf.append(torch.empty((ci, 9, co), dtype=torch.bfloat16, device=self.dev))
+            self.m.append(torch.zeros_like(w32))
+            self.v.append(torch.zeros_like(w32))
+            self.dw.append(torch.zeros_like(w32))
+        self.step = 0
+        self._shape = None
+        self._loss = torch.zeros(1, dtype=torch.float64, device=self.dev)
+        self._part = torch.zeros(1024, dtype=torch.float64, device=self.dev)
+
+    def n_params(self):
+        return int(sum(w.numel() for w in self.w32))
+
+    @staticmethod
+    def _lvl():
+        """Resolution level (0 = full) of each convolution."""
+        return [0, 0, 1, 1, 2, 2, 3, 2, 1, 0, 0]
+
+    def _buffers(self, n, h, w):
+        if self._shape == (n, h, w):
+            return
+        if h % 8 or w % 8:
+            raise ValueError("U-Net inputs need H and W multiples of 8 (got %d x %d)" % (h, w))
+        torch = _torch()
+        bf = torch.bfloat16
+        b = self.base
+        L = [(n, h, w), (n, h // 2, w // 2), (n, h // 4, w // 4), (n, h // 8, w // 8)]
+        spec = dict(e1a=(0, b), s1=(0, b), p1=(1, b), e2a=(1, 2 * b), s2=(1, 2 * b), p2=(2, 2 * b),
+                    e3a=(2, 4 * b), s3=(2, 4 * b), p3=(3, 4 * b), b=(3, 8 * b), u3=(2, 8 * b), c3=(2, 12 * b),
+                    d3=(2, 4 * b), u2=(1, 4 * b), c2=(1, 6 * b), d2=(1, 2 * b), u1=(0, 2 * b), c1=(0, 3 * b),
+                    d1=(0, b))
+        t = lambda lv, c: torch.empty(L[lv] + (c,), dtype=bf, device=self.dev)
+        self.a = {k: t(lv, c) for k, (lv, c) in spec.items()}     # activations
+        self.g = {k: t(lv, c) for k, (lv, c) in spec.items()}     # their gradients
+        self.g["y"] = t(0, _COUT)
+        self.levels = L
+        self.y32 = torch.empty(L[0] + (_COUT,), dtype=torch.float32, device=self.dev)
+        dzmax = max(n * (h >> lv) * (w >> lv) * co for lv, (ci, co) in zip(self._lvl(), self.chans))
+        self.dz = torch.empty(dzmax, dtype=bf, device=self.dev)
+        need = 1
+        for lv, (ci, co) in zip(self._lvl(), self.chans):
+            f = ctypes.c_longlong()
+            check(_lib.lib().eio_unet_wgrad_scratch(n, h >> lv, w >> lv, ci, co, ctypes.byref(f)))
+            need = max(need, f.value)
+        self.scratch = torch.empty(need, dtype=torch.float32, device=self.dev)
+        self._shape = (n, h, w)
+
+    def _stream(self):
+        return ctypes.c_void_p(_torch().cuda.current_stream(self.dev).cuda_stream)
+
+    def _npix(self, lv):
+        n, h, w = self.levels[lv]
+        return n * h * w
+
+    def _conv(self, k, x, lv, out16=None, out32=None, relu=1):
+        n, h, w = self.levels[lv]
+        ci, co = self.chans[k]
+        check(_lib.lib().eio_unet_conv3x3(n, h, w, ci, co, _p(x), _p(self.wb[k]),
+                                          _p(out32) if out32 is not None else None,
+                                          _p(out16) if out16 is not None else None, relu, self._stream()))
+
+    def _conv_back(self, k, x, lv, y, dy, dx):
+        """Layer k: input x, output y (post-ReLU; None for the head), its
+        gradient dy -> the weight gradient dw[k] and, when dx is given, the
+        input's gradient."""
+        L = _lib.lib()
+        st = self._stream()
+        n, h, w = self.levels[lv]
+        ci, co = self.chans[k]
+        if y is not None:
+            check(L.eio_unet_relu_adj(n * h * w * co, _p(dy), _p(y), _p(self.dz), 0, st))
+            dz = self.dz
+        else:
+            dz = dy
+        check(L.eio_unet_conv3x3_wgrad(n, h, w, ci, co, _p(x), _p(dz), _p(self.dw[k]), _p(self.scratch),
+                                       self.scratch.numel(), st))
+        if dx is not None:
+            check(L.eio_unet_flip(co, ci, _p(self.wb[k]), _p(self.wf[k]), st))
+            check(L.eio_unet_conv3x3(n, h, w, co, ci, _p(dz), _p(self.wf[k]), None, _p(dx), 0, st))
+
+    # ------------------------------------------------------------ passes
+    def forward(self, x):
+        """x: BF16 [N][H][W][16] (device) -> FP32 [N][H][W][16] (device)."""
+        torch = _torch()
+        n, h, w, c = x.shape
+        if c != _CIN or x.dtype != torch.bfloat16 or not x.is_contiguous() or x.device != self.dev:
+            raise ValueError("input must be a contiguous BF16 [N][H][W][%d] tensor on %s" % (_CIN, self.dev))
+        self._buffers(n, h, w)
+        L = _lib.lib()
+        st = self._stream()
+        a, b = self.a, self.base
+        self.x = x
+
+        def pool(src, lv, c, dst):
+            nn, hh, ww = self.levels[lv]
+            check(L.eio_unet_resample(0, nn, hh, ww, c, _p(src), _p(dst), 0, st))
+
+        def up_cat(src, lv, cu, skip, cs, up, cat):
+            # cat = [up2(src), skip] at level lv - 1
+            nn, hh, ww = self.levels[lv]
+            check(L.eio_unet_resample(2, nn, hh, ww, cu, _p(src), _p(up), 0, st))
+            check(L.eio_unet_concat(0, self._npix(lv - 1), cu, cs, _p(up), 0, _p(skip), 0, _p(cat), st))
+
+        self._conv(0, x, 0, out16=a["e1a"])
+        self._conv(1, a["e1a"], 0, out16=a["s1"])
+        pool(a["s1"], 0, b, a["p1"])
+        self._conv(2, a["p1"], 1, out16=a["e2a"])
+        self._conv(3, a["e2a"], 1, out16=a["s2"])
+        pool(a["s2"], 1, 2 * b, a["p2"])
+        self._conv(4, a["p2"], 2, out16=a["e3a"])
+        self._conv(5, a["e3a"], 2, out16=a["s3"])
+        pool(a["s3"], 2, 4 * b, a["p3"])
+        self._conv(6, a["p3"], 3, out16=a["b"])
+        up_cat(a["b"], 3, 8 * b, a["s3"], 4 * b, a["u3"], a["c3"])
+        self._conv(7, a["c3"], 2, out16=a["d3"])
+        up_cat(a["d3"], 2, 4 * b, a["s2"], 2 * b, a["u2"], a["c2"])
+        self._conv(8, a["c2"], 1, out16=a["d2"])
+        up_cat(a["d2"], 1, 2 * b, a["s1"], b, a["u1"], a["c1"])
+        self._conv(9, a["c1"], 0, out16=a["d1"])
+        self._conv(10, a["d1"], 0, out32=self.y32, relu=0)
+        return self.y32
+
+    def backward(self, target):
+        """Weight gradients of 0.5 mean((y - target)^2) over the first nout
+        channels (target FP32 [N][H][W][nout], device) after ``forward``.
+        Returns the loss as a device scalar (FP64)."""
+        torch = _torch()
+        n, h, w = self._shape
+        if tuple(target.shape) != (n, h, w, self.nout) or target.dtype != torch.float32 or \
+                not target.is_contiguous():
+            raise ValueError("target must be a contiguous FP32 [%d][%d][%d][%d] tensor" % (n, h, w, self.nout))
+        L = _lib.lib()
+        st = self._stream()
+        a, g, b = self.a, self.g, self.base
+        check(L.eio_cnn_mse(n * h * w, _COUT, self.nout, _p(self.y32), _p(target), _p(g["y"]), _p(self._part),
+                            _p(self._loss), st))
+
+        def split_up(cat_grad, lv, cu, cs, up_grad, skip_grad, src_grad):
+            # [d up, d skip] = d cat (the skip's gradient overwritten); d src = up2^T (d up)
+            check(L.eio_unet_concat(1, self._npix(lv), cu, cs, _p(up_grad), 0, _p(skip_grad), 0, _p(cat_grad), st))
+            nn, hh, ww = self.levels[lv + 1]
+            check(L.eio_unet_resample(3, nn, hh, ww, cu, _p(up_grad), _p(src_grad), 0, st))
+
+        def pool_back(pooled_grad, lv, c, skip_grad):
+            # the skip's gradient += pool^T (d pooled)
+            nn, hh, ww = self.levels[lv]
+            check(L.eio_unet_resample(1, nn, hh, ww, c, _p(pooled_grad), _p(skip_grad), 1, st))
+
+        self._conv_back(10, a["d1"], 0, None, g["y"], g["d1"])
+        self._conv_back(9, a["c1"], 0, a["d1"], g["d1"], g["c1"])
+        split_up(g["c1"], 0, 2 * b, b, g["u1"], g["s1"], g["d2"])
+        self._conv_back(8, a["c2"], 1, a["d2"], g["d2"], g["c2"])
+        split_up(g["c2"], 1, 4 * b, 2 * b, g["u2"], g["s2"], g["d3"])
+        self._conv_back(7, a["c3"], 2, a["d3"], g["d3"], g["c3"])
+        split_up(g["c3"], 2, 8 * b, 4 * b, g["u3"], g["s3"], g["b"])
+        self._conv_back(6, a["p3"], 3, a["b"], g["b"], g["p3"])
+        pool_back(g["p3"], 2, 4 * b, g["s3"])
+        self._conv_back(5, a["e3a"], 2, a["s3"], g["s3"], g["e3a"])
+        self._conv_back(4, a["p2"], 2, a["e3a"], g["e3a"], g["p2"])
+        pool_back(g["p2"], 1, 2 * b, g["s2"])
+        self._conv_back(3, a["e2a"], 1, a["s2"], g["s2"], g["e2a"])
+        self._conv_back(2, a["p1"], 1, a["e2a"], g["e2a"], g["p1"])
+        pool_back(g["p1"], 0, b, g["s1"])
+        self._conv_back(1, a["e1a"], 0, a["s1"], g["s1"], g["e1a"])
+        self._conv_back(0, self.x, 0, a["e1a"], g["e1a"], None)
+        return self._loss
+
+    def adam(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
+        L = _lib.lib()
+        st = self._stream()
+        self.step += 1
+        for l in range(len(self.w32)):
+            check(L.eio_cnn_adam(self.w32[l].numel(), _p(self.w32[l]), _p(self.m[l]), _p(self.v[l]),
+                                 _p(self.dw[l]), lr, b1, b2, eps, self.step, _p(self.wb[l]), st))
+
+    def weights(self):
+        """FP32 master weights as numpy arrays [Cout][9][Cin]."""
+        return [w.cpu().numpy() for w in self.w32]
+
+    def set_weights(self, ws):
+        torch = _torch()
+        for l, w in enumerate(ws):
+            self.w32[l].copy_(torch.as_tensor(np.asarray(w, np.float32)))
+            self.wb[l].copy_(self.w32[l].to(torch.bfloat16))
+
+
 def smooth_perturbation(shape, rng, sigma, interior=None):
     """Unit-RMS smooth random field [nx][nz] (Gaussian-filtered white noise),
     zero outside ``interior`` = (x0, x1, z0, z1) when given."""
@@ -186,7 +424,7 @@ class LearnedPreconditioner:
     ``fwi.lbfgs(precond=...)``; it needs make_pairs (which fixes the target
     scale K) and train first."""
 
-    def __init__(self, born, m0, interior=None, net=None, sigma=3.0, rel_rms=0.02, seed=0):
+    def __init__(self, born, m0, interior=None, net=None, sigma=3.0, rel_rms=0.02, seed=0, arch="convnet"):
         self.born = born
         self.m0 = np.ascontiguousarray(m0, dtype=np.float32)
         self.scale = np.abs(self.m0.reshape(3, -1)).mean(axis=1).astype(np.float64)
@@ -198,7 +436,11 @@ class LearnedPreconditioner:
                         nz - fd.zPadPlus - fd.fat)
         self.interior = interior
         self.sigma, self.rel_rms = sigma, rel_rms
-        self.net = net if net is not None else ConvNet(seed=seed)
+        if net is None:
+            if arch not in ("convnet", "unet"):
+                raise ValueError("arch is 'convnet' or 'unet'")
+            net = ConvNet(seed=seed) if arch == "convnet" else UNet(seed=seed)
+        self.net = net
         self.K = None
         self.born.setBackground(self.m0)
         self.illum = self._illumination()
@@ -253,6 +495,13 @@ class LearnedPreconditioner:
         T = np.moveaxis(rel * (self.K / S)[:, None, None, None], 1, -1).astype(np.float32)
         return X, T, S, D
 
+    def _pad(self, a):
+        """[n][nx][nz][c] with zero rows / columns appended up to the network's
+        size multiple (the U-Net's pooling levels); outputs are cut back."""
+        mult = getattr(self.net, "multiple", 1)
+        px, pz = (-a.shape[1]) % mult, (-a.shape[2]) % mult
+        return np.pad(a, ((0, 0), (0, px), (0, pz), (0, 0))) if px or pz else a
+
     # ------------------------------------------------------------ training
     def train(self, X, T, epochs=40, batch=8, lr=2e-3, seed=0):
         """Adam on shuffled mini-batches of (X, T) (numpy, as make_pairs gives
@@ -262,8 +511,8 @@ class LearnedPreconditioner:
             raise ValueError("need at least one batch of %d pairs (got %d)" % (batch, X.shape[0]))
         torch = _torch()
         dev = self.net.dev
-        Xd = torch.as_tensor(X, device=dev).to(torch.bfloat16)
-        Td = torch.as_tensor(np.ascontiguousarray(T), device=dev)
+        Xd = torch.as_tensor(self._pad(X), device=dev).to(torch.bfloat16)
+        Td = torch.as_tensor(np.ascontiguousarray(self._pad(T)), device=dev)
         n = X.shape[0]
         rng = np.random.default_rng(seed)
         hist = []
@@ -288,8 +537,9 @@ class LearnedPreconditioner:
             raise RuntimeError("make_pairs (and train) before predict: the target scale is not set")
         torch = _torch()
         f, s = self.features(g)
-        x = torch.as_tensor(f[None], device=self.net.dev).to(torch.bfloat16).contiguous()
-        y = self.net.forward(x)[0, ..., :3].double().cpu().numpy()
+        nx, nz = f.shape[:2]
+        x = torch.as_tensor(self._pad(f[None]), device=self.net.dev).to(torch.bfloat16).contiguous()
+        y = self.net.forward(x)[0, :nx, :nz, :3].double().cpu().numpy()
         rel = np.moveaxis(y, -1, 0) * (s / self.K)
         return (rel * self.scale[:, None, None]).astype(np.float32)
 

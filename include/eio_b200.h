@@ -458,6 +458,56 @@ int eio_cnn_mse(long long npix, int c, int nc, const float *y32, const float *ta
 int eio_cnn_adam(long long n, float *p, float *m, float *v, const float *g, float lr, float b1, float b2, float eps,
                  int step, void *pb, void *stream);
 
+/* ---- U-Net preconditioner kernels (no reference counterpart) ----------------
+ * The layers of precond.UNet.  Device pointers, 16-byte aligned; BF16 NHWC
+ * activations, channel counts multiples of 8; queued on `stream` (NULL = the
+ * default stream), nothing synchronises.  Convolution weights are
+ * [cout][9][cin], tap = 3 dy + dx. */
+/* C[M][N] = A[M][K] . B[N][K]^T on tcgen05: BF16 A, B stored K-major (row-major,
+ * leading dimensions lda, ldb >= K, multiples of 8), FP32 accumulation.  C32
+ * (optional, FP32, ldc = N) and/or C16 (optional, BF16): ReLU when relu != 0,
+ * or a multiply by (mask > 0) when mask (BF16 [M][N]) is given.  splits > 1
+ * splits K over at most that many slices into scratch (splits x M x N
+ * floats), then adds the slices in a fixed order (no ReLU or mask then). */
+int eio_gemm_bf16(long long M, long long N, long long K, const void *A, long long lda, const void *B, long long ldb,
+                  float *C32, void *C16, const void *mask, int relu, int splits, float *scratch, void *stream);
+/* bound of the GEMM kernel's accumulator waits (polls; < 0: default 2^22);
+ * after a timeout the CTA drains its MMAs and copies and eio_gemm_status
+ * reports 1 (2 if the drain ran out too); reset != 0 clears the flag
+ * (synchronises) */
+int eio_gemm_set_wait_limit(long long polls);
+int eio_gemm_status(int reset, int *err);
+/* 3x3 convolution (zero padding) as an implicit GEMM on tcgen05: y[p][co] =
+ * sum_{tap, ci} x[p + off(tap)][ci] w[co][tap][ci], x BF16 [n][h][w][cin],
+ * FP32 y32 and / or BF16 y16 [n][h][w][cout], ReLU when relu != 0.  The 3x3
+ * neighbourhoods are gathered by the GEMM's copy loop (no column matrix).
+ * The data gradient is the same call on the output gradient with the flipped
+ * weights (eio_unet_flip). */
+int eio_unet_conv3x3(int n, int h, int w, int cin, int cout, const void *x, const void *wt, float *y32, void *y16,
+                     int relu, void *stream);
+/* floats of scratch eio_unet_conv3x3_wgrad needs for this shape */
+int eio_unet_wgrad_scratch(int n, int h, int w, int cin, int cout, long long *floats);
+/* dw[co][tap][ci] = sum_p dz[p][co] x[p + off(tap)][ci] (FP32, overwritten): a
+ * tcgen05 GEMM over the pixels with both operands read MN-major in place (x
+ * gathered per tap, dz as stored), split over the pixels into scratch and
+ * summed in a fixed order (bitwise reproducible) */
+int eio_unet_conv3x3_wgrad(int n, int h, int w, int cin, int cout, const void *x, const void *dz, float *dw,
+                           float *scratch, long long scratchFloats, void *stream);
+/* wf[ci][tap][co] = w[co][8 - tap][ci]: the weights of the data gradient */
+int eio_unet_flip(int cout, int cin, const void *w, void *wf, void *stream);
+/* op 0: 2x2 average pooling of [n][h][w][c] into [n][h/2][w/2][c]; 1: its
+ * adjoint into [n][h][w][c] (h, w: the fine size); 2: nearest 2x upsampling
+ * of [n][h][w][c] into [n][2h][2w][c]; 3: its adjoint into [n][h][w][c].  The
+ * adjoints add into `out` when add != 0 (a skip connection's gradient). */
+int eio_unet_resample(int op, int n, int h, int w, int c, const void *in, void *out, int add, void *stream);
+/* adj = 0: z[p] = [a[p] (ca channels), b[p] (cb channels)]; adj = 1: a[p] (+)=
+ * z[p][0:ca], b[p] (+)= z[p][ca:] (accumulating where addA / addB != 0) */
+int eio_unet_concat(int adj, long long pixels, int ca, int cb, void *a, int addA, void *b, int addB, void *z,
+                    void *stream);
+/* dst (+)= src * (mask > 0) over n BF16 values, n a multiple of 8 (the ReLU
+ * derivative) */
+int eio_unet_relu_adj(long long n, const void *src, const void *mask, void *dst, int add, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -108,3 +108,111 @@ def backward(a, ws, t, nc, bf16=False):
         if l > 0:
             d = r(d * (a[l] > 0))
     return grads, d
+
+
+# ---------------------------------------------------------------- U-Net
+# The four-level U-Net of precond.UNet: weights [Cout][9][Cin] per layer in
+# the order below; encoder levels of two convolutions (the second one's
+# output is the skip connection), 2x2 average pooling down, a bottleneck
+# convolution, then per decoder level nearest 2x upsampling, concatenation
+# [upsampled, skip] and one convolution; a linear head.
+UNET_LAYERS = ("e1a", "e1b", "e2a", "e2b", "e3a", "e3b", "bott", "d3", "d2", "d1", "head")
+
+
+def unet_channels(base=32, cin=16, cout=16):
+    b = base
+    return [(cin, b), (b, b), (b, 2 * b), (2 * b, 2 * b), (2 * b, 4 * b), (4 * b, 4 * b), (4 * b, 8 * b),
+            (8 * b + 4 * b, 4 * b), (4 * b + 2 * b, 2 * b), (2 * b + b, b), (b, cout)]
+
+
+def _conv(x, w):
+    return conv3x3(x, np.transpose(np.asarray(w, np.float64), (1, 0, 2)))
+
+
+def _convT(dy, w):
+    return conv3x3_transpose(dy, np.transpose(np.asarray(w, np.float64), (1, 0, 2)))
+
+
+def _wgrad(x, dy):
+    return np.transpose(conv3x3_wgrad(x, dy), (1, 0, 2))
+
+
+def pool2(x):
+    return 0.25 * (x[:, 0::2, 0::2] + x[:, 1::2, 0::2] + x[:, 0::2, 1::2] + x[:, 1::2, 1::2])
+
+
+def pool2_adj(dy):
+    return np.repeat(np.repeat(0.25 * dy, 2, axis=1), 2, axis=2)
+
+
+def up2(x):
+    return np.repeat(np.repeat(x, 2, axis=1), 2, axis=2)
+
+
+def up2_adj(dy):
+    return dy[:, 0::2, 0::2] + dy[:, 1::2, 0::2] + dy[:, 0::2, 1::2] + dy[:, 1::2, 1::2]
+
+
+def unet_forward(x, ws, bf16=False):
+    """Every activation of the U-Net (a dict); 'y' is the head output.
+    bf16=True rounds every stored activation to BF16 where the kernels do."""
+    r = _bf16_64 if bf16 else _keep
+    a = {"x": np.asarray(x, np.float64)}
+    relu = lambda z: r(np.maximum(z, 0.0))
+    a["e1a"] = relu(_conv(a["x"], ws[0]))
+    a["s1"] = relu(_conv(a["e1a"], ws[1]))
+    a["p1"] = r(pool2(a["s1"]))
+    a["e2a"] = relu(_conv(a["p1"], ws[2]))
+    a["s2"] = relu(_conv(a["e2a"], ws[3]))
+    a["p2"] = r(pool2(a["s2"]))
+    a["e3a"] = relu(_conv(a["p2"], ws[4]))
+    a["s3"] = relu(_conv(a["e3a"], ws[5]))
+    a["p3"] = r(pool2(a["s3"]))
+    a["b"] = relu(_conv(a["p3"], ws[6]))
+    a["c3"] = np.concatenate([up2(a["b"]), a["s3"]], axis=-1)
+    a["d3"] = relu(_conv(a["c3"], ws[7]))
+    a["c2"] = np.concatenate([up2(a["d3"]), a["s2"]], axis=-1)
+    a["d2"] = relu(_conv(a["c2"], ws[8]))
+    a["c1"] = np.concatenate([up2(a["d2"]), a["s1"]], axis=-1)
+    a["d1"] = relu(_conv(a["c1"], ws[9]))
+    a["y"] = _conv(a["d1"], ws[10])
+    return a
+
+
+def unet_backward(a, ws, t, nc, bf16=False):
+    """Weight gradients (list, [Cout][9][Cin]) of ``loss(a['y'], t, nc)``."""
+    r = _bf16_64 if bf16 else _keep
+    y = a["y"]
+    d = np.zeros_like(y)
+    d[..., :nc] = (y[..., :nc] - np.asarray(t, np.float64)) / (y[..., :nc].size)
+    d = r(d)
+    g = [None] * len(ws)
+    g[10] = _wgrad(a["d1"], d)
+    dd1 = r(_convT(d, ws[10]))
+
+    def layer(k, xin, yout, dy):
+        dz = dy * (yout > 0)
+        g[k] = _wgrad(xin, dz)
+        return r(_convT(dz, ws[k]))
+
+    dc1 = layer(9, a["c1"], a["d1"], dd1)
+    cu1 = a["d2"].shape[-1]
+    dd2, ds1 = r(up2_adj(dc1[..., :cu1])), dc1[..., cu1:]
+    dc2 = layer(8, a["c2"], a["d2"], dd2)
+    cu2 = a["d3"].shape[-1]
+    dd3, ds2 = r(up2_adj(dc2[..., :cu2])), dc2[..., cu2:]
+    dc3 = layer(7, a["c3"], a["d3"], dd3)
+    cu3 = a["b"].shape[-1]
+    db, ds3 = r(up2_adj(dc3[..., :cu3])), dc3[..., cu3:]
+    dp3 = layer(6, a["p3"], a["b"], db)
+    ds3 = r(ds3 + pool2_adj(dp3))
+    de3a = layer(5, a["e3a"], a["s3"], ds3)
+    dp2 = layer(4, a["p2"], a["e3a"], de3a)
+    ds2 = r(ds2 + pool2_adj(dp2))
+    de2a = layer(3, a["e2a"], a["s2"], ds2)
+    dp1 = layer(2, a["p1"], a["e2a"], de2a)
+    ds1 = r(ds1 + pool2_adj(dp1))
+    de1a = layer(1, a["e1a"], a["s1"], ds1)
+    dz = de1a * (a["e1a"] > 0)
+    g[0] = _wgrad(a["x"], dz)
+    return g

@@ -53,3 +53,34 @@ def test_bf16_rounding():
     assert abs(r[4] + 3.140625) < 1e-7
     assert r[5] == 0.0
     assert (r.view(np.uint32) & 0xFFFF == 0).all()
+
+
+def test_unet_backward_matches_central_differences():
+    """The U-Net oracle (three poolings, three upsamplings, concatenated skips)
+    is pinned by FP64 central differences of its loss: weight gradients of an
+    encoder, the bottleneck side, a decoder and the head layer."""
+    rng = np.random.default_rng(0)
+    ch = C.unet_channels(8)
+    ws = [rng.standard_normal((co, 9, ci)) * np.sqrt(2.0 / (9 * ci)) for ci, co in ch]
+    x = rng.standard_normal((1, 8, 8, 16))
+    t = rng.standard_normal((1, 8, 8, 3))
+    g = C.unet_backward(C.unet_forward(x, ws), ws, t, 3)
+    assert [w.shape for w in g] == [w.shape for w in ws]
+    h = 1e-6
+    for k, idx in ((0, (1, 4, 2)), (3, (5, 8, 7)), (4, (1, 4, 2)), (6, (60, 0, 30)), (7, (1, 4, 2)),
+                   (9, (0, 3, 17)), (10, (1, 4, 2))):
+        wp = [w.copy() for w in ws]
+        wm = [w.copy() for w in ws]
+        wp[k][idx] += h
+        wm[k][idx] -= h
+        fd = (C.loss(C.unet_forward(x, wp)["y"], t, 3) - C.loss(C.unet_forward(x, wm)["y"], t, 3)) / (2 * h)
+        assert abs(fd - g[k][idx]) <= 1e-6 * max(abs(fd), 1e-7), (k, idx, fd, g[k][idx])
+
+
+def test_unet_resampling_adjoints():
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal((2, 6, 4, 3))
+    y = rng.standard_normal((2, 3, 2, 3))
+    assert np.isclose((C.pool2(x) * y).sum(), (x * C.pool2_adj(y)).sum())
+    u = rng.standard_normal((2, 12, 8, 3))
+    assert np.isclose((C.up2(x) * u).sum(), (x * C.up2_adj(u)).sum())
