@@ -4,12 +4,12 @@
 // k_gemm_tc: C[M][N] = A[M][K] . B[N][K]^T, BF16 operands, FP32 accumulation
 // in tensor memory, on tcgen05.  A tile of C is 128 x BN (BN = 32, 64, 128 or
 // 256 TMEM columns, twice over); its K range (the whole K, or one slice of a
-// split-K grid) streams through a 4- to 8-stage shared-memory ring in
-// 64-wide slices, each filled by 16-byte cp.async copies into the
-// non-swizzled UMMA operand layouts (K-major, or MN-major for operands whose
-// rows are contiguous in memory) and consumed by four tcgen05.mma.kind::f16
+// split-K grid) streams through a 4- to 10-stage shared-memory ring in
+// 64-wide slices, each filled by 16-byte cp.async copies into the 128-byte
+// swizzled UMMA operand layouts (K-major, or MN-major for operands whose rows
+// are contiguous in memory; 8 lanes copy one 128-byte row) and consumed by four tcgen05.mma.kind::f16
 // (M = 128, N = BN, K = 16) that one thread issues and commits to the
-// stage's mbarrier.  A stage is refilled once the MMAs that read it have
+// stage's mbarrier (256 threads copy and run the epilogue).  A stage is refilled once the MMAs that read it have
 // arrived.  Rows past M, columns past N and K past K read zeros.  The
 // epilogue reads the accumulator with tcgen05.ld (each warp its 32 lanes) and
 // writes FP32 and/or BF16 (optional ReLU, or a multiply by (mask > 0), the
@@ -56,7 +56,7 @@ using bf16 = __nv_bfloat16;
 
 constexpr int G_BM = 128;                    // rows of a CTA tile (TMEM lanes)
 constexpr int G_BK = 64;                     // K of one ring stage
-constexpr int G_THREADS = 128;
+constexpr int G_THREADS = 256;                // 8 warps: copies and epilogue; thread 0 issues the MMAs
 constexpr long long G_WAIT = 1LL << 22;      // default polls of an accumulator wait
 constexpr long long G_DRAIN = 1LL << 24;     // polls of a drain wait after a timeout
 
@@ -73,38 +73,48 @@ enum : int {
 
 template <int BN>
 struct GCfg {
-    static constexpr int STAGES = BN >= 256 ? 4 : (BN >= 128 ? 6 : 8);
+    static constexpr int STAGES = BN >= 256 ? 4 : (BN >= 128 ? 6 : (BN >= 64 ? 8 : 10));
+    static constexpr int LAG = STAGES >= 8 ? 3 : (STAGES >= 6 ? 2 : 1);   // MMA batches in flight
+    static constexpr int AHEAD = STAGES - LAG;                              // slices of copies in flight
     static constexpr int A_BYTES = G_BM * G_BK * 2;
     static constexpr int B_BYTES = BN * G_BK * 2;
-    static constexpr int STAGE = A_BYTES + B_BYTES;
-    static constexpr int BAR = STAGES * STAGE;            // STAGES mbarriers, then the TMEM address
+    static constexpr int STAGE = A_BYTES + B_BYTES;                         // multiple of 1024
+    static constexpr int BAR = 1024 + STAGES * STAGE;                       // after the 1024-byte alignment slack
     static constexpr int SMEM = BAR + 8 * STAGES + 16;
 };
 
 __device__ __forceinline__ unsigned g_smem(const void* p) { return static_cast<unsigned>(__cvta_generic_to_shared(p)); }
 
+// Shared-memory matrix descriptor, 128-byte swizzle (sm_100 encoding: version
+// 1 at bit 46, swizzle mode 2 at bits 61-63)
 __device__ __forceinline__ unsigned long long g_desc(unsigned addr, unsigned lbo, unsigned sbo)
 {
     return (unsigned long long)((addr >> 4) & 0x3FFF) | ((unsigned long long)((lbo >> 4) & 0x3FFF) << 16) |
-           ((unsigned long long)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+           ((unsigned long long)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46) | (2ull << 61);
 }
 
-// Operand descriptor of the kk-th K16 step of a stage holding `rows` rows.
-// Non-swizzled layouts of core matrices (8 rows x 16 bytes), the leading
-// byte offset being the K-direction stride between core matrices and the
-// stride byte offset the M/N-direction one:
-//   K-major:  chunk (row r, K chunk c) at (c * rows + r) * 16       (LBO rows x 16, SBO 128)
-//   MN-major: chunk (row group g, k) at (k / 16) * rows * 32 + (2 g + (k / 8) % 2) * 128 + (k % 8) * 16
-//             (LBO 128, SBO 256)
-// Both put the kk-th K16 step at byte kk * rows * 32.
+// Operand layouts of a stage holding `rows` rows x 64 K (all 128-byte
+// swizzled, 1024-byte atoms of 8 x 128 bytes, chunk position XOR row % 8):
+//   K-major:  row r is 128 bytes of K; chunk c (K 8c .. 8c+7) of row r at
+//             (r / 8) * 1024 + (r % 8) * 128 + ((c ^ r % 8) * 16).
+//             Descriptor of K16 step kk: start + 32 kk, SBO 1024 (8-row groups).
+//   MN-major: K row k holds 64 consecutive rows (MN) in 128 bytes; chunk of MN
+//             group g (rows 8g .. 8g+7) at K k sits in atom (k / 8, g / 8) at
+//             ((k / 8) * (rows / 64) + g / 8) * 1024 + (k % 8) * 128 + (((g ^ k) % 8) * 16).
+//             Descriptor of K16 step kk: start + 2 kk (rows / 64) 1024,
+//             LBO 1024 (MN atoms), SBO (rows / 64) * 1024 (K groups of 8).
+__device__ __forceinline__ unsigned g_kmaj(int r, int c)
+{
+    return (unsigned)((r >> 3) * 1024 + (r & 7) * 128 + ((c ^ (r & 7)) << 4));
+}
+__device__ __forceinline__ unsigned g_mnmaj(int rows, int g, int k)
+{
+    return (unsigned)(((k >> 3) * (rows >> 6) + (g >> 3)) * 1024 + (k & 7) * 128 + (((g ^ k) & 7) << 4));
+}
 __device__ __forceinline__ unsigned long long g_opdesc(unsigned base, int rows, int kk, bool mn)
 {
-    return mn ? g_desc(base + (unsigned)(kk * rows * 32), 128, 256)
-              : g_desc(base + (unsigned)(kk * rows * 32), (unsigned)(rows * 16), 128);
-}
-__device__ __forceinline__ unsigned g_mn_off(int rows, int g, int k)
-{
-    return (unsigned)((k >> 4) * rows * 32 + (2 * g + ((k >> 3) & 1)) * 128 + (k & 7) * 16);
+    return mn ? g_desc(base + (unsigned)(kk * 2 * (rows >> 6) * 1024), 1024, (unsigned)((rows >> 6) * 1024))
+              : g_desc(base + (unsigned)(kk * 32), 16, 1024);
 }
 
 // instruction descriptor: F32 accumulator, BF16 A and B (K-major unless
@@ -132,17 +142,21 @@ __device__ __forceinline__ bool g_wait(unsigned bar, unsigned parity, long long 
     return false;
 }
 
-__device__ __forceinline__ void g_ld16(unsigned taddr, float* v)
+// 32 accumulator columns of this warp's 32 lanes
+__device__ __forceinline__ void g_ld32(unsigned taddr, float* v)
 {
-    unsigned r[16];
+    unsigned r[32];
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
 // 16 bytes from global memory into shared memory, zeros when !in (src is then
@@ -175,54 +189,75 @@ __device__ __forceinline__ long long g_tap_src(long long p, int y, int x, int ta
     return (sy >= 0 && sy < H && sx >= 0 && sx < W) ? p + (long long)dy * W + dx : -1;
 }
 
-// Slice [k0, k0 + 64) (K < ke) of A's rows [m0, m0 + 128) into stage dst.
-// Pixel indices stay below 2^31 + 128 (pixel counts are capped at 2^31).
-__device__ __forceinline__ void g_load_a(const GemmArgs& g, long long m0, long long k0, long long ke, unsigned dst)
+// K-major copy loops: thread t copies chunk t % 8 of rows t / 8 + 32 j, so
+// that 8 lanes read the 128 contiguous bytes of one row.  For OP_CONV, yx[j]
+// holds (y << 16 | x) of row t / 8 + 32 j's pixel, -1 past M (set per tile;
+// widths and heights below 2^15).  Pixel indices stay below 2^31 + 128
+// (pixel counts are capped at 2^31).
+constexpr int G_RPT = G_BM * 8 / G_THREADS;   // A rows per thread (4)
+__device__ __forceinline__ void g_tile_pixels(const GemmArgs& g, long long m0, int* yx)
+{
+    const int r0 = threadIdx.x >> 3;
+#pragma unroll
+    for (int j = 0; j < G_RPT; j++) {
+        const long long p = m0 + r0 + (G_THREADS / 8) * j;
+        const unsigned pu = (unsigned)p, cw = (unsigned)g.cw;
+        yx[j] = p < g.M ? (int)((((pu / cw) % (unsigned)g.ch) << 16) | (pu % cw)) : -1;
+    }
+}
+
+// Slice [k0, k0 + 64) (K < ke) of A's rows [m0, m0 + 128) into stage dst
+__device__ __forceinline__ void g_load_a(const GemmArgs& g, long long m0, long long k0, long long ke, unsigned dst,
+                                         const int* yx)
 {
     const int tid = threadIdx.x;
     if (g.amode == OP_PLAIN) {
-        const long long row = m0 + tid;
+        const int c = tid & 7;
+        const long long k = k0 + 8 * c;
 #pragma unroll
-        for (int c = 0; c < 8; c++) {
-            const long long k = k0 + 8 * c;
+        for (int j = 0; j < G_RPT; j++) {
+            const int r = (tid >> 3) + (G_THREADS / 8) * j;
+            const long long row = m0 + r;
             const bool in = row < g.M && k < ke;
-            g_cp16(dst + (unsigned)(c * G_BM + tid) * 16, in ? g.A + row * g.lda + k : g.A, in);
+            g_cp16(dst + g_kmaj(r, c), in ? g.A + row * g.lda + k : g.A, in);
         }
     } else if (g.amode == OP_CONV) {
-        // thread = pixel row; 8 consecutive K chunks (channel groups of one or more taps)
-        const long long p = m0 + tid;
-        const unsigned pu = (unsigned)p, cw = (unsigned)g.cw;
-        const int x = (int)(pu % cw), y = (int)((pu / cw) % (unsigned)g.ch);
-        int tap = (int)((unsigned)k0 / (unsigned)g.cc), c8 = (int)(k0 - (long long)tap * g.cc);
+        const int c = tid & 7;
+        const long long k = k0 + 8 * c;
+        const int tap = (int)((unsigned)k / (unsigned)g.cc), c8 = (int)(k - (long long)tap * g.cc);
+        const bool kin = k < ke;
 #pragma unroll
-        for (int c = 0; c < 8; c++) {
-            const long long k = k0 + 8 * c;
+        for (int j = 0; j < G_RPT; j++) {
+            const int r = (tid >> 3) + (G_THREADS / 8) * j;
             long long src = -1;
-            if (p < g.M && k < ke) src = g_tap_src(p, y, x, tap, g.ch, g.cw);
-            g_cp16(dst + (unsigned)(c * G_BM + tid) * 16, src >= 0 ? g.A + src * g.cc + c8 : g.A, src >= 0);
-            c8 += 8;
-            if (c8 == g.cc) {
-                c8 = 0;
-                tap++;
-            }
+            if (kin && yx[j] >= 0) src = g_tap_src(m0 + r, yx[j] >> 16, yx[j] & 0xFFFF, tap, g.ch, g.cw);
+            g_cp16(dst + g_kmaj(r, c), src >= 0 ? g.A + src * g.cc + c8 : g.A, src >= 0);
         }
-    } else {   // OP_CONVT: rows tap * C + c, K = pixels; thread = pixel k0 + tid % 64, row groups tid / 64 + 2 j
-        const int kp = tid & 63;
-        const long long p = k0 + kp;
-        const unsigned pu = (unsigned)p, cw = (unsigned)g.cw;
-        const int x = (int)(pu % cw), y = (int)((pu / cw) % (unsigned)g.ch);
+    } else {
+        // OP_CONVT: rows (M) = tap * C + c, K = pixels.  Thread t copies MN
+        // group t % 16 (8 channels of one tap) of pixels k0 + t / 16 + 16 j, so
+        // that lanes read consecutive channels of one pixel.
+        const int gr = tid & 15;
+        const long long m = m0 + 8 * gr;
+        const bool min_ = m < g.M;
+        const int tap = min_ ? (int)((unsigned)m / (unsigned)g.cc) : 0;
+        const int c8 = (int)(m - (long long)tap * g.cc);
+        const int kp0 = tid >> 4;
+        long long p = k0 + kp0;
+        const unsigned pu = (unsigned)p, cw = (unsigned)g.cw, chh = (unsigned)g.ch;
+        int x = (int)(pu % cw), y = (int)((pu / cw) % chh);
+        constexpr int STEP = G_THREADS / 16;  // pixels between a thread's copies
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-            const int gr = (tid >> 6) + 2 * j;
-            const long long m = m0 + 8 * gr;
+        for (int j = 0; j < 64 / STEP; j++) {
             long long src = -1;
-            int c8 = 0;
-            if (p < ke && m < g.M) {
-                const int tap = (int)((unsigned)m / (unsigned)g.cc);
-                c8 = (int)(m - (long long)tap * g.cc);
-                src = g_tap_src(p, y, x, tap, g.ch, g.cw);
+            if (min_ && p < ke) src = g_tap_src(p, y, x, tap, g.ch, g.cw);
+            g_cp16(dst + g_mnmaj(G_BM, gr, kp0 + STEP * j), src >= 0 ? g.A + src * g.cc + c8 : g.A, src >= 0);
+            p += STEP;
+            x += STEP;
+            while (x >= g.cw) {
+                x -= g.cw;
+                if (++y == g.ch) y = 0;
             }
-            g_cp16(dst + g_mn_off(G_BM, gr, kp), src >= 0 ? g.A + src * g.cc + c8 : g.A, src >= 0);
         }
     }
 }
@@ -233,63 +268,61 @@ __device__ __forceinline__ void g_load_b(const GemmArgs& g, long long n0, long l
 {
     const int tid = threadIdx.x;
     if (g.bmode == OP_PLAIN) {
+        const int c = tid & 7;
+        const long long k = k0 + 8 * c;
 #pragma unroll
-        for (int i = tid; i < BN * 8; i += G_THREADS) {
-            const int r = i % BN, c = i / BN;
-            const long long row = n0 + r, k = k0 + 8 * c;
+        for (int j = 0; j < BN * 8 / G_THREADS; j++) {
+            const int r = (tid >> 3) + (G_THREADS / 8) * j;
+            const long long row = n0 + r;
             const bool in = row < g.N && k < ke;
-            g_cp16(dst + (unsigned)(c * BN + r) * 16, in ? g.B + row * g.ldb + k : g.B, in);
+            g_cp16(dst + g_kmaj(r, c), in ? g.B + row * g.ldb + k : g.B, in);
         }
-    } else {   // OP_MN: B[k][n] at k * ldb + n
+    } else {   // OP_MN: B[k][n] at k * ldb + n; lanes read consecutive 8-column groups of one k
+        constexpr int G = BN / 8;
 #pragma unroll
-        for (int i = tid; i < BN * 8; i += G_THREADS) {
-            const int kp = i & 63, gr = i >> 6;
+        for (int j = 0; j < BN * 8 / G_THREADS; j++) {
+            const int i = threadIdx.x + G_THREADS * j;
+            const int gr = i % G, kp = i / G;
             const long long k = k0 + kp, n = n0 + 8 * gr;
             const bool in = k < ke && n < g.N;
-            g_cp16(dst + g_mn_off(BN, gr, kp), in ? g.B + k * g.ldb + n : g.B, in);
+            g_cp16(dst + g_mnmaj(BN, gr, kp), in ? g.B + k * g.ldb + n : g.B, in);
         }
     }
 }
 
-// Accumulator buffer -> C (rows of this warp's 32 TMEM lanes)
+// Accumulator buffer -> C: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its
+// quarter) and the 32-column groups (w / 4) + 2 i
 template <int BN>
 __device__ __forceinline__ void g_epilogue(const GemmArgs& g, unsigned tbuf, long long m0, long long n0, int z)
 {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long long row = m0 + warp * 32 + lane;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, quarter = warp & 3;
+    const long long row = m0 + quarter * 32 + lane;
     float* c32 = g.C32 ? g.C32 + (long long)z * g.M * g.N : nullptr;
 #pragma unroll 1
-    for (int c = 0; c < BN; c += 16) {
-        float v[16];
-        g_ld16(tbuf + ((unsigned)(warp * 32) << 16) + (unsigned)c, v);
+    for (int c = (warp >> 2) * 32; c < BN; c += 64) {
+        float v[32];
+        g_ld32(tbuf + ((unsigned)(quarter * 32) << 16) + (unsigned)c, v);
         const long long col = n0 + c;
         if (row >= g.M || col >= g.N) continue;
-        const int nv = (int)min((long long)16, g.N - col);
-        const bool vec = nv == 16 && (g.N & 7) == 0;
+        const int nv = (int)min((long long)32, g.N - col);
+        const bool vec = (g.N & 7) == 0;      // 8-column groups stay 16-byte aligned
         if (g.mask) {
             const bf16* mk = g.mask + row * g.N + col;
-            if (vec) {
-                uint4 u[2];
-                u[0] = *reinterpret_cast<const uint4*>(mk);
-                u[1] = *reinterpret_cast<const uint4*>(mk + 8);
-                const bf16* mb = reinterpret_cast<const bf16*>(u);
-#pragma unroll
-                for (int i = 0; i < 16; i++)
-                    if (!(__bfloat162float(mb[i]) > 0.f)) v[i] = 0.f;
-            } else {
-                for (int i = 0; i < nv; i++)
-                    if (!(__bfloat162float(mk[i]) > 0.f)) v[i] = 0.f;
-            }
+            for (int i = 0; i < nv; i++)
+                if (!(__bfloat162float(mk[i]) > 0.f)) v[i] = 0.f;
         } else if (g.relu) {
 #pragma unroll
-            for (int i = 0; i < 16; i++) v[i] = fmaxf(v[i], 0.f);
+            for (int i = 0; i < 32; i++) v[i] = fmaxf(v[i], 0.f);
         }
         if (c32) {
             float* dst = c32 + row * g.N + col;
             if (vec) {
 #pragma unroll
-                for (int i = 0; i < 16; i += 4)
-                    *reinterpret_cast<float4*>(dst + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+                for (int i = 0; i < 32; i += 8)
+                    if (i < nv) {
+                        *reinterpret_cast<float4*>(dst + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+                        *reinterpret_cast<float4*>(dst + i + 4) = make_float4(v[i + 4], v[i + 5], v[i + 6], v[i + 7]);
+                    }
             } else {
                 for (int i = 0; i < nv; i++) dst[i] = v[i];
             }
@@ -297,12 +330,15 @@ __device__ __forceinline__ void g_epilogue(const GemmArgs& g, unsigned tbuf, lon
         if (g.C16) {
             bf16* dst = g.C16 + row * g.N + col;
             if (vec) {
-                uint4 u[2];
-                bf16* ub = reinterpret_cast<bf16*>(u);
 #pragma unroll
-                for (int i = 0; i < 16; i++) ub[i] = __float2bfloat16_rn(v[i]);
-                *reinterpret_cast<uint4*>(dst) = u[0];
-                *reinterpret_cast<uint4*>(dst + 8) = u[1];
+                for (int i = 0; i < 32; i += 8)
+                    if (i < nv) {
+                        uint4 u;
+                        bf16* ub = reinterpret_cast<bf16*>(&u);
+#pragma unroll
+                        for (int e = 0; e < 8; e++) ub[e] = __float2bfloat16_rn(v[i + e]);
+                        *reinterpret_cast<uint4*>(dst + i) = u;
+                    }
             } else {
                 for (int i = 0; i < nv; i++) dst[i] = __float2bfloat16_rn(v[i]);
             }
@@ -310,15 +346,23 @@ __device__ __forceinline__ void g_epilogue(const GemmArgs& g, unsigned tbuf, lon
     }
 }
 
-// Persistent tcgen05 GEMM (tile id: N tile fastest, then M tile, then K split)
+// Persistent tcgen05 GEMM (tile id: N tile fastest, then M tile, then K split).
+// Slice q of this CTA lives in stage q % S; its MMAs commit to that stage's
+// mbarrier.  After issuing slice q's MMAs the CTA refills the stage of slice
+// q - LAG (waiting for those MMAs) with slice q + AHEAD, so LAG batches of
+// MMAs and AHEAD slices of copies are in flight.  A tile's accumulator is
+// read out once its last MMAs are known complete, while the next tile
+// accumulates in the other TMEM buffer.
 template <int BN>
 __global__ void __launch_bounds__(G_THREADS, 1) k_gemm_tc(const __grid_constant__ GemmArgs g)
 {
     using Cf = GCfg<BN>;
-    constexpr int S = Cf::STAGES;
-    extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem + Cf::BAR);
-    unsigned* tslot = reinterpret_cast<unsigned*>(smem + Cf::BAR + 8 * S);
+    constexpr int S = Cf::STAGES, LAG = Cf::LAG, AHEAD = Cf::AHEAD;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const unsigned raw = g_smem(smem_raw);
+    unsigned char* smem = smem_raw + ((1024u - (raw & 1023u)) & 1023u);   // 1024-byte aligned stages
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem_raw + Cf::BAR);
+    unsigned* tslot = reinterpret_cast<unsigned*>(smem_raw + Cf::BAR + 8 * S);
     const int tid = threadIdx.x, warp = tid >> 5;
     const int tiles = g.mt * g.nt * g.splits;
 
@@ -350,14 +394,24 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_gemm_tc(const __grid_constant_
     // copy cursor: the next slice to load is slice l_t of tile l_tile, the
     // l_n-th of this CTA (stage l_n % S); one copy group per slice, empty
     // groups past the last tile
-    int l_tile = blockIdx.x, l_t = 0, l_n = 0;
+    int l_tile = blockIdx.x, l_t = 0, l_n = 0, l_kt = 0;
+    long long l_m0 = 0, l_n0 = 0, l_kb = 0, l_ke = 0;
+    int yx[G_RPT];
     auto load_next = [&]() {
         if (l_tile < tiles) {
             const int s = l_n % S;
-            const long long k0 = t_kb(l_tile) + (long long)l_t * G_BK, ke = t_ke(l_tile);
-            g_load_a(g, t_m0(l_tile), k0, ke, stageA(s));
-            g_load_b<BN>(g, t_n0(l_tile), k0, ke, stageB(s));
-            if (++l_t == t_kt(l_tile)) {
+            if (l_t == 0) {                    // a new tile: its coordinates once
+                l_m0 = t_m0(l_tile);
+                l_n0 = t_n0(l_tile);
+                l_kb = t_kb(l_tile);
+                l_ke = t_ke(l_tile);
+                l_kt = t_kt(l_tile);
+                if (g.amode == OP_CONV) g_tile_pixels(g, l_m0, yx);
+            }
+            const long long k0 = l_kb + (long long)l_t * G_BK;
+            g_load_a(g, l_m0, k0, l_ke, stageA(s), yx);
+            g_load_b<BN>(g, l_n0, k0, l_ke, stageB(s));
+            if (++l_t == l_kt) {
                 l_t = 0;
                 l_tile += gridDim.x;
             }
@@ -365,18 +419,42 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_gemm_tc(const __grid_constant_
         l_n++;
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
-    for (int i = 0; i < S - 1; i++) load_next();
+    for (int i = 0; i < AHEAD; i++) load_next();
 
     const bool amn = g.amode == OP_CONVT, bmn = g.bmode == OP_MN;
     const unsigned idesc = g_idesc<BN>(amn, bmn);
     bool bad = false;
-    int q = 0, pend_a = -1, pend_b = -1, it = 0, prev = -1;
+    int q = 0, it = 0;
+    int ep_tile[2] = {-1, -1}, ep_last[2] = {0, 0};   // per TMEM buffer: tile awaiting its epilogue, its last slice
+    auto epilogue = [&](int b) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        g_epilogue<BN>(g, tmem + (unsigned)(b * BN), t_m0(ep_tile[b]), t_n0(ep_tile[b]), t_z(ep_tile[b]));
+        ep_tile[b] = -1;
+    };
+    // epilogues of tiles whose last slice is <= done (older tile first)
+    auto drain_epilogues = [&](int done) {
+        const int o = (ep_tile[0] >= 0 && ep_tile[1] >= 0) ? (ep_last[0] < ep_last[1] ? 0 : 1)
+                                                           : (ep_tile[0] >= 0 ? 0 : 1);
+        if (ep_tile[o] >= 0 && ep_last[o] <= done) epilogue(o);
+        if (ep_tile[o ^ 1] >= 0 && ep_last[o ^ 1] <= done) epilogue(o ^ 1);
+    };
     for (int tile = blockIdx.x; tile < tiles && !bad; tile += gridDim.x, it++) {
+        const int b = it & 1;
+        if (ep_tile[b] >= 0) {
+            // the buffer still holds an older tile's sums: every MMA issued so far
+            // is complete once the latest one is
+            const bool ok = g_wait(g_smem(bar + (q - 1) % S), (unsigned)(((q - 1) / S) & 1), g.wait);
+            if (__syncthreads_or(!ok)) {
+                bad = true;
+                break;
+            }
+            drain_epilogues(q - 1);
+        }
         const int KT = t_kt(tile);
-        const unsigned acc_buf = tmem + (unsigned)((it & 1) * BN);
+        const unsigned acc_buf = tmem + (unsigned)(b * BN);
         for (int t = 0; t < KT; t++, q++) {
             const int s = q % S;
-            asm volatile("cp.async.wait_group %0;" ::"n"(S - 2) : "memory");
+            asm volatile("cp.async.wait_group %0;" ::"n"(AHEAD - 1) : "memory");
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncthreads();
@@ -399,43 +477,35 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_gemm_tc(const __grid_constant_
                                  g_smem(bar + s))
                              : "memory");
             }
-            pend_b = pend_a;
-            pend_a = q;
-            // the stage of slice q - 1 is refilled next: its MMAs must have read it
-            if (q >= 1) {
-                const int p = q - 1;
+            // the stage of slice q - LAG is refilled next (with slice q + AHEAD):
+            // its MMAs must have read it
+            if (q >= LAG) {
+                const int p = q - LAG;
                 const bool ok = g_wait(g_smem(bar + p % S), (unsigned)((p / S) & 1), g.wait);
                 if (__syncthreads_or(!ok)) {
                     bad = true;
+                    q++;
                     break;
                 }
-                pend_b = -1;
+                drain_epilogues(p);
             }
             load_next();
-            if (t == 0 && prev >= 0) {   // every MMA of the previous tile has completed
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                g_epilogue<BN>(g, tmem + (unsigned)(((it - 1) & 1) * BN), t_m0(prev), t_n0(prev), t_z(prev));
-            }
         }
-        prev = tile;
+        if (!bad) {
+            ep_tile[b] = tile;
+            ep_last[b] = q - 1;
+        }
     }
     if (!bad && q > 0) {
-        const int p = q - 1;
-        const bool ok = g_wait(g_smem(bar + p % S), (unsigned)((p / S) & 1), g.wait);
-        if (__syncthreads_or(!ok)) {
-            bad = true;
-        } else {
-            pend_a = -1;
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            g_epilogue<BN>(g, tmem + (unsigned)(((it - 1) & 1) * BN), t_m0(prev), t_n0(prev), t_z(prev));
-        }
+        const bool ok = g_wait(g_smem(bar + (q - 1) % S), (unsigned)(((q - 1) / S) & 1), g.wait);
+        if (__syncthreads_or(!ok)) bad = true;
+        else drain_epilogues(q - 1);
     }
     if (bad) {
-        // drain the MMAs that may still run and the copies in flight before the
-        // tensor memory is freed and the CTA leaves
+        // drain: every MMA issued is complete once the latest one is; then the
+        // copies in flight; then the tensor memory is freed and the CTA leaves
         bool drained = true;
-        if (pend_a >= 0) drained = g_wait(g_smem(bar + pend_a % S), (unsigned)((pend_a / S) & 1), G_DRAIN) && drained;
-        if (pend_b >= 0) drained = g_wait(g_smem(bar + pend_b % S), (unsigned)((pend_b / S) & 1), G_DRAIN) && drained;
+        if (q > 0) drained = g_wait(g_smem(bar + (q - 1) % S), (unsigned)(((q - 1) / S) & 1), G_DRAIN);
         asm volatile("cp.async.wait_all;" ::: "memory");
         drained = !__syncthreads_or(!drained);
         if (tid == 0) atomicMax(&g_gemm_err, drained ? 1 : 2);
@@ -649,7 +719,7 @@ void launch_gemm(GemmArgs& a, cudaStream_t st)
 
 void launch_any(GemmArgs& a, cudaStream_t st)
 {
-    if (a.N <= 32) launch_gemm<32>(a, st);
+    if (a.N <= 32 && a.bmode != OP_MN) launch_gemm<32>(a, st);   // MN-major operands come in 64-row atoms
     else if (a.N <= 64) launch_gemm<64>(a, st);
     else if (a.N <= 128) launch_gemm<128>(a, st);
     else launch_gemm<256>(a, st);
@@ -677,7 +747,7 @@ int fit_splits(long long kt, int splits, long long* kchunk)
 // least four slices (256 pixels)
 int wgrad_splits(long long M, long long N, long long K)
 {
-    const long long bn = N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : 256;
+    const long long bn = N <= 64 ? 64 : N <= 128 ? 128 : 256;     // the B operand is MN-major: BN >= 64
     const long long base = ((M + G_BM - 1) / G_BM) * ((N + bn - 1) / bn);
     const long long kt = (K + G_BK - 1) / G_BK;
     long long s = (2LL * g_sms() + base - 1) / base;
@@ -691,6 +761,7 @@ void conv_geometry(int n, int h, int w, int cin, int cout)
     if (n < 1 || h < 1 || w < 1 || cin < 8 || cout < 8 || cin % 8 || cout % 8)
         throw Error(EIO_ERR_ARG, "conv3x3: positive sizes, channel counts multiples of 8");
     if ((long long)n * h * w > (1LL << 31)) throw Error(EIO_ERR_ARG, "conv3x3: too many pixels");
+    if (h >= (1 << 15) || w >= (1 << 15)) throw Error(EIO_ERR_ARG, "conv3x3: height and width below 32768");
 }
 
 unsigned chunks(long long values, const char* what)
