@@ -108,6 +108,8 @@ _SIGS = {
                           ctypes.c_longlong, P, P, P, I, I, P, P]),
     "eio_gemm_set_wait_limit": (I, [ctypes.c_longlong]),
     "eio_gemm_status": (I, [I, P]),
+    "eio_unet_set_tma": (I, [I]),
+    "eio_unet_get_tma": (I, [P]),
     "eio_unet_conv3x3": (I, [I, I, I, I, I, P, P, P, P, I, P]),
     "eio_unet_wgrad_scratch": (I, [I, I, I, I, I, P]),
     "eio_unet_conv3x3_wgrad": (I, [I, I, I, I, I, P, P, P, P, ctypes.c_longlong, P]),

@@ -33,6 +33,7 @@
 // flip, 2x2 average pooling and nearest 2x upsampling (forward and adjoint),
 // channel concatenation and its adjoint (adding into the skip connection's
 // gradient), the ReLU derivative.
+#include <cuda.h>   // CUtensorMap and the tensor-map encoder's types (the encoder is fetched at run time)
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -685,6 +686,345 @@ __global__ void __launch_bounds__(256) k_relu_adj(const bf16* __restrict__ src, 
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// k_conv_tma: the 3x3 convolutions with their operands brought in by TMA.
+// When the pixels of a 128-row tile (or of a 64-pixel weight-gradient slice)
+// form a rectangle of the NHWC image (widths that divide the box or are
+// divided by it), the 3x3 gather of one tap and one block of 16 / 32 / 64
+// channels is ONE 4-D tiled TMA box of the activation tensor at the tile's
+// origin shifted by the tap; the tensor's out-of-bounds fill supplies the
+// zero padding.  Roles: warp 0 (one lane) issues the copies, warp 1 (one
+// lane) the MMAs, warps 2-5 read the accumulators out (one TMEM lane quarter
+// each).  Stages are handed over through full / empty mbarriers, the two
+// TMEM accumulators through their own pair; every wait is bounded and a role
+// that gives up raises a shared abort flag that ends the others' waits.
+//   conv (forward, data gradient): A = boxes {cb channels, bw x bh pixels}
+//     (K-major, swizzle 2 cb bytes), up to 64 K per stage; B = the weights
+//     [cout][9 cin] as one 2-D box {64 K, BN rows} (K-major, 128-byte swizzle).
+//   weight gradient: A = boxes {cb channels, 64 pixels} of the input shifted by
+//     the tap of each 128-row tile's channel blocks (MN-major), B = boxes
+//     {cbB channels, 64 pixels} of dz (MN-major); K = pixels, split over the grid.
+constexpr int T_THREADS = 192;
+
+struct ConvTma {
+    int wgrad;                 // 0: convolution, 1: weight gradient
+    int C, cb;                 // channels of the gathered tensor, channel block of its boxes
+    int W, H;                  // image size
+    long long M, N, K;         // GEMM sizes; K = 9 C (convolution) or pixels (weight gradient)
+    int mt, nt, splits;        // tiles: M, N, K splits
+    long long kchunk;          // weight gradient: pixels per split (a multiple of 64)
+    int cbB;                   // weight gradient: channel block of dz's boxes
+    float* C32;                // optional [splits][M][N]
+    bf16* C16;                 // optional [M][N]
+    int relu;
+    long long wait;
+};
+
+template <int BN>
+struct TCfg {
+    static constexpr int A_BYTES = 16384;
+    static constexpr int B_BYTES = BN * 128;
+    static constexpr int STAGE = A_BYTES + B_BYTES;        // multiple of 1024
+    static constexpr int S0 = (200 * 1024) / STAGE;
+    static constexpr int STAGES = S0 > 8 ? 8 : S0;
+    static constexpr int COLS = BN < 32 ? 32 : BN;          // TMEM columns of one accumulator buffer
+    static constexpr int TALLOC = 2 * COLS <= 64 ? 64 : 2 * COLS <= 128 ? 128 : 2 * COLS <= 256 ? 256 : 512;
+    static constexpr int BAR = 1024 + STAGES * STAGE;       // after the 1024-byte alignment slack
+    static constexpr int SMEM = BAR + 8 * (2 * STAGES + 4) + 32;
+};
+
+__device__ __forceinline__ unsigned long long t_desc(unsigned addr, unsigned lbo, unsigned sbo, int swz)
+{
+    const unsigned long long mode = swz == 128 ? 2 : (swz == 64 ? 4 : 6);
+    return (unsigned long long)((addr >> 4) & 0x3FFF) | ((unsigned long long)((lbo >> 4) & 0x3FFF) << 16) |
+           ((unsigned long long)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46) | (mode << 61);
+}
+__device__ __forceinline__ void t_load4(unsigned dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                        unsigned bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+        ::"r"(dst), "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ void t_load2(unsigned dst, const CUtensorMap* map, int c0, int c1, unsigned bar)
+{
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                 ::"r"(dst), "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ void t_expect(unsigned bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void t_arrive(unsigned bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+// bounded wait; also gives up once another role raised the abort flag
+__device__ __forceinline__ bool t_wait(unsigned bar, unsigned parity, long long limit, const volatile int* abort)
+{
+    for (long long it = 0; it < limit; it++) {
+        unsigned done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((it & 255) == 255 && *abort) return false;
+    }
+    return false;
+}
+__device__ __forceinline__ void t_mma(unsigned acc, unsigned long long ad, unsigned long long bd, unsigned idesc,
+                                      bool accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(acc), "l"(ad), "l"(bd), "r"(idesc), "r"(accumulate ? 1u : 0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+__device__ __forceinline__ void t_commit(unsigned bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+template <int BN>
+__global__ void __launch_bounds__(T_THREADS, 1) k_conv_tma(const __grid_constant__ CUtensorMap ta,
+                                                          const __grid_constant__ CUtensorMap tb,
+                                                          const __grid_constant__ ConvTma g)
+{
+    using Cf = TCfg<BN>;
+    constexpr int S = Cf::STAGES;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const unsigned raw = g_smem(smem_raw);
+    const unsigned s0 = raw + ((1024u - (raw & 1023u)) & 1023u);   // 1024-byte aligned stages
+    const unsigned bars = raw + Cf::BAR;                            // full[S], empty[S], tfull[2], tempty[2]
+    auto full = [&](int s) { return bars + 8u * s; };
+    auto empty = [&](int s) { return bars + 8u * (S + s); };
+    auto tfull = [&](int b) { return bars + 8u * (2 * S + b); };
+    auto tempty = [&](int b) { return bars + 8u * (2 * S + 2 + b); };
+    unsigned* tslot = reinterpret_cast<unsigned*>(smem_raw + Cf::BAR + 8 * (2 * S + 4));
+    volatile int* abort = reinterpret_cast<volatile int*>(tslot + 1);
+    int* qprod = reinterpret_cast<int*>(tslot + 2);
+    int* qmma = reinterpret_cast<int*>(tslot + 3);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tiles = g.mt * g.nt * g.splits;
+    const int cpt = g.C / g.cb;                  // channel blocks per tap
+    const int nbox = 9 * cpt, nbs = 64 / g.cb;   // convolution: boxes per tile, boxes per stage
+
+    if (tid == 0) {
+        for (int s = 0; s < S; s++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(full(s)) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(empty(s)) : "memory");
+        }
+        for (int b = 0; b < 2; b++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tfull(b)) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(tempty(b)) : "memory");
+        }
+        *abort = 0;
+        *qprod = 0;
+        *qmma = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(g_smem(tslot)),
+                     "r"(Cf::TALLOC)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const unsigned tmem = *tslot;
+    auto stageA = [&](int s) { return s0 + (unsigned)(s * Cf::STAGE); };
+    auto stageB = [&](int s) { return s0 + (unsigned)(s * Cf::STAGE + Cf::A_BYTES); };
+    auto t_mi = [&](int id) { return (id / g.nt) % g.mt; };
+    auto t_ni = [&](int id) { return id % g.nt; };
+    auto t_z = [&](int id) { return id / (g.nt * g.mt); };
+    auto slices = [&](int id) {
+        if (!g.wgrad) return (nbox + nbs - 1) / nbs;
+        const long long kb = (long long)t_z(id) * g.kchunk, ke = min(g.K, kb + g.kchunk);
+        return (int)((ke - kb) / 64);
+    };
+    const long long HW = (long long)g.H * g.W;
+
+    if (warp == 0 && lane == 0) {
+        // ---- copies
+        int q = 0;
+        bool ok = true;
+        for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+            const int mi = t_mi(tile), ni = t_ni(tile), ns = slices(tile);
+            const long long m0 = (long long)mi * G_BM;
+            for (int j = 0; j < ns; j++, q++) {
+                const int s = q % S;
+                if (!t_wait(empty(s), (unsigned)(((q / S) & 1) ^ 1), g.wait, abort)) {
+                    ok = false;
+                    break;
+                }
+                if (!g.wgrad) {
+                    // pixels m0 .. m0 + 127: a bw x bh rectangle at (n, y0, x0)
+                    const int n = (int)(m0 / HW);
+                    const long long rem = m0 - n * HW;
+                    const int y0 = (int)(rem / g.W), x0 = (int)(rem - (long long)y0 * g.W);
+                    const int b0 = j * nbs, nb = min(nbox - b0, nbs);
+                    t_expect(full(s), (unsigned)(nb * G_BM * g.cb * 2 + BN * 128));
+                    for (int i = 0; i < nb; i++) {
+                        const int b = b0 + i, tap = b / cpt, c0 = (b - tap * cpt) * g.cb;
+                        t_load4(stageA(s) + (unsigned)(i * G_BM * g.cb * 2), &ta, c0, x0 + tap % 3 - 1,
+                                y0 + tap / 3 - 1, n, full(s));
+                    }
+                    t_load2(stageB(s), &tb, b0 * g.cb, ni * BN, full(s));
+                } else {
+                    const long long p0 = (long long)t_z(tile) * g.kchunk + 64LL * j;
+                    const int n = (int)(p0 / HW);
+                    const long long rem = p0 - n * HW;
+                    const int y = (int)(rem / g.W), x = (int)(rem - (long long)y * g.W);
+                    const int na = (int)min((long long)(G_BM / g.cb), (g.M - m0 + g.cb - 1) / g.cb);
+                    const int nbB = BN / g.cbB;
+                    t_expect(full(s), (unsigned)(na * 64 * g.cb * 2 + nbB * 64 * g.cbB * 2));
+                    for (int i = 0; i < na; i++) {
+                        const long long m = m0 + (long long)i * g.cb;
+                        const int tap = (int)(m / g.C), c0 = (int)(m - (long long)tap * g.C);
+                        t_load4(stageA(s) + (unsigned)(i * 64 * g.cb * 2), &ta, c0, x + tap % 3 - 1, y + tap / 3 - 1,
+                                n, full(s));
+                    }
+                    for (int i = 0; i < nbB; i++)
+                        t_load2(stageB(s) + (unsigned)(i * 64 * g.cbB * 2), &tb, i * g.cbB, (int)p0, full(s));
+                }
+            }
+        }
+        *qprod = q;
+        if (!ok) *abort = 1;
+    } else if (warp == 1 && lane == 0) {
+        // ---- MMAs
+        const unsigned idesc = (1u << 4) | (1u << 7) | (1u << 10) | (g.wgrad ? (1u << 15) | (1u << 16) : 0u) |
+                               ((unsigned)(BN >> 3) << 17) | ((unsigned)(G_BM >> 4) << 24);
+        const int swA = 2 * g.cb, swB = g.wgrad ? 2 * g.cbB : 128;
+        int q = 0, it = 0;
+        bool ok = true;
+        for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x, it++) {
+            const int b = it & 1, ns = slices(tile);
+            if (!t_wait(tempty(b), (unsigned)(((it >> 1) & 1) ^ 1), g.wait, abort)) {
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const unsigned acc = tmem + (unsigned)(b * Cf::COLS);
+            for (int j = 0; j < ns; j++, q++) {
+                const int s = q % S;
+                if (!t_wait(full(s), (unsigned)((q / S) & 1), g.wait, abort)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                if (!g.wgrad) {
+                    const int nb = min(nbox - j * nbs, nbs), steps = nb * g.cb / 16;
+                    for (int kk = 0; kk < steps; kk++) {
+                        const int i = kk * 16 / g.cb, off = (kk * 16 % g.cb) * 2;
+                        const unsigned long long ad =
+                            t_desc(stageA(s) + (unsigned)(i * G_BM * swA + off), 16, (unsigned)(8 * swA), swA);
+                        const unsigned long long bd = t_desc(stageB(s) + (unsigned)(kk * 32), 16, 1024, 128);
+                        t_mma(acc, ad, bd, idesc, (j | kk) != 0);
+                    }
+                } else {
+                    for (int kk = 0; kk < 4; kk++) {
+                        const unsigned long long ad = t_desc(stageA(s) + (unsigned)(kk * 16 * swA),
+                                                             (unsigned)(64 * swA), (unsigned)(8 * swA), swA);
+                        const unsigned long long bd = t_desc(stageB(s) + (unsigned)(kk * 16 * swB),
+                                                             (unsigned)(64 * swB), (unsigned)(8 * swB), swB);
+                        t_mma(acc, ad, bd, idesc, (j | kk) != 0);
+                    }
+                }
+                t_commit(empty(s));   // the stage is free once these MMAs have read it
+            }
+            if (!ok) break;
+            t_commit(tfull(b));       // the accumulator is complete once every MMA so far is
+        }
+        *qmma = q;
+        if (!ok) *abort = 1;
+    } else if (warp >= 2) {
+        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
+        const int quarter = warp & 3;
+        int it = 0;
+        for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, it++) {
+            const int b = it & 1;
+            // every lane waits (and acquires); the warp goes on only if all lanes saw the
+            // accumulator complete (tcgen05.ld is warp-collective)
+            const bool seen = t_wait(tfull(b), (unsigned)((it >> 1) & 1), g.wait, abort);
+            if (!__all_sync(0xffffffffu, seen)) {
+                if (lane == 0) *abort = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const long long row = (long long)t_mi(tile) * G_BM + quarter * 32 + lane;
+            const long long n0 = (long long)t_ni(tile) * BN;
+            float* c32 = g.C32 ? g.C32 + (long long)t_z(tile) * g.M * g.N : nullptr;
+#pragma unroll 1
+            for (int c = 0; c < BN; c += 32) {
+                float v[32];
+                g_ld32(tmem + (unsigned)(b * Cf::COLS + c) + ((unsigned)(quarter * 32) << 16), v);
+                const long long col = n0 + c;
+                if (row >= g.M || col >= g.N) continue;
+                const int nv = (int)min((long long)32, g.N - col);
+                if (g.relu) {
+#pragma unroll
+                    for (int i = 0; i < 32; i++) v[i] = fmaxf(v[i], 0.f);
+                }
+                if (c32) {
+                    float* dst = c32 + row * g.N + col;
+#pragma unroll
+                    for (int i = 0; i < 32; i += 8)
+                        if (i < nv) {
+                            *reinterpret_cast<float4*>(dst + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+                            *reinterpret_cast<float4*>(dst + i + 4) =
+                                make_float4(v[i + 4], v[i + 5], v[i + 6], v[i + 7]);
+                        }
+                }
+                if (g.C16) {
+                    bf16* dst = g.C16 + row * g.N + col;
+#pragma unroll
+                    for (int i = 0; i < 32; i += 8)
+                        if (i < nv) {
+                            uint4 u;
+                            bf16* ub = reinterpret_cast<bf16*>(&u);
+#pragma unroll
+                            for (int e = 0; e < 8; e++) ub[e] = __float2bfloat16_rn(v[i + e]);
+                            *reinterpret_cast<uint4*>(dst + i) = u;
+                        }
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) t_arrive(tempty(b));
+        }
+    }
+    __syncthreads();
+    if (*abort && tid == 0) {
+        // drain: copies issued but never consumed, then the MMAs (all complete
+        // once the last committed batch is), before the tensor memory is freed
+        bool drained = true;
+        const volatile int never = 0;
+        for (int q = *qmma; q < *qprod; q++)
+            drained = t_wait(full(q % S), (unsigned)((q / S) & 1), G_DRAIN, &never) && drained;
+        if (*qmma > 0) {
+            const int q = *qmma - 1;
+            drained = t_wait(empty(q % S), (unsigned)((q / S) & 1), G_DRAIN, &never) && drained;
+        }
+        atomicMax(&g_gemm_err, drained ? 1 : 2);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cf::TALLOC) : "memory");
+}
+
 int g_sms()
 {
     int dev = 0, n = 148;
@@ -764,6 +1104,114 @@ void conv_geometry(int n, int h, int w, int cin, int cout)
     if (h >= (1 << 15) || w >= (1 << 15)) throw Error(EIO_ERR_ARG, "conv3x3: height and width below 32768");
 }
 
+// ---- TMA path (k_conv_tma): tensor maps and eligibility
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+int g_use_tma = 1;
+
+EncodeTiledFn tma_encoder()
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        GCUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !p) throw Error(EIO_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+        fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// BF16 tensor map: dims / box innermost first, strides (bytes) of dims 1 ..;
+// swizzle = the box's inner extent in bytes (32, 64 or 128); out-of-bounds reads give zeros
+void tma_map(CUtensorMap* m, const void* base, int rank, const cuuint64_t* dims, const cuuint64_t* strides,
+             const cuuint32_t* box, int swz)
+{
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    const CUtensorMapSwizzle sw = swz == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                  : swz == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                              : CU_TENSOR_MAP_SWIZZLE_32B;
+    const CUresult r = tma_encoder()(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (cuuint32_t)rank, const_cast<void*>(base),
+                                     dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+                                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(EIO_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+}
+
+// the largest of 64 / 32 / 16 channels dividing c (0: none)
+int chan_block(long long c) { return c % 64 == 0 ? 64 : c % 32 == 0 ? 32 : c % 16 == 0 ? 16 : 0; }
+
+// a box of px pixels as a bw x bh rectangle that tiles the h x w image
+bool rect_box(int h, int w, int px, int* bw, int* bh)
+{
+    if (w % px == 0) {
+        *bw = px;
+        *bh = 1;
+        return true;
+    }
+    if (px % w == 0 && h % (px / w) == 0) {
+        *bw = w;
+        *bh = px / w;
+        return true;
+    }
+    return false;
+}
+
+int tma_bn(long long n)
+{
+    const int opts[] = {16, 32, 64, 96, 128, 192, 256};
+    for (int b : opts)
+        if (n <= b) return b;
+    return 192;
+}
+
+template <int BN>
+void launch_tma(const CUtensorMap& ta, const CUtensorMap& tb, const ConvTma& a, cudaStream_t st)
+{
+    static int opened[64] = {};
+    int dev = 0;
+    GCUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw Error(EIO_ERR_ARG, "device index above 63");
+    if (!opened[dev]) {
+        GCUDA(cudaFuncSetAttribute(k_conv_tma<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, TCfg<BN>::SMEM));
+        opened[dev] = 1;
+    }
+    const long long tiles = (long long)a.mt * a.nt * a.splits;
+    k_conv_tma<BN><<<(unsigned)std::min<long long>(tiles, g_sms()), T_THREADS, TCfg<BN>::SMEM, st>>>(ta, tb, a);
+    GCUDA(cudaGetLastError());
+}
+void launch_tma_any(int bn, const CUtensorMap& ta, const CUtensorMap& tb, const ConvTma& a, cudaStream_t st)
+{
+    switch (bn) {
+        case 16: launch_tma<16>(ta, tb, a, st); break;
+        case 32: launch_tma<32>(ta, tb, a, st); break;
+        case 64: launch_tma<64>(ta, tb, a, st); break;
+        case 96: launch_tma<96>(ta, tb, a, st); break;
+        case 128: launch_tma<128>(ta, tb, a, st); break;
+        case 192: launch_tma<192>(ta, tb, a, st); break;
+        default: launch_tma<256>(ta, tb, a, st); break;
+    }
+}
+
+// eligibility and splits of the two TMA forms
+bool tma_conv_ok(int h, int w, int cin)
+{
+    int bw, bh;
+    return g_use_tma && chan_block(cin) && rect_box(h, w, 128, &bw, &bh);
+}
+bool tma_wgrad_ok(int h, int w, int cin, int cout)
+{
+    int bw, bh;
+    return g_use_tma && chan_block(cin) && cout % 16 == 0 && cout <= 256 && rect_box(h, w, 64, &bw, &bh);
+}
+int tma_wgrad_splits(long long M, long long P, long long* kchunk)
+{
+    const long long base = (M + G_BM - 1) / G_BM, kt = P / 64;
+    long long s = (2LL * g_sms() + base - 1) / base;
+    s = std::max<long long>(1, std::min<long long>(s, kt / 4));
+    return fit_splits(kt, (int)std::min<long long>(s, 4096), kchunk);
+}
+
 unsigned chunks(long long values, const char* what)
 {
     if (values % 8) throw Error(EIO_ERR_ARG, std::string(what) + ": value counts must be multiples of 8");
@@ -816,6 +1264,9 @@ void gemm_bf16(long long M, long long N, long long K, const void* A, long long l
 
 void gemm_set_wait_limit(long long polls) { g_gemm_wait = polls < 0 ? G_WAIT : polls; }
 
+void unet_set_tma(int on) { g_use_tma = on ? 1 : 0; }
+int unet_get_tma() { return g_use_tma; }
+
 int gemm_status(int reset)
 {
     int e = 0;
@@ -837,6 +1288,38 @@ void unet_conv3x3(int n, int h, int w, int cin, int cout, const void* x, const v
     if (!y32 && !y16) throw Error(EIO_ERR_ARG, "conv3x3: no output");
     check16opt(y32, "FP32 output");
     check16opt(y16, "BF16 output");
+    if (tma_conv_ok(h, w, cin)) {
+        int bw, bh;
+        rect_box(h, w, 128, &bw, &bh);
+        ConvTma t{};
+        t.wgrad = 0;
+        t.C = cin;
+        t.cb = chan_block(cin);
+        t.W = w;
+        t.H = h;
+        t.M = (long long)n * h * w;
+        t.N = cout;
+        t.K = 9LL * cin;
+        const int bn = tma_bn(cout);
+        t.mt = (int)(t.M / G_BM);
+        t.nt = (int)((cout + bn - 1) / bn);
+        t.splits = 1;
+        t.C32 = y32;
+        t.C16 = static_cast<bf16*>(y16);
+        t.relu = relu;
+        t.wait = g_gemm_wait;
+        CUtensorMap ta, tb;
+        const cuuint64_t da[4] = {(cuuint64_t)cin, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)n};
+        const cuuint64_t sa[3] = {(cuuint64_t)cin * 2, (cuuint64_t)w * cin * 2, (cuuint64_t)h * w * cin * 2};
+        const cuuint32_t ba[4] = {(cuuint32_t)t.cb, (cuuint32_t)bw, (cuuint32_t)bh, 1};
+        tma_map(&ta, x, 4, da, sa, ba, 2 * t.cb);
+        const cuuint64_t db[2] = {(cuuint64_t)(9LL * cin), (cuuint64_t)cout};
+        const cuuint64_t sb[1] = {(cuuint64_t)(9LL * cin * 2)};
+        const cuuint32_t bb[2] = {64, (cuuint32_t)bn};
+        tma_map(&tb, wt, 2, db, sb, bb, 128);
+        launch_tma_any(bn, ta, tb, t, static_cast<cudaStream_t>(stream));
+        return;
+    }
     GemmArgs a{};
     a.A = static_cast<const bf16*>(x);
     a.B = static_cast<const bf16*>(wt);
@@ -858,7 +1341,12 @@ long long unet_wgrad_scratch(int n, int h, int w, int cin, int cout)
 {
     conv_geometry(n, h, w, cin, cout);
     const long long M = 9LL * cin, N = cout, K = (long long)n * h * w;
-    return (long long)wgrad_splits(M, N, K) * M * N;
+    long long need = (long long)wgrad_splits(M, N, K) * M * N;
+    if (tma_wgrad_ok(h, w, cin, cout)) {
+        long long kc;
+        need = std::max(need, (long long)tma_wgrad_splits(M, K, &kc) * M * N);
+    }
+    return need;
 }
 
 // dw[co][tap][ci] = sum_p dz[p][co] x[p + off(tap)][ci]: C[tap ci][co] with A
@@ -872,6 +1360,42 @@ void unet_conv3x3_wgrad(int n, int h, int w, int cin, int cout, const void* x, c
     check16(dz, "output gradient");
     check16(dw, "weight gradient");
     check16(scratch, "scratch");
+    auto st = static_cast<cudaStream_t>(stream);
+    if (tma_wgrad_ok(h, w, cin, cout)) {
+        int bw, bh;
+        rect_box(h, w, 64, &bw, &bh);
+        ConvTma t{};
+        t.wgrad = 1;
+        t.C = cin;
+        t.cb = chan_block(cin);
+        t.W = w;
+        t.H = h;
+        t.M = 9LL * cin;
+        t.N = cout;
+        t.K = (long long)n * h * w;
+        const int bn = tma_bn(cout);
+        t.cbB = chan_block(bn);
+        t.mt = (int)((t.M + G_BM - 1) / G_BM);
+        t.nt = 1;
+        t.splits = tma_wgrad_splits(t.M, t.K, &t.kchunk);
+        if ((long long)t.splits * t.M * t.N > scratch_floats)
+            throw Error(EIO_ERR_ARG, "conv3x3 weight gradient: scratch too small (eio_unet_wgrad_scratch)");
+        t.C32 = scratch;
+        t.wait = g_gemm_wait;
+        CUtensorMap ta, tb;
+        const cuuint64_t da[4] = {(cuuint64_t)cin, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)n};
+        const cuuint64_t sa[3] = {(cuuint64_t)cin * 2, (cuuint64_t)w * cin * 2, (cuuint64_t)h * w * cin * 2};
+        const cuuint32_t ba[4] = {(cuuint32_t)t.cb, (cuuint32_t)bw, (cuuint32_t)bh, 1};
+        tma_map(&ta, x, 4, da, sa, ba, 2 * t.cb);
+        const cuuint64_t db[2] = {(cuuint64_t)cout, (cuuint64_t)t.K};
+        const cuuint64_t sb[1] = {(cuuint64_t)cout * 2};
+        const cuuint32_t bb[2] = {(cuuint32_t)t.cbB, 64};
+        tma_map(&tb, dz, 2, db, sb, bb, 2 * t.cbB);
+        launch_tma_any(bn, ta, tb, t, st);
+        k_sum_splits<<<g_grid(t.M * t.N), 256, 0, st>>>(scratch, t.splits, t.M, t.N, 1, 0, dw, nullptr);
+        GCUDA(cudaGetLastError());
+        return;
+    }
     GemmArgs a{};
     a.A = static_cast<const bf16*>(x);
     a.B = static_cast<const bf16*>(dz);
@@ -886,7 +1410,6 @@ void unet_conv3x3_wgrad(int n, int h, int w, int cin, int cout, const void* x, c
         throw Error(EIO_ERR_ARG, "conv3x3 weight gradient: scratch too small (eio_unet_wgrad_scratch)");
     a.C32 = scratch;
     a.wait = g_gemm_wait;
-    auto st = static_cast<cudaStream_t>(stream);
     launch_any(a, st);
     k_sum_splits<<<g_grid(a.M * a.N), 256, 0, st>>>(scratch, a.splits, a.M, a.N, 1, 0, dw, nullptr);
     GCUDA(cudaGetLastError());

@@ -1737,6 +1737,15 @@ EIO_API int eio_gemm_status(int reset, int* err) {
         *err = gemm_status(reset);
     });
 }
+EIO_API int eio_unet_set_tma(int on) {
+    return guarded([&] { unet_set_tma(on); });
+}
+EIO_API int eio_unet_get_tma(int* on) {
+    return guarded([&] {
+        if (!on) throw Error(EIO_ERR_ARG, "null result");
+        *on = unet_get_tma();
+    });
+}
 EIO_API int eio_unet_conv3x3(int n, int h, int w, int cin, int cout, const void* x, const void* wt, float* y32,
                              void* y16, int relu, void* stream) {
     return guarded([&] { unet_conv3x3(n, h, w, cin, cout, x, wt, y32, y16, relu, stream); });

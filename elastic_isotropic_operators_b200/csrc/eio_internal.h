@@ -163,6 +163,8 @@ void gemm_bf16(long long M, long long N, long long K, const void* A, long long l
                float* C32, void* C16, const void* mask, int relu, int splits, float* scratch, void* stream);
 void gemm_set_wait_limit(long long polls);
 int gemm_status(int reset);
+void unet_set_tma(int on);
+int unet_get_tma();
 void unet_conv3x3(int n, int h, int w, int cin, int cout, const void* x, const void* wt, float* y32, void* y16,
                   int relu, void* stream);
 long long unet_wgrad_scratch(int n, int h, int w, int cin, int cout);

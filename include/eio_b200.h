@@ -477,6 +477,16 @@ int eio_gemm_bf16(long long M, long long N, long long K, const void *A, long lon
  * (synchronises) */
 int eio_gemm_set_wait_limit(long long polls);
 int eio_gemm_status(int reset, int *err);
+/* The convolution kernels bring their operands in by TMA where the image
+ * allows it (a 128-pixel tile, and a 64-pixel slice of the weight gradient,
+ * form a rectangle of the image: widths that divide 128 / 64 or are
+ * multiples of them, heights that the rectangle divides; input channels a
+ * multiple of 16; for the weight gradient cout a multiple of 16, <= 256):
+ * one 4-D tensor box per tap and channel block, the zero padding from the
+ * box's out-of-bounds fill.  Other shapes use the copy-loop kernel.  on = 0
+ * forces the copy loop everywhere (process-wide; default 1). */
+int eio_unet_set_tma(int on);
+int eio_unet_get_tma(int *on);
 /* 3x3 convolution (zero padding) as an implicit GEMM on tcgen05: y[p][co] =
  * sum_{tap, ci} x[p + off(tap)][ci] w[co][tap][ci], x BF16 [n][h][w][cin],
  * FP32 y32 and / or BF16 y16 [n][h][w][cout], ReLU when relu != 0.  The 3x3

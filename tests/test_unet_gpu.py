@@ -154,8 +154,53 @@ def test_conv3x3_weight_gradient_matches_numpy(n, h, w, cin, cout):
     assert torch.equal(dw, dw2)
     assert _status_clear() == 0
     with pytest.raises(_lib.EioError):
-        _lib.check(L.eio_unet_conv3x3_wgrad(n, h, w, cin, cout, _p(X), _p(DZ), _p(dw2), _p(scratch),
-                                            f.value - 1, None))
+        _lib.check(L.eio_unet_conv3x3_wgrad(n, h, w, cin, cout, _p(X), _p(DZ), _p(dw2), _p(scratch), 0, None))
+
+
+def _tma(on):
+    _lib.check(_lib.lib().eio_unet_set_tma(on))
+
+
+@pytest.mark.parametrize("n,h,w,cin,cout", [(2, 16, 8, 16, 32), (1, 4, 32, 32, 16), (2, 2, 64, 96, 32),
+                                             (1, 3, 128, 64, 64), (1, 2, 256, 128, 256), (2, 8, 16, 384, 128),
+                                             (1, 4, 32, 32, 384), (1, 8, 16, 256, 96)])
+def test_conv3x3_tma_path_matches_numpy_and_the_copy_loop(n, h, w, cin, cout):
+    """Shapes whose 128-pixel tiles (and 64-pixel weight-gradient slices) are
+    rectangles of the image run on the TMA kernel (one 4-D box per tap and
+    channel block, zero padding from the out-of-bounds fill): the convolution
+    against FP64 to 1e-5 and bitwise equal to the copy-loop kernel (the same K
+    order); the weight gradient against FP64 to 1e-5 and the copy loop to 1e-6
+    (the pixels are split differently)."""
+    rng = np.random.default_rng(n + 10 * h + w + cin + cout)
+    x = C.bf16_round(rng.standard_normal((n, h, w, cin)))
+    wt = C.bf16_round(rng.standard_normal((cout, 9, cin)) / np.sqrt(9 * cin))
+    dz = C.bf16_round(rng.standard_normal((n, h, w, cout)))
+    L = _lib.lib()
+    X, W, DZ = _bf(x), _bf(wt), _bf(dz)
+    f = ctypes.c_longlong()
+    _lib.check(L.eio_unet_wgrad_scratch(n, h, w, cin, cout, ctypes.byref(f)))
+    scratch = torch.empty((f.value,), dtype=torch.float32, device="cuda")
+    out = {}
+    try:
+        for on in (1, 0):
+            _tma(on)
+            y32 = torch.empty((n, h, w, cout), dtype=torch.float32, device="cuda")
+            y16 = torch.empty((n, h, w, cout), dtype=torch.bfloat16, device="cuda")
+            dw = torch.empty((cout, 9, cin), dtype=torch.float32, device="cuda")
+            _lib.check(L.eio_unet_conv3x3(n, h, w, cin, cout, _p(X), _p(W), _p(y32), _p(y16), 1, None))
+            _lib.check(L.eio_unet_conv3x3_wgrad(n, h, w, cin, cout, _p(X), _p(DZ), _p(dw), _p(scratch), f.value,
+                                                None))
+            torch.cuda.synchronize()
+            out[on] = (y32.cpu().numpy(), _np(y16), dw.cpu().numpy())
+    finally:
+        _tma(1)
+    assert _status_clear() == 0
+    want = np.maximum(C._conv(x, wt), 0.0)
+    assert _rel(out[1][0], want) < 1e-5
+    assert np.array_equal(out[1][0], out[0][0])
+    assert np.array_equal(out[1][1], C.bf16_round(out[1][0]))
+    assert _rel(out[1][2], C._wgrad(x, dz)) < 1e-5
+    assert _rel(out[1][2], out[0][2]) < 1e-6
 
 
 def test_flip():
