@@ -65,11 +65,13 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="born_600x1800",
                     choices=["born_600x1800", "nl_312x520", "nl_shots", "fwi_1000x3400", "fwi_learned",
-                             "cnn_train"])
+                             "cnn_train", "fwi_cfg5"])
     ap.add_argument("--batch", type=int, default=None,
                     help="shots per lockstep launch (1 = one shot at a time on the lanes); nl_shots default 8, "
                          "born_600x1800 default: the library's (1)")
-    ap.add_argument("--pairs", type=int, default=48, help="fwi_learned: Born training pairs")
+    ap.add_argument("--pairs", type=int, default=48, help="fwi_learned / fwi_cfg5: Born training pairs")
+    ap.add_argument("--reduced", action="store_true",
+                    help="fwi_cfg5: the 136x520, 8-shot, nts=1200 stand-in instead of 1000x3400 (a quick check)")
     ap.add_argument("--conv-path", type=int, default=-1, choices=[-1, 0, 1],
                     help="cnn_train: forward convolutions on mma.sync (0) or tcgen05 (1); "
                          "-1 keeps the library default (mma.sync)")
@@ -869,6 +871,158 @@ class _Reached(Exception):
     pass
 
 
+def _interior_error(m, true, pad):
+    """Relative L2 error of each elastic parameter against the true model over
+    the interior (the absorbing pads excluded)."""
+    sl = (slice(None), slice(pad, -pad), slice(pad, -pad))
+    d = (np.asarray(m, np.float64) - true)[sl]
+    t = np.asarray(true, np.float64)[sl]
+    return [round(float(np.linalg.norm(d[c]) / np.linalg.norm(t[c])), 6) for c in range(3)]
+
+
+CFG5_BANDS = ((0.5, 1.0, 3.0, 4.5), (0.5, 1.0, 5.0, 6.5), (0.5, 1.0, 10.0, 12.0))   # 3 -> 5 -> 10 Hz
+
+
+def run_ours_cfg5(args, ws, rank, local):
+    """End-to-end elastic FWI on the batched-FWI model (1000x3400, 120 shots,
+    nts=5000 at 1 ms): L-BFGS over the 3 -> 5 -> 10 Hz bands (fwi.multiscale,
+    --steps iterations per band, 10 by default: 30 in all), once with the plain
+    gradient and once with learned steps (precond.LearnedPreconditioner, U-Net
+    by default: --pairs Born normal-operator images J^T J dm of seeded smooth
+    perturbations at the start model, --epochs of training; each learned step
+    is kept only when the exact misfit accepts it, else the plain step runs).
+    Reports the wall-clock to a 1e-2 reduction of the final band's misfit,
+    the learned method's wall-clock (with and without training) to the plain
+    method's final misfit, iterations and the model error against the true
+    model.  --reduced: the 136x520, 8-shot stand-in (a quick check)."""
+    import torch
+    from elastic_isotropic_operators_b200 import _lib, fwi, precond, prop, synthetic
+    if args.reduced:
+        nsh = args.shots or 8
+        w = synthetic.fwi_1000x3400(nz=136, nx=520, nts=1200, nshots=nsh, nrec=60, pad=20, window_km=(2.0, 4.0))
+        pad = 20
+    else:
+        nsh = args.shots or 120
+        w = synthetic.fwi_1000x3400(nshots=nsh)
+        pad = 50
+    w.par.set("iGpu", str(local))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    src, rec = w.geometry()
+    sig = w.source_signal()
+    nl = prop.nonlinearFwiPropElasticShotsGpu(w.elastic, w.par, sig[None], *src, *rec)
+    born = prop.BornElasticShotsGpu(w.elastic, w.par, [sig], *src, *rec)
+    for op in (nl, born):
+        pin_kernel(op._L, op.ctx, args)
+    true = np.asarray(w.extra["true_model"], np.float64)
+    pad += synthetic.FAT                                       # the interior starts past the pads and the stencil halo
+    d_obs = nl.dataSpace()
+    nl.forward(False, w.extra["true_model"], d_obs)          # observed data from the true model, untimed
+    d_obs = np.array(d_obs.getNdArray(), copy=True)
+    m0 = w.extra["start_model"]
+    niter = args.steps
+    final_band = CFG5_BANDS[-1]
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1) / 1e3
+
+    # the final band's misfit at the start model (untimed): the reference of the 1e-2 reduction
+    f0 = fwi.band_objective(nl, born, d_obs, None, w.dts, final_band).value(m0)
+
+    def run_traced(precond_obj):
+        """multiscale L-BFGS; trace: per iteration (band, iteration, misfit, seconds since the start)"""
+        trace, stats = [], {}
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev0.record()
+
+        def objective_for_band(band):
+            return fwi.band_objective(nl, born, d_obs, None, w.dts, band)
+
+        def cb(k, it, m, f, g):
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record()
+            torch.cuda.synchronize()
+            trace.append((k, it + 1, float(f), ev0.elapsed_time(ev) / 1e3))
+
+        m, hists = fwi.multiscale(objective_for_band, m0, CFG5_BANDS, niter=niter, iter_callback=cb, scale=m0,
+                                  precond=precond_obj, stats=stats)
+        return m, hists, trace, stats
+
+    # plain
+    barrier(ws)
+    clocks = ClockSampler(None)
+    clocks.start()
+    (m_plain, h_plain, tr_plain, _), t_plain = timed(lambda: run_traced(None))
+    # learned: training pairs + training at the start model (broadband sources), then the same multiscale run
+    P = [None]
+
+    def train():
+        born.setSourceSignals([sig])
+        net = (precond.ConvNet(depth=args.depth, device=local, seed=0) if args.net == "convnet" else
+               precond.UNet(device=local, seed=0))
+        P[0] = precond.LearnedPreconditioner(born, m0, sigma=args.sigma, seed=0, net=net)
+        X, T, _, _ = P[0].make_pairs(args.pairs, seed=1)
+        P[0].train(X, T, epochs=args.epochs, batch=min(4, args.pairs), lr=1e-3)
+
+    _, t_train = timed(train)
+    (m_learn, h_learn, tr_learn, st_learn), t_learn = timed(lambda: run_traced(P[0]))
+    clk = clocks.stop()
+    f_plain_end = fwi.band_objective(nl, born, d_obs, None, w.dts, final_band).value(m_plain)
+    f_learn_end = fwi.band_objective(nl, born, d_obs, None, w.dts, final_band).value(m_learn)
+    # wall-clock to a 1e-2 reduction of the final band's misfit and, for the learned run, to the plain run's
+    # final misfit: the first iteration of the final band at or below the level (None if never)
+    def first(trace, level, offset=0.0):
+        for b, it, f, t in trace:
+            if b == len(CFG5_BANDS) - 1 and f <= level:
+                return round(t + offset, 3)
+        return None
+    t1e2_plain = first(tr_plain, 1e-2 * f0)
+    t1e2_learn = first(tr_learn, 1e-2 * f0)
+    plain_final = tr_plain[-1][2] if tr_plain else None
+    t_to_plain = first(tr_learn, plain_final) if plain_final is not None else None
+    err0, err_plain, err_learn = _interior_error(m0, true, pad), _interior_error(m_plain, true, pad), \
+        _interior_error(m_learn, true, pad)
+    speed = (round(t_plain / (t_to_plain + t_train), 3) if t_to_plain is not None else 0.0)
+    speed_nt = (round(t_plain / t_to_plain, 3) if t_to_plain else 0.0)
+    grid = "136x520 stand-in" if args.reduced else "1000x3400"
+    return {"metric": "FWI wall-clock speed-up to the plain method's final misfit (learned vs plain, training "
+                      "included)", "value": speed, "unit": "x", "n_gpus": ws, "steps": 3 * niter,
+            "warmup": 0, "ms_per_step": round(1e3 * t_plain / (3 * niter), 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 propagation, bf16 network", "data": "synthetic",
+            "config": {"workload": "fwi_cfg5: %s batched-FWI model (12.5 m, nts=%d at 1 ms, %d shots with 2-8 km "
+                                   "windows), L-BFGS over the 3/5/10 Hz bands, %d iterations each, plain vs "
+                                   "learned (%s, %d Born normal-operator images, %d epochs)"
+                                   % (grid, w.nts, nsh, niter, "ConvNet" if args.net == "convnet" else "U-Net",
+                                      args.pairs, args.epochs),
+                       "l2": "each gradient streams the source history of every shot through HBM"},
+            "speedup_without_training": speed_nt, "target": ">= 3x", "target_met": bool(speed >= 3.0),
+            "final_band_misfit_at_start": f0,
+            "plain": {"seconds": round(t_plain, 3), "iterations": len(tr_plain),
+                      "final_band_misfit_reduction": round(f_plain_end / f0, 6),
+                      "seconds_to_1e-2_reduction": t1e2_plain,
+                      "band_histories": [[float(v) for v in h] for h in h_plain],
+                      "model_rel_error_rho_lambda_mu": err_plain},
+            "learned": {"seconds": round(t_learn, 3), "training_seconds": round(t_train, 3),
+                        "iterations": len(tr_learn),
+                        "final_band_misfit_reduction": round(f_learn_end / f0, 6),
+                        "seconds_to_1e-2_reduction": t1e2_learn,
+                        "seconds_to_plain_final_misfit": t_to_plain,
+                        "learned_steps_accepted": st_learn.get("learned", 0),
+                        "learned_steps_rejected": st_learn.get("rejected", 0),
+                        "band_histories": [[float(v) for v in h] for h in h_learn],
+                        "model_rel_error_rho_lambda_mu": err_learn},
+            "start_model_rel_error_rho_lambda_mu": err0,
+            "cpu_baseline": None, "clocks": clk,
+            "gpu_launches": int(sum(read_stats(_lib.lib(), op.ctx)["launches"] for op in (nl, born)))}
+
+
 def run_ours_learned(args, ws, rank, local):
     """Learned vs plain FWI: wall-clock to the misfit that plain L-BFGS reaches in
     --steps iterations, plain against learned (Born training pairs + training +
@@ -1210,6 +1364,8 @@ def main():
         out = run_ours_nl_shots(args, ws, rank, local)
     elif args.workload == "fwi_learned":
         out = run_ours_learned(args, ws, rank, local)
+    elif args.workload == "fwi_cfg5":
+        out = run_ours_cfg5(args, ws, rank, local)
     elif args.workload == "cnn_train":
         out = run_ours_cnn(args, ws, rank, local)
     else:

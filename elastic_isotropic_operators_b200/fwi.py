@@ -484,16 +484,18 @@ def band_objective(nl, born, d_obs, sources, dts, band, **objective_kw):
     return FwiObjective(nl, born, d_b, **objective_kw)
 
 
-def multiscale(objective_for_band, m0, bands, niter=10, callback=None, **lbfgs_kw):
+def multiscale(objective_for_band, m0, bands, niter=10, callback=None, iter_callback=None, **lbfgs_kw):
     """L-BFGS band after band: ``objective_for_band(band)`` gives the objective
     of a band (e.g. band_objective), each band starts from the model the
-    previous one reached.  ``callback(k, band, m, history)`` after each band.
-    Returns (m, [history of each band])."""
+    previous one reached.  ``callback(k, band, m, history)`` after each band;
+    ``iter_callback(k, it, m, f, g)`` after each iteration of band k (the
+    L-BFGS callback).  Returns (m, [history of each band])."""
     m = np.array(m0, dtype=np.float32, copy=True)
     hists = []
     for k, band in enumerate(bands):
         obj = objective_for_band(band)
-        m, hist = lbfgs(obj, m, niter=niter, **lbfgs_kw)
+        cb = None if iter_callback is None else (lambda it, mm, f, g, k=k: iter_callback(k, it, mm, f, g))
+        m, hist = lbfgs(obj, m, niter=niter, callback=cb, **lbfgs_kw)
         hists.append(hist)
         if callback is not None:
             callback(k, band, m, hist)

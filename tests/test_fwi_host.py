@@ -138,10 +138,16 @@ def test_multiscale_runs_each_band_from_the_previous_model():
         seen.append(band)
         return Band(targets[band])
 
-    starts = []
+    starts, iters = [], []
     m, hists = fwi.multiscale(for_band, np.full(8, 0.5, np.float32), list(targets), niter=20, init_step=0.5,
-                              callback=lambda k, band, mk, h: starts.append(mk.copy()))
+                              callback=lambda k, band, mk, h: starts.append(mk.copy()),
+                              iter_callback=lambda k, it, mk, f, g: iters.append((k, it, f)))
     assert seen == list(targets) and len(hists) == 2
+    # the per-iteration hook sees every iteration of every band, tagged with the band, misfits as recorded
+    for k in (0, 1):
+        fk = [f for kk, it, f in iters if kk == k]
+        assert [it for kk, it, f in iters if kk == k] == list(range(len(fk)))
+        assert np.allclose(fk, hists[k][1:len(fk) + 1])
     assert np.allclose(starts[0], 1.0, atol=1e-3) and np.allclose(m, 2.0, atol=1e-3)
     # the second band started where the first ended: its first misfit is that of m = 1
     assert abs(hists[1][0] - 0.5 * 8 * 1.0) < 1e-2
