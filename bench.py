@@ -72,6 +72,12 @@ def parse():
     ap.add_argument("--pairs", type=int, default=48, help="fwi_learned / fwi_cfg5: Born training pairs")
     ap.add_argument("--reduced", action="store_true",
                     help="fwi_cfg5: the 136x520, 8-shot, nts=1200 stand-in instead of 1000x3400 (a quick check)")
+    ap.add_argument("--phase", default="both", choices=["both", "plain", "learned"],
+                    help="fwi_cfg5: run both methods, or one (a long run split over two calls)")
+    ap.add_argument("--record", default=None,
+                    help="fwi_cfg5: write the plain method's results to this JSON file as soon as they exist")
+    ap.add_argument("--plain-record", default=None,
+                    help="fwi_cfg5 --phase learned: the plain method's results (--record of a --phase plain run)")
     ap.add_argument("--conv-path", type=int, default=-1, choices=[-1, 0, 1],
                     help="cnn_train: forward convolutions on mma.sync (0) or tcgen05 (1); "
                          "-1 keeps the library default (mma.sync)")
@@ -955,45 +961,73 @@ def run_ours_cfg5(args, ws, rank, local):
                                   precond=precond_obj, stats=stats)
         return m, hists, trace, stats
 
-    # plain
+    def first(trace, level):
+        """seconds at the first final-band iteration whose misfit is at or below level (None: never)"""
+        for b, it, f, t in trace:
+            if b == len(CFG5_BANDS) - 1 and f <= level:
+                return round(t, 3)
+        return None
+
     barrier(ws)
     clocks = ClockSampler(None)
     clocks.start()
-    (m_plain, h_plain, tr_plain, _), t_plain = timed(lambda: run_traced(None))
-    # learned: training pairs + training at the start model (broadband sources), then the same multiscale run
-    P = [None]
+    if args.phase in ("both", "plain"):
+        (m_plain, h_plain, tr_plain, _), t_plain = timed(lambda: run_traced(None))
+        f_plain_end = fwi.band_objective(nl, born, d_obs, None, w.dts, final_band).value(m_plain)
+        plain = {"seconds": round(t_plain, 3), "iterations": len(tr_plain),
+                 "final_band_misfit_reduction": round(f_plain_end / f0, 6),
+                 "seconds_to_1e-2_reduction": first(tr_plain, 1e-2 * f0),
+                 "band_histories": [[float(v) for v in h] for h in h_plain],
+                 "model_rel_error_rho_lambda_mu": _interior_error(m_plain, true, pad),
+                 "trace": [list(t) for t in tr_plain]}
+        if args.record and rank == 0:
+            with open(args.record, "w") as f:
+                json.dump(plain, f)
+        print("fwi_cfg5 plain: %.1f s, final-band misfit reduction %.4g" % (t_plain, f_plain_end / f0),
+              file=sys.stderr, flush=True)
+    else:
+        if not args.plain_record:
+            raise SystemExit("fwi_cfg5 --phase learned needs --plain-record (the JSON of a --phase plain run)")
+        with open(args.plain_record) as f:
+            plain = json.load(f)
+        t_plain = plain["seconds"]
+    tr_plain = [tuple(t) for t in plain["trace"]]
+    learned, t_train, t_to_plain = None, 0.0, None
+    if args.phase in ("both", "learned"):
+        # training pairs + training at the start model (broadband sources), then the same multiscale run
+        P = [None]
 
-    def train():
-        born.setSourceSignals([sig])
-        net = (precond.ConvNet(depth=args.depth, device=local, seed=0) if args.net == "convnet" else
-               precond.UNet(device=local, seed=0))
-        P[0] = precond.LearnedPreconditioner(born, m0, sigma=args.sigma, seed=0, net=net)
-        X, T, _, _ = P[0].make_pairs(args.pairs, seed=1)
-        P[0].train(X, T, epochs=args.epochs, batch=min(4, args.pairs), lr=1e-3)
+        def train():
+            born.setSourceSignals([sig])
+            net = (precond.ConvNet(depth=args.depth, device=local, seed=0) if args.net == "convnet" else
+                   precond.UNet(device=local, seed=0))
+            P[0] = precond.LearnedPreconditioner(born, m0, sigma=args.sigma, seed=0, net=net)
+            X, T, _, _ = P[0].make_pairs(args.pairs, seed=1)
+            P[0].train(X, T, epochs=args.epochs, batch=min(4, args.pairs), lr=1e-3)
 
-    _, t_train = timed(train)
-    (m_learn, h_learn, tr_learn, st_learn), t_learn = timed(lambda: run_traced(P[0]))
+        _, t_train = timed(train)
+        (m_learn, h_learn, tr_learn, st_learn), t_learn = timed(lambda: run_traced(P[0]))
+        f_learn_end = fwi.band_objective(nl, born, d_obs, None, w.dts, final_band).value(m_learn)
+        plain_final = tr_plain[-1][2] if tr_plain else None
+        t_to_plain = first(tr_learn, plain_final) if plain_final is not None else None
+        learned = {"seconds": round(t_learn, 3), "training_seconds": round(t_train, 3),
+                   "iterations": len(tr_learn),
+                   "final_band_misfit_reduction": round(f_learn_end / f0, 6),
+                   "seconds_to_1e-2_reduction": first(tr_learn, 1e-2 * f0),
+                   "seconds_to_plain_final_misfit": t_to_plain,
+                   "learned_steps_accepted": st_learn.get("learned", 0),
+                   "learned_steps_rejected": st_learn.get("rejected", 0),
+                   "band_histories": [[float(v) for v in h] for h in h_learn],
+                   "model_rel_error_rho_lambda_mu": _interior_error(m_learn, true, pad)}
     clk = clocks.stop()
-    f_plain_end = fwi.band_objective(nl, born, d_obs, None, w.dts, final_band).value(m_plain)
-    f_learn_end = fwi.band_objective(nl, born, d_obs, None, w.dts, final_band).value(m_learn)
-    # wall-clock to a 1e-2 reduction of the final band's misfit and, for the learned run, to the plain run's
-    # final misfit: the first iteration of the final band at or below the level (None if never)
-    def first(trace, level, offset=0.0):
-        for b, it, f, t in trace:
-            if b == len(CFG5_BANDS) - 1 and f <= level:
-                return round(t + offset, 3)
-        return None
-    t1e2_plain = first(tr_plain, 1e-2 * f0)
-    t1e2_learn = first(tr_learn, 1e-2 * f0)
-    plain_final = tr_plain[-1][2] if tr_plain else None
-    t_to_plain = first(tr_learn, plain_final) if plain_final is not None else None
-    err0, err_plain, err_learn = _interior_error(m0, true, pad), _interior_error(m_plain, true, pad), \
-        _interior_error(m_learn, true, pad)
+    err0 = _interior_error(m0, true, pad)
+    plain.pop("trace", None)
     speed = (round(t_plain / (t_to_plain + t_train), 3) if t_to_plain is not None else 0.0)
     speed_nt = (round(t_plain / t_to_plain, 3) if t_to_plain else 0.0)
     grid = "136x520 stand-in" if args.reduced else "1000x3400"
     return {"metric": "FWI wall-clock speed-up to the plain method's final misfit (learned vs plain, training "
-                      "included)", "value": speed, "unit": "x", "n_gpus": ws, "steps": 3 * niter,
+                      "included)", "value": speed if learned is not None else None, "unit": "x", "n_gpus": ws,
+            "steps": 3 * niter,
             "warmup": 0, "ms_per_step": round(1e3 * t_plain / (3 * niter), 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 propagation, bf16 network", "data": "synthetic",
             "config": {"workload": "fwi_cfg5: %s batched-FWI model (12.5 m, nts=%d at 1 ms, %d shots with 2-8 km "
@@ -1003,21 +1037,7 @@ def run_ours_cfg5(args, ws, rank, local):
                                       args.pairs, args.epochs),
                        "l2": "each gradient streams the source history of every shot through HBM"},
             "speedup_without_training": speed_nt, "target": ">= 3x", "target_met": bool(speed >= 3.0),
-            "final_band_misfit_at_start": f0,
-            "plain": {"seconds": round(t_plain, 3), "iterations": len(tr_plain),
-                      "final_band_misfit_reduction": round(f_plain_end / f0, 6),
-                      "seconds_to_1e-2_reduction": t1e2_plain,
-                      "band_histories": [[float(v) for v in h] for h in h_plain],
-                      "model_rel_error_rho_lambda_mu": err_plain},
-            "learned": {"seconds": round(t_learn, 3), "training_seconds": round(t_train, 3),
-                        "iterations": len(tr_learn),
-                        "final_band_misfit_reduction": round(f_learn_end / f0, 6),
-                        "seconds_to_1e-2_reduction": t1e2_learn,
-                        "seconds_to_plain_final_misfit": t_to_plain,
-                        "learned_steps_accepted": st_learn.get("learned", 0),
-                        "learned_steps_rejected": st_learn.get("rejected", 0),
-                        "band_histories": [[float(v) for v in h] for h in h_learn],
-                        "model_rel_error_rho_lambda_mu": err_learn},
+            "final_band_misfit_at_start": f0, "phase": args.phase, "plain": plain, "learned": learned,
             "start_model_rel_error_rho_lambda_mu": err0,
             "cpu_baseline": None, "clocks": clk,
             "gpu_launches": int(sum(read_stats(_lib.lib(), op.ctx)["launches"] for op in (nl, born)))}

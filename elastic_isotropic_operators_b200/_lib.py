@@ -21,6 +21,7 @@ _ERRORS = {
     -5: "unsupported option",
     -6: "out of memory",
     -7: "device wait timed out",
+    -8: "non-finite output",
 }
 
 F = ctypes.c_float
@@ -108,6 +109,11 @@ _SIGS = {
                           ctypes.c_longlong, P, P, P, I, I, P, P]),
     "eio_gemm_set_wait_limit": (I, [ctypes.c_longlong]),
     "eio_gemm_status": (I, [I, P]),
+    "eio_ctx_set_history_location": (I, [P, I]),
+    "eio_ctx_get_history_location": (I, [P, P]),
+    "eio_ctx_set_check_finite": (I, [P, I]),
+    "eio_set_device_memory_cap": (I, [ctypes.c_longlong]),
+    "eio_get_device_memory_used": (I, [P]),
     "eio_unet_set_tma": (I, [I]),
     "eio_unet_get_tma": (I, [P]),
     "eio_unet_conv3x3": (I, [I, I, I, I, I, P, P, P, P, I, P]),

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -33,26 +34,68 @@ namespace eio {
             throw Error(EIO_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_));               \
     } while (0)
 
-// growable device buffer
+// Bytes the library's growable buffers hold on the devices, and an optional
+// cap on them (eio_set_device_memory_cap: 0 = none), so that an out-of-memory
+// condition can be produced on purpose and its handling tested.
+std::atomic<long long> g_dbuf_used{0};
+std::atomic<long long> g_dbuf_cap{0};
+
+// growable device buffer; where = 0 (the source history): device memory, or
+// mapped pinned host memory reached through its device address when the
+// device allocation does not fit; 1: device only; 2: host only
 struct DBuf {
-    void* p = nullptr;
+    void* p = nullptr;      // device address (the mapped alias for host memory)
     size_t cap = 0;
-    void ensure(size_t bytes) {
-        if (bytes <= cap) return;
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-        cudaError_t e = cudaMalloc(&p, bytes);
-        if (e != cudaSuccess) {
+    bool host = false;
+    void* hp = nullptr;     // host address of mapped memory
+    void ensure(size_t bytes, int where = 1) {
+        if (bytes <= cap && (where == 0 || host == (where == 2))) return;
+        release();
+        if (where != 2) {
+            const long long lim = g_dbuf_cap.load();
+            const bool capped = lim > 0 && g_dbuf_used.load() + (long long)bytes > lim;
+            cudaError_t e = capped ? cudaErrorMemoryAllocation : cudaMalloc(&p, bytes);
+            if (e == cudaSuccess) {
+                cap = bytes;
+                g_dbuf_used += (long long)bytes;
+                return;
+            }
             p = nullptr;
-            throw Error(e == cudaErrorMemoryAllocation ? EIO_ERR_NOMEM : EIO_ERR_CUDA,
-                        std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+            if (!capped) cudaGetLastError();   // a failed allocation leaves no sticky error
+            if (e != cudaErrorMemoryAllocation)
+                throw Error(EIO_ERR_CUDA, std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+            if (where == 1)
+                throw Error(EIO_ERR_NOMEM, std::string("cudaMalloc(") + std::to_string(bytes) + "): " +
+                                               (capped ? "above the library's device-memory cap" : cudaGetErrorString(e)));
         }
+        cudaError_t e = cudaHostAlloc(&hp, bytes, cudaHostAllocMapped | cudaHostAllocPortable);
+        if (e != cudaSuccess) {
+            hp = nullptr;
+            cudaGetLastError();
+            throw Error(EIO_ERR_NOMEM, std::string("neither device nor pinned host memory for ") + std::to_string(bytes) +
+                                           " bytes: " + cudaGetErrorString(e));
+        }
+        void* dp = nullptr;
+        e = cudaHostGetDevicePointer(&dp, hp, 0);
+        if (e != cudaSuccess) {
+            cudaFreeHost(hp);
+            hp = nullptr;
+            throw Error(EIO_ERR_CUDA, std::string("cudaHostGetDevicePointer: ") + cudaGetErrorString(e));
+        }
+        p = dp;
+        host = true;
         cap = bytes;
     }
     void release() {
-        if (p) cudaFree(p);
+        if (host) {
+            if (hp) cudaFreeHost(hp);
+        } else if (p) {
+            cudaFree(p);
+            g_dbuf_used -= (long long)cap;
+        }
         p = nullptr;
+        hp = nullptr;
+        host = false;
         cap = 0;
     }
     float* f() const { return static_cast<float*>(p); }
@@ -85,6 +128,7 @@ struct Engine {
     float dts_inv = 0.f;
     int ntz = 0, ntx = 0, ntiles = 0;
     int ckpt = 0;           // source-wavefield snapshots: 0 FP32, 1 BF16, 2 FP16 (scaled per snapshot)
+    int hist_where = 0;     // source-wavefield history: 0 device, host when it does not fit; 1 device; 2 host
     DBuf Wq, wscale, wstage, wpmax;   // 16-bit history, scales [nts][2], FP32 staging row pair, warp maxima
     // wavefield levels: two sets of 5 slices for the single-step kernels, four
     // for the two-step kernel (it writes both new levels to the free sets)
@@ -1299,7 +1343,7 @@ static void born_source_q(Engine* e, const PointList& src, StepArgs a, const Spa
         throw Error(EIO_ERR_UNSUPPORTED, "16-bit source-wavefield snapshots need sub = 1 (two fine steps per sample)");
     const size_t qbytes = sizeof(unsigned short) * 2 * (size_t)e->nts * e->n;
     if (e->Wq.cap < qbytes || e->wq_n != e->n) {
-        e->Wq.ensure(qbytes);
+        e->Wq.ensure(qbytes, e->hist_where);
         EIO_CUDA(cudaMemsetAsync(e->Wq.p, 0, qbytes, e->st));   // the FAT frame is never written
         e->wq_n = e->n;
     }
@@ -1387,7 +1431,7 @@ static void born_source(Engine* e, const PointList& src, StepArgs a, const Spars
     }
     const size_t wbytes = sizeof(float) * 2 * (size_t)e->nts * e->n;
     const bool fresh = e->W.cap < wbytes;
-    e->W.ensure(wbytes);
+    e->W.ensure(wbytes, e->hist_where);
     const bool tri = (e->S == 2);
     // running sums need a zeroed history; single writes only need the never
     // written FAT frame to be zero, which holds from the first clear on
@@ -1768,7 +1812,18 @@ __global__ void __launch_bounds__(256) k_add4(float* __restrict__ dst, const flo
 
 bool engine_is_tuned(const Engine* e) { return e->tuned; }
 // device bytes of source-wavefield history this engine already holds
-size_t engine_history_bytes(const Engine* e) { return e->W.cap + e->Wq.cap; }
+size_t engine_history_bytes(const Engine* e) { return (e->W.host ? 0 : e->W.cap) + (e->Wq.host ? 0 : e->Wq.cap); }
+void engine_set_history_where(Engine* e, int where) {
+    if (where < 0 || where > 2) throw Error(EIO_ERR_ARG, "history location: 0 (device, host when short), 1 device, 2 host");
+    e->hist_where = where;
+}
+// 0: no history held, 1: device memory, 2: mapped host memory
+int engine_history_where(const Engine* e) {
+    const DBuf& b = e->ckpt ? e->Wq : e->W;
+    return b.cap == 0 ? 0 : (b.host ? 2 : 1);
+}
+void set_device_memory_cap(long long bytes) { g_dbuf_cap = bytes > 0 ? bytes : 0; }
+long long device_memory_used() { return g_dbuf_used.load(); }
 int engine_get_checkpoint(const Engine* e) { return e->ckpt; }
 int engine_get_graphs(const Engine* e) { return e->use_graphs ? 1 : 0; }
 size_t engine_cells(const Engine* e) { return (size_t)e->nz * e->full_nx; }
@@ -2247,7 +2302,7 @@ static void batch_source(ShotBatch& B, std::vector<PointList>& src, const Sparse
         Engine* e = B.es[i];
         const size_t wbytes = sizeof(float) * 2 * (size_t)e->nts * e->n;
         const bool fresh = e->W.cap < wbytes;
-        e->W.ensure(wbytes);
+        e->W.ensure(wbytes, e->hist_where);
         if (fresh || !e->w_clean || e->w_n != e->n) EIO_CUDA(cudaMemsetAsync(e->W.p, 0, wbytes, e->st));
         e->w_clean = true;
         e->w_n = e->n;

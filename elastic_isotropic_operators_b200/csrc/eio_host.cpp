@@ -12,6 +12,7 @@
 //   nonlinearPropElasticShotsGpu::forward/adjoint  F/src/nonlinearPropElasticShotsGpu.cpp:80-422
 //   BornElasticShotsGpu::forward/adjoint           F/src/BornElasticShotsGpu.cpp:85-378
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -118,6 +119,20 @@ void build_fdparam(const eio_fd_params& pin, const float* ep, FdParam& o) {
     o.p = p;
     const int nz = p.nz, nx = p.nx, fat = p.fat;
     const long long n = (long long)nz * nx;
+    // every cell of the medium enters the stencil: a NaN or Inf would spread through the wavefields (and
+    // pass the velocity QC below, whose comparisons are false for NaN)
+    {
+        long long bad = LLONG_MAX;
+#pragma omp parallel for reduction(min : bad) schedule(static)
+        for (long long i = 0; i < 3 * n; i++)
+            if (!std::isfinite(ep[i]) && i < bad) bad = i;
+        if (bad != LLONG_MAX) {
+            static const char* names[3] = {"rho", "lambda", "mu"};
+            const long long k = bad % n;
+            throw Error(EIO_ERR_ARG, std::string("non-finite elastic parameter ") + names[bad / n] + " at ix=" +
+                                         std::to_string(k / nz) + ", iz=" + std::to_string(k % nz));
+        }
+    }
     // velocity range, fdParamElastic.cpp:80-97 (note the reference's 2*fat upper bound)
     float vmin = 10000.f, vmax = -1.f;
     for (int ix = fat; ix < nx - 2 * fat; ix++)
@@ -381,6 +396,8 @@ struct eio_ctx {
     int batch = STEP_BATCH;   // nonlinear operators: shots per lockstep launch (1 = lanes)
     int born_batch = 1;       // Born operators: shots per lockstep group (1 = lanes, measured faster)
     std::vector<std::vector<float>> lane_tmp;   // per-lane host staging of one shot's data (kept across calls)
+    int hist_where = 0;       // source-history location policy of every lane (eio_ctx_set_history_location)
+    int check_finite = 0;     // scan host inputs and outputs of each call for NaN / Inf (eio_ctx_set_check_finite)
 };
 
 // lane k's staging buffer of at least n floats (contents undefined)
@@ -429,6 +446,7 @@ static int ensure_lanes(eio_ctx* c, int nShots, size_t lane_bytes, int want = 0)
             engine_set_graphs(e, engine_get_graphs(c->eng));
             engine_set_wait_limit(e, engine_get_wait_limit(c->eng));
             engine_set_persistent(e, engine_get_persistent(c->eng));
+            engine_set_history_where(e, c->hist_where);
             engine_share_medium(e, c->eng);   // one copy of the medium for every lane (L2)
         } catch (...) {
             engine_destroy(e);
@@ -631,6 +649,35 @@ EIO_API void eio_ctx_destroy(eio_ctx* c) {
     for (Engine* e : c->extra) engine_destroy(e);
     engine_destroy(c->eng);
     delete c;
+}
+EIO_API int eio_ctx_set_history_location(eio_ctx* c, int where) {
+    return guarded([&] {
+        if (!c) throw Error(EIO_ERR_ARG, "null context");
+        engine_set_history_where(c->eng, where);
+        for (Engine* e : c->extra) engine_set_history_where(e, where);
+        c->hist_where = where;
+    });
+}
+EIO_API int eio_ctx_get_history_location(const eio_ctx* c, int* where) {
+    return guarded([&] {
+        if (!c || !where) throw Error(EIO_ERR_ARG, "null argument");
+        *where = engine_history_where(c->eng);
+    });
+}
+EIO_API int eio_ctx_set_check_finite(eio_ctx* c, int on) {
+    return guarded([&] {
+        if (!c) throw Error(EIO_ERR_ARG, "null context");
+        c->check_finite = on ? 1 : 0;
+    });
+}
+EIO_API int eio_set_device_memory_cap(long long bytes) {
+    return guarded([&] { set_device_memory_cap(bytes); });
+}
+EIO_API int eio_get_device_memory_used(long long* bytes) {
+    return guarded([&] {
+        if (!bytes) throw Error(EIO_ERR_ARG, "null result");
+        *bytes = device_memory_used();
+    });
 }
 EIO_API int eio_ctx_set_checkpoint_precision(eio_ctx* c, int mode) {
     return guarded([&] {
@@ -1340,14 +1387,62 @@ static int nl_adjoint_impl(eio_ctx* c, int add, int nExp, int nModelExp, float* 
     });
 }
 
+// ---- optional NaN / Inf scans of a call's host inputs and outputs (eio_ctx_set_check_finite)
+struct FSpan {
+    const float* p;
+    size_t n;
+    const char* what;
+};
+static void require_finite(const FSpan& s, int code, const char* side) {
+    if (!s.p) return;
+    long long bad = LLONG_MAX;
+#pragma omp parallel for reduction(min : bad) schedule(static)
+    for (long long i = 0; i < (long long)s.n; i++)
+        if (!std::isfinite(s.p[i]) && i < bad) bad = i;
+    if (bad != LLONG_MAX)
+        throw Error(code, std::string("non-finite value in the ") + side + " " + s.what + " at element " +
+                              std::to_string(bad) + (code == EIO_ERR_NONFINITE ? " (unstable propagation?)" : ""));
+}
+// inputs rejected with EIO_ERR_ARG before the call; outputs with EIO_ERR_NONFINITE after it
+template <class In, class Call, class Out>
+static int finite_call(eio_ctx* c, In inputs, Call call, Out outputs) {
+    if (c && c->check_finite) {
+        const int rc = guarded([&] {
+            for (const FSpan& f : inputs()) require_finite(f, EIO_ERR_ARG, "input");
+        });
+        if (rc != EIO_OK) return rc;
+    }
+    int rc = call();
+    if (rc == EIO_OK && c && c->check_finite)
+        rc = guarded([&] {
+            for (const FSpan& f : outputs()) require_finite(f, EIO_ERR_NONFINITE, "output");
+        });
+    return rc;
+}
+// elements of a multi-shot call's data (nExp shots of 5 x receivers x nts) and source-model arrays
+static size_t data_elems(eio_ctx* c, eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom, int nExp) {
+    ShotGrids g = shot_grids(src, rec, nRecGeom, 0);
+    return (size_t)nExp * 5 * g.r[0]->nIrreg * c->fd.p.nts;
+}
+static size_t src_elems(eio_ctx* c, eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom, int nModelExp) {
+    ShotGrids g = shot_grids(src, rec, nRecGeom, 0);
+    return (size_t)nModelExp * 5 * g.s[0]->nIrreg * c->fd.p.nts;
+}
+
 EIO_API int eio_nl_forward(eio_ctx* c, int add, int nExp, int nModelExp, const float* model, float* data,
                            eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom) {
-    return nl_forward_impl(c, add, nExp, nModelExp, model, data, src, rec, nRecGeom, -1, nullptr);
+    return finite_call(
+        c, [&] { return std::vector<FSpan>{{model, src_elems(c, src, rec, nRecGeom, nModelExp), "source traces"}}; },
+        [&] { return nl_forward_impl(c, add, nExp, nModelExp, model, data, src, rec, nRecGeom, -1, nullptr); },
+        [&] { return std::vector<FSpan>{{data, data_elems(c, src, rec, nRecGeom, nExp), "data"}}; });
 }
 
 EIO_API int eio_nl_adjoint(eio_ctx* c, int add, int nExp, int nModelExp, float* model, const float* data,
                            eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom) {
-    return nl_adjoint_impl(c, add, nExp, nModelExp, model, data, src, rec, nRecGeom, -1, nullptr);
+    return finite_call(
+        c, [&] { return std::vector<FSpan>{{data, data_elems(c, src, rec, nRecGeom, nExp), "data"}}; },
+        [&] { return nl_adjoint_impl(c, add, nExp, nModelExp, model, data, src, rec, nRecGeom, -1, nullptr); },
+        [&] { return std::vector<FSpan>{{model, src_elems(c, src, rec, nRecGeom, nModelExp), "source traces"}}; });
 }
 
 static void check_wavefield_shot(int nExp, int wShot, const float* wfld) {
@@ -1410,7 +1505,7 @@ static void born_group(eio_ctx* c, int adj, int s0, int n, int nExp, eio_sinterp
     engine_born_shots_batch(es.data(), n, adj, sp.data(), dmv.data(), g.data(), recs.data(), dataIrreg);
 }
 
-EIO_API int eio_born_forward(eio_ctx* c, int add, int nExp, const float* model, float* data,
+static int eio_born_forward_impl(eio_ctx* c, int add, int nExp, const float* model, float* data,
                              const float* const* sigs, int nSignals, eio_sinterp* const* src, eio_sinterp* const* rec,
                              int nRecGeom) {
     return guarded([&] {
@@ -1506,7 +1601,7 @@ static void image_to_model(eio_ctx* c, int nl, float* const dm[5], std::vector<f
     }
 }
 
-EIO_API int eio_born_adjoint(eio_ctx* c, int add, int nExp, float* model, const float* data,
+static int eio_born_adjoint_impl(eio_ctx* c, int add, int nExp, float* model, const float* data,
                              const float* const* sigs, int nSignals, eio_sinterp* const* src, eio_sinterp* const* rec,
                              int nRecGeom) {
     return guarded([&] {
@@ -1608,7 +1703,7 @@ double shot_residual(void* p, const float* d, float* rt) {
 
 }  // namespace
 
-EIO_API int eio_fwi_gradient(eio_ctx* c, int nExp, int nModelExp, const float* model, const float* dobs, int nComp,
+static int eio_fwi_gradient_impl(eio_ctx* c, int nExp, int nModelExp, const float* model, const float* dobs, int nComp,
                              const int* comps, eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom,
                              float* data, float* grad, double* misfit) {
     return guarded([&] {
@@ -1672,6 +1767,39 @@ EIO_API int eio_fwi_gradient(eio_ctx* c, int nExp, int nModelExp, const float* m
 }
 
 // ------------------------------------------------------------ learned preconditioner
+
+EIO_API int eio_born_forward(eio_ctx* c, int add, int nExp, const float* model, float* data,
+                             const float* const* sigs, int nSignals, eio_sinterp* const* src, eio_sinterp* const* rec,
+                             int nRecGeom) {
+    return finite_call(
+        c, [&] { return std::vector<FSpan>{{model, (size_t)3 * c->fd.p.nz * c->fd.p.nx, "model perturbation"}}; },
+        [&] { return eio_born_forward_impl(c, add, nExp, model, data, sigs, nSignals, src, rec, nRecGeom); },
+        [&] { return std::vector<FSpan>{{data, data_elems(c, src, rec, nRecGeom, nExp), "data"}}; });
+}
+EIO_API int eio_born_adjoint(eio_ctx* c, int add, int nExp, float* model, const float* data,
+                             const float* const* sigs, int nSignals, eio_sinterp* const* src, eio_sinterp* const* rec,
+                             int nRecGeom) {
+    return finite_call(
+        c, [&] { return std::vector<FSpan>{{data, data_elems(c, src, rec, nRecGeom, nExp), "data"}}; },
+        [&] { return eio_born_adjoint_impl(c, add, nExp, model, data, sigs, nSignals, src, rec, nRecGeom); },
+        [&] { return std::vector<FSpan>{{model, (size_t)3 * c->fd.p.nz * c->fd.p.nx, "model perturbation"}}; });
+}
+EIO_API int eio_fwi_gradient(eio_ctx* c, int nExp, int nModelExp, const float* model, const float* dobs, int nComp,
+                             const int* comps, eio_sinterp* const* src, eio_sinterp* const* rec, int nRecGeom,
+                             float* data, float* grad, double* misfit) {
+    return finite_call(
+        c, [&] { return std::vector<FSpan>{}; },   // the model is the medium: always checked
+        [&] {
+            return eio_fwi_gradient_impl(c, nExp, nModelExp, model, dobs, nComp, comps, src, rec, nRecGeom, data, grad,
+                                         misfit);
+        },
+        [&] {
+            if (misfit && !std::isfinite(*misfit))
+                throw Error(EIO_ERR_NONFINITE, "non-finite misfit (unstable propagation?)");
+            return std::vector<FSpan>{{grad, (size_t)3 * c->fd.p.nz * c->fd.p.nx, "gradient"}};
+        });
+}
+
 EIO_API int eio_cnn_conv3x3(int n, int h, int w, int cin, int cout, const void* x, const void* wt, const void* mask,
                             int relu, void* y, float* y32, void* stream) {
     return guarded([&] { cnn_conv3x3(n, h, w, cin, cout, x, wt, mask, relu, y, y32, stream); });

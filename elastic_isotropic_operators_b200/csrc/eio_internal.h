@@ -153,6 +153,10 @@ void engine_born_batch_dev(Engine* const* es, int nb, int adj, float* const* ds,
                            const ShotGeom* g);
 bool engine_batchable(const Engine* e);   // sub = 1 and an FP32 history
 long long engine_step_cells(const Engine* e);
+void engine_set_history_where(Engine* e, int where);
+int engine_history_where(const Engine* e);
+void set_device_memory_cap(long long bytes);
+long long device_memory_used();
 void engine_nl_shot(Engine* e, int adj, float* const modelReg[5], const ShotGeom& g, const SInterp* const rec[4],
                     float* dataIrreg, float* wfld = nullptr);
 void engine_born_host(Engine* e, int adj, float* const srcDtw[5], float* const dm[5], float* const data[5],

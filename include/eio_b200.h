@@ -46,6 +46,8 @@ extern "C" {
 #define EIO_ERR_TIMEOUT -7 /* a bounded device wait gave up: that call's output is incomplete; the kernel
                               drained its copies before returning, so the context stays usable (the
                               reference exits the process on any CUDA error, F/src/cudaErrors.cu:4-29) */
+#define EIO_ERR_NONFINITE -8 /* a call's output holds NaN / Inf (an unstable propagation); only with
+                              eio_ctx_set_check_finite on */
 
 typedef struct eio_sinterp eio_sinterp;
 typedef struct eio_ctx eio_ctx;
@@ -126,6 +128,31 @@ int eio_ctx_create(const eio_fd_params *p, const float *elasticParam, int device
 /* setBackground: rebuild the medium (QC may fail) (PF/pyElastic_iso_float_nl.cpp:48) */
 int eio_ctx_set_background(eio_ctx *c, const float *elasticParam);
 void eio_ctx_destroy(eio_ctx *c);
+/* Where the Born operators' source-wavefield history lives (the reference
+ * streams it to host RAM when it is large, useStreams = 1,
+ * F/src/BornElasticGpuFunctions.cu:850-1096): 0 (default) = device memory, or,
+ * when the device allocation fails, pinned host memory mapped into the device
+ * address space (the kernels write and read it across the host link: slower,
+ * same results); 1 = device only (EIO_ERR_NOMEM when it does not fit);
+ * 2 = mapped host memory.  eio_ctx_get_history_location: 0 = none held yet,
+ * 1 = device, 2 = host. */
+int eio_ctx_set_history_location(eio_ctx *c, int where);
+int eio_ctx_get_history_location(const eio_ctx *c, int *where);
+/* NaN / Inf checks.  The elastic parameters are always checked at
+ * eio_ctx_create / eio_ctx_set_background (EIO_ERR_ARG naming the parameter and
+ * cell).  With on != 0 every eio_nl_forward / eio_nl_adjoint / eio_born_forward /
+ * eio_born_adjoint / eio_fwi_gradient call also scans its host inputs
+ * (EIO_ERR_ARG before any work) and its outputs (EIO_ERR_NONFINITE after the
+ * propagation, e.g. an unstable model); off by default (a pass over the
+ * arrays on the host). */
+int eio_ctx_set_check_finite(eio_ctx *c, int on);
+/* A process-wide cap on the device memory the library's own buffers may hold
+ * (bytes; 0 = none), and the bytes they hold now: an allocation above the cap
+ * fails as if the device were full (EIO_ERR_NOMEM, or the host-memory history
+ * above), so callers can reserve memory for others and tests can produce
+ * out-of-memory on purpose. */
+int eio_set_device_memory_cap(long long bytes);
+int eio_get_device_memory_used(long long *bytes);
 /* Source-wavefield snapshot storage for the Born operators (no reference
  * counterpart; the reference keeps FP32 snapshots): 0 = FP32 (bit-faithful to
  * the reference), 1 = BF16, 2 = FP16, both as 16-bit codes with one scale per

@@ -126,6 +126,32 @@ def test_qc_errors_come_back_as_status(small_case):
     assert st == -2 and b"SUB_MAX" in L.eio_last_error()
 
 
+@pytest.mark.parametrize("param,ix,iz,value", [(0, 0, 0, np.nan), (1, 50, 30, np.inf), (2, 103, 71, -np.inf)])
+def test_non_finite_medium_is_rejected_with_its_cell(small_case, param, ix, iz, value):
+    """A NaN or Inf anywhere in the elastic parameters (pads included: every
+    cell enters the stencil) is an argument error naming the parameter and the
+    cell, before the QC (whose comparisons a NaN would slip through)."""
+    w = small_case
+    L = _lib.lib()
+    ep = np.ascontiguousarray(w.elastic.getNdArray(), np.float32).copy()
+    ep[param, ix, iz] = value
+    out = [np.zeros((w.nx, w.nz), np.float32) for _ in range(5)]
+    fd = prop.fd_params_from_par(w.par, w.elastic)
+    st = L.eio_medium_prepare(ctypes.byref(fd), _lib.fptr(ep), *[_lib.fptr(o) for o in out])
+    msg = L.eio_last_error().decode()
+    assert st == -1, msg
+    assert ("rho", "lambda", "mu")[param] in msg and "ix=%d, iz=%d" % (ix, iz) in msg
+
+
+def test_device_memory_cap_is_process_wide_and_host_only_to_set():
+    L = _lib.lib()
+    used = ctypes.c_longlong(-1)
+    _lib.check(L.eio_get_device_memory_used(ctypes.byref(used)))
+    assert used.value >= 0
+    _lib.check(L.eio_set_device_memory_cap(1 << 20))
+    _lib.check(L.eio_set_device_memory_cap(0))
+
+
 def test_no_cpu_fallback_without_gpu(small_case):
     """Without a usable CUDA device the engine fails loudly (no CPU path)."""
     import torch
