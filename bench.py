@@ -83,6 +83,9 @@ def parse():
                          "-1 keeps the library default (mma.sync)")
     ap.add_argument("--epochs", type=int, default=80, help="fwi_learned: training epochs")
     ap.add_argument("--depth", type=int, default=6, help="fwi_learned: convolution layers of the ConvNet")
+    ap.add_argument("--tma", type=int, default=None, choices=[0, 1, 2, 3],
+                    help="cnn_train (U-Net): 0 copy-loop convolution kernel, 1 TMA kernel with one CTA per SM, "
+                         "2 with up to two, 3 with up to four (the library's default)")
     ap.add_argument("--net", default=None, choices=["unet", "convnet"],
                     help="preconditioner network: the four-level U-Net (cnn_train default) or the plain ConvNet "
                          "(fwi_learned default)")
@@ -1216,6 +1219,8 @@ def run_ours_cnn(args, ws, rank, local):
     batch = args.shots or 16
     h = w = 256
     unet = (args.net or "unet") == "unet"
+    if args.tma is not None:
+        _lib.check(_lib.lib().eio_unet_set_tma(args.tma))
     net = precond.UNet(device=local, seed=0) if unet else precond.ConvNet(depth=6, hidden=32, device=local, seed=0)
     g = torch.Generator(device=dev)
     g.manual_seed(1)
@@ -1272,7 +1277,8 @@ def run_ours_cnn(args, ws, rank, local):
     if unet:
         desc = ("cnn_train: %d patches of 256x256 per step, U-Net 32/64/128/256 channels (%d parameters), "
                 "2x2 average pooling, nearest upsampling, concatenated skips" % (batch, net.n_params()))
-        kern = "k_gemm_tc (tcgen05, TMEM accumulators; implicit 3x3 gathers) for forward, data and weight gradients"
+        kern = ("k_conv_tma (tcgen05, TMA-fed implicit GEMM, up to 4 CTAs per SM) for forward, data and weight "
+                "gradients")
     else:
         desc = "cnn_train: %d patches of 256x256 per step, 6 conv layers 16-32-32-32-32-32-16" % batch
         kern = (("k_conv3_tc (tcgen05, TMEM accumulator)" if path.value == 1 else

@@ -721,12 +721,16 @@ struct ConvTma {
     long long wait;
 };
 
-template <int BN>
+// CPS CTAs per SM (1, 2, 3 or 4): fewer stages each, and every CTA's TMEM
+// allocation fits next to the others' (BN <= 128 for 2, <= 64 for 3 and 4);
+// more CTAs keep more copies in flight per SM, which the small-channel
+// layers' short box rows need
+template <int BN, int CPS = 1>
 struct TCfg {
     static constexpr int A_BYTES = 16384;
     static constexpr int B_BYTES = BN * 128;
     static constexpr int STAGE = A_BYTES + B_BYTES;        // multiple of 1024
-    static constexpr int S0 = (200 * 1024) / STAGE;
+    static constexpr int S0 = ((CPS == 1 ? 200 : CPS == 2 ? 96 : CPS == 3 ? 64 : 46) * 1024) / STAGE;
     static constexpr int STAGES = S0 > 8 ? 8 : S0;
     static constexpr int COLS = BN < 32 ? 32 : BN;          // TMEM columns of one accumulator buffer
     static constexpr int TALLOC = 2 * COLS <= 64 ? 64 : 2 * COLS <= 128 ? 128 : 2 * COLS <= 256 ? 256 : 512;
@@ -795,12 +799,14 @@ __device__ __forceinline__ void t_commit(unsigned bar)
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
-template <int BN>
-__global__ void __launch_bounds__(T_THREADS, 1) k_conv_tma(const __grid_constant__ CUtensorMap ta,
-                                                          const __grid_constant__ CUtensorMap tb,
-                                                          const __grid_constant__ ConvTma g)
+template <int BN, int CPS>
+__global__ void __launch_bounds__(T_THREADS, CPS) k_conv_tma(const __grid_constant__ CUtensorMap ta,
+                                                            const __grid_constant__ CUtensorMap tb,
+                                                            const __grid_constant__ ConvTma g)
 {
-    using Cf = TCfg<BN>;
+    using Cf = TCfg<BN, CPS>;
+    static_assert(Cf::STAGES >= 2, "at least two stages");
+    static_assert(Cf::TALLOC * CPS <= 512, "the CTAs of an SM share its 512 TMEM columns");
     constexpr int S = Cf::STAGES;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     const unsigned raw = g_smem(smem_raw);
@@ -1108,7 +1114,7 @@ void conv_geometry(int n, int h, int w, int cin, int cout)
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-int g_use_tma = 1;
+int g_use_tma = 3;   // TMA kernel, up to four CTAs per SM where the tile width allows
 
 EncodeTiledFn tma_encoder()
 {
@@ -1165,7 +1171,7 @@ int tma_bn(long long n)
     return 192;
 }
 
-template <int BN>
+template <int BN, int CPS>
 void launch_tma(const CUtensorMap& ta, const CUtensorMap& tb, const ConvTma& a, cudaStream_t st)
 {
     static int opened[64] = {};
@@ -1173,24 +1179,58 @@ void launch_tma(const CUtensorMap& ta, const CUtensorMap& tb, const ConvTma& a, 
     GCUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) throw Error(EIO_ERR_ARG, "device index above 63");
     if (!opened[dev]) {
-        GCUDA(cudaFuncSetAttribute(k_conv_tma<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, TCfg<BN>::SMEM));
+        GCUDA(cudaFuncSetAttribute(k_conv_tma<BN, CPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   TCfg<BN, CPS>::SMEM));
         opened[dev] = 1;
     }
     const long long tiles = (long long)a.mt * a.nt * a.splits;
-    k_conv_tma<BN><<<(unsigned)std::min<long long>(tiles, g_sms()), T_THREADS, TCfg<BN>::SMEM, st>>>(ta, tb, a);
+    const long long ctas = std::min<long long>(tiles, (long long)CPS * g_sms());
+    k_conv_tma<BN, CPS><<<(unsigned)ctas, T_THREADS, TCfg<BN, CPS>::SMEM, st>>>(ta, tb, a);
     GCUDA(cudaGetLastError());
 }
+// tile widths each CTA count takes: 4 per SM up to 32 columns, 3 up to 64, 2 up to 128
+template <int CPS>
+bool launch_tma_cps(int bn, const CUtensorMap& ta, const CUtensorMap& tb, const ConvTma& a, cudaStream_t st)
+{
+    constexpr int maxbn = CPS == 4 ? 32 : CPS == 3 ? 64 : CPS == 2 ? 128 : 256;
+    if (bn > maxbn) return false;
+    if (bn == 16) {
+        launch_tma<16, CPS>(ta, tb, a, st);
+        return true;
+    }
+    if (bn == 32) {
+        launch_tma<32, CPS>(ta, tb, a, st);
+        return true;
+    }
+    if constexpr (maxbn >= 64) {
+        if (bn == 64) {
+            launch_tma<64, CPS>(ta, tb, a, st);
+            return true;
+        }
+    }
+    if constexpr (maxbn >= 128) {
+        if (bn == 96) {
+            launch_tma<96, CPS>(ta, tb, a, st);
+            return true;
+        }
+        if (bn == 128) {
+            launch_tma<128, CPS>(ta, tb, a, st);
+            return true;
+        }
+    }
+    if constexpr (maxbn >= 256) {
+        if (bn == 192) launch_tma<192, CPS>(ta, tb, a, st);
+        else launch_tma<256, CPS>(ta, tb, a, st);
+        return true;
+    }
+    return false;
+}
+// g_use_tma: 1 one CTA per SM; 2 up to two; 3 up to four (as many as the tile width allows)
 void launch_tma_any(int bn, const CUtensorMap& ta, const CUtensorMap& tb, const ConvTma& a, cudaStream_t st)
 {
-    switch (bn) {
-        case 16: launch_tma<16>(ta, tb, a, st); break;
-        case 32: launch_tma<32>(ta, tb, a, st); break;
-        case 64: launch_tma<64>(ta, tb, a, st); break;
-        case 96: launch_tma<96>(ta, tb, a, st); break;
-        case 128: launch_tma<128>(ta, tb, a, st); break;
-        case 192: launch_tma<192>(ta, tb, a, st); break;
-        default: launch_tma<256>(ta, tb, a, st); break;
-    }
+    if (g_use_tma >= 3 && (launch_tma_cps<4>(bn, ta, tb, a, st) || launch_tma_cps<3>(bn, ta, tb, a, st))) return;
+    if (g_use_tma >= 2 && launch_tma_cps<2>(bn, ta, tb, a, st)) return;
+    launch_tma_cps<1>(bn, ta, tb, a, st);
 }
 
 // eligibility and splits of the two TMA forms
@@ -1264,7 +1304,12 @@ void gemm_bf16(long long M, long long N, long long K, const void* A, long long l
 
 void gemm_set_wait_limit(long long polls) { g_gemm_wait = polls < 0 ? G_WAIT : polls; }
 
-void unet_set_tma(int on) { g_use_tma = on ? 1 : 0; }
+void unet_set_tma(int on)
+{
+    if (on < 0 || on > 3)
+        throw Error(EIO_ERR_ARG, "TMA mode: 0 copy loop, 1 TMA, 2 up to two CTAs per SM, 3 up to four");
+    g_use_tma = on;
+}
 int unet_get_tma() { return g_use_tma; }
 
 int gemm_status(int reset)

@@ -511,7 +511,10 @@ int eio_gemm_status(int reset, int *err);
  * multiple of 16; for the weight gradient cout a multiple of 16, <= 256):
  * one 4-D tensor box per tap and channel block, the zero padding from the
  * box's out-of-bounds fill.  Other shapes use the copy-loop kernel.  on = 0
- * forces the copy loop everywhere (process-wide; default 1). */
+ * forces the copy loop everywhere; 1 runs the TMA kernel with one CTA per SM,
+ * 2 with up to two (tiles up to 128 columns), 3 (default) with up to four
+ * (three for 64-column tiles, four up to 32): fewer stages each, more copies
+ * in flight per SM.  Process-wide. */
 int eio_unet_set_tma(int on);
 int eio_unet_get_tma(int *on);
 /* 3x3 convolution (zero padding) as an implicit GEMM on tcgen05: y[p][co] =

@@ -170,7 +170,8 @@ def test_conv3x3_tma_path_matches_numpy_and_the_copy_loop(n, h, w, cin, cout):
     channel block, zero padding from the out-of-bounds fill): the convolution
     against FP64 to 1e-5 and bitwise equal to the copy-loop kernel (the same K
     order); the weight gradient against FP64 to 1e-5 and the copy loop to 1e-6
-    (the pixels are split differently)."""
+    (the pixels are split differently); the launches with up to two and four CTAs
+    per SM (modes 2, 3) bitwise equal to mode 1."""
     rng = np.random.default_rng(n + 10 * h + w + cin + cout)
     x = C.bf16_round(rng.standard_normal((n, h, w, cin)))
     wt = C.bf16_round(rng.standard_normal((cout, 9, cin)) / np.sqrt(9 * cin))
@@ -181,8 +182,10 @@ def test_conv3x3_tma_path_matches_numpy_and_the_copy_loop(n, h, w, cin, cout):
     _lib.check(L.eio_unet_wgrad_scratch(n, h, w, cin, cout, ctypes.byref(f)))
     scratch = torch.empty((f.value,), dtype=torch.float32, device="cuda")
     out = {}
+    mode = ctypes.c_int()
+    _lib.check(L.eio_unet_get_tma(ctypes.byref(mode)))
     try:
-        for on in (1, 0):
+        for on in (1, 2, 3, 0):
             _tma(on)
             y32 = torch.empty((n, h, w, cout), dtype=torch.float32, device="cuda")
             y16 = torch.empty((n, h, w, cout), dtype=torch.bfloat16, device="cuda")
@@ -193,7 +196,7 @@ def test_conv3x3_tma_path_matches_numpy_and_the_copy_loop(n, h, w, cin, cout):
             torch.cuda.synchronize()
             out[on] = (y32.cpu().numpy(), _np(y16), dw.cpu().numpy())
     finally:
-        _tma(1)
+        _tma(mode.value)
     assert _status_clear() == 0
     want = np.maximum(C._conv(x, wt), 0.0)
     assert _rel(out[1][0], want) < 1e-5
@@ -201,6 +204,9 @@ def test_conv3x3_tma_path_matches_numpy_and_the_copy_loop(n, h, w, cin, cout):
     assert np.array_equal(out[1][1], C.bf16_round(out[1][0]))
     assert _rel(out[1][2], C._wgrad(x, dz)) < 1e-5
     assert _rel(out[1][2], out[0][2]) < 1e-6
+    # two or four CTAs per SM: the same tiles and splits, the same bits
+    for on in (2, 3):
+        assert all(np.array_equal(a, b) for a, b in zip(out[on], out[1]))
 
 
 def test_flip():
