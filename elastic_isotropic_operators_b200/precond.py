@@ -34,7 +34,7 @@ import numpy as np
 from . import _lib
 from ._lib import check
 
-__all__ = ["ConvNet", "UNet", "unet_channels", "LearnedPreconditioner", "smooth_perturbation"]
+__all__ = ["ConvNet", "UNet", "unet_channels", "unet_pad_shape", "LearnedPreconditioner", "smooth_perturbation"]
 
 _CIN = 16    # input channels of the first layer (4 features used)
 _COUT = 16   # output channels of the last layer (3 used)
@@ -167,6 +167,33 @@ class ConvNet:
             self.wb[l].copy_(self.w32[l].to(torch.bfloat16))
 
 
+def _tma_level_ok(h, w):
+    """The U-Net kernels' TMA boxes tile an h x w image: 128-pixel convolution
+    tiles and 64-pixel weight-gradient slices are rectangles of it (widths that
+    are multiples of the box or divide it, heights the rectangle divides)."""
+    for px in (128, 64):
+        if w % px and not (px % w == 0 and h % (px // w) == 0):
+            return False
+    return True
+
+
+def unet_pad_shape(h, w, levels=4, slack=0.15):
+    """(h', w') >= (h, w), multiples of 2^(levels-1): the smallest such shape
+    within ``slack`` more pixels whose every level (h / 2^l, w / 2^l) the TMA
+    kernels tile (e.g. 3400 x 1000 -> 3400 x 1024); else the sizes rounded up to
+    the multiple (the copy-loop kernel takes those)."""
+    m = 1 << (levels - 1)
+    h0, w0 = -(-h // m) * m, -(-w // m) * m
+    best = None
+    for hh in range(h0, int(h * (1 + slack)) + 1, m):
+        for ww in range(w0, int(w * (1 + slack)) + 1, m):
+            if hh * ww > (1 + slack) * h * w or (best is not None and hh * ww >= best[0] * best[1]):
+                continue
+            if all(_tma_level_ok(hh >> l, ww >> l) for l in range(levels)):
+                best = (hh, ww)
+    return best if best is not None else (h0, w0)
+
+
 def unet_channels(base=32):
     """(cin, cout) of the U-Net's eleven 3x3 convolutions: two per encoder level
     (base, 2 base, 4 base channels), the bottleneck (8 base), one per decoder
@@ -223,6 +250,11 @@ class UNet:
         self._shape = None
         self._loss = torch.zeros(1, dtype=torch.float64, device=self.dev)
         self._part = torch.zeros(1024, dtype=torch.float64, device=self.dev)
+
+    @staticmethod
+    def pad_shape(h, w):
+        """The image size the network runs an h x w image at (unet_pad_shape)."""
+        return unet_pad_shape(h, w)
 
     def n_params(self):
         return int(sum(w.numel() for w in self.w32))
@@ -496,10 +528,15 @@ class LearnedPreconditioner:
         return X, T, S, D
 
     def _pad(self, a):
-        """[n][nx][nz][c] with zero rows / columns appended up to the network's
-        size multiple (the U-Net's pooling levels); outputs are cut back."""
-        mult = getattr(self.net, "multiple", 1)
-        px, pz = (-a.shape[1]) % mult, (-a.shape[2]) % mult
+        """[n][nx][nz][c] with zero rows / columns appended up to the size the
+        network runs at (its size multiple; for the U-Net, a few percent more
+        where that lets its TMA kernels tile every level); outputs are cut back."""
+        if hasattr(self.net, "pad_shape"):
+            hh, ww = self.net.pad_shape(a.shape[1], a.shape[2])
+            px, pz = hh - a.shape[1], ww - a.shape[2]
+        else:
+            mult = getattr(self.net, "multiple", 1)
+            px, pz = (-a.shape[1]) % mult, (-a.shape[2]) % mult
         return np.pad(a, ((0, 0), (0, px), (0, pz), (0, 0))) if px or pz else a
 
     # ------------------------------------------------------------ training
