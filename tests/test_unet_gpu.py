@@ -387,3 +387,38 @@ def test_unet_rejects_sizes_off_its_multiple():
     net = precond.UNet(base=16)
     with pytest.raises(ValueError):
         net.forward(torch.zeros((1, 36, 64, 16), dtype=torch.bfloat16, device="cuda"))
+
+
+def test_unet_runs_fwi_shaped_images_at_their_tma_size():
+    """A 40 x 1000 image (the FWI grid's 1000-cell depth) runs at the padded
+    size unet_pad_shape picks, 40 x 1024, where every level is on the TMA
+    kernels: the whole network's output is bitwise that of the copy-loop
+    kernel at the same size, its weight gradients within 1e-6 (the pixels are
+    split differently)."""
+    from elastic_isotropic_operators_b200 import precond
+    h, w = precond.unet_pad_shape(40, 1000)
+    assert (h, w) == (40, 1024)
+    rng = np.random.default_rng(12)
+    x = np.zeros((1, h, w, 16), np.float32)
+    x[..., :4] = rng.standard_normal((1, h, w, 4))
+    X = _bf(C.bf16_round(x))
+    T = torch.as_tensor(rng.standard_normal((1, h, w, 3)).astype(np.float32), device="cuda")
+    L = _lib.lib()
+    mode = ctypes.c_int()
+    _lib.check(L.eio_unet_get_tma(ctypes.byref(mode)))
+    out = {}
+    try:
+        for on in (mode.value, 0):
+            _tma(on)
+            net = precond.UNet(seed=2)
+            y = net.forward(X).clone()
+            loss = float(net.backward(T).item())
+            torch.cuda.synchronize()
+            out[on] = (y.cpu().numpy(), loss, [d.cpu().numpy() for d in net.dw])
+    finally:
+        _tma(mode.value)
+    assert _status_clear() == 0
+    a, b = out[mode.value], out[0]
+    assert np.isfinite(a[0]).all() and np.array_equal(a[0], b[0])
+    assert a[1] == b[1]
+    assert max(_rel(p, q) for p, q in zip(a[2], b[2])) < 1e-6
